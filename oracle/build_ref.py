@@ -1,0 +1,268 @@
+#!/usr/bin/env python3
+"""Build recipe for the reference HARM binary used as the pinning oracle.
+
+Test infrastructure only.  It copies the reference C sources from the
+read-only reference tree into a scratch directory OUTSIDE this repository,
+applies two mechanical compatibility patches and a problem/config overlay,
+swaps the reference main.c for oracle/ref_harness.c, and compiles with gcc.
+Only the resulting executable is written, into oracle/_ref/ (git-ignored).
+
+Mechanical patches (the reference targets icc):
+  (a) block-scope ``static`` function prototypes are hoisted to file scope
+      (gcc rejects them: "invalid storage class"); files: utoprim_jon.c,
+      utoprim_jon_eos.c, u2p_util.c, utoprim_2d_final.c, utoprim_1d_final.c,
+      utoprim_5d2_final.c, dudp_calc.c.
+  (b) mpi_fileio.c:1978-2035 reuse one va_list across several vfprintf calls
+      (undefined behaviour on x86-64); each call gets its own va_copy.
+  (c) initbase.c:95-99 dumps the never-filled panalytic array at init; its
+      wave-speed diagnostic hits myexit(10001) on the zeros (vchar.c:279).
+      The dump is diagnostic output only, so the harness build skips it.
+
+Config overlay (settings only, no algorithm change): the FM torus problem
+file init.fishmon.c / init.fishmon.h / bounds.fishmon.c with
+  EOMTYPE EOMGRMHD (init.fishmon.h:170 has EOMFFDE), defcoord=LOGRSINTH
+  (init.fishmon.c:73 has 9), UTOPRIMVERSION=UTOPRIM2DFINAL
+  (init.fishmon.c:46), lim/fluxmethod/cour as requested, TIMEORDER=2,
+  DOENOFLUX=NOENOFLUX, rescaletype=0 (r^-1.5 / r^-2.5 floors), N1/N2/N3.
+
+usage: python oracle/build_ref.py --n1 64 --n2 64 --n3 1 --lim MC --flux HLL
+"""
+import argparse
+import os
+import re
+import shutil
+import subprocess
+import sys
+import tempfile
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+OUT = os.path.join(HERE, "_ref")
+DEFAULT_REF = "/root/reference"
+
+HOIST_FILES = ["utoprim_jon.c", "utoprim_jon_eos.c", "u2p_util.c", "utoprim_2d_final.c",
+               "utoprim_1d_final.c", "utoprim_5d2_final.c", "dudp_calc.c"]
+
+# maketail.harm.inc:185-232 (SRCSMANYPOINTS + SRCSONEPOINT); main.c replaced by the harness
+SOURCES = """init.c initbase.c restart.c set_arrays.c set_grid.c
+advance.c reconstructeno.c flux.c wavespeeds.c boundsflux.c fluxct.c fluxcompute.c
+bounds.c boundsint.c diag.c dump.c dumpgen.c dump_ener.c image.c fail.c fixup.c
+mpi_init.c mpi_fileio.c boundmpi.c boundmpiint.c
+interppoint.c interpline.c monointerp.c jmonointerp.c smonointerp.c
+metric.c coord.c phys.c step_ch.c phys.ffde.c phys.coldgrmhd.c eos.c
+vchar.c transforms.c sources.c gaussj.c lubksb.c ludcmp.c mnewt.c nrutil.c ranc.c tensor.c
+utoprimgen.c dudp_calc_3vel.c dudp_calc.c utoprim.c utoprim_2d.c utoprim_1d.c
+utoprim_1d_opt.c utoprim_ldz.c utoprim_jon.c utoprim_1d_final.c utoprim_2d_final.c
+utoprim_5d2_final.c freespace.c""".split()
+
+LIMS = {"DONOR": "DONOR", "MC": "MC", "PARA": "PARA", "WENO5": "WENO5", "MINM": "MINM", "VANL": "VANL"}
+FLUXES = {"HLL": "HLLFLUX", "LAXF": "LAXFFLUX"}
+
+
+def hoist_block_statics(text):
+    """Move block-scope `static <type> name(...);` prototypes to file scope."""
+    lines = text.split("\n")
+    depth = 0
+    out = []
+    hoisted = []
+    seen = set()
+    i = 0
+    in_comment = False
+    while i < len(lines):
+        line = lines[i]
+        stripped = line.strip()
+        if depth > 0 and not in_comment and re.match(r"static\s+[A-Za-z_]", stripped) and "(" in stripped \
+                and "=" not in stripped.split("(")[0]:
+            # gather a possibly multi-line prototype up to ';' (must not open a body)
+            j = i
+            buf = [lines[j]]
+            while ";" not in lines[j] and "{" not in lines[j] and j + 1 < len(lines):
+                j += 1
+                buf.append(lines[j])
+            joined = " ".join(b.strip() for b in buf)
+            if ";" in joined and "{" not in joined:
+                key = re.sub(r"\s+", " ", joined)
+                if key not in seen:
+                    seen.add(key)
+                    hoisted.append(joined)
+                out.extend([""] * len(buf))
+                i = j + 1
+                continue
+        # brace depth tracking (ignores braces inside // and /* */ comments and strings)
+        k = 0
+        s = line
+        in_str = False
+        while k < len(s):
+            c = s[k]
+            if in_comment:
+                if s.startswith("*/", k):
+                    in_comment = False
+                    k += 2
+                    continue
+                k += 1
+                continue
+            if in_str:
+                if c == "\\":
+                    k += 2
+                    continue
+                if c == '"':
+                    in_str = False
+                k += 1
+                continue
+            if s.startswith("//", k):
+                break
+            if s.startswith("/*", k):
+                in_comment = True
+                k += 2
+                continue
+            if c == '"':
+                in_str = True
+            elif c == "'":
+                k += 3 if k + 2 < len(s) and s[k + 2] == "'" else 1
+                continue
+            elif c == "{":
+                depth += 1
+            elif c == "}":
+                depth -= 1
+            k += 1
+        out.append(line)
+        i += 1
+    if not hoisted:
+        return text, 0
+    # insert after the last #include/#define that precedes the first '{' of the file
+    first_brace = next((n for n, l in enumerate(out) if "{" in l and not l.strip().startswith("//")), len(out))
+    ins = 0
+    for n in range(first_brace):
+        if out[n].strip().startswith("#include") or out[n].strip().startswith("#define"):
+            ins = n + 1
+    block = ["/* prototypes hoisted to file scope by oracle/build_ref.py */"] + hoisted
+    out = out[:ins] + block + out[ins:]
+    return "\n".join(out), len(hoisted)
+
+
+def patch_va_copy(text):
+    pat = re.compile(r"vfprintf\s*\(\s*([A-Za-z_]+)\s*,\s*format\s*,\s*arglist\s*\)\s*;")
+    new, n = pat.subn(r"{ va_list ac__; va_copy(ac__, arglist); vfprintf(\1, format, ac__); va_end(ac__); }", text)
+    return new, n
+
+
+def sub_once(text, old, new, count=1, where=""):
+    n = text.count(old)
+    if n != count:
+        raise SystemExit(f"overlay: expected {count} occurrence(s) of {old!r} in {where}, found {n}")
+    return text.replace(old, new)
+
+
+def overlay_init_h(text, n1, n2, n3, maxbnd):
+    text = sub_once(text, "#define EOMTYPE EOMFFDE", "#define EOMTYPE EOMGRMHD", where="init.fishmon.h")
+    text = sub_once(text, "#define N1 64", f"#define N1 {n1}", where="init.fishmon.h")
+    text = sub_once(text, "#define N2 64", f"#define N2 {n2}", where="init.fishmon.h")
+    text = sub_once(text, "#define N3 1", f"#define N3 {n3}", where="init.fishmon.h")
+    text = sub_once(text, "#define MAXBND 11", f"#define MAXBND {maxbnd}", where="init.fishmon.h")
+    return text
+
+
+def overlay_init_c(text, lim, flux, cour):
+    w = "init.fishmon.c"
+    text = sub_once(text, "  defcoord = 9;", "  defcoord = LOGRSINTH;", where=w)
+    text = sub_once(text, "  UTOPRIMVERSION = UTOPRIMJONNONRELCOMPAT;", "  UTOPRIMVERSION = UTOPRIM2DFINAL;", where=w)
+    text = sub_once(text, "  lim = PARA;", f"  lim = {LIMS[lim]};", where=w)
+    text = sub_once(text, "  TIMEORDER=4;", "  TIMEORDER=2;", where=w)
+    text = sub_once(text, "  DOENOFLUX = ENOFINITEVOLUME;", "  DOENOFLUX = NOENOFLUX;", count=2, where=w)
+    text = sub_once(text, "  fluxmethod=HLLFLUX;", f"  fluxmethod={FLUXES[flux]};", where=w)
+    text = sub_once(text, "  rescaletype=1;", "  rescaletype=0;", where=w)
+    text = sub_once(text, "  cour=0.8;", f"  cour={cour!r};", where=w)
+    return text
+
+
+AFTER_MPI_STUB = """
+
+/* bounds.fishmon.c has no bound_prim_user_after_mpi(); step_ch.c:bound_prim()
+   calls one after bound_mpi().  With USEMPI=0 it has nothing to do. */
+int bound_prim_user_after_mpi(int boundstage, FTYPE prim[][N2M][N3M][NPR])
+{
+  return(0);
+}
+"""
+
+
+def build(ref, n1, n2, n3, lim, flux, cour, maxbnd, name=None, keep=False, verbose=False):
+    os.makedirs(OUT, exist_ok=True)
+    name = name or f"harm_ref_{n1}x{n2}x{n3}_{lim}_{flux}"
+    scratch = tempfile.mkdtemp(prefix="harmref_")
+    try:
+        for fn in os.listdir(ref):
+            if fn.endswith(".c") or fn.endswith(".h"):
+                shutil.copy(os.path.join(ref, fn), os.path.join(scratch, fn))
+        for fn in HOIST_FILES:
+            p = os.path.join(scratch, fn)
+            with open(p) as f:
+                t = f.read()
+            t, n = hoist_block_statics(t)
+            with open(p, "w") as f:
+                f.write(t)
+            if verbose:
+                print(f"hoisted {n} prototypes in {fn}")
+        p = os.path.join(scratch, "mpi_fileio.c")
+        with open(p) as f:
+            t = f.read()
+        t, n = patch_va_copy(t)
+        if n < 6:
+            raise SystemExit(f"va_copy patch matched {n} calls, expected >= 6")
+        with open(p, "w") as f:
+            f.write(t)
+        p = os.path.join(scratch, "initbase.c")
+        with open(p) as f:
+            t = f.read()
+        t = sub_once(t, "    if (dump(9999) >= 1){", "    if (0 && dump(9999) >= 1){", where="initbase.c")
+        with open(p, "w") as f:
+            f.write(t)
+        # problem overlay
+        with open(os.path.join(ref, "init.fishmon.h")) as f:
+            ih = overlay_init_h(f.read(), n1, n2, n3, maxbnd)
+        with open(os.path.join(scratch, "init.h"), "w") as f:
+            f.write(ih)
+        with open(os.path.join(ref, "init.fishmon.c")) as f:
+            ic = overlay_init_c(f.read(), lim, flux, cour)
+        with open(os.path.join(scratch, "init.c"), "w") as f:
+            f.write(ic)
+        with open(os.path.join(ref, "bounds.fishmon.c")) as f:
+            bc = f.read() + AFTER_MPI_STUB
+        with open(os.path.join(scratch, "bounds.c"), "w") as f:
+            f.write(bc)
+        shutil.copy(os.path.join(HERE, "ref_harness.c"), os.path.join(scratch, "ref_harness.c"))
+        srcs = SOURCES + ["ref_harness.c"]
+        exe = os.path.join(OUT, name)
+        cmd = ["gcc", "-O2", "-ffp-contract=off", "-fno-fast-math", "-fcommon", "-w",
+               "-mcmodel=medium", "-o", exe] + srcs + ["-lm"]
+        r = subprocess.run(cmd, cwd=scratch, capture_output=True, text=True)
+        if r.returncode != 0:
+            sys.stderr.write(r.stderr[-6000:])
+            raise SystemExit(f"reference build failed (scratch kept at {scratch})")
+        if verbose:
+            print("built", exe)
+        return exe
+    finally:
+        if not keep:
+            shutil.rmtree(scratch, ignore_errors=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--ref", default=os.environ.get("HARM_REFERENCE_DIR", DEFAULT_REF))
+    ap.add_argument("--n1", type=int, default=64)
+    ap.add_argument("--n2", type=int, default=64)
+    ap.add_argument("--n3", type=int, default=1)
+    ap.add_argument("--lim", default="MC", choices=sorted(LIMS))
+    ap.add_argument("--flux", default="HLL", choices=sorted(FLUXES))
+    ap.add_argument("--cour", type=float, default=0.8)
+    ap.add_argument("--maxbnd", type=int, default=11)
+    ap.add_argument("--name", default=None)
+    ap.add_argument("--keep", action="store_true")
+    a = ap.parse_args()
+    if not os.path.isdir(a.ref):
+        raise SystemExit(f"reference tree not found: {a.ref}")
+    build(a.ref, a.n1, a.n2, a.n3, a.lim, a.flux, a.cour, a.maxbnd, a.name, a.keep, verbose=True)
+
+
+if __name__ == "__main__":
+    main()

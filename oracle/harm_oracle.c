@@ -1,0 +1,1564 @@
+/*
+ * harm_oracle.c -- CPU restatement of HARM's per-zone conservative update.
+ *
+ * TEST INFRASTRUCTURE ONLY.  This file is the parity checker for the CUDA
+ * path in harm_finalwham_b200/csrc.  Only tests/, __graft_entry__.smoke() and
+ * bench.py's cpu_baseline leg may load it, and only to check or to time the
+ * CPU baseline; the product never links it.
+ *
+ * It restates, in the reference's own floating-point operation order (so
+ * that with gcc -O2 -ffp-contract=off results are bit-identical to the
+ * reference build in oracle/_ref), the path
+ *
+ *   step_ch_simplempi (step_ch.c:35-252, midpoint RK2 tables :504-524)
+ *     pre_fixup          (fixup.c:25; flags only, no effect on state here)
+ *     advance_standard   (advance.c:58-238)
+ *       fluxcalc         (flux.c:7-318), fluxcalc_standard (flux.c:469-680)
+ *         MC slopes      (interppoint.c:387-397, getp2interplr flux.c:753-810)
+ *         p2SFUevolve    (fluxcompute.c:57-65), get_wavespeeds (wavespeeds.c:12)
+ *         vchar/simplefast (vchar.c:37-312), cminmax_calc (wavespeeds.c:325)
+ *         HLL / LAXF     (fluxcompute.c:75-78, :223-264)
+ *       flux_ct          (fluxct.c:10-844, FLUXCTTOTH, CORNGDETVERSION=1)
+ *       per zone: primtoU, source_conn (phys.c:578-752), flux2dUavg + dUtoU
+ *                 (advance.c:741-949), Utoprimgen (utoprimgen.c:23-436) ->
+ *                 Utoprim_2d_final (utoprim_2d_final.c:34-1278), fixup1zone
+ *                 (fixup.c:341-447) on the final substep
+ *     bound_prim         (bounds.fishmon.c:29-345 with inflow_check_rel4vel
+ *                         fixup.c:2271 and limit_gamma fixup.c:1859)
+ *     post_fixup         (fixup.c:37-96: bound_pflag boundsint.c:6,
+ *                         fixup_checksolution fixup.c:460, fixup_utoprim
+ *                         fixup.c:669-1470)
+ *     dt update          (advance.c:231, step_ch.c:236-247)
+ *
+ * for the build options of the FM-torus configuration: WHICHVEL=VELREL4,
+ * REMOVERESTMASSFROMUU=2, WHICHEOM=WITHGDET, EOMTYPE=EOMGRMHD, ideal gas,
+ * DOENOFLUX=NOENOFLUX, FLUXB=FLUXCTTOTH, UTOPRIMVERSION=UTOPRIM2DFINAL,
+ * TIMEORDER=2, LIMADJUST/FLUXADJUST fixed, STEPOVERNEG*=-1, CHECKSOLUTION=1,
+ * UTOPRIMADJUST=UTOPRIMAVG, BDIRCONT=1, EVOLVECHECKS=0.
+ *
+ * Geometry (gcov/gcon/gcovpert/gdet at the 8 grid locations, conn at CENT)
+ * and the density floors are inputs: the reference computes them once on the
+ * host (set_grid.c:7-151, fixup.c:1542-1654) and they carry no per-step work.
+ * The metric is stored per (i,j): it does not depend on x3.
+ */
+#include <math.h>
+#include <stdint.h>
+#include <stdlib.h>
+#include <string.h>
+#include <stdio.h>
+
+#include "harm_oracle.h"
+
+#define NPR 8
+#define NDIM 4
+#define RHO 0
+#define UU 1
+#define U1 2
+#define U2 3
+#define U3 4
+#define B1 5
+#define B2 6
+#define B3 7
+#define TT 0
+
+/* grid locations (global.h:948-955) */
+#define FACE1 0
+#define FACE2 1
+#define FACE3 2
+#define CORN1 3
+#define CORN2 4
+#define CORN3 5
+#define CORNT 6
+#define CENT 7
+
+/* failure codes (global.h:782-799) */
+#define UTOPRIMFAILFIXED -1
+#define UTOPRIMNOFAIL 0
+#define UTOPRIMFAILCONV 1
+#define UTOPRIMFAILCONVW 2
+#define UTOPRIMFAILCONVUTSQ 3
+#define UTOPRIMFAILCONVGUESSUTSQ 4
+#define UTOPRIMFAILCONVUTSQVERYBAD 5
+#define UTOPRIMFAILCONVBADINVERTCOMPARE 6
+#define UTOPRIMFAILNANGUESS 7
+#define UTOPRIMFAILNANRESULT 8
+#define UTOPRIMFAILRHONEG 9
+#define UTOPRIMFAILUNEG 10
+#define UTOPRIMFAILRHOUNEG 11
+#define UTOPRIMFAILGAMMAPERC 12
+#define UTOPRIMFAILUPERC 13
+#define UTOPRIMFAILU2AVG1 14
+#define UTOPRIMFAILU2AVG2 15
+#define UTOPRIMFAILCONVRET 101
+
+#define NUMEPSILON (2.2204460492503131e-16)
+#define BIG (1.e+50)
+
+/* u2p_defs.h (PRECISEINVERSION=1, NEWCONVERGE=1, OPTIMIZED=1) */
+#define MAX_NEWT_ITER 200
+#define NEWT_TOL (1E3 * NUMEPSILON)
+#define MIN_NEWT_TOL (1E-6)
+#define EXTRA_NEWT_ITER 0
+#define MAXNEGUTSQ (1E-10)
+#define MAXNEGVSQ (1.0 - 1.0 / (MAXNEGUTSQ + 1.0))
+#define FAIL_VAL 1.e30
+
+/* fixup.c:447-460,484 */
+#define GAMMAPERCDIFFMAX 2.0
+#define UPERCDIFFMAX 10.0
+#define MAXVOTES 8
+
+typedef struct {
+  const double *gcov; /* [4][4] */
+  const double *gcon; /* [4][4] */
+  const double *gcovpert; /* [4] */
+  double g;
+} geomref;
+
+typedef struct {
+  double ucon[NDIM], ucov[NDIM], bcon[NDIM], bcov[NDIM];
+} zstate;
+
+#define GCOV(g, a, b) ((g)->gcov[(a) * 4 + (b)])
+#define GCON(g, a, b) ((g)->gcon[(a) * 4 + (b)])
+
+/* error bits reported to the caller (the reference calls fail()/myexit()) */
+#define ERR_UTCALC_DISCR 1
+#define ERR_COEFF_NEG 2
+#define ERR_COEFF_SUP 4
+#define ERR_VCHAR_DISCR 8
+#define ERR_VSQ_NEG 16
+#define ERR_NONFINITE_SPEED 32
+#define ERR_PREF_NEG 64
+
+/* ------------------------------------------------------------------ */
+/* domain bookkeeping                                                  */
+/* ------------------------------------------------------------------ */
+typedef struct {
+  const hgo_config *c;
+  int n[4];      /* active sizes, index 1..3 */
+  int ng[4];     /* ghost widths */
+  int nt[4];     /* totals with ghosts */
+  int sh[4];     /* SHIFTd = (n>1) */
+  int gt[3];     /* geometry totals per (i,j): nt+sh */
+  const double *gcov, *gcon, *gcovpert, *gdet, *conn, *floors;
+  int err;
+} dom;
+
+static inline long zidx(const dom *d, int i, int j, int k)
+{
+  return ((long)(i + d->ng[1]) * d->nt[2] + (j + d->ng[2])) * d->nt[3] + (k + d->ng[3]);
+}
+
+static inline long gidx(const dom *d, int i, int j)
+{
+  return (long)(i + d->ng[1]) * d->gt[2] + (j + d->ng[2]);
+}
+
+static void get_geometry(const dom *d, int i, int j, int loc, geomref *g)
+{
+  long q = gidx(d, i, j) * 8 + loc;
+  g->gcov = d->gcov + q * 16;
+  g->gcon = d->gcon + q * 16;
+  g->gcovpert = d->gcovpert + q * 4;
+  g->g = d->gdet[q];
+}
+
+/* ------------------------------------------------------------------ */
+/* per-zone physics (phys.c)                                           */
+/* ------------------------------------------------------------------ */
+
+/* lower_vec (phys.c:766-787): upper-triangle gcov entries */
+static void lower_vec(const double *ucon, const geomref *g, double *ucov)
+{
+  ucov[0] = GCOV(g, 0, 0) * ucon[0] + GCOV(g, 0, 1) * ucon[1] + GCOV(g, 0, 2) * ucon[2] + GCOV(g, 0, 3) * ucon[3];
+  ucov[1] = GCOV(g, 0, 1) * ucon[0] + GCOV(g, 1, 1) * ucon[1] + GCOV(g, 1, 2) * ucon[2] + GCOV(g, 1, 3) * ucon[3];
+  ucov[2] = GCOV(g, 0, 2) * ucon[0] + GCOV(g, 1, 2) * ucon[1] + GCOV(g, 2, 2) * ucon[2] + GCOV(g, 2, 3) * ucon[3];
+  ucov[3] = GCOV(g, 0, 3) * ucon[0] + GCOV(g, 1, 3) * ucon[1] + GCOV(g, 2, 3) * ucon[2] + GCOV(g, 3, 3) * ucon[3];
+}
+
+/* raise_vec (phys.c:826-846) */
+static void raise_vec(const double *ucov, const geomref *g, double *ucon)
+{
+  ucon[0] = GCON(g, 0, 0) * ucov[0] + GCON(g, 0, 1) * ucov[1] + GCON(g, 0, 2) * ucov[2] + GCON(g, 0, 3) * ucov[3];
+  ucon[1] = GCON(g, 0, 1) * ucov[0] + GCON(g, 1, 1) * ucov[1] + GCON(g, 1, 2) * ucov[2] + GCON(g, 1, 3) * ucov[3];
+  ucon[2] = GCON(g, 0, 2) * ucov[0] + GCON(g, 1, 2) * ucov[1] + GCON(g, 2, 2) * ucov[2] + GCON(g, 2, 3) * ucov[3];
+  ucon[3] = GCON(g, 0, 3) * ucov[0] + GCON(g, 1, 3) * ucov[1] + GCON(g, 2, 3) * ucov[2] + GCON(g, 3, 3) * ucov[3];
+}
+
+static inline double dot4(const double *a, const double *b)
+{
+  return a[0] * b[0] + a[1] * b[1] + a[2] * b[2] + a[3] * b[3];
+}
+
+/* qsq_calc (phys.c:1077-1090) */
+static double qsq_calc(const double *u, const geomref *g)
+{
+  return +GCOV(g, 1, 1) * u[1] * u[1] + GCOV(g, 2, 2) * u[2] * u[2] + GCOV(g, 3, 3) * u[3] * u[3] +
+         2. * (GCOV(g, 1, 2) * u[1] * u[2] + GCOV(g, 1, 3) * u[1] * u[3] + GCOV(g, 2, 3) * u[2] * u[3]);
+}
+
+/* gamma_calc_fromuconrel (phys.c:1047-1074) */
+static int gamma_calc_fromuconrel(const double *uconrel, const geomref *g, double *gamma)
+{
+  double qsq = qsq_calc(uconrel, g);
+  if (qsq < 0.0) {
+    if (qsq > -NUMEPSILON * 100) qsq = 0.0;
+    else return 1;
+  }
+  *gamma = sqrt(1. + qsq);
+  return 0;
+}
+
+/* gamma_calc (phys.c:1022-1044) */
+static int gamma_calc(const double *pr, const geomref *g, double *gamma)
+{
+  double u[NDIM];
+  u[0] = 0;
+  u[1] = pr[U1];
+  u[2] = pr[U2];
+  u[3] = pr[U3];
+  return gamma_calc_fromuconrel(u, g, gamma);
+}
+
+/* ucon_calc_rel4vel (phys.c:983-1019) */
+static int ucon_calc(const double *pr, const geomref *g, double *ucon)
+{
+  double alpha, gamma, beta[NDIM], u[NDIM];
+  int j;
+  u[0] = 0;
+  u[1] = pr[U1];
+  u[2] = pr[U2];
+  u[3] = pr[U3];
+  alpha = 1. / sqrt(-GCON(g, TT, TT));
+  for (j = 1; j < NDIM; j++) beta[j] = GCON(g, TT, j) * alpha * alpha;
+  if (gamma_calc_fromuconrel(u, g, &gamma)) return 1;
+  ucon[TT] = gamma / alpha;
+  for (j = 1; j < NDIM; j++) ucon[j] = u[j] - ucon[TT] * beta[j];
+  return 0;
+}
+
+/* bcon_calc (phys.c:309-318) */
+static void bcon_calc(const double *pr, const double *ucon, const double *ucov, double *bcon)
+{
+  int j;
+  bcon[TT] = pr[B1] * ucov[1] + pr[B2] * ucov[2] + pr[B3] * ucov[3];
+  for (j = 1; j <= 3; j++) bcon[j] = (pr[B1 - 1 + j] + bcon[TT] * ucon[j]) / ucon[TT];
+}
+
+/* get_state (phys.c:849-859) */
+static int get_state(const double *pr, const geomref *g, zstate *q)
+{
+  if (ucon_calc(pr, g, q->ucon)) return 1;
+  lower_vec(q->ucon, g, q->ucov);
+  bcon_calc(pr, q->ucon, q->ucov, q->bcon);
+  lower_vec(q->bcon, g, q->bcov);
+  return 0;
+}
+
+/* Mcon_calc, PRIMMAXWELL (phys.c:178-210) */
+static void mcon_calc(const double *pr, const zstate *q, double M[NDIM][NDIM])
+{
+  int j, k;
+  for (j = 0; j < NDIM; j++) M[j][j] = 0.0;
+  for (k = 1; k < NDIM; k++) {
+    M[k][0] = pr[B1 + k - 1];
+    M[0][k] = -M[k][0];
+  }
+  for (j = 1; j < NDIM; j++)
+    for (k = 1; k < NDIM; k++) M[j][k] = (pr[B1 + j - 1] * q->ucon[k] - pr[B1 + k - 1] * q->ucon[j]) / q->ucon[0];
+}
+
+/* lower_A (phys.ffde.c:1707-1735) */
+static void lower_A(double Acon[NDIM][NDIM], const geomref *g, double Acov[NDIM][NDIM])
+{
+  int j, k;
+  for (j = 0; j < NDIM; j++)
+    for (k = 0; k < NDIM; k++) Acov[j][k] = 0.;
+  for (j = 0; j < NDIM; j++)
+    for (k = 0; k < NDIM; k++) {
+      Acov[0][1] += (GCOV(g, 0, j)) * (GCOV(g, 1, k)) * Acon[j][k];
+      Acov[0][2] += (GCOV(g, 0, j)) * (GCOV(g, 2, k)) * Acon[j][k];
+      Acov[0][3] += (GCOV(g, 0, j)) * (GCOV(g, 3, k)) * Acon[j][k];
+      Acov[1][2] += (GCOV(g, 1, j)) * (GCOV(g, 2, k)) * Acon[j][k];
+      Acov[2][3] += (GCOV(g, 2, j)) * (GCOV(g, 3, k)) * Acon[j][k];
+      Acov[3][1] += (GCOV(g, 3, j)) * (GCOV(g, 1, k)) * Acon[j][k];
+    }
+  Acov[1][0] = -Acov[0][1];
+  Acov[2][0] = -Acov[0][2];
+  Acov[3][0] = -Acov[0][3];
+  Acov[2][1] = -Acov[1][2];
+  Acov[3][2] = -Acov[2][3];
+  Acov[1][3] = -Acov[3][1];
+}
+
+/* compute_1plusud0 (phys.c:541-575) */
+static double compute_1plusud0(const geomref *g, const zstate *q)
+{
+  int j, k;
+  double plus1gv00, vsq, gvtt, alpha, uu0, vcon[NDIM];
+  for (j = 1; j < NDIM; j++) vcon[j] = q->ucon[j] / q->ucon[TT];
+  plus1gv00 = g->gcovpert[TT];
+  vsq = g->gcovpert[TT];
+  for (j = 1; j < NDIM; j++) vsq += 2.0 * GCOV(g, TT, j) * vcon[j];
+  for (j = 1; j < NDIM; j++)
+    for (k = 1; k < NDIM; k++) vsq += GCOV(g, j, k) * vcon[j] * vcon[k];
+  gvtt = GCOV(g, TT, TT);
+  alpha = 0.0;
+  for (j = 1; j < NDIM; j++) alpha += GCOV(g, j, TT) * q->ucon[j];
+  uu0 = q->ucon[TT];
+  return alpha + ((1.0 - gvtt) * plus1gv00 - uu0 * uu0 * vsq * gvtt * gvtt) / (1.0 - gvtt * uu0);
+}
+
+/* Per-state electromagnetic pieces that mhd_calc_norestmass recomputes on
+   every call (Mcon_calc, lower_A, Msq, 1+u_t); computing them once per state
+   gives the same bits. */
+typedef struct {
+  double Mcon[NDIM][NDIM], Mcov[NDIM][NDIM], Msq, plus1ud0;
+} emstate;
+
+static void em_prepare(const double *pr, const geomref *g, const zstate *q, emstate *e)
+{
+  int j, k;
+  mcon_calc(pr, q, e->Mcon);
+  lower_A(e->Mcon, g, e->Mcov);
+  e->Msq = 0.;
+  for (j = 0; j < NDIM; j++)
+    for (k = 0; k < NDIM; k++) e->Msq += e->Mcov[j][k] * e->Mcon[j][k];
+  e->plus1ud0 = compute_1plusud0(g, q);
+}
+
+/* mhd_calc_norestmass (phys.c:442-506) + ffdestresstensor_dir
+   (phys.ffde.c:1483-1515): T^dir_mu without rest mass */
+static void mhd_calc(const double *pr, int dir, const double gam, const zstate *q, const emstate *e, double *mhd)
+{
+  int j, i;
+  double rho = pr[RHO], u = pr[UU];
+  double P = (gam - 1.) * u;
+  double w = P + rho + u;
+  double eta = w, ptot = P;
+  double TEM[NDIM];
+  j = 0;
+  mhd[j] = (P + u) * q->ucon[dir] * q->ucov[j] + rho * q->ucon[dir] * e->plus1ud0 + ptot * ((dir == j) ? 1. : 0.);
+  for (j = 1; j < NDIM; j++) mhd[j] = eta * q->ucon[dir] * q->ucov[j] + ptot * ((dir == j) ? 1. : 0.);
+  for (j = 0; j < NDIM; j++) TEM[j] = 0.;
+  for (j = 0; j < NDIM; j++)
+    for (i = 0; i < NDIM; i++) TEM[j] += e->Mcon[dir][i] * e->Mcov[j][i];
+  TEM[dir] -= 0.25 * e->Msq;
+  for (j = 0; j < NDIM; j++) mhd[j] += TEM[j];
+}
+
+/* primtoflux (phys.c:16-55) with UEVOLVE; WITHGDET so every EOM factor is gdet */
+static void primtoflux(const double *pr, const zstate *q, const emstate *e, int dir, const geomref *g, double gam,
+                       double *flux)
+{
+  double fin[NPR];
+  fin[RHO] = pr[RHO] * q->ucon[dir];
+  mhd_calc(pr, dir, gam, q, e, &fin[UU]);
+  if (dir > 0) {
+    fin[B1] = (pr[B1] * q->ucon[dir] - pr[B1 + dir - 1] * q->ucon[1]) / q->ucon[0];
+    fin[B2] = (pr[B2] * q->ucon[dir] - pr[B1 + dir - 1] * q->ucon[2]) / q->ucon[0];
+    fin[B3] = (pr[B3] * q->ucon[dir] - pr[B1 + dir - 1] * q->ucon[3]) / q->ucon[0];
+  } else {
+    fin[B1] = pr[B1];
+    fin[B2] = pr[B2];
+    fin[B3] = pr[B3];
+  }
+  for (int pl = 0; pl < NPR; pl++) flux[pl] = fin[pl] * g->g;
+}
+
+/* ------------------------------------------------------------------ */
+/* wave speeds (vchar.c, wavespeeds.c)                                 */
+/* ------------------------------------------------------------------ */
+
+/* simplefast (vchar.c:213-312) */
+static int simplefast(int dir, const geomref *g, const zstate *q, double cms2, double *vmin, double *vmax)
+{
+  double discr, Acov[NDIM], Bcov[NDIM], Acon[NDIM], Bcon[NDIM];
+  double Asq, Bsq, Au, Bu, AB, Au2, Bu2, AuBu, A, B, vm, vp;
+  int j;
+  for (j = 0; j < NDIM; j++) Acov[j] = 0.;
+  Acov[dir] = 1.;
+  raise_vec(Acov, g, Acon);
+  for (j = 0; j < NDIM; j++) Bcov[j] = 0.;
+  Bcov[TT] = 1.;
+  raise_vec(Bcov, g, Bcon);
+  Asq = dot4(Acon, Acov);
+  Bsq = dot4(Bcon, Bcov);
+  Au = dot4(Acov, q->ucon);
+  Bu = dot4(Bcov, q->ucon);
+  AB = dot4(Acon, Bcov);
+  Au2 = Au * Au;
+  Bu2 = Bu * Bu;
+  AuBu = Au * Bu;
+  A = Bu2 * (1.0 - cms2) - Bsq * cms2;
+  B = 2. * (AuBu * (1.0 - cms2) - AB * cms2);
+  discr = 4.0 * cms2 * ((AB * AB - Asq * Bsq) * cms2 + (2.0 * AB * Au * Bu - Asq * Bu2 - Bsq * Au2) * (cms2 - 1.0));
+  if ((discr < 0.0) && (discr > -1E-10)) discr = 0.0;
+  else if (discr < 0.0) return ERR_VCHAR_DISCR;
+  discr = sqrt(discr);
+  vm = -(-B + discr) / (2. * A);
+  vp = -(-B - discr) / (2. * A);
+  if ((!isfinite(vm)) || (!isfinite(vp))) return ERR_NONFINITE_SPEED;
+  if (vp < vm) {
+    *vmax = vm;
+    *vmin = vp;
+  } else {
+    *vmax = vp;
+    *vmin = vm;
+  }
+  return 0;
+}
+
+/* vchar (vchar.c:37-171), TRUEFAST=0 */
+static int vchar(const double *pr, const zstate *q, int dir, const geomref *g, double gam, double *vmax,
+                 double *vmin)
+{
+  double bsq, WW, EF, va2, cs2, cms2, rho, u, P;
+  bsq = dot4(q->bcon, q->bcov);
+  rho = pr[RHO];
+  u = pr[UU];
+  if (u < 0) u = 0;
+  if (rho < 0) rho = 0;
+  P = (gam - 1.) * u;
+  WW = rho + u + P;
+  if (WW > 0.0) {
+    double pressure = (gam - 1.) * u;
+    double h = rho + u + pressure;
+    cs2 = gam * pressure / h;
+  } else WW = cs2 = 0.0;
+  if (cs2 >= 1.0) cs2 = 1.0 - 1e-9;
+  else if (cs2 <= 0.0) cs2 = 0.0;
+  EF = bsq + WW;
+  if (EF > 0.0) va2 = bsq / EF;
+  else EF = va2 = 0.0;
+  cms2 = cs2 + va2 - cs2 * va2;
+  if (cms2 < 0.0) {
+    if (cms2 / (cs2 + va2) > -NUMEPSILON * 100.0) cms2 = 0.0;
+    else return ERR_COEFF_NEG;
+  }
+  if (cms2 > 1.) {
+    if (cms2 < 1.0 + NUMEPSILON * 100.0) cms2 = 1.0;
+    else if (rho < 0.0) cms2 = 1.0;
+    else return ERR_COEFF_SUP;
+  }
+  return simplefast(dir, g, q, cms2, vmin, vmax);
+}
+
+static inline double fmax_ref(double a, double b) { return (a > b) ? a : b; } /* phys.c:1797 */
+static inline double fmin_ref(double a, double b) { return (a > b) ? b : a; } /* phys.c:1804 */
+static inline double fmin_macro(double a, double b) { return ((a) < (b)) ? (a) : (b); } /* MIN, global.h:751 */
+
+/* ------------------------------------------------------------------ */
+/* slopes and face fluxes (interppoint.c, flux.c, fluxcompute.c)       */
+/* ------------------------------------------------------------------ */
+
+#define MINMODB(a, b) ((fabs(a) < fabs(b)) ? (a) : (b))
+#define MINMOD(a, b) (((a) * (b) <= 0) ? 0.0 : MINMODB(a, b))
+
+/* slope_lim_3points (interppoint.c:387-443) */
+static double slope3(int lim, double yl, double yc, double yr)
+{
+  double Dqm, Dqp, Dqc, s;
+  if (lim == HGO_LIM_MC) {
+    Dqm = 2.0 * (yc - yl);
+    Dqp = 2.0 * (yr - yc);
+    Dqc = 0.5 * (yr - yl);
+    return MINMOD(Dqc, MINMOD(Dqm, Dqp));
+  } else if (lim == HGO_LIM_VANL) {
+    Dqm = (yc - yl);
+    Dqp = (yr - yc);
+    s = Dqm * Dqp;
+    if (s <= 0.) return 0.;
+    return (2.0 * s / (Dqm + Dqp));
+  } else if (lim == HGO_LIM_MINM) {
+    Dqm = 1.0 * (yc - yl);
+    Dqp = 1.0 * (yr - yc);
+    Dqc = 0.5 * (yr - yl);
+    return MINMOD(MINMOD(Dqm, Dqc), Dqp);
+  }
+  return 0.0; /* DONOR */
+}
+
+/* flux_compute_general (fluxcompute.c:12-51) for one face */
+static int face_flux(const hgo_config *c, int dir, const geomref *g, double *p_l, double *p_r, double *F, double *ctop)
+{
+  zstate ql, qr;
+  emstate el, er;
+  double Fl[NPR], Fr[NPR], Ul[NPR], Ur[NPR];
+  double cminl, cmaxl, cminr, cmaxr, lmin, lmax, cmin, cmax;
+  int pl, e;
+  if (get_state(p_l, g, &ql)) return ERR_UTCALC_DISCR;
+  em_prepare(p_l, g, &ql, &el);
+  primtoflux(p_l, &ql, &el, dir, g, c->gam, Fl);
+  primtoflux(p_l, &ql, &el, TT, g, c->gam, Ul);
+  if (get_state(p_r, g, &qr)) return ERR_UTCALC_DISCR;
+  em_prepare(p_r, g, &qr, &er);
+  primtoflux(p_r, &qr, &er, dir, g, c->gam, Fr);
+  primtoflux(p_r, &qr, &er, TT, g, c->gam, Ur);
+  if ((e = vchar(p_l, &ql, dir, g, c->gam, &cmaxl, &cminl))) return e;
+  if ((e = vchar(p_r, &qr, dir, g, c->gam, &cmaxr, &cminr))) return e;
+  /* cminmax_calc (wavespeeds.c:325-385), HYPERHLL=0 */
+  lmin = fmin_ref(cminl, cminr);
+  lmax = fmax_ref(cmaxl, cmaxr);
+  lmin = fabs(fmax_ref(0., -lmin));
+  lmax = fabs(fmax_ref(0., lmax));
+  cmin = lmin;
+  cmax = lmax;
+  *ctop = fmax_ref(lmax, lmin);
+  if (c->fluxmethod == HGO_FLUX_HLL && (cmax + cmin != 0.0)) {
+    for (pl = 0; pl < NPR; pl++) F[pl] = ((cmax * Fl[pl] + cmin * Fr[pl]) - (cmax * cmin) * (Ur[pl] - Ul[pl])) / (cmax + cmin);
+  } else {
+    for (pl = 0; pl < NPR; pl++) F[pl] = (0.5 * ((Fl[pl] + Fr[pl]) - (*ctop) * (Ur[pl] - Ul[pl])));
+  }
+  return 0;
+}
+
+/* fluxcalc_standard for one direction (flux.c:469-680) with MC-type slopes */
+static void fluxcalc_dir(dom *d, const double *pr, int dir, double *F, double *dq, double *ndt)
+{
+  const hgo_config *c = d->c;
+  int is, ie, js, je, ks, ke, i, j, k, pl;
+  int di = (dir == 1), dj = (dir == 2), dk = (dir == 3);
+  int n1 = d->n[1], n2 = d->n[2], n3 = d->n[3];
+  geomref g;
+  double p_l[NPR], p_r[NPR], ctop = 0.0, dtij;
+  int loc = (dir == 1) ? FACE1 : ((dir == 2) ? FACE2 : FACE3);
+  long dofs = (long)di * d->nt[2] * d->nt[3] + (long)dj * d->nt[3] + dk;
+
+  *ndt = BIG;
+  if (d->n[dir] == 1) return;
+
+  /* interp_loop_set (initbase.c:1010-1058), NOENOFLUX */
+  is = (dir == 1) ? 0 : -d->sh[1];
+  ie = (dir == 1) ? n1 - 1 + d->sh[1] : n1 - 1 + d->sh[1];
+  js = (dir == 2) ? 0 : -d->sh[2];
+  je = (dir == 2) ? n2 - 1 + d->sh[2] : n2 - 1 + d->sh[2];
+  ks = (dir == 3) ? 0 : -d->sh[3];
+  ke = (dir == 3) ? n3 - 1 + d->sh[3] : n3 - 1 + d->sh[3];
+
+  /* slopes over the zones the faces read: centers (face-1) and (face) */
+  for (i = is - di; i <= ie; i++)
+    for (j = js - dj; j <= je; j++)
+      for (k = ks - dk; k <= ke; k++) {
+        long z = zidx(d, i, j, k);
+        for (pl = 0; pl < NPR; pl++)
+          dq[z * NPR + pl] = slope3(c->lim, pr[(z - dofs) * NPR + pl], pr[z * NPR + pl], pr[(z + dofs) * NPR + pl]);
+      }
+
+  for (i = is; i <= ie; i++)
+    for (j = js; j <= je; j++)
+      for (k = ks; k <= ke; k++) {
+        long z = zidx(d, i, j, k);
+        long zm = z - dofs;
+        int e;
+        /* getp2interplr (flux.c:788-808) */
+        for (pl = 0; pl < NPR; pl++) {
+          p_l[pl] = pr[zm * NPR + pl] + 0.5 * dq[zm * NPR + pl];
+          p_r[pl] = pr[z * NPR + pl] - 0.5 * dq[z * NPR + pl];
+        }
+        get_geometry(d, i, j, loc, &g);
+        /* BDIRCONT (flux.c:629-633) */
+        p_l[B1 + dir - 1] = p_r[B1 + dir - 1] = 0.5 * (p_l[B1 + dir - 1] + p_r[B1 + dir - 1]);
+        e = face_flux(c, dir, &g, p_l, p_r, &F[z * NPR], &ctop);
+        if (e) d->err |= e;
+        dtij = c->cour * c->dx[dir] / ctop;
+        if (dtij < *ndt) *ndt = dtij;
+      }
+}
+
+/* flux_ct, FLUXCTTOTH with CORNGDETVERSION=1 (fluxct.c:10-844).
+   The reference strips/averages over nearly the whole array; only the faces
+   of the flux loops (initbase.c:1010-1058) and the corners that the updated
+   faces read matter, and those are the ranges used here. */
+static void flux_ct(dom *d, double *F1, double *F2, double *F3, double *emf)
+{
+  int n1 = d->n[1], n2 = d->n[2], n3 = d->n[3];
+  int s1 = d->sh[1], s2 = d->sh[2], s3 = d->sh[3];
+  int i, j, k;
+  long ntot = (long)d->nt[1] * d->nt[2] * d->nt[3];
+  long o1 = (long)d->nt[2] * d->nt[3], o2 = d->nt[3], o3 = 1;
+  double coef1, coef2, coef3;
+  double *e1 = emf, *e2 = emf + ntot, *e3 = emf + 2 * ntot;
+  geomref g;
+
+  /* strip gdet (fluxct.c:74-96) on the flux-loop faces */
+  if (n1 > 1)
+    for (i = 0; i <= n1; i++)
+      for (j = -s2; j <= n2 - 1 + s2; j++)
+        for (k = -s3; k <= n3 - 1 + s3; k++) {
+          long z = zidx(d, i, j, k);
+          get_geometry(d, i, j, FACE1, &g);
+          F1[z * NPR + B1] /= g.g;
+          F1[z * NPR + B2] /= g.g;
+          F1[z * NPR + B3] /= g.g;
+        }
+  if (n2 > 1)
+    for (i = -s1; i <= n1 - 1 + s1; i++)
+      for (j = 0; j <= n2; j++)
+        for (k = -s3; k <= n3 - 1 + s3; k++) {
+          long z = zidx(d, i, j, k);
+          get_geometry(d, i, j, FACE2, &g);
+          F2[z * NPR + B1] /= g.g;
+          F2[z * NPR + B2] /= g.g;
+          F2[z * NPR + B3] /= g.g;
+        }
+  if (n3 > 1)
+    for (i = -s1; i <= n1 - 1 + s1; i++)
+      for (j = -s2; j <= n2 - 1 + s2; j++)
+        for (k = 0; k <= n3; k++) {
+          long z = zidx(d, i, j, k);
+          get_geometry(d, i, j, FACE3, &g);
+          F3[z * NPR + B1] /= g.g;
+          F3[z * NPR + B2] /= g.g;
+          F3[z * NPR + B3] /= g.g;
+        }
+
+  coef1 = ((n2 > 1) && (n3 > 1)) ? 0.25 : 0.5;
+  coef2 = ((n1 > 1) && (n3 > 1)) ? 0.25 : 0.5;
+  coef3 = ((n1 > 1) && (n2 > 1)) ? 0.25 : 0.5;
+
+  /* emf1 (fluxct.c:148-161) on i=0..n1-1, j=0..n2-1+s2, k=0..n3-1+s3; x CORN1 gdet */
+  for (i = 0; i <= n1 - 1; i++)
+    for (j = 0; j <= n2 - 1 + s2; j++)
+      for (k = 0; k <= n3 - 1 + s3; k++) {
+        long z = zidx(d, i, j, k);
+        double v;
+        if (n2 > 1 && n3 > 1)
+          v = coef1 * (+F2[z * NPR + B3] + F2[(z - s3 * o3) * NPR + B3] - F3[z * NPR + B2] - F3[(z - s2 * o2) * NPR + B2]);
+        else if (n2 > 1)
+          v = coef1 * (+F2[z * NPR + B3] + F2[(z - s3 * o3) * NPR + B3]);
+        else if (n3 > 1)
+          v = coef1 * (-F3[z * NPR + B2] - F3[(z - s2 * o2) * NPR + B2]);
+        else
+          v = 0.0;
+        get_geometry(d, i, j, CORN1, &g);
+        e1[z] = v * g.g;
+      }
+  /* emf2 (fluxct.c:166-179) on i=0..n1-1+s1, j=0..n2-1, k=0..n3-1+s3; x CORN2 gdet */
+  for (i = 0; i <= n1 - 1 + s1; i++)
+    for (j = 0; j <= n2 - 1; j++)
+      for (k = 0; k <= n3 - 1 + s3; k++) {
+        long z = zidx(d, i, j, k);
+        double v;
+        if (n1 > 1 && n3 > 1)
+          v = coef2 * (+F3[z * NPR + B1] + F3[(z - s1 * o1) * NPR + B1] - F1[z * NPR + B3] - F1[(z - s3 * o3) * NPR + B3]);
+        else if (n3 > 1)
+          v = coef2 * (+F3[z * NPR + B1] + F3[(z - s1 * o1) * NPR + B1]);
+        else if (n1 > 1)
+          v = coef2 * (-F1[z * NPR + B3] - F1[(z - s3 * o3) * NPR + B3]);
+        else
+          v = 0.0;
+        get_geometry(d, i, j, CORN2, &g);
+        e2[z] = v * g.g;
+      }
+  /* emf3 (fluxct.c:184-197) on i=0..n1-1+s1, j=0..n2-1+s2, k=0..n3-1; x CORN3 gdet */
+  for (i = 0; i <= n1 - 1 + s1; i++)
+    for (j = 0; j <= n2 - 1 + s2; j++)
+      for (k = 0; k <= n3 - 1; k++) {
+        long z = zidx(d, i, j, k);
+        double v;
+        if (n1 > 1 && n2 > 1)
+          v = coef3 * (+F1[z * NPR + B2] + F1[(z - s2 * o2) * NPR + B2] - F2[z * NPR + B1] - F2[(z - s1 * o1) * NPR + B1]);
+        else if (n1 > 1)
+          v = coef3 * (+F1[z * NPR + B2] + F1[(z - s2 * o2) * NPR + B2]);
+        else if (n2 > 1)
+          v = coef3 * (-F2[z * NPR + B1] - F2[(z - s1 * o1) * NPR + B1]);
+        else
+          v = 0.0;
+        get_geometry(d, i, j, CORN3, &g);
+        e3[z] = v * g.g;
+      }
+
+  /* B fluxes from EMFs on the faces read by the update (fluxct.c:724-781) */
+  if (n1 > 1)
+    for (i = 0; i <= n1; i++)
+      for (j = 0; j <= n2 - 1; j++)
+        for (k = 0; k <= n3 - 1; k++) {
+          long z = zidx(d, i, j, k);
+          F1[z * NPR + B1] = 0.;
+          F1[z * NPR + B2] = 0.5 * (e3[z] + e3[z + s2 * o2]);
+          F1[z * NPR + B3] = -0.5 * (e2[z] + e2[z + s3 * o3]);
+        }
+  if (n2 > 1)
+    for (i = 0; i <= n1 - 1; i++)
+      for (j = 0; j <= n2; j++)
+        for (k = 0; k <= n3 - 1; k++) {
+          long z = zidx(d, i, j, k);
+          F2[z * NPR + B1] = -0.5 * (e3[z] + e3[z + s1 * o1]);
+          F2[z * NPR + B2] = 0.;
+          F2[z * NPR + B3] = 0.5 * (e1[z] + e1[z + s3 * o3]);
+        }
+  if (n3 > 1)
+    for (i = 0; i <= n1 - 1; i++)
+      for (j = 0; j <= n2 - 1; j++)
+        for (k = 0; k <= n3; k++) {
+          long z = zidx(d, i, j, k);
+          F3[z * NPR + B1] = 0.5 * (e2[z] + e2[z + s1 * o1]);
+          F3[z * NPR + B2] = -0.5 * (e1[z] + e1[z + s2 * o2]);
+          F3[z * NPR + B3] = 0.;
+        }
+}
+
+/* ------------------------------------------------------------------ */
+/* con-to-prim: Utoprim_2d_final (utoprim_2d_final.c)                   */
+/* ------------------------------------------------------------------ */
+typedef struct {
+  double Bsq, QdotBsq, Qtsq, Qdotn, D, wglobal, gam, gammasq_too_big, vsq_too_big;
+  int iters;
+} u2pctx;
+
+/* vsq_calc (utoprim_2d_final.c:457-470) */
+static double vsq_calc(const u2pctx *c, double W)
+{
+  double Wsq = W * W;
+  double Xsq = (c->Bsq + W) * (c->Bsq + W);
+  return ((Wsq * c->Qtsq + c->QdotBsq * (c->Bsq + 2. * W)) / (Wsq * Xsq));
+}
+
+/* EOS pieces (utoprim_jon_eos.c:83-108, :214-247, :316-345, :433-437; eos.c:178-194) */
+static double wmrho0_compute_vsq(double Wp, double D, double vsq, double gamma, double gammasq)
+{
+  return (Wp / gammasq - D * vsq / (1.0 + gamma));
+}
+
+static double pressure_W_vsq(const u2pctx *c, double W, double D, double vsq)
+{
+  double Wp = W - D;
+  double gamma = 1.0 / sqrt(1.0 - vsq);
+  double gammasq = gamma * gamma;
+  double wmrho0 = wmrho0_compute_vsq(Wp, D, vsq, gamma, gammasq);
+  return ((c->gam - 1.0) / c->gam) * wmrho0; /* pressure_wmrho0_grmhd: IGAMMAR*wmrho0 */
+}
+
+static double dpdW_calc_vsq(const u2pctx *c, double W, double D, double vsq)
+{
+  double Wp = W - D;
+  double gamma = 1.0 / sqrt(1.0 - vsq);
+  double gammasq = gamma * gamma;
+  double idwmrho0dp, dwmrho0dW, drho0dW, idrho0dp;
+  (void)wmrho0_compute_vsq(Wp, D, vsq, gamma, gammasq);
+  idwmrho0dp = (c->gam - 1.0) / c->gam; /* compute_idwmrho0dp_grmhd: GAMMAM1/GAMMA */
+  dwmrho0dW = 1.0 - vsq;
+  drho0dW = 0.0;
+  idrho0dp = 0.0; /* compute_idrho0dp_grmhd */
+  return drho0dW * idrho0dp + dwmrho0dW * idwmrho0dp;
+}
+
+static double dpdvsq_calc(const u2pctx *c, double W, double D, double vsq)
+{
+  double Wp = W - D;
+  double gamma = 1.0 / sqrt(1.0 - vsq);
+  double idwmrho0dp, dwmrho0dvsq, drho0dvsq, idrho0dp;
+  idwmrho0dp = (c->gam - 1.0) / c->gam;
+  dwmrho0dvsq = (D * (gamma * 0.5 - 1.0) - Wp);
+  drho0dvsq = -D * gamma * 0.5;
+  idrho0dp = 0.0;
+  return drho0dvsq * idrho0dp + dwmrho0dvsq * idwmrho0dp;
+}
+
+/* func_vsq2 (utoprim_2d_final.c:1189-1278) */
+static void func_vsq2(const u2pctx *c, const double x[2], double dx[2], double *f, double *df)
+{
+  double W = x[0], vsq = x[1], Wsq = W * W;
+  double p_tmp = pressure_W_vsq(c, W, c->D, vsq);
+  double dPdW = dpdW_calc_vsq(c, W, c->D, vsq);
+  double dPdvsq = dpdvsq_calc(c, W, c->D, vsq);
+  double t2, t3, t4, t9, t11, t16, t18, t21, t23, t24, t25, t35, t36, t40;
+  double Bsq = c->Bsq, QdotBsq = c->QdotBsq, Qtsq = c->Qtsq, Qdotn = c->Qdotn;
+  double resid0, resid1;
+  t2 = -0.5 * Bsq + dPdvsq;
+  t3 = Bsq + W;
+  t4 = t3 * t3;
+  t9 = 1 / Wsq;
+  t11 = Qtsq - vsq * t4 + QdotBsq * (Bsq + 2.0 * W) * t9;
+  t16 = QdotBsq * t9;
+  t18 = -Qdotn - 0.5 * Bsq * (1.0 + vsq) + 0.5 * t16 - W + p_tmp;
+  t21 = 1 / t3;
+  t23 = 1 / W;
+  t24 = t16 * t23;
+  t25 = -1.0 + dPdW - t24;
+  t35 = t25 * t3 + (Bsq - 2.0 * dPdvsq) * (QdotBsq + vsq * Wsq * W) * t9 * t23;
+  t36 = 1 / t35;
+  dx[0] = -(t2 * t11 + t4 * t18) * t21 * t36;
+  t40 = (vsq + t24) * t3;
+  dx[1] = -(-t25 * t11 - 2.0 * t40 * t18) * t21 * t36;
+  resid0 = t11;
+  resid1 = t18;
+  *df = -resid0 * resid0 - resid1 * resid1;
+  *f = -0.5 * (*df);
+}
+
+/* general_newton_raphson with do_line_search = USE_LINE_SEARCH = -2
+   (utoprim_2d_final.c:736-1119): plain Newton steps */
+static int general_newton_raphson(u2pctx *c, double x[2])
+{
+  double f, df, dx[2], x_old[2], errx;
+  int n_iter = 0, keep_iterating = 1, id, doing_extra = 0, i_extra = 0;
+  errx = 1.;
+  df = f = 1.;
+  for (id = 0; id < 2; id++) x_old[id] = x[id];
+  while (keep_iterating) {
+    c->iters++;
+    func_vsq2(c, x, dx, &f, &df);
+    errx = 0.;
+    for (id = 0; id < 2; id++) x_old[id] = x[id];
+    for (id = 0; id < 2; id++) x[id] += dx[id];
+    errx = (x[0] == 0.) ? fabs(dx[0]) : fabs(dx[0] / x[0]);
+    /* validate_x (utoprim_2d_final.c:708-728) */
+    x[0] = fabs(x[0]);
+    x[0] = (x[0] / c->wglobal > c->gammasq_too_big) ? x_old[0] : x[0];
+    x[1] = (x[1] > 1.) ? c->vsq_too_big : x[1];
+    if ((fabs(errx) <= NEWT_TOL) && (doing_extra == 0) && (EXTRA_NEWT_ITER > 0)) doing_extra = 1;
+    if (doing_extra == 1) i_extra++;
+    if (((fabs(errx) <= NEWT_TOL) && (doing_extra == 0)) || (i_extra > EXTRA_NEWT_ITER) || (n_iter >= (MAX_NEWT_ITER - 1)))
+      keep_iterating = 0;
+    n_iter++;
+  }
+  if ((isfinite(f) == 0) || (isfinite(df) == 0) || (isfinite(x[0]) == 0) || (isfinite(x[1]) == 0)) return 1;
+  if (fabs(errx) > MIN_NEWT_TOL) return 1;
+  return 0;
+}
+
+/* Utoprim_2d_final + Utoprim_new_body.  U is the geometry-free conserved
+   vector with rest mass included in U[UU] (utoprimgen.c:76-85); prim holds
+   the guess on input.  Returns the pflag code. */
+static int utoprim_2d_final(const double *U, const geomref *g, const hgo_config *cfg, double *prim, int *iters)
+{
+  double U_tmp[NPR], prim_tmp[NPR], alpha;
+  double Bcon[4], Bcov[4], Qcov[4], Qcon[4], ncov[4], ncon[4], Qtcon[4];
+  double QdotB, Qsq, rho0, u, p, w, gammasq, gamma, gtmp, W_last, W, utsq, vsq, Wtest;
+  int i, j, retval, i_increase, lpflag;
+  u2pctx c;
+  double x[2];
+
+  c.gam = cfg->gam;
+  c.gammasq_too_big = cfg->gammafail * cfg->gammafail;
+  c.vsq_too_big = (c.gammasq_too_big - 1.0) / (c.gammasq_too_big);
+  c.iters = 0;
+
+  for (i = B1; i <= B3; i++) prim[i] = U[i];
+  alpha = 1.0 / sqrt(-GCON(g, 0, 0));
+  for (i = RHO; i <= B3; i++) U_tmp[i] = alpha * U[i];
+  for (i = 0; i < B1; i++) prim_tmp[i] = prim[i];
+  for (i = B1; i <= B3; i++) prim_tmp[i] = alpha * prim[i];
+
+  /* Utoprim_new_body (utoprim_2d_final.c:152-453) */
+  lpflag = UTOPRIMNOFAIL;
+  for (i = B1; i <= B3; i++) prim_tmp[i] = U_tmp[i];
+  Bcon[0] = 0.;
+  for (i = 1; i < 4; i++) Bcon[i] = U_tmp[B1 + i - 1];
+  /* lower_g / raise_g (u2p_util.c:120-143): full-matrix sums starting from 0 */
+  for (i = 0; i < 4; i++) {
+    Bcov[i] = 0.;
+    for (j = 0; j < 4; j++) Bcov[i] += GCOV(g, i, j) * Bcon[j];
+  }
+  for (i = 0; i < 4; i++) Qcov[i] = U_tmp[UU + i];
+  for (i = 0; i < 4; i++) {
+    Qcon[i] = 0.;
+    for (j = 0; j < 4; j++) Qcon[i] += GCON(g, i, j) * Qcov[j];
+  }
+  c.Bsq = 0.;
+  for (i = 1; i < 4; i++) c.Bsq += Bcon[i] * Bcov[i];
+  QdotB = 0.;
+  for (i = 0; i < 4; i++) QdotB += Qcov[i] * Bcon[i];
+  c.QdotBsq = QdotB * QdotB;
+  {
+    /* ncov_calc (u2p_util.c:146-157) */
+    double lapse = sqrt(-1. / GCON(g, 0, 0));
+    ncov[0] = -lapse;
+    ncov[1] = 0.;
+    ncov[2] = 0.;
+    ncov[3] = 0.;
+  }
+  for (i = 0; i < 4; i++) {
+    ncon[i] = 0.;
+    for (j = 0; j < 4; j++) ncon[i] += GCON(g, i, j) * ncov[j];
+  }
+  c.Qdotn = Qcon[0] * ncov[0];
+  Qsq = 0.;
+  for (i = 0; i < 4; i++) Qsq += Qcov[i] * Qcon[i];
+  c.Qtsq = Qsq + c.Qdotn * c.Qdotn;
+  c.D = U_tmp[RHO];
+
+  utsq = 0.;
+  for (i = 1; i < 4; i++)
+    for (j = 1; j < 4; j++) utsq += GCOV(g, i, j) * prim_tmp[U1 + i - 1] * prim_tmp[U1 + j - 1];
+  if ((utsq < 0.) && (fabs(utsq) < MAXNEGUTSQ)) utsq = 0.0;
+  if (utsq < 0. || utsq > ((cfg->gammafail - 1.0) * (cfg->gammafail - 1.0))) {
+    *iters = c.iters;
+    return UTOPRIMFAILCONVGUESSUTSQ;
+  }
+  gammasq = 1. + utsq;
+  gamma = sqrt(gammasq);
+  rho0 = c.D / gamma;
+  u = prim_tmp[UU];
+  p = (cfg->gam - 1.) * u;
+  w = rho0 + u + p;
+  W_last = w * gammasq;
+  i_increase = 0;
+  while (((W_last * W_last * W_last * (W_last + 2. * c.Bsq) - c.QdotBsq * (2. * W_last + c.Bsq)) <=
+          W_last * W_last * (c.Qtsq - c.Bsq * c.Bsq)) &&
+         (i_increase < 10)) {
+    W_last *= 10.;
+    i_increase++;
+  }
+  c.wglobal = w;
+  /* find_root_2D_gen (utoprim_2d_final.c:573-644), MAX_NEWT_RETRIES=0 */
+  x[0] = fabs(W_last);
+  {
+    double vs = vsq_calc(&c, W_last);
+    x[1] = (vs > 1.) ? c.vsq_too_big : vs;
+  }
+  retval = general_newton_raphson(&c, x);
+  W = x[0];
+  *iters = c.iters;
+  if ((retval != 0) || (W == FAIL_VAL)) {
+    return retval * 100 + 1;
+  } else {
+    Wtest = W / c.wglobal;
+    if (Wtest <= 0. || Wtest > c.gammasq_too_big) return UTOPRIMFAILCONVW;
+  }
+  vsq = vsq_calc(&c, W);
+  if ((vsq < 0.) && (fabs(vsq) < MAXNEGVSQ)) vsq = 0.0;
+  if ((vsq > c.vsq_too_big) || (vsq < 0.0)) return UTOPRIMFAILCONVUTSQ;
+  gtmp = sqrt(1. - vsq);
+  gamma = 1. / gtmp;
+  rho0 = c.D * gtmp;
+  w = W * (1. - vsq);
+  {
+    double wmrho0 = w - rho0; /* pressure_rho0_w (eos.c:550-558) */
+    p = ((cfg->gam - 1.0) / cfg->gam) * wmrho0;
+  }
+  u = w - (rho0 + p);
+  if ((rho0 <= 0.) || (u < 0.)) {
+    if ((rho0 <= 0.) && (u >= 0.)) lpflag = UTOPRIMFAILRHONEG;
+    if ((rho0 > 0.) && (u < 0.)) lpflag = UTOPRIMFAILUNEG;
+    if ((rho0 <= 0.) && (u < 0.)) lpflag = UTOPRIMFAILRHOUNEG;
+    /* UTOPRIMFAILRETURNTYPE==UTOPRIMRETURNADJUSTED: assign anyway */
+  }
+  prim_tmp[RHO] = rho0;
+  prim_tmp[UU] = u;
+  for (i = 1; i < 4; i++) Qtcon[i] = Qcon[i] + ncon[i] * c.Qdotn;
+  for (i = 1; i < 4; i++) prim_tmp[U1 + i - 1] = gamma / (W + c.Bsq) * (Qtcon[i] + QdotB * Bcon[i] / W);
+  for (i = B1; i <= B3; i++) prim_tmp[i] = U_tmp[i];
+  /* back in Utoprim_2d_final: ret == retval == 0 here */
+  for (i = 0; i < B1; i++) prim[i] = prim_tmp[i];
+  return lpflag;
+}
+
+/* Utoprimgen (utoprimgen.c:23-436): geometry-free U, rest mass, inversion.
+   U is the evolved conserved vector (with gdet).  Returns pflag. */
+static int utoprimgen(const double *U, const geomref *g, const hgo_config *cfg, double *pr, int *iters)
+{
+  double Ugf[NPR];
+  int pl;
+  for (pl = 0; pl < NPR; pl++) Ugf[pl] = U[pl] / g->g; /* UtoU UEVOLVE->UNOTHING */
+  Ugf[UU] -= Ugf[RHO];                                  /* REMOVERESTMASSFROMUU==2 (utoprimgen.c:76-85) */
+  return utoprim_2d_final(Ugf, g, cfg, pr, iters);
+}
+
+/* ------------------------------------------------------------------ */
+/* fixups (fixup.c)                                                    */
+/* ------------------------------------------------------------------ */
+
+/* limit_gamma (fixup.c:1859-1905) */
+static int limit_gamma(double gammamax, double *pr, const geomref *g, int *err)
+{
+  double f, gamma, pref;
+  if (gammamax <= 1.0) return 0;
+  if (gamma_calc(pr, g, &gamma)) {
+    *err |= ERR_UTCALC_DISCR;
+    return 1;
+  }
+  if ((gamma > gammamax && (gamma != 1.0))) {
+    pref = (gammamax * gammamax - 1.) / (gamma * gamma - 1.);
+    if (pref < 0.0) {
+      *err |= ERR_PREF_NEG;
+      return 1;
+    }
+    f = sqrt(pref);
+    pr[U1] *= f;
+    pr[U2] *= f;
+    pr[U3] *= f;
+    return -1;
+  }
+  return 0;
+}
+
+/* fixup1zone (fixup.c:341-447) with floors precomputed per zone */
+static void fixup1zone(double *pr, const geomref *g, const double *floor2, const hgo_config *c, int *err)
+{
+  double prfloor[2];
+  prfloor[RHO] = floor2[0];
+  prfloor[UU] = floor2[1];
+  if (prfloor[RHO] < c->rhominlimit) prfloor[RHO] = c->rhominlimit;
+  if (prfloor[UU] < c->uuminlimit) prfloor[UU] = c->uuminlimit;
+  if (prfloor[RHO] > pr[RHO]) pr[RHO] = prfloor[RHO];
+  if (prfloor[UU] > pr[UU]) pr[UU] = prfloor[UU];
+  limit_gamma(c->gammamax, pr, g, err);
+}
+
+/* inflow_check_rel4vel for dir 1 at a CENT ghost zone (fixup.c:2271-2400) */
+static void inflow_check_x1(const dom *d, int i, double *pr, const geomref *g, int *err)
+{
+  double ucon[NDIM], gamma, alpha, betacon, vsq;
+  int dofix = 0, j, k;
+  if (ucon_calc(pr, g, ucon)) {
+    *err |= ERR_UTCALC_DISCR;
+    return;
+  }
+  if (((i <= -1) && (d->c->bc[HGO_X1DN] == HGO_BC_OUTFLOW) && (ucon[1] > 0.)) ||
+      ((i >= d->n[1]) && (d->c->bc[HGO_X1UP] == HGO_BC_OUTFLOW) && (ucon[1] < 0.)))
+    dofix = 1;
+  if (!dofix) return;
+  if (gamma_calc(pr, g, &gamma)) {
+    *err |= ERR_UTCALC_DISCR;
+    return;
+  }
+  pr[U1] /= gamma;
+  pr[U2] /= gamma;
+  pr[U3] /= gamma;
+  alpha = 1. / sqrt(-GCON(g, 0, 0));
+  betacon = GCON(g, 0, 1) * alpha * alpha;
+  pr[U1] = betacon / alpha;
+  vsq = 0.;
+  for (j = 1; j < NDIM; j++)
+    for (k = 1; k < NDIM; k++) vsq += GCOV(g, j, k) * pr[U1 + j - 1] * pr[U1 + k - 1];
+  if (vsq < 0.0) {
+    if (vsq > -NUMEPSILON * 100.0) vsq = 0.0;
+    else {
+      *err |= ERR_VSQ_NEG;
+      return;
+    }
+  }
+  if (vsq >= 1.0) vsq = 1.0 - 1.0 / (d->c->gammamax * d->c->gammamax);
+  gamma = 1. / sqrt(1. - vsq);
+  pr[U1] *= gamma;
+  pr[U2] *= gamma;
+  pr[U3] *= gamma;
+}
+
+/* bound_prim_user (bounds.fishmon.c:29-345): x1 OUTFLOW with inflow check
+   and gamma limit, x2 POLARAXIS (POSDEFMETRIC=0, POLEDEATH=1), x3 PERIODIC */
+static void bound_prim(dom *d, double *p)
+{
+  int n1 = d->n[1], n2 = d->n[2], n3 = d->n[3];
+  int g1 = d->ng[1], g2 = d->ng[2], g3 = d->ng[3];
+  int i, j, k, pl;
+  geomref g;
+  const hgo_config *c = d->c;
+  if (n1 > 1) {
+    if (c->bc[HGO_X1DN] == HGO_BC_OUTFLOW) {
+      for (j = 0; j < n2; j++)
+        for (k = 0; k < n3; k++) {
+          for (i = -g1; i <= -1; i++)
+            for (pl = 0; pl < NPR; pl++) p[zidx(d, i, j, k) * NPR + pl] = p[zidx(d, 0, j, k) * NPR + pl];
+          for (i = -g1; i <= -1; i++) {
+            double *pr = &p[zidx(d, i, j, k) * NPR];
+            get_geometry(d, i, j, CENT, &g);
+            inflow_check_x1(d, i, pr, &g, &d->err);
+            limit_gamma(c->gammamax, pr, &g, &d->err);
+          }
+        }
+    }
+    if (c->bc[HGO_X1UP] == HGO_BC_OUTFLOW) {
+      for (j = 0; j < n2; j++)
+        for (k = 0; k < n3; k++) {
+          for (i = n1; i <= n1 + g1 - 1; i++)
+            for (pl = 0; pl < NPR; pl++) p[zidx(d, i, j, k) * NPR + pl] = p[zidx(d, n1 - 1, j, k) * NPR + pl];
+          for (i = n1; i <= n1 + g1 - 1; i++) {
+            double *pr = &p[zidx(d, i, j, k) * NPR];
+            get_geometry(d, i, j, CENT, &g);
+            inflow_check_x1(d, i, pr, &g, &d->err);
+            limit_gamma(c->gammamax, pr, &g, &d->err);
+          }
+        }
+    }
+  }
+  if (n2 > 1) {
+    if (c->bc[HGO_X2DN] == HGO_BC_POLARAXIS) {
+      for (i = -g1; i <= n1 - 1 + g1; i++)
+        for (k = 0; k < n3; k++)
+          for (j = -g2; j <= -1; j++)
+            for (pl = 0; pl < NPR; pl++) p[zidx(d, i, j, k) * NPR + pl] = p[zidx(d, i, -j - 1, k) * NPR + pl];
+      /* antisymmetry factors are 1 for POSDEFMETRIC=0; POLEDEATH zeroes U2,B2 */
+      for (i = -g1; i <= n1 - 1 + g1; i++)
+        for (k = 0; k < n3; k++)
+          for (j = -g2; j < 0 + 1; j++) {
+            p[zidx(d, i, j, k) * NPR + U2] *= 0;
+            p[zidx(d, i, j, k) * NPR + B2] *= 0.;
+          }
+    }
+    if (c->bc[HGO_X2UP] == HGO_BC_POLARAXIS) {
+      for (i = -g1; i <= n1 - 1 + g1; i++)
+        for (k = 0; k < n3; k++)
+          for (j = n2; j <= n2 + g2 - 1; j++)
+            for (pl = 0; pl < NPR; pl++)
+              p[zidx(d, i, j, k) * NPR + pl] = p[zidx(d, i, (n2 - 1) + ((n2 - 1) - j + 1), k) * NPR + pl];
+      for (i = -g1; i <= n1 - 1 + g1; i++)
+        for (k = 0; k < n3; k++)
+          for (j = n2 - 1; j <= n2 - 1 + g2; j++) {
+            p[zidx(d, i, j, k) * NPR + U2] *= 0;
+            p[zidx(d, i, j, k) * NPR + B2] *= 0.;
+          }
+    }
+  }
+  if (n3 > 1 && c->bc[HGO_X3DN] == HGO_BC_PERIODIC && c->bc[HGO_X3UP] == HGO_BC_PERIODIC) {
+    for (i = -g1; i <= n1 - 1 + g1; i++)
+      for (j = -g2; j <= n2 - 1 + g2; j++) {
+        for (k = -g3; k <= -1; k++)
+          for (pl = 0; pl < NPR; pl++) p[zidx(d, i, j, k) * NPR + pl] = p[zidx(d, i, j, n3 + k) * NPR + pl];
+        for (k = n3; k <= n3 + g3 - 1; k++)
+          for (pl = 0; pl < NPR; pl++) p[zidx(d, i, j, k) * NPR + pl] = p[zidx(d, i, j, k - n3) * NPR + pl];
+      }
+  }
+}
+
+/* bound_pflag_user (boundsint.c:6-266), FLAGUTOPRIMFAIL only */
+static void bound_pflag(dom *d, int *pf)
+{
+  int n1 = d->n[1], n2 = d->n[2], n3 = d->n[3];
+  int g1 = d->ng[1], g2 = d->ng[2], g3 = d->ng[3];
+  int i, j, k;
+  const hgo_config *c = d->c;
+  if (n3 > 1 && c->bc[HGO_X3DN] == HGO_BC_PERIODIC && c->bc[HGO_X3UP] == HGO_BC_PERIODIC) {
+    for (i = -g1; i <= n1 - 1 + g1; i++)
+      for (j = -g2; j <= n2 - 1 + g2; j++) {
+        for (k = -g3; k <= -1; k++) pf[zidx(d, i, j, k)] = pf[zidx(d, i, j, n3 + k)];
+        for (k = n3; k <= n3 + g3 - 1; k++) pf[zidx(d, i, j, k)] = pf[zidx(d, i, j, k - n3)];
+      }
+  }
+  if (n1 > 1 && c->bc[HGO_X1DN] == HGO_BC_OUTFLOW)
+    for (j = -g2; j <= n2 - 1 + g2; j++)
+      for (k = -g3; k <= n3 - 1 + g3; k++)
+        for (i = -g1; i <= -1; i++) pf[zidx(d, i, j, k)] = pf[zidx(d, 0, j, k)];
+  if (n1 > 1 && c->bc[HGO_X1UP] == HGO_BC_OUTFLOW)
+    for (j = -g2; j <= n2 - 1 + g2; j++)
+      for (k = -g3; k <= n3 - 1 + g3; k++)
+        for (i = n1; i <= n1 + g1 - 1; i++) pf[zidx(d, i, j, k)] = pf[zidx(d, n1 - 1, j, k)];
+  if (n2 > 1 && c->bc[HGO_X2DN] == HGO_BC_POLARAXIS)
+    for (i = -g1; i <= n1 - 1 + g1; i++)
+      for (k = -g3; k <= n3 - 1 + g3; k++)
+        for (j = -g2; j <= -1; j++) pf[zidx(d, i, j, k)] = pf[zidx(d, i, -j - 1, k)];
+  if (n2 > 1 && c->bc[HGO_X2UP] == HGO_BC_POLARAXIS)
+    for (i = -g1; i <= n1 - 1 + g1; i++)
+      for (k = -g3; k <= n3 - 1 + g3; k++)
+        for (j = n2; j <= n2 + g2 - 1; j++) pf[zidx(d, i, j, k)] = pf[zidx(d, i, (n2 - 1) + ((n2 - 1) - j + 1), k)];
+}
+
+/* fixup_checksolution (fixup.c:460-560) */
+static void fixup_checksolution(dom *d, const double *pv, int *pf, double *gammacheck)
+{
+  int n1 = d->n[1], n2 = d->n[2], n3 = d->n[3];
+  int s1 = d->sh[1], s2 = d->sh[2], s3 = d->sh[3];
+  int i, j, k, l;
+  geomref g;
+  /* gammacheck stored on the zone grid at the zone's own index */
+  for (i = -s1; i <= n1 - 1 + s1; i++)
+    for (j = -s2; j <= n2 - 1 + s2; j++)
+      for (k = -s3; k <= n3 - 1 + s3; k++) {
+        long z = zidx(d, i, j, k);
+        get_geometry(d, i, j, CENT, &g);
+        if (gamma_calc(&pv[z * NPR], &g, &gammacheck[z])) d->err |= ERR_UTCALC_DISCR;
+      }
+  for (i = 0; i < n1; i++)
+    for (j = 0; j < n2; j++)
+      for (k = 0; k < n3; k++) {
+        long z = zidx(d, i, j, k);
+        double percdiff[8], percdiff2[8], gc = gammacheck[z], uc = pv[z * NPR + UU];
+        int vote0 = 0, vote1 = 0, numvotes = 0;
+        int im = i - s1, ip = i + s1, jm = j - s2, jp = j + s2;
+        if (!(gc >= 2.0)) continue;
+#define NB(ii, jj) zidx(d, ii, jj, k)
+#define PD(idx, ii, jj)                                                                         \
+  percdiff[idx] = (pf[NB(ii, jj)] <= UTOPRIMNOFAIL) ? (gammacheck[NB(ii, jj)] / gc) : -1;        \
+  percdiff2[idx] = (pf[NB(ii, jj)] <= UTOPRIMNOFAIL) ? (pv[NB(ii, jj) * NPR + UU] / uc) : -1;
+        PD(0, i, jp);
+        PD(1, i, jm);
+        PD(2, ip, j);
+        PD(3, im, j);
+        PD(4, ip, jp);
+        PD(5, ip, jm);
+        PD(6, ip, jp);
+        PD(7, im, jm);
+#undef PD
+#undef NB
+        for (l = 0; l < MAXVOTES; l++) {
+          if (percdiff[0] >= 0.0) {
+            if ((fabs(percdiff[l]) > GAMMAPERCDIFFMAX) || (fabs(percdiff[l]) < 1.0 / GAMMAPERCDIFFMAX)) vote0++;
+            if (((fabs(percdiff2[l]) > UPERCDIFFMAX) || (fabs(percdiff2[l]) < 1.0 / UPERCDIFFMAX))) vote1++;
+            numvotes++;
+          }
+        }
+        if (vote0 > numvotes * 0.5) pf[z] = UTOPRIMFAILGAMMAPERC;
+        if (vote1 > numvotes * 0.5) pf[z] = UTOPRIMFAILUPERC;
+      }
+}
+
+/* fixup_utoprim (fixup.c:669-1470), GENERALAVERAGE=1, ORDERINDEPENDENT=1,
+   HOWTOAVG_WHEN_U2AVG=MAXUPOSAVG, CAUSALAVG=0, TODONOGOOD=NOGOODAVERAGE,
+   STEPOVERNEG*=-1, DOCOUNTNEG*=1, ADJUSTCONSERVEDQUANTITY=0 */
+static void fixup_utoprim(dom *d, double *pv, double *ptoavg, int *pf, int finalstep)
+{
+  int n1 = d->n[1], n2 = d->n[2], n3 = d->n[3];
+  int s1 = d->sh[1], s2 = d->sh[2], s3 = d->sh[3];
+  long ntot = (long)d->nt[1] * d->nt[2] * d->nt[3];
+  int i, j, k, pl, qq;
+  int rnx = (s1 == 1) ? 3 * s1 : 1, rny = (s2 == 1) ? 3 * s2 : 1;
+  int numupairs = (int)(pow(3, s1 + s2 + s3) - 1) / 2;
+  geomref g;
+  memcpy(ptoavg, pv, sizeof(double) * NPR * ntot);
+  for (i = 0; i < n1; i++)
+    for (j = 0; j < n2; j++)
+      for (k = 0; k < n3; k++) {
+        long z = zidx(d, i, j, k);
+        int mypflag = pf[z], fixed = 0, failtype;
+        if (mypflag != 0) {
+          get_geometry(d, i, j, CENT, &g);
+          if (mypflag == UTOPRIMFAILUNEG || mypflag == UTOPRIMFAILRHONEG || mypflag == UTOPRIMFAILRHOUNEG) fixed = 1;
+          if (fixed == 0) {
+            double gamma = 1.0, mysum[2][NPR], lastmin[NPR], avganswer0[NPR], avganswer1[NPR];
+            int startpl, endpl, failavglooptype, numavg, numavg0 = 0, numavg1 = 0;
+            if (gamma_calc(&ptoavg[z * NPR], &g, &gamma)) d->err |= ERR_UTCALC_DISCR;
+            if (gamma > d->c->gammamax) gamma = d->c->gammamax;
+            if (mypflag == UTOPRIMFAILU2AVG1 || mypflag == UTOPRIMFAILU2AVG2) {
+              startpl = UU;
+              endpl = UU;
+              failavglooptype = 1;
+            } else {
+              startpl = RHO;
+              endpl = U3;
+              failavglooptype = 0;
+            }
+            for (pl = startpl; pl <= endpl; pl++) {
+              mysum[0][pl] = 0.0;
+              mysum[1][pl] = 0.0;
+              lastmin[pl] = 1E50;
+            }
+            for (qq = 0; qq < numupairs; qq++) {
+              int ii = (int)(qq % rnx) - s1;
+              int jj = (int)((qq % (rnx * rny)) / rnx) - s2;
+              int kk = (int)(qq / (rnx * rny)) - s3;
+              long za = zidx(d, i + ii, j + jj, k + kk), zb = zidx(d, i - ii, j - jj, k - kk);
+              int thisnotfail = pf[za] <= UTOPRIMNOFAIL;
+              int thatnotfail = pf[zb] <= UTOPRIMNOFAIL;
+              numavg1 += (ptoavg[za * NPR + UU] > 0.0);
+              numavg1 += (ptoavg[zb * NPR + UU] > 0.0);
+              numavg0 += thisnotfail + thatnotfail;
+              if (failavglooptype == 0) {
+                for (pl = startpl; pl <= endpl; pl++)
+                  mysum[qq % 2][pl] += ptoavg[za * NPR + pl] * thisnotfail + ptoavg[zb * NPR + pl] * thatnotfail;
+              } else {
+                for (pl = startpl; pl <= endpl; pl++) {
+                  double ftemp = ptoavg[za * NPR + pl];
+                  if (ftemp >= 0.0) lastmin[pl] = fmin_macro(lastmin[pl], ftemp);
+                  ftemp = ptoavg[zb * NPR + pl];
+                  if (ftemp >= 0.0) lastmin[pl] = fmin_macro(lastmin[pl], ftemp);
+                }
+              }
+            }
+            if (failavglooptype == 0) {
+              if (numavg0 != 0)
+                for (pl = startpl; pl <= endpl; pl++) avganswer0[pl] = (mysum[0][pl] + mysum[1][pl]) / ((double)(numavg0));
+              if (numavg0 != 0)
+                for (pl = startpl; pl <= endpl; pl++) pv[z * NPR + pl] = avganswer0[pl];
+              numavg = numavg0;
+            } else {
+              for (pl = startpl; pl <= endpl; pl++) avganswer1[pl] = lastmin[pl];
+              if (numavg1 != 0)
+                for (pl = startpl; pl <= endpl; pl++) pv[z * NPR + pl] = avganswer1[pl];
+              numavg = numavg1;
+            }
+            if (mypflag == UTOPRIMFAILU2AVG2) numavg++;
+            if (numavg == 0) {
+              /* NOGOODAVERAGE: 0.5*(AVG4_1 + AVG4_2) of ptoavg (fixup.c:562-566) */
+              for (pl = startpl; pl <= endpl; pl++) {
+                double a41 = (0.25 * ((ptoavg[zidx(d, i, j + s2, k) * NPR + pl] + ptoavg[zidx(d, i, j - s2, k) * NPR + pl]) +
+                                      (ptoavg[zidx(d, i - s1, j, k) * NPR + pl] + ptoavg[zidx(d, i + s1, j, k) * NPR + pl])));
+                double a42 = (0.25 * ((ptoavg[zidx(d, i + s1, j + s2, k) * NPR + pl] + ptoavg[zidx(d, i + s1, j - s2, k) * NPR + pl]) +
+                                      (ptoavg[zidx(d, i - s1, j + s2, k) * NPR + pl] + ptoavg[zidx(d, i - s1, j - s2, k) * NPR + pl])));
+                pv[z * NPR + pl] = 0.5 * (a41 + a42);
+              }
+            }
+            limit_gamma(gamma, &pv[z * NPR], &g, &d->err);
+          }
+        }
+        /* accounting: which failures get reset to UTOPRIMFAILFIXED */
+        if (mypflag == UTOPRIMNOFAIL) failtype = -1;
+        else if (mypflag == UTOPRIMFAILRHONEG || mypflag == UTOPRIMFAILUNEG || mypflag == UTOPRIMFAILU2AVG1 ||
+                 mypflag == UTOPRIMFAILU2AVG2 || mypflag == UTOPRIMFAILRHOUNEG)
+          failtype = finalstep ? 1 : -1;
+        else failtype = 1;
+        if (failtype != -1) pf[z] = UTOPRIMFAILFIXED;
+      }
+}
+
+/* ------------------------------------------------------------------ */
+/* drivers                                                             */
+/* ------------------------------------------------------------------ */
+
+static void dom_init(dom *d, const hgo_config *c, const hgo_geometry *g)
+{
+  int dd;
+  d->c = c;
+  d->n[1] = c->n1;
+  d->n[2] = c->n2;
+  d->n[3] = c->n3;
+  for (dd = 1; dd <= 3; dd++) {
+    d->sh[dd] = d->n[dd] > 1;
+    d->ng[dd] = d->sh[dd] ? c->ng : 0;
+    d->nt[dd] = d->n[dd] + 2 * d->ng[dd];
+  }
+  d->gt[1] = d->nt[1] + d->sh[1];
+  d->gt[2] = d->nt[2] + d->sh[2];
+  d->gcov = g->gcov;
+  d->gcon = g->gcon;
+  d->gcovpert = g->gcovpert;
+  d->gdet = g->gdet;
+  d->conn = g->conn;
+  d->floors = g->floors;
+  d->err = 0;
+}
+
+static long dom_ntot(const dom *d) { return (long)d->nt[1] * d->nt[2] * d->nt[3]; }
+
+/* source() + source_conn() at CENT (phys.c:578-752); cooling=0 so the
+   physics sources are zero and only the connection term contributes */
+static int source_conn(const dom *d, int i, int j, const double *pr, const geomref *g, double *dU)
+{
+  zstate q;
+  emstate e;
+  double mhd[NDIM][NDIM], dUconn[NPR];
+  const double *conn = d->conn + gidx(d, i, j) * 64;
+  int jj, kk, l, pl;
+  if (get_state(pr, g, &q)) return ERR_UTCALC_DISCR;
+  em_prepare(pr, g, &q, &e);
+  for (jj = 0; jj < NDIM; jj++) mhd_calc(pr, jj, d->c->gam, &q, &e, mhd[jj]);
+  for (pl = 0; pl < NPR; pl++) dUconn[pl] = 0;
+  for (l = 0; l < NDIM; l++)
+    for (jj = 0; jj < NDIM; jj++)
+      for (kk = 0; kk < NDIM; kk++) dUconn[UU + l] += mhd[jj][kk] * conn[(kk * 4 + l) * 4 + jj];
+  for (l = 0; l < NDIM; l++)
+    for (jj = 0; jj < NDIM; jj++) dUconn[UU + l] += -pr[RHO] * q.ucon[jj] * conn[(TT * 4 + l) * 4 + jj];
+  /* dU = sum over the NUMSOURCES components; only GEOMSOURCE is nonzero:
+     dUcomp[0] = 0 + g*dUconn, the other six components are 0 */
+  for (pl = 0; pl < NPR; pl++) {
+    double comp0 = 0. + g->g * dUconn[pl];
+    double acc = 0.;
+    acc += comp0;
+    for (l = 1; l < 7; l++) acc += 0.0;
+    dU[pl] = acc;
+  }
+  return 0;
+}
+
+typedef struct {
+  double CUf[4], Cunew[4];
+} rkstage;
+
+/* midpoint method tables (step_ch.c:504-524) */
+static void rk2_stage(int timeorder, rkstage *s)
+{
+  if (timeorder == 0) {
+    s->CUf[0] = 1.0; s->CUf[1] = 0.0; s->CUf[2] = 0.5; s->CUf[3] = 0.0;
+    s->Cunew[0] = 0.0; s->Cunew[1] = 0.0; s->Cunew[2] = 0.0; s->Cunew[3] = 0.0;
+  } else {
+    s->CUf[0] = 1.0; s->CUf[1] = 0.0; s->CUf[2] = 1.0; s->CUf[3] = 0.0;
+    s->Cunew[0] = 0.0; s->Cunew[1] = 0.0; s->Cunew[2] = 1.0; s->Cunew[3] = 0.0;
+  }
+}
+
+typedef struct {
+  double *dq, *emf, *ptoavg, *gammacheck;
+} scratch;
+
+/* advance_standard (advance.c:58-238) for the midpoint RK2 stage `timeorder` */
+static void advance(dom *d, const double *pi, const double *pb, double *pf, double *uf, double *ucum, double *F1,
+                    double *F2, double *F3, int *pflag, double dt, int timeorder, int numtimeorders, double *ndt,
+                    scratch *sc, long *iters)
+{
+  const hgo_config *c = d->c;
+  double ndt1, ndt2, ndt3;
+  rkstage rk;
+  int i, j, k, pl;
+  double idx1 = 1.0 / c->dx[1], idx2 = 1.0 / c->dx[2], idx3 = 1.0 / c->dx[3];
+  long o1 = (long)d->nt[2] * d->nt[3], o2 = d->nt[3], o3 = 1;
+  int finalstep = (timeorder == numtimeorders - 1);
+  rk2_stage(timeorder, &rk);
+
+  fluxcalc_dir(d, pb, 1, F1, sc->dq, &ndt1);
+  fluxcalc_dir(d, pb, 2, F2, sc->dq, &ndt2);
+  fluxcalc_dir(d, pb, 3, F3, sc->dq, &ndt3);
+  flux_ct(d, F1, F2, F3, sc->emf);
+
+  for (i = 0; i < d->n[1]; i++)
+    for (j = 0; j < d->n[2]; j++)
+      for (k = 0; k < d->n[3]; k++) {
+        long z = zidx(d, i, j, k);
+        geomref g;
+        zstate q;
+        emstate e;
+        double Ui[NPR], dUgeom[NPR], dU1[NPR], dU2[NPR], dU3[NPR], dUr[NPR], Uf[NPR];
+        int it = 0, r;
+        if (timeorder == 0)
+          for (pl = 0; pl < NPR; pl++) uf[z * NPR + pl] = ucum[z * NPR + pl] = 0.0;
+        get_geometry(d, i, j, CENT, &g);
+        if (get_state(&pi[z * NPR], &g, &q)) d->err |= ERR_UTCALC_DISCR;
+        em_prepare(&pi[z * NPR], &g, &q, &e);
+        primtoflux(&pi[z * NPR], &q, &e, TT, &g, c->gam, Ui);
+        if ((r = source_conn(d, i, j, &pb[z * NPR], &g, dUgeom))) d->err |= r;
+        /* flux2dUavg (advance.c:741-914) */
+        for (pl = 0; pl < NPR; pl++) {
+          dU1[pl] = 0;
+          dU2[pl] = 0;
+          dU3[pl] = 0;
+          if (d->n[1] > 1) dU1[pl] = (-(F1[(z + o1) * NPR + pl] - F1[z * NPR + pl]) * idx1);
+          if (d->n[2] > 1) dU2[pl] = (-(F2[(z + o2) * NPR + pl] - F2[z * NPR + pl]) * idx2);
+          if (d->n[3] > 1) dU3[pl] = (-(F3[(z + o3) * NPR + pl] - F3[z * NPR + pl]) * idx3);
+          dUr[pl] = dU1[pl] + dU2[pl] + dU3[pl];
+        }
+        /* dUtoU (advance.c:922-949) */
+        for (pl = 0; pl < NPR; pl++)
+          uf[z * NPR + pl] = Uf[pl] =
+              rk.CUf[0] * Ui[pl] + rk.CUf[1] * uf[z * NPR + pl] + rk.CUf[2] * dt * (dUr[pl] + dUgeom[pl]);
+        for (pl = 0; pl < NPR; pl++)
+          ucum[z * NPR + pl] += rk.Cunew[0] * Ui[pl] + rk.Cunew[1] * dt * (dUr[pl] + dUgeom[pl]) + rk.Cunew[2] * Uf[pl];
+        for (pl = 0; pl < NPR; pl++) pf[z * NPR + pl] = pb[z * NPR + pl];
+        if (finalstep) pflag[z] = utoprimgen(&ucum[z * NPR], &g, c, &pf[z * NPR], &it);
+        else pflag[z] = utoprimgen(Uf, &g, c, &pf[z * NPR], &it);
+        *iters += it;
+        if (finalstep) fixup1zone(&pf[z * NPR], &g, &d->floors[gidx(d, i, j) * 2], c, &d->err);
+      }
+  *ndt = c->defcon * 1. / (1. / ndt1 + 1. / ndt2 + 1. / ndt3);
+}
+
+static int alloc_scratch(const dom *d, scratch *sc)
+{
+  long n = dom_ntot(d);
+  sc->dq = (double *)calloc((size_t)n * NPR, sizeof(double));
+  sc->emf = (double *)calloc((size_t)n * 3, sizeof(double));
+  sc->ptoavg = (double *)calloc((size_t)n * NPR, sizeof(double));
+  sc->gammacheck = (double *)calloc((size_t)n, sizeof(double));
+  return (sc->dq && sc->emf && sc->ptoavg && sc->gammacheck) ? 0 : -1;
+}
+
+static void free_scratch(scratch *sc)
+{
+  free(sc->dq);
+  free(sc->emf);
+  free(sc->ptoavg);
+  free(sc->gammacheck);
+}
+
+/* one RK stage with its boundary/fixup sequence (step_ch.c:94-186) */
+static void stage_with_fixups(dom *d, const double *pi, const double *pb, double *pf, double *uf, double *ucum,
+                              double *F1, double *F2, double *F3, int *pflag, double dt, int timeorder,
+                              int numtimeorders, double *ndt, scratch *sc, long *iters)
+{
+  int finalstep = (timeorder == numtimeorders - 1);
+  /* pre_fixup: b^2 flags only (LIMADJUST=FLUXADJUST=0), no state change */
+  advance(d, pi, pb, pf, uf, ucum, F1, F2, F3, pflag, dt, timeorder, numtimeorders, ndt, sc, iters);
+  bound_prim(d, pf);
+  bound_pflag(d, pflag);
+  fixup_checksolution(d, pf, pflag, sc->gammacheck);
+  fixup_utoprim(d, pf, sc->ptoavg, pflag, finalstep);
+  bound_prim(d, pf);
+}
+
+int hgo_substep(const hgo_config *c, const hgo_geometry *g, const double *pi, const double *pb, double *pf,
+                double *uf, double *ucum, double *F1, double *F2, double *F3, int *pflag, double dt, int timeorder,
+                double *ndt, hgo_stats *st)
+{
+  dom d;
+  scratch sc;
+  long iters = 0;
+  dom_init(&d, c, g);
+  if (alloc_scratch(&d, &sc)) return -1;
+  stage_with_fixups(&d, pi, pb, pf, uf, ucum, F1, F2, F3, pflag, dt, timeorder, 2, ndt, &sc, &iters);
+  free_scratch(&sc);
+  if (st) {
+    st->newton_iters = iters;
+    st->err = d.err;
+  }
+  return d.err;
+}
+
+int hgo_step(const hgo_config *c, const hgo_geometry *g, double *p, int *pflag, double *t, double *dt, int nsteps,
+             hgo_stats *st)
+{
+  dom d;
+  scratch sc;
+  long n, iters = 0;
+  double *pk, *uf, *ucum, *F1, *F2, *F3;
+  int s, z, nf = 0;
+  dom_init(&d, c, g);
+  n = dom_ntot(&d);
+  if (alloc_scratch(&d, &sc)) return -1;
+  pk = (double *)calloc((size_t)n * NPR, sizeof(double));
+  uf = (double *)calloc((size_t)n * NPR, sizeof(double));
+  ucum = (double *)calloc((size_t)n * NPR, sizeof(double));
+  F1 = (double *)calloc((size_t)n * NPR, sizeof(double));
+  F2 = (double *)calloc((size_t)n * NPR, sizeof(double));
+  F3 = (double *)calloc((size_t)n * NPR, sizeof(double));
+  if (!pk || !uf || !ucum || !F1 || !F2 || !F3) return -1;
+  for (s = 0; s < nsteps; s++) {
+    double ndt;
+    /* pii/pbb/pff of the midpoint method: (p,p,pk0), (p,pk0,p) */
+    memcpy(pk, p, sizeof(double) * NPR * n);
+    stage_with_fixups(&d, p, p, pk, uf, ucum, F1, F2, F3, pflag, *dt, 0, 2, &ndt, &sc, &iters);
+    stage_with_fixups(&d, p, pk, p, uf, ucum, F1, F2, F3, pflag, *dt, 1, 2, &ndt, &sc, &iters);
+    /* step_ch.c:236-247 */
+    *t += *dt;
+    if (ndt > c->safe * (*dt)) ndt = c->safe * (*dt);
+    *dt = ndt;
+    if (*t + *dt > c->tf) *dt = c->tf - *t;
+  }
+  for (z = 0; z < n; z++) nf += (pflag[z] != 0);
+  free(pk);
+  free(uf);
+  free(ucum);
+  free(F1);
+  free(F2);
+  free(F3);
+  free_scratch(&sc);
+  if (st) {
+    st->newton_iters = iters;
+    st->err = d.err;
+    st->nfail_final = nf;
+  }
+  return d.err;
+}
+
+int hgo_bound_prim(const hgo_config *c, const hgo_geometry *g, double *p)
+{
+  dom d;
+  dom_init(&d, c, g);
+  bound_prim(&d, p);
+  return d.err;
+}
+
+int hgo_utoprim_batch(const double *U, const double *gcov, const double *gcon, const double *gdet, double *pr,
+                      int *pflag, long n, double gam, double gammafail, long *iters)
+{
+  hgo_config c;
+  long z;
+  long tot = 0;
+  memset(&c, 0, sizeof(c));
+  c.gam = gam;
+  c.gammafail = gammafail;
+  for (z = 0; z < n; z++) {
+    geomref g;
+    int it = 0;
+    g.gcov = gcov + z * 16;
+    g.gcon = gcon + z * 16;
+    g.gcovpert = NULL;
+    g.g = gdet[z];
+    pflag[z] = utoprimgen(&U[z * NPR], &g, &c, &pr[z * NPR], &it);
+    tot += it;
+  }
+  if (iters) *iters = tot;
+  return 0;
+}
+
+int hgo_abi_version(void) { return 1; }

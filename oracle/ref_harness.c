@@ -1,0 +1,150 @@
+/*
+ * Test harness main() for the reference HARM build (oracle/_ref).
+ *
+ * This file is NOT part of the product.  It is compiled by oracle/build_ref.py
+ * together with the reference's own sources (copied to a scratch directory,
+ * never into this repository) in place of the reference main.c
+ * (main.c:5-98).  It runs the reference's init() and step_ch() exactly as the
+ * reference main loop does (main.c:33-49: nstroke=0; step_ch(); nstep++),
+ * skipping only the diagnostics/dump cadence (diag(), postdt()), and writes the
+ * reference's own arrays to raw binary files so that the CPU restatement
+ * (oracle/harm_oracle.c) and the CUDA path can be pinned against them.
+ *
+ * usage: harm_ref <outdir> <nsteps> [dumpstep ...]
+ *   writes <outdir>/init_*  (geometry, floors, initial primitives/flags, meta)
+ *          <outdir>/s<step>_* after each listed step (and always after nsteps)
+ */
+#include "defs.h"  /* defines the reference globals, as the reference main.c does */
+#include <sys/stat.h>
+
+extern int init(int argc, char *argv[]);
+extern int step_ch(void);
+extern int error_check(int wherefrom);
+extern int set_density_floors(struct of_geom *ptrgeom, FTYPE *pr, FTYPE *prfloor);
+
+static char outdir[1024];
+
+static void wbin(const char *tag, const char *name, const void *ptr, size_t nbytes)
+{
+  char fn[2048];
+  FILE *f;
+  snprintf(fn, sizeof(fn), "%s/%s_%s.bin", outdir, tag, name);
+  f = fopen(fn, "wb");
+  if (!f) { fprintf(stderr, "harness: cannot write %s\n", fn); exit(3); }
+  if (fwrite(ptr, 1, nbytes, f) != nbytes) { fprintf(stderr, "harness: short write %s\n", fn); exit(3); }
+  fclose(f);
+}
+
+static void write_meta(const char *tag)
+{
+  char fn[2048];
+  FILE *f;
+  int pl;
+  snprintf(fn, sizeof(fn), "%s/%s_meta.txt", outdir, tag);
+  f = fopen(fn, "w");
+  if (!f) { fprintf(stderr, "harness: cannot write %s\n", fn); exit(3); }
+  fprintf(f, "N1 %d\nN2 %d\nN3 %d\nMAXBND %d\nNPR %d\nNPG %d\nNUMPFLAGS %d\n",
+          N1, N2, N3, MAXBND, NPR, NPG, NUMPFLAGS);
+  fprintf(f, "SHIFT1 %d\nSHIFT2 %d\nSHIFT3 %d\n", SHIFT1, SHIFT2, SHIFT3);
+  fprintf(f, "t %.17g\ndt %.17g\nnstep %ld\nrealnstep %ld\n", (double)t, (double)dt, nstep, realnstep);
+  fprintf(f, "gam %.17g\ncour %.17g\nSAFE %.17g\ndefcon %.17g\ntf %.17g\n",
+          (double)gam, (double)cour, (double)SAFE, (double)defcon, (double)tf);
+  fprintf(f, "dx1 %.17g\ndx2 %.17g\ndx3 %.17g\n", (double)dx[1], (double)dx[2], (double)dx[3]);
+  fprintf(f, "startx1 %.17g\nstartx2 %.17g\nstartx3 %.17g\n",
+          (double)startx[1], (double)startx[2], (double)startx[3]);
+  fprintf(f, "RHOMIN %.17g\nUUMIN %.17g\nRHOMINLIMIT %.17g\nUUMINLIMIT %.17g\n",
+          (double)RHOMIN, (double)UUMIN, (double)RHOMINLIMIT, (double)UUMINLIMIT);
+  fprintf(f, "GAMMAMAX %.17g\nGAMMAFAIL %.17g\n", (double)GAMMAMAX, (double)GAMMAFAIL);
+  fprintf(f, "a %.17g\nhslope %.17g\nRin %.17g\nRout %.17g\nR0 %.17g\n",
+          (double)a, (double)hslope, (double)Rin, (double)Rout, (double)R0);
+  fprintf(f, "lim %d\nfluxmethod %d\nFLUXB %d\nUTOPRIMVERSION %d\nTIMEORDER %d\nDOENOFLUX %d\n",
+          lim, fluxmethod, FLUXB, UTOPRIMVERSION, TIMEORDER, DOENOFLUX);
+  fprintf(f, "rescaletype %d\ndefcoord %d\n", rescaletype, defcoord);
+  for (pl = 0; pl < 6; pl++) fprintf(f, "BCtype%d %d\n", pl, BCtype[pl]);
+  fprintf(f, "failed %d\nnstroke %.17g\n", failed, (double)nstroke);
+  fclose(f);
+}
+
+static void dump_state(const char *tag, int with_fluxes)
+{
+  write_meta(tag);
+  wbin(tag, "p", a_p, sizeof(a_p));
+  wbin(tag, "pflag", a_pflag, sizeof(a_pflag));
+  if (with_fluxes) {
+    wbin(tag, "pk", a_pk, sizeof(a_pk));
+    wbin(tag, "unew", a_unew, sizeof(a_unew));
+#if(N1>1)
+    wbin(tag, "F1", a_F1, sizeof(a_F1));
+#endif
+#if(N2>1)
+    wbin(tag, "F2", a_F2, sizeof(a_F2));
+#endif
+#if(N3>1)
+    wbin(tag, "F3", a_F3, sizeof(a_F3));
+#endif
+    wbin(tag, "emf", a_emf, sizeof(a_emf));
+  }
+}
+
+static void dump_geometry(void)
+{
+  /* floors as the reference's fixup1zone() computes them at CENT
+     (fixup.c:341-447 via set_density_floors fixup.c:1542) */
+  static FTYPE floors[N1M][N2M][N3M][2];
+  struct of_geom geom;
+  FTYPE prfloor[NPR];
+  int i, j, k;
+  FULLLOOP {
+    get_geometry(i, j, k, CENT, &geom);
+    set_density_floors(&geom, p[i][j][k], prfloor);
+    floors[i + N1BND][j + N2BND][k + N3BND][0] = prfloor[RHO];
+    floors[i + N1BND][j + N2BND][k + N3BND][1] = prfloor[UU];
+  }
+  wbin("init", "floors", floors, sizeof(floors));
+  wbin("init", "gcov", a_gcov, sizeof(a_gcov));
+  wbin("init", "gcon", a_gcon, sizeof(a_gcon));
+  wbin("init", "gcovpert", a_gcovpert, sizeof(a_gcovpert));
+  wbin("init", "gdet", a_gdet, sizeof(a_gdet));
+  wbin("init", "conn", a_conn, sizeof(a_conn));
+}
+
+int main(int argc, char *argv[])
+{
+  char *fakeargv[2];
+  int nsteps, s, d, ndump = 0;
+  int dumps[64];
+
+  if (argc < 3) {
+    fprintf(stderr, "usage: %s <outdir> <nsteps> [dumpstep ...]\n", argv[0]);
+    return 2;
+  }
+  snprintf(outdir, sizeof(outdir), "%s", argv[1]);
+  mkdir(outdir, 0755);
+  nsteps = atoi(argv[2]);
+  for (d = 3; d < argc && ndump < 64; d++) dumps[ndump++] = atoi(argv[d]);
+
+  fakeargv[0] = argv[0];
+  fakeargv[1] = NULL;
+  if (init(1, fakeargv) >= 1) {
+    fprintf(stderr, "harness: init failed\n");
+    return 1;
+  }
+  dump_geometry();
+  dump_state("init", 0);
+
+  for (s = 1; s <= nsteps; s++) {
+    char tag[64];
+    int want = (s == nsteps);
+    nstroke = 0;
+    if (step_ch() != 0) { fprintf(stderr, "harness: step_ch failed at step %d\n", s); return 1; }
+    if (error_check(2)) { fprintf(stderr, "harness: error_check failed at step %d\n", s); return 1; }
+    nstep++;
+    for (d = 0; d < ndump; d++) if (dumps[d] == s) want = 1;
+    if (want) {
+      snprintf(tag, sizeof(tag), "s%d", s);
+      dump_state(tag, 1);
+    }
+  }
+  fprintf(stderr, "harness: done %d steps t=%.17g dt=%.17g\n", nsteps, (double)t, (double)dt);
+  return 0;
+}
