@@ -1,0 +1,550 @@
+// harm_device.cuh -- per-zone GRMHD physics as sm_100a device functions.
+//
+// Every function keeps the floating-point operation order of the reference
+// routine it cites, and the translation unit is compiled with -fmad=false, so
+// that the FP64 path reproduces the reference CPU build bit for bit (the
+// reference is built with -ffp-contract=off).  sqrt and '/' are IEEE
+// correctly rounded on both sides.
+//
+// Build options mirrored: WHICHVEL=VELREL4, REMOVERESTMASSFROMUU=2,
+// WHICHEOM=WITHGDET, EOMTYPE=EOMGRMHD, ideal-gas EOS (eos.c:58-194),
+// MAXWELL=PRIMMAXWELL (phys.c:140), TRUEFAST=0 (vchar.c:33),
+// UTOPRIMVERSION=UTOPRIM2DFINAL with PRECISEINVERSION=1 (u2p_defs.h).
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace hg {
+
+constexpr int NPR = 8;
+constexpr int RHO = 0, UU = 1, U1 = 2, U2 = 3, U3 = 4, B1 = 5, B2 = 6, B3 = 7;
+constexpr int TT = 0;
+
+// failure codes (global.h:782-799)
+constexpr int UTOPRIMFAILFIXED = -1;
+constexpr int UTOPRIMNOFAIL = 0;
+constexpr int UTOPRIMFAILCONVW = 2;
+constexpr int UTOPRIMFAILCONVUTSQ = 3;
+constexpr int UTOPRIMFAILCONVGUESSUTSQ = 4;
+constexpr int UTOPRIMFAILRHONEG = 9;
+constexpr int UTOPRIMFAILUNEG = 10;
+constexpr int UTOPRIMFAILRHOUNEG = 11;
+constexpr int UTOPRIMFAILGAMMAPERC = 12;
+constexpr int UTOPRIMFAILUPERC = 13;
+constexpr int UTOPRIMFAILU2AVG1 = 14;
+constexpr int UTOPRIMFAILU2AVG2 = 15;
+
+constexpr double NUMEPSILON = 2.2204460492503131e-16;
+constexpr double BIGNUM = 1.e+50;
+
+// error bits (conditions where the reference calls fail() or myexit())
+constexpr int ERR_UTCALC_DISCR = 1;
+constexpr int ERR_COEFF_NEG = 2;
+constexpr int ERR_COEFF_SUP = 4;
+constexpr int ERR_VCHAR_DISCR = 8;
+constexpr int ERR_VSQ_NEG = 16;
+constexpr int ERR_NONFINITE_SPEED = 32;
+constexpr int ERR_PREF_NEG = 64;
+
+// Metric at one grid location.  gcov is stored in full because the
+// reference's gcov is not exactly symmetric (differences ~1e-13) and its
+// routines read different triangles in different places.
+struct Metric {
+  double gcov[16];
+  double gcon[16];
+  double gcovpert_tt;
+  double g;
+};
+
+struct State {
+  double ucon[4], ucov[4], bcon[4], bcov[4];
+};
+
+// Per-state electromagnetic pieces reused by every T^dir_mu row
+// (Mcon_calc phys.c:178, lower_A phys.ffde.c:1707, Msq and 1+u_t).
+struct EM {
+  double Mcon[4][4];
+  double Mcov[4][4];
+  double Msq;
+  double plus1ud0;
+};
+
+#define GCOV(m, a, b) ((m).gcov[(a) * 4 + (b)])
+#define GCON(m, a, b) ((m).gcon[(a) * 4 + (b)])
+
+__device__ __forceinline__ double dot4(const double *a, const double *b) {
+  return a[0] * b[0] + a[1] * b[1] + a[2] * b[2] + a[3] * b[3];
+}
+
+// lower_vec (phys.c:766-787)
+__device__ __forceinline__ void lower_vec(const double *ucon, const Metric &m, double *ucov) {
+  ucov[0] = GCOV(m, 0, 0) * ucon[0] + GCOV(m, 0, 1) * ucon[1] + GCOV(m, 0, 2) * ucon[2] + GCOV(m, 0, 3) * ucon[3];
+  ucov[1] = GCOV(m, 0, 1) * ucon[0] + GCOV(m, 1, 1) * ucon[1] + GCOV(m, 1, 2) * ucon[2] + GCOV(m, 1, 3) * ucon[3];
+  ucov[2] = GCOV(m, 0, 2) * ucon[0] + GCOV(m, 1, 2) * ucon[1] + GCOV(m, 2, 2) * ucon[2] + GCOV(m, 2, 3) * ucon[3];
+  ucov[3] = GCOV(m, 0, 3) * ucon[0] + GCOV(m, 1, 3) * ucon[1] + GCOV(m, 2, 3) * ucon[2] + GCOV(m, 3, 3) * ucon[3];
+}
+
+// raise_vec (phys.c:826-846)
+__device__ __forceinline__ void raise_vec(const double *ucov, const Metric &m, double *ucon) {
+  ucon[0] = GCON(m, 0, 0) * ucov[0] + GCON(m, 0, 1) * ucov[1] + GCON(m, 0, 2) * ucov[2] + GCON(m, 0, 3) * ucov[3];
+  ucon[1] = GCON(m, 0, 1) * ucov[0] + GCON(m, 1, 1) * ucov[1] + GCON(m, 1, 2) * ucov[2] + GCON(m, 1, 3) * ucov[3];
+  ucon[2] = GCON(m, 0, 2) * ucov[0] + GCON(m, 1, 2) * ucov[1] + GCON(m, 2, 2) * ucov[2] + GCON(m, 2, 3) * ucov[3];
+  ucon[3] = GCON(m, 0, 3) * ucov[0] + GCON(m, 1, 3) * ucov[1] + GCON(m, 2, 3) * ucov[2] + GCON(m, 3, 3) * ucov[3];
+}
+
+// qsq_calc (phys.c:1077-1090) on the relative 4-velocity u~^i
+__device__ __forceinline__ double qsq_calc(double u1, double u2, double u3, const Metric &m) {
+  return +GCOV(m, 1, 1) * u1 * u1 + GCOV(m, 2, 2) * u2 * u2 + GCOV(m, 3, 3) * u3 * u3 +
+         2. * (GCOV(m, 1, 2) * u1 * u2 + GCOV(m, 1, 3) * u1 * u3 + GCOV(m, 2, 3) * u2 * u3);
+}
+
+// gamma_calc (phys.c:1022-1074); returns nonzero if qsq is negative beyond
+// round-off (the reference calls fail(FAIL_UTCALC_DISCR))
+__device__ __forceinline__ int gamma_calc(const double *pr, const Metric &m, double *gamma) {
+  double qsq = qsq_calc(pr[U1], pr[U2], pr[U3], m);
+  if (qsq < 0.0) {
+    if (qsq > -NUMEPSILON * 100) qsq = 0.0;
+    else return 1;
+  }
+  *gamma = sqrt(1. + qsq);
+  return 0;
+}
+
+// ucon_calc_rel4vel (phys.c:983-1019)
+__device__ __forceinline__ int ucon_calc(const double *pr, const Metric &m, double *ucon) {
+  double alpha = 1. / sqrt(-GCON(m, 0, 0));
+  double beta1 = GCON(m, 0, 1) * alpha * alpha;
+  double beta2 = GCON(m, 0, 2) * alpha * alpha;
+  double beta3 = GCON(m, 0, 3) * alpha * alpha;
+  double gamma;
+  if (gamma_calc(pr, m, &gamma)) return 1;
+  ucon[0] = gamma / alpha;
+  ucon[1] = pr[U1] - ucon[0] * beta1;
+  ucon[2] = pr[U2] - ucon[0] * beta2;
+  ucon[3] = pr[U3] - ucon[0] * beta3;
+  return 0;
+}
+
+// get_state (phys.c:849-859) with bcon_calc (phys.c:309-318)
+__device__ __forceinline__ int get_state(const double *pr, const Metric &m, State &q) {
+  if (ucon_calc(pr, m, q.ucon)) return 1;
+  lower_vec(q.ucon, m, q.ucov);
+  q.bcon[0] = pr[B1] * q.ucov[1] + pr[B2] * q.ucov[2] + pr[B3] * q.ucov[3];
+#pragma unroll
+  for (int j = 1; j <= 3; j++) q.bcon[j] = (pr[B1 - 1 + j] + q.bcon[0] * q.ucon[j]) / q.ucon[0];
+  lower_vec(q.bcon, m, q.bcov);
+  return 0;
+}
+
+// compute_1plusud0 (phys.c:541-575)
+__device__ __forceinline__ double compute_1plusud0(const Metric &m, const State &q) {
+  double vcon[4];
+#pragma unroll
+  for (int j = 1; j < 4; j++) vcon[j] = q.ucon[j] / q.ucon[0];
+  double plus1gv00 = m.gcovpert_tt;
+  double vsq = m.gcovpert_tt;
+#pragma unroll
+  for (int j = 1; j < 4; j++) vsq += 2.0 * GCOV(m, 0, j) * vcon[j];
+#pragma unroll
+  for (int j = 1; j < 4; j++)
+#pragma unroll
+    for (int k = 1; k < 4; k++) vsq += GCOV(m, j, k) * vcon[j] * vcon[k];
+  double gvtt = GCOV(m, 0, 0);
+  double alpha = 0.0;
+#pragma unroll
+  for (int j = 1; j < 4; j++) alpha += GCOV(m, j, 0) * q.ucon[j];
+  double uu0 = q.ucon[0];
+  return alpha + ((1.0 - gvtt) * plus1gv00 - uu0 * uu0 * vsq * gvtt * gvtt) / (1.0 - gvtt * uu0);
+}
+
+// Mcon_calc PRIMMAXWELL (phys.c:178-210), lower_A (phys.ffde.c:1707-1735),
+// Msq (phys.ffde.c:1507) and 1+u_t
+__device__ __forceinline__ void em_prepare(const double *pr, const Metric &m, const State &q, EM &e) {
+#pragma unroll
+  for (int j = 0; j < 4; j++) e.Mcon[j][j] = 0.0;
+#pragma unroll
+  for (int k = 1; k < 4; k++) {
+    e.Mcon[k][0] = pr[B1 + k - 1];
+    e.Mcon[0][k] = -e.Mcon[k][0];
+  }
+#pragma unroll
+  for (int j = 1; j < 4; j++)
+#pragma unroll
+    for (int k = 1; k < 4; k++) e.Mcon[j][k] = (pr[B1 + j - 1] * q.ucon[k] - pr[B1 + k - 1] * q.ucon[j]) / q.ucon[0];
+  double a01 = 0., a02 = 0., a03 = 0., a12 = 0., a23 = 0., a31 = 0.;
+#pragma unroll
+  for (int j = 0; j < 4; j++)
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+      double A = e.Mcon[j][k];
+      a01 += (GCOV(m, 0, j)) * (GCOV(m, 1, k)) * A;
+      a02 += (GCOV(m, 0, j)) * (GCOV(m, 2, k)) * A;
+      a03 += (GCOV(m, 0, j)) * (GCOV(m, 3, k)) * A;
+      a12 += (GCOV(m, 1, j)) * (GCOV(m, 2, k)) * A;
+      a23 += (GCOV(m, 2, j)) * (GCOV(m, 3, k)) * A;
+      a31 += (GCOV(m, 3, j)) * (GCOV(m, 1, k)) * A;
+    }
+  e.Mcov[0][0] = 0.;
+  e.Mcov[1][1] = 0.;
+  e.Mcov[2][2] = 0.;
+  e.Mcov[3][3] = 0.;
+  e.Mcov[0][1] = a01;
+  e.Mcov[0][2] = a02;
+  e.Mcov[0][3] = a03;
+  e.Mcov[1][2] = a12;
+  e.Mcov[2][3] = a23;
+  e.Mcov[3][1] = a31;
+  e.Mcov[1][0] = -a01;
+  e.Mcov[2][0] = -a02;
+  e.Mcov[3][0] = -a03;
+  e.Mcov[2][1] = -a12;
+  e.Mcov[3][2] = -a23;
+  e.Mcov[1][3] = -a31;
+  double Msq = 0.;
+#pragma unroll
+  for (int j = 0; j < 4; j++)
+#pragma unroll
+    for (int k = 0; k < 4; k++) Msq += e.Mcov[j][k] * e.Mcon[j][k];
+  e.Msq = Msq;
+  e.plus1ud0 = compute_1plusud0(m, q);
+}
+
+// mhd_calc_norestmass (phys.c:442-506) + ffdestresstensor_dir
+// (phys.ffde.c:1483-1515): one row T^dir_mu without rest mass
+__device__ __forceinline__ void mhd_row(const double *pr, int dir, double gam, const State &q, const EM &e, double *mhd) {
+  double rho = pr[RHO], u = pr[UU];
+  double P = (gam - 1.) * u;
+  double w = P + rho + u;
+  double eta = w, ptot = P;
+  mhd[0] = (P + u) * q.ucon[dir] * q.ucov[0] + rho * q.ucon[dir] * e.plus1ud0 + ptot * ((dir == 0) ? 1. : 0.);
+#pragma unroll
+  for (int j = 1; j < 4; j++) mhd[j] = eta * q.ucon[dir] * q.ucov[j] + ptot * ((dir == j) ? 1. : 0.);
+  double TEM[4];
+#pragma unroll
+  for (int j = 0; j < 4; j++) {
+    TEM[j] = 0.;
+#pragma unroll
+    for (int i = 0; i < 4; i++) TEM[j] += e.Mcon[dir][i] * e.Mcov[j][i];
+  }
+  TEM[dir] -= 0.25 * e.Msq;
+#pragma unroll
+  for (int j = 0; j < 4; j++) mhd[j] += TEM[j];
+}
+
+// primtoflux (phys.c:16-55), UEVOLVE, every EOM factor = gdet
+__device__ __forceinline__ void primtoflux(const double *pr, const State &q, const EM &e, int dir, const Metric &m,
+                                           double gam, double *flux) {
+  double fin[NPR];
+  fin[RHO] = pr[RHO] * q.ucon[dir];
+  mhd_row(pr, dir, gam, q, e, &fin[UU]);
+  if (dir > 0) {
+    fin[B1] = (pr[B1] * q.ucon[dir] - pr[B1 + dir - 1] * q.ucon[1]) / q.ucon[0];
+    fin[B2] = (pr[B2] * q.ucon[dir] - pr[B1 + dir - 1] * q.ucon[2]) / q.ucon[0];
+    fin[B3] = (pr[B3] * q.ucon[dir] - pr[B1 + dir - 1] * q.ucon[3]) / q.ucon[0];
+  } else {
+    fin[B1] = pr[B1];
+    fin[B2] = pr[B2];
+    fin[B3] = pr[B3];
+  }
+#pragma unroll
+  for (int pl = 0; pl < NPR; pl++) flux[pl] = fin[pl] * m.g;
+}
+
+// simplefast (vchar.c:213-312) with Acov = e_dir, Bcov = e_t
+__device__ __forceinline__ int simplefast(int dir, const Metric &m, const State &q, double cms2, double *vmin,
+                                          double *vmax) {
+  double Acov[4] = {0., 0., 0., 0.}, Bcov[4] = {0., 0., 0., 0.}, Acon[4], Bcon[4];
+  Acov[dir] = 1.;
+  raise_vec(Acov, m, Acon);
+  Bcov[0] = 1.;
+  raise_vec(Bcov, m, Bcon);
+  double Asq = dot4(Acon, Acov);
+  double Bsq = dot4(Bcon, Bcov);
+  double Au = dot4(Acov, q.ucon);
+  double Bu = dot4(Bcov, q.ucon);
+  double AB = dot4(Acon, Bcov);
+  double Au2 = Au * Au;
+  double Bu2 = Bu * Bu;
+  double AuBu = Au * Bu;
+  double A = Bu2 * (1.0 - cms2) - Bsq * cms2;
+  double B = 2. * (AuBu * (1.0 - cms2) - AB * cms2);
+  double discr = 4.0 * cms2 * ((AB * AB - Asq * Bsq) * cms2 + (2.0 * AB * Au * Bu - Asq * Bu2 - Bsq * Au2) * (cms2 - 1.0));
+  if ((discr < 0.0) && (discr > -1E-10)) discr = 0.0;
+  else if (discr < 0.0) return ERR_VCHAR_DISCR;
+  discr = sqrt(discr);
+  double vm = -(-B + discr) / (2. * A);
+  double vp = -(-B - discr) / (2. * A);
+  if ((!isfinite(vm)) || (!isfinite(vp))) return ERR_NONFINITE_SPEED;
+  if (vp < vm) {
+    *vmax = vm;
+    *vmin = vp;
+  } else {
+    *vmax = vp;
+    *vmin = vm;
+  }
+  return 0;
+}
+
+// vchar (vchar.c:37-171)
+__device__ __forceinline__ int vchar(const double *pr, const State &q, int dir, const Metric &m, double gam,
+                                     double *vmax, double *vmin) {
+  double bsq = dot4(q.bcon, q.bcov);
+  double rho = pr[RHO], u = pr[UU], cs2, va2, EF, WW, P;
+  if (u < 0) u = 0;
+  if (rho < 0) rho = 0;
+  P = (gam - 1.) * u;
+  WW = rho + u + P;
+  if (WW > 0.0) {
+    double pressure = (gam - 1.) * u;
+    double h = rho + u + pressure;
+    cs2 = gam * pressure / h;
+  } else WW = cs2 = 0.0;
+  if (cs2 >= 1.0) cs2 = 1.0 - 1e-9;
+  else if (cs2 <= 0.0) cs2 = 0.0;
+  EF = bsq + WW;
+  if (EF > 0.0) va2 = bsq / EF;
+  else EF = va2 = 0.0;
+  double cms2 = cs2 + va2 - cs2 * va2;
+  if (cms2 < 0.0) {
+    if (cms2 / (cs2 + va2) > -NUMEPSILON * 100.0) cms2 = 0.0;
+    else return ERR_COEFF_NEG;
+  }
+  if (cms2 > 1.) {
+    if (cms2 < 1.0 + NUMEPSILON * 100.0) cms2 = 1.0;
+    else if (rho < 0.0) cms2 = 1.0;
+    else return ERR_COEFF_SUP;
+  }
+  return simplefast(dir, m, q, cms2, vmin, vmax);
+}
+
+__device__ __forceinline__ double max_ref(double a, double b) { return (a > b) ? a : b; }  // phys.c:1797
+__device__ __forceinline__ double min_ref(double a, double b) { return (a > b) ? b : a; }  // phys.c:1804
+__device__ __forceinline__ double min_macro(double a, double b) { return ((a) < (b)) ? (a) : (b); }  // global.h:751
+
+// limit_gamma (fixup.c:1859-1905); returns -1 if it changed pr
+__device__ __forceinline__ int limit_gamma(double gammamax, double *pr, const Metric &m, int *err) {
+  if (gammamax <= 1.0) return 0;
+  double gamma;
+  if (gamma_calc(pr, m, &gamma)) {
+    *err |= ERR_UTCALC_DISCR;
+    return 1;
+  }
+  if ((gamma > gammamax && (gamma != 1.0))) {
+    double pref = (gammamax * gammamax - 1.) / (gamma * gamma - 1.);
+    if (pref < 0.0) {
+      *err |= ERR_PREF_NEG;
+      return 1;
+    }
+    double f = sqrt(pref);
+    pr[U1] *= f;
+    pr[U2] *= f;
+    pr[U3] *= f;
+    return -1;
+  }
+  return 0;
+}
+
+// ---------------------------------------------------------------------------
+// Con-to-prim: Utoprimgen (utoprimgen.c:23) -> Utoprim_2d_final
+// (utoprim_2d_final.c:34-453) with the 2D Newton on (W, v^2)
+// (general_newton_raphson :736-1119, func_vsq2 :1189-1278, USE_LINE_SEARCH=-2)
+// ---------------------------------------------------------------------------
+struct U2P {
+  double Bsq, QdotBsq, Qtsq, Qdotn, D, wglobal, gam, gammasq_too_big, vsq_too_big;
+};
+
+__device__ __forceinline__ double vsq_calc(const U2P &c, double W) {
+  double Wsq = W * W;
+  double Xsq = (c.Bsq + W) * (c.Bsq + W);
+  return ((Wsq * c.Qtsq + c.QdotBsq * (c.Bsq + 2. * W)) / (Wsq * Xsq));
+}
+
+// func_vsq2 with the EOS pieces of utoprim_jon_eos.c (pressure_W_vsq :83,
+// dpdW_calc_vsq :214, dpdvsq_calc :316) for the ideal gas
+__device__ __forceinline__ void func_vsq2(const U2P &c, double W, double vsq, double *dx0, double *dx1, double *f,
+                                          double *df) {
+  double Wsq = W * W;
+  double D = c.D;
+  double gamma = 1.0 / sqrt(1.0 - vsq);
+  double gammasq = gamma * gamma;
+  double Wp = W - D;
+  double wmrho0 = (Wp / gammasq - D * vsq / (1.0 + gamma));
+  double igr = (c.gam - 1.0) / c.gam;
+  double p_tmp = igr * wmrho0;
+  double dPdW = 0.0 * 0.0 + (1.0 - vsq) * igr;
+  double dwmrho0dvsq = (D * (gamma * 0.5 - 1.0) - Wp);
+  double drho0dvsq = -D * gamma * 0.5;
+  double dPdvsq = drho0dvsq * 0.0 + dwmrho0dvsq * igr;
+  double Bsq = c.Bsq, QdotBsq = c.QdotBsq, Qtsq = c.Qtsq, Qdotn = c.Qdotn;
+  double t2 = -0.5 * Bsq + dPdvsq;
+  double t3 = Bsq + W;
+  double t4 = t3 * t3;
+  double t9 = 1 / Wsq;
+  double t11 = Qtsq - vsq * t4 + QdotBsq * (Bsq + 2.0 * W) * t9;
+  double t16 = QdotBsq * t9;
+  double t18 = -Qdotn - 0.5 * Bsq * (1.0 + vsq) + 0.5 * t16 - W + p_tmp;
+  double t21 = 1 / t3;
+  double t23 = 1 / W;
+  double t24 = t16 * t23;
+  double t25 = -1.0 + dPdW - t24;
+  double t35 = t25 * t3 + (Bsq - 2.0 * dPdvsq) * (QdotBsq + vsq * Wsq * W) * t9 * t23;
+  double t36 = 1 / t35;
+  *dx0 = -(t2 * t11 + t4 * t18) * t21 * t36;
+  double t40 = (vsq + t24) * t3;
+  *dx1 = -(-t25 * t11 - 2.0 * t40 * t18) * t21 * t36;
+  *df = -t11 * t11 - t18 * t18;
+  *f = -0.5 * (*df);
+}
+
+// Inversion of the evolved conserved vector U (includes gdet) with guess in
+// prim; returns the pflag code and the Newton iteration count.
+__device__ __forceinline__ int utoprimgen(const double *U, const Metric &m, double gam, double gammafail, double *prim,
+                                          int *iters) {
+  constexpr int MAX_NEWT_ITER = 200;
+  constexpr double NEWT_TOL = 1E3 * NUMEPSILON;
+  constexpr double MIN_NEWT_TOL = 1E-6;
+  constexpr double MAXNEGUTSQ = 1E-10;
+  const double MAXNEGVSQ = (1.0 - 1.0 / (MAXNEGUTSQ + 1.0));
+  U2P c;
+  c.gam = gam;
+  c.gammasq_too_big = gammafail * gammafail;
+  c.vsq_too_big = (c.gammasq_too_big - 1.0) / (c.gammasq_too_big);
+  double Ugf[NPR], Ut[NPR];
+  // UtoU(UEVOLVE->UNOTHING) and rest-mass convention (utoprimgen.c:55,76-85)
+#pragma unroll
+  for (int pl = 0; pl < NPR; pl++) Ugf[pl] = U[pl] / m.g;
+  Ugf[UU] -= Ugf[RHO];
+  // Utoprim_2d_final (utoprim_2d_final.c:34-117)
+  prim[B1] = Ugf[B1];
+  prim[B2] = Ugf[B2];
+  prim[B3] = Ugf[B3];
+  double alpha = 1.0 / sqrt(-GCON(m, 0, 0));
+#pragma unroll
+  for (int i = 0; i < NPR; i++) Ut[i] = alpha * Ugf[i];
+  // Utoprim_new_body (:152-453)
+  double Bcon[4], Bcov[4], Qcov[4], Qcon[4], ncov[4], ncon[4];
+  Bcon[0] = 0.;
+  Bcon[1] = Ut[B1];
+  Bcon[2] = Ut[B2];
+  Bcon[3] = Ut[B3];
+#pragma unroll
+  for (int i = 0; i < 4; i++) {
+    double s = 0.;
+#pragma unroll
+    for (int j = 0; j < 4; j++) s += GCOV(m, i, j) * Bcon[j];
+    Bcov[i] = s;
+  }
+#pragma unroll
+  for (int i = 0; i < 4; i++) Qcov[i] = Ut[UU + i];
+#pragma unroll
+  for (int i = 0; i < 4; i++) {
+    double s = 0.;
+#pragma unroll
+    for (int j = 0; j < 4; j++) s += GCON(m, i, j) * Qcov[j];
+    Qcon[i] = s;
+  }
+  double Bsq = 0.;
+#pragma unroll
+  for (int i = 1; i < 4; i++) Bsq += Bcon[i] * Bcov[i];
+  c.Bsq = Bsq;
+  double QdotB = 0.;
+#pragma unroll
+  for (int i = 0; i < 4; i++) QdotB += Qcov[i] * Bcon[i];
+  c.QdotBsq = QdotB * QdotB;
+  double lapse = sqrt(-1. / GCON(m, 0, 0));
+  ncov[0] = -lapse;
+  ncov[1] = 0.;
+  ncov[2] = 0.;
+  ncov[3] = 0.;
+#pragma unroll
+  for (int i = 0; i < 4; i++) {
+    double s = 0.;
+#pragma unroll
+    for (int j = 0; j < 4; j++) s += GCON(m, i, j) * ncov[j];
+    ncon[i] = s;
+  }
+  c.Qdotn = Qcon[0] * ncov[0];
+  double Qsq = 0.;
+#pragma unroll
+  for (int i = 0; i < 4; i++) Qsq += Qcov[i] * Qcon[i];
+  c.Qtsq = Qsq + c.Qdotn * c.Qdotn;
+  c.D = Ut[RHO];
+  double utsq = 0.;
+#pragma unroll
+  for (int i = 1; i < 4; i++)
+#pragma unroll
+    for (int j = 1; j < 4; j++) utsq += GCOV(m, i, j) * prim[U1 + i - 1] * prim[U1 + j - 1];
+  *iters = 0;
+  if ((utsq < 0.) && (fabs(utsq) < MAXNEGUTSQ)) utsq = 0.0;
+  if (utsq < 0. || utsq > ((gammafail - 1.0) * (gammafail - 1.0))) return UTOPRIMFAILCONVGUESSUTSQ;
+  double gammasq = 1. + utsq;
+  double gamma = sqrt(gammasq);
+  double rho0 = c.D / gamma;
+  double u = prim[UU];
+  double p = (gam - 1.) * u;
+  double w = rho0 + u + p;
+  double W_last = w * gammasq;
+  int i_increase = 0;
+  while (((W_last * W_last * W_last * (W_last + 2. * c.Bsq) - c.QdotBsq * (2. * W_last + c.Bsq)) <=
+          W_last * W_last * (c.Qtsq - c.Bsq * c.Bsq)) &&
+         (i_increase < 10)) {
+    W_last *= 10.;
+    i_increase++;
+  }
+  c.wglobal = w;
+  // find_root_2D_gen (:573-644)
+  double x0 = fabs(W_last);
+  double vs0 = vsq_calc(c, W_last);
+  double x1 = (vs0 > 1.) ? c.vsq_too_big : vs0;
+  // general_newton_raphson (:736-1119) with plain Newton steps
+  double f = 1., df = 1., errx = 1.;
+  int n_iter = 0;
+  bool keep = true;
+  while (keep) {
+    double dx0, dx1;
+    func_vsq2(c, x0, x1, &dx0, &dx1, &f, &df);
+    double x0old = x0;
+    x0 += dx0;
+    x1 += dx1;
+    errx = (x0 == 0.) ? fabs(dx0) : fabs(dx0 / x0);
+    // validate_x (:708-728)
+    x0 = fabs(x0);
+    x0 = (x0 / c.wglobal > c.gammasq_too_big) ? x0old : x0;
+    x1 = (x1 > 1.) ? c.vsq_too_big : x1;
+    if ((fabs(errx) <= NEWT_TOL) || (n_iter >= (MAX_NEWT_ITER - 1))) keep = false;
+    n_iter++;
+  }
+  *iters = n_iter;
+  int retval = 0;
+  if ((isfinite(f) == 0) || (isfinite(df) == 0) || (isfinite(x0) == 0) || (isfinite(x1) == 0)) retval = 1;
+  else if (fabs(errx) > MIN_NEWT_TOL) retval = 1;
+  double W = x0;
+  if ((retval != 0) || (W == 1.e30)) return retval * 100 + 1;
+  double Wtest = W / c.wglobal;
+  if (Wtest <= 0. || Wtest > c.gammasq_too_big) return UTOPRIMFAILCONVW;
+  double vsq = vsq_calc(c, W);
+  if ((vsq < 0.) && (fabs(vsq) < MAXNEGVSQ)) vsq = 0.0;
+  if ((vsq > c.vsq_too_big) || (vsq < 0.0)) return UTOPRIMFAILCONVUTSQ;
+  double gtmp = sqrt(1. - vsq);
+  gamma = 1. / gtmp;
+  rho0 = c.D * gtmp;
+  w = W * (1. - vsq);
+  p = ((gam - 1.0) / gam) * (w - rho0);
+  u = w - (rho0 + p);
+  int lpflag = UTOPRIMNOFAIL;
+  if ((rho0 <= 0.) || (u < 0.)) {
+    if ((rho0 <= 0.) && (u >= 0.)) lpflag = UTOPRIMFAILRHONEG;
+    if ((rho0 > 0.) && (u < 0.)) lpflag = UTOPRIMFAILUNEG;
+    if ((rho0 <= 0.) && (u < 0.)) lpflag = UTOPRIMFAILRHOUNEG;
+  }
+  prim[RHO] = rho0;
+  prim[UU] = u;
+#pragma unroll
+  for (int i = 1; i < 4; i++) {
+    double Qtcon = Qcon[i] + ncon[i] * c.Qdotn;
+    prim[U1 + i - 1] = gamma / (W + c.Bsq) * (Qtcon + QdotB * Bcon[i] / W);
+  }
+  return lpflag;
+}
+
+}  // namespace hg

@@ -1,0 +1,1557 @@
+// harm_gpu.cu -- sm_100a kernels of HARM's per-zone conservative update and
+// the C ABI declared in include/harmgpu.h.
+//
+// Device data layout (resident in HBM for the whole run):
+//   primitives, conserved accumulators, fluxes: SoA planes [8][nt1][nt2][nt3]
+//     with x3 fastest, so that the 32 threads of a warp walk x3 at one (i,j)
+//     and read one metric row (broadcast) -- the metric depends on (i,j) only.
+//   geometry: SoA [component][gt1*gt2], 205 doubles per (i,j):
+//     4 locations (FACE1, FACE2, FACE3, CENT) x {gcov 16, gcon 16, gcovpert_tt, gdet},
+//     CORN1..3 gdet, conn[64] at CENT, floors[2].
+//
+// Work per RK substep (the reference's advance(), step_ch.c:94-186):
+//   flux_kernel<dir>  fluxcalc_standard (flux.c:469-680) fused with the MC
+//                     slopes, both Riemann states, vchar, HLL/LaxF, the gdet
+//                     strip of flux_ct and the dt-min
+//   emf_kernel        corner EMFs of flux_ct (fluxct.c:148-218)
+//   update_kernel     advance_standard zone loop (advance.c:143-213): U(pi),
+//                     source_conn, flux divergence (B fluxes rebuilt from the
+//                     EMFs, fluxct.c:724-781), dUtoU, Utoprimgen, fixup1zone
+//   bound kernels     bound_prim (bounds.fishmon.c:29-345)
+//   fixup kernels     post_fixup (fixup.c:37-96) in an order-independent
+//                     formulation that reproduces the reference's sequential
+//                     sweep exactly (see checksol_resolve / fixup_compute)
+//   finalize_kernel   ndt combine (advance.c:231) and dt update (step_ch.c:236-247)
+#include <cuda_runtime.h>
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+
+#include <new>
+#include <vector>
+
+#include "harm_device.cuh"
+#include "harmgpu.h"
+
+using namespace hg;
+
+namespace {
+
+thread_local char g_errbuf[512] = "";
+
+void set_err(const char *fmt, const char *a = "", int b = 0) {
+  snprintf(g_errbuf, sizeof(g_errbuf), fmt, a, b);
+}
+
+#define CUDA_TRY(call)                                                         \
+  do {                                                                         \
+    cudaError_t e__ = (call);                                                  \
+    if (e__ != cudaSuccess) {                                                  \
+      set_err("CUDA error: %s (line %d)", cudaGetErrorString(e__), __LINE__);  \
+      return HGPU_E_CUDA;                                                      \
+    }                                                                          \
+  } while (0)
+
+// geometry component offsets
+constexpr int GLOC = 34;                  // per location: gcov 16, gcon 16, gcovpert_tt, gdet
+constexpr int G_FACE1 = 0, G_FACE2 = 1, G_FACE3 = 2, G_CENT = 3;
+constexpr int G_CORN = 4 * GLOC;          // CORN1, CORN2, CORN3 gdet
+constexpr int G_CONN = G_CORN + 3;        // 64
+constexpr int G_FLOOR = G_CONN + 64;      // 2
+constexpr int G_NCOMP = G_FLOOR + 2;      // 205
+
+// reference location ids (global.h:948-955)
+constexpr int R_FACE1 = 0, R_FACE2 = 1, R_FACE3 = 2, R_CORN1 = 3, R_CORN2 = 4, R_CORN3 = 5, R_CENT = 7;
+
+struct Dims {
+  int n1, n2, n3;
+  int g1, g2, g3;
+  int nt1, nt2, nt3;
+  int s1, s2, s3;
+  int gt1, gt2;
+  long long nz, nij;
+};
+
+struct Params {
+  double gam, cour, gammamax, gammafail, rhominlimit, uuminlimit, defcon, safe, tf;
+  double dx1, dx2, dx3;
+  int lim, flux;
+  int bc[6];
+};
+
+// device scalars
+struct Scalars {
+  double t, dt;
+  unsigned long long ndtbits[4];   // per-direction min of cour*dx/ctop as ordered bits
+  unsigned long long iters;        // Newton iterations
+  int err;
+  int nfail;                       // failures after Utoprimgen in the last stage
+  int ncand;                       // checksolution candidates
+  int nfixlist;                    // fixup_utoprim list length
+  int nfixed;
+  int overflow;
+};
+
+__device__ __forceinline__ long long zix(const Dims &d, int i, int j, int k) {
+  return ((long long)(i + d.g1) * d.nt2 + (j + d.g2)) * d.nt3 + (k + d.g3);
+}
+__device__ __forceinline__ long long gix(const Dims &d, int i, int j) {
+  return (long long)(i + d.g1) * d.gt2 + (j + d.g2);
+}
+
+__device__ __forceinline__ void load_metric(const double *__restrict__ G, const Dims &d, long long ij, int slot,
+                                            Metric &m) {
+  const double *b = G + (long long)slot * GLOC * d.nij + ij;
+#pragma unroll
+  for (int q = 0; q < 16; q++) m.gcov[q] = __ldg(b + (long long)q * d.nij);
+#pragma unroll
+  for (int q = 0; q < 16; q++) m.gcon[q] = __ldg(b + (long long)(16 + q) * d.nij);
+  m.gcovpert_tt = __ldg(b + (long long)32 * d.nij);
+  m.g = __ldg(b + (long long)33 * d.nij);
+}
+
+__device__ __forceinline__ void load_prim(const double *__restrict__ P, const Dims &d, long long z, double *pr) {
+#pragma unroll
+  for (int v = 0; v < NPR; v++) pr[v] = P[(long long)v * d.nz + z];
+}
+__device__ __forceinline__ void store_prim(double *__restrict__ P, const Dims &d, long long z, const double *pr) {
+#pragma unroll
+  for (int v = 0; v < NPR; v++) P[(long long)v * d.nz + z] = pr[v];
+}
+
+// box iteration helper: flat index -> (i,j,k) with k fastest
+struct Box {
+  int i0, j0, k0, ni, nj, nk;
+  __host__ __device__ long long size() const { return (long long)ni * nj * nk; }
+};
+__device__ __forceinline__ void box_ijk(const Box &b, long long t, int &i, int &j, int &k) {
+  k = (int)(t % b.nk);
+  long long r = t / b.nk;
+  j = (int)(r % b.nj);
+  i = (int)(r / b.nj);
+  i += b.i0;
+  j += b.j0;
+  k += b.k0;
+}
+
+__device__ __forceinline__ void warp_min_atomic(unsigned long long *dst, double v, bool active) {
+  unsigned long long bits = active ? (unsigned long long)__double_as_longlong(v) : 0xFFFFFFFFFFFFFFFFull;
+  // NaN is never selected by the reference's `if (dtij < ndt)`: map it out
+  if (active && !(v == v)) bits = 0xFFFFFFFFFFFFFFFFull;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    unsigned long long ob = __shfl_xor_sync(0xffffffffu, bits, o);
+    bits = ob < bits ? ob : bits;
+  }
+  if ((threadIdx.x & 31) == 0 && bits != 0xFFFFFFFFFFFFFFFFull) atomicMin(dst, bits);
+}
+
+// MC / VANL / MINM / DONOR slopes (interppoint.c:387-443)
+__device__ __forceinline__ double slope3(int lim, double yl, double yc, double yr) {
+  if (lim == HGPU_LIM_MC) {
+    double Dqm = 2.0 * (yc - yl);
+    double Dqp = 2.0 * (yr - yc);
+    double Dqc = 0.5 * (yr - yl);
+    double mm = ((Dqm) * (Dqp) <= 0) ? 0.0 : ((fabs(Dqm) < fabs(Dqp)) ? (Dqm) : (Dqp));
+    return ((Dqc) * (mm) <= 0) ? 0.0 : ((fabs(Dqc) < fabs(mm)) ? (Dqc) : (mm));
+  } else if (lim == HGPU_LIM_VANL) {
+    double Dqm = (yc - yl);
+    double Dqp = (yr - yc);
+    double s = Dqm * Dqp;
+    if (s <= 0.) return 0.;
+    return (2.0 * s / (Dqm + Dqp));
+  } else if (lim == HGPU_LIM_MINM) {
+    double Dqm = 1.0 * (yc - yl);
+    double Dqp = 1.0 * (yr - yc);
+    double Dqc = 0.5 * (yr - yl);
+    double mm = ((Dqm) * (Dqc) <= 0) ? 0.0 : ((fabs(Dqm) < fabs(Dqc)) ? (Dqm) : (Dqc));
+    return ((mm) * (Dqp) <= 0) ? 0.0 : ((fabs(mm) < fabs(Dqp)) ? (mm) : (Dqp));
+  }
+  return 0.0;
+}
+
+// ---------------------------------------------------------------------------
+// face flux kernel (one per direction)
+// ---------------------------------------------------------------------------
+template <int DIR>
+__global__ void __launch_bounds__(128) flux_kernel(Dims d, Params P, Box box, const double *__restrict__ pb,
+                                                   const double *__restrict__ G, double *__restrict__ F,
+                                                   Scalars *sc) {
+  long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  bool active = t < box.size();
+  double dtij = 0.0;
+  if (active) {
+    int i, j, k;
+    box_ijk(box, t, i, j, k);
+    long long z = zix(d, i, j, k);
+    const long long o = (DIR == 1) ? (long long)d.nt2 * d.nt3 : ((DIR == 2) ? (long long)d.nt3 : 1);
+    double p_l[NPR], p_r[NPR];
+#pragma unroll
+    for (int v = 0; v < NPR; v++) {
+      const double *q = pb + (long long)v * d.nz + z;
+      double ym2 = __ldg(q - 2 * o), ym1 = __ldg(q - o), y0 = __ldg(q), yp1 = __ldg(q + o);
+      double dqm = slope3(P.lim, ym2, ym1, y0);
+      double dq0 = slope3(P.lim, ym1, y0, yp1);
+      // getp2interplr (flux.c:788-808)
+      p_l[v] = ym1 + 0.5 * dqm;
+      p_r[v] = y0 - 0.5 * dq0;
+    }
+    // BDIRCONT (flux.c:629-633)
+    p_l[B1 + DIR - 1] = p_r[B1 + DIR - 1] = 0.5 * (p_l[B1 + DIR - 1] + p_r[B1 + DIR - 1]);
+    Metric m;
+    load_metric(G, d, gix(d, i, j), DIR - 1, m);
+    State ql, qr;
+    EM el, er;
+    double Fl[NPR], Fr[NPR], Ul[NPR], Ur[NPR];
+    int err = 0;
+    if (get_state(p_l, m, ql)) err |= ERR_UTCALC_DISCR;
+    em_prepare(p_l, m, ql, el);
+    primtoflux(p_l, ql, el, DIR, m, P.gam, Fl);
+    primtoflux(p_l, ql, el, 0, m, P.gam, Ul);
+    if (get_state(p_r, m, qr)) err |= ERR_UTCALC_DISCR;
+    em_prepare(p_r, m, qr, er);
+    primtoflux(p_r, qr, er, DIR, m, P.gam, Fr);
+    primtoflux(p_r, qr, er, 0, m, P.gam, Ur);
+    double cmaxl = 0., cminl = 0., cmaxr = 0., cminr = 0.;
+    err |= vchar(p_l, ql, DIR, m, P.gam, &cmaxl, &cminl);
+    err |= vchar(p_r, qr, DIR, m, P.gam, &cmaxr, &cminr);
+    // cminmax_calc (wavespeeds.c:325-385)
+    double lmin = min_ref(cminl, cminr);
+    double lmax = max_ref(cmaxl, cmaxr);
+    lmin = fabs(max_ref(0., -lmin));
+    lmax = fabs(max_ref(0., lmax));
+    double cmin = lmin, cmax = lmax, ctop = max_ref(lmax, lmin);
+    double Fo[NPR];
+    if (P.flux == HGPU_FLUX_HLL && (cmax + cmin != 0.0)) {
+#pragma unroll
+      for (int v = 0; v < NPR; v++) Fo[v] = ((cmax * Fl[v] + cmin * Fr[v]) - (cmax * cmin) * (Ur[v] - Ul[v])) / (cmax + cmin);
+    } else {
+#pragma unroll
+      for (int v = 0; v < NPR; v++) Fo[v] = (0.5 * ((Fl[v] + Fr[v]) - ctop * (Ur[v] - Ul[v])));
+    }
+    // flux_ct gdet strip (fluxct.c:74-96)
+    Fo[B1] /= m.g;
+    Fo[B2] /= m.g;
+    Fo[B3] /= m.g;
+    store_prim(F, d, z, Fo);
+    double dxd = (DIR == 1) ? P.dx1 : ((DIR == 2) ? P.dx2 : P.dx3);
+    dtij = P.cour * dxd / ctop;
+    if (err) atomicOr(&sc->err, err);
+  }
+  warp_min_atomic(&sc->ndtbits[DIR], dtij, active);
+}
+
+// ---------------------------------------------------------------------------
+// corner EMFs (fluxct.c:104-218) on the corners the updated faces read
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(256) emf_kernel(Dims d, Box box, const double *__restrict__ F1,
+                                                  const double *__restrict__ F2, const double *__restrict__ F3,
+                                                  const double *__restrict__ G, double *__restrict__ E) {
+  long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= box.size()) return;
+  int i, j, k;
+  box_ijk(box, t, i, j, k);
+  long long z = zix(d, i, j, k);
+  const long long o1 = (long long)d.nt2 * d.nt3, o2 = d.nt3, o3 = 1;
+  const long long ij = gix(d, i, j);
+  const int n1 = d.n1, n2 = d.n2, n3 = d.n3;
+  double coef1 = ((n2 > 1) && (n3 > 1)) ? 0.25 : 0.5;
+  double coef2 = ((n1 > 1) && (n3 > 1)) ? 0.25 : 0.5;
+  double coef3 = ((n1 > 1) && (n2 > 1)) ? 0.25 : 0.5;
+  const long long nz = d.nz;
+  if (i <= n1 - 1) {
+    double v;
+    if (n2 > 1 && n3 > 1)
+      v = coef1 * (+F2[B3 * nz + z] + F2[B3 * nz + z - d.s3 * o3] - F3[B2 * nz + z] - F3[B2 * nz + z - d.s2 * o2]);
+    else if (n2 > 1)
+      v = coef1 * (+F2[B3 * nz + z] + F2[B3 * nz + z - d.s3 * o3]);
+    else if (n3 > 1)
+      v = coef1 * (-F3[B2 * nz + z] - F3[B2 * nz + z - d.s2 * o2]);
+    else
+      v = 0.0;
+    E[0 * nz + z] = v * __ldg(G + (long long)(G_CORN + 0) * d.nij + ij);
+  }
+  if (j <= n2 - 1) {
+    double v;
+    if (n1 > 1 && n3 > 1)
+      v = coef2 * (+F3[B1 * nz + z] + F3[B1 * nz + z - d.s1 * o1] - F1[B3 * nz + z] - F1[B3 * nz + z - d.s3 * o3]);
+    else if (n3 > 1)
+      v = coef2 * (+F3[B1 * nz + z] + F3[B1 * nz + z - d.s1 * o1]);
+    else if (n1 > 1)
+      v = coef2 * (-F1[B3 * nz + z] - F1[B3 * nz + z - d.s3 * o3]);
+    else
+      v = 0.0;
+    E[1 * nz + z] = v * __ldg(G + (long long)(G_CORN + 1) * d.nij + ij);
+  }
+  if (k <= n3 - 1) {
+    double v;
+    if (n1 > 1 && n2 > 1)
+      v = coef3 * (+F1[B2 * nz + z] + F1[B2 * nz + z - d.s2 * o2] - F2[B1 * nz + z] - F2[B1 * nz + z - d.s1 * o1]);
+    else if (n1 > 1)
+      v = coef3 * (+F1[B2 * nz + z] + F1[B2 * nz + z - d.s2 * o2]);
+    else if (n2 > 1)
+      v = coef3 * (-F2[B1 * nz + z] - F2[B1 * nz + z - d.s1 * o1]);
+    else
+      v = 0.0;
+    E[2 * nz + z] = v * __ldg(G + (long long)(G_CORN + 2) * d.nij + ij);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// zone update: advance_standard's CZLOOP body (advance.c:143-213)
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(128) update_kernel(Dims d, Params P, Box box, const double *pi, const double *pb,
+                                                     double *pf, double *__restrict__ uf, double *__restrict__ ucum,
+                                                     const double *__restrict__ F1, const double *__restrict__ F2,
+                                                     const double *__restrict__ F3, const double *__restrict__ E,
+                                                     const double *__restrict__ G, int *__restrict__ pflag,
+                                                     Scalars *sc, double CUf0, double CUf1, double CUf2,
+                                                     double Cunew0, double Cunew1, double Cunew2, int timeorder,
+                                                     int finalstep) {
+  long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  unsigned long long my_iters = 0;
+  int my_fail = 0;
+  if (t < box.size()) {
+    int i, j, k;
+    box_ijk(box, t, i, j, k);
+    const long long z = zix(d, i, j, k);
+    const long long nz = d.nz;
+    const long long o1 = (long long)d.nt2 * d.nt3, o2 = d.nt3, o3 = 1;
+    const long long ij = gix(d, i, j);
+    const double dt = sc->dt;
+    Metric m;
+    load_metric(G, d, ij, G_CENT, m);
+    int err = 0;
+    double Ui[NPR], dUg[NPR], dUr[NPR];
+    {
+      double pr[NPR];
+      load_prim(pi, d, z, pr);
+      State q;
+      EM e;
+      if (get_state(pr, m, q)) err |= ERR_UTCALC_DISCR;
+      em_prepare(pr, m, q, e);
+      primtoflux(pr, q, e, 0, m, P.gam, Ui);
+    }
+    double pbz[NPR];
+    load_prim(pb, d, z, pbz);
+    {
+      // source() -> source_conn() (phys.c:578-752)
+      State q;
+      EM e;
+      if (get_state(pbz, m, q)) err |= ERR_UTCALC_DISCR;
+      em_prepare(pbz, m, q, e);
+      double dUconn[4] = {0., 0., 0., 0.};
+      const double *conn = G + (long long)G_CONN * d.nij + ij;
+      double mhd[4][4];
+#pragma unroll
+      for (int jj = 0; jj < 4; jj++) mhd_row(pbz, jj, P.gam, q, e, mhd[jj]);
+#pragma unroll
+      for (int l = 0; l < 4; l++) {
+        double s = dUconn[l];
+#pragma unroll
+        for (int jj = 0; jj < 4; jj++)
+#pragma unroll
+          for (int kk = 0; kk < 4; kk++) s += mhd[jj][kk] * __ldg(conn + (long long)((kk * 4 + l) * 4 + jj) * d.nij);
+        dUconn[l] = s;
+      }
+#pragma unroll
+      for (int l = 0; l < 4; l++) {
+        double s = dUconn[l];
+#pragma unroll
+        for (int jj = 0; jj < 4; jj++) s += -pbz[RHO] * q.ucon[jj] * __ldg(conn + (long long)((0 * 4 + l) * 4 + jj) * d.nij);
+        dUconn[l] = s;
+      }
+      // dU = sum of the NUMSOURCES components; only GEOMSOURCE is nonzero
+      double full[NPR] = {0., dUconn[0], dUconn[1], dUconn[2], dUconn[3], 0., 0., 0.};
+#pragma unroll
+      for (int pl = 0; pl < NPR; pl++) {
+        double comp0 = 0. + m.g * full[pl];
+        double acc = 0.;
+        acc += comp0;
+#pragma unroll
+        for (int l = 1; l < 7; l++) acc += 0.0;
+        dUg[pl] = acc;
+      }
+    }
+    // flux2dUavg (advance.c:741-914) with the B fluxes of flux_ct (fluxct.c:724-781)
+    {
+      const double idx1 = 1.0 / P.dx1, idx2 = 1.0 / P.dx2, idx3 = 1.0 / P.dx3;
+      const double *e1 = E, *e2 = E + nz, *e3 = E + 2 * nz;
+#pragma unroll
+      for (int pl = 0; pl < NPR; pl++) {
+        double a1 = 0, a2 = 0, a3 = 0;
+        if (d.n1 > 1) {
+          double fa, fb;
+          if (pl == B1) { fa = 0.; fb = 0.; }
+          else if (pl == B2) { fa = 0.5 * (e3[z] + e3[z + d.s2 * o2]); fb = 0.5 * (e3[z + o1] + e3[z + o1 + d.s2 * o2]); }
+          else if (pl == B3) { fa = -0.5 * (e2[z] + e2[z + d.s3 * o3]); fb = -0.5 * (e2[z + o1] + e2[z + o1 + d.s3 * o3]); }
+          else { fa = F1[pl * nz + z]; fb = F1[pl * nz + z + o1]; }
+          a1 = (-(fb - fa) * idx1);
+        }
+        if (d.n2 > 1) {
+          double fa, fb;
+          if (pl == B1) { fa = -0.5 * (e3[z] + e3[z + d.s1 * o1]); fb = -0.5 * (e3[z + o2] + e3[z + o2 + d.s1 * o1]); }
+          else if (pl == B2) { fa = 0.; fb = 0.; }
+          else if (pl == B3) { fa = 0.5 * (e1[z] + e1[z + d.s3 * o3]); fb = 0.5 * (e1[z + o2] + e1[z + o2 + d.s3 * o3]); }
+          else { fa = F2[pl * nz + z]; fb = F2[pl * nz + z + o2]; }
+          a2 = (-(fb - fa) * idx2);
+        }
+        if (d.n3 > 1) {
+          double fa, fb;
+          if (pl == B1) { fa = 0.5 * (e2[z] + e2[z + d.s1 * o1]); fb = 0.5 * (e2[z + o3] + e2[z + o3 + d.s1 * o1]); }
+          else if (pl == B2) { fa = -0.5 * (e1[z] + e1[z + d.s2 * o2]); fb = -0.5 * (e1[z + o3] + e1[z + o3 + d.s2 * o2]); }
+          else if (pl == B3) { fa = 0.; fb = 0.; }
+          else { fa = F3[pl * nz + z]; fb = F3[pl * nz + z + o3]; }
+          a3 = (-(fb - fa) * idx3);
+        }
+        dUr[pl] = a1 + a2 + a3;
+      }
+    }
+    // dUtoU (advance.c:922-949)
+    double Uf[NPR], Ucum[NPR];
+#pragma unroll
+    for (int pl = 0; pl < NPR; pl++) {
+      double ufo = (timeorder == 0) ? 0.0 : uf[pl * nz + z];
+      double uco = (timeorder == 0) ? 0.0 : ucum[pl * nz + z];
+      Uf[pl] = CUf0 * Ui[pl] + CUf1 * ufo + CUf2 * dt * (dUr[pl] + dUg[pl]);
+      Ucum[pl] = uco + (Cunew0 * Ui[pl] + Cunew1 * dt * (dUr[pl] + dUg[pl]) + Cunew2 * Uf[pl]);
+      uf[pl * nz + z] = Uf[pl];
+      ucum[pl * nz + z] = Ucum[pl];
+    }
+    // guess = pb, invert (advance.c:188-205)
+    double pr[NPR];
+#pragma unroll
+    for (int v = 0; v < NPR; v++) pr[v] = pbz[v];
+    int it = 0;
+    int flag = utoprimgen(finalstep ? Ucum : Uf, m, P.gam, P.gammafail, pr, &it);
+    my_iters = (unsigned long long)it;
+    my_fail = (flag != 0);
+    if (finalstep) {
+      // fixup1zone (fixup.c:341-447)
+      const double *fl = G + (long long)G_FLOOR * d.nij + ij;
+      double fr = __ldg(fl), fu = __ldg(fl + d.nij);
+      if (fr < P.rhominlimit) fr = P.rhominlimit;
+      if (fu < P.uuminlimit) fu = P.uuminlimit;
+      if (fr > pr[RHO]) pr[RHO] = fr;
+      if (fu > pr[UU]) pr[UU] = fu;
+      limit_gamma(P.gammamax, pr, m, &err);
+    }
+    store_prim(pf, d, z, pr);
+    pflag[z] = flag;
+    if (err) atomicOr(&sc->err, err);
+  }
+  // block-level aggregation of counters
+  unsigned long long s_it = my_iters;
+  int s_f = my_fail;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    s_it += __shfl_xor_sync(0xffffffffu, s_it, o);
+    s_f += __shfl_xor_sync(0xffffffffu, s_f, o);
+  }
+  if ((threadIdx.x & 31) == 0) {
+    if (s_it) atomicAdd(&sc->iters, s_it);
+    if (s_f) atomicAdd(&sc->nfail, s_f);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// boundaries: bound_prim_user (bounds.fishmon.c:29-345)
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ int map_idx(int i, int n, int bcdn, int bcup) {
+  if (i < 0) {
+    if (bcdn == HGPU_BC_PERIODIC) return i + n;
+    if (bcdn == HGPU_BC_POLARAXIS) return -i - 1;
+    return 0;  // OUTFLOW
+  }
+  if (i >= n) {
+    if (bcup == HGPU_BC_PERIODIC) return i - n;
+    if (bcup == HGPU_BC_POLARAXIS) return (n - 1) + ((n - 1) - i + 1);
+    return n - 1;
+  }
+  return i;
+}
+
+// inflow_check_rel4vel for dir 1 at CENT (fixup.c:2271-2407)
+__device__ __forceinline__ void inflow_check_x1(const Dims &d, const Params &P, int i, double *pr, const Metric &m,
+                                                int *err) {
+  double ucon[4];
+  if (ucon_calc(pr, m, ucon)) {
+    *err |= ERR_UTCALC_DISCR;
+    return;
+  }
+  bool dofix = ((i <= -1) && (P.bc[1] == HGPU_BC_OUTFLOW) && (ucon[1] > 0.)) ||
+               ((i >= d.n1) && (P.bc[0] == HGPU_BC_OUTFLOW) && (ucon[1] < 0.));
+  if (!dofix) return;
+  double gamma;
+  if (gamma_calc(pr, m, &gamma)) {
+    *err |= ERR_UTCALC_DISCR;
+    return;
+  }
+  pr[U1] /= gamma;
+  pr[U2] /= gamma;
+  pr[U3] /= gamma;
+  double alpha = 1. / sqrt(-GCON(m, 0, 0));
+  double betacon = GCON(m, 0, 1) * alpha * alpha;
+  pr[U1] = betacon / alpha;
+  double vsq = 0.;
+#pragma unroll
+  for (int j = 1; j < 4; j++)
+#pragma unroll
+    for (int k = 1; k < 4; k++) vsq += GCOV(m, j, k) * pr[U1 + j - 1] * pr[U1 + k - 1];
+  if (vsq < 0.0) {
+    if (vsq > -NUMEPSILON * 100.0) vsq = 0.0;
+    else {
+      *err |= ERR_VSQ_NEG;
+      return;
+    }
+  }
+  if (vsq >= 1.0) vsq = 1.0 - 1.0 / (P.gammamax * P.gammamax);
+  gamma = 1. / sqrt(1. - vsq);
+  pr[U1] *= gamma;
+  pr[U2] *= gamma;
+  pr[U3] *= gamma;
+}
+
+// Every ghost zone of the full box as the composition of the reference's
+// sequential fills: x1 (active j,k: copy + inflow check + gamma limit with the
+// ghost's own metric), then x2 (full i, active k: reflection, POLEDEATH
+// zeroing of u~2 and B2), then x3 (full i, full j: periodic copy).  Reads only
+// active zones, which this kernel does not write.
+__global__ void __launch_bounds__(128) bound_ghost_kernel(Dims d, Params P, double *p, const double *__restrict__ G,
+                                                          Scalars *sc) {
+  long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= d.nz) return;
+  int k = (int)(t % d.nt3) - d.g3;
+  long long r = t / d.nt3;
+  int j = (int)(r % d.nt2) - d.g2;
+  int i = (int)(r / d.nt2) - d.g1;
+  bool gi = (i < 0 || i >= d.n1), gj = (j < 0 || j >= d.n2), gk = (k < 0 || k >= d.n3);
+  if (!(gi || gj || gk)) return;
+  int si = map_idx(i, d.n1, P.bc[1], P.bc[0]);
+  int sj = map_idx(j, d.n2, P.bc[3], P.bc[2]);
+  int sk = map_idx(k, d.n3, P.bc[5], P.bc[4]);
+  double pr[NPR];
+  load_prim(p, d, zix(d, si, sj, sk), pr);
+  int err = 0;
+  if (gi && (P.bc[1] == HGPU_BC_OUTFLOW || P.bc[0] == HGPU_BC_OUTFLOW) &&
+      ((i < 0 && P.bc[1] == HGPU_BC_OUTFLOW) || (i >= d.n1 && P.bc[0] == HGPU_BC_OUTFLOW))) {
+    Metric m;
+    load_metric(G, d, gix(d, i, sj), G_CENT, m);
+    inflow_check_x1(d, P, i, pr, m, &err);
+    limit_gamma(P.gammamax, pr, m, &err);
+  }
+  // POLEDEATH rows: x2 ghosts and the first/last active row (bounds.fishmon.c:238-250, 300-312)
+  bool pole_dn = (P.bc[3] == HGPU_BC_POLARAXIS) && (j <= 0) && d.n2 > 1;
+  bool pole_up = (P.bc[2] == HGPU_BC_POLARAXIS) && (j >= d.n2 - 1) && d.n2 > 1;
+  if (pole_dn || pole_up) {
+    pr[U2] *= 0;
+    pr[B2] *= 0.;
+  }
+  store_prim(p, d, t, pr);
+  if (err) atomicOr(&sc->err, err);
+}
+
+// POLEDEATH on the active first/last x2 rows (after the ghosts have read them)
+__global__ void bound_pole_kernel(Dims d, Params P, double *p) {
+  long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  long long rows = (long long)d.n1 * d.n3;
+  if (t >= 2 * rows) return;
+  int side = (int)(t / rows);
+  long long r = t % rows;
+  int i = (int)(r / d.n3), k = (int)(r % d.n3);
+  int j;
+  if (side == 0) {
+    if (!(P.bc[3] == HGPU_BC_POLARAXIS)) return;
+    j = 0;
+  } else {
+    if (!(P.bc[2] == HGPU_BC_POLARAXIS)) return;
+    j = d.n2 - 1;
+  }
+  long long z = zix(d, i, j, k);
+  p[(long long)U2 * d.nz + z] *= 0;
+  p[(long long)B2 * d.nz + z] *= 0.;
+}
+
+// bound_pflag_user (boundsint.c:6-266) as the same composition
+__global__ void bound_pflag_kernel(Dims d, Params P, int *pflag) {
+  long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= d.nz) return;
+  int k = (int)(t % d.nt3) - d.g3;
+  long long r = t / d.nt3;
+  int j = (int)(r % d.nt2) - d.g2;
+  int i = (int)(r / d.nt2) - d.g1;
+  bool gi = (i < 0 || i >= d.n1), gj = (j < 0 || j >= d.n2), gk = (k < 0 || k >= d.n3);
+  if (!(gi || gj || gk)) return;
+  int si = map_idx(i, d.n1, P.bc[1], P.bc[0]);
+  int sj = map_idx(j, d.n2, P.bc[3], P.bc[2]);
+  int sk = map_idx(k, d.n3, P.bc[5], P.bc[4]);
+  pflag[t] = pflag[zix(d, si, sj, sk)];
+}
+
+// ---------------------------------------------------------------------------
+// post_fixup (fixup.c:37-96)
+// ---------------------------------------------------------------------------
+// fixup_checksolution (fixup.c:460-560), part 1: gamma on i,j,k = -1..N and
+// the list of active candidate zones (gamma >= 2)
+__global__ void checksol_gamma_kernel(Dims d, Box box, const double *__restrict__ pv, const double *__restrict__ G,
+                                      double *__restrict__ gammacheck, long long *__restrict__ cand, int cap,
+                                      Scalars *sc) {
+  long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= box.size()) return;
+  int i, j, k;
+  box_ijk(box, t, i, j, k);
+  long long z = zix(d, i, j, k);
+  Metric m;
+  load_metric(G, d, gix(d, i, j), G_CENT, m);
+  double pr[NPR];
+  load_prim(pv, d, z, pr);
+  double gamma = 0.0;
+  if (gamma_calc(pr, m, &gamma)) atomicOr(&sc->err, ERR_UTCALC_DISCR);
+  gammacheck[z] = gamma;
+  bool activez = (i >= 0 && i < d.n1 && j >= 0 && j < d.n2 && k >= 0 && k < d.n3);
+  if (activez && gamma >= 2.0) {
+    int slot = atomicAdd(&sc->ncand, 1);
+    if (slot < cap) cand[slot] = z;
+    else atomicOr(&sc->overflow, 1);
+  }
+}
+
+// In the reference the candidates are visited in loop order (i, then j, then
+// k) and each visit may overwrite the zone's pflag with 12/13, which later
+// visits of its neighbours read.  The zone index z is lexicographic in
+// (i,j,k), so "visited earlier" is "smaller z".  This single-block kernel
+// iterates a fixpoint in which every candidate sees the current decision of
+// its earlier candidate neighbours and the unchanged flags of everything
+// else; a dependency chain of length L settles after L sweeps, which gives
+// exactly the reference's sequential result.  candmap maps a zone to its
+// candidate slot (-1 otherwise) and is restored to -1 before returning.
+__global__ void __launch_bounds__(1024) checksol_resolve_kernel(Dims d, const double *__restrict__ pv,
+                                                                const double *__restrict__ gammacheck, int *pflag,
+                                                                const long long *__restrict__ cand, int *candmap,
+                                                                int *orig, int *dec, int cap, Scalars *sc) {
+  int n = sc->ncand;
+  if (n > cap) n = cap;
+  if (n == 0) return;
+  const int tid = threadIdx.x, nt = blockDim.x;
+  for (int a = tid; a < n; a += nt) {
+    long long z = cand[a];
+    candmap[z] = a;
+    orig[a] = pflag[z];
+    dec[a] = orig[a];
+  }
+  __syncthreads();
+  __shared__ int changed;
+  const long long o1 = (long long)d.nt2 * d.nt3, o2 = d.nt3;
+  // a chain can be at most n long; the sweep count is also capped so that a
+  // pathological input ends with an error flag instead of a long kernel
+  const int max_sweeps = n + 1 < 4096 ? n + 1 : 4096;
+  for (int sweep = 0; sweep < max_sweeps; sweep++) {
+    if (sweep == max_sweeps - 1 && tid == 0 && max_sweeps < n + 1) atomicOr(&sc->overflow, 4);
+    if (tid == 0) changed = 0;
+    __syncthreads();
+    for (int a = tid; a < n; a += nt) {
+      long long z = cand[a];
+      double gc = gammacheck[z], uc = pv[(long long)UU * d.nz + z];
+      // neighbour order of fixup.c:508-526
+      long long nb[8] = {z + d.s2 * o2,        z - d.s2 * o2,        z + d.s1 * o1,        z - d.s1 * o1,
+                         z + d.s1 * o1 + d.s2 * o2, z + d.s1 * o1 - d.s2 * o2, z + d.s1 * o1 + d.s2 * o2,
+                         z - d.s1 * o1 - d.s2 * o2};
+      double pd[8], pd2[8];
+#pragma unroll
+      for (int q = 0; q < 8; q++) {
+        int f = pflag[nb[q]];
+        if (nb[q] < z) {
+          int c = candmap[nb[q]];
+          if (c >= 0) f = dec[c];
+        }
+        pd[q] = (f <= UTOPRIMNOFAIL) ? (gammacheck[nb[q]] / gc) : -1;
+        pd2[q] = (f <= UTOPRIMNOFAIL) ? (pv[(long long)UU * d.nz + nb[q]] / uc) : -1;
+      }
+      int vote0 = 0, vote1 = 0, numvotes = 0;
+#pragma unroll
+      for (int l = 0; l < 8; l++) {
+        if (pd[0] >= 0.0) {
+          if ((fabs(pd[l]) > 2.0) || (fabs(pd[l]) < 1.0 / 2.0)) vote0++;
+          if ((fabs(pd2[l]) > 10.0) || (fabs(pd2[l]) < 1.0 / 10.0)) vote1++;
+          numvotes++;
+        }
+      }
+      int nd = orig[a];
+      if (vote0 > numvotes * 0.5) nd = UTOPRIMFAILGAMMAPERC;
+      if (vote1 > numvotes * 0.5) nd = UTOPRIMFAILUPERC;
+      if (nd != dec[a]) {
+        dec[a] = nd;
+        changed = 1;
+      }
+    }
+    __syncthreads();
+    if (!changed) break;
+    __syncthreads();
+  }
+  __syncthreads();
+  for (int a = tid; a < n; a += nt) {
+    long long z = cand[a];
+    pflag[z] = dec[a];
+    candmap[z] = -1;
+  }
+}
+
+// fixup_utoprim (fixup.c:669-1470), part 1: list the active failed zones
+__global__ void fixup_collect_kernel(Dims d, Box box, const int *__restrict__ pflag, long long *__restrict__ list,
+                                     int cap, Scalars *sc) {
+  long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= box.size()) return;
+  int i, j, k;
+  box_ijk(box, t, i, j, k);
+  long long z = zix(d, i, j, k);
+  if (pflag[z] != 0) {
+    int slot = atomicAdd(&sc->nfixlist, 1);
+    if (slot < cap) list[slot] = z;
+    else atomicOr(&sc->overflow, 2);
+  }
+}
+
+__device__ __forceinline__ bool becomes_fixed(int f, int finalstep) {
+  // accounting branch of fixup.c:1399-1470: which codes are reset to
+  // UTOPRIMFAILFIXED (STEPOVERNEG*=-1, DOCOUNTNEG*=1)
+  if (f == 0) return false;
+  if (f == UTOPRIMFAILRHONEG || f == UTOPRIMFAILUNEG || f == UTOPRIMFAILU2AVG1 || f == UTOPRIMFAILU2AVG2 ||
+      f == UTOPRIMFAILRHOUNEG)
+    return finalstep != 0;
+  return true;
+}
+
+// part 2: new primitives of each listed zone.  The reference averages
+// neighbour values from a snapshot of pv taken before the sweep (ptoavg) and
+// tests neighbour pflags that earlier visits may already have reset to -1; a
+// neighbour's reset depends only on its own code, so "earlier active failed
+// neighbour that becomes fixed" counts as good here.
+__global__ void fixup_compute_kernel(Dims d, Params P, const double *__restrict__ pv, const int *__restrict__ pflag,
+                                     const double *__restrict__ G, const long long *__restrict__ list,
+                                     double *__restrict__ outv, int cap, int finalstep, Scalars *sc) {
+  int n = sc->nfixlist;
+  if (n > cap) n = cap;
+  for (int a = blockIdx.x * blockDim.x + threadIdx.x; a < n; a += gridDim.x * blockDim.x) {
+  long long z = list[a];
+  int k = (int)(z % d.nt3) - d.g3;
+  long long r = z / d.nt3;
+  int j = (int)(r % d.nt2) - d.g2;
+  int i = (int)(r / d.nt2) - d.g1;
+  int mypflag = pflag[z];
+  double pr[NPR];
+  load_prim(pv, d, z, pr);
+  int err = 0;
+  bool fixed = (mypflag == UTOPRIMFAILUNEG || mypflag == UTOPRIMFAILRHONEG || mypflag == UTOPRIMFAILRHOUNEG);
+  if (!fixed) {
+    Metric m;
+    load_metric(G, d, gix(d, i, j), G_CENT, m);
+    double gamma = 1.0;
+    if (gamma_calc(pr, m, &gamma)) err |= ERR_UTCALC_DISCR;
+    if (gamma > P.gammamax) gamma = P.gammamax;
+    int startpl, endpl, looptype;
+    if (mypflag == UTOPRIMFAILU2AVG1 || mypflag == UTOPRIMFAILU2AVG2) {
+      startpl = UU;
+      endpl = UU;
+      looptype = 1;
+    } else {
+      startpl = RHO;
+      endpl = U3;
+      looptype = 0;
+    }
+    double mysum0[5] = {0, 0, 0, 0, 0}, mysum1[5] = {0, 0, 0, 0, 0}, lastmin[5] = {1E50, 1E50, 1E50, 1E50, 1E50};
+    const int s1 = d.s1, s2 = d.s2, s3 = d.s3;
+    const int rnx = (s1 == 1) ? 3 : 1, rny = (s2 == 1) ? 3 : 1;
+    const int npow = s1 + s2 + s3;
+    int p3 = 1;
+    for (int q = 0; q < npow; q++) p3 *= 3;
+    const int numupairs = (p3 - 1) / 2;
+    int numavg0 = 0, numavg1 = 0;
+    for (int qq = 0; qq < numupairs; qq++) {
+      int ii = (qq % rnx) - s1;
+      int jj = ((qq % (rnx * rny)) / rnx) - s2;
+      int kk = (qq / (rnx * rny)) - s3;
+      long long za = zix(d, i + ii, j + jj, k + kk), zb = zix(d, i - ii, j - jj, k - kk);
+      int ia = i + ii, ja = j + jj, ka = k + kk, ib = i - ii, jb = j - jj, kb = k - kk;
+      bool act_a = ia >= 0 && ia < d.n1 && ja >= 0 && ja < d.n2 && ka >= 0 && ka < d.n3;
+      bool act_b = ib >= 0 && ib < d.n1 && jb >= 0 && jb < d.n2 && kb >= 0 && kb < d.n3;
+      int fa = pflag[za], fb = pflag[zb];
+      int thisnotfail = (fa <= UTOPRIMNOFAIL) || (act_a && za < z && becomes_fixed(fa, finalstep));
+      int thatnotfail = (fb <= UTOPRIMNOFAIL) || (act_b && zb < z && becomes_fixed(fb, finalstep));
+      numavg1 += (pv[(long long)UU * d.nz + za] > 0.0);
+      numavg1 += (pv[(long long)UU * d.nz + zb] > 0.0);
+      numavg0 += thisnotfail + thatnotfail;
+      for (int pl = startpl; pl <= endpl; pl++) {
+        double va = pv[(long long)pl * d.nz + za], vb = pv[(long long)pl * d.nz + zb];
+        if (looptype == 0) {
+          double add = va * thisnotfail + vb * thatnotfail;
+          if (qq % 2) mysum1[pl] += add;
+          else mysum0[pl] += add;
+        } else {
+          if (va >= 0.0) lastmin[pl] = min_macro(lastmin[pl], va);
+          if (vb >= 0.0) lastmin[pl] = min_macro(lastmin[pl], vb);
+        }
+      }
+    }
+    int numavg;
+    if (looptype == 0) {
+      if (numavg0 != 0)
+        for (int pl = startpl; pl <= endpl; pl++) pr[pl] = (mysum0[pl] + mysum1[pl]) / ((double)(numavg0));
+      numavg = numavg0;
+    } else {
+      if (numavg1 != 0)
+        for (int pl = startpl; pl <= endpl; pl++) pr[pl] = lastmin[pl];
+      numavg = numavg1;
+    }
+    if (mypflag == UTOPRIMFAILU2AVG2) numavg++;
+    if (numavg == 0) {
+      for (int pl = startpl; pl <= endpl; pl++) {
+        const double *pp = pv + (long long)pl * d.nz;
+        double a41 = (0.25 * ((pp[zix(d, i, j + s2, k)] + pp[zix(d, i, j - s2, k)]) +
+                              (pp[zix(d, i - s1, j, k)] + pp[zix(d, i + s1, j, k)])));
+        double a42 = (0.25 * ((pp[zix(d, i + s1, j + s2, k)] + pp[zix(d, i + s1, j - s2, k)]) +
+                              (pp[zix(d, i - s1, j + s2, k)] + pp[zix(d, i - s1, j - s2, k)])));
+        pr[pl] = 0.5 * (a41 + a42);
+      }
+    }
+    limit_gamma(gamma, pr, m, &err);
+  }
+#pragma unroll
+  for (int v = 0; v < 5; v++) outv[(long long)a * 5 + v] = pr[v];
+  if (err) atomicOr(&sc->err, err);
+  }
+}
+
+__global__ void fixup_scatter_kernel(Dims d, double *pv, int *pflag, const long long *__restrict__ list,
+                                     const double *__restrict__ outv, int cap, int finalstep, Scalars *sc) {
+  int n = sc->nfixlist;
+  if (n > cap) n = cap;
+  for (int a = blockIdx.x * blockDim.x + threadIdx.x; a < n; a += gridDim.x * blockDim.x) {
+    long long z = list[a];
+#pragma unroll
+    for (int v = 0; v < 5; v++) pv[(long long)v * d.nz + z] = outv[(long long)a * 5 + v];
+    int f = pflag[z];
+    if (becomes_fixed(f, finalstep)) {
+      pflag[z] = UTOPRIMFAILFIXED;
+      atomicAdd(&sc->nfixed, 1);
+    }
+  }
+}
+
+// B components of the fluxes after flux_ct (fluxct.c:724-781) on the faces
+// the update reads; used only to hand fluxes back through hgpu_fluxcalc (the
+// update kernel rebuilds them from the EMFs on the fly)
+__global__ void bflux_kernel(Dims d, int dir, Box box, const double *__restrict__ E, double *__restrict__ F) {
+  long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= box.size()) return;
+  int i, j, k;
+  box_ijk(box, t, i, j, k);
+  long long z = zix(d, i, j, k), nz = d.nz;
+  const long long o1 = (long long)d.nt2 * d.nt3, o2 = d.nt3, o3 = 1;
+  const double *e1 = E, *e2 = E + nz, *e3 = E + 2 * nz;
+  if (dir == 1) {
+    F[B1 * nz + z] = 0.;
+    F[B2 * nz + z] = 0.5 * (e3[z] + e3[z + d.s2 * o2]);
+    F[B3 * nz + z] = -0.5 * (e2[z] + e2[z + d.s3 * o3]);
+  } else if (dir == 2) {
+    F[B1 * nz + z] = -0.5 * (e3[z] + e3[z + d.s1 * o1]);
+    F[B2 * nz + z] = 0.;
+    F[B3 * nz + z] = 0.5 * (e1[z] + e1[z + d.s3 * o3]);
+  } else {
+    F[B1 * nz + z] = 0.5 * (e2[z] + e2[z + d.s1 * o1]);
+    F[B2 * nz + z] = -0.5 * (e1[z] + e1[z + d.s2 * o2]);
+    F[B3 * nz + z] = 0.;
+  }
+}
+
+// ndt (advance.c:231) and the dt update of step_ch (step_ch.c:236-247)
+__global__ void finalize_kernel(Params P, Scalars *sc, int advance_time) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  double n1 = __longlong_as_double((long long)sc->ndtbits[1]);
+  double n2 = __longlong_as_double((long long)sc->ndtbits[2]);
+  double n3 = __longlong_as_double((long long)sc->ndtbits[3]);
+  double ndt = P.defcon * 1. / (1. / n1 + 1. / n2 + 1. / n3);
+  if (advance_time) {
+    double dt = sc->dt;
+    sc->t += dt;
+    if (ndt > P.safe * dt) ndt = P.safe * dt;
+    dt = ndt;
+    if (sc->t + dt > P.tf) dt = P.tf - sc->t;
+    sc->dt = dt;
+  }
+  // keep the last ndt where the host can read it
+  sc->ndtbits[0] = (unsigned long long)__double_as_longlong(ndt);
+}
+
+__global__ void reset_stage_kernel(Scalars *sc) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  unsigned long long big = (unsigned long long)__double_as_longlong(BIGNUM);
+  sc->ndtbits[1] = big;
+  sc->ndtbits[2] = big;
+  sc->ndtbits[3] = big;
+  sc->nfail = 0;
+  sc->ncand = 0;
+  sc->nfixlist = 0;
+}
+
+// reference AoS [zone][8] <-> device SoA [8][zone]
+__global__ void aos_to_soa_kernel(const double *__restrict__ a, double *__restrict__ s, long long nz) {
+  long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= nz * NPR) return;
+  long long z = t / NPR;
+  int v = (int)(t % NPR);
+  s[(long long)v * nz + z] = a[t];
+}
+__global__ void soa_to_aos_kernel(const double *__restrict__ s, double *__restrict__ a, long long nz) {
+  long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= nz * NPR) return;
+  long long z = t / NPR;
+  int v = (int)(t % NPR);
+  a[t] = s[(long long)v * nz + z];
+}
+
+// batched inversion on arbitrary per-zone metrics (hgpu_utoprim_batch)
+__global__ void utoprim_batch_kernel(const double *__restrict__ U, const double *__restrict__ gcov,
+                                     const double *__restrict__ gcon, const double *__restrict__ gdet, double *pr,
+                                     int *pflag, long long n, double gam, double gammafail,
+                                     unsigned long long *iters) {
+  long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  unsigned long long it_total = 0;
+  if (t < n) {
+    Metric m;
+#pragma unroll
+    for (int q = 0; q < 16; q++) {
+      m.gcov[q] = gcov[t * 16 + q];
+      m.gcon[q] = gcon[t * 16 + q];
+    }
+    m.gcovpert_tt = 0.0;
+    m.g = gdet[t];
+    double u[NPR], p[NPR];
+#pragma unroll
+    for (int v = 0; v < NPR; v++) {
+      u[v] = U[t * NPR + v];
+      p[v] = pr[t * NPR + v];
+    }
+    int it = 0;
+    pflag[t] = utoprimgen(u, m, gam, gammafail, p, &it);
+#pragma unroll
+    for (int v = 0; v < NPR; v++) pr[t * NPR + v] = p[v];
+    it_total = (unsigned long long)it;
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) it_total += __shfl_xor_sync(0xffffffffu, it_total, o);
+  if ((threadIdx.x & 31) == 0 && it_total) atomicAdd(iters, it_total);
+}
+
+inline unsigned grid_for(long long n, int block) { return (unsigned)((n + block - 1) / block); }
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// host context
+// ---------------------------------------------------------------------------
+enum KernelId {
+  K_RESET, K_FLUX1, K_FLUX2, K_FLUX3, K_EMF, K_UPDATE, K_BOUND_GHOST, K_BOUND_POLE, K_BOUND_PFLAG, K_CHECK_GAMMA,
+  K_CHECK_RESOLVE, K_FIX_COLLECT, K_FIX_COMPUTE, K_FIX_SCATTER, K_FINALIZE, K_OTHER, K_NKERNELS
+};
+static const char *kKernelNames[K_NKERNELS] = {
+    "reset_stage",  "flux_x1",         "flux_x2",       "flux_x3",       "emf",           "update",
+    "bound_ghost",  "bound_pole",      "bound_pflag",   "checksol_gamma", "checksol_resolve", "fixup_collect",
+    "fixup_compute", "fixup_scatter",  "finalize",      "other"};
+
+struct ProfEvent {
+  int kid;
+  cudaEvent_t a, b;
+};
+
+struct hgpu_ctx {
+  long long launches = 0;
+  bool profiling = false;
+  std::vector<ProfEvent> pending;
+  std::vector<cudaEvent_t> freelist;
+  double kms[K_NKERNELS] = {0};
+  long long kcount[K_NKERNELS] = {0};
+  hgpu_config cfg;
+  Dims d;
+  Params P;
+  cudaStream_t stream;
+  double *p = nullptr, *pk = nullptr, *uf = nullptr, *ucum = nullptr;
+  double *F[4] = {nullptr, nullptr, nullptr, nullptr};
+  double *E = nullptr;
+  double *G = nullptr;
+  int *pflag = nullptr;
+  double *gammacheck = nullptr;
+  long long *cand = nullptr, *fixlist = nullptr;
+  int *cand_orig = nullptr, *cand_dec = nullptr, *candmap = nullptr;
+  double *fixvals = nullptr;
+  int cap = 0;
+  Scalars *sc = nullptr;
+  double *staging = nullptr;  // AoS staging for uploads/downloads
+  int *istaging = nullptr;
+  Box face_box[4], emf_box, active_box, dq_box;
+};
+
+static cudaEvent_t take_event(hgpu_ctx *x) {
+  if (!x->freelist.empty()) {
+    cudaEvent_t e = x->freelist.back();
+    x->freelist.pop_back();
+    return e;
+  }
+  cudaEvent_t e;
+  cudaEventCreate(&e);
+  return e;
+}
+
+struct ProfScope {
+  hgpu_ctx *x;
+  int kid;
+  cudaEvent_t a = nullptr;
+  ProfScope(hgpu_ctx *x_, int kid_) : x(x_), kid(kid_) {
+    if (x->profiling) {
+      a = take_event(x);
+      cudaEventRecord(a, x->stream);
+    }
+  }
+  ~ProfScope() {
+    x->launches++;
+    if (x->profiling) {
+      cudaEvent_t b = take_event(x);
+      cudaEventRecord(b, x->stream);
+      x->pending.push_back(ProfEvent{kid, a, b});
+    }
+  }
+};
+
+// every launch of the library goes through this macro: it counts the launch
+// and, when profiling is on, brackets it with events on the context's stream
+#define LAUNCH(x, kid, kernel, grid, block, ...)                 \
+  do {                                                          \
+    ProfScope ps__(x, kid);                                     \
+    kernel<<<(grid), (block), 0, (x)->stream>>>(__VA_ARGS__);   \
+  } while (0)
+
+static void collect_profile(hgpu_ctx *x) {
+  for (auto &pe : x->pending) {
+    float ms = 0.f;
+    if (cudaEventElapsedTime(&ms, pe.a, pe.b) == cudaSuccess) {
+      x->kms[pe.kid] += ms;
+      x->kcount[pe.kid] += 1;
+    }
+    x->freelist.push_back(pe.a);
+    x->freelist.push_back(pe.b);
+  }
+  x->pending.clear();
+}
+
+static int validate(const hgpu_config *c) {
+  if (!c) return HGPU_E_INVALID;
+  if (c->n1 < 1 || c->n2 < 1 || c->n3 < 1 || c->ng < 2) return HGPU_E_INVALID;
+  if (c->lim != HGPU_LIM_MC && c->lim != HGPU_LIM_VANL && c->lim != HGPU_LIM_MINM && c->lim != HGPU_LIM_DONOR)
+    return HGPU_E_INVALID;
+  if (c->fluxmethod != HGPU_FLUX_HLL && c->fluxmethod != HGPU_FLUX_LAXF) return HGPU_E_INVALID;
+  for (int f = 0; f < 6; f++)
+    if (c->bc[f] != HGPU_BC_OUTFLOW && c->bc[f] != HGPU_BC_POLARAXIS && c->bc[f] != HGPU_BC_PERIODIC)
+      return HGPU_E_INVALID;
+  // reflections and periodic wraps read inside the active range
+  if (c->n2 > 1 && c->n2 < c->ng) return HGPU_E_INVALID;
+  if (c->n3 > 1 && c->n3 < c->ng) return HGPU_E_INVALID;
+  if (c->n1 > 1 && c->n1 < c->ng) return HGPU_E_INVALID;
+  if (c->precision != HGPU_PREC_FP64) return HGPU_E_INVALID;
+  return HGPU_OK;
+}
+
+extern "C" {
+
+int hgpu_abi_version(void) { return HGPU_ABI_VERSION; }
+
+const char *hgpu_last_error(void) { return g_errbuf; }
+
+void hgpu_destroy(hgpu_ctx *x) {
+  if (!x) return;
+  cudaStreamSynchronize(x->stream);
+  collect_profile(x);
+  for (cudaEvent_t e : x->freelist) cudaEventDestroy(e);
+  void *ptrs[] = {x->p, x->pk, x->uf, x->ucum, x->F[1], x->F[2], x->F[3], x->E, x->G, x->pflag, x->gammacheck,
+                  x->cand, x->fixlist, x->cand_orig, x->cand_dec, x->candmap, x->fixvals, x->sc, x->staging, x->istaging};
+  for (void *q : ptrs)
+    if (q) cudaFree(q);
+  cudaStreamDestroy(x->stream);
+  delete x;
+}
+
+int hgpu_create(const hgpu_config *cfg, hgpu_ctx **out) {
+  if (!out) return HGPU_E_INVALID;
+  *out = nullptr;
+  int rc = validate(cfg);
+  if (rc) {
+    set_err("invalid configuration");
+    return rc;
+  }
+  hgpu_ctx *x = new (std::nothrow) hgpu_ctx();
+  if (!x) return HGPU_E_NOMEM;
+  x->cfg = *cfg;
+  Dims &d = x->d;
+  d.n1 = cfg->n1;
+  d.n2 = cfg->n2;
+  d.n3 = cfg->n3;
+  d.s1 = d.n1 > 1;
+  d.s2 = d.n2 > 1;
+  d.s3 = d.n3 > 1;
+  d.g1 = d.s1 ? cfg->ng : 0;
+  d.g2 = d.s2 ? cfg->ng : 0;
+  d.g3 = d.s3 ? cfg->ng : 0;
+  d.nt1 = d.n1 + 2 * d.g1;
+  d.nt2 = d.n2 + 2 * d.g2;
+  d.nt3 = d.n3 + 2 * d.g3;
+  d.gt1 = d.nt1 + d.s1;
+  d.gt2 = d.nt2 + d.s2;
+  d.nz = (long long)d.nt1 * d.nt2 * d.nt3;
+  d.nij = (long long)d.gt1 * d.gt2;
+  Params &P = x->P;
+  P.gam = cfg->gam;
+  P.cour = cfg->cour;
+  P.gammamax = cfg->gammamax;
+  P.gammafail = cfg->gammafail;
+  P.rhominlimit = cfg->rhominlimit;
+  P.uuminlimit = cfg->uuminlimit;
+  P.defcon = cfg->defcon;
+  P.safe = cfg->safe;
+  P.tf = cfg->tf;
+  P.dx1 = cfg->dx[1];
+  P.dx2 = cfg->dx[2];
+  P.dx3 = cfg->dx[3];
+  P.lim = cfg->lim;
+  P.flux = cfg->fluxmethod;
+  for (int f = 0; f < 6; f++) P.bc[f] = cfg->bc[f];
+  // loop ranges (initbase.c:1010-1058 and fixup.c:477 DQZLOOP)
+  x->face_box[1] = Box{0, -d.s2, -d.s3, d.n1 + 1, d.n2 + 2 * d.s2, d.n3 + 2 * d.s3};
+  x->face_box[2] = Box{-d.s1, 0, -d.s3, d.n1 + 2 * d.s1, d.n2 + 1, d.n3 + 2 * d.s3};
+  x->face_box[3] = Box{-d.s1, -d.s2, 0, d.n1 + 2 * d.s1, d.n2 + 2 * d.s2, d.n3 + 1};
+  x->emf_box = Box{0, 0, 0, d.n1 + d.s1, d.n2 + d.s2, d.n3 + d.s3};
+  x->active_box = Box{0, 0, 0, d.n1, d.n2, d.n3};
+  x->dq_box = Box{-d.s1, -d.s2, -d.s3, d.n1 + 2 * d.s1, d.n2 + 2 * d.s2, d.n3 + 2 * d.s3};
+  long long nz = d.nz;
+  x->cap = (int)((long long)d.n1 * d.n2 * d.n3 < (1LL << 22) ? (long long)d.n1 * d.n2 * d.n3 : (1LL << 22));
+  if (cudaStreamCreateWithFlags(&x->stream, cudaStreamNonBlocking) != cudaSuccess) {
+    delete x;
+    set_err("cudaStreamCreate failed");
+    return HGPU_E_CUDA;
+  }
+  size_t pb = sizeof(double) * NPR * nz;
+  bool ok = cudaMalloc(&x->p, pb) == cudaSuccess && cudaMalloc(&x->pk, pb) == cudaSuccess &&
+            cudaMalloc(&x->uf, pb) == cudaSuccess && cudaMalloc(&x->ucum, pb) == cudaSuccess &&
+            cudaMalloc(&x->E, sizeof(double) * 3 * nz) == cudaSuccess &&
+            cudaMalloc(&x->G, sizeof(double) * G_NCOMP * d.nij) == cudaSuccess &&
+            cudaMalloc(&x->pflag, sizeof(int) * nz) == cudaSuccess &&
+            cudaMalloc(&x->gammacheck, sizeof(double) * nz) == cudaSuccess &&
+            cudaMalloc(&x->cand, sizeof(long long) * x->cap) == cudaSuccess &&
+            cudaMalloc(&x->fixlist, sizeof(long long) * x->cap) == cudaSuccess &&
+            cudaMalloc(&x->cand_orig, sizeof(int) * x->cap) == cudaSuccess &&
+            cudaMalloc(&x->cand_dec, sizeof(int) * x->cap) == cudaSuccess &&
+            cudaMalloc(&x->candmap, sizeof(int) * nz) == cudaSuccess &&
+            cudaMalloc(&x->fixvals, sizeof(double) * 5 * x->cap) == cudaSuccess &&
+            cudaMalloc(&x->sc, sizeof(Scalars)) == cudaSuccess;
+  for (int dd = 1; dd <= 3 && ok; dd++) ok = cudaMalloc(&x->F[dd], pb) == cudaSuccess;
+  if (!ok) {
+    hgpu_destroy(x);
+    set_err("device allocation failed");
+    return HGPU_E_NOMEM;
+  }
+  cudaMemsetAsync(x->p, 0, pb, x->stream);
+  cudaMemsetAsync(x->pk, 0, pb, x->stream);
+  cudaMemsetAsync(x->uf, 0, pb, x->stream);
+  cudaMemsetAsync(x->ucum, 0, pb, x->stream);
+  cudaMemsetAsync(x->E, 0, sizeof(double) * 3 * nz, x->stream);
+  for (int dd = 1; dd <= 3; dd++) cudaMemsetAsync(x->F[dd], 0, pb, x->stream);
+  cudaMemsetAsync(x->pflag, 0, sizeof(int) * nz, x->stream);
+  cudaMemsetAsync(x->candmap, 0xFF, sizeof(int) * nz, x->stream);
+  cudaMemsetAsync(x->sc, 0, sizeof(Scalars), x->stream);
+  if (cudaStreamSynchronize(x->stream) != cudaSuccess) {
+    hgpu_destroy(x);
+    set_err("initialisation failed");
+    return HGPU_E_CUDA;
+  }
+  *out = x;
+  return HGPU_OK;
+}
+
+int hgpu_upload_geometry(hgpu_ctx *x, const double *gcov, const double *gcon, const double *gcovpert,
+                         const double *gdet, const double *conn, const double *floors) {
+  if (!x || !gcov || !gcon || !gcovpert || !gdet || !conn || !floors) return HGPU_E_INVALID;
+  const Dims &d = x->d;
+  long long nij = d.nij;
+  double *h = (double *)malloc(sizeof(double) * G_NCOMP * nij);
+  if (!h) return HGPU_E_NOMEM;
+  const int locs[4] = {R_FACE1, R_FACE2, R_FACE3, R_CENT};
+  for (long long ij = 0; ij < nij; ij++) {
+    for (int s = 0; s < 4; s++) {
+      int L = locs[s];
+      for (int q = 0; q < 16; q++) {
+        h[(long long)(s * GLOC + q) * nij + ij] = gcov[(ij * 8 + L) * 16 + q];
+        h[(long long)(s * GLOC + 16 + q) * nij + ij] = gcon[(ij * 8 + L) * 16 + q];
+      }
+      h[(long long)(s * GLOC + 32) * nij + ij] = gcovpert[(ij * 8 + L) * 4 + 0];
+      h[(long long)(s * GLOC + 33) * nij + ij] = gdet[ij * 8 + L];
+    }
+    h[(long long)(G_CORN + 0) * nij + ij] = gdet[ij * 8 + R_CORN1];
+    h[(long long)(G_CORN + 1) * nij + ij] = gdet[ij * 8 + R_CORN2];
+    h[(long long)(G_CORN + 2) * nij + ij] = gdet[ij * 8 + R_CORN3];
+    for (int q = 0; q < 64; q++) h[(long long)(G_CONN + q) * nij + ij] = conn[ij * 64 + q];
+    h[(long long)(G_FLOOR + 0) * nij + ij] = floors[ij * 2 + 0];
+    h[(long long)(G_FLOOR + 1) * nij + ij] = floors[ij * 2 + 1];
+  }
+  cudaError_t e = cudaMemcpy(x->G, h, sizeof(double) * G_NCOMP * nij, cudaMemcpyHostToDevice);
+  free(h);
+  if (e != cudaSuccess) {
+    set_err("geometry upload: %s", cudaGetErrorString(e));
+    return HGPU_E_CUDA;
+  }
+  return HGPU_OK;
+}
+
+static int ensure_staging(hgpu_ctx *x) {
+  if (!x->staging) CUDA_TRY(cudaMalloc(&x->staging, sizeof(double) * NPR * x->d.nz));
+  return HGPU_OK;
+}
+
+int hgpu_upload_state(hgpu_ctx *x, const double *p, const int *pflag, double t, double dt) {
+  if (!x || !p) return HGPU_E_INVALID;
+  int rc = ensure_staging(x);
+  if (rc) return rc;
+  long long nz = x->d.nz;
+  CUDA_TRY(cudaMemcpyAsync(x->staging, p, sizeof(double) * NPR * nz, cudaMemcpyHostToDevice, x->stream));
+  LAUNCH(x, K_OTHER, aos_to_soa_kernel, grid_for(nz * NPR, 256), 256, x->staging, x->p, nz);
+  if (pflag) CUDA_TRY(cudaMemcpyAsync(x->pflag, pflag, sizeof(int) * nz, cudaMemcpyHostToDevice, x->stream));
+  Scalars s;
+  memset(&s, 0, sizeof(s));
+  s.t = t;
+  s.dt = dt;
+  CUDA_TRY(cudaMemcpyAsync(x->sc, &s, sizeof(Scalars), cudaMemcpyHostToDevice, x->stream));
+  CUDA_TRY(cudaStreamSynchronize(x->stream));
+  CUDA_TRY(cudaGetLastError());
+  return HGPU_OK;
+}
+
+int hgpu_download_state(hgpu_ctx *x, double *p, int *pflag, double *t, double *dt) {
+  if (!x) return HGPU_E_INVALID;
+  long long nz = x->d.nz;
+  if (p) {
+    int rc = ensure_staging(x);
+    if (rc) return rc;
+    LAUNCH(x, K_OTHER, soa_to_aos_kernel, grid_for(nz * NPR, 256), 256, x->p, x->staging, nz);
+    CUDA_TRY(cudaMemcpyAsync(p, x->staging, sizeof(double) * NPR * nz, cudaMemcpyDeviceToHost, x->stream));
+  }
+  if (pflag) CUDA_TRY(cudaMemcpyAsync(pflag, x->pflag, sizeof(int) * nz, cudaMemcpyDeviceToHost, x->stream));
+  Scalars s;
+  CUDA_TRY(cudaMemcpyAsync(&s, x->sc, sizeof(Scalars), cudaMemcpyDeviceToHost, x->stream));
+  CUDA_TRY(cudaStreamSynchronize(x->stream));
+  CUDA_TRY(cudaGetLastError());
+  if (t) *t = s.t;
+  if (dt) *dt = s.dt;
+  return HGPU_OK;
+}
+
+// one stage: fluxes, EMFs, update, bound, post_fixup, bound
+static void launch_fluxes(hgpu_ctx *x, const double *pb) {
+  const Dims &d = x->d;
+  cudaStream_t s = x->stream;
+  (void)s;
+  if (d.n1 > 1)
+    LAUNCH(x, K_FLUX1, flux_kernel<1>, grid_for(x->face_box[1].size(), 128), 128, d, x->P, x->face_box[1], pb, x->G,
+           x->F[1], x->sc);
+  if (d.n2 > 1)
+    LAUNCH(x, K_FLUX2, flux_kernel<2>, grid_for(x->face_box[2].size(), 128), 128, d, x->P, x->face_box[2], pb, x->G,
+           x->F[2], x->sc);
+  if (d.n3 > 1)
+    LAUNCH(x, K_FLUX3, flux_kernel<3>, grid_for(x->face_box[3].size(), 128), 128, d, x->P, x->face_box[3], pb, x->G,
+           x->F[3], x->sc);
+  LAUNCH(x, K_EMF, emf_kernel, grid_for(x->emf_box.size(), 256), 256, d, x->emf_box, x->F[1], x->F[2], x->F[3], x->G,
+         x->E);
+}
+
+static void launch_bound(hgpu_ctx *x, double *pv) {
+  const Dims &d = x->d;
+  LAUNCH(x, K_BOUND_GHOST, bound_ghost_kernel, grid_for(d.nz, 128), 128, d, x->P, pv, x->G, x->sc);
+  if (d.n2 > 1) LAUNCH(x, K_BOUND_POLE, bound_pole_kernel, grid_for(2LL * d.n1 * d.n3, 128), 128, d, x->P, pv);
+}
+
+static void launch_stage(hgpu_ctx *x, int timeorder) {
+  const Dims &d = x->d;
+  cudaStream_t s = x->stream;
+  const double *pi = x->p;
+  const double *pb = (timeorder == 0) ? x->p : x->pk;
+  double *pf = (timeorder == 0) ? x->pk : x->p;
+  int finalstep = (timeorder == 1);
+  // midpoint tables (step_ch.c:504-524)
+  double CUf0 = 1.0, CUf1 = 0.0, CUf2 = (timeorder == 0) ? 0.5 : 1.0;
+  double Cn0 = 0.0, Cn1 = 0.0, Cn2 = (timeorder == 0) ? 0.0 : 1.0;
+  (void)s;
+  LAUNCH(x, K_RESET, reset_stage_kernel, 1, 32, x->sc);
+  launch_fluxes(x, pb);
+  LAUNCH(x, K_UPDATE, update_kernel, grid_for(x->active_box.size(), 128), 128, d, x->P, x->active_box, pi, pb, pf, x->uf,
+         x->ucum, x->F[1], x->F[2], x->F[3], x->E, x->G, x->pflag, x->sc, CUf0, CUf1, CUf2, Cn0, Cn1, Cn2, timeorder,
+         finalstep);
+  launch_bound(x, pf);
+  // post_fixup (fixup.c:37-96)
+  LAUNCH(x, K_BOUND_PFLAG, bound_pflag_kernel, grid_for(d.nz, 256), 256, d, x->P, x->pflag);
+  LAUNCH(x, K_CHECK_GAMMA, checksol_gamma_kernel, grid_for(x->dq_box.size(), 128), 128, d, x->dq_box, pf, x->G,
+         x->gammacheck, x->cand, x->cap, x->sc);
+  LAUNCH(x, K_CHECK_RESOLVE, checksol_resolve_kernel, 1, 1024, d, pf, x->gammacheck, x->pflag, x->cand, x->candmap,
+         x->cand_orig, x->cand_dec, x->cap, x->sc);
+  LAUNCH(x, K_FIX_COLLECT, fixup_collect_kernel, grid_for(x->active_box.size(), 256), 256, d, x->active_box, x->pflag,
+         x->fixlist, x->cap, x->sc);
+  // grid-stride over the device-side list length; idle blocks exit at once
+  int fixgrid = (int)grid_for(x->cap, 128);
+  if (fixgrid > 296) fixgrid = 296;
+  LAUNCH(x, K_FIX_COMPUTE, fixup_compute_kernel, fixgrid, 128, d, x->P, pf, x->pflag, x->G, x->fixlist, x->fixvals,
+         x->cap, finalstep, x->sc);
+  LAUNCH(x, K_FIX_SCATTER, fixup_scatter_kernel, fixgrid, 128, d, pf, x->pflag, x->fixlist, x->fixvals, x->cap,
+         finalstep, x->sc);
+  launch_bound(x, pf);
+}
+
+static int read_stats(hgpu_ctx *x, hgpu_stats *st) {
+  Scalars s;
+  CUDA_TRY(cudaMemcpyAsync(&s, x->sc, sizeof(Scalars), cudaMemcpyDeviceToHost, x->stream));
+  CUDA_TRY(cudaStreamSynchronize(x->stream));
+  CUDA_TRY(cudaGetLastError());
+  if (st) {
+    st->newton_iters = (long long)s.iters;
+    st->err = s.err;
+    st->nfail = s.nfail;
+    st->nfixed = s.nfixed;
+  }
+  if (s.overflow) {
+    set_err("fixup list capacity exceeded (%s%d)", "", s.overflow);
+    return HGPU_E_PHYSICS;
+  }
+  if (s.err) {
+    set_err("physics failure bits %s%d", "", s.err);
+    return HGPU_E_PHYSICS;
+  }
+  return HGPU_OK;
+}
+
+static void clear_counters(hgpu_ctx *x) {
+  // iters, err, nfixed, overflow accumulate over a call
+  cudaMemsetAsync(&x->sc->iters, 0, sizeof(unsigned long long), x->stream);
+  cudaMemsetAsync(&x->sc->err, 0, sizeof(int), x->stream);
+  cudaMemsetAsync(&x->sc->nfixed, 0, sizeof(int), x->stream);
+  cudaMemsetAsync(&x->sc->overflow, 0, sizeof(int), x->stream);
+}
+
+int hgpu_step_ch(hgpu_ctx *x, int nsteps, hgpu_stats *stats) {
+  if (!x || nsteps < 0) return HGPU_E_INVALID;
+  clear_counters(x);
+  for (int n = 0; n < nsteps; n++) {
+    launch_stage(x, 0);
+    launch_stage(x, 1);
+    LAUNCH(x, K_FINALIZE, finalize_kernel, 1, 32, x->P, x->sc, 1);
+  }
+  CUDA_TRY(cudaGetLastError());
+  if (stats) return read_stats(x, stats);
+  return HGPU_OK;
+}
+
+int hgpu_advance_stage(hgpu_ctx *x, int timeorder, double *ndt, hgpu_stats *stats) {
+  if (!x || (timeorder != 0 && timeorder != 1)) return HGPU_E_INVALID;
+  clear_counters(x);
+  launch_stage(x, timeorder);
+  LAUNCH(x, K_FINALIZE, finalize_kernel, 1, 32, x->P, x->sc, 0);
+  CUDA_TRY(cudaGetLastError());
+  int rc = read_stats(x, stats);
+  if (ndt) {
+    unsigned long long b;
+    CUDA_TRY(cudaMemcpy(&b, &x->sc->ndtbits[0], sizeof(b), cudaMemcpyDeviceToHost));
+    double v;
+    memcpy(&v, &b, sizeof(v));
+    *ndt = v;
+  }
+  return rc;
+}
+
+int hgpu_fluxcalc(hgpu_ctx *x, int which, double *F1, double *F2, double *F3, double *ndt1, double *ndt2,
+                  double *ndt3) {
+  if (!x || (which != 0 && which != 1)) return HGPU_E_INVALID;
+  LAUNCH(x, K_RESET, reset_stage_kernel, 1, 32, x->sc);
+  launch_fluxes(x, which ? x->pk : x->p);
+  CUDA_TRY(cudaGetLastError());
+  Scalars s;
+  CUDA_TRY(cudaMemcpyAsync(&s, x->sc, sizeof(Scalars), cudaMemcpyDeviceToHost, x->stream));
+  CUDA_TRY(cudaStreamSynchronize(x->stream));
+  double v[4];
+  for (int q = 1; q <= 3; q++) memcpy(&v[q], &s.ndtbits[q], sizeof(double));
+  if (ndt1) *ndt1 = v[1];
+  if (ndt2) *ndt2 = v[2];
+  if (ndt3) *ndt3 = v[3];
+  {
+    // faces read by the update (advance.c:777-790)
+    const Dims &d = x->d;
+    Box fb[4] = {Box{0, 0, 0, 0, 0, 0}, Box{0, 0, 0, d.n1 + 1, d.n2, d.n3}, Box{0, 0, 0, d.n1, d.n2 + 1, d.n3},
+                 Box{0, 0, 0, d.n1, d.n2, d.n3 + 1}};
+    int nd[4] = {0, d.n1, d.n2, d.n3};
+    for (int q = 1; q <= 3; q++)
+      if (nd[q] > 1) bflux_kernel<<<grid_for(fb[q].size(), 256), 256, 0, x->stream>>>(d, q, fb[q], x->E, x->F[q]);
+  }
+  double *outs[4] = {nullptr, F1, F2, F3};
+  int rc = ensure_staging(x);
+  if (rc) return rc;
+  long long nz = x->d.nz;
+  for (int q = 1; q <= 3; q++) {
+    if (!outs[q]) continue;
+    soa_to_aos_kernel<<<grid_for(nz * NPR, 256), 256, 0, x->stream>>>(x->F[q], x->staging, nz);
+    CUDA_TRY(cudaMemcpyAsync(outs[q], x->staging, sizeof(double) * NPR * nz, cudaMemcpyDeviceToHost, x->stream));
+    CUDA_TRY(cudaStreamSynchronize(x->stream));
+  }
+  return HGPU_OK;
+}
+
+int hgpu_bound_prim(hgpu_ctx *x, int which) {
+  if (!x || (which != 0 && which != 1)) return HGPU_E_INVALID;
+  launch_bound(x, which ? x->pk : x->p);
+  CUDA_TRY(cudaGetLastError());
+  CUDA_TRY(cudaStreamSynchronize(x->stream));
+  return HGPU_OK;
+}
+
+int hgpu_device_prims(hgpu_ctx *x, int which, double **dptr) {
+  if (!x || !dptr) return HGPU_E_INVALID;
+  *dptr = which ? x->pk : x->p;
+  return HGPU_OK;
+}
+
+int hgpu_sync(hgpu_ctx *x) {
+  if (!x) return HGPU_E_INVALID;
+  CUDA_TRY(cudaStreamSynchronize(x->stream));
+  CUDA_TRY(cudaGetLastError());
+  return HGPU_OK;
+}
+
+int hgpu_utoprim_batch(const double *U, const double *gcov, const double *gcon, const double *gdet, double *pr,
+                       int *pflag, long long n, double gam, double gammafail, long long *iters) {
+  if (n < 0 || (n > 0 && (!U || !gcov || !gcon || !gdet || !pr || !pflag))) return HGPU_E_INVALID;
+  if (n == 0) {
+    if (iters) *iters = 0;
+    return HGPU_OK;
+  }
+  double *dU = nullptr, *dgcov = nullptr, *dgcon = nullptr, *dg = nullptr, *dpr = nullptr;
+  int *dpf = nullptr;
+  unsigned long long *dit = nullptr;
+  int rc = HGPU_OK;
+  cudaError_t e = cudaSuccess;
+  if ((e = cudaMalloc(&dU, sizeof(double) * 8 * n)) != cudaSuccess ||
+      (e = cudaMalloc(&dgcov, sizeof(double) * 16 * n)) != cudaSuccess ||
+      (e = cudaMalloc(&dgcon, sizeof(double) * 16 * n)) != cudaSuccess ||
+      (e = cudaMalloc(&dg, sizeof(double) * n)) != cudaSuccess ||
+      (e = cudaMalloc(&dpr, sizeof(double) * 8 * n)) != cudaSuccess ||
+      (e = cudaMalloc(&dpf, sizeof(int) * n)) != cudaSuccess ||
+      (e = cudaMalloc(&dit, sizeof(unsigned long long))) != cudaSuccess) {
+    rc = HGPU_E_NOMEM;
+  } else {
+    cudaMemcpy(dU, U, sizeof(double) * 8 * n, cudaMemcpyHostToDevice);
+    cudaMemcpy(dgcov, gcov, sizeof(double) * 16 * n, cudaMemcpyHostToDevice);
+    cudaMemcpy(dgcon, gcon, sizeof(double) * 16 * n, cudaMemcpyHostToDevice);
+    cudaMemcpy(dg, gdet, sizeof(double) * n, cudaMemcpyHostToDevice);
+    cudaMemcpy(dpr, pr, sizeof(double) * 8 * n, cudaMemcpyHostToDevice);
+    cudaMemset(dit, 0, sizeof(unsigned long long));
+    utoprim_batch_kernel<<<grid_for(n, 128), 128>>>(dU, dgcov, dgcon, dg, dpr, dpf, n, gam, gammafail, dit);
+    e = cudaGetLastError();
+    if (e == cudaSuccess) e = cudaDeviceSynchronize();
+    if (e == cudaSuccess) {
+      unsigned long long it = 0;
+      cudaMemcpy(pr, dpr, sizeof(double) * 8 * n, cudaMemcpyDeviceToHost);
+      cudaMemcpy(pflag, dpf, sizeof(int) * n, cudaMemcpyDeviceToHost);
+      cudaMemcpy(&it, dit, sizeof(it), cudaMemcpyDeviceToHost);
+      if (iters) *iters = (long long)it;
+    } else {
+      set_err("utoprim batch: %s", cudaGetErrorString(e));
+      rc = HGPU_E_CUDA;
+    }
+  }
+  cudaFree(dU);
+  cudaFree(dgcov);
+  cudaFree(dgcon);
+  cudaFree(dg);
+  cudaFree(dpr);
+  cudaFree(dpf);
+  cudaFree(dit);
+  return rc;
+}
+
+__global__ void set_dt_kernel(Scalars *sc) {
+  if (threadIdx.x == 0 && blockIdx.x == 0) sc->dt = __longlong_as_double((long long)sc->ndtbits[0]);
+}
+
+int hgpu_init_dt(hgpu_ctx *x, double *dt) {
+  if (!x) return HGPU_E_INVALID;
+  LAUNCH(x, K_RESET, reset_stage_kernel, 1, 32, x->sc);
+  launch_fluxes(x, x->p);
+  LAUNCH(x, K_FINALIZE, finalize_kernel, 1, 32, x->P, x->sc, 0);
+  LAUNCH(x, K_OTHER, set_dt_kernel, 1, 32, x->sc);
+  CUDA_TRY(cudaGetLastError());
+  Scalars s;
+  CUDA_TRY(cudaMemcpyAsync(&s, x->sc, sizeof(Scalars), cudaMemcpyDeviceToHost, x->stream));
+  CUDA_TRY(cudaStreamSynchronize(x->stream));
+  if (dt) *dt = s.dt;
+  return HGPU_OK;
+}
+
+int hgpu_step_ch_timed(hgpu_ctx *x, int nsteps, float *ms, hgpu_stats *stats) {
+  if (!x || nsteps < 0) return HGPU_E_INVALID;
+  cudaEvent_t a, b;
+  CUDA_TRY(cudaEventCreate(&a));
+  CUDA_TRY(cudaEventCreate(&b));
+  clear_counters(x);
+  CUDA_TRY(cudaEventRecord(a, x->stream));
+  for (int n = 0; n < nsteps; n++) {
+    launch_stage(x, 0);
+    launch_stage(x, 1);
+    LAUNCH(x, K_FINALIZE, finalize_kernel, 1, 32, x->P, x->sc, 1);
+  }
+  CUDA_TRY(cudaEventRecord(b, x->stream));
+  CUDA_TRY(cudaEventSynchronize(b));
+  float t = 0.f;
+  cudaEventElapsedTime(&t, a, b);
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  if (ms) *ms = t;
+  return read_stats(x, stats);
+}
+
+int hgpu_set_profiling(hgpu_ctx *x, int on) {
+  if (!x) return HGPU_E_INVALID;
+  CUDA_TRY(cudaStreamSynchronize(x->stream));
+  collect_profile(x);
+  x->profiling = (on != 0);
+  for (int k = 0; k < K_NKERNELS; k++) {
+    x->kms[k] = 0.0;
+    x->kcount[k] = 0;
+  }
+  return HGPU_OK;
+}
+
+int hgpu_kernel_times(hgpu_ctx *x, const char **names, double *ms, long long *launches, int n) {
+  if (!x) return -HGPU_E_INVALID;
+  if (cudaStreamSynchronize(x->stream) != cudaSuccess) return -HGPU_E_CUDA;
+  collect_profile(x);
+  for (int k = 0; k < K_NKERNELS && k < n; k++) {
+    if (names) names[k] = kKernelNames[k];
+    if (ms) ms[k] = x->kms[k];
+    if (launches) launches[k] = x->kcount[k];
+  }
+  return K_NKERNELS;
+}
+
+long long hgpu_launch_count(hgpu_ctx *x) { return x ? x->launches : -1; }
+
+int hgpu_alloc_pinned(size_t bytes, void **ptr) {
+  if (!ptr) return HGPU_E_INVALID;
+  CUDA_TRY(cudaHostAlloc(ptr, bytes, cudaHostAllocDefault));
+  return HGPU_OK;
+}
+
+int hgpu_free_pinned(void *ptr) {
+  if (ptr) CUDA_TRY(cudaFreeHost(ptr));
+  return HGPU_OK;
+}
+
+}  // extern "C"

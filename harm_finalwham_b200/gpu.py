@@ -1,0 +1,230 @@
+"""ctypes bindings of the C ABI in include/harmgpu.h.
+
+The class mirrors the reference's entry points for the per-zone update:
+``step_ch`` (step_ch.c:16), ``advance_stage`` (advance.c:16 plus the per-stage
+bound/post_fixup sequence of step_ch.c:94-186), ``fluxcalc`` (flux.c:7 with
+flux_ct fluxct.c:10), ``bound_prim`` (step_ch.c:568) and ``utoprim_batch``
+(utoprimgen.c:23, batched).  Host arrays use the reference's layouts; errors
+are raised as HarmGPUError carrying the library's return code and message.
+There is no CPU fallback: if the library or a GPU is missing, calls fail.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+from . import build as _build
+
+NPR = 8
+LIM = {"DONOR": 0, "VANL": 1, "MINM": 2, "MC": 3, "WENO5": 9}
+FLUX = {"LAXF": 0, "HLL": 1}
+BC = {"OUTFLOW": 0, "POLARAXIS": 4, "PERIODIC": 7}
+PREC = {"fp64": 0, "mixed": 1}
+
+_lib = None
+
+
+class HarmGPUError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"libharmgpu error {code}: {msg}")
+        self.code = code
+
+
+class hgpu_config(ctypes.Structure):
+    _fields_ = [("n1", ctypes.c_int), ("n2", ctypes.c_int), ("n3", ctypes.c_int), ("ng", ctypes.c_int),
+                ("lim", ctypes.c_int), ("fluxmethod", ctypes.c_int), ("bc", ctypes.c_int * 6),
+                ("precision", ctypes.c_int), ("dx", ctypes.c_double * 4), ("gam", ctypes.c_double),
+                ("cour", ctypes.c_double), ("safe", ctypes.c_double), ("defcon", ctypes.c_double),
+                ("tf", ctypes.c_double), ("rhominlimit", ctypes.c_double), ("uuminlimit", ctypes.c_double),
+                ("gammamax", ctypes.c_double), ("gammafail", ctypes.c_double)]
+
+
+class hgpu_stats(ctypes.Structure):
+    _fields_ = [("newton_iters", ctypes.c_longlong), ("err", ctypes.c_int), ("nfail", ctypes.c_int),
+                ("nfixed", ctypes.c_int)]
+
+
+_P = ctypes.POINTER
+_dp = _P(ctypes.c_double)
+_ip = _P(ctypes.c_int)
+
+
+def load_library(path=None):
+    """Load libharmgpu.so (building it in-tree first if sources are newer)."""
+    global _lib
+    if _lib is not None and path is None:
+        return _lib
+    if path is None:
+        path = _build.LIB
+        if not os.path.exists(path):
+            path = _build.build()
+    L = ctypes.CDLL(path)
+    L.hgpu_abi_version.restype = ctypes.c_int
+    L.hgpu_last_error.restype = ctypes.c_char_p
+    L.hgpu_create.argtypes = [_P(hgpu_config), _P(ctypes.c_void_p)]
+    L.hgpu_destroy.argtypes = [ctypes.c_void_p]
+    L.hgpu_destroy.restype = None
+    L.hgpu_upload_geometry.argtypes = [ctypes.c_void_p] + [_dp] * 6
+    L.hgpu_upload_state.argtypes = [ctypes.c_void_p, _dp, _ip, ctypes.c_double, ctypes.c_double]
+    L.hgpu_download_state.argtypes = [ctypes.c_void_p, _dp, _ip, _dp, _dp]
+    L.hgpu_step_ch.argtypes = [ctypes.c_void_p, ctypes.c_int, _P(hgpu_stats)]
+    L.hgpu_advance_stage.argtypes = [ctypes.c_void_p, ctypes.c_int, _dp, _P(hgpu_stats)]
+    L.hgpu_fluxcalc.argtypes = [ctypes.c_void_p, ctypes.c_int, _dp, _dp, _dp, _dp, _dp, _dp]
+    L.hgpu_bound_prim.argtypes = [ctypes.c_void_p, ctypes.c_int]
+    L.hgpu_utoprim_batch.argtypes = [_dp, _dp, _dp, _dp, _dp, _ip, ctypes.c_longlong, ctypes.c_double,
+                                     ctypes.c_double, _P(ctypes.c_longlong)]
+    L.hgpu_device_prims.argtypes = [ctypes.c_void_p, ctypes.c_int, _P(ctypes.c_void_p)]
+    L.hgpu_sync.argtypes = [ctypes.c_void_p]
+    for name in ("hgpu_create", "hgpu_upload_geometry", "hgpu_upload_state", "hgpu_download_state", "hgpu_step_ch",
+                 "hgpu_advance_stage", "hgpu_fluxcalc", "hgpu_bound_prim", "hgpu_utoprim_batch",
+                 "hgpu_device_prims", "hgpu_sync"):
+        getattr(L, name).restype = ctypes.c_int
+    if path == _build.LIB:
+        _lib = L
+    return L
+
+
+def _check(L, rc):
+    if rc != 0:
+        raise HarmGPUError(rc, L.hgpu_last_error().decode(errors="replace"))
+
+
+def _ptr(a, ctype=ctypes.c_double):
+    if a is None:
+        return None
+    return a.ctypes.data_as(ctypes.POINTER(ctype))
+
+
+def _contig(a, dtype):
+    a = np.asarray(a)
+    if a.dtype != dtype or not a.flags.c_contiguous:
+        a = np.ascontiguousarray(a, dtype=dtype)
+    return a
+
+
+class HarmGPU:
+    """One device-resident domain (the reference's global state for one run)."""
+
+    def __init__(self, n1, n2, n3, ng, dx, lim="MC", flux="HLL", bc=("OUTFLOW", "OUTFLOW", "POLARAXIS",
+                 "POLARAXIS", "PERIODIC", "PERIODIC"), precision="fp64", gam=4.0 / 3.0, cour=0.8, safe=1.3,
+                 defcon=1.0, tf=2000.0, rhominlimit=1e-20, uuminlimit=1e-20, gammamax=25.0, gammafail=2500.0):
+        self.L = load_library()
+        c = hgpu_config()
+        c.n1, c.n2, c.n3, c.ng = n1, n2, n3, ng
+        c.lim = LIM[lim] if isinstance(lim, str) else int(lim)
+        c.fluxmethod = FLUX[flux] if isinstance(flux, str) else int(flux)
+        for i, b in enumerate(bc):
+            c.bc[i] = BC[b] if isinstance(b, str) else int(b)
+        c.precision = PREC[precision] if isinstance(precision, str) else int(precision)
+        c.dx[0] = 0.0
+        for i in range(3):
+            c.dx[i + 1] = float(dx[i])
+        c.gam, c.cour, c.safe, c.defcon, c.tf = gam, cour, safe, defcon, tf
+        c.rhominlimit, c.uuminlimit, c.gammamax, c.gammafail = rhominlimit, uuminlimit, gammamax, gammafail
+        self.cfg = c
+        self.n = (n1, n2, n3)
+        self.g = tuple(ng if n > 1 else 0 for n in self.n)
+        self.s = tuple(1 if n > 1 else 0 for n in self.n)
+        self.nt = tuple(n + 2 * g for n, g in zip(self.n, self.g))
+        self.gt = (self.nt[0] + self.s[0], self.nt[1] + self.s[1])
+        h = ctypes.c_void_p()
+        _check(self.L, self.L.hgpu_create(ctypes.byref(c), ctypes.byref(h)))
+        self.h = h
+
+    @classmethod
+    def from_problem(cls, pr, precision="fp64"):
+        """Build from an object with the oracle Problem's attributes."""
+        inv_bc = {0: "OUTFLOW", 4: "POLARAXIS", 7: "PERIODIC"}
+        o = cls(pr.n[0], pr.n[1], pr.n[2], pr.ng, pr.dx, lim=pr.lim, flux=pr.flux,
+                bc=tuple(inv_bc[b] for b in pr.bc), precision=precision, gam=pr.gam, cour=pr.cour, safe=pr.safe,
+                defcon=pr.defcon, tf=pr.tf, rhominlimit=pr.rhominlimit, uuminlimit=pr.uuminlimit,
+                gammamax=pr.gammamax, gammafail=pr.gammafail)
+        o.upload_geometry(pr.gcov, pr.gcon, pr.gcovpert, pr.gdet, pr.conn, pr.floors)
+        o.upload_state(pr.p, pr.pflag, pr.t, pr.dt)
+        return o
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.L.hgpu_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def upload_geometry(self, gcov, gcon, gcovpert, gdet, conn, floors):
+        arrs = [_contig(a, np.float64) for a in (gcov, gcon, gcovpert, gdet, conn, floors)]
+        nij = self.gt[0] * self.gt[1]
+        expect = [nij * 128, nij * 128, nij * 32, nij * 8, nij * 64, nij * 2]
+        for a, e in zip(arrs, expect):
+            if a.size != e:
+                raise ValueError(f"geometry array has {a.size} values, expected {e}")
+        _check(self.L, self.L.hgpu_upload_geometry(self.h, *[_ptr(a) for a in arrs]))
+
+    def upload_state(self, p, pflag=None, t=0.0, dt=0.0):
+        p = _contig(p, np.float64)
+        if p.size != np.prod(self.nt) * NPR:
+            raise ValueError("primitive array has the wrong size")
+        pf = None if pflag is None else _contig(pflag, np.int32)
+        _check(self.L, self.L.hgpu_upload_state(self.h, _ptr(p), _ptr(pf, ctypes.c_int), float(t), float(dt)))
+
+    def download_state(self):
+        p = np.empty(self.nt + (NPR,))
+        pf = np.empty(self.nt, dtype=np.int32)
+        t = ctypes.c_double()
+        dt = ctypes.c_double()
+        _check(self.L, self.L.hgpu_download_state(self.h, _ptr(p), _ptr(pf, ctypes.c_int), ctypes.byref(t),
+                                                  ctypes.byref(dt)))
+        return p, pf, t.value, dt.value
+
+    def step_ch(self, nsteps=1, stats=True):
+        st = hgpu_stats()
+        _check(self.L, self.L.hgpu_step_ch(self.h, int(nsteps), ctypes.byref(st) if stats else None))
+        return st
+
+    def advance_stage(self, timeorder):
+        st = hgpu_stats()
+        ndt = ctypes.c_double()
+        _check(self.L, self.L.hgpu_advance_stage(self.h, int(timeorder), ctypes.byref(ndt), ctypes.byref(st)))
+        return ndt.value, st
+
+    def fluxcalc(self, which=0):
+        F = [np.zeros(self.nt + (NPR,)) for _ in range(3)]
+        nd = [ctypes.c_double() for _ in range(3)]
+        _check(self.L, self.L.hgpu_fluxcalc(self.h, int(which), _ptr(F[0]), _ptr(F[1]), _ptr(F[2]),
+                                            *[ctypes.byref(x) for x in nd]))
+        return F, [x.value for x in nd]
+
+    def bound_prim(self, which=0):
+        _check(self.L, self.L.hgpu_bound_prim(self.h, int(which)))
+
+    def sync(self):
+        _check(self.L, self.L.hgpu_sync(self.h))
+
+    def active(self, a):
+        g = self.g
+        return a[g[0]:g[0] + self.n[0], g[1]:g[1] + self.n[1], g[2]:g[2] + self.n[2]]
+
+
+def utoprim_batch(U, gcov, gcon, gdet, guess, gam, gammafail):
+    """Batched Utoprimgen on the GPU (hgpu_utoprim_batch)."""
+    L = load_library()
+    U = _contig(U, np.float64)
+    gcov = _contig(gcov, np.float64)
+    gcon = _contig(gcon, np.float64)
+    gdet = _contig(gdet, np.float64)
+    pr = np.array(guess, dtype=np.float64, order="C", copy=True)
+    n = U.shape[0]
+    pflag = np.zeros(n, dtype=np.int32)
+    it = ctypes.c_longlong(0)
+    _check(L, L.hgpu_utoprim_batch(_ptr(U), _ptr(gcov), _ptr(gcon), _ptr(gdet), _ptr(pr), _ptr(pflag, ctypes.c_int),
+                                   n, gam, gammafail, ctypes.byref(it)))
+    return pr, pflag, it.value

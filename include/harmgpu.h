@@ -1,0 +1,165 @@
+/*
+ * harmgpu.h -- C ABI of the B200 per-zone conservative update of HARM.
+ *
+ * Plain C types only (pointers, sizes, ints, doubles).  A caller that can
+ * link C (the reference's own C host loop, Python ctypes, cgo, JNI ...)
+ * drives the GPU through these entry points.  Each entry point names the
+ * reference routine it stands in for.
+ *
+ * Host array layouts are the reference's (defs.h:27-206 with the pointer
+ * shift of set_arrays.c:14-78), restricted to `ng` ghost zones per
+ * dimension that has more than one zone:
+ *   primitives   double [n1+2g1][n2+2g2][n3+2g3][8]   (rho,u,u~1..3,B1..3)
+ *   pflag        int    [n1+2g1][n2+2g2][n3+2g3]      (FLAGUTOPRIMFAIL slot)
+ *   geometry     per (i,j) only -- the metric does not depend on x3:
+ *     gcov, gcon double [n1+2g1+s1][n2+2g2+s2][8 locations][4][4]
+ *     gcovpert   double [..][8][4]
+ *     gdet       double [..][8]
+ *     conn       double [..][4][4][4]   (CENT; conn[k][l][j] as set_grid.c:118)
+ *     floors     double [..][2]         (rho, u floor at CENT: set_density_floors, fixup.c:1542)
+ *   with gd = (nd>1 ? ng : 0), sd = (nd>1).
+ *
+ * Error convention: every entry point returns 0 on success, nonzero on
+ * failure (HGPU_E_*), and never aborts the process.  Physical failures are
+ * not errors: they are per-zone pflag codes (global.h:782-799) repaired by
+ * the fixups, exactly as in the reference.
+ */
+#ifndef HARMGPU_H
+#define HARMGPU_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define HGPU_ABI_VERSION 1
+
+/* return codes */
+#define HGPU_OK 0
+#define HGPU_E_INVALID 1      /* bad argument or unsupported option */
+#define HGPU_E_CUDA 2         /* CUDA runtime error */
+#define HGPU_E_PHYSICS 3      /* the reference would have called fail()/myexit() */
+#define HGPU_E_NOMEM 4
+
+/* option ids: the reference's own numbering (global.h:247-314, definit.h:300-310) */
+#define HGPU_LIM_DONOR 0
+#define HGPU_LIM_VANL 1
+#define HGPU_LIM_MINM 2
+#define HGPU_LIM_MC 3
+#define HGPU_LIM_WENO5 9
+#define HGPU_FLUX_LAXF 0
+#define HGPU_FLUX_HLL 1
+#define HGPU_BC_OUTFLOW 0
+#define HGPU_BC_POLARAXIS 4
+#define HGPU_BC_PERIODIC 7
+
+/* precision modes */
+#define HGPU_PREC_FP64 0      /* bit-identical to the reference CPU build */
+#define HGPU_PREC_MIXED 1     /* FP32 reconstruction, wave speeds and Riemann flux */
+
+typedef struct {
+  int n1, n2, n3;   /* active zones (N1,N2,N3 of the reference) */
+  int ng;           /* ghost zones kept on the device (>= 2 for MC, >= 3 for WENO5) */
+  int lim;          /* slope limiter (lim) */
+  int fluxmethod;   /* Riemann solver (fluxmethod) */
+  int bc[6];        /* BCtype[X1UP,X1DN,X2UP,X2DN,X3UP,X3DN] */
+  int precision;    /* HGPU_PREC_* */
+  double dx[4];     /* dx[1..3] */
+  double gam, cour, safe, defcon, tf;
+  double rhominlimit, uuminlimit, gammamax, gammafail;
+} hgpu_config;
+
+typedef struct hgpu_ctx hgpu_ctx;
+
+typedef struct {
+  long long newton_iters;   /* Newton iterations in the last call (the reference's nstroke) */
+  int err;                  /* error bits: conditions where the reference calls fail() */
+  int nfail;                /* zones with nonzero FLAGUTOPRIMFAIL after the last substep */
+  int nfixed;               /* zones repaired by fixup_utoprim in the last call */
+} hgpu_stats;
+
+/* Library/ABI identification. */
+int hgpu_abi_version(void);
+
+/* Create a device context on the current CUDA device (init-time set_arrays.c / set_grid.c
+   storage).  Returns HGPU_OK and *out, or an error code. */
+int hgpu_create(const hgpu_config *cfg, hgpu_ctx **out);
+void hgpu_destroy(hgpu_ctx *ctx);
+
+/* Upload the precomputed geometry (set_grid.c:7-151) and floors
+   (set_density_floors, fixup.c:1542-1654); host layouts above. */
+int hgpu_upload_geometry(hgpu_ctx *ctx, const double *gcov, const double *gcon, const double *gcovpert,
+                         const double *gdet, const double *conn, const double *floors);
+
+/* Upload primitives p (and optionally pflag, may be NULL) plus t and dt. */
+int hgpu_upload_state(hgpu_ctx *ctx, const double *p, const int *pflag, double t, double dt);
+/* Download primitives/pflag (either may be NULL) and t, dt. */
+int hgpu_download_state(hgpu_ctx *ctx, double *p, int *pflag, double *t, double *dt);
+
+/* step_ch (step_ch.c:16-252): nsteps full midpoint-RK2 steps with
+   boundaries, fixups and the dt update.  Asynchronous on the context's stream
+   unless stats is non-NULL (then it synchronises and fills stats). */
+int hgpu_step_ch(hgpu_ctx *ctx, int nsteps, hgpu_stats *stats);
+
+/* advance (advance.c:16) for RK stage `timeorder` of the midpoint method,
+   followed by the reference's per-stage bound_prim/post_fixup/bound_prim
+   sequence (step_ch.c:94-186).  Buffers: stage 0 reads p, writes pk;
+   stage 1 reads p and pk, writes p.  ndt receives the new dt estimate. */
+int hgpu_advance_stage(hgpu_ctx *ctx, int timeorder, double *ndt, hgpu_stats *stats);
+
+/* fluxcalc (flux.c:7-318) including flux_ct (fluxct.c:10), on the current
+   primitives (which=0: p, which=1: pk).  Fluxes F1..F3 are returned in the
+   reference layout when the pointers are non-NULL (only the faces the update
+   reads are defined).  ndt1..3 as fluxcalc. */
+int hgpu_fluxcalc(hgpu_ctx *ctx, int which, double *F1, double *F2, double *F3, double *ndt1, double *ndt2,
+                  double *ndt3);
+
+/* bound_prim (step_ch.c:568) on p (which=0) or pk (which=1). */
+int hgpu_bound_prim(hgpu_ctx *ctx, int which);
+
+/* Utoprimgen (utoprimgen.c:23) for a batch of n zones in host memory:
+   U (evolved conserved, with gdet) [n][8], per-zone CENT metric gcov/gcon [n][16],
+   gdet [n]; pr holds the guess and receives the result; pflag receives the
+   codes.  iters (may be NULL) receives the total Newton iterations. */
+int hgpu_utoprim_batch(const double *U, const double *gcov, const double *gcon, const double *gdet, double *pr,
+                       int *pflag, long long n, double gam, double gammafail, long long *iters);
+
+/* Raw device pointers of the resident state for callers that keep data on
+   the GPU (e.g. a graph-captured serving loop): primitive planes
+   [8][nt1][nt2][nt3] of p (which=0) or pk (which=1). */
+int hgpu_device_prims(hgpu_ctx *ctx, int which, double **dptr);
+
+/* Set dt from the face wave speeds of the current primitives: the ndt of
+   advance.c:231 evaluated on p (the reference's init uses set_dt,
+   advance.c:957, with zone-centre speeds).  *dt (may be NULL) receives it. */
+int hgpu_init_dt(hgpu_ctx *ctx, double *dt);
+
+/* step_ch for nsteps with CUDA events recorded on the context's stream
+   around the launches; *ms receives the device time. */
+int hgpu_step_ch_timed(hgpu_ctx *ctx, int nsteps, float *ms, hgpu_stats *stats);
+
+/* Per-kernel CUDA-event timing (off by default).  While on, every launch
+   is bracketed by events on the launching stream.  hgpu_kernel_times fills
+   up to n entries: names[i] (static strings), ms[i] total device time and
+   launches[i]; returns the number of kernel kinds or a negative error. */
+int hgpu_set_profiling(hgpu_ctx *ctx, int on);
+int hgpu_kernel_times(hgpu_ctx *ctx, const char **names, double *ms, long long *launches, int n);
+
+/* Number of kernels this context has launched since creation. */
+long long hgpu_launch_count(hgpu_ctx *ctx);
+
+/* Page-locked host buffers for fast host<->device copies. */
+int hgpu_alloc_pinned(size_t bytes, void **ptr);
+int hgpu_free_pinned(void *ptr);
+
+/* Synchronise the context's stream and report pending CUDA errors. */
+int hgpu_sync(hgpu_ctx *ctx);
+
+/* Human-readable text of the last error on this thread. */
+const char *hgpu_last_error(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,36 @@
+"""Load the committed golden fixtures (tests/golden/*.npz) into oracle Problems."""
+import os
+
+import numpy as np
+
+from oracle.pyoracle import Problem
+
+GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+CASES = ["torus2d_16x16_mc_hll", "torus3d_12x12x6_mc_laxf"]
+
+
+def load(name):
+    d = np.load(os.path.join(GOLDEN, name + ".npz"))
+    n = tuple(int(x) for x in d["n"])
+    pr = Problem(n[0], n[1], n[2], int(d["ng"]), tuple(float(x) for x in d["dx"]), gam=float(d["gam"]),
+                 cour=float(d["cour"]), lim=str(d["lim"]), flux=str(d["flux"]), bc=tuple(int(x) for x in d["bc"]),
+                 safe=float(d["safe"]), defcon=float(d["defcon"]), tf=float(d["tf"]),
+                 rhominlimit=float(d["rhominlimit"]), uuminlimit=float(d["uuminlimit"]),
+                 gammamax=float(d["gammamax"]), gammafail=float(d["gammafail"]))
+    for k in ("gcov", "gcon", "gcovpert", "gdet", "conn", "floors"):
+        getattr(pr, k)[...] = d[k]
+    pr.p[...] = d["p_init"]
+    pr.pflag[...] = d["pflag_init"]
+    pr.t = float(d["t_init"])
+    pr.dt = float(d["dt_init"])
+    steps = [int(s) for s in d["steps"]]
+    ref = {s: dict(p=d[f"p_s{s}"], pflag=d[f"pflag_s{s}"], t=float(d[f"t_s{s}"]), dt=float(d[f"dt_s{s}"]),
+                   nstroke=float(d[f"nstroke_s{s}"])) for s in steps}
+    return pr, ref
+
+
+def same(a, b):
+    """Bit-level equality up to the sign of zero (NaN equal to NaN)."""
+    a = np.asarray(a)
+    b = np.asarray(b)
+    return a.shape == b.shape and bool(np.all((a == b) | (np.isnan(a) & np.isnan(b))))

@@ -1,0 +1,38 @@
+"""The CPU restatement (oracle/) reproduces the reference's own outputs bit for
+bit on the golden fixtures generated from the reference build."""
+import numpy as np
+import pytest
+
+from oracle.pyoracle import Oracle
+from tests.fixtures import CASES, load, same
+
+
+@pytest.fixture(scope="module")
+def orc():
+    return Oracle()
+
+
+@pytest.mark.parametrize("name", CASES)
+def test_oracle_matches_reference(orc, name):
+    pr, ref = load(name)
+    done = 0
+    for s in sorted(ref):
+        orc.step(pr, s - done)
+        done = s
+        r = ref[s]
+        assert same(pr.p, r["p"]), f"primitives differ after step {s}"
+        assert np.array_equal(pr.pflag, r["pflag"]), f"pflag map differs after step {s}"
+        assert pr.dt == r["dt"] and pr.t == r["t"]
+
+
+@pytest.mark.parametrize("name", CASES)
+def test_oracle_newton_iterations_match_reference(orc, name):
+    # the reference counts Newton iterations per step in nstroke (main.c:35)
+    pr, ref = load(name)
+    done = 0
+    for s in sorted(ref):
+        if s - done != 1:
+            orc.step(pr, s - done - 1)
+        st = orc.step(pr, 1)
+        done = s
+        assert st.newton_iters == ref[s]["nstroke"]
