@@ -1,0 +1,410 @@
+#!/usr/bin/env python3
+"""Benchmark of the B200 per-zone conservative update (zone-updates/s).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Workload: 3D Fishbone-Moncrief torus around a Kerr hole (a=0.9375, beta=100,
+MKS hslope=0.3, Rout=40) on 256x128x128 zones, FP64, HLL + flux-CT + 2D
+Noble inversion + fixups + boundaries, midpoint RK2.  One step = one full
+time step (both RK substeps) of the whole domain; one zone-update = one
+active zone advanced by one full step.
+
+Our arm:
+  value       zone-updates/s with the state resident in HBM, timed with CUDA
+              events on the library's stream (max over ranks); the state
+              arrays (300 MB each) exceed L2, so no flush is needed.
+  e2e         the same metric through the C ABI with host-owned arrays, as a
+              drop-in step_ch() on reference-owned memory does: every step
+              uploads the primitives from pinned host memory, steps, and
+              downloads primitives and flags (wall clock incl. copies).
+  roofline    dominant kernel: algorithmic bytes per launch / its average
+              CUDA-event duration vs the measured HBM peak, plus its FP64
+              operation rate vs the FP64 peak measured in this run.
+  cpu_baseline  the reference CPU build (oracle/_ref) on a bounded 3D torus
+              sample on the host cores, one process per core.
+Reference arm (--impl reference): the reference CPU build, one process per
+host core on the bounded sample, aggregate zone-updates/s.
+
+Multi-GPU: replicas (each rank advances its own torus; no data-path
+collective), weak scaling; value = all ranks' zone-updates / max time.
+"""
+import argparse
+import json
+import os
+import re
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+WORKLOADS = {
+    # name: (n1, n2, n3, lim, flux)
+    "torus3d_256x128x128": (256, 128, 128, "MC", "HLL"),
+    "torus3d_128x64x32": (128, 64, 32, "MC", "HLL"),
+    "torus2d_64x64": (64, 64, 1, "MC", "HLL"),
+}
+DEFAULT_WORKLOAD = "torus3d_256x128x128"
+# CPU sample for the reference build: same problem, smaller 3D grid
+CPU_SAMPLE = (64, 32, 32, "MC", "HLL")
+
+METRIC = "zone-updates/s FP64 vs mixed on 3D Kerr torus at stated L1; batch p50/p99 latency"
+
+
+def rank_info():
+    r = int(os.environ.get("RANK", "0"))
+    w = int(os.environ.get("WORLD_SIZE", "1"))
+    lr = int(os.environ.get("LOCAL_RANK", "0"))
+    return r, w, lr
+
+
+def pin_device(local_rank, world):
+    """One process per GPU: expose only this rank's GPU to the CUDA runtime."""
+    if world <= 1:
+        return
+    vis = os.environ.get("CUDA_VISIBLE_DEVICES")
+    devs = vis.split(",") if vis else [str(i) for i in range(64)]
+    os.environ["CUDA_VISIBLE_DEVICES"] = devs[local_rank % len(devs)]
+
+
+class ClockSampler:
+    """nvidia-smi clocks/throttle reasons sampled during the timed region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self):
+        self.proc = None
+        self.out = tempfile.NamedTemporaryFile(mode="w+", suffix=".csv", delete=False)
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                                          "-lms", "200"], stdout=self.out, stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.out.flush()
+        self.out.seek(0)
+        rows = [r.split(",") for r in self.out.read().strip().splitlines() if r.strip()]
+        os.unlink(self.out.name)
+        dev = os.environ.get("CUDA_VISIBLE_DEVICES", "0").split(",")[0]
+        rows = [r for r in rows if len(r) >= 9 and r[0].strip() == dev] or [r for r in rows if len(r) >= 9]
+        if not rows:
+            return None
+        sm = [float(r[1]) for r in rows]
+        smax = max(float(r[2]) for r in rows)
+        reasons = set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            for nm, v in zip(names, r[5:9]):
+                if v.strip().lower() == "active":
+                    reasons.add(nm)
+        loaded = [s for s in sm if s > 0.5 * smax] or sm
+        return {"sm_mhz": statistics.median(loaded), "sm_max_mhz": smax, "reasons": sorted(reasons),
+                "samples": len(rows), "power_w_max": max(float(r[3]) for r in rows if r[3].strip()
+                                                           .replace('.', '', 1).isdigit()) if rows else None}
+
+
+def measured_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return json.load(f), "measured"
+    except OSError:
+        return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}, "fallback"
+
+
+def profile_traffic(kernel):
+    """DRAM bytes per launch of `kernel` from the committed ncu summary, if any."""
+    path = os.path.join(ROOT, "profiles", "traffic.md")
+    try:
+        txt = open(path).read()
+    except OSError:
+        return None
+    m = re.search(rf"^\|\s*{re.escape(kernel)}\s*\|\s*([0-9.eE+]+)\s*\|", txt, re.M)
+    return float(m.group(1)) if m else None
+
+
+# ---------------------------------------------------------------------------
+# reference CPU build
+# ---------------------------------------------------------------------------
+def ref_binary(sample):
+    n1, n2, n3, lim, flux = sample
+    return os.path.join(ROOT, "oracle", "_ref", f"harm_ref_{n1}x{n2}x{n3}_{lim}_{flux}")
+
+
+def run_reference(sample, steps, warmup, procs):
+    """Run `procs` independent reference processes; return aggregate zone-updates/s."""
+    exe = ref_binary(sample)
+    if not os.path.exists(exe):
+        return None, f"reference binary {os.path.basename(exe)} not built"
+    n1, n2, n3 = sample[:3]
+    total = warmup + steps
+    with tempfile.TemporaryDirectory() as tmp:
+        ps = []
+        for i in range(procs):
+            wd = os.path.join(tmp, f"r{i}")
+            os.makedirs(wd)
+            ps.append(subprocess.Popen([exe, "-", str(total)], cwd=wd, stdout=subprocess.DEVNULL,
+                                       stderr=subprocess.PIPE, text=True))
+        spans = []
+        for p in ps:
+            _, err = p.communicate()
+            if p.returncode != 0:
+                return None, f"reference run failed rc={p.returncode}"
+            st = {int(a): float(b) for a, b in re.findall(r"harness: step (\d+) start ([0-9.]+)", err)}
+            en = {int(a): float(b) for a, b in re.findall(r"harness: step (\d+) end ([0-9.]+)", err)}
+            spans.append((st[warmup + 1], en[total]))
+    # aggregate throughput of the concurrent processes: sum of per-process rates
+    zu = float(n1 * n2 * n3) * steps
+    return sum(zu / (e - s) for s, e in spans), None
+
+
+def host_cores():
+    try:
+        return len(os.sched_getaffinity(0))
+    except AttributeError:
+        return os.cpu_count() or 1
+
+
+# ---------------------------------------------------------------------------
+# our arm
+# ---------------------------------------------------------------------------
+def bench_ours(args, rank, world):
+    import numpy as np
+
+    from harm_finalwham_b200 import torus
+    from harm_finalwham_b200.gpu import HarmGPU, load_library
+
+    n1, n2, n3, lim, flux = WORKLOADS[args.workload]
+    t_gen = time.time()
+    dom = torus.fm_torus(n1, n2, n3, ng=3, lim=lim, flux=flux, seed=7 + rank)
+    t_gen = time.time() - t_gen
+    L = load_library()
+    g = HarmGPU(n1, n2, n3, dom.ng, dom.dx, lim=lim, flux=flux, precision=args.precision, gam=dom.gam,
+                cour=dom.cour)
+    g.upload_geometry(dom.gcov, dom.gcon, dom.gcovpert, dom.gdet, dom.conn, dom.floors)
+    g.upload_state(dom.p, dom.pflag, 0.0, 0.0)
+    dt0 = g.init_dt()
+
+    dist = None
+    if world > 1:
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(0)
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=300))
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+
+    def allmax(v):
+        if dist is None:
+            return v
+        import torch
+        t = torch.tensor([v], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    # warm-up
+    g.step_ch(args.warmup)
+    barrier()
+    launches0 = L.hgpu_launch_count(g.h)
+    clocks = ClockSampler()
+    clocks.start()
+    ms, st = g.step_ch_timed(args.steps)
+    clk = clocks.stop()
+    launches = L.hgpu_launch_count(g.h) - launches0
+    barrier()
+    ms_max = allmax(ms)
+    zones = n1 * n2 * n3
+    value = zones * args.steps * world / (ms_max / 1e3)
+
+    # per-kernel device times for the roofline (a separate profiled pass)
+    g.set_profiling(True)
+    prof_steps = max(2, min(args.steps, 5))
+    g.step_ch(prof_steps)
+    ktimes = g.kernel_times()
+    g.set_profiling(False)
+
+    # e2e through the C ABI with host-owned arrays
+    e2e = None
+    if not args.no_e2e:
+        p_host, pf_host = g.pinned_state_buffers()
+        p_host[...] = dom.p
+        pf_host[...] = 0
+        t_now, dt_now = g.time()
+        barrier()
+        e2e_steps = max(1, min(args.steps, args.e2e_steps))
+        t0 = time.perf_counter()
+        for _ in range(e2e_steps):
+            g.upload_state(p_host, pf_host, t_now, dt_now)
+            g.step_ch(1)
+            _, _, t_now, dt_now = g.download_state(out=(p_host, pf_host))
+        el = time.perf_counter() - t0
+        el = allmax(el)
+        h2d = p_host.nbytes + pf_host.nbytes
+        d2h = p_host.nbytes + pf_host.nbytes
+        e2e = {"value": zones * e2e_steps * world / el, "unit": "zone-updates/s", "h2d_bytes_per_step": h2d,
+               "d2h_bytes_per_step": d2h, "steps": e2e_steps,
+               "mode": "host-owned arrays: upload p+pflag, step_ch(1), download p+pflag every step"}
+
+    # roofline on the dominant kernel
+    dom_k = max(ktimes, key=lambda k: ktimes[k]["ms"])
+    kt = ktimes[dom_k]
+    avg_s = kt["ms"] / kt["launches"] / 1e3
+    alg = algorithmic_bytes(dom_k, n1, n2, n3)
+    peaks, peaks_kind = measured_peaks()
+    achieved = alg / avg_s / 1e9
+    roof = {"kernel": dom_k, "bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
+            "frac": achieved / peaks["hbm_gbs"], "traffic": profile_traffic(dom_k),
+            "peak_source": f"hbm_gbs ({peaks_kind})", "algorithmic_bytes_per_launch": alg,
+            "avg_launch_ms": avg_s * 1e3,
+            "share": kt["ms"] / sum(v["ms"] for v in ktimes.values())}
+    fp64 = fp64_roof(kt, dom_k, n1, n2, n3, args)
+    if fp64:
+        roof["fp64"] = fp64
+
+    result = {
+        "metric": METRIC, "value": value, "unit": "zone-updates/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64" if args.precision == "fp64" else "f64+f32", "data": "synthetic",
+        "config": {"workload": f"{args.workload}: 3D Fishbone-Moncrief torus a=0.9375 beta=100 MKS, "
+                               f"{lim}+{flux}+flux-CT, 2D Noble inversion, midpoint RK2, {args.precision}",
+                   "zones": zones, "ghosts": dom.ng, "parallelism": f"replicas x{world}" if world > 1 else "single",
+                   "l2": "inputs larger than L2 (300 MB per state array)", "init_dt": dt0,
+                   "newton_iters_per_zone_step": st.newton_iters / (zones * args.steps * 2.0)},
+        "gpu_launches": launches,
+        "roofline": roof,
+        "kernels": {k: {"ms": round(v["ms"], 4), "launches": v["launches"]} for k, v in ktimes.items() if v["launches"]},
+        "e2e": e2e,
+        "clocks": clk,
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        procs = min(host_cores(), args.cpu_procs)
+        v, why = run_reference(CPU_SAMPLE, args.cpu_steps, 2, procs)
+        result["cpu_baseline"] = ({"value": v, "unit": "zone-updates/s", "cores": procs, "kind": "reference",
+                                   "sample": f"reference CPU build (gcc -O2 -ffp-contract=off), 3D torus "
+                                             f"{CPU_SAMPLE[0]}x{CPU_SAMPLE[1]}x{CPU_SAMPLE[2]} {CPU_SAMPLE[3]}+"
+                                             f"{CPU_SAMPLE[4]}, {args.cpu_steps} steps after 2 warm-up, one "
+                                             f"process per core"}
+                                  if v else {"value": None, "unavailable": why})
+    result["gen_seconds"] = t_gen
+    if dist is not None:
+        dist.destroy_process_group()
+    g.close()
+    return result
+
+
+def algorithmic_bytes(kernel, n1, n2, n3):
+    """Compulsory HBM bytes per launch (FP64, state resident; per-(i,j) metric
+    amortised over x3).  Units: faces for the flux kernels, zones otherwise."""
+    zones = n1 * n2 * n3
+    faces = {"flux_x1": (n1 + 1) * (n2 + 2) * (n3 + 2), "flux_x2": (n1 + 2) * (n2 + 1) * (n3 + 2),
+             "flux_x3": (n1 + 2) * (n2 + 2) * (n3 + 1)}
+    if kernel in faces:
+        return faces[kernel] * (64 + 64)          # read one zone's 8 primitives, write 8 face fluxes
+    if kernel == "update":
+        # mean of the two substeps: p(64) [+pk 64] + 5 F comps x3 dirs (120) + 3 EMFs (24)
+        # + uf/ucum write (128) [+read 128] + pf (64) + pflag (4)
+        return zones * (468 + 596) / 2.0
+    if kernel == "emf":
+        return zones * (6 * 8 + 3 * 8)
+    if kernel == "bound_ghost":
+        return zones * 0.0 + (2 * 3 * 8 * 8) * ((n2 + 6) * (n3 + 6) + (n1 + 6) * (n3 + 6) + (n1 + 6) * (n2 + 6))
+    return zones * 8.0
+
+
+def fp64_roof(kt, kernel, n1, n2, n3, args):
+    """FP64 rate of the dominant kernel from the per-unit FP64 operation count
+    measured with ncu (profiles/traffic.md) vs the FP64 peak measured here."""
+    path = os.path.join(ROOT, "profiles", "traffic.md")
+    try:
+        txt = open(path).read()
+    except OSError:
+        return None
+    m = re.search(rf"^\|\s*{re.escape(kernel)}\s*\|\s*[0-9.eE+]+\s*\|\s*([0-9.eE+]+)\s*\|", txt, re.M)
+    if not m:
+        return None
+    ops_per_launch = float(m.group(1))
+    avg_s = kt["ms"] / kt["launches"] / 1e3
+    achieved = ops_per_launch / avg_s / 1e12
+    peak = measure_fp64_peak()
+    return {"achieved_tflops": achieved, "peak_tflops": peak, "frac": achieved / peak if peak else None,
+            "note": "FP64 DADD+DMUL+2*DFMA per launch from ncu; peak = measured DADD/DMUL issue rate (no FMA: "
+                    "the FP64 path is built with -fmad=false for bit-identity)"}
+
+
+_FP64_PEAK = None
+
+
+def measure_fp64_peak():
+    global _FP64_PEAK
+    if _FP64_PEAK is None:
+        from harm_finalwham_b200.gpu import fp64_peak_tflops
+        _FP64_PEAK = fp64_peak_tflops()
+    return _FP64_PEAK
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default=DEFAULT_WORKLOAD, choices=sorted(WORKLOADS))
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--e2e-steps", type=int, default=5)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-steps", type=int, default=3)
+    ap.add_argument("--cpu-procs", type=int, default=16)
+    args = ap.parse_args()
+    rank, world, local = rank_info()
+    if args.warmup < 3:
+        args.warmup = 3
+
+    if args.impl == "reference":
+        if rank != 0:
+            return 0
+        procs = min(host_cores(), args.cpu_procs)
+        # each step: one step of every process's bounded sample
+        v, why = run_reference(CPU_SAMPLE, args.steps, args.warmup, procs)
+        if v is None:
+            print(json.dumps({"impl": "reference", "unavailable": why}))
+            return 0
+        n1, n2, n3 = CPU_SAMPLE[:3]
+        sample = (f"reference CPU build (its own C sources, gcc -O2 -ffp-contract=off): 3D torus {n1}x{n2}x{n3} "
+                  f"{CPU_SAMPLE[3]}+{CPU_SAMPLE[4]} per process, {procs} processes (the code is single-threaded "
+                  f"and non-reentrant), {args.steps} timed steps after {args.warmup}")
+        out = {"impl": "reference", "metric": METRIC, "value": v, "unit": "zone-updates/s", "n_gpus": args.gpus,
+               "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
+               "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+               "config": {"workload": f"{args.workload} (CPU sample {n1}x{n2}x{n3} per core)"},
+               "cpu_baseline": {"value": v, "unit": "zone-updates/s", "cores": procs, "kind": "reference",
+                                "sample": sample},
+               "e2e": {"value": v, "unit": "zone-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+        print(json.dumps(out))
+        return 0
+
+    pin_device(local, world)
+    res = bench_ours(args, rank, world)
+    if rank == 0:
+        print(json.dumps(res))
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1543,6 +1543,49 @@ int hgpu_kernel_times(hgpu_ctx *x, const char **names, double *ms, long long *la
 
 long long hgpu_launch_count(hgpu_ctx *x) { return x ? x->launches : -1; }
 
+// 8 independent multiply/add chains per thread; -fmad=false keeps DMUL and
+// DADD separate (the instruction mix of the FP64 path)
+__global__ void fp64_probe_kernel(double *out, int iters, double b, double c) {
+  double a0 = threadIdx.x * 1e-9, a1 = a0 + 1e-3, a2 = a0 + 2e-3, a3 = a0 + 3e-3;
+  double a4 = a0 + 4e-3, a5 = a0 + 5e-3, a6 = a0 + 6e-3, a7 = a0 + 7e-3;
+  for (int it = 0; it < iters; it++) {
+    a0 = a0 * b + c; a1 = a1 * b + c; a2 = a2 * b + c; a3 = a3 * b + c;
+    a4 = a4 * b + c; a5 = a5 * b + c; a6 = a6 * b + c; a7 = a7 * b + c;
+  }
+  double s = a0 + a1 + a2 + a3 + a4 + a5 + a6 + a7;
+  if (s == 12345.678) out[blockIdx.x] = s;  // keeps the chains alive
+}
+
+int hgpu_fp64_peak(double *tflops) {
+  if (!tflops) return HGPU_E_INVALID;
+  int dev = 0, sms = 0;
+  CUDA_TRY(cudaGetDevice(&dev));
+  CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+  double *out = nullptr;
+  CUDA_TRY(cudaMalloc(&out, sizeof(double) * sms * 8));
+  const int iters = 4096, blocks = sms * 8, threads = 256;
+  cudaEvent_t a, b;
+  cudaEventCreate(&a);
+  cudaEventCreate(&b);
+  fp64_probe_kernel<<<blocks, threads>>>(out, 64, 0.999999, 1e-7);  // warm-up
+  cudaEventRecord(a);
+  fp64_probe_kernel<<<blocks, threads>>>(out, iters, 0.999999, 1e-7);
+  cudaEventRecord(b);
+  cudaError_t e = cudaEventSynchronize(b);
+  float ms = 0.f;
+  cudaEventElapsedTime(&ms, a, b);
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  cudaFree(out);
+  if (e != cudaSuccess) {
+    set_err("fp64 probe: %s", cudaGetErrorString(e));
+    return HGPU_E_CUDA;
+  }
+  double ops = 2.0 * 8.0 * (double)iters * (double)blocks * (double)threads;
+  *tflops = ops / (ms * 1e-3) / 1e12;
+  return HGPU_OK;
+}
+
 int hgpu_alloc_pinned(size_t bytes, void **ptr) {
   if (!ptr) return HGPU_E_INVALID;
   CUDA_TRY(cudaHostAlloc(ptr, bytes, cudaHostAllocDefault));

@@ -75,6 +75,18 @@ def load_library(path=None):
                                      ctypes.c_double, _P(ctypes.c_longlong)]
     L.hgpu_device_prims.argtypes = [ctypes.c_void_p, ctypes.c_int, _P(ctypes.c_void_p)]
     L.hgpu_sync.argtypes = [ctypes.c_void_p]
+    L.hgpu_init_dt.argtypes = [ctypes.c_void_p, _dp]
+    L.hgpu_step_ch_timed.argtypes = [ctypes.c_void_p, ctypes.c_int, _P(ctypes.c_float), _P(hgpu_stats)]
+    L.hgpu_set_profiling.argtypes = [ctypes.c_void_p, ctypes.c_int]
+    L.hgpu_kernel_times.argtypes = [ctypes.c_void_p, _P(ctypes.c_char_p), _dp, _P(ctypes.c_longlong), ctypes.c_int]
+    L.hgpu_launch_count.argtypes = [ctypes.c_void_p]
+    L.hgpu_launch_count.restype = ctypes.c_longlong
+    L.hgpu_alloc_pinned.argtypes = [ctypes.c_size_t, _P(ctypes.c_void_p)]
+    L.hgpu_free_pinned.argtypes = [ctypes.c_void_p]
+    L.hgpu_fp64_peak.argtypes = [_dp]
+    for name in ("hgpu_init_dt", "hgpu_step_ch_timed", "hgpu_set_profiling", "hgpu_kernel_times", "hgpu_alloc_pinned",
+                 "hgpu_free_pinned", "hgpu_fp64_peak"):
+        getattr(L, name).restype = ctypes.c_int
     for name in ("hgpu_create", "hgpu_upload_geometry", "hgpu_upload_state", "hgpu_download_state", "hgpu_step_ch",
                  "hgpu_advance_stage", "hgpu_fluxcalc", "hgpu_bound_prim", "hgpu_utoprim_batch",
                  "hgpu_device_prims", "hgpu_sync"):
@@ -147,6 +159,9 @@ class HarmGPU:
         if getattr(self, "h", None):
             self.L.hgpu_destroy(self.h)
             self.h = None
+        for ptr in getattr(self, "_pinned", []):
+            self.L.hgpu_free_pinned(ptr)
+        self._pinned = []
 
     def __del__(self):
         try:
@@ -176,9 +191,12 @@ class HarmGPU:
         pf = None if pflag is None else _contig(pflag, np.int32)
         _check(self.L, self.L.hgpu_upload_state(self.h, _ptr(p), _ptr(pf, ctypes.c_int), float(t), float(dt)))
 
-    def download_state(self):
-        p = np.empty(self.nt + (NPR,))
-        pf = np.empty(self.nt, dtype=np.int32)
+    def download_state(self, out=None):
+        if out is None:
+            p = np.empty(self.nt + (NPR,))
+            pf = np.empty(self.nt, dtype=np.int32)
+        else:
+            p, pf = out
         t = ctypes.c_double()
         dt = ctypes.c_double()
         _check(self.L, self.L.hgpu_download_state(self.h, _ptr(p), _ptr(pf, ctypes.c_int), ctypes.byref(t),
@@ -202,6 +220,51 @@ class HarmGPU:
         _check(self.L, self.L.hgpu_fluxcalc(self.h, int(which), _ptr(F[0]), _ptr(F[1]), _ptr(F[2]),
                                             *[ctypes.byref(x) for x in nd]))
         return F, [x.value for x in nd]
+
+    def init_dt(self):
+        dt = ctypes.c_double()
+        _check(self.L, self.L.hgpu_init_dt(self.h, ctypes.byref(dt)))
+        return dt.value
+
+    def time(self):
+        t = ctypes.c_double()
+        dt = ctypes.c_double()
+        _check(self.L, self.L.hgpu_download_state(self.h, None, None, ctypes.byref(t), ctypes.byref(dt)))
+        return t.value, dt.value
+
+    def step_ch_timed(self, nsteps):
+        st = hgpu_stats()
+        ms = ctypes.c_float()
+        _check(self.L, self.L.hgpu_step_ch_timed(self.h, int(nsteps), ctypes.byref(ms), ctypes.byref(st)))
+        return ms.value, st
+
+    def set_profiling(self, on):
+        _check(self.L, self.L.hgpu_set_profiling(self.h, 1 if on else 0))
+
+    def kernel_times(self):
+        n = 32
+        names = (ctypes.c_char_p * n)()
+        ms = (ctypes.c_double * n)()
+        cnt = (ctypes.c_longlong * n)()
+        k = self.L.hgpu_kernel_times(self.h, names, ms, cnt, n)
+        if k < 0:
+            raise HarmGPUError(-k, self.L.hgpu_last_error().decode(errors="replace"))
+        return {names[i].decode(): {"ms": ms[i], "launches": cnt[i]} for i in range(k)}
+
+    def launch_count(self):
+        return self.L.hgpu_launch_count(self.h)
+
+    def pinned_state_buffers(self):
+        """Primitive and flag arrays in page-locked host memory (owned by this object)."""
+        nz = int(np.prod(self.nt))
+        bufs = []
+        for nbytes, dtype, shape in ((nz * NPR * 8, np.float64, self.nt + (NPR,)), (nz * 4, np.int32, self.nt)):
+            ptr = ctypes.c_void_p()
+            _check(self.L, self.L.hgpu_alloc_pinned(nbytes, ctypes.byref(ptr)))
+            self._pinned = getattr(self, "_pinned", []) + [ptr]
+            arr = np.ctypeslib.as_array(ctypes.cast(ptr, ctypes.POINTER(ctypes.c_byte)), shape=(nbytes,))
+            bufs.append(arr.view(dtype).reshape(shape))
+        return bufs[0], bufs[1]
 
     def bound_prim(self, which=0):
         _check(self.L, self.L.hgpu_bound_prim(self.h, int(which)))
@@ -228,3 +291,11 @@ def utoprim_batch(U, gcov, gcon, gdet, guess, gam, gammafail):
     _check(L, L.hgpu_utoprim_batch(_ptr(U), _ptr(gcov), _ptr(gcon), _ptr(gdet), _ptr(pr), _ptr(pflag, ctypes.c_int),
                                    n, gam, gammafail, ctypes.byref(it)))
     return pr, pflag, it.value
+
+
+def fp64_peak_tflops():
+    """Measured FP64 DMUL/DADD issue rate of the current GPU (hgpu_fp64_peak)."""
+    L = load_library()
+    v = ctypes.c_double()
+    _check(L, L.hgpu_fp64_peak(ctypes.byref(v)))
+    return v.value

@@ -153,6 +153,11 @@ long long hgpu_launch_count(hgpu_ctx *ctx);
 int hgpu_alloc_pinned(size_t bytes, void **ptr);
 int hgpu_free_pinned(void *ptr);
 
+/* FP64 issue-rate probe of the current device: separate DMUL and DADD
+   (no FMA), the instruction mix of the bit-identical FP64 path.  Returns the
+   measured rate in TFLOP/s (one multiply or add = one flop). */
+int hgpu_fp64_peak(double *tflops);
+
 /* Synchronise the context's stream and report pending CUDA errors. */
 int hgpu_sync(hgpu_ctx *ctx);
 

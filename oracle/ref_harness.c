@@ -10,12 +10,15 @@
  * reference's own arrays to raw binary files so that the CPU restatement
  * (oracle/harm_oracle.c) and the CUDA path can be pinned against them.
  *
- * usage: harm_ref <outdir> <nsteps> [dumpstep ...]
+ * usage: harm_ref <outdir|-> <nsteps> [dumpstep ...]
  *   writes <outdir>/init_*  (geometry, floors, initial primitives/flags, meta)
  *          <outdir>/s<step>_* after each listed step (and always after nsteps)
+ *   and prints the CLOCK_MONOTONIC start/end of every step to stderr (the
+ *   CPU baseline's step-loop timing).  "-" as outdir writes no files.
  */
 #include "defs.h"  /* defines the reference globals, as the reference main.c does */
 #include <sys/stat.h>
+#include <time.h>
 
 extern int init(int argc, char *argv[]);
 extern int step_ch(void);
@@ -111,15 +114,17 @@ static void dump_geometry(void)
 int main(int argc, char *argv[])
 {
   char *fakeargv[2];
-  int nsteps, s, d, ndump = 0;
+  int nsteps, s, d, ndump = 0, nodump = 0;
   int dumps[64];
 
   if (argc < 3) {
-    fprintf(stderr, "usage: %s <outdir> <nsteps> [dumpstep ...]\n", argv[0]);
+    fprintf(stderr, "usage: %s <outdir|-> <nsteps> [dumpstep ...]\n", argv[0]);
     return 2;
   }
+  /* outdir "-" runs the steps for timing only and writes nothing */
+  nodump = (strcmp(argv[1], "-") == 0);
   snprintf(outdir, sizeof(outdir), "%s", argv[1]);
-  mkdir(outdir, 0755);
+  if (!nodump) mkdir(outdir, 0755);
   nsteps = atoi(argv[2]);
   for (d = 3; d < argc && ndump < 64; d++) dumps[ndump++] = atoi(argv[d]);
 
@@ -129,16 +134,23 @@ int main(int argc, char *argv[])
     fprintf(stderr, "harness: init failed\n");
     return 1;
   }
-  dump_geometry();
-  dump_state("init", 0);
+  if (!nodump) {
+    dump_geometry();
+    dump_state("init", 0);
+  }
 
   for (s = 1; s <= nsteps; s++) {
     char tag[64];
-    int want = (s == nsteps);
+    int want = (s == nsteps) && !nodump;
+    struct timespec ts;
     nstroke = 0;
+    clock_gettime(CLOCK_MONOTONIC, &ts);
+    fprintf(stderr, "harness: step %d start %.9f\n", s, ts.tv_sec + 1e-9 * ts.tv_nsec);
     if (step_ch() != 0) { fprintf(stderr, "harness: step_ch failed at step %d\n", s); return 1; }
     if (error_check(2)) { fprintf(stderr, "harness: error_check failed at step %d\n", s); return 1; }
     nstep++;
+    clock_gettime(CLOCK_MONOTONIC, &ts);
+    fprintf(stderr, "harness: step %d end %.9f\n", s, ts.tv_sec + 1e-9 * ts.tv_nsec);
     for (d = 0; d < ndump; d++) if (dumps[d] == s) want = 1;
     if (want) {
       snprintf(tag, sizeof(tag), "s%d", s);
