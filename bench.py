@@ -45,6 +45,7 @@ sys.path.insert(0, ROOT)
 WORKLOADS = {
     # name: (n1, n2, n3, lim, flux)
     "torus3d_256x128x128": (256, 128, 128, "MC", "HLL"),
+    "torus3d_256x128x64": (256, 128, 64, "MC", "HLL"),
     "torus3d_128x64x32": (128, 64, 32, "MC", "HLL"),
     "torus2d_64x64": (64, 64, 1, "MC", "HLL"),
 }
@@ -231,6 +232,10 @@ def bench_ours(args, rank, world):
     ms_max = allmax(ms)
     zones = n1 * n2 * n3
     value = zones * args.steps * world / (ms_max / 1e3)
+    if args.kernels_only:
+        g.close()
+        return {"metric": METRIC, "value": value, "unit": "zone-updates/s", "note": "kernels-only run",
+                "ms_per_step": ms_max / args.steps, "gpu_launches": launches}
 
     # per-kernel device times for the roofline (a separate profiled pass)
     g.set_profiling(True)
@@ -371,6 +376,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-steps", type=int, default=3)
     ap.add_argument("--cpu-procs", type=int, default=16)
+    ap.add_argument("--kernels-only", action="store_true",
+                    help="set-up, warm-up and the timed steps only (for profiler runs)")
     args = ap.parse_args()
     rank, world, local = rank_info()
     if args.warmup < 3:
