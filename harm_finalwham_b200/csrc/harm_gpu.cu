@@ -27,6 +27,7 @@
 #include <stdlib.h>
 #include <string.h>
 
+#include <mutex>
 #include <new>
 #include <vector>
 
@@ -1598,3 +1599,90 @@ int hgpu_free_pinned(void *ptr) {
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// hgpu_utoprim_batch_noalloc: the batched inversion with its device scratch in
+// a fixed file-scope array instead of cudaMalloc'd buffers.
+// ---------------------------------------------------------------------------
+namespace {
+
+// per zone: U 8, gcov 16, gcon 16, gdet 1, pr 8 doubles; then pflag ints and
+// the iteration counter
+constexpr long long NA_DOUBLES_PER_ZONE = 8 + 16 + 16 + 1 + 8;
+constexpr long long NA_MAX = HGPU_NOALLOC_MAX_ZONES;
+constexpr size_t NA_BYTES = sizeof(double) * NA_DOUBLES_PER_ZONE * NA_MAX + sizeof(int) * NA_MAX + 256;
+
+static __device__ __align__(256) unsigned char g_noalloc_scratch[NA_BYTES];
+
+constexpr int NA_MAX_DEVICES = 64;
+std::mutex g_na_mutex;
+unsigned char *g_na_addr[NA_MAX_DEVICES] = {nullptr};
+
+// device address of the scratch array on the current device (looked up once
+// per device; the host-side symbol is only a handle, never a device pointer)
+int noalloc_scratch_address(unsigned char **out) {
+  int dev = 0;
+  CUDA_TRY(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= NA_MAX_DEVICES) {
+    set_err("device index %s%d out of range", "", dev);
+    return HGPU_E_INVALID;
+  }
+  std::lock_guard<std::mutex> lock(g_na_mutex);
+  if (!g_na_addr[dev]) {
+    void *ptr = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&ptr, g_noalloc_scratch);
+    if (e != cudaSuccess || !ptr) {
+      set_err("cudaGetSymbolAddress: %s", cudaGetErrorString(e));
+      return HGPU_E_CUDA;
+    }
+    g_na_addr[dev] = (unsigned char *)ptr;
+  }
+  *out = g_na_addr[dev];
+  return HGPU_OK;
+}
+
+}  // namespace
+
+extern "C" int hgpu_utoprim_batch_noalloc(const double *U, const double *gcov, const double *gcon, const double *gdet,
+                                          double *pr, int *pflag, long long n, double gam, double gammafail,
+                                          long long *iters) {
+  if (n < 0 || (n > 0 && (!U || !gcov || !gcon || !gdet || !pr || !pflag))) {
+    set_err("invalid arguments");
+    return HGPU_E_INVALID;
+  }
+  if (n > NA_MAX) {
+    snprintf(g_errbuf, sizeof(g_errbuf), "batch of %lld zones exceeds HGPU_NOALLOC_MAX_ZONES=%lld; split the batch",
+             n, (long long)NA_MAX);
+    return HGPU_E_INVALID;
+  }
+  if (n == 0) {
+    if (iters) *iters = 0;
+    return HGPU_OK;
+  }
+  unsigned char *base = nullptr;
+  int rc = noalloc_scratch_address(&base);
+  if (rc) return rc;
+  double *dU = (double *)base;
+  double *dgcov = dU + 8 * NA_MAX;
+  double *dgcon = dgcov + 16 * NA_MAX;
+  double *dg = dgcon + 16 * NA_MAX;
+  double *dpr = dg + NA_MAX;
+  int *dpf = (int *)(dpr + 8 * NA_MAX);
+  unsigned long long *dit = (unsigned long long *)(((uintptr_t)(dpf + NA_MAX) + 255) & ~(uintptr_t)255);
+  CUDA_TRY(cudaMemcpy(dU, U, sizeof(double) * 8 * n, cudaMemcpyHostToDevice));
+  CUDA_TRY(cudaMemcpy(dgcov, gcov, sizeof(double) * 16 * n, cudaMemcpyHostToDevice));
+  CUDA_TRY(cudaMemcpy(dgcon, gcon, sizeof(double) * 16 * n, cudaMemcpyHostToDevice));
+  CUDA_TRY(cudaMemcpy(dg, gdet, sizeof(double) * n, cudaMemcpyHostToDevice));
+  CUDA_TRY(cudaMemcpy(dpr, pr, sizeof(double) * 8 * n, cudaMemcpyHostToDevice));
+  // the counter keeps the previous call's value: clear it
+  CUDA_TRY(cudaMemset(dit, 0, sizeof(unsigned long long)));
+  utoprim_batch_kernel<<<grid_for(n, 128), 128>>>(dU, dgcov, dgcon, dg, dpr, dpf, n, gam, gammafail, dit);
+  CUDA_TRY(cudaGetLastError());
+  CUDA_TRY(cudaDeviceSynchronize());
+  unsigned long long it = 0;
+  CUDA_TRY(cudaMemcpy(pr, dpr, sizeof(double) * 8 * n, cudaMemcpyDeviceToHost));
+  CUDA_TRY(cudaMemcpy(pflag, dpf, sizeof(int) * n, cudaMemcpyDeviceToHost));
+  CUDA_TRY(cudaMemcpy(&it, dit, sizeof(it), cudaMemcpyDeviceToHost));
+  if (iters) *iters = (long long)it;
+  return HGPU_OK;
+}

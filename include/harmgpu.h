@@ -125,6 +125,24 @@ int hgpu_bound_prim(hgpu_ctx *ctx, int which);
 int hgpu_utoprim_batch(const double *U, const double *gcov, const double *gcon, const double *gdet, double *pr,
                        int *pflag, long long n, double gam, double gammafail, long long *iters);
 
+/* Utoprimgen batch that allocates nothing (no counterpart in the reference).
+   Same arguments and results as hgpu_utoprim_batch, for callers that cannot
+   call cudaMalloc/cudaFree: a process whose device memory is already held by
+   another allocator's pool (cudaMalloc would fail), or a host loop that calls
+   the inversion often on small batches -- as the reference calls Utoprimgen
+   zone by zone -- where cudaFree's implicit device synchronisation and
+   per-call allocation would dominate.  Device scratch is a fixed file-scope
+   array in the library: at most HGPU_NOALLOC_MAX_ZONES zones per call (larger
+   n is rejected with HGPU_E_INVALID and a message), held by every GPU that
+   loads the library until the process exits.  The first call on a device
+   looks up the array's device address (cudaGetSymbolAddress) with that device
+   current; make that first call before any stream capture.  All calls share
+   the array and each call overwrites it, so calls that overlap on the GPU
+   (other host threads, other streams) race: serialise them. */
+#define HGPU_NOALLOC_MAX_ZONES 16384
+int hgpu_utoprim_batch_noalloc(const double *U, const double *gcov, const double *gcon, const double *gdet,
+                               double *pr, int *pflag, long long n, double gam, double gammafail, long long *iters);
+
 /* Raw device pointers of the resident state for callers that keep data on
    the GPU (e.g. a graph-captured serving loop): primitive planes
    [8][nt1][nt2][nt3] of p (which=0) or pk (which=1). */
