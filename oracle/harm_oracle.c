@@ -41,6 +41,7 @@
  * host (set_grid.c:7-151, fixup.c:1542-1654) and they carry no per-step work.
  * The metric is stored per (i,j): it does not depend on x3.
  */
+#include <float.h>
 #include <math.h>
 #include <stdint.h>
 #include <stdlib.h>
@@ -93,6 +94,7 @@
 
 #define NUMEPSILON (2.2204460492503131e-16)
 #define BIG (1.e+50)
+#define SMALL (1.e-50) /* global.h:1041 */
 
 /* u2p_defs.h (PRECISEINVERSION=1, NEWCONVERGE=1, OPTIMIZED=1) */
 #define MAX_NEWT_ITER 200
@@ -480,6 +482,314 @@ static double slope3(int lim, double yl, double yc, double yr)
   return 0.0; /* DONOR */
 }
 
+/* ------------------------------------------------------------------ */
+/* WENO5 centre-to-edge line reconstruction (lim = WENO5)              */
+/*                                                                     */
+/* slope_lim_linetype_c2e (interpline.c:517-678) with the options of   */
+/* the torus build: VARTOINTERP=PRIMTOINTERP, COMPUTEDRHODP=1, SMONO   */
+/* (DOMONOINTERP=SMONOINTERP, SMONO_DO_SMOOTH_TRANSITION=1), stencil   */
+/* reduction "AND" (DO_OR_STENCIL_REDUCTION=0), post/pre-shock dP/P    */
+/* reduction, DO_SMOOTH_ADJUSTMENT_UNOPTIMIZED_WEIGHTS=1, no stencil   */
+/* shift (STOREWAVESPEEDS=0), WENO_REDUCE_TYPE_DEFAULT.  The shock     */
+/* indicator (get_shock_indicator, interpline.c:2025) is computed by   */
+/* the reference but only read by the PPM-type reduction, so it has no */
+/* effect here and is not computed.                                    */
+/*                                                                     */
+/* One output cell c reads the line from c-5 to c+5: unoptimised       */
+/* weights and SMONO indicators at c-3..c+3 (each from c-2..c+2 of the */
+/* line), weight ratios at c-1..c+1, dP/P at c (from c-1..c+1).  The   */
+/* reference feeds the whole line including MAXBND ghosts; with its    */
+/* default MAXBND=11 no stencil of an output cell -1..N reaches the    */
+/* ends of the line, so every boundary-truncation branch of            */
+/* compute_cf_stencil_weights / compute_weights_ratios is dead and     */
+/* only ghost cells up to depth 6 are read.                            */
+/* ------------------------------------------------------------------ */
+
+#define WENO_EPS 1.e-26     /* WENO_EPSILON = REDUCEEPSILON (reconstructeno.h:195-200) */
+#define SMONO_EPS 1.e-13    /* SMONO_EPSILON = SQRT_WENO_EPSILON (reconstructeno.h:73,196) */
+#define W_MIN_RAT 1.3       /* MIN_TRANSITION_RATIO, AND reduction (reconstructeno.h:175-176) */
+#define W_MAX_RAT 1.6
+#define W_DP_FRAC (0.5)     /* REDUCE_DP_FRACTION (reconstructeno.h:96) */
+#define W_BIG (1.e+50)      /* BIG (global.h:1040) */
+#define W_MIN(a, b) (((a) < (b)) ? (a) : (b)) /* global.h:750-751 */
+#define W_MAX(a, b) (((a) > (b)) ? (a) : (b))
+
+/* sign (phys.c:1778-1783) */
+static inline double w_sign(double a) { return (a > 0.0) ? 1.0 : ((a < 0.0) ? -1.0 : 0.0); }
+
+/* get_sum_of_elements with SYMMETRIZE_WENO (reconstructeno.c:1920-1946):
+   pairs a[i] with a[n-1-i], then adds the middle element times (n odd) */
+static double w_sum(int n, const double *a)
+{
+  double s = 0.0;
+  int i, h = n / 2;
+  for (i = 0; i < h; i++) s += a[i] + a[n - 1 - i];
+  s += a[i] * (double)(n % 2);
+  return s;
+}
+
+/* normalize_array (reconstructeno.c:1948-1960) */
+static double w_normalize(int n, double eps, double *a)
+{
+  double s = w_sum(n, a);
+  int i;
+  for (i = 0; i < n; i++) a[i] /= (s + eps);
+  return s;
+}
+
+/* check_for_cusp_new (smonointerp.c:439-476) at line cell y[0] */
+static int w_cusp(const double *y)
+{
+  double df[4], ddf[3], norm, f1a, f1, f2, f3, f3a, f4, f4a, f5a, f5, f6, f7, f7a, f8, f8a;
+  double *dfp = df + 1, *ddfp = ddf + 1;
+  int k;
+  for (k = -1; k <= 2; k++) dfp[k] = y[k] - y[k - 1];
+  for (k = -1; k <= 1; k++) ddfp[k] = dfp[k + 1] - dfp[k];
+  norm = (fabs(y[-2]) + fabs(y[-1]) + fabs(y[0]) + fabs(y[1]) + fabs(y[2]) + SMALL);
+  norm = norm * SMONO_EPS;
+  f1a = fabs(dfp[0]) - norm;
+  f1 = ddfp[-1] * w_sign(dfp[0]) - norm;
+  f2 = -ddfp[0] * w_sign(dfp[0]) - norm;
+  f3 = -dfp[2] * w_sign(dfp[0]) - norm;
+  f3a = fabs(-dfp[2] - dfp[0]) - 0.25 * (fabs(dfp[2]) + fabs(dfp[0]));
+  f4 = -dfp[1] * w_sign(dfp[0]) - norm;
+  f4a = fabs(-dfp[1] - dfp[0]) - 0.25 * (fabs(dfp[1]) + fabs(dfp[0]));
+  if (f1a > 0 && f1 > 0 && f2 > 0 && ((f3 > 0 && f3a > 0) || (f4 > 0 && f4a > 0))) return 1;
+  f5a = fabs(dfp[1]) - norm;
+  f5 = -ddfp[1] * w_sign(dfp[1]) - norm;
+  f6 = ddfp[0] * w_sign(dfp[1]) - norm;
+  f7 = -dfp[-1] * w_sign(dfp[1]) - norm;
+  f7a = fabs(-dfp[-1] - dfp[1]) - 0.25 * (fabs(dfp[-1]) + fabs(dfp[1]));
+  f8 = -dfp[0] * w_sign(dfp[1]) - norm;
+  f8a = fabs(-dfp[0] - dfp[1]) - 0.25 * (fabs(dfp[0]) + fabs(dfp[1]));
+  if (f5a > 0 && f5 > 0 && f6 > 0 && ((f7 > 0 && f7a > 0) || (f8 > 0 && f8a > 0))) return 1;
+  return 0;
+}
+
+/* compute_mono_indicator_point_eno5 (smonointerp.c:296-425) with
+   DO_MONO_1ST_DERIVATIVE=1, DO_3RD_DER=1, and transition_function
+   (smonointerp.c:428-437): derivatives of the 5-point polynomial at -1 and +1 */
+static double w_mono(const double *y)
+{
+  double ld[4], rd[4], mm, minabs = W_BIG, norm, cut, v;
+  int n;
+  ld[1] = (((-3 * y[-2] + y[2]) + (-10 * y[-1] - 6 * y[1])) + 18 * y[0]) / 12.;
+  ld[2] = (((11 * y[-2] - y[2]) + (-20 * y[-1] + 4 * y[1])) + 6 * y[0]) / 12.;
+  ld[3] = (((-3 * y[-2] - y[2]) + (10 * y[-1] + 6 * y[1])) - 12 * y[0]) / 2.;
+  rd[1] = (((-y[-2] + 3 * y[2]) + (6 * y[-1] + 10 * y[1])) - 18 * y[0]) / 12.;
+  rd[2] = (((-y[-2] + 11 * y[2]) + (4 * y[-1] - 20 * y[1])) + 6 * y[0]) / 12.;
+  rd[3] = (((y[-2] + 3 * y[2]) - (6 * y[-1] + 10 * y[1])) + 12 * y[0]) / 2.;
+  ld[1] = MINMOD(ld[1], y[-1] - y[-2]);
+  rd[1] = MINMOD(rd[1], y[2] - y[1]);
+  for (n = 1; n <= 3; n++) {
+    mm = MINMOD(ld[n], rd[n]);
+    minabs = W_MIN(minabs, fabs(mm));
+  }
+  norm = fabs(y[0]) + ((fabs(y[-1]) + fabs(y[1])) + (fabs(y[-2]) + fabs(y[2])));
+  cut = norm * SMONO_EPS + DBL_MIN;
+  v = (minabs - 0.0) / (cut - 0.0);
+  return W_MAX(0., W_MIN(1., v));
+}
+
+/* c2e_simple_eno(5, ...) (reconstructeno.c:826-901): the central row of the
+   5-point centre-to-left / centre-to-right Lagrange matrices */
+static double w_eno5(int right, const double *y)
+{
+  static const double cl[5] = {-5. / 128., 15. / 32., 45. / 64., -5. / 32., 3. / 128.};
+  static const double cr[5] = {3. / 128., -5. / 32., 45. / 64., 15. / 32., -5. / 128.};
+  const double *c = right ? cr : cl;
+  double d[5];
+  int k;
+  for (k = 0; k < 5; k++) d[k] = c[k] * y[k - 2];
+  return w_sum(5, d);
+}
+
+/* WENO weight set of one cell: weights[0..order-1] unoptimised,
+   [order..2order-1] left-face, [2order..3order-1] right-face optimised
+   (weno_weights_s, reconstructeno.h:146-160) */
+typedef struct {
+  double w[9];
+  int order;
+  double lof, fordpp;
+} wset;
+
+/* optimal centre-to-face weights c2e_optimal_weights_{left,right}face
+   (reconstructeno_static.h) for order 2 and 3 */
+static const double w_optl[2][3] = {{1. / 4., 3. / 4, 0.0}, {1. / 16., 5. / 8., 5. / 16.}};
+static const double w_optr[2][3] = {{3. / 4., 1. / 4., 0.0}, {5. / 16., 5. / 8., 1. / 16.}};
+
+/* compute_cf_stencil_weights (reconstructeno.c:1406-1614) for order 2 or 3
+   on a long line, followed for order 3 by mono_adjust_unoptimized_weights
+   (reconstructeno.c:702-728); m0 = monoindicator[0], cusp = (m0 == 0 and
+   monoindicator[1] != 0) */
+static void w_unopt(int order, double m0, int cusp, const double *u, wset *s)
+{
+  double si[3], fd[3], sd[3], u2[5], normu, e;
+  int sh, i;
+  s->lof = 0.;
+  s->order = order;
+  if (m0 == 1) {
+    for (i = 0; i < order; i++) s->w[i] = 1.0 / order;
+    return;
+  } else if (m0 == 0 && cusp) {
+    s->lof = 1.0;
+  }
+  if (order == 2) {
+    fd[0] = u[1] - u[0];
+    fd[1] = u[0] - u[-1];
+    for (sh = 0; sh < 2; sh++) si[sh] = fd[sh] * fd[sh];
+  } else {
+    fd[0] = -(3 * u[0] + u[2]) + 4 * u[1];
+    fd[1] = u[1] - u[-1];
+    fd[2] = (3 * u[0] + u[-2]) - 4 * u[-1];
+    sd[0] = (u[0] + u[2]) - 2 * u[1];
+    sd[1] = (u[-1] + u[1]) - 2 * u[0];
+    sd[2] = (u[0] + u[-2]) - 2 * u[-1];
+    for (sh = 0; sh < 3; sh++) si[sh] = 13. / 12. * sd[sh] * sd[sh] + 1. / 4. * fd[sh] * fd[sh];
+  }
+  /* desensitise_smoothness_indicators (reconstructeno.c:1687-1707), USE_NORMU=1 */
+  for (i = -order + 1; i < order; i++) u2[i + order - 1] = u[i] * u[i];
+  normu = w_sum(2 * order - 1, u2);
+  e = normu * WENO_EPS;
+  for (sh = 0; sh < order; sh++) si[sh] += e;
+  /* DO_NORMALIZE_SMOOTHNESS_INDICATORS=1 */
+  w_normalize(order, DBL_MIN, si);
+  /* compute_weights_from_smoothness_indicators (reconstructeno.c:1878-1917) */
+  for (sh = 0; sh < order; sh++) {
+    double t = si[sh] + WENO_EPS / 1.;
+    t *= t;
+    s->w[sh] = 1. / t;
+  }
+  w_normalize(order, 0, s->w);
+  if (order == 3 && m0 > 0.0 && m0 < 1.0) {
+    double simple = 1.0 / (double)order;
+    for (i = 0; i < order; i++) s->w[i] = (1.0 - m0) * s->w[i] + m0 * simple;
+  }
+}
+
+/* compute_optimized_cf_stencil_weights (reconstructeno.c:1617-1683) */
+static void w_opt(double m0, wset *s)
+{
+  int o = s->order, sh;
+  if (m0 == 1 || m0 == -1) return;
+  for (sh = 0; sh < o; sh++) {
+    s->w[o + sh] = s->w[sh] * w_optl[o - 2][sh];
+    s->w[2 * o + sh] = s->w[sh] * w_optr[o - 2][sh];
+  }
+  w_normalize(o, DBL_MIN, &s->w[o]);
+  w_normalize(o, DBL_MIN, &s->w[2 * o]);
+}
+
+/* eno_cvt (reconstructeno.c:730-823) for CVT_C2L (right=0) / CVT_C2R (right=1)
+   with the order-2/3 centre-to-face matrices (reconstructeno_static.h) */
+static double w_cvt(const wset *s, int right, const double *u)
+{
+  static const double l2[2][2] = {{3. / 2., -1. / 2.}, {1. / 2., 1. / 2.}};
+  static const double r2[2][2] = {{1. / 2., 1. / 2.}, {-1. / 2., 3. / 2.}};
+  static const double l3[3][3] = {{15. / 8., -5. / 4., 3. / 8.}, {3. / 8., 3. / 4., -1. / 8.}, {-1. / 8., 3. / 4., 3. / 8.}};
+  static const double r3[3][3] = {{3. / 8., 3. / 4., -1. / 8.}, {-1. / 8., 3. / 4., 3. / 8.}, {3. / 8., -5. / 4., 15. / 8.}};
+  int o = s->order, sh, j;
+  const double *w = s->w + o * (right ? 2 : 1);
+  double pu[3], su[3];
+  for (sh = 0; sh < o; sh++) {
+    for (j = 0; j < o; j++) pu[j] = (o == 2 ? (right ? r2[sh][j] : l2[sh][j]) : (right ? r3[sh][j] : l3[sh][j])) * u[j - sh];
+    su[sh] = 0.0;
+    if (w[sh] != 0.0) su[sh] = w[sh] * w_sum(o, pu);
+  }
+  return w_sum(o, su);
+}
+
+/* compute_df_line_new (interpline.c:2148-2222): dP/P-type jump indicator at
+   line cell c from the primitives at c-1, c, c+1 and their CENT metrics */
+static double w_dp(const double *pm, const double *p0, const double *pp, const geomref *gm, const geomref *g0,
+                   const geomref *gp, double gam)
+{
+  zstate ql, q, qr;
+  double a, b, c_, parl, par, parr, uparl, upar, uparr;
+  get_state(pm, gm, &ql);
+  get_state(p0, g0, &q);
+  get_state(pp, gp, &qr);
+  a = compute_1plusud0(gm, &ql);
+  b = compute_1plusud0(g0, &q);
+  c_ = compute_1plusud0(gp, &qr);
+  parl = a * (ql.ucon[TT]);
+  par = b * (q.ucon[TT]);
+  parr = c_ * (qr.ucon[TT]);
+  uparl = gam * pm[UU] * (ql.ucon[TT] * ql.ucov[TT]) + (gam - 1.0) * pm[UU];
+  upar = gam * p0[UU] * (q.ucon[TT] * q.ucov[TT]) + (gam - 1.0) * p0[UU];
+  uparr = gam * pp[UU] * (qr.ucon[TT] * qr.ucov[TT]) + (gam - 1.0) * pp[UU];
+  return (fabs(p0[RHO] * (parr - parl)) + fabs(uparr - uparl)) / (fabs(p0[RHO] * par) + fabs(upar) + DBL_MIN);
+}
+
+/* eno_line_reconstruct (reconstructeno.c:261-563) for CVT_C2E together with
+   compute_smonotonicity_line (smonointerp.c:15-175): y is the line of one
+   primitive (valid at -6..n+5), dP the jump indicator (valid at -1..n);
+   yl/yr receive the left/right face values of cells -1..n (index +1). */
+static void weno5_line(int n, const double *y, const double *dP, double *yl, double *yr, wset *ws, double *m0,
+                       int *cusp)
+{
+  int c;
+  /* SMONO indicators and unoptimised weights at -4..n+3 (index +4) */
+  for (c = -4; c <= n + 3; c++) {
+    int q = c + 4;
+    cusp[q] = w_cusp(&y[c]);
+    m0[q] = cusp[q] ? 0.0 : w_mono(&y[c]);
+    w_unopt(3, m0[q], cusp[q], &y[c], &ws[q]);
+  }
+  /* compute_weights_ratios (reconstructeno.c:1962-2083) at -2..n+1: both
+     neighbours are inside the line, AND reduction, C2E ratios */
+  for (c = -2; c <= n + 1; c++) {
+    wset *s = &ws[c + 4];
+    double wrl, wrr, wr, lof, minr = W_MIN_RAT, maxr = W_MAX_RAT;
+    wrl = (s->w[2] + WENO_EPS) / (ws[c + 4 - 2].w[0] + WENO_EPS);
+    wrr = (s->w[0] + WENO_EPS) / (ws[c + 4 + 2].w[2] + WENO_EPS);
+    wr = W_MIN(wrl, wrr);
+    lof = (wr - minr) / (maxr - minr);
+    lof = W_MAX(0., W_MIN(lof, 1.0));
+    s->lof = W_MAX(lof, s->lof);
+    s->fordpp = s->lof;
+  }
+  /* apply_additional_reduction_to_weights (reconstructeno.c:650-700): post-
+     and pre-shock reduction from dP/P; reads fordpp only, so order-free */
+  for (c = -1; c <= n; c++) {
+    wset *s = &ws[c + 4];
+    double ss = W_MIN((fabs(dP[c]) - 0.5 * W_DP_FRAC) / (0.5 * W_DP_FRAC), 1.);
+    double lof = s->lof;
+    lof = W_MAX(lof, ss * ws[c + 4 + 1].fordpp);
+    lof = W_MAX(lof, ss * ws[c + 4 - 1].fordpp);
+    s->lof = lof;
+  }
+  /* optimised weights, choose_weno_order (reconstructeno.c:2087-2247) and
+     the output combination (reconstructeno.c:470-545) */
+  for (c = -1; c <= n; c++) {
+    int q = c + 4, side;
+    wset hi = ws[q], lo;
+    double lof, mi = m0[q];
+    w_opt(mi, &hi);
+    lof = hi.lof;
+    if (0.0 < lof) {
+      int k;
+      for (k = 3; k < 9; k++) hi.w[k] *= (1. - lof);
+      w_unopt(2, mi, cusp[q], &y[c], &lo);
+      w_opt(mi, &lo);
+      for (k = 0; k < 6; k++) lo.w[k] *= lof;
+    }
+    for (side = 0; side < 2; side++) {
+      double *out = side ? &yr[c + 1] : &yl[c + 1];
+      /* SMONO's 5-point value where its indicator is nonzero (cusps have
+         indicator 0); eno_line_reconstruct zeroes the output where it is 0 */
+      double prev = (mi != 0.0) ? w_eno5(side, &y[c]) : 0.0;
+      if (mi >= 0.0 && mi < 1.0) {
+        double v = 0.0;
+        v += w_cvt(&hi, side, &y[c]);
+        if (0.0 < lof) v += w_cvt(&lo, side, &y[c]);
+        prev = (1.0 - mi) * v + mi * prev;
+      }
+      *out = prev;
+    }
+  }
+}
+
 /* flux_compute_general (fluxcompute.c:12-51) for one face */
 static int face_flux(const hgo_config *c, int dir, const geomref *g, double *p_l, double *p_r, double *F, double *ctop)
 {
@@ -514,6 +824,53 @@ static int face_flux(const hgo_config *c, int dir, const geomref *g, double *p_l
   return 0;
 }
 
+static long dom_ntot(const dom *d);
+
+/* slope_lim_linetype_c2e (interpline.c:517-678) for the lines along `dir`
+   through the transverse ranges of the flux loop: pleft/pright (the
+   reference's arrays, AoS with NPR per zone) of the line cells -1..n */
+static void weno5_faces(dom *d, const double *pr, int dir, int is, int ie, int js, int je, int ks, int ke,
+                        double *pleft, double *pright)
+{
+  int n = d->n[dir], a, b, c, pl;
+  int ta0, ta1, tb0, tb1;
+  int L = n + 12; /* line cells -6..n+5 */
+  double *y = (double *)malloc(sizeof(double) * L), *dP = (double *)malloc(sizeof(double) * (n + 2));
+  double *yl = (double *)malloc(sizeof(double) * (n + 2)), *yr = (double *)malloc(sizeof(double) * (n + 2));
+  double *m0 = (double *)malloc(sizeof(double) * (n + 8));
+  int *cusp = (int *)malloc(sizeof(int) * (n + 8));
+  wset *ws = (wset *)malloc(sizeof(wset) * (n + 8));
+  /* transverse ranges: the two directions other than dir */
+  if (dir == 1) { ta0 = js; ta1 = je; tb0 = ks; tb1 = ke; }
+  else if (dir == 2) { ta0 = is; ta1 = ie; tb0 = ks; tb1 = ke; }
+  else { ta0 = is; ta1 = ie; tb0 = js; tb1 = je; }
+  for (a = ta0; a <= ta1; a++)
+    for (b = tb0; b <= tb1; b++) {
+#define CELL(cc) ((dir == 1) ? zidx(d, (cc), a, b) : ((dir == 2) ? zidx(d, a, (cc), b) : zidx(d, a, b, (cc))))
+      /* dP/P from the primitives along the line (get_df_line_gen_new, interpline.c:1152-1198) */
+      for (c = -1; c <= n; c++) {
+        geomref gm, g0, gp;
+        int im = (dir == 1) ? c - 1 : a, jm = (dir == 2) ? c - 1 : ((dir == 1) ? a : b);
+        int i0 = (dir == 1) ? c : a, j0 = (dir == 2) ? c : ((dir == 1) ? a : b);
+        int ip = (dir == 1) ? c + 1 : a, jp = (dir == 2) ? c + 1 : ((dir == 1) ? a : b);
+        get_geometry(d, im, jm, CENT, &gm);
+        get_geometry(d, i0, j0, CENT, &g0);
+        get_geometry(d, ip, jp, CENT, &gp);
+        dP[c + 1] = w_dp(&pr[CELL(c - 1) * NPR], &pr[CELL(c) * NPR], &pr[CELL(c + 1) * NPR], &gm, &g0, &gp, d->c->gam);
+      }
+      for (pl = 0; pl < NPR; pl++) {
+        for (c = -6; c <= n + 5; c++) y[c + 6] = pr[CELL(c) * NPR + pl];
+        weno5_line(n, y + 6, dP + 1, yl, yr, ws, m0, cusp);
+        for (c = -1; c <= n; c++) {
+          pleft[CELL(c) * NPR + pl] = yl[c + 1];
+          pright[CELL(c) * NPR + pl] = yr[c + 1];
+        }
+      }
+#undef CELL
+    }
+  free(y); free(dP); free(yl); free(yr); free(m0); free(cusp); free(ws);
+}
+
 /* fluxcalc_standard for one direction (flux.c:469-680) with MC-type slopes */
 static void fluxcalc_dir(dom *d, const double *pr, int dir, double *F, double *dq, double *ndt)
 {
@@ -537,14 +894,18 @@ static void fluxcalc_dir(dom *d, const double *pr, int dir, double *F, double *d
   ks = (dir == 3) ? 0 : -d->sh[3];
   ke = (dir == 3) ? n3 - 1 + d->sh[3] : n3 - 1 + d->sh[3];
 
-  /* slopes over the zones the faces read: centers (face-1) and (face) */
-  for (i = is - di; i <= ie; i++)
-    for (j = js - dj; j <= je; j++)
-      for (k = ks - dk; k <= ke; k++) {
-        long z = zidx(d, i, j, k);
-        for (pl = 0; pl < NPR; pl++)
-          dq[z * NPR + pl] = slope3(c->lim, pr[(z - dofs) * NPR + pl], pr[z * NPR + pl], pr[(z + dofs) * NPR + pl]);
-      }
+  if (c->lim == HGO_LIM_WENO5) {
+    weno5_faces(d, pr, dir, is, ie, js, je, ks, ke, dq, dq + dom_ntot(d) * NPR);
+  } else {
+    /* slopes over the zones the faces read: centers (face-1) and (face) */
+    for (i = is - di; i <= ie; i++)
+      for (j = js - dj; j <= je; j++)
+        for (k = ks - dk; k <= ke; k++) {
+          long z = zidx(d, i, j, k);
+          for (pl = 0; pl < NPR; pl++)
+            dq[z * NPR + pl] = slope3(c->lim, pr[(z - dofs) * NPR + pl], pr[z * NPR + pl], pr[(z + dofs) * NPR + pl]);
+        }
+  }
 
   for (i = is; i <= ie; i++)
     for (j = js; j <= je; j++)
@@ -553,9 +914,17 @@ static void fluxcalc_dir(dom *d, const double *pr, int dir, double *F, double *d
         long zm = z - dofs;
         int e;
         /* getp2interplr (flux.c:788-808) */
-        for (pl = 0; pl < NPR; pl++) {
-          p_l[pl] = pr[zm * NPR + pl] + 0.5 * dq[zm * NPR + pl];
-          p_r[pl] = pr[z * NPR + pl] - 0.5 * dq[z * NPR + pl];
+        if (c->lim == HGO_LIM_WENO5) {
+          const double *pleft = dq, *pright = dq + dom_ntot(d) * NPR;
+          for (pl = 0; pl < NPR; pl++) {
+            p_l[pl] = pright[zm * NPR + pl];
+            p_r[pl] = pleft[z * NPR + pl];
+          }
+        } else {
+          for (pl = 0; pl < NPR; pl++) {
+            p_l[pl] = pr[zm * NPR + pl] + 0.5 * dq[zm * NPR + pl];
+            p_r[pl] = pr[z * NPR + pl] - 0.5 * dq[z * NPR + pl];
+          }
         }
         get_geometry(d, i, j, loc, &g);
         /* BDIRCONT (flux.c:629-633) */
@@ -1436,7 +1805,7 @@ static void advance(dom *d, const double *pi, const double *pb, double *pf, doub
 static int alloc_scratch(const dom *d, scratch *sc)
 {
   long n = dom_ntot(d);
-  sc->dq = (double *)calloc((size_t)n * NPR, sizeof(double));
+  sc->dq = (double *)calloc((size_t)n * NPR * 2, sizeof(double)); /* MC slopes, or WENO5 pleft|pright */
   sc->emf = (double *)calloc((size_t)n * 3, sizeof(double));
   sc->ptoavg = (double *)calloc((size_t)n * NPR, sizeof(double));
   sc->gammacheck = (double *)calloc((size_t)n, sizeof(double));
