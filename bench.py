@@ -4,8 +4,9 @@
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
 Workload: 3D Fishbone-Moncrief torus around a Kerr hole (a=0.9375, beta=100,
-MKS hslope=0.3, Rout=40) on 256x128x128 zones, FP64, HLL + flux-CT + 2D
-Noble inversion + fixups + boundaries, midpoint RK2.  One step = one full
+MKS hslope=0.3, Rout=40) on 256x128x128 zones, FP64, WENO5 + HLL + flux-CT +
+2D Noble inversion + fixups + boundaries, midpoint RK2 (the MC variants and
+smaller grids are selectable with --workload).  One step = one full
 time step (both RK substeps) of the whole domain; one zone-update = one
 active zone advanced by one full step.
 
@@ -44,14 +45,22 @@ sys.path.insert(0, ROOT)
 
 WORKLOADS = {
     # name: (n1, n2, n3, lim, flux)
-    "torus3d_256x128x128": (256, 128, 128, "MC", "HLL"),
-    "torus3d_256x128x64": (256, 128, 64, "MC", "HLL"),
-    "torus3d_128x64x32": (128, 64, 32, "MC", "HLL"),
+    "torus3d_256x128x128": (256, 128, 128, "WENO5", "HLL"),
+    "torus3d_256x128x64": (256, 128, 64, "WENO5", "HLL"),
+    "torus3d_128x64x32": (128, 64, 32, "WENO5", "HLL"),
+    "torus3d_256x128x128_mc": (256, 128, 128, "MC", "HLL"),
+    "torus3d_256x128x64_mc": (256, 128, 64, "MC", "HLL"),
     "torus2d_64x64": (64, 64, 1, "MC", "HLL"),
 }
 DEFAULT_WORKLOAD = "torus3d_256x128x128"
-# CPU sample for the reference build: same problem, smaller 3D grid
-CPU_SAMPLE = (64, 32, 32, "MC", "HLL")
+# ghost zones kept on the device: MC reads 2 per side, WENO5 6 (the reference's
+# MAXBND=11 lines never truncate a WENO5 stencil, and 6 is what its stencils read)
+GHOSTS = {"MC": 3, "WENO5": 6}
+
+
+def cpu_sample(lim):
+    """CPU sample for the reference build: same problem and scheme, 3D 64x32x32."""
+    return (64, 32, 32, lim, "HLL")
 
 METRIC = "zone-updates/s FP64 vs mixed on 3D Kerr torus at stated L1; batch p50/p99 latency"
 
@@ -127,15 +136,23 @@ def measured_peaks():
         return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}, "fallback"
 
 
-def profile_traffic(kernel):
-    """DRAM bytes per launch of `kernel` from the committed ncu summary, if any."""
+def _traffic_row(workload, kernel):
+    """(DRAM bytes, FP64 flop) per launch of `kernel` on `workload` from the
+    committed ncu summary profiles/traffic.md, or None."""
     path = os.path.join(ROOT, "profiles", "traffic.md")
     try:
         txt = open(path).read()
     except OSError:
         return None
-    m = re.search(rf"^\|\s*{re.escape(kernel)}\s*\|\s*([0-9.eE+]+)\s*\|", txt, re.M)
-    return float(m.group(1)) if m else None
+    m = re.search(rf"^\|\s*{re.escape(workload)}\s*\|\s*{re.escape(kernel)}\s*\|\s*([0-9.eE+]+)\s*\|\s*([0-9.eE+]+)\s*\|",
+                  txt, re.M)
+    return (float(m.group(1)), float(m.group(2))) if m else None
+
+
+def profile_traffic(workload, kernel):
+    """DRAM bytes per launch of `kernel` from the committed ncu summary, if any."""
+    r = _traffic_row(workload, kernel)
+    return r[0] if r else None
 
 
 # ---------------------------------------------------------------------------
@@ -191,7 +208,7 @@ def bench_ours(args, rank, world):
 
     n1, n2, n3, lim, flux = WORKLOADS[args.workload]
     t_gen = time.time()
-    dom = torus.fm_torus(n1, n2, n3, ng=3, lim=lim, flux=flux, seed=7 + rank)
+    dom = torus.fm_torus(n1, n2, n3, ng=GHOSTS[lim], lim=lim, flux=flux, seed=7 + rank)
     t_gen = time.time() - t_gen
     L = load_library()
     g = HarmGPU(n1, n2, n3, dom.ng, dom.dx, lim=lim, flux=flux, precision=args.precision, gam=dom.gam,
@@ -270,15 +287,15 @@ def bench_ours(args, rank, world):
     dom_k = max(ktimes, key=lambda k: ktimes[k]["ms"])
     kt = ktimes[dom_k]
     avg_s = kt["ms"] / kt["launches"] / 1e3
-    alg = algorithmic_bytes(dom_k, n1, n2, n3)
+    alg = algorithmic_bytes(dom_k, n1, n2, n3, lim)
     peaks, peaks_kind = measured_peaks()
     achieved = alg / avg_s / 1e9
     roof = {"kernel": dom_k, "bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
-            "frac": achieved / peaks["hbm_gbs"], "traffic": profile_traffic(dom_k),
+            "frac": achieved / peaks["hbm_gbs"], "traffic": profile_traffic(args.workload, dom_k),
             "peak_source": f"hbm_gbs ({peaks_kind})", "algorithmic_bytes_per_launch": alg,
             "avg_launch_ms": avg_s * 1e3,
             "share": kt["ms"] / sum(v["ms"] for v in ktimes.values())}
-    fp64 = fp64_roof(kt, dom_k, n1, n2, n3, args)
+    fp64 = fp64_roof(kt, dom_k, args)
     if fp64:
         roof["fp64"] = fp64
 
@@ -299,12 +316,12 @@ def bench_ours(args, rank, world):
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         procs = min(host_cores(), args.cpu_procs)
-        v, why = run_reference(CPU_SAMPLE, args.cpu_steps, 2, procs)
+        cs = cpu_sample(lim)
+        v, why = run_reference(cs, args.cpu_steps, 2, procs)
         result["cpu_baseline"] = ({"value": v, "unit": "zone-updates/s", "cores": procs, "kind": "reference",
                                    "sample": f"reference CPU build (gcc -O2 -ffp-contract=off), 3D torus "
-                                             f"{CPU_SAMPLE[0]}x{CPU_SAMPLE[1]}x{CPU_SAMPLE[2]} {CPU_SAMPLE[3]}+"
-                                             f"{CPU_SAMPLE[4]}, {args.cpu_steps} steps after 2 warm-up, one "
-                                             f"process per core"}
+                                             f"{cs[0]}x{cs[1]}x{cs[2]} {cs[3]}+{cs[4]}, {args.cpu_steps} steps "
+                                             f"after 2 warm-up, one process per core"}
                                   if v else {"value": None, "unavailable": why})
     result["gen_seconds"] = t_gen
     if dist is not None:
@@ -313,14 +330,23 @@ def bench_ours(args, rank, world):
     return result
 
 
-def algorithmic_bytes(kernel, n1, n2, n3):
+def algorithmic_bytes(kernel, n1, n2, n3, lim="MC"):
     """Compulsory HBM bytes per launch (FP64, state resident; per-(i,j) metric
     amortised over x3).  Units: faces for the flux kernels, zones otherwise."""
     zones = n1 * n2 * n3
     faces = {"flux_x1": (n1 + 1) * (n2 + 2) * (n3 + 2), "flux_x2": (n1 + 2) * (n2 + 1) * (n3 + 2),
              "flux_x3": (n1 + 2) * (n2 + 2) * (n3 + 1)}
     if kernel in faces:
+        if lim == "WENO5":
+            return faces[kernel] * (128 + 64)     # read the two face states (16 doubles), write 8 fluxes
         return faces[kernel] * (64 + 64)          # read one zone's 8 primitives, write 8 face fluxes
+    # the WENO5 passes run once per direction under one name: mean cells per launch
+    nd = [n for n in (n1, n2, n3) if n > 1]
+    if kernel in ("weno_a", "weno_b"):
+        ext = 8 if kernel == "weno_a" else 2
+        cells = sum(zones / n * (n + ext) for n in nd) / len(nd)
+        # A: read 8 primitives, write 4 planes x 8; B: read 8 primitives + 4x8 planes, write 16 face values
+        return cells * ((64 + 256) if kernel == "weno_a" else (64 + 256 + 128))
     if kernel == "update":
         # mean of the two substeps: p(64) [+pk 64] + 5 F comps x3 dirs (120) + 3 EMFs (24)
         # + uf/ucum write (128) [+read 128] + pf (64) + pflag (4)
@@ -332,18 +358,13 @@ def algorithmic_bytes(kernel, n1, n2, n3):
     return zones * 8.0
 
 
-def fp64_roof(kt, kernel, n1, n2, n3, args):
-    """FP64 rate of the dominant kernel from the per-unit FP64 operation count
+def fp64_roof(kt, kernel, args):
+    """FP64 rate of the dominant kernel from the per-launch FP64 operation count
     measured with ncu (profiles/traffic.md) vs the FP64 peak measured here."""
-    path = os.path.join(ROOT, "profiles", "traffic.md")
-    try:
-        txt = open(path).read()
-    except OSError:
+    r = _traffic_row(args.workload, kernel)
+    if not r:
         return None
-    m = re.search(rf"^\|\s*{re.escape(kernel)}\s*\|\s*[0-9.eE+]+\s*\|\s*([0-9.eE+]+)\s*\|", txt, re.M)
-    if not m:
-        return None
-    ops_per_launch = float(m.group(1))
+    ops_per_launch = r[1]
     avg_s = kt["ms"] / kt["launches"] / 1e3
     achieved = ops_per_launch / avg_s / 1e12
     peak = measure_fp64_peak()
@@ -387,14 +408,15 @@ def main():
         if rank != 0:
             return 0
         procs = min(host_cores(), args.cpu_procs)
+        cs = cpu_sample(WORKLOADS[args.workload][3])
         # each step: one step of every process's bounded sample
-        v, why = run_reference(CPU_SAMPLE, args.steps, args.warmup, procs)
+        v, why = run_reference(cs, args.steps, args.warmup, procs)
         if v is None:
             print(json.dumps({"impl": "reference", "unavailable": why}))
             return 0
-        n1, n2, n3 = CPU_SAMPLE[:3]
+        n1, n2, n3 = cs[:3]
         sample = (f"reference CPU build (its own C sources, gcc -O2 -ffp-contract=off): 3D torus {n1}x{n2}x{n3} "
-                  f"{CPU_SAMPLE[3]}+{CPU_SAMPLE[4]} per process, {procs} processes (the code is single-threaded "
+                  f"{cs[3]}+{cs[4]} per process, {procs} processes (the code is single-threaded "
                   f"and non-reentrant), {args.steps} timed steps after {args.warmup}")
         out = {"impl": "reference", "metric": METRIC, "value": v, "unit": "zone-updates/s", "n_gpus": args.gpus,
                "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",

@@ -17,7 +17,7 @@ CSRC = os.path.join(PKG, "csrc")
 LIBDIR = os.path.join(PKG, "lib")
 LIB = os.path.join(LIBDIR, "libharmgpu.so")
 SOURCES = ["harm_gpu.cu"]
-HEADERS = ["harm_device.cuh", os.path.join(ROOT, "include", "harmgpu.h")]
+HEADERS = ["harm_device.cuh", "weno5.cuh", os.path.join(ROOT, "include", "harmgpu.h")]
 
 NVCC_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-lineinfo", "-std=c++17",
               "-fmad=false", "-Xcompiler", "-fPIC", "-shared", "--expt-relaxed-constexpr",

@@ -10,6 +10,8 @@
 //     CORN1..3 gdet, conn[64] at CENT, floors[2].
 //
 // Work per RK substep (the reference's advance(), step_ch.c:94-186):
+//   weno_a/weno_b     WENO5 line reconstruction (interpline.c:517-678) in two
+//                     cell-parallel passes (lim = WENO5 only; weno5.cuh)
 //   flux_kernel<dir>  fluxcalc_standard (flux.c:469-680) fused with the MC
 //                     slopes, both Riemann states, vchar, HLL/LaxF, the gdet
 //                     strip of flux_ct and the dt-min
@@ -33,6 +35,7 @@
 
 #include "harm_device.cuh"
 #include "harmgpu.h"
+#include "weno5.cuh"
 
 using namespace hg;
 
@@ -172,10 +175,119 @@ __device__ __forceinline__ double slope3(int lim, double yl, double yc, double y
 }
 
 // ---------------------------------------------------------------------------
-// face flux kernel (one per direction)
+// WENO5 line reconstruction (slope_lim_linetype_c2e, interpline.c:517-678) as
+// two cell-parallel passes; see weno5.cuh.  Scratch WA holds, per primitive
+// v, 4 planes: the SMONO code (indicator in [0,1], -1 at a cusp) and the
+// three unoptimised weights.
 // ---------------------------------------------------------------------------
+constexpr int W5_PLANES = 4;
+
 template <int DIR>
+__device__ __forceinline__ long long dir_stride(const Dims &d) {
+  return (DIR == 1) ? (long long)d.nt2 * d.nt3 : ((DIR == 2) ? (long long)d.nt3 : 1);
+}
+
+// pass A over line cells -4..n+3: cusp test, SMONO indicator, unoptimised weights
+template <int DIR>
+__global__ void __launch_bounds__(128) weno_a_kernel(Dims d, Box box, const double *__restrict__ pb,
+                                                     double *__restrict__ WA) {
+  long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= box.size()) return;
+  int i, j, k;
+  box_ijk(box, t, i, j, k);
+  long long z = zix(d, i, j, k);
+  const long long o = dir_stride<DIR>(d);
+  for (int v = 0; v < NPR; v++) {
+    const double *q = pb + (long long)v * d.nz + z;
+    double ya[5] = {__ldg(q - 2 * o), __ldg(q - o), __ldg(q), __ldg(q + o), __ldg(q + 2 * o)};
+    const double *y = ya + 2;
+    bool c = w5::cusp(y);
+    double m0 = c ? 0.0 : w5::mono(y);
+    double w[3];
+    w5::unopt3(m0, y, w);
+    double *out = WA + (long long)v * W5_PLANES * d.nz + z;
+    out[0] = c ? -1.0 : m0;
+    out[d.nz] = w[0];
+    out[2 * d.nz] = w[1];
+    out[3 * d.nz] = w[2];
+  }
+}
+
+// pass B over line cells -1..n: dP/P, ratios, reduction, face values
+template <int DIR>
+__global__ void __launch_bounds__(128) weno_b_kernel(Dims d, Params P, Box box, const double *__restrict__ pb,
+                                                     const double *__restrict__ G, const double *__restrict__ WA,
+                                                     double *__restrict__ pL, double *__restrict__ pR) {
+  long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= box.size()) return;
+  int i, j, k;
+  box_ijk(box, t, i, j, k);
+  long long z = zix(d, i, j, k);
+  const long long o = dir_stride<DIR>(d);
+  // compute_df_line_new (interpline.c:2148-2222): jump indicator from the
+  // primitives of the cells -1, 0, +1 along the line and their CENT metrics
+  double dP;
+  {
+    double pm[NPR], p0[NPR], pp[NPR];
+    load_prim(pb, d, z - o, pm);
+    load_prim(pb, d, z, p0);
+    load_prim(pb, d, z + o, pp);
+    State ql, q, qr;
+    double a, b, c;
+    Metric m;
+    load_metric(G, d, gix(d, i - (DIR == 1), j - (DIR == 2)), G_CENT, m);
+    get_state(pm, m, ql);
+    a = compute_1plusud0(m, ql);
+    load_metric(G, d, gix(d, i, j), G_CENT, m);
+    get_state(p0, m, q);
+    b = compute_1plusud0(m, q);
+    load_metric(G, d, gix(d, i + (DIR == 1), j + (DIR == 2)), G_CENT, m);
+    get_state(pp, m, qr);
+    c = compute_1plusud0(m, qr);
+    double gam = P.gam;
+    double parl = a * (ql.ucon[0]);
+    double par = b * (q.ucon[0]);
+    double parr = c * (qr.ucon[0]);
+    double uparl = gam * pm[UU] * (ql.ucon[0] * ql.ucov[0]) + (gam - 1.0) * pm[UU];
+    double upar = gam * p0[UU] * (q.ucon[0] * q.ucov[0]) + (gam - 1.0) * p0[UU];
+    double uparr = gam * pp[UU] * (qr.ucon[0] * qr.ucov[0]) + (gam - 1.0) * pp[UU];
+    dP = (fabs(p0[RHO] * (parr - parl)) + fabs(uparr - uparl)) / (fabs(p0[RHO] * par) + fabs(upar) + w5::kDblMin);
+  }
+  // apply_additional_reduction_to_weights (reconstructeno.c:650-700)
+  double ss = w5::wmin((fabs(dP) - 0.5 * w5::kDpFrac) / (0.5 * w5::kDpFrac), 1.);
+  for (int v = 0; v < NPR; v++) {
+    const double *wa = WA + (long long)v * W5_PLANES * d.nz + z;
+    // codes of cells -1, 0, +1 and weights of cells -3..+3 (w0 and w2 of the neighbours)
+    double cm = __ldg(wa - o), c0 = __ldg(wa), cp = __ldg(wa + o);
+    const double *w0p = wa + d.nz, *w1p = wa + 2 * d.nz, *w2p = wa + 3 * d.nz;
+    double wc[3] = {__ldg(w0p), __ldg(w1p), __ldg(w2p)};
+    double wm[3] = {__ldg(w0p - o), 0.0, __ldg(w2p - o)};
+    double wp[3] = {__ldg(w0p + o), 0.0, __ldg(w2p + o)};
+    double w_m3_0 = __ldg(w0p - 3 * o), w_m2_0 = __ldg(w0p - 2 * o);
+    double w_p2_2 = __ldg(w2p + 2 * o), w_p3_2 = __ldg(w2p + 3 * o);
+    double fd_m = w5::ratio_lof(wm, w_m3_0, __ldg(w2p + o), cm == -1.0 ? 1.0 : 0.0);
+    double fd_p = w5::ratio_lof(wp, __ldg(w0p - o), w_p3_2, cp == -1.0 ? 1.0 : 0.0);
+    double lof = w5::ratio_lof(wc, w_m2_0, w_p2_2, c0 == -1.0 ? 1.0 : 0.0);
+    lof = w5::wmax(lof, ss * fd_p);
+    lof = w5::wmax(lof, ss * fd_m);
+    const double *q = pb + (long long)v * d.nz + z;
+    double ya[5] = {__ldg(q - 2 * o), __ldg(q - o), __ldg(q), __ldg(q + o), __ldg(q + 2 * o)};
+    bool cu = (c0 == -1.0);
+    double m0 = cu ? 0.0 : c0;
+    double yl, yr;
+    w5::faces(ya + 2, m0, cu, wc, lof, &yl, &yr);
+    pL[(long long)v * d.nz + z] = yl;
+    pR[(long long)v * d.nz + z] = yr;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// face flux kernel (one per direction); RECON 0: MC-type slopes in the
+// kernel, RECON 1: Riemann states from the WENO5 face values pL/pR
+// ---------------------------------------------------------------------------
+template <int DIR, int RECON>
 __global__ void __launch_bounds__(128) flux_kernel(Dims d, Params P, Box box, const double *__restrict__ pb,
+                                                   const double *__restrict__ pL, const double *__restrict__ pR,
                                                    const double *__restrict__ G, double *__restrict__ F,
                                                    Scalars *sc) {
   long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -185,17 +297,26 @@ __global__ void __launch_bounds__(128) flux_kernel(Dims d, Params P, Box box, co
     int i, j, k;
     box_ijk(box, t, i, j, k);
     long long z = zix(d, i, j, k);
-    const long long o = (DIR == 1) ? (long long)d.nt2 * d.nt3 : ((DIR == 2) ? (long long)d.nt3 : 1);
+    const long long o = dir_stride<DIR>(d);
     double p_l[NPR], p_r[NPR];
+    if (RECON == 1) {
+      // getp2interplr (flux.c:788-808), line-type branch
 #pragma unroll
-    for (int v = 0; v < NPR; v++) {
-      const double *q = pb + (long long)v * d.nz + z;
-      double ym2 = __ldg(q - 2 * o), ym1 = __ldg(q - o), y0 = __ldg(q), yp1 = __ldg(q + o);
-      double dqm = slope3(P.lim, ym2, ym1, y0);
-      double dq0 = slope3(P.lim, ym1, y0, yp1);
-      // getp2interplr (flux.c:788-808)
-      p_l[v] = ym1 + 0.5 * dqm;
-      p_r[v] = y0 - 0.5 * dq0;
+      for (int v = 0; v < NPR; v++) {
+        p_l[v] = __ldg(pR + (long long)v * d.nz + z - o);
+        p_r[v] = __ldg(pL + (long long)v * d.nz + z);
+      }
+    } else {
+#pragma unroll
+      for (int v = 0; v < NPR; v++) {
+        const double *q = pb + (long long)v * d.nz + z;
+        double ym2 = __ldg(q - 2 * o), ym1 = __ldg(q - o), y0 = __ldg(q), yp1 = __ldg(q + o);
+        double dqm = slope3(P.lim, ym2, ym1, y0);
+        double dq0 = slope3(P.lim, ym1, y0, yp1);
+        // getp2interplr (flux.c:788-808)
+        p_l[v] = ym1 + 0.5 * dqm;
+        p_r[v] = y0 - 0.5 * dq0;
+      }
     }
     // BDIRCONT (flux.c:629-633)
     p_l[B1 + DIR - 1] = p_r[B1 + DIR - 1] = 0.5 * (p_l[B1 + DIR - 1] + p_r[B1 + DIR - 1]);
@@ -952,12 +1073,12 @@ inline unsigned grid_for(long long n, int block) { return (unsigned)((n + block 
 // ---------------------------------------------------------------------------
 enum KernelId {
   K_RESET, K_FLUX1, K_FLUX2, K_FLUX3, K_EMF, K_UPDATE, K_BOUND_GHOST, K_BOUND_POLE, K_BOUND_PFLAG, K_CHECK_GAMMA,
-  K_CHECK_RESOLVE, K_FIX_COLLECT, K_FIX_COMPUTE, K_FIX_SCATTER, K_FINALIZE, K_OTHER, K_NKERNELS
+  K_CHECK_RESOLVE, K_FIX_COLLECT, K_FIX_COMPUTE, K_FIX_SCATTER, K_FINALIZE, K_WENO_A, K_WENO_B, K_OTHER, K_NKERNELS
 };
 static const char *kKernelNames[K_NKERNELS] = {
     "reset_stage",  "flux_x1",         "flux_x2",       "flux_x3",       "emf",           "update",
     "bound_ghost",  "bound_pole",      "bound_pflag",   "checksol_gamma", "checksol_resolve", "fixup_collect",
-    "fixup_compute", "fixup_scatter",  "finalize",      "other"};
+    "fixup_compute", "fixup_scatter",  "finalize",      "weno_a",        "weno_b",        "other"};
 
 struct ProfEvent {
   int kid;
@@ -987,6 +1108,8 @@ struct hgpu_ctx {
   int cap = 0;
   Scalars *sc = nullptr;
   double *staging = nullptr;  // AoS staging for uploads/downloads
+  double *pL = nullptr, *pR = nullptr, *WA = nullptr;  // WENO5 face values and weights scratch
+  Box wa_box[4], wb_box[4];
   int *istaging = nullptr;
   Box face_box[4], emf_box, active_box, dq_box;
 };
@@ -1046,8 +1169,11 @@ static void collect_profile(hgpu_ctx *x) {
 static int validate(const hgpu_config *c) {
   if (!c) return HGPU_E_INVALID;
   if (c->n1 < 1 || c->n2 < 1 || c->n3 < 1 || c->ng < 2) return HGPU_E_INVALID;
-  if (c->lim != HGPU_LIM_MC && c->lim != HGPU_LIM_VANL && c->lim != HGPU_LIM_MINM && c->lim != HGPU_LIM_DONOR)
+  if (c->lim != HGPU_LIM_MC && c->lim != HGPU_LIM_VANL && c->lim != HGPU_LIM_MINM && c->lim != HGPU_LIM_DONOR &&
+      c->lim != HGPU_LIM_WENO5)
     return HGPU_E_INVALID;
+  // WENO5 reads the line up to 5 cells beyond the faces' cells -1..n
+  if (c->lim == HGPU_LIM_WENO5 && c->ng < 6) return HGPU_E_INVALID;
   if (c->fluxmethod != HGPU_FLUX_HLL && c->fluxmethod != HGPU_FLUX_LAXF) return HGPU_E_INVALID;
   for (int f = 0; f < 6; f++)
     if (c->bc[f] != HGPU_BC_OUTFLOW && c->bc[f] != HGPU_BC_POLARAXIS && c->bc[f] != HGPU_BC_PERIODIC)
@@ -1072,7 +1198,8 @@ void hgpu_destroy(hgpu_ctx *x) {
   collect_profile(x);
   for (cudaEvent_t e : x->freelist) cudaEventDestroy(e);
   void *ptrs[] = {x->p, x->pk, x->uf, x->ucum, x->F[1], x->F[2], x->F[3], x->E, x->G, x->pflag, x->gammacheck,
-                  x->cand, x->fixlist, x->cand_orig, x->cand_dec, x->candmap, x->fixvals, x->sc, x->staging, x->istaging};
+                  x->cand, x->fixlist, x->cand_orig, x->cand_dec, x->candmap, x->fixvals, x->sc, x->staging, x->istaging,
+                  x->pL, x->pR, x->WA};
   for (void *q : ptrs)
     if (q) cudaFree(q);
   cudaStreamDestroy(x->stream);
@@ -1130,6 +1257,17 @@ int hgpu_create(const hgpu_config *cfg, hgpu_ctx **out) {
   x->emf_box = Box{0, 0, 0, d.n1 + d.s1, d.n2 + d.s2, d.n3 + d.s3};
   x->active_box = Box{0, 0, 0, d.n1, d.n2, d.n3};
   x->dq_box = Box{-d.s1, -d.s2, -d.s3, d.n1 + 2 * d.s1, d.n2 + 2 * d.s2, d.n3 + 2 * d.s3};
+  // WENO5 passes: line cells -4..n+3 (A) and -1..n (B) along the direction,
+  // the flux loop's transverse ranges across it
+  for (int q = 1; q <= 3; q++) {
+    Box a = x->face_box[q], b = x->face_box[q];
+    int n = (q == 1) ? d.n1 : ((q == 2) ? d.n2 : d.n3);
+    if (q == 1) { a.i0 = -4; a.ni = n + 8; b.i0 = -1; b.ni = n + 2; }
+    if (q == 2) { a.j0 = -4; a.nj = n + 8; b.j0 = -1; b.nj = n + 2; }
+    if (q == 3) { a.k0 = -4; a.nk = n + 8; b.k0 = -1; b.nk = n + 2; }
+    x->wa_box[q] = a;
+    x->wb_box[q] = b;
+  }
   long long nz = d.nz;
   x->cap = (int)((long long)d.n1 * d.n2 * d.n3 < (1LL << 22) ? (long long)d.n1 * d.n2 * d.n3 : (1LL << 22));
   if (cudaStreamCreateWithFlags(&x->stream, cudaStreamNonBlocking) != cudaSuccess) {
@@ -1152,6 +1290,9 @@ int hgpu_create(const hgpu_config *cfg, hgpu_ctx **out) {
             cudaMalloc(&x->fixvals, sizeof(double) * 5 * x->cap) == cudaSuccess &&
             cudaMalloc(&x->sc, sizeof(Scalars)) == cudaSuccess;
   for (int dd = 1; dd <= 3 && ok; dd++) ok = cudaMalloc(&x->F[dd], pb) == cudaSuccess;
+  if (ok && cfg->lim == HGPU_LIM_WENO5)
+    ok = cudaMalloc(&x->pL, pb) == cudaSuccess && cudaMalloc(&x->pR, pb) == cudaSuccess &&
+         cudaMalloc(&x->WA, pb * W5_PLANES) == cudaSuccess;
   if (!ok) {
     hgpu_destroy(x);
     set_err("device allocation failed");
@@ -1254,17 +1395,36 @@ int hgpu_download_state(hgpu_ctx *x, double *p, int *pflag, double *t, double *d
 // one stage: fluxes, EMFs, update, bound, post_fixup, bound
 static void launch_fluxes(hgpu_ctx *x, const double *pb) {
   const Dims &d = x->d;
-  cudaStream_t s = x->stream;
-  (void)s;
-  if (d.n1 > 1)
-    LAUNCH(x, K_FLUX1, flux_kernel<1>, grid_for(x->face_box[1].size(), 128), 128, d, x->P, x->face_box[1], pb, x->G,
-           x->F[1], x->sc);
-  if (d.n2 > 1)
-    LAUNCH(x, K_FLUX2, flux_kernel<2>, grid_for(x->face_box[2].size(), 128), 128, d, x->P, x->face_box[2], pb, x->G,
-           x->F[2], x->sc);
-  if (d.n3 > 1)
-    LAUNCH(x, K_FLUX3, flux_kernel<3>, grid_for(x->face_box[3].size(), 128), 128, d, x->P, x->face_box[3], pb, x->G,
-           x->F[3], x->sc);
+  const int nd[4] = {0, d.n1, d.n2, d.n3};
+  const int kid[4] = {0, K_FLUX1, K_FLUX2, K_FLUX3};
+  bool weno = x->P.lim == HGPU_LIM_WENO5;
+  for (int q = 1; q <= 3; q++) {
+    if (nd[q] <= 1) continue;
+    unsigned gf = grid_for(x->face_box[q].size(), 128);
+    if (weno) {
+      unsigned ga = grid_for(x->wa_box[q].size(), 128), gb = grid_for(x->wb_box[q].size(), 128);
+      if (q == 1) {
+        LAUNCH(x, K_WENO_A, weno_a_kernel<1>, ga, 128, d, x->wa_box[1], pb, x->WA);
+        LAUNCH(x, K_WENO_B, weno_b_kernel<1>, gb, 128, d, x->P, x->wb_box[1], pb, x->G, x->WA, x->pL, x->pR);
+        LAUNCH(x, kid[1], (flux_kernel<1, 1>), gf, 128, d, x->P, x->face_box[1], pb, x->pL, x->pR, x->G, x->F[1], x->sc);
+      } else if (q == 2) {
+        LAUNCH(x, K_WENO_A, weno_a_kernel<2>, ga, 128, d, x->wa_box[2], pb, x->WA);
+        LAUNCH(x, K_WENO_B, weno_b_kernel<2>, gb, 128, d, x->P, x->wb_box[2], pb, x->G, x->WA, x->pL, x->pR);
+        LAUNCH(x, kid[2], (flux_kernel<2, 1>), gf, 128, d, x->P, x->face_box[2], pb, x->pL, x->pR, x->G, x->F[2], x->sc);
+      } else {
+        LAUNCH(x, K_WENO_A, weno_a_kernel<3>, ga, 128, d, x->wa_box[3], pb, x->WA);
+        LAUNCH(x, K_WENO_B, weno_b_kernel<3>, gb, 128, d, x->P, x->wb_box[3], pb, x->G, x->WA, x->pL, x->pR);
+        LAUNCH(x, kid[3], (flux_kernel<3, 1>), gf, 128, d, x->P, x->face_box[3], pb, x->pL, x->pR, x->G, x->F[3], x->sc);
+      }
+    } else {
+      if (q == 1)
+        LAUNCH(x, kid[1], (flux_kernel<1, 0>), gf, 128, d, x->P, x->face_box[1], pb, nullptr, nullptr, x->G, x->F[1], x->sc);
+      else if (q == 2)
+        LAUNCH(x, kid[2], (flux_kernel<2, 0>), gf, 128, d, x->P, x->face_box[2], pb, nullptr, nullptr, x->G, x->F[2], x->sc);
+      else
+        LAUNCH(x, kid[3], (flux_kernel<3, 0>), gf, 128, d, x->P, x->face_box[3], pb, nullptr, nullptr, x->G, x->F[3], x->sc);
+    }
+  }
   LAUNCH(x, K_EMF, emf_kernel, grid_for(x->emf_box.size(), 256), 256, d, x->emf_box, x->F[1], x->F[2], x->F[3], x->G,
          x->E);
 }
