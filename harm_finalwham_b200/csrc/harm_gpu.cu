@@ -182,6 +182,24 @@ __device__ __forceinline__ double slope3(int lim, double yl, double yc, double y
 // ---------------------------------------------------------------------------
 constexpr int W5_PLANES = 4;
 
+// Minimum resident 128-thread blocks per SM asked of the register allocator
+// for the FP64-heavy kernels (launch_bounds' second argument).  With 64K
+// registers per SM, B blocks cap a thread at 65536 / (128 B) registers:
+// 1-2 -> 255 (8 warps/SM), 3 -> 170 (12 warps), 4 -> 128 (16 warps), more
+// warps to hide FP64 latency at the price of spills to local memory.
+#ifndef HG_MINB_FLUX
+#define HG_MINB_FLUX 1
+#endif
+#ifndef HG_MINB_UPDATE
+#define HG_MINB_UPDATE 1
+#endif
+#ifndef HG_MINB_WENO_A
+#define HG_MINB_WENO_A 1
+#endif
+#ifndef HG_MINB_WENO_B
+#define HG_MINB_WENO_B 1
+#endif
+
 template <int DIR>
 __device__ __forceinline__ long long dir_stride(const Dims &d) {
   return (DIR == 1) ? (long long)d.nt2 * d.nt3 : ((DIR == 2) ? (long long)d.nt3 : 1);
@@ -189,7 +207,7 @@ __device__ __forceinline__ long long dir_stride(const Dims &d) {
 
 // pass A over line cells -4..n+3: cusp test, SMONO indicator, unoptimised weights
 template <int DIR>
-__global__ void __launch_bounds__(128) weno_a_kernel(Dims d, Box box, const double *__restrict__ pb,
+__global__ void __launch_bounds__(128, HG_MINB_WENO_A) weno_a_kernel(Dims d, Box box, const double *__restrict__ pb,
                                                      double *__restrict__ WA) {
   long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= box.size()) return;
@@ -215,7 +233,7 @@ __global__ void __launch_bounds__(128) weno_a_kernel(Dims d, Box box, const doub
 
 // pass B over line cells -1..n: dP/P, ratios, reduction, face values
 template <int DIR>
-__global__ void __launch_bounds__(128) weno_b_kernel(Dims d, Params P, Box box, const double *__restrict__ pb,
+__global__ void __launch_bounds__(128, HG_MINB_WENO_B) weno_b_kernel(Dims d, Params P, Box box, const double *__restrict__ pb,
                                                      const double *__restrict__ G, const double *__restrict__ WA,
                                                      double *__restrict__ pL, double *__restrict__ pR) {
   long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -286,7 +304,7 @@ __global__ void __launch_bounds__(128) weno_b_kernel(Dims d, Params P, Box box, 
 // kernel, RECON 1: Riemann states from the WENO5 face values pL/pR
 // ---------------------------------------------------------------------------
 template <int DIR, int RECON>
-__global__ void __launch_bounds__(128) flux_kernel(Dims d, Params P, Box box, const double *__restrict__ pb,
+__global__ void __launch_bounds__(128, HG_MINB_FLUX) flux_kernel(Dims d, Params P, Box box, const double *__restrict__ pb,
                                                    const double *__restrict__ pL, const double *__restrict__ pR,
                                                    const double *__restrict__ G, double *__restrict__ F,
                                                    Scalars *sc) {
@@ -422,7 +440,7 @@ __global__ void __launch_bounds__(256) emf_kernel(Dims d, Box box, const double 
 // ---------------------------------------------------------------------------
 // zone update: advance_standard's CZLOOP body (advance.c:143-213)
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(128) update_kernel(Dims d, Params P, Box box, const double *pi, const double *pb,
+__global__ void __launch_bounds__(128, HG_MINB_UPDATE) update_kernel(Dims d, Params P, Box box, const double *pi, const double *pb,
                                                      double *pf, double *__restrict__ uf, double *__restrict__ ucum,
                                                      const double *__restrict__ F1, const double *__restrict__ F2,
                                                      const double *__restrict__ F3, const double *__restrict__ E,
