@@ -254,6 +254,34 @@ def bench_ours(args, rank, world):
         return {"metric": METRIC, "value": value, "unit": "zone-updates/s", "note": "kernels-only run",
                 "ms_per_step": ms_max / args.steps, "gpu_launches": launches}
 
+    # the other precision mode on the same initial state: its rate and its
+    # error against this run after the same number of steps
+    other = None
+    if not args.no_compare:
+        other_prec = "mixed" if args.precision == "fp64" else "fp64"
+        p_this, _, _, _ = g.download_state()
+        g2 = HarmGPU(n1, n2, n3, dom.ng, dom.dx, lim=lim, flux=flux, precision=other_prec, gam=dom.gam, cour=dom.cour)
+        g2.upload_geometry(dom.gcov, dom.gcon, dom.gcovpert, dom.gdet, dom.conn, dom.floors)
+        g2.upload_state(dom.p, dom.pflag, 0.0, 0.0)
+        g2.init_dt()
+        g2.step_ch(args.warmup)
+        barrier()
+        ms2, st2 = g2.step_ch_timed(args.steps)
+        barrier()
+        ms2 = allmax(ms2)
+        p_other, _, _, _ = g2.download_state()
+        g2.close()
+        p64, p32 = (p_this, p_other) if args.precision == "fp64" else (p_other, p_this)
+        a32, a64 = g.active(p32), g.active(p64)
+        names = ["rho", "u", "u1", "u2", "u3", "B1", "B2", "B3"]
+        err = {nm: float(np.abs(a32[..., q] - a64[..., q]).sum() / np.abs(a64[..., q]).sum())
+               for q, nm in enumerate(names)}
+        other = {"precision": other_prec, "value": zones * args.steps * world / (ms2 / 1e3),
+                 "ms_per_step": ms2 / args.steps, "steps_compared": args.warmup + args.steps,
+                 "rel_l1_mixed_vs_fp64": err,
+                 "note": "mixed = FP32 reconstruction, wave speeds and Riemann fluxes; FP64 flux-CT, conserved "
+                         "update, con-to-prim and fixups; both runs from the same initial state"}
+
     # per-kernel device times for the roofline (a separate profiled pass)
     g.set_profiling(True)
     prof_steps = max(2, min(args.steps, 5))
@@ -314,6 +342,8 @@ def bench_ours(args, rank, world):
         "e2e": e2e,
         "clocks": clk,
     }
+    if other is not None:
+        result["other_precision"] = other
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         procs = min(host_cores(), args.cpu_procs)
         cs = cpu_sample(lim)
@@ -393,6 +423,8 @@ def main():
     ap.add_argument("--workload", default=DEFAULT_WORKLOAD, choices=sorted(WORKLOADS))
     ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-compare", action="store_true",
+                    help="skip the run of the other precision mode (rate and error vs FP64)")
     ap.add_argument("--e2e-steps", type=int, default=5)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-steps", type=int, default=3)

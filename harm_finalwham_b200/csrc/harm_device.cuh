@@ -46,38 +46,62 @@ constexpr int ERR_VSQ_NEG = 16;
 constexpr int ERR_NONFINITE_SPEED = 32;
 constexpr int ERR_PREF_NEG = 64;
 
+// Tolerances of the reference's round-off guards, per arithmetic type.  The
+// FP64 values are the reference's own (NUMEPSILON = DBL_EPSILON, global.h);
+// the FP32 ones scale the same guards to FP32 round-off for the mixed
+// precision path (reconstruction, wave speeds and Riemann fluxes in FP32).
+template <typename T> struct Tol;
+template <> struct Tol<double> {
+  static constexpr double numeps = NUMEPSILON;       // gamma_calc, vchar cms2 guards
+  static constexpr double discr = 1E-10;             // simplefast discriminant (vchar.c:268)
+  static constexpr double cs2cap = 1e-9;             // vchar cs2 cap (vchar.c:77)
+};
+template <> struct Tol<float> {
+  static constexpr float numeps = 1.1920929e-07f;    // FLT_EPSILON
+  static constexpr float discr = 1E-5f;
+  static constexpr float cs2cap = 1e-6f;
+};
+
 // Metric at one grid location.  gcov is stored in full because the
 // reference's gcov is not exactly symmetric (differences ~1e-13) and its
 // routines read different triangles in different places.
-struct Metric {
-  double gcov[16];
-  double gcon[16];
-  double gcovpert_tt;
-  double g;
+template <typename T>
+struct MetricT {
+  T gcov[16];
+  T gcon[16];
+  T gcovpert_tt;
+  T g;
 };
+using Metric = MetricT<double>;
 
-struct State {
-  double ucon[4], ucov[4], bcon[4], bcov[4];
+template <typename T>
+struct StateT {
+  T ucon[4], ucov[4], bcon[4], bcov[4];
 };
+using State = StateT<double>;
 
 // Per-state electromagnetic pieces reused by every T^dir_mu row
 // (Mcon_calc phys.c:178, lower_A phys.ffde.c:1707, Msq and 1+u_t).
-struct EM {
-  double Mcon[4][4];
-  double Mcov[4][4];
-  double Msq;
-  double plus1ud0;
+template <typename T>
+struct EMT {
+  T Mcon[4][4];
+  T Mcov[4][4];
+  T Msq;
+  T plus1ud0;
 };
+using EM = EMT<double>;
 
 #define GCOV(m, a, b) ((m).gcov[(a) * 4 + (b)])
 #define GCON(m, a, b) ((m).gcon[(a) * 4 + (b)])
 
-__device__ __forceinline__ double dot4(const double *a, const double *b) {
+template <typename T>
+__device__ __forceinline__ T dot4(const T *a, const T *b) {
   return a[0] * b[0] + a[1] * b[1] + a[2] * b[2] + a[3] * b[3];
 }
 
 // lower_vec (phys.c:766-787)
-__device__ __forceinline__ void lower_vec(const double *ucon, const Metric &m, double *ucov) {
+template <typename T>
+__device__ __forceinline__ void lower_vec(const T *ucon, const MetricT<T> &m, T *ucov) {
   ucov[0] = GCOV(m, 0, 0) * ucon[0] + GCOV(m, 0, 1) * ucon[1] + GCOV(m, 0, 2) * ucon[2] + GCOV(m, 0, 3) * ucon[3];
   ucov[1] = GCOV(m, 0, 1) * ucon[0] + GCOV(m, 1, 1) * ucon[1] + GCOV(m, 1, 2) * ucon[2] + GCOV(m, 1, 3) * ucon[3];
   ucov[2] = GCOV(m, 0, 2) * ucon[0] + GCOV(m, 1, 2) * ucon[1] + GCOV(m, 2, 2) * ucon[2] + GCOV(m, 2, 3) * ucon[3];
@@ -85,7 +109,8 @@ __device__ __forceinline__ void lower_vec(const double *ucon, const Metric &m, d
 }
 
 // raise_vec (phys.c:826-846)
-__device__ __forceinline__ void raise_vec(const double *ucov, const Metric &m, double *ucon) {
+template <typename T>
+__device__ __forceinline__ void raise_vec(const T *ucov, const MetricT<T> &m, T *ucon) {
   ucon[0] = GCON(m, 0, 0) * ucov[0] + GCON(m, 0, 1) * ucov[1] + GCON(m, 0, 2) * ucov[2] + GCON(m, 0, 3) * ucov[3];
   ucon[1] = GCON(m, 0, 1) * ucov[0] + GCON(m, 1, 1) * ucov[1] + GCON(m, 1, 2) * ucov[2] + GCON(m, 1, 3) * ucov[3];
   ucon[2] = GCON(m, 0, 2) * ucov[0] + GCON(m, 1, 2) * ucov[1] + GCON(m, 2, 2) * ucov[2] + GCON(m, 2, 3) * ucov[3];
@@ -93,30 +118,33 @@ __device__ __forceinline__ void raise_vec(const double *ucov, const Metric &m, d
 }
 
 // qsq_calc (phys.c:1077-1090) on the relative 4-velocity u~^i
-__device__ __forceinline__ double qsq_calc(double u1, double u2, double u3, const Metric &m) {
+template <typename T>
+__device__ __forceinline__ T qsq_calc(T u1, T u2, T u3, const MetricT<T> &m) {
   return +GCOV(m, 1, 1) * u1 * u1 + GCOV(m, 2, 2) * u2 * u2 + GCOV(m, 3, 3) * u3 * u3 +
-         2. * (GCOV(m, 1, 2) * u1 * u2 + GCOV(m, 1, 3) * u1 * u3 + GCOV(m, 2, 3) * u2 * u3);
+         T(2.) * (GCOV(m, 1, 2) * u1 * u2 + GCOV(m, 1, 3) * u1 * u3 + GCOV(m, 2, 3) * u2 * u3);
 }
 
 // gamma_calc (phys.c:1022-1074); returns nonzero if qsq is negative beyond
 // round-off (the reference calls fail(FAIL_UTCALC_DISCR))
-__device__ __forceinline__ int gamma_calc(const double *pr, const Metric &m, double *gamma) {
-  double qsq = qsq_calc(pr[U1], pr[U2], pr[U3], m);
-  if (qsq < 0.0) {
-    if (qsq > -NUMEPSILON * 100) qsq = 0.0;
+template <typename T>
+__device__ __forceinline__ int gamma_calc(const T *pr, const MetricT<T> &m, T *gamma) {
+  T qsq = qsq_calc(pr[U1], pr[U2], pr[U3], m);
+  if (qsq < T(0.0)) {
+    if (qsq > -Tol<T>::numeps * T(100)) qsq = T(0.0);
     else return 1;
   }
-  *gamma = sqrt(1. + qsq);
+  *gamma = sqrt(T(1.) + qsq);
   return 0;
 }
 
 // ucon_calc_rel4vel (phys.c:983-1019)
-__device__ __forceinline__ int ucon_calc(const double *pr, const Metric &m, double *ucon) {
-  double alpha = 1. / sqrt(-GCON(m, 0, 0));
-  double beta1 = GCON(m, 0, 1) * alpha * alpha;
-  double beta2 = GCON(m, 0, 2) * alpha * alpha;
-  double beta3 = GCON(m, 0, 3) * alpha * alpha;
-  double gamma;
+template <typename T>
+__device__ __forceinline__ int ucon_calc(const T *pr, const MetricT<T> &m, T *ucon) {
+  T alpha = T(1.) / sqrt(-GCON(m, 0, 0));
+  T beta1 = GCON(m, 0, 1) * alpha * alpha;
+  T beta2 = GCON(m, 0, 2) * alpha * alpha;
+  T beta3 = GCON(m, 0, 3) * alpha * alpha;
+  T gamma;
   if (gamma_calc(pr, m, &gamma)) return 1;
   ucon[0] = gamma / alpha;
   ucon[1] = pr[U1] - ucon[0] * beta1;
@@ -126,7 +154,8 @@ __device__ __forceinline__ int ucon_calc(const double *pr, const Metric &m, doub
 }
 
 // get_state (phys.c:849-859) with bcon_calc (phys.c:309-318)
-__device__ __forceinline__ int get_state(const double *pr, const Metric &m, State &q) {
+template <typename T>
+__device__ __forceinline__ int get_state(const T *pr, const MetricT<T> &m, StateT<T> &q) {
   if (ucon_calc(pr, m, q.ucon)) return 1;
   lower_vec(q.ucon, m, q.ucov);
   q.bcon[0] = pr[B1] * q.ucov[1] + pr[B2] * q.ucov[2] + pr[B3] * q.ucov[3];
@@ -137,31 +166,33 @@ __device__ __forceinline__ int get_state(const double *pr, const Metric &m, Stat
 }
 
 // compute_1plusud0 (phys.c:541-575)
-__device__ __forceinline__ double compute_1plusud0(const Metric &m, const State &q) {
-  double vcon[4];
+template <typename T>
+__device__ __forceinline__ T compute_1plusud0(const MetricT<T> &m, const StateT<T> &q) {
+  T vcon[4];
 #pragma unroll
   for (int j = 1; j < 4; j++) vcon[j] = q.ucon[j] / q.ucon[0];
-  double plus1gv00 = m.gcovpert_tt;
-  double vsq = m.gcovpert_tt;
+  T plus1gv00 = m.gcovpert_tt;
+  T vsq = m.gcovpert_tt;
 #pragma unroll
-  for (int j = 1; j < 4; j++) vsq += 2.0 * GCOV(m, 0, j) * vcon[j];
+  for (int j = 1; j < 4; j++) vsq += T(2.0) * GCOV(m, 0, j) * vcon[j];
 #pragma unroll
   for (int j = 1; j < 4; j++)
 #pragma unroll
     for (int k = 1; k < 4; k++) vsq += GCOV(m, j, k) * vcon[j] * vcon[k];
-  double gvtt = GCOV(m, 0, 0);
-  double alpha = 0.0;
+  T gvtt = GCOV(m, 0, 0);
+  T alpha = T(0.0);
 #pragma unroll
   for (int j = 1; j < 4; j++) alpha += GCOV(m, j, 0) * q.ucon[j];
-  double uu0 = q.ucon[0];
-  return alpha + ((1.0 - gvtt) * plus1gv00 - uu0 * uu0 * vsq * gvtt * gvtt) / (1.0 - gvtt * uu0);
+  T uu0 = q.ucon[0];
+  return alpha + ((T(1.0) - gvtt) * plus1gv00 - uu0 * uu0 * vsq * gvtt * gvtt) / (T(1.0) - gvtt * uu0);
 }
 
 // Mcon_calc PRIMMAXWELL (phys.c:178-210), lower_A (phys.ffde.c:1707-1735),
 // Msq (phys.ffde.c:1507) and 1+u_t
-__device__ __forceinline__ void em_prepare(const double *pr, const Metric &m, const State &q, EM &e) {
+template <typename T>
+__device__ __forceinline__ void em_prepare(const T *pr, const MetricT<T> &m, const StateT<T> &q, EMT<T> &e) {
 #pragma unroll
-  for (int j = 0; j < 4; j++) e.Mcon[j][j] = 0.0;
+  for (int j = 0; j < 4; j++) e.Mcon[j][j] = T(0.0);
 #pragma unroll
   for (int k = 1; k < 4; k++) {
     e.Mcon[k][0] = pr[B1 + k - 1];
@@ -171,12 +202,12 @@ __device__ __forceinline__ void em_prepare(const double *pr, const Metric &m, co
   for (int j = 1; j < 4; j++)
 #pragma unroll
     for (int k = 1; k < 4; k++) e.Mcon[j][k] = (pr[B1 + j - 1] * q.ucon[k] - pr[B1 + k - 1] * q.ucon[j]) / q.ucon[0];
-  double a01 = 0., a02 = 0., a03 = 0., a12 = 0., a23 = 0., a31 = 0.;
+  T a01 = T(0.), a02 = T(0.), a03 = T(0.), a12 = T(0.), a23 = T(0.), a31 = T(0.);
 #pragma unroll
   for (int j = 0; j < 4; j++)
 #pragma unroll
     for (int k = 0; k < 4; k++) {
-      double A = e.Mcon[j][k];
+      T A = e.Mcon[j][k];
       a01 += (GCOV(m, 0, j)) * (GCOV(m, 1, k)) * A;
       a02 += (GCOV(m, 0, j)) * (GCOV(m, 2, k)) * A;
       a03 += (GCOV(m, 0, j)) * (GCOV(m, 3, k)) * A;
@@ -184,10 +215,10 @@ __device__ __forceinline__ void em_prepare(const double *pr, const Metric &m, co
       a23 += (GCOV(m, 2, j)) * (GCOV(m, 3, k)) * A;
       a31 += (GCOV(m, 3, j)) * (GCOV(m, 1, k)) * A;
     }
-  e.Mcov[0][0] = 0.;
-  e.Mcov[1][1] = 0.;
-  e.Mcov[2][2] = 0.;
-  e.Mcov[3][3] = 0.;
+  e.Mcov[0][0] = T(0.);
+  e.Mcov[1][1] = T(0.);
+  e.Mcov[2][2] = T(0.);
+  e.Mcov[3][3] = T(0.);
   e.Mcov[0][1] = a01;
   e.Mcov[0][2] = a02;
   e.Mcov[0][3] = a03;
@@ -200,7 +231,7 @@ __device__ __forceinline__ void em_prepare(const double *pr, const Metric &m, co
   e.Mcov[2][1] = -a12;
   e.Mcov[3][2] = -a23;
   e.Mcov[1][3] = -a31;
-  double Msq = 0.;
+  T Msq = T(0.);
 #pragma unroll
   for (int j = 0; j < 4; j++)
 #pragma unroll
@@ -211,30 +242,32 @@ __device__ __forceinline__ void em_prepare(const double *pr, const Metric &m, co
 
 // mhd_calc_norestmass (phys.c:442-506) + ffdestresstensor_dir
 // (phys.ffde.c:1483-1515): one row T^dir_mu without rest mass
-__device__ __forceinline__ void mhd_row(const double *pr, int dir, double gam, const State &q, const EM &e, double *mhd) {
-  double rho = pr[RHO], u = pr[UU];
-  double P = (gam - 1.) * u;
-  double w = P + rho + u;
-  double eta = w, ptot = P;
-  mhd[0] = (P + u) * q.ucon[dir] * q.ucov[0] + rho * q.ucon[dir] * e.plus1ud0 + ptot * ((dir == 0) ? 1. : 0.);
+template <typename T>
+__device__ __forceinline__ void mhd_row(const T *pr, int dir, T gam, const StateT<T> &q, const EMT<T> &e, T *mhd) {
+  T rho = pr[RHO], u = pr[UU];
+  T P = (gam - T(1.)) * u;
+  T w = P + rho + u;
+  T eta = w, ptot = P;
+  mhd[0] = (P + u) * q.ucon[dir] * q.ucov[0] + rho * q.ucon[dir] * e.plus1ud0 + ptot * ((dir == 0) ? T(1.) : T(0.));
 #pragma unroll
-  for (int j = 1; j < 4; j++) mhd[j] = eta * q.ucon[dir] * q.ucov[j] + ptot * ((dir == j) ? 1. : 0.);
-  double TEM[4];
+  for (int j = 1; j < 4; j++) mhd[j] = eta * q.ucon[dir] * q.ucov[j] + ptot * ((dir == j) ? T(1.) : T(0.));
+  T TEM[4];
 #pragma unroll
   for (int j = 0; j < 4; j++) {
-    TEM[j] = 0.;
+    TEM[j] = T(0.);
 #pragma unroll
     for (int i = 0; i < 4; i++) TEM[j] += e.Mcon[dir][i] * e.Mcov[j][i];
   }
-  TEM[dir] -= 0.25 * e.Msq;
+  TEM[dir] -= T(0.25) * e.Msq;
 #pragma unroll
   for (int j = 0; j < 4; j++) mhd[j] += TEM[j];
 }
 
 // primtoflux (phys.c:16-55), UEVOLVE, every EOM factor = gdet
-__device__ __forceinline__ void primtoflux(const double *pr, const State &q, const EM &e, int dir, const Metric &m,
-                                           double gam, double *flux) {
-  double fin[NPR];
+template <typename T>
+__device__ __forceinline__ void primtoflux(const T *pr, const StateT<T> &q, const EMT<T> &e, int dir,
+                                           const MetricT<T> &m, T gam, T *flux) {
+  T fin[NPR];
   fin[RHO] = pr[RHO] * q.ucon[dir];
   mhd_row(pr, dir, gam, q, e, &fin[UU]);
   if (dir > 0) {
@@ -251,29 +284,31 @@ __device__ __forceinline__ void primtoflux(const double *pr, const State &q, con
 }
 
 // simplefast (vchar.c:213-312) with Acov = e_dir, Bcov = e_t
-__device__ __forceinline__ int simplefast(int dir, const Metric &m, const State &q, double cms2, double *vmin,
-                                          double *vmax) {
-  double Acov[4] = {0., 0., 0., 0.}, Bcov[4] = {0., 0., 0., 0.}, Acon[4], Bcon[4];
-  Acov[dir] = 1.;
+template <typename T>
+__device__ __forceinline__ int simplefast(int dir, const MetricT<T> &m, const StateT<T> &q, T cms2, T *vmin,
+                                          T *vmax) {
+  T Acov[4] = {T(0.), T(0.), T(0.), T(0.)}, Bcov[4] = {T(0.), T(0.), T(0.), T(0.)}, Acon[4], Bcon[4];
+  Acov[dir] = T(1.);
   raise_vec(Acov, m, Acon);
-  Bcov[0] = 1.;
+  Bcov[0] = T(1.);
   raise_vec(Bcov, m, Bcon);
-  double Asq = dot4(Acon, Acov);
-  double Bsq = dot4(Bcon, Bcov);
-  double Au = dot4(Acov, q.ucon);
-  double Bu = dot4(Bcov, q.ucon);
-  double AB = dot4(Acon, Bcov);
-  double Au2 = Au * Au;
-  double Bu2 = Bu * Bu;
-  double AuBu = Au * Bu;
-  double A = Bu2 * (1.0 - cms2) - Bsq * cms2;
-  double B = 2. * (AuBu * (1.0 - cms2) - AB * cms2);
-  double discr = 4.0 * cms2 * ((AB * AB - Asq * Bsq) * cms2 + (2.0 * AB * Au * Bu - Asq * Bu2 - Bsq * Au2) * (cms2 - 1.0));
-  if ((discr < 0.0) && (discr > -1E-10)) discr = 0.0;
-  else if (discr < 0.0) return ERR_VCHAR_DISCR;
+  T Asq = dot4(Acon, Acov);
+  T Bsq = dot4(Bcon, Bcov);
+  T Au = dot4(Acov, q.ucon);
+  T Bu = dot4(Bcov, q.ucon);
+  T AB = dot4(Acon, Bcov);
+  T Au2 = Au * Au;
+  T Bu2 = Bu * Bu;
+  T AuBu = Au * Bu;
+  T A = Bu2 * (T(1.0) - cms2) - Bsq * cms2;
+  T B = T(2.) * (AuBu * (T(1.0) - cms2) - AB * cms2);
+  T discr = T(4.0) * cms2 *
+            ((AB * AB - Asq * Bsq) * cms2 + (T(2.0) * AB * Au * Bu - Asq * Bu2 - Bsq * Au2) * (cms2 - T(1.0)));
+  if ((discr < T(0.0)) && (discr > -Tol<T>::discr)) discr = T(0.0);
+  else if (discr < T(0.0)) return ERR_VCHAR_DISCR;
   discr = sqrt(discr);
-  double vm = -(-B + discr) / (2. * A);
-  double vp = -(-B - discr) / (2. * A);
+  T vm = -(-B + discr) / (T(2.) * A);
+  T vp = -(-B - discr) / (T(2.) * A);
   if ((!isfinite(vm)) || (!isfinite(vp))) return ERR_NONFINITE_SPEED;
   if (vp < vm) {
     *vmax = vm;
@@ -286,39 +321,42 @@ __device__ __forceinline__ int simplefast(int dir, const Metric &m, const State 
 }
 
 // vchar (vchar.c:37-171)
-__device__ __forceinline__ int vchar(const double *pr, const State &q, int dir, const Metric &m, double gam,
-                                     double *vmax, double *vmin) {
-  double bsq = dot4(q.bcon, q.bcov);
-  double rho = pr[RHO], u = pr[UU], cs2, va2, EF, WW, P;
-  if (u < 0) u = 0;
-  if (rho < 0) rho = 0;
-  P = (gam - 1.) * u;
+template <typename T>
+__device__ __forceinline__ int vchar(const T *pr, const StateT<T> &q, int dir, const MetricT<T> &m, T gam, T *vmax,
+                                     T *vmin) {
+  T bsq = dot4(q.bcon, q.bcov);
+  T rho = pr[RHO], u = pr[UU], cs2, va2, EF, WW, P;
+  if (u < T(0)) u = T(0);
+  if (rho < T(0)) rho = T(0);
+  P = (gam - T(1.)) * u;
   WW = rho + u + P;
-  if (WW > 0.0) {
-    double pressure = (gam - 1.) * u;
-    double h = rho + u + pressure;
+  if (WW > T(0.0)) {
+    T pressure = (gam - T(1.)) * u;
+    T h = rho + u + pressure;
     cs2 = gam * pressure / h;
-  } else WW = cs2 = 0.0;
-  if (cs2 >= 1.0) cs2 = 1.0 - 1e-9;
-  else if (cs2 <= 0.0) cs2 = 0.0;
+  } else WW = cs2 = T(0.0);
+  if (cs2 >= T(1.0)) cs2 = T(1.0) - Tol<T>::cs2cap;
+  else if (cs2 <= T(0.0)) cs2 = T(0.0);
   EF = bsq + WW;
-  if (EF > 0.0) va2 = bsq / EF;
-  else EF = va2 = 0.0;
-  double cms2 = cs2 + va2 - cs2 * va2;
-  if (cms2 < 0.0) {
-    if (cms2 / (cs2 + va2) > -NUMEPSILON * 100.0) cms2 = 0.0;
+  if (EF > T(0.0)) va2 = bsq / EF;
+  else EF = va2 = T(0.0);
+  T cms2 = cs2 + va2 - cs2 * va2;
+  if (cms2 < T(0.0)) {
+    if (cms2 / (cs2 + va2) > -Tol<T>::numeps * T(100.0)) cms2 = T(0.0);
     else return ERR_COEFF_NEG;
   }
-  if (cms2 > 1.) {
-    if (cms2 < 1.0 + NUMEPSILON * 100.0) cms2 = 1.0;
-    else if (rho < 0.0) cms2 = 1.0;
+  if (cms2 > T(1.)) {
+    if (cms2 < T(1.0) + Tol<T>::numeps * T(100.0)) cms2 = T(1.0);
+    else if (rho < T(0.0)) cms2 = T(1.0);
     else return ERR_COEFF_SUP;
   }
   return simplefast(dir, m, q, cms2, vmin, vmax);
 }
 
-__device__ __forceinline__ double max_ref(double a, double b) { return (a > b) ? a : b; }  // phys.c:1797
-__device__ __forceinline__ double min_ref(double a, double b) { return (a > b) ? b : a; }  // phys.c:1804
+template <typename T>
+__device__ __forceinline__ T max_ref(T a, T b) { return (a > b) ? a : b; }  // phys.c:1797
+template <typename T>
+__device__ __forceinline__ T min_ref(T a, T b) { return (a > b) ? b : a; }  // phys.c:1804
 __device__ __forceinline__ double min_macro(double a, double b) { return ((a) < (b)) ? (a) : (b); }  // global.h:751
 
 // limit_gamma (fixup.c:1859-1905); returns -1 if it changed pr

@@ -76,11 +76,27 @@ struct Dims {
   long long nz, nij;
 };
 
+// One instance of a batch: a 1D problem occupying the x1 cells
+// i0-ng .. i0+n+ng-1 of the concatenated line (its own ghosts included),
+// with its own gamma, dx, time and dt (step_ch's t, dt, tf per problem).
+struct Inst {
+  int i0, n;
+  double dx, gam, tf;
+  double t, dt;
+  unsigned long long ndtbits;  // x1 min of cour*dx/ctop as ordered bits
+  int done;                    // t reached tf: the instance no longer advances
+  int nsteps;                  // time steps this instance has taken
+};
+
 struct Params {
   double gam, cour, gammamax, gammafail, rhominlimit, uuminlimit, defcon, safe, tf;
   double dx1, dx2, dx3;
   int lim, flux;
   int bc[6];
+  // batch of independent 1D instances (nullptr: one domain)
+  const int *cell_inst;  // instance of every cell of the line
+  Inst *inst;
+  int ninst;
 };
 
 // device scalars
@@ -151,27 +167,63 @@ __device__ __forceinline__ void warp_min_atomic(unsigned long long *dst, double 
 }
 
 // MC / VANL / MINM / DONOR slopes (interppoint.c:387-443)
-__device__ __forceinline__ double slope3(int lim, double yl, double yc, double yr) {
+template <typename T>
+__device__ __forceinline__ T slope3(int lim, T yl, T yc, T yr) {
   if (lim == HGPU_LIM_MC) {
-    double Dqm = 2.0 * (yc - yl);
-    double Dqp = 2.0 * (yr - yc);
-    double Dqc = 0.5 * (yr - yl);
-    double mm = ((Dqm) * (Dqp) <= 0) ? 0.0 : ((fabs(Dqm) < fabs(Dqp)) ? (Dqm) : (Dqp));
-    return ((Dqc) * (mm) <= 0) ? 0.0 : ((fabs(Dqc) < fabs(mm)) ? (Dqc) : (mm));
+    T Dqm = T(2.0) * (yc - yl);
+    T Dqp = T(2.0) * (yr - yc);
+    T Dqc = T(0.5) * (yr - yl);
+    T mm = ((Dqm) * (Dqp) <= T(0)) ? T(0.0) : ((fabs(Dqm) < fabs(Dqp)) ? (Dqm) : (Dqp));
+    return ((Dqc) * (mm) <= T(0)) ? T(0.0) : ((fabs(Dqc) < fabs(mm)) ? (Dqc) : (mm));
   } else if (lim == HGPU_LIM_VANL) {
-    double Dqm = (yc - yl);
-    double Dqp = (yr - yc);
-    double s = Dqm * Dqp;
-    if (s <= 0.) return 0.;
-    return (2.0 * s / (Dqm + Dqp));
+    T Dqm = (yc - yl);
+    T Dqp = (yr - yc);
+    T s = Dqm * Dqp;
+    if (s <= T(0.)) return T(0.);
+    return (T(2.0) * s / (Dqm + Dqp));
   } else if (lim == HGPU_LIM_MINM) {
-    double Dqm = 1.0 * (yc - yl);
-    double Dqp = 1.0 * (yr - yc);
-    double Dqc = 0.5 * (yr - yl);
-    double mm = ((Dqm) * (Dqc) <= 0) ? 0.0 : ((fabs(Dqm) < fabs(Dqc)) ? (Dqm) : (Dqc));
-    return ((mm) * (Dqp) <= 0) ? 0.0 : ((fabs(mm) < fabs(Dqp)) ? (mm) : (Dqp));
+    T Dqm = T(1.0) * (yc - yl);
+    T Dqp = T(1.0) * (yr - yc);
+    T Dqc = T(0.5) * (yr - yl);
+    T mm = ((Dqm) * (Dqc) <= T(0)) ? T(0.0) : ((fabs(Dqm) < fabs(Dqc)) ? (Dqm) : (Dqc));
+    return ((mm) * (Dqp) <= T(0)) ? T(0.0) : ((fabs(mm) < fabs(Dqp)) ? (mm) : (Dqp));
   }
-  return 0.0;
+  return T(0.0);
+}
+
+// para4 (interppoint.c:736-869) with PARA2LIM=MC and JONPARAREDUCE=0: face
+// values of the cell at y[0] from y[-2..2]
+template <typename T>
+__device__ __forceinline__ void para4(const T *y, T *lout, T *rout) {
+  T dq[3];
+#pragma unroll
+  for (int mm = -1; mm <= 1; mm++) {
+    T Dqm = T(2.0) * (y[mm] - y[mm - 1]);
+    T Dqp = T(2.0) * (y[mm + 1] - y[mm]);
+    T Dqc = T(0.5) * (y[mm + 1] - y[mm - 1]);
+    T aDqm = fabs(Dqm), aDqp = fabs(Dqp), aDqc = fabs(Dqc);
+    T s = Dqm * Dqp;
+    T sg = (Dqc > T(0.0)) ? T(1.0) : ((Dqc < T(0.0)) ? T(-1.0) : T(0.0));
+    dq[mm + 1] = (s <= T(0.)) ? T(0.) : min_ref(aDqc, min_ref(aDqm, aDqp)) * sg;
+  }
+  T l = T(0.5) * (y[0] + y[-1]) - (dq[1] - dq[0]) / T(8.0);
+  T r = T(0.5) * (y[1] + y[0]) - (dq[2] - dq[1]) / T(8.0);
+  l = max_ref(min_ref(y[0], y[-1]), l);
+  l = min_ref(max_ref(y[0], y[-1]), l);
+  r = max_ref(min_ref(y[0], y[1]), r);
+  r = min_ref(max_ref(y[0], y[1]), r);
+  T qa = (r - y[0]) * (y[0] - l);
+  T qd = (r - l);
+  T qe = T(6.0) * (y[0] - T(0.5) * (l + r));
+  if (qa <= T(0.)) {
+    l = y[0];
+    r = y[0];
+  } else {
+    if (qd * (qd - qe) < T(0.0)) l = T(3.0) * y[0] - T(2.0) * r;
+    if (qd * (qd + qe) < T(0.0)) r = T(3.0) * y[0] - T(2.0) * l;
+  }
+  *lout = l;
+  *rout = r;
 }
 
 // ---------------------------------------------------------------------------
@@ -187,28 +239,63 @@ constexpr int W5_PLANES = 4;
 // registers per SM, B blocks cap a thread at 65536 / (128 B) registers:
 // 1-2 -> 255 (8 warps/SM), 3 -> 170 (12 warps), 4 -> 128 (16 warps), more
 // warps to hide FP64 latency at the price of spills to local memory.
+// Defaults from a B200 sweep (256x128x128 torus, 1/3/4/5 blocks for flux and
+// update, 1/5/6/8 for weno_b, 1/8/10 for weno_a): flux 4 (-11% WENO5, -21%
+// MC), weno_b 8 (-33%), weno_a 8 (-3%); update is fastest unconstrained.
 #ifndef HG_MINB_FLUX
-#define HG_MINB_FLUX 1
+#define HG_MINB_FLUX 4
 #endif
 #ifndef HG_MINB_UPDATE
 #define HG_MINB_UPDATE 1
 #endif
 #ifndef HG_MINB_WENO_A
-#define HG_MINB_WENO_A 1
+#define HG_MINB_WENO_A 8
 #endif
 #ifndef HG_MINB_WENO_B
-#define HG_MINB_WENO_B 1
+#define HG_MINB_WENO_B 8
 #endif
+// the same for the FP32 kernels of the mixed-precision path (B200 sweep of
+// 4/6/8 for flux, 8/10/12 for weno_a/b: flux 8 -4%, the rest within 2%)
+#ifndef HG_MINB_FLUX_F32
+#define HG_MINB_FLUX_F32 8
+#endif
+#ifndef HG_MINB_WENO_A_F32
+#define HG_MINB_WENO_A_F32 12
+#endif
+#ifndef HG_MINB_WENO_B_F32
+#define HG_MINB_WENO_B_F32 8
+#endif
+template <typename T> struct MinBlocks;
+template <> struct MinBlocks<double> {
+  static constexpr int flux = HG_MINB_FLUX, weno_a = HG_MINB_WENO_A, weno_b = HG_MINB_WENO_B;
+};
+template <> struct MinBlocks<float> {
+  static constexpr int flux = HG_MINB_FLUX_F32, weno_a = HG_MINB_WENO_A_F32, weno_b = HG_MINB_WENO_B_F32;
+};
 
 template <int DIR>
 __device__ __forceinline__ long long dir_stride(const Dims &d) {
   return (DIR == 1) ? (long long)d.nt2 * d.nt3 : ((DIR == 2) ? (long long)d.nt3 : 1);
 }
 
-// pass A over line cells -4..n+3: cusp test, SMONO indicator, unoptimised weights
-template <int DIR>
-__global__ void __launch_bounds__(128, HG_MINB_WENO_A) weno_a_kernel(Dims d, Box box, const double *__restrict__ pb,
-                                                     double *__restrict__ WA) {
+// metric of one location converted to the arithmetic type of a kernel
+template <typename T>
+__device__ __forceinline__ void load_metric_t(const double *__restrict__ G, const Dims &d, long long ij, int slot,
+                                              MetricT<T> &m) {
+  const double *b = G + (long long)slot * GLOC * d.nij + ij;
+#pragma unroll
+  for (int q = 0; q < 16; q++) m.gcov[q] = (T)__ldg(b + (long long)q * d.nij);
+#pragma unroll
+  for (int q = 0; q < 16; q++) m.gcon[q] = (T)__ldg(b + (long long)(16 + q) * d.nij);
+  m.gcovpert_tt = (T)__ldg(b + (long long)32 * d.nij);
+  m.g = (T)__ldg(b + (long long)33 * d.nij);
+}
+
+// pass A over line cells -4..n+3: cusp test, SMONO indicator, unoptimised
+// weights.  T = double: the reference's arithmetic; T = float: mixed path.
+template <int DIR, typename T>
+__global__ void __launch_bounds__(128, MinBlocks<T>::weno_a) weno_a_kernel(Dims d, Box box, const double *__restrict__ pb,
+                                                                     T *__restrict__ WA) {
   long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= box.size()) return;
   int i, j, k;
@@ -217,14 +304,14 @@ __global__ void __launch_bounds__(128, HG_MINB_WENO_A) weno_a_kernel(Dims d, Box
   const long long o = dir_stride<DIR>(d);
   for (int v = 0; v < NPR; v++) {
     const double *q = pb + (long long)v * d.nz + z;
-    double ya[5] = {__ldg(q - 2 * o), __ldg(q - o), __ldg(q), __ldg(q + o), __ldg(q + 2 * o)};
-    const double *y = ya + 2;
+    T ya[5] = {(T)__ldg(q - 2 * o), (T)__ldg(q - o), (T)__ldg(q), (T)__ldg(q + o), (T)__ldg(q + 2 * o)};
+    const T *y = ya + 2;
     bool c = w5::cusp(y);
-    double m0 = c ? 0.0 : w5::mono(y);
-    double w[3];
+    T m0 = c ? T(0.0) : w5::mono(y);
+    T w[3];
     w5::unopt3(m0, y, w);
-    double *out = WA + (long long)v * W5_PLANES * d.nz + z;
-    out[0] = c ? -1.0 : m0;
+    T *out = WA + (long long)v * W5_PLANES * d.nz + z;
+    out[0] = c ? T(-1.0) : m0;
     out[d.nz] = w[0];
     out[2 * d.nz] = w[1];
     out[3 * d.nz] = w[2];
@@ -232,10 +319,12 @@ __global__ void __launch_bounds__(128, HG_MINB_WENO_A) weno_a_kernel(Dims d, Box
 }
 
 // pass B over line cells -1..n: dP/P, ratios, reduction, face values
-template <int DIR>
-__global__ void __launch_bounds__(128, HG_MINB_WENO_B) weno_b_kernel(Dims d, Params P, Box box, const double *__restrict__ pb,
-                                                     const double *__restrict__ G, const double *__restrict__ WA,
-                                                     double *__restrict__ pL, double *__restrict__ pR) {
+template <int DIR, typename T>
+__global__ void __launch_bounds__(128, MinBlocks<T>::weno_b) weno_b_kernel(Dims d, Params P, Box box,
+                                                                     const double *__restrict__ pb,
+                                                                     const double *__restrict__ G,
+                                                                     const T *__restrict__ WA, T *__restrict__ pL,
+                                                                     T *__restrict__ pR) {
   long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= box.size()) return;
   int i, j, k;
@@ -244,55 +333,58 @@ __global__ void __launch_bounds__(128, HG_MINB_WENO_B) weno_b_kernel(Dims d, Par
   const long long o = dir_stride<DIR>(d);
   // compute_df_line_new (interpline.c:2148-2222): jump indicator from the
   // primitives of the cells -1, 0, +1 along the line and their CENT metrics
-  double dP;
+  T dP;
   {
-    double pm[NPR], p0[NPR], pp[NPR];
-    load_prim(pb, d, z - o, pm);
-    load_prim(pb, d, z, p0);
-    load_prim(pb, d, z + o, pp);
-    State ql, q, qr;
-    double a, b, c;
-    Metric m;
-    load_metric(G, d, gix(d, i - (DIR == 1), j - (DIR == 2)), G_CENT, m);
+    T pm[NPR], p0[NPR], pp[NPR];
+#pragma unroll
+    for (int v = 0; v < NPR; v++) {
+      pm[v] = (T)pb[(long long)v * d.nz + z - o];
+      p0[v] = (T)pb[(long long)v * d.nz + z];
+      pp[v] = (T)pb[(long long)v * d.nz + z + o];
+    }
+    StateT<T> ql, q, qr;
+    T a, b, c;
+    MetricT<T> m;
+    load_metric_t(G, d, gix(d, i - (DIR == 1), j - (DIR == 2)), G_CENT, m);
     get_state(pm, m, ql);
     a = compute_1plusud0(m, ql);
-    load_metric(G, d, gix(d, i, j), G_CENT, m);
+    load_metric_t(G, d, gix(d, i, j), G_CENT, m);
     get_state(p0, m, q);
     b = compute_1plusud0(m, q);
-    load_metric(G, d, gix(d, i + (DIR == 1), j + (DIR == 2)), G_CENT, m);
+    load_metric_t(G, d, gix(d, i + (DIR == 1), j + (DIR == 2)), G_CENT, m);
     get_state(pp, m, qr);
     c = compute_1plusud0(m, qr);
-    double gam = P.gam;
-    double parl = a * (ql.ucon[0]);
-    double par = b * (q.ucon[0]);
-    double parr = c * (qr.ucon[0]);
-    double uparl = gam * pm[UU] * (ql.ucon[0] * ql.ucov[0]) + (gam - 1.0) * pm[UU];
-    double upar = gam * p0[UU] * (q.ucon[0] * q.ucov[0]) + (gam - 1.0) * p0[UU];
-    double uparr = gam * pp[UU] * (qr.ucon[0] * qr.ucov[0]) + (gam - 1.0) * pp[UU];
-    dP = (fabs(p0[RHO] * (parr - parl)) + fabs(uparr - uparl)) / (fabs(p0[RHO] * par) + fabs(upar) + w5::kDblMin);
+    T gam = (T)(P.cell_inst ? P.inst[P.cell_inst[z]].gam : P.gam);
+    T parl = a * (ql.ucon[0]);
+    T par = b * (q.ucon[0]);
+    T parr = c * (qr.ucon[0]);
+    T uparl = gam * pm[UU] * (ql.ucon[0] * ql.ucov[0]) + (gam - T(1.0)) * pm[UU];
+    T upar = gam * p0[UU] * (q.ucon[0] * q.ucov[0]) + (gam - T(1.0)) * p0[UU];
+    T uparr = gam * pp[UU] * (qr.ucon[0] * qr.ucov[0]) + (gam - T(1.0)) * pp[UU];
+    dP = (fabs(p0[RHO] * (parr - parl)) + fabs(uparr - uparl)) / (fabs(p0[RHO] * par) + fabs(upar) + w5::K<T>::tiny);
   }
   // apply_additional_reduction_to_weights (reconstructeno.c:650-700)
-  double ss = w5::wmin((fabs(dP) - 0.5 * w5::kDpFrac) / (0.5 * w5::kDpFrac), 1.);
+  T ss = w5::wmin((fabs(dP) - T(0.5 * w5::kDpFrac)) / T(0.5 * w5::kDpFrac), T(1.));
   for (int v = 0; v < NPR; v++) {
-    const double *wa = WA + (long long)v * W5_PLANES * d.nz + z;
+    const T *wa = WA + (long long)v * W5_PLANES * d.nz + z;
     // codes of cells -1, 0, +1 and weights of cells -3..+3 (w0 and w2 of the neighbours)
-    double cm = __ldg(wa - o), c0 = __ldg(wa), cp = __ldg(wa + o);
-    const double *w0p = wa + d.nz, *w1p = wa + 2 * d.nz, *w2p = wa + 3 * d.nz;
-    double wc[3] = {__ldg(w0p), __ldg(w1p), __ldg(w2p)};
-    double wm[3] = {__ldg(w0p - o), 0.0, __ldg(w2p - o)};
-    double wp[3] = {__ldg(w0p + o), 0.0, __ldg(w2p + o)};
-    double w_m3_0 = __ldg(w0p - 3 * o), w_m2_0 = __ldg(w0p - 2 * o);
-    double w_p2_2 = __ldg(w2p + 2 * o), w_p3_2 = __ldg(w2p + 3 * o);
-    double fd_m = w5::ratio_lof(wm, w_m3_0, __ldg(w2p + o), cm == -1.0 ? 1.0 : 0.0);
-    double fd_p = w5::ratio_lof(wp, __ldg(w0p - o), w_p3_2, cp == -1.0 ? 1.0 : 0.0);
-    double lof = w5::ratio_lof(wc, w_m2_0, w_p2_2, c0 == -1.0 ? 1.0 : 0.0);
+    T cm = __ldg(wa - o), c0 = __ldg(wa), cp = __ldg(wa + o);
+    const T *w0p = wa + d.nz, *w1p = wa + 2 * d.nz, *w2p = wa + 3 * d.nz;
+    T wc[3] = {__ldg(w0p), __ldg(w1p), __ldg(w2p)};
+    T wm[3] = {__ldg(w0p - o), T(0.0), __ldg(w2p - o)};
+    T wp[3] = {__ldg(w0p + o), T(0.0), __ldg(w2p + o)};
+    T w_m3_0 = __ldg(w0p - 3 * o), w_m2_0 = __ldg(w0p - 2 * o);
+    T w_p2_2 = __ldg(w2p + 2 * o), w_p3_2 = __ldg(w2p + 3 * o);
+    T fd_m = w5::ratio_lof(wm, w_m3_0, __ldg(w2p + o), cm == T(-1.0) ? T(1.0) : T(0.0));
+    T fd_p = w5::ratio_lof(wp, __ldg(w0p - o), w_p3_2, cp == T(-1.0) ? T(1.0) : T(0.0));
+    T lof = w5::ratio_lof(wc, w_m2_0, w_p2_2, c0 == T(-1.0) ? T(1.0) : T(0.0));
     lof = w5::wmax(lof, ss * fd_p);
     lof = w5::wmax(lof, ss * fd_m);
     const double *q = pb + (long long)v * d.nz + z;
-    double ya[5] = {__ldg(q - 2 * o), __ldg(q - o), __ldg(q), __ldg(q + o), __ldg(q + 2 * o)};
-    bool cu = (c0 == -1.0);
-    double m0 = cu ? 0.0 : c0;
-    double yl, yr;
+    T ya[5] = {(T)__ldg(q - 2 * o), (T)__ldg(q - o), (T)__ldg(q), (T)__ldg(q + o), (T)__ldg(q + 2 * o)};
+    bool cu = (c0 == T(-1.0));
+    T m0 = cu ? T(0.0) : c0;
+    T yl, yr;
     w5::faces(ya + 2, m0, cu, wc, lof, &yl, &yr);
     pL[(long long)v * d.nz + z] = yl;
     pR[(long long)v * d.nz + z] = yr;
@@ -303,11 +395,12 @@ __global__ void __launch_bounds__(128, HG_MINB_WENO_B) weno_b_kernel(Dims d, Par
 // face flux kernel (one per direction); RECON 0: MC-type slopes in the
 // kernel, RECON 1: Riemann states from the WENO5 face values pL/pR
 // ---------------------------------------------------------------------------
-template <int DIR, int RECON>
-__global__ void __launch_bounds__(128, HG_MINB_FLUX) flux_kernel(Dims d, Params P, Box box, const double *__restrict__ pb,
-                                                   const double *__restrict__ pL, const double *__restrict__ pR,
-                                                   const double *__restrict__ G, double *__restrict__ F,
-                                                   Scalars *sc) {
+template <int DIR, int RECON, typename T>
+__global__ void __launch_bounds__(128, MinBlocks<T>::flux) flux_kernel(Dims d, Params P, Box box,
+                                                                 const double *__restrict__ pb,
+                                                                 const T *__restrict__ pL, const T *__restrict__ pR,
+                                                                 const double *__restrict__ G, double *__restrict__ F,
+                                                                 Scalars *sc) {
   long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   bool active = t < box.size();
   double dtij = 0.0;
@@ -316,7 +409,7 @@ __global__ void __launch_bounds__(128, HG_MINB_FLUX) flux_kernel(Dims d, Params 
     box_ijk(box, t, i, j, k);
     long long z = zix(d, i, j, k);
     const long long o = dir_stride<DIR>(d);
-    double p_l[NPR], p_r[NPR];
+    T p_l[NPR], p_r[NPR];
     if (RECON == 1) {
       // getp2interplr (flux.c:788-808), line-type branch
 #pragma unroll
@@ -324,59 +417,87 @@ __global__ void __launch_bounds__(128, HG_MINB_FLUX) flux_kernel(Dims d, Params 
         p_l[v] = __ldg(pR + (long long)v * d.nz + z - o);
         p_r[v] = __ldg(pL + (long long)v * d.nz + z);
       }
+    } else if (RECON == 2) {
+      // PARA: pright of the cell on the left, pleft of the cell on the right
+#pragma unroll
+      for (int v = 0; v < NPR; v++) {
+        const double *q = pb + (long long)v * d.nz + z;
+        T y[6];
+#pragma unroll
+        for (int l = 0; l < 6; l++) y[l] = (T)__ldg(q + (l - 3) * o);
+        T dummy;
+        para4(y + 2, &dummy, &p_l[v]);
+        para4(y + 3, &p_r[v], &dummy);
+      }
     } else {
 #pragma unroll
       for (int v = 0; v < NPR; v++) {
         const double *q = pb + (long long)v * d.nz + z;
-        double ym2 = __ldg(q - 2 * o), ym1 = __ldg(q - o), y0 = __ldg(q), yp1 = __ldg(q + o);
-        double dqm = slope3(P.lim, ym2, ym1, y0);
-        double dq0 = slope3(P.lim, ym1, y0, yp1);
+        T ym2 = (T)__ldg(q - 2 * o), ym1 = (T)__ldg(q - o), y0 = (T)__ldg(q), yp1 = (T)__ldg(q + o);
+        T dqm = slope3(P.lim, ym2, ym1, y0);
+        T dq0 = slope3(P.lim, ym1, y0, yp1);
         // getp2interplr (flux.c:788-808)
-        p_l[v] = ym1 + 0.5 * dqm;
-        p_r[v] = y0 - 0.5 * dq0;
+        p_l[v] = ym1 + T(0.5) * dqm;
+        p_r[v] = y0 - T(0.5) * dq0;
       }
     }
     // BDIRCONT (flux.c:629-633)
-    p_l[B1 + DIR - 1] = p_r[B1 + DIR - 1] = 0.5 * (p_l[B1 + DIR - 1] + p_r[B1 + DIR - 1]);
-    Metric m;
-    load_metric(G, d, gix(d, i, j), DIR - 1, m);
-    State ql, qr;
-    EM el, er;
-    double Fl[NPR], Fr[NPR], Ul[NPR], Ur[NPR];
+    p_l[B1 + DIR - 1] = p_r[B1 + DIR - 1] = T(0.5) * (p_l[B1 + DIR - 1] + p_r[B1 + DIR - 1]);
+    MetricT<T> m;
+    load_metric_t(G, d, gix(d, i, j), DIR - 1, m);
+    StateT<T> ql, qr;
+    EMT<T> el, er;
+    T Fl[NPR], Fr[NPR], Ul[NPR], Ur[NPR];
+    int b = P.cell_inst ? P.cell_inst[z] : -1;
+    const T gam = (T)(b >= 0 ? P.inst[b].gam : P.gam);
     int err = 0;
     if (get_state(p_l, m, ql)) err |= ERR_UTCALC_DISCR;
     em_prepare(p_l, m, ql, el);
-    primtoflux(p_l, ql, el, DIR, m, P.gam, Fl);
-    primtoflux(p_l, ql, el, 0, m, P.gam, Ul);
+    primtoflux(p_l, ql, el, DIR, m, gam, Fl);
+    primtoflux(p_l, ql, el, 0, m, gam, Ul);
     if (get_state(p_r, m, qr)) err |= ERR_UTCALC_DISCR;
     em_prepare(p_r, m, qr, er);
-    primtoflux(p_r, qr, er, DIR, m, P.gam, Fr);
-    primtoflux(p_r, qr, er, 0, m, P.gam, Ur);
-    double cmaxl = 0., cminl = 0., cmaxr = 0., cminr = 0.;
-    err |= vchar(p_l, ql, DIR, m, P.gam, &cmaxl, &cminl);
-    err |= vchar(p_r, qr, DIR, m, P.gam, &cmaxr, &cminr);
+    primtoflux(p_r, qr, er, DIR, m, gam, Fr);
+    primtoflux(p_r, qr, er, 0, m, gam, Ur);
+    T cmaxl = T(0.), cminl = T(0.), cmaxr = T(0.), cminr = T(0.);
+    err |= vchar(p_l, ql, DIR, m, gam, &cmaxl, &cminl);
+    err |= vchar(p_r, qr, DIR, m, gam, &cmaxr, &cminr);
     // cminmax_calc (wavespeeds.c:325-385)
-    double lmin = min_ref(cminl, cminr);
-    double lmax = max_ref(cmaxl, cmaxr);
-    lmin = fabs(max_ref(0., -lmin));
-    lmax = fabs(max_ref(0., lmax));
-    double cmin = lmin, cmax = lmax, ctop = max_ref(lmax, lmin);
+    T lmin = min_ref(cminl, cminr);
+    T lmax = max_ref(cmaxl, cmaxr);
+    lmin = fabs(max_ref(T(0.), -lmin));
+    lmax = fabs(max_ref(T(0.), lmax));
+    T cmin = lmin, cmax = lmax, ctop = max_ref(lmax, lmin);
     double Fo[NPR];
-    if (P.flux == HGPU_FLUX_HLL && (cmax + cmin != 0.0)) {
+    if (P.flux == HGPU_FLUX_HLL && (cmax + cmin != T(0.0))) {
 #pragma unroll
-      for (int v = 0; v < NPR; v++) Fo[v] = ((cmax * Fl[v] + cmin * Fr[v]) - (cmax * cmin) * (Ur[v] - Ul[v])) / (cmax + cmin);
+      for (int v = 0; v < NPR; v++)
+        Fo[v] = (double)(((cmax * Fl[v] + cmin * Fr[v]) - (cmax * cmin) * (Ur[v] - Ul[v])) / (cmax + cmin));
     } else {
 #pragma unroll
-      for (int v = 0; v < NPR; v++) Fo[v] = (0.5 * ((Fl[v] + Fr[v]) - ctop * (Ur[v] - Ul[v])));
+      for (int v = 0; v < NPR; v++) Fo[v] = (double)(T(0.5) * ((Fl[v] + Fr[v]) - ctop * (Ur[v] - Ul[v])));
     }
-    // flux_ct gdet strip (fluxct.c:74-96)
-    Fo[B1] /= m.g;
-    Fo[B2] /= m.g;
-    Fo[B3] /= m.g;
+    // flux_ct gdet strip (fluxct.c:74-96), in FP64 in both precision modes
+    const double gface = __ldg(G + (long long)((DIR - 1) * GLOC + 33) * d.nij + gix(d, i, j));
+    Fo[B1] /= gface;
+    Fo[B2] /= gface;
+    Fo[B3] /= gface;
     store_prim(F, d, z, Fo);
     double dxd = (DIR == 1) ? P.dx1 : ((DIR == 2) ? P.dx2 : P.dx3);
-    dtij = P.cour * dxd / ctop;
-    if (err) atomicOr(&sc->err, err);
+    if (b >= 0) {
+      // batch: faces 0..n of a running instance feed its own dt
+      const Inst &I = P.inst[b];
+      int loc = i - I.i0;
+      active = false;
+      if (loc >= 0 && loc <= I.n && !I.done) {
+        dtij = P.cour * I.dx / (double)ctop;
+        if (dtij == dtij) atomicMin(&P.inst[b].ndtbits, (unsigned long long)__double_as_longlong(dtij));
+        if (err) atomicOr(&sc->err, err);
+      }
+    } else {
+      dtij = P.cour * dxd / (double)ctop;
+      if (err) atomicOr(&sc->err, err);
+    }
   }
   warp_min_atomic(&sc->ndtbits[DIR], dtij, active);
 }
@@ -458,7 +579,18 @@ __global__ void __launch_bounds__(128, HG_MINB_UPDATE) update_kernel(Dims d, Par
     const long long nz = d.nz;
     const long long o1 = (long long)d.nt2 * d.nt3, o2 = d.nt3, o3 = 1;
     const long long ij = gix(d, i, j);
-    const double dt = sc->dt;
+    double dt = sc->dt, gam = P.gam, dx1 = P.dx1;
+    bool run = true;
+    if (P.cell_inst) {
+      // batch: only the active cells of running instances advance
+      const Inst &I = P.inst[P.cell_inst[z]];
+      int loc = i - I.i0;
+      run = (loc >= 0 && loc < I.n && !I.done);
+      dt = I.dt;
+      gam = I.gam;
+      dx1 = I.dx;
+    }
+    if (run) {
     Metric m;
     load_metric(G, d, ij, G_CENT, m);
     int err = 0;
@@ -470,7 +602,7 @@ __global__ void __launch_bounds__(128, HG_MINB_UPDATE) update_kernel(Dims d, Par
       EM e;
       if (get_state(pr, m, q)) err |= ERR_UTCALC_DISCR;
       em_prepare(pr, m, q, e);
-      primtoflux(pr, q, e, 0, m, P.gam, Ui);
+      primtoflux(pr, q, e, 0, m, gam, Ui);
     }
     double pbz[NPR];
     load_prim(pb, d, z, pbz);
@@ -484,7 +616,7 @@ __global__ void __launch_bounds__(128, HG_MINB_UPDATE) update_kernel(Dims d, Par
       const double *conn = G + (long long)G_CONN * d.nij + ij;
       double mhd[4][4];
 #pragma unroll
-      for (int jj = 0; jj < 4; jj++) mhd_row(pbz, jj, P.gam, q, e, mhd[jj]);
+      for (int jj = 0; jj < 4; jj++) mhd_row(pbz, jj, gam, q, e, mhd[jj]);
 #pragma unroll
       for (int l = 0; l < 4; l++) {
         double s = dUconn[l];
@@ -515,7 +647,7 @@ __global__ void __launch_bounds__(128, HG_MINB_UPDATE) update_kernel(Dims d, Par
     }
     // flux2dUavg (advance.c:741-914) with the B fluxes of flux_ct (fluxct.c:724-781)
     {
-      const double idx1 = 1.0 / P.dx1, idx2 = 1.0 / P.dx2, idx3 = 1.0 / P.dx3;
+      const double idx1 = 1.0 / dx1, idx2 = 1.0 / P.dx2, idx3 = 1.0 / P.dx3;
       const double *e1 = E, *e2 = E + nz, *e3 = E + 2 * nz;
 #pragma unroll
       for (int pl = 0; pl < NPR; pl++) {
@@ -563,7 +695,7 @@ __global__ void __launch_bounds__(128, HG_MINB_UPDATE) update_kernel(Dims d, Par
 #pragma unroll
     for (int v = 0; v < NPR; v++) pr[v] = pbz[v];
     int it = 0;
-    int flag = utoprimgen(finalstep ? Ucum : Uf, m, P.gam, P.gammafail, pr, &it);
+    int flag = utoprimgen(finalstep ? Ucum : Uf, m, gam, P.gammafail, pr, &it);
     my_iters = (unsigned long long)it;
     my_fail = (flag != 0);
     if (finalstep) {
@@ -579,6 +711,7 @@ __global__ void __launch_bounds__(128, HG_MINB_UPDATE) update_kernel(Dims d, Par
     store_prim(pf, d, z, pr);
     pflag[z] = flag;
     if (err) atomicOr(&sc->err, err);
+    }
   }
   // block-level aggregation of counters
   unsigned long long s_it = my_iters;
@@ -728,12 +861,34 @@ __global__ void bound_pflag_kernel(Dims d, Params P, int *pflag) {
   pflag[t] = pflag[zix(d, si, sj, sk)];
 }
 
+// Batch of 1D instances: every instance's ghost cells are a plain copy of its
+// first / last active cell (bounds.c OUTFLOW, bounds.c:84-135, 218-292), for
+// the primitives (pv != nullptr) or the failure flags (pflag != nullptr).
+__global__ void bound_batch_kernel(Dims d, Params P, double *pv, int *pflag) {
+  long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= d.nz) return;
+  int i = (int)t - d.g1;  // the batch line is 1D
+  const Inst &I = P.inst[P.cell_inst[t]];
+  int loc = i - I.i0;
+  int src;
+  if (loc < 0) src = I.i0;
+  else if (loc >= I.n) src = I.i0 + I.n - 1;
+  else return;
+  long long zs = zix(d, src, 0, 0);
+  if (pv) {
+#pragma unroll
+    for (int v = 0; v < NPR; v++) pv[(long long)v * d.nz + t] = pv[(long long)v * d.nz + zs];
+  }
+  if (pflag) pflag[t] = pflag[zs];
+}
+
 // ---------------------------------------------------------------------------
 // post_fixup (fixup.c:37-96)
 // ---------------------------------------------------------------------------
 // fixup_checksolution (fixup.c:460-560), part 1: gamma on i,j,k = -1..N and
 // the list of active candidate zones (gamma >= 2)
-__global__ void checksol_gamma_kernel(Dims d, Box box, const double *__restrict__ pv, const double *__restrict__ G,
+__global__ void checksol_gamma_kernel(Dims d, Params P, Box box, const double *__restrict__ pv,
+                                      const double *__restrict__ G,
                                       double *__restrict__ gammacheck, long long *__restrict__ cand, int cap,
                                       Scalars *sc) {
   long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -749,6 +904,11 @@ __global__ void checksol_gamma_kernel(Dims d, Box box, const double *__restrict_
   if (gamma_calc(pr, m, &gamma)) atomicOr(&sc->err, ERR_UTCALC_DISCR);
   gammacheck[z] = gamma;
   bool activez = (i >= 0 && i < d.n1 && j >= 0 && j < d.n2 && k >= 0 && k < d.n3);
+  if (P.cell_inst) {
+    const Inst &I = P.inst[P.cell_inst[z]];
+    int loc = i - I.i0;
+    activez = (loc >= 0 && loc < I.n && !I.done);
+  }
   if (activez && gamma >= 2.0) {
     int slot = atomicAdd(&sc->ncand, 1);
     if (slot < cap) cand[slot] = z;
@@ -837,13 +997,18 @@ __global__ void __launch_bounds__(1024) checksol_resolve_kernel(Dims d, const do
 }
 
 // fixup_utoprim (fixup.c:669-1470), part 1: list the active failed zones
-__global__ void fixup_collect_kernel(Dims d, Box box, const int *__restrict__ pflag, long long *__restrict__ list,
-                                     int cap, Scalars *sc) {
+__global__ void fixup_collect_kernel(Dims d, Params P, Box box, const int *__restrict__ pflag,
+                                     long long *__restrict__ list, int cap, Scalars *sc) {
   long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= box.size()) return;
   int i, j, k;
   box_ijk(box, t, i, j, k);
   long long z = zix(d, i, j, k);
+  if (P.cell_inst) {
+    const Inst &I = P.inst[P.cell_inst[z]];
+    int loc = i - I.i0;
+    if (!(loc >= 0 && loc < I.n && !I.done)) return;
+  }
   if (pflag[z] != 0) {
     int slot = atomicAdd(&sc->nfixlist, 1);
     if (slot < cap) list[slot] = z;
@@ -1022,6 +1187,35 @@ __global__ void finalize_kernel(Params P, Scalars *sc, int advance_time) {
   sc->ndtbits[0] = (unsigned long long)__double_as_longlong(ndt);
 }
 
+// batch: per-instance ndt combine and dt update (the same formulas per
+// instance; dims of size 1 contribute BIG as in the one-domain case)
+__global__ void finalize_batch_kernel(Params P, int advance_time) {
+  int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= P.ninst) return;
+  Inst &I = P.inst[b];
+  double n1 = __longlong_as_double((long long)I.ndtbits);
+  double ndt = P.defcon * 1. / (1. / n1 + 1. / BIGNUM + 1. / BIGNUM);
+  if (advance_time) {
+    if (I.done) return;
+    double dt = I.dt;
+    I.t += dt;
+    I.nsteps++;
+    if (ndt > P.safe * dt) ndt = P.safe * dt;
+    dt = ndt;
+    if (I.t + dt > I.tf) dt = I.tf - I.t;
+    I.dt = dt;
+    if (!(I.t < I.tf)) I.done = 1;
+  } else {
+    I.dt = ndt;
+  }
+}
+
+__global__ void reset_batch_kernel(Params P) {
+  int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= P.ninst) return;
+  P.inst[b].ndtbits = (unsigned long long)__double_as_longlong(BIGNUM);
+}
+
 __global__ void reset_stage_kernel(Scalars *sc) {
   if (threadIdx.x != 0 || blockIdx.x != 0) return;
   unsigned long long big = (unsigned long long)__double_as_longlong(BIGNUM);
@@ -1129,6 +1323,14 @@ struct hgpu_ctx {
   double *pL = nullptr, *pR = nullptr, *WA = nullptr;  // WENO5 face values and weights scratch
   Box wa_box[4], wb_box[4];
   int *istaging = nullptr;
+  // batch of 1D instances (hgpu_create_batch)
+  int *cell_inst = nullptr;
+  Inst *inst = nullptr;
+  int ninst = 0;
+  // one captured time step (hgpu_step_graph)
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t graph_exec = nullptr;
+  long long launches_per_step = 0;
   Box face_box[4], emf_box, active_box, dq_box;
 };
 
@@ -1188,19 +1390,22 @@ static int validate(const hgpu_config *c) {
   if (!c) return HGPU_E_INVALID;
   if (c->n1 < 1 || c->n2 < 1 || c->n3 < 1 || c->ng < 2) return HGPU_E_INVALID;
   if (c->lim != HGPU_LIM_MC && c->lim != HGPU_LIM_VANL && c->lim != HGPU_LIM_MINM && c->lim != HGPU_LIM_DONOR &&
-      c->lim != HGPU_LIM_WENO5)
+      c->lim != HGPU_LIM_PARA && c->lim != HGPU_LIM_WENO5)
     return HGPU_E_INVALID;
+  // PARA reads 3 zones beyond the faces' cells
+  if (c->lim == HGPU_LIM_PARA && c->ng < 3) return HGPU_E_INVALID;
   // WENO5 reads the line up to 5 cells beyond the faces' cells -1..n
   if (c->lim == HGPU_LIM_WENO5 && c->ng < 6) return HGPU_E_INVALID;
   if (c->fluxmethod != HGPU_FLUX_HLL && c->fluxmethod != HGPU_FLUX_LAXF) return HGPU_E_INVALID;
   for (int f = 0; f < 6; f++)
-    if (c->bc[f] != HGPU_BC_OUTFLOW && c->bc[f] != HGPU_BC_POLARAXIS && c->bc[f] != HGPU_BC_PERIODIC)
+    if (c->bc[f] != HGPU_BC_OUTFLOW && c->bc[f] != HGPU_BC_POLARAXIS && c->bc[f] != HGPU_BC_PERIODIC &&
+        c->bc[f] != HGPU_BC_OUTFLOW_COPY)
       return HGPU_E_INVALID;
   // reflections and periodic wraps read inside the active range
   if (c->n2 > 1 && c->n2 < c->ng) return HGPU_E_INVALID;
   if (c->n3 > 1 && c->n3 < c->ng) return HGPU_E_INVALID;
   if (c->n1 > 1 && c->n1 < c->ng) return HGPU_E_INVALID;
-  if (c->precision != HGPU_PREC_FP64) return HGPU_E_INVALID;
+  if (c->precision != HGPU_PREC_FP64 && c->precision != HGPU_PREC_MIXED) return HGPU_E_INVALID;
   return HGPU_OK;
 }
 
@@ -1213,11 +1418,13 @@ const char *hgpu_last_error(void) { return g_errbuf; }
 void hgpu_destroy(hgpu_ctx *x) {
   if (!x) return;
   cudaStreamSynchronize(x->stream);
+  if (x->graph_exec) cudaGraphExecDestroy(x->graph_exec);
+  if (x->graph) cudaGraphDestroy(x->graph);
   collect_profile(x);
   for (cudaEvent_t e : x->freelist) cudaEventDestroy(e);
   void *ptrs[] = {x->p, x->pk, x->uf, x->ucum, x->F[1], x->F[2], x->F[3], x->E, x->G, x->pflag, x->gammacheck,
                   x->cand, x->fixlist, x->cand_orig, x->cand_dec, x->candmap, x->fixvals, x->sc, x->staging, x->istaging,
-                  x->pL, x->pR, x->WA};
+                  x->pL, x->pR, x->WA, x->cell_inst, x->inst};
   for (void *q : ptrs)
     if (q) cudaFree(q);
   cudaStreamDestroy(x->stream);
@@ -1334,6 +1541,93 @@ int hgpu_create(const hgpu_config *cfg, hgpu_ctx **out) {
   return HGPU_OK;
 }
 
+int hgpu_create_batch(const hgpu_config *cfg, int ninst, const int *n1, const double *dx1, const double *gam,
+                      const double *tf, hgpu_ctx **out) {
+  if (!cfg || !out || ninst < 1 || !n1 || !dx1 || !gam || !tf) return HGPU_E_INVALID;
+  *out = nullptr;
+  if (cfg->n2 != 1 || cfg->n3 != 1) {
+    set_err("a batch holds 1D instances: n2 = n3 = 1");
+    return HGPU_E_INVALID;
+  }
+  if (cfg->bc[0] != HGPU_BC_OUTFLOW_COPY || cfg->bc[1] != HGPU_BC_OUTFLOW_COPY) {
+    set_err("a batch needs HGPU_BC_OUTFLOW_COPY at both x1 ends");
+    return HGPU_E_INVALID;
+  }
+  long long total = 0;
+  for (int b = 0; b < ninst; b++) {
+    if (n1[b] < cfg->ng || !(dx1[b] > 0.0) || !(gam[b] > 1.0)) {
+      set_err("instance %s%d: n1 < ng, dx1 <= 0 or gam <= 1", "", b);
+      return HGPU_E_INVALID;
+    }
+    total += n1[b] + 2LL * cfg->ng;
+  }
+  if (total - 2LL * cfg->ng > (1LL << 30)) return HGPU_E_INVALID;
+  hgpu_config c = *cfg;
+  c.n1 = (int)(total - 2LL * cfg->ng);
+  int rc = hgpu_create(&c, out);
+  if (rc) return rc;
+  hgpu_ctx *x = *out;
+  const Dims &d = x->d;
+  std::vector<Inst> hi(ninst);
+  std::vector<int> hc(d.nz);
+  long long start = 0;  // global x1 index of the instance's first ghost is start - ng
+  for (int b = 0; b < ninst; b++) {
+    Inst I;
+    memset(&I, 0, sizeof(I));
+    I.i0 = (int)start;
+    I.n = n1[b];
+    I.dx = dx1[b];
+    I.gam = gam[b];
+    I.tf = tf[b];
+    hi[b] = I;
+    for (long long q = start - cfg->ng; q < start + n1[b] + cfg->ng; q++) hc[q + d.g1] = b;
+    start += n1[b] + 2LL * cfg->ng;
+  }
+  if (cudaMalloc(&x->inst, sizeof(Inst) * ninst) != cudaSuccess ||
+      cudaMalloc(&x->cell_inst, sizeof(int) * d.nz) != cudaSuccess) {
+    hgpu_destroy(x);
+    *out = nullptr;
+    set_err("device allocation failed");
+    return HGPU_E_NOMEM;
+  }
+  if (cudaMemcpy(x->inst, hi.data(), sizeof(Inst) * ninst, cudaMemcpyHostToDevice) != cudaSuccess ||
+      cudaMemcpy(x->cell_inst, hc.data(), sizeof(int) * d.nz, cudaMemcpyHostToDevice) != cudaSuccess) {
+    hgpu_destroy(x);
+    *out = nullptr;
+    set_err("batch table upload failed");
+    return HGPU_E_CUDA;
+  }
+  x->ninst = ninst;
+  x->P.cell_inst = x->cell_inst;
+  x->P.inst = x->inst;
+  x->P.ninst = ninst;
+  return HGPU_OK;
+}
+
+int hgpu_batch_layout(hgpu_ctx *x, int *i0) {
+  if (!x || !x->inst || !i0) return HGPU_E_INVALID;
+  std::vector<Inst> hi(x->ninst);
+  CUDA_TRY(cudaMemcpy(hi.data(), x->inst, sizeof(Inst) * x->ninst, cudaMemcpyDeviceToHost));
+  for (int b = 0; b < x->ninst; b++) i0[b] = hi[b].i0;
+  return HGPU_OK;
+}
+
+int hgpu_batch_status(hgpu_ctx *x, double *t, double *dt, int *done, int *ndone) {
+  if (!x || !x->inst) return HGPU_E_INVALID;
+  std::vector<Inst> hi(x->ninst);
+  CUDA_TRY(cudaMemcpyAsync(hi.data(), x->inst, sizeof(Inst) * x->ninst, cudaMemcpyDeviceToHost, x->stream));
+  CUDA_TRY(cudaStreamSynchronize(x->stream));
+  int nd = 0;
+  for (int b = 0; b < x->ninst; b++) {
+    if (t) t[b] = hi[b].t;
+    if (dt) dt[b] = hi[b].dt;
+    if (done) done[b] = hi[b].done;
+    nd += hi[b].done != 0;
+  }
+  if (ndone) *ndone = nd;
+  return HGPU_OK;
+}
+
 int hgpu_upload_geometry(hgpu_ctx *x, const double *gcov, const double *gcon, const double *gcovpert,
                          const double *gdet, const double *conn, const double *floors) {
   if (!x || !gcov || !gcon || !gcovpert || !gdet || !conn || !floors) return HGPU_E_INVALID;
@@ -1411,46 +1705,90 @@ int hgpu_download_state(hgpu_ctx *x, double *p, int *pflag, double *t, double *d
 }
 
 // one stage: fluxes, EMFs, update, bound, post_fixup, bound
-static void launch_fluxes(hgpu_ctx *x, const double *pb) {
+extern "C++" {
+template <typename T>
+static void launch_fluxes_t(hgpu_ctx *x, const double *pb) {
   const Dims &d = x->d;
   const int nd[4] = {0, d.n1, d.n2, d.n3};
-  const int kid[4] = {0, K_FLUX1, K_FLUX2, K_FLUX3};
   bool weno = x->P.lim == HGPU_LIM_WENO5;
+  T *WA = (T *)x->WA, *pL = (T *)x->pL, *pR = (T *)x->pR;
   for (int q = 1; q <= 3; q++) {
     if (nd[q] <= 1) continue;
     unsigned gf = grid_for(x->face_box[q].size(), 128);
-    if (weno) {
-      unsigned ga = grid_for(x->wa_box[q].size(), 128), gb = grid_for(x->wb_box[q].size(), 128);
-      if (q == 1) {
-        LAUNCH(x, K_WENO_A, weno_a_kernel<1>, ga, 128, d, x->wa_box[1], pb, x->WA);
-        LAUNCH(x, K_WENO_B, weno_b_kernel<1>, gb, 128, d, x->P, x->wb_box[1], pb, x->G, x->WA, x->pL, x->pR);
-        LAUNCH(x, kid[1], (flux_kernel<1, 1>), gf, 128, d, x->P, x->face_box[1], pb, x->pL, x->pR, x->G, x->F[1], x->sc);
-      } else if (q == 2) {
-        LAUNCH(x, K_WENO_A, weno_a_kernel<2>, ga, 128, d, x->wa_box[2], pb, x->WA);
-        LAUNCH(x, K_WENO_B, weno_b_kernel<2>, gb, 128, d, x->P, x->wb_box[2], pb, x->G, x->WA, x->pL, x->pR);
-        LAUNCH(x, kid[2], (flux_kernel<2, 1>), gf, 128, d, x->P, x->face_box[2], pb, x->pL, x->pR, x->G, x->F[2], x->sc);
+    unsigned ga = grid_for(x->wa_box[q].size(), 128), gb = grid_for(x->wb_box[q].size(), 128);
+    const Params &P = x->P;
+    if (q == 1) {
+      if (weno) {
+        LAUNCH(x, K_WENO_A, (weno_a_kernel<1, T>), ga, 128, d, x->wa_box[1], pb, WA);
+        LAUNCH(x, K_WENO_B, (weno_b_kernel<1, T>), gb, 128, d, P, x->wb_box[1], pb, x->G, WA, pL, pR);
+        LAUNCH(x, K_FLUX1, (flux_kernel<1, 1, T>), gf, 128, d, P, x->face_box[1], pb, pL, pR, x->G, x->F[1], x->sc);
+      } else if (P.lim == HGPU_LIM_PARA) {
+        LAUNCH(x, K_FLUX1, (flux_kernel<1, 2, T>), gf, 128, d, P, x->face_box[1], pb, nullptr, nullptr, x->G, x->F[1],
+               x->sc);
       } else {
-        LAUNCH(x, K_WENO_A, weno_a_kernel<3>, ga, 128, d, x->wa_box[3], pb, x->WA);
-        LAUNCH(x, K_WENO_B, weno_b_kernel<3>, gb, 128, d, x->P, x->wb_box[3], pb, x->G, x->WA, x->pL, x->pR);
-        LAUNCH(x, kid[3], (flux_kernel<3, 1>), gf, 128, d, x->P, x->face_box[3], pb, x->pL, x->pR, x->G, x->F[3], x->sc);
+        LAUNCH(x, K_FLUX1, (flux_kernel<1, 0, T>), gf, 128, d, P, x->face_box[1], pb, nullptr, nullptr, x->G, x->F[1],
+               x->sc);
+      }
+    } else if (q == 2) {
+      if (weno) {
+        LAUNCH(x, K_WENO_A, (weno_a_kernel<2, T>), ga, 128, d, x->wa_box[2], pb, WA);
+        LAUNCH(x, K_WENO_B, (weno_b_kernel<2, T>), gb, 128, d, P, x->wb_box[2], pb, x->G, WA, pL, pR);
+        LAUNCH(x, K_FLUX2, (flux_kernel<2, 1, T>), gf, 128, d, P, x->face_box[2], pb, pL, pR, x->G, x->F[2], x->sc);
+      } else if (P.lim == HGPU_LIM_PARA) {
+        LAUNCH(x, K_FLUX2, (flux_kernel<2, 2, T>), gf, 128, d, P, x->face_box[2], pb, nullptr, nullptr, x->G, x->F[2],
+               x->sc);
+      } else {
+        LAUNCH(x, K_FLUX2, (flux_kernel<2, 0, T>), gf, 128, d, P, x->face_box[2], pb, nullptr, nullptr, x->G, x->F[2],
+               x->sc);
       }
     } else {
-      if (q == 1)
-        LAUNCH(x, kid[1], (flux_kernel<1, 0>), gf, 128, d, x->P, x->face_box[1], pb, nullptr, nullptr, x->G, x->F[1], x->sc);
-      else if (q == 2)
-        LAUNCH(x, kid[2], (flux_kernel<2, 0>), gf, 128, d, x->P, x->face_box[2], pb, nullptr, nullptr, x->G, x->F[2], x->sc);
-      else
-        LAUNCH(x, kid[3], (flux_kernel<3, 0>), gf, 128, d, x->P, x->face_box[3], pb, nullptr, nullptr, x->G, x->F[3], x->sc);
+      if (weno) {
+        LAUNCH(x, K_WENO_A, (weno_a_kernel<3, T>), ga, 128, d, x->wa_box[3], pb, WA);
+        LAUNCH(x, K_WENO_B, (weno_b_kernel<3, T>), gb, 128, d, P, x->wb_box[3], pb, x->G, WA, pL, pR);
+        LAUNCH(x, K_FLUX3, (flux_kernel<3, 1, T>), gf, 128, d, P, x->face_box[3], pb, pL, pR, x->G, x->F[3], x->sc);
+      } else if (P.lim == HGPU_LIM_PARA) {
+        LAUNCH(x, K_FLUX3, (flux_kernel<3, 2, T>), gf, 128, d, P, x->face_box[3], pb, nullptr, nullptr, x->G, x->F[3],
+               x->sc);
+      } else {
+        LAUNCH(x, K_FLUX3, (flux_kernel<3, 0, T>), gf, 128, d, P, x->face_box[3], pb, nullptr, nullptr, x->G, x->F[3],
+               x->sc);
+      }
     }
   }
+}
+}  // extern "C++"
+
+// fluxcalc + the EMFs of flux_ct.  HGPU_PREC_MIXED runs reconstruction, wave
+// speeds and the Riemann flux in FP32; the fluxes are stored in FP64 and
+// everything after them (flux-CT, update, inversion) stays FP64.
+static void launch_fluxes(hgpu_ctx *x, const double *pb) {
+  const Dims &d = x->d;
+  if (x->cfg.precision == HGPU_PREC_MIXED) launch_fluxes_t<float>(x, pb);
+  else launch_fluxes_t<double>(x, pb);
   LAUNCH(x, K_EMF, emf_kernel, grid_for(x->emf_box.size(), 256), 256, d, x->emf_box, x->F[1], x->F[2], x->F[3], x->G,
          x->E);
 }
 
 static void launch_bound(hgpu_ctx *x, double *pv) {
   const Dims &d = x->d;
+  if (x->P.cell_inst) {
+    LAUNCH(x, K_BOUND_GHOST, bound_batch_kernel, grid_for(d.nz, 128), 128, d, x->P, pv, (int *)nullptr);
+    return;
+  }
   LAUNCH(x, K_BOUND_GHOST, bound_ghost_kernel, grid_for(d.nz, 128), 128, d, x->P, pv, x->G, x->sc);
   if (d.n2 > 1) LAUNCH(x, K_BOUND_POLE, bound_pole_kernel, grid_for(2LL * d.n1 * d.n3, 128), 128, d, x->P, pv);
+}
+
+static void launch_reset(hgpu_ctx *x) {
+  LAUNCH(x, K_RESET, reset_stage_kernel, 1, 32, x->sc);
+  if (x->P.cell_inst) LAUNCH(x, K_RESET, reset_batch_kernel, grid_for(x->P.ninst, 128), 128, x->P);
+}
+
+static void launch_finalize(hgpu_ctx *x, int advance_time) {
+  if (x->P.cell_inst)
+    LAUNCH(x, K_FINALIZE, finalize_batch_kernel, grid_for(x->P.ninst, 128), 128, x->P, advance_time);
+  else
+    LAUNCH(x, K_FINALIZE, finalize_kernel, 1, 32, x->P, x->sc, advance_time);
 }
 
 static void launch_stage(hgpu_ctx *x, int timeorder) {
@@ -1464,19 +1802,22 @@ static void launch_stage(hgpu_ctx *x, int timeorder) {
   double CUf0 = 1.0, CUf1 = 0.0, CUf2 = (timeorder == 0) ? 0.5 : 1.0;
   double Cn0 = 0.0, Cn1 = 0.0, Cn2 = (timeorder == 0) ? 0.0 : 1.0;
   (void)s;
-  LAUNCH(x, K_RESET, reset_stage_kernel, 1, 32, x->sc);
+  launch_reset(x);
   launch_fluxes(x, pb);
   LAUNCH(x, K_UPDATE, update_kernel, grid_for(x->active_box.size(), 128), 128, d, x->P, x->active_box, pi, pb, pf, x->uf,
          x->ucum, x->F[1], x->F[2], x->F[3], x->E, x->G, x->pflag, x->sc, CUf0, CUf1, CUf2, Cn0, Cn1, Cn2, timeorder,
          finalstep);
   launch_bound(x, pf);
   // post_fixup (fixup.c:37-96)
-  LAUNCH(x, K_BOUND_PFLAG, bound_pflag_kernel, grid_for(d.nz, 256), 256, d, x->P, x->pflag);
-  LAUNCH(x, K_CHECK_GAMMA, checksol_gamma_kernel, grid_for(x->dq_box.size(), 128), 128, d, x->dq_box, pf, x->G,
+  if (x->P.cell_inst)
+    LAUNCH(x, K_BOUND_PFLAG, bound_batch_kernel, grid_for(d.nz, 256), 256, d, x->P, (double *)nullptr, x->pflag);
+  else
+    LAUNCH(x, K_BOUND_PFLAG, bound_pflag_kernel, grid_for(d.nz, 256), 256, d, x->P, x->pflag);
+  LAUNCH(x, K_CHECK_GAMMA, checksol_gamma_kernel, grid_for(x->dq_box.size(), 128), 128, d, x->P, x->dq_box, pf, x->G,
          x->gammacheck, x->cand, x->cap, x->sc);
   LAUNCH(x, K_CHECK_RESOLVE, checksol_resolve_kernel, 1, 1024, d, pf, x->gammacheck, x->pflag, x->cand, x->candmap,
          x->cand_orig, x->cand_dec, x->cap, x->sc);
-  LAUNCH(x, K_FIX_COLLECT, fixup_collect_kernel, grid_for(x->active_box.size(), 256), 256, d, x->active_box, x->pflag,
+  LAUNCH(x, K_FIX_COLLECT, fixup_collect_kernel, grid_for(x->active_box.size(), 256), 256, d, x->P, x->active_box, x->pflag,
          x->fixlist, x->cap, x->sc);
   // grid-stride over the device-side list length; idle blocks exit at once
   int fixgrid = (int)grid_for(x->cap, 128);
@@ -1524,9 +1865,50 @@ int hgpu_step_ch(hgpu_ctx *x, int nsteps, hgpu_stats *stats) {
   for (int n = 0; n < nsteps; n++) {
     launch_stage(x, 0);
     launch_stage(x, 1);
-    LAUNCH(x, K_FINALIZE, finalize_kernel, 1, 32, x->P, x->sc, 1);
+    launch_finalize(x, 1);
   }
   CUDA_TRY(cudaGetLastError());
+  if (stats) return read_stats(x, stats);
+  return HGPU_OK;
+}
+
+// nsteps replays of one captured time step.  The capture is made on the
+// first call (profiling must be off) and reused; the step's launches read t,
+// dt and every bound from device memory, so the same graph advances any state.
+int hgpu_step_graph(hgpu_ctx *x, int nsteps, hgpu_stats *stats) {
+  if (!x || nsteps < 0) return HGPU_E_INVALID;
+  if (x->profiling) {
+    set_err("hgpu_step_graph: turn profiling off first");
+    return HGPU_E_INVALID;
+  }
+  if (!x->graph_exec) {
+    CUDA_TRY(cudaStreamSynchronize(x->stream));
+    CUDA_TRY(cudaStreamBeginCapture(x->stream, cudaStreamCaptureModeThreadLocal));
+    long long l0 = x->launches;
+    launch_stage(x, 0);
+    launch_stage(x, 1);
+    launch_finalize(x, 1);
+    x->launches_per_step = x->launches - l0;
+    x->launches = l0;
+    cudaGraph_t g = nullptr;
+    cudaError_t e = cudaStreamEndCapture(x->stream, &g);
+    if (e != cudaSuccess) {
+      set_err("step capture failed: %s", cudaGetErrorString(e));
+      return HGPU_E_CUDA;
+    }
+    e = cudaGraphInstantiate(&x->graph_exec, g, 0);
+    if (e != cudaSuccess) {
+      cudaGraphDestroy(g);
+      set_err("graph instantiation failed: %s", cudaGetErrorString(e));
+      return HGPU_E_CUDA;
+    }
+    x->graph = g;
+  }
+  clear_counters(x);
+  for (int n = 0; n < nsteps; n++) {
+    CUDA_TRY(cudaGraphLaunch(x->graph_exec, x->stream));
+    x->launches += x->launches_per_step;
+  }
   if (stats) return read_stats(x, stats);
   return HGPU_OK;
 }
@@ -1535,7 +1917,7 @@ int hgpu_advance_stage(hgpu_ctx *x, int timeorder, double *ndt, hgpu_stats *stat
   if (!x || (timeorder != 0 && timeorder != 1)) return HGPU_E_INVALID;
   clear_counters(x);
   launch_stage(x, timeorder);
-  LAUNCH(x, K_FINALIZE, finalize_kernel, 1, 32, x->P, x->sc, 0);
+  launch_finalize(x, 0);
   CUDA_TRY(cudaGetLastError());
   int rc = read_stats(x, stats);
   if (ndt) {
@@ -1551,7 +1933,7 @@ int hgpu_advance_stage(hgpu_ctx *x, int timeorder, double *ndt, hgpu_stats *stat
 int hgpu_fluxcalc(hgpu_ctx *x, int which, double *F1, double *F2, double *F3, double *ndt1, double *ndt2,
                   double *ndt3) {
   if (!x || (which != 0 && which != 1)) return HGPU_E_INVALID;
-  LAUNCH(x, K_RESET, reset_stage_kernel, 1, 32, x->sc);
+  launch_reset(x);
   launch_fluxes(x, which ? x->pk : x->p);
   CUDA_TRY(cudaGetLastError());
   Scalars s;
@@ -1662,10 +2044,10 @@ __global__ void set_dt_kernel(Scalars *sc) {
 
 int hgpu_init_dt(hgpu_ctx *x, double *dt) {
   if (!x) return HGPU_E_INVALID;
-  LAUNCH(x, K_RESET, reset_stage_kernel, 1, 32, x->sc);
+  launch_reset(x);
   launch_fluxes(x, x->p);
-  LAUNCH(x, K_FINALIZE, finalize_kernel, 1, 32, x->P, x->sc, 0);
-  LAUNCH(x, K_OTHER, set_dt_kernel, 1, 32, x->sc);
+  launch_finalize(x, 0);
+  if (!x->P.cell_inst) LAUNCH(x, K_OTHER, set_dt_kernel, 1, 32, x->sc);
   CUDA_TRY(cudaGetLastError());
   Scalars s;
   CUDA_TRY(cudaMemcpyAsync(&s, x->sc, sizeof(Scalars), cudaMemcpyDeviceToHost, x->stream));
@@ -1684,7 +2066,7 @@ int hgpu_step_ch_timed(hgpu_ctx *x, int nsteps, float *ms, hgpu_stats *stats) {
   for (int n = 0; n < nsteps; n++) {
     launch_stage(x, 0);
     launch_stage(x, 1);
-    LAUNCH(x, K_FINALIZE, finalize_kernel, 1, 32, x->P, x->sc, 1);
+    launch_finalize(x, 1);
   }
   CUDA_TRY(cudaEventRecord(b, x->stream));
   CUDA_TRY(cudaEventSynchronize(b));
@@ -1776,6 +2158,47 @@ int hgpu_free_pinned(void *ptr) {
   return HGPU_OK;
 }
 
+int hgpu_batch_run(hgpu_ctx *x, int check_every, int max_steps, int *steps, float *ms, int *steps_per_instance,
+                   float *done_ms) {
+  if (!x || !x->inst || check_every < 1 || max_steps < 0) return HGPU_E_INVALID;
+  cudaEvent_t a, b;
+  CUDA_TRY(cudaEventCreate(&a));
+  CUDA_TRY(cudaEventCreate(&b));
+  std::vector<Inst> hi(x->ninst);
+  std::vector<float> fin(x->ninst, -1.f);
+  int taken = 0, rc = HGPU_OK;
+  CUDA_TRY(cudaEventRecord(a, x->stream));
+  while (taken < max_steps) {
+    int k = check_every < max_steps - taken ? check_every : max_steps - taken;
+    rc = hgpu_step_graph(x, k, nullptr);
+    if (rc) break;
+    taken += k;
+    CUDA_TRY(cudaMemcpyAsync(hi.data(), x->inst, sizeof(Inst) * x->ninst, cudaMemcpyDeviceToHost, x->stream));
+    CUDA_TRY(cudaEventRecord(b, x->stream));
+    CUDA_TRY(cudaEventSynchronize(b));
+    float now = 0.f;
+    cudaEventElapsedTime(&now, a, b);
+    int nd = 0;
+    for (int q = 0; q < x->ninst; q++) {
+      if (hi[q].done && fin[q] < 0.f) fin[q] = now;
+      nd += hi[q].done != 0;
+    }
+    if (nd == x->ninst) break;
+  }
+  float total = 0.f;
+  cudaEventElapsedTime(&total, a, b);
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  if (rc) return rc;
+  if (steps) *steps = taken;
+  if (ms) *ms = total;
+  for (int q = 0; q < x->ninst; q++) {
+    if (steps_per_instance) steps_per_instance[q] = hi[q].nsteps;
+    if (done_ms) done_ms[q] = fin[q];
+  }
+  return read_stats(x, nullptr);
+}
+
 }  // extern "C"
 
 // ---------------------------------------------------------------------------
@@ -1863,4 +2286,5 @@ extern "C" int hgpu_utoprim_batch_noalloc(const double *U, const double *gcov, c
   CUDA_TRY(cudaMemcpy(&it, dit, sizeof(it), cudaMemcpyDeviceToHost));
   if (iters) *iters = (long long)it;
   return HGPU_OK;
+
 }

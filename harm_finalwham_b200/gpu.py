@@ -16,9 +16,9 @@ import numpy as np
 from . import build as _build
 
 NPR = 8
-LIM = {"DONOR": 0, "VANL": 1, "MINM": 2, "MC": 3, "WENO5": 9}
+LIM = {"DONOR": 0, "VANL": 1, "MINM": 2, "MC": 3, "PARA": 4, "WENO5": 9}
 FLUX = {"LAXF": 0, "HLL": 1}
-BC = {"OUTFLOW": 0, "POLARAXIS": 4, "PERIODIC": 7}
+BC = {"OUTFLOW": 0, "POLARAXIS": 4, "PERIODIC": 7, "OUTFLOW_COPY": 1000}
 PREC = {"fp64": 0, "mixed": 1}
 
 _lib = None
@@ -84,12 +84,19 @@ def load_library(path=None):
     L.hgpu_alloc_pinned.argtypes = [ctypes.c_size_t, _P(ctypes.c_void_p)]
     L.hgpu_free_pinned.argtypes = [ctypes.c_void_p]
     L.hgpu_fp64_peak.argtypes = [_dp]
+    L.hgpu_create_batch.argtypes = [_P(hgpu_config), ctypes.c_int, _ip, _dp, _dp, _dp, _P(ctypes.c_void_p)]
+    L.hgpu_batch_layout.argtypes = [ctypes.c_void_p, _ip]
+    L.hgpu_batch_status.argtypes = [ctypes.c_void_p, _dp, _dp, _ip, _ip]
+    L.hgpu_step_graph.argtypes = [ctypes.c_void_p, ctypes.c_int, _P(hgpu_stats)]
+    L.hgpu_batch_run.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, _ip, _P(ctypes.c_float), _ip,
+                                 _P(ctypes.c_float)]
     for name in ("hgpu_init_dt", "hgpu_step_ch_timed", "hgpu_set_profiling", "hgpu_kernel_times", "hgpu_alloc_pinned",
                  "hgpu_free_pinned", "hgpu_fp64_peak"):
         getattr(L, name).restype = ctypes.c_int
     for name in ("hgpu_create", "hgpu_upload_geometry", "hgpu_upload_state", "hgpu_download_state", "hgpu_step_ch",
                  "hgpu_advance_stage", "hgpu_fluxcalc", "hgpu_bound_prim", "hgpu_utoprim_batch",
-                 "hgpu_device_prims", "hgpu_sync"):
+                 "hgpu_device_prims", "hgpu_sync", "hgpu_create_batch", "hgpu_batch_layout", "hgpu_batch_status",
+                 "hgpu_step_graph", "hgpu_batch_run"):
         getattr(L, name).restype = ctypes.c_int
     if path == _build.LIB:
         _lib = L
@@ -146,7 +153,7 @@ class HarmGPU:
     @classmethod
     def from_problem(cls, pr, precision="fp64"):
         """Build from an object with the oracle Problem's attributes."""
-        inv_bc = {0: "OUTFLOW", 4: "POLARAXIS", 7: "PERIODIC"}
+        inv_bc = {v: k for k, v in BC.items()}
         o = cls(pr.n[0], pr.n[1], pr.n[2], pr.ng, pr.dx, lim=pr.lim, flux=pr.flux,
                 bc=tuple(inv_bc[b] for b in pr.bc), precision=precision, gam=pr.gam, cour=pr.cour, safe=pr.safe,
                 defcon=pr.defcon, tf=pr.tf, rhominlimit=pr.rhominlimit, uuminlimit=pr.uuminlimit,
@@ -206,6 +213,12 @@ class HarmGPU:
     def step_ch(self, nsteps=1, stats=True):
         st = hgpu_stats()
         _check(self.L, self.L.hgpu_step_ch(self.h, int(nsteps), ctypes.byref(st) if stats else None))
+        return st
+
+    def step_graph(self, nsteps=1, stats=True):
+        """step_ch as replays of one captured CUDA graph per time step."""
+        st = hgpu_stats()
+        _check(self.L, self.L.hgpu_step_graph(self.h, int(nsteps), ctypes.byref(st) if stats else None))
         return st
 
     def advance_stage(self, timeorder):
@@ -299,3 +312,79 @@ def fp64_peak_tflops():
     v = ctypes.c_double()
     _check(L, L.hgpu_fp64_peak(ctypes.byref(v)))
     return v.value
+
+
+class HarmBatch(HarmGPU):
+    """Many independent 1D problems in one context (hgpu_create_batch): one
+    launch of every kernel advances all of them, each with its own gamma, dx,
+    t, dt and end time.  The state is one concatenated 1D line; `layout`
+    gives each instance's first active zone (relative to the line's first
+    active zone) and `split` cuts a line array into per-instance arrays
+    with their own ng ghosts."""
+
+    def __init__(self, n1s, dx1s, gams, tfs, ng=3, lim="MC", flux="HLL", precision="fp64", cour=0.5, safe=1.3,
+                 defcon=1.0, rhominlimit=1e-20, uuminlimit=1e-20, gammamax=25.0, gammafail=2500.0):
+        self.L = load_library()
+        n1s = np.ascontiguousarray(n1s, dtype=np.int32)
+        self.ninst = len(n1s)
+        c = hgpu_config()
+        c.n1, c.n2, c.n3, c.ng = int(n1s.sum() + 2 * ng * (self.ninst - 1)), 1, 1, ng
+        c.lim = LIM[lim] if isinstance(lim, str) else int(lim)
+        c.fluxmethod = FLUX[flux] if isinstance(flux, str) else int(flux)
+        for i, b in enumerate(("OUTFLOW_COPY", "OUTFLOW_COPY", "OUTFLOW", "OUTFLOW", "OUTFLOW", "OUTFLOW")):
+            c.bc[i] = BC[b]
+        c.precision = PREC[precision] if isinstance(precision, str) else int(precision)
+        c.dx[1] = c.dx[2] = c.dx[3] = 1.0
+        c.gam, c.cour, c.safe, c.defcon, c.tf = 4.0 / 3.0, cour, safe, defcon, 0.0
+        c.rhominlimit, c.uuminlimit, c.gammamax, c.gammafail = rhominlimit, uuminlimit, gammamax, gammafail
+        self.cfg = c
+        self.n = (c.n1, 1, 1)
+        self.g = (ng, 0, 0)
+        self.s = (1, 0, 0)
+        self.nt = (c.n1 + 2 * ng, 1, 1)
+        self.gt = (self.nt[0] + 1, 1)
+        self.n1s = n1s
+        self.ng = ng
+        h = ctypes.c_void_p()
+        _check(self.L, self.L.hgpu_create_batch(ctypes.byref(c), self.ninst, _ptr(n1s, ctypes.c_int),
+                                                _ptr(_contig(dx1s, np.float64)), _ptr(_contig(gams, np.float64)),
+                                                _ptr(_contig(tfs, np.float64)), ctypes.byref(h)))
+        self.h = h
+        i0 = np.zeros(self.ninst, dtype=np.int32)
+        _check(self.L, self.L.hgpu_batch_layout(self.h, _ptr(i0, ctypes.c_int)))
+        self.i0 = i0
+
+    def status(self):
+        t = np.zeros(self.ninst)
+        dt = np.zeros(self.ninst)
+        done = np.zeros(self.ninst, dtype=np.int32)
+        nd = ctypes.c_int()
+        _check(self.L, self.L.hgpu_batch_status(self.h, _ptr(t), _ptr(dt), _ptr(done, ctypes.c_int),
+                                                ctypes.byref(nd)))
+        return t, dt, done, nd.value
+
+    def split(self, line):
+        """Per-instance views (own ghosts included) of a line array [nt1, ...]."""
+        ng = self.ng
+        return [line[ng + i0 - ng: ng + i0 + n + ng] for i0, n in zip(self.i0, self.n1s)]
+
+    def join(self, parts, fill=None):
+        """The inverse of split: one line array from per-instance arrays."""
+        shape = (self.nt[0],) + parts[0].shape[1:]
+        out = np.zeros(shape, dtype=parts[0].dtype) if fill is None else np.full(shape, fill, dtype=parts[0].dtype)
+        ng = self.ng
+        for part, i0, n in zip(parts, self.i0, self.n1s):
+            out[ng + i0 - ng: ng + i0 + n + ng] = part
+        return out
+
+    def run(self, check_every=50, max_steps=1_000_000):
+        """Advance until every instance has reached its end time (CUDA-graph
+        replays).  Returns (batch steps, device ms, steps per instance, ms at
+        which each instance was seen finished)."""
+        steps = ctypes.c_int()
+        ms = ctypes.c_float()
+        per = np.zeros(self.ninst, dtype=np.int32)
+        fin = np.zeros(self.ninst, dtype=np.float32)
+        _check(self.L, self.L.hgpu_batch_run(self.h, int(check_every), int(max_steps), ctypes.byref(steps),
+                                             ctypes.byref(ms), _ptr(per, ctypes.c_int), _ptr(fin, ctypes.c_float)))
+        return steps.value, ms.value, per, fin

@@ -47,12 +47,18 @@ extern "C" {
 #define HGPU_LIM_VANL 1
 #define HGPU_LIM_MINM 2
 #define HGPU_LIM_MC 3
+#define HGPU_LIM_PARA 4
 #define HGPU_LIM_WENO5 9
 #define HGPU_FLUX_LAXF 0
 #define HGPU_FLUX_HLL 1
 #define HGPU_BC_OUTFLOW 0
 #define HGPU_BC_POLARAXIS 4
 #define HGPU_BC_PERIODIC 7
+/* x1 OUTFLOW of the reference's general bounds.c (bounds.c:84-135, 218-292):
+   a plain zero-gradient copy.  HGPU_BC_OUTFLOW is the OUTFLOW of
+   bounds.fishmon.c (copy + inflow check + gamma limit); the reference uses
+   id 0 for both, the problem file decides, so the copy gets its own id. */
+#define HGPU_BC_OUTFLOW_COPY 1000
 
 /* precision modes */
 #define HGPU_PREC_FP64 0      /* bit-identical to the reference CPU build */
@@ -60,7 +66,7 @@ extern "C" {
 
 typedef struct {
   int n1, n2, n3;   /* active zones (N1,N2,N3 of the reference) */
-  int ng;           /* ghost zones kept on the device (>= 2 for MC, >= 3 for WENO5) */
+  int ng;           /* ghost zones kept on the device (>= 2 for MC, >= 3 for PARA, >= 6 for WENO5) */
   int lim;          /* slope limiter (lim) */
   int fluxmethod;   /* Riemann solver (fluxmethod) */
   int bc[6];        /* BCtype[X1UP,X1DN,X2UP,X2DN,X3UP,X3DN] */
@@ -142,6 +148,39 @@ int hgpu_utoprim_batch(const double *U, const double *gcov, const double *gcon, 
 #define HGPU_NOALLOC_MAX_ZONES 16384
 int hgpu_utoprim_batch_noalloc(const double *U, const double *gcov, const double *gcon, const double *gdet,
                                double *pr, int *pflag, long long n, double gam, double gammafail, long long *iters);
+
+/* Batch of independent 1D problems in one context (no counterpart in the
+   reference, which runs one problem per process): instance b has n1[b]
+   active zones, zone size dx1[b], adiabatic index gam[b] and end time tf[b],
+   and its own t and dt (step_ch's dt rule per instance; an instance stops
+   when its t reaches tf).  The instances are concatenated along x1, each
+   with its own cfg->ng ghost zones on both sides, in a line of
+   sum(n1[b] + 2 ng) zones that hgpu_upload_state/hgpu_download_state
+   exchange as one 1D array; hgpu_batch_layout gives the x1 index of every
+   instance's first active zone in that line (relative to the line's first
+   active zone).  cfg: n2 = n3 = 1, bc[X1UP] = bc[X1DN] = HGPU_BC_OUTFLOW_COPY;
+   cfg->n1, dx, gam and tf are ignored.  Geometry is uploaded per zone of the
+   line as for a 1D domain.  Every kernel of a step covers all instances. */
+int hgpu_create_batch(const hgpu_config *cfg, int ninst, const int *n1, const double *dx1, const double *gam,
+                      const double *tf, hgpu_ctx **out);
+int hgpu_batch_layout(hgpu_ctx *ctx, int *i0);
+/* per-instance t, dt, done flag (each may be NULL) and the number of finished instances */
+int hgpu_batch_status(hgpu_ctx *ctx, double *t, double *dt, int *done, int *ndone);
+
+/* Advance a batch until every instance has reached its end time (or
+   max_steps batch steps): CUDA-graph replays of check_every steps between
+   reads of the instances' done flags.  *steps: batch steps taken; *ms:
+   device time of the whole run; steps_per_instance[b]: time steps of
+   instance b; done_ms[b]: time at which instance b was seen finished
+   (resolution check_every steps; -1 if it did not finish).  Pointers may be
+   NULL. */
+int hgpu_batch_run(hgpu_ctx *ctx, int check_every, int max_steps, int *steps, float *ms, int *steps_per_instance,
+                   float *done_ms);
+
+/* step_ch as nsteps replays of one CUDA graph holding a whole time step
+   (captured on the first call; profiling must be off).  Same results as
+   hgpu_step_ch. */
+int hgpu_step_graph(hgpu_ctx *ctx, int nsteps, hgpu_stats *stats);
 
 /* Raw device pointers of the resident state for callers that keep data on
    the GPU (e.g. a graph-captured serving loop): primitive planes

@@ -482,6 +482,44 @@ static double slope3(int lim, double yl, double yc, double yr)
   return 0.0; /* DONOR */
 }
 
+/* para4 (interppoint.c:736-869) with PARA2LIM=MC (global.h:425-427, the
+   "Xiaoyue" branch) and JONPARAREDUCE=0: left/right face values of the cell
+   at y[0] from y[-2..2]; min/max are the functions of phys.c:1797-1812 */
+static void para4(const double *y, double *lout, double *rout)
+{
+  double dq0[3], *dq = dq0 + 1, Dqm, Dqp, Dqc, aDqm, aDqp, aDqc, s, l, r, qa, qd, qe;
+  int mm;
+  for (mm = -1; mm <= 1; mm++) {
+    Dqm = 2.0 * (y[mm] - y[mm - 1]);
+    Dqp = 2.0 * (y[mm + 1] - y[mm]);
+    Dqc = 0.5 * (y[mm + 1] - y[mm - 1]);
+    aDqm = fabs(Dqm);
+    aDqp = fabs(Dqp);
+    aDqc = fabs(Dqc);
+    s = Dqm * Dqp;
+    if (s <= 0.) dq[mm] = 0.;
+    else dq[mm] = fmin_ref(aDqc, fmin_ref(aDqm, aDqp)) * ((Dqc > 0.0) ? 1.0 : ((Dqc < 0.0) ? -1.0 : 0.0));
+  }
+  l = 0.5 * (y[0] + y[-1]) - (dq[0] - dq[-1]) / 8.0;
+  r = 0.5 * (y[1] + y[0]) - (dq[1] - dq[0]) / 8.0;
+  l = fmax_ref(fmin_ref(y[0], y[-1]), l);
+  l = fmin_ref(fmax_ref(y[0], y[-1]), l);
+  r = fmax_ref(fmin_ref(y[0], y[1]), r);
+  r = fmin_ref(fmax_ref(y[0], y[1]), r);
+  qa = (r - y[0]) * (y[0] - l);
+  qd = (r - l);
+  qe = 6.0 * (y[0] - 0.5 * (l + r));
+  if (qa <= 0.) {
+    l = y[0];
+    r = y[0];
+  } else {
+    if (qd * (qd - qe) < 0.0) l = 3.0 * y[0] - 2.0 * r;
+    if (qd * (qd + qe) < 0.0) r = 3.0 * y[0] - 2.0 * l;
+  }
+  *lout = l;
+  *rout = r;
+}
+
 /* ------------------------------------------------------------------ */
 /* WENO5 centre-to-edge line reconstruction (lim = WENO5)              */
 /*                                                                     */
@@ -896,6 +934,21 @@ static void fluxcalc_dir(dom *d, const double *pr, int dir, double *F, double *d
 
   if (c->lim == HGO_LIM_WENO5) {
     weno5_faces(d, pr, dir, is, ie, js, je, ks, ke, dq, dq + dom_ntot(d) * NPR);
+  } else if (c->lim == HGO_LIM_PARA) {
+    /* slope_lim_pointtype (interppoint.c:21-151) -> slope_lim_point -> para4
+       on the cells the faces read; pleft | pright as for the line methods */
+    double *pleft = dq, *pright = dq + dom_ntot(d) * NPR;
+    for (i = is - di; i <= ie; i++)
+      for (j = js - dj; j <= je; j++)
+        for (k = ks - dk; k <= ke; k++) {
+          long z = zidx(d, i, j, k);
+          for (pl = 0; pl < NPR; pl++) {
+            double y[5];
+            int l;
+            for (l = -2; l <= 2; l++) y[l + 2] = pr[(z + l * dofs) * NPR + pl];
+            para4(y + 2, &pleft[z * NPR + pl], &pright[z * NPR + pl]);
+          }
+        }
   } else {
     /* slopes over the zones the faces read: centers (face-1) and (face) */
     for (i = is - di; i <= ie; i++)
@@ -914,7 +967,7 @@ static void fluxcalc_dir(dom *d, const double *pr, int dir, double *F, double *d
         long zm = z - dofs;
         int e;
         /* getp2interplr (flux.c:788-808) */
-        if (c->lim == HGO_LIM_WENO5) {
+        if (c->lim == HGO_LIM_WENO5 || c->lim == HGO_LIM_PARA) {
           const double *pleft = dq, *pright = dq + dom_ntot(d) * NPR;
           for (pl = 0; pl < NPR; pl++) {
             p_l[pl] = pright[zm * NPR + pl];
@@ -1409,7 +1462,8 @@ static void inflow_check_x1(const dom *d, int i, double *pr, const geomref *g, i
 }
 
 /* bound_prim_user (bounds.fishmon.c:29-345): x1 OUTFLOW with inflow check
-   and gamma limit, x2 POLARAXIS (POSDEFMETRIC=0, POLEDEATH=1), x3 PERIODIC */
+   and gamma limit, x2 POLARAXIS (POSDEFMETRIC=0, POLEDEATH=1), x3 PERIODIC;
+   and the plain x1 OUTFLOW copy of bounds.c (HGO_BC_OUTFLOW_COPY) */
 static void bound_prim(dom *d, double *p)
 {
   int n1 = d->n[1], n2 = d->n[2], n3 = d->n[3];
@@ -1418,6 +1472,16 @@ static void bound_prim(dom *d, double *p)
   geomref g;
   const hgo_config *c = d->c;
   if (n1 > 1) {
+    if (c->bc[HGO_X1DN] == HGO_BC_OUTFLOW_COPY)
+      for (j = 0; j < n2; j++)
+        for (k = 0; k < n3; k++)
+          for (i = -g1; i <= -1; i++)
+            for (pl = 0; pl < NPR; pl++) p[zidx(d, i, j, k) * NPR + pl] = p[zidx(d, 0, j, k) * NPR + pl];
+    if (c->bc[HGO_X1UP] == HGO_BC_OUTFLOW_COPY)
+      for (j = 0; j < n2; j++)
+        for (k = 0; k < n3; k++)
+          for (i = n1; i <= n1 + g1 - 1; i++)
+            for (pl = 0; pl < NPR; pl++) p[zidx(d, i, j, k) * NPR + pl] = p[zidx(d, n1 - 1, j, k) * NPR + pl];
     if (c->bc[HGO_X1DN] == HGO_BC_OUTFLOW) {
       for (j = 0; j < n2; j++)
         for (k = 0; k < n3; k++) {
@@ -1498,11 +1562,11 @@ static void bound_pflag(dom *d, int *pf)
         for (k = n3; k <= n3 + g3 - 1; k++) pf[zidx(d, i, j, k)] = pf[zidx(d, i, j, k - n3)];
       }
   }
-  if (n1 > 1 && c->bc[HGO_X1DN] == HGO_BC_OUTFLOW)
+  if (n1 > 1 && (c->bc[HGO_X1DN] == HGO_BC_OUTFLOW || c->bc[HGO_X1DN] == HGO_BC_OUTFLOW_COPY))
     for (j = -g2; j <= n2 - 1 + g2; j++)
       for (k = -g3; k <= n3 - 1 + g3; k++)
         for (i = -g1; i <= -1; i++) pf[zidx(d, i, j, k)] = pf[zidx(d, 0, j, k)];
-  if (n1 > 1 && c->bc[HGO_X1UP] == HGO_BC_OUTFLOW)
+  if (n1 > 1 && (c->bc[HGO_X1UP] == HGO_BC_OUTFLOW || c->bc[HGO_X1UP] == HGO_BC_OUTFLOW_COPY))
     for (j = -g2; j <= n2 - 1 + g2; j++)
       for (k = -g3; k <= n3 - 1 + g3; k++)
         for (i = n1; i <= n1 + g1 - 1; i++) pf[zidx(d, i, j, k)] = pf[zidx(d, n1 - 1, j, k)];

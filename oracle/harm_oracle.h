@@ -35,6 +35,10 @@ extern "C" {
 #define HGO_BC_OUTFLOW 0
 #define HGO_BC_POLARAXIS 4
 #define HGO_BC_PERIODIC 7
+/* x1 OUTFLOW of the general bounds.c (bounds.c:84-135, 218-292): a plain
+   zero-gradient copy, without the inflow check and gamma limit that
+   bounds.fishmon.c applies to OUTFLOW (own id: the reference reuses 0) */
+#define HGO_BC_OUTFLOW_COPY 1000
 /* face ids as global.h:467-472 */
 #define HGO_X1UP 0
 #define HGO_X1DN 1

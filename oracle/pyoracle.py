@@ -25,7 +25,7 @@ CENT = 7
 
 LIM = {"DONOR": 0, "VANL": 1, "MINM": 2, "MC": 3, "PARA": 4, "WENO5": 9}
 FLUX = {"LAXF": 0, "HLL": 1}
-BC_OUTFLOW, BC_POLARAXIS, BC_PERIODIC = 0, 4, 7
+BC_OUTFLOW, BC_POLARAXIS, BC_PERIODIC, BC_OUTFLOW_COPY = 0, 4, 7, 1000
 
 
 def build_oracle(force=False):

@@ -1,0 +1,46 @@
+"""Corner-centred div B of the flux-CT scheme (the reference's DIVBFLUXCT,
+global.h:1586-1645): B*gdet at cell centres averaged onto cell corners, then
+differenced, normalised by max(dx) / (|sum of the averages| * gdet_corner / 3)."""
+import numpy as np
+
+SMALL = 1e-50
+
+
+def divb_max(p, gdet, ng, dx, n):
+    """max |div B| over the interior corners of primitives p [nt1][nt2][nt3][8]
+    with gdet [gt1][gt2][8] (CENT=7, CORNT=6): x1 corners 1..n1-1, all x3
+    corners, x2 corners 2..n2-2 -- the polar boundary (POLEDEATH,
+    bounds.fishmon.c) resets B2 in the first and last active rows, so the
+    corners next to them are not constrained by flux-CT."""
+    n1, n2, n3 = n
+    g1, g2, g3 = (ng if n1 > 1 else 0), (ng if n2 > 1 else 0), (ng if n3 > 1 else 0)
+    gc = gdet[:p.shape[0], :p.shape[1], 7][:, :, None]
+    Fg = p[..., 5:8] * gc[..., None]
+    i = np.arange(1, n1) + g1
+    j = np.arange(2, n2 - 1) + g2
+    k = (np.arange(0, n3) if n3 > 1 else np.array([0])) + g3
+    I, J, K = np.meshgrid(i, j, k, indexing="ij")
+    km = K - (1 if n3 > 1 else 0)
+
+    def F(a, b, c, q):
+        return Fg[a, b, c, q]
+
+    def for1(a):  # B1 averaged over (j-1..j, k-1..k) at x1 index a
+        return 0.5 * (0.5 * (F(a, J, K, 0) + F(a, J - 1, K, 0)) + 0.5 * (F(a, J, km, 0) + F(a, J - 1, km, 0)))
+
+    def for2(b):
+        return 0.5 * (0.5 * (F(I, b, K, 1) + F(I - 1, b, K, 1)) + 0.5 * (F(I, b, km, 1) + F(I - 1, b, km, 1)))
+
+    def for3(c):
+        return 0.5 * (0.5 * (F(I, J, c, 2) + F(I, J - 1, c, 2)) + 0.5 * (F(I - 1, J, c, 2) + F(I - 1, J - 1, c, 2)))
+
+    dxs = (dx[0] if n1 > 1 else 1.0, dx[1] if n2 > 1 else 1.0, dx[2] if n3 > 1 else 1.0)
+    diff = (for1(I) - for1(I - 1)) / dxs[0] + (for2(J) - for2(J - 1)) / dxs[1]
+    norm = for1(I) + for1(I - 1) + for2(J) + for2(J - 1)
+    if n3 > 1:
+        diff = diff + (for3(K) - for3(km)) / dxs[2]
+        norm = norm + for3(K) + for3(km)
+    gcorn = gdet[I, J, 6]
+    dmax = max(dx[0], dx[1], dx[2] if n3 > 1 else 0.0)
+    d = diff * (dmax / ((1.0 / 3.0) * gcorn * np.abs(norm) + SMALL))
+    return float(np.max(np.abs(d)))

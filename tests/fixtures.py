@@ -6,7 +6,8 @@ import numpy as np
 from oracle.pyoracle import Problem
 
 GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
-CASES = ["torus2d_16x16_mc_hll", "torus3d_12x12x6_mc_laxf", "torus2d_16x16_weno5_hll", "torus3d_12x12x6_weno5_laxf"]
+CASES = ["torus2d_16x16_mc_hll", "torus3d_12x12x6_mc_laxf", "torus2d_16x16_weno5_hll", "torus3d_12x12x6_weno5_laxf",
+         "torus2d_16x16_para_hll", "torus3d_12x12x6_para_laxf"]
 
 
 def load(name):

@@ -25,9 +25,9 @@ sys.path.insert(0, ROOT)
 from oracle import build_ref  # noqa: E402
 from oracle.pyoracle import RefDump  # noqa: E402
 
-# ghost zones kept in the fixture: MC reads 2, WENO5 (with the reference's
-# MAXBND=11 line lengths) reads 6 per side
-NG = {"MC": 3, "WENO5": 6}
+# ghost zones kept in the fixture: MC reads 2, PARA 3, WENO5 (with the
+# reference's MAXBND=11 line lengths) 6 per side
+NG = {"MC": 3, "PARA": 3, "WENO5": 6}
 
 # name: (n1, n2, n3, lim, flux, cour, nsteps, dump steps)
 CASES = {
@@ -35,6 +35,8 @@ CASES = {
     "torus3d_12x12x6_mc_laxf": (12, 12, 6, "MC", "LAXF", 0.8, 10, [1, 10]),
     "torus2d_16x16_weno5_hll": (16, 16, 1, "WENO5", "HLL", 0.8, 5, [1, 5]),
     "torus3d_12x12x6_weno5_laxf": (12, 12, 6, "WENO5", "LAXF", 0.8, 5, [1, 5]),
+    "torus2d_16x16_para_hll": (16, 16, 1, "PARA", "HLL", 0.8, 5, [1, 5]),
+    "torus3d_12x12x6_para_laxf": (12, 12, 6, "PARA", "LAXF", 0.8, 5, [1, 5]),
 }
 
 

@@ -36,3 +36,14 @@ def test_oracle_newton_iterations_match_reference(orc, name):
         st = orc.step(pr, 1)
         done = s
         assert st.newton_iters == ref[s]["nstroke"]
+
+
+@pytest.mark.parametrize("name", CASES)
+def test_divb_roundoff_in_reference_and_oracle(orc, name):
+    # flux-CT keeps the corner-centred div B at round-off (global.h:1586-1645)
+    from tests.divb import divb_max
+    pr, ref = load(name)
+    for s in sorted(ref):
+        assert divb_max(ref[s]["p"], pr.gdet, pr.ng, pr.dx, pr.n) < 1e-12
+    orc.step(pr, 10)
+    assert divb_max(pr.p, pr.gdet, pr.ng, pr.dx, pr.n) < 1e-12
