@@ -344,6 +344,9 @@ def bench_ours(args, rank, world):
     }
     if other is not None:
         result["other_precision"] = other
+    if not args.no_batch:
+        result["batch_riemann1d"] = bench_riemann_batch()
+        result["serving"] = bench_serving()
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         procs = min(host_cores(), args.cpu_procs)
         cs = cpu_sample(lim)
@@ -358,6 +361,177 @@ def bench_ours(args, rank, world):
         dist.destroy_process_group()
     g.close()
     return result
+
+
+def bench_riemann_batch(ninst=256, seed=2024, sample_single=12, check_every=25):
+    """Batched uneven 1D relativistic-MHD Riemann problems (MC + HLL, CFL 0.5,
+    x in [-0.5, 0.5], t = 0.4): all instances advanced together by shared
+    launches (hgpu_create_batch, CUDA-graph steps) until each reaches t = 0.4,
+    against the same solves run one at a time."""
+    import numpy as np
+
+    from harm_finalwham_b200 import riemann
+    from harm_finalwham_b200.gpu import HarmBatch, HarmGPU
+
+    ng, tf = 3, 0.4
+    probs = riemann.draw(ninst, seed=seed)
+
+    def batch_of(ps):
+        b = HarmBatch([p.n for p in ps], [p.dx for p in ps], [p.gam for p in ps], [tf] * len(ps), ng=ng, lim="MC",
+                      flux="HLL", cour=0.5)
+        b.upload_geometry(*riemann.minkowski_geometry(b.nt[0]))
+        b.upload_state(b.join([riemann.primitives(p, ng) for p in ps]), None, 0.0, 0.0)
+        b.init_dt()
+        return b
+
+    # warm-up: graph capture and instantiation on a small batch
+    w = batch_of(probs[:4])
+    w.run(check_every)
+    w.close()
+    b = batch_of(probs)
+    steps, ms, per, fin = b.run(check_every)
+    b.close()
+    zu = float(np.sum(np.array([p.n for p in probs]) * per))
+    fin = fin[fin >= 0]
+    out = {"instances": ninst, "zones": int(sum(p.n for p in probs)), "zone_updates": zu, "batch_steps": steps,
+           "ms": ms, "value": zu / (ms / 1e3), "unit": "zone-updates/s",
+           "time_to_solution_ms": {"p50": float(np.percentile(fin, 50)), "p99": float(np.percentile(fin, 99)),
+                                   "resolution_steps": check_every},
+           "scheme": "MC + HLL + flux-CT, CFL 0.5, t = 0.4, N ~ U{200..2000}, seeded states",
+           "timing": "device time (CUDA events) of the whole run incl. the done-flag polls"}
+    # one solve at a time: (a) the plain host loop, one step_ch(1) and a time read per step;
+    # (b) the same graph machinery on a batch of one
+    sub = probs[:sample_single]
+    t_plain = 0.0
+    zu_sub = 0.0
+    for pb in sub:
+        g = HarmGPU(pb.n, 1, 1, ng, (pb.dx, 1.0, 1.0), lim="MC", flux="HLL",
+                    bc=("OUTFLOW_COPY", "OUTFLOW_COPY", "OUTFLOW", "OUTFLOW", "OUTFLOW", "OUTFLOW"), gam=pb.gam,
+                    cour=0.5, tf=tf)
+        g.upload_geometry(*riemann.minkowski_geometry(pb.n + 2 * ng))
+        g.upload_state(riemann.primitives(pb, ng), None, 0.0, 0.0)
+        g.init_dt()
+        g.sync()
+        t0 = time.perf_counter()
+        n = 0
+        while n < 100000:
+            g.step_ch(1, stats=False)
+            n += 1
+            if g.time()[0] >= tf:
+                break
+        t_plain += time.perf_counter() - t0
+        zu_sub += pb.n * n
+        g.close()
+    ms_graph = 0.0
+    zu_graph = 0.0
+    for pb in sub:
+        one = batch_of([pb])
+        st, m1, per1, _ = one.run(check_every)
+        one.close()
+        ms_graph += m1
+        zu_graph += pb.n * float(per1[0])
+    out["one_at_a_time"] = {"instances": len(sub), "plain_launches": zu_sub / t_plain,
+                            "graph_batch_of_one": zu_graph / (ms_graph / 1e3), "unit": "zone-updates/s",
+                            "timing": "wall clock per solve (plain), device time (graph)"}
+    out["speedup_vs_one_at_a_time"] = {"plain_launches": out["value"] / (zu_sub / t_plain),
+                                       "graph_batch_of_one": out["value"] / (zu_graph / (ms_graph / 1e3))}
+    return out
+
+
+def serving_requests(count, seed):
+    """A seeded request stream: 60% Kerr torus, 40% Bondi (Schwarzschild,
+    r_s = 8M, monopole field), grids from {32x32, 64x64, 128x128, 256x128}
+    (2D) or {64x32x16, 96x48x32} (3D tori), spin a ~ U(0, 0.99), beta ~
+    logU[10, 1000], 4% internal-energy noise; arrival gaps exponential."""
+    import numpy as np
+
+    from harm_finalwham_b200 import bondi, torus
+
+    rng = np.random.default_rng(seed)
+    grids2 = [(32, 32), (64, 64), (128, 128), (256, 128)]
+    grids3 = [(64, 32, 16), (96, 48, 32)]
+    out = []
+    for q in range(count):
+        beta = 10.0 ** rng.uniform(1.0, 3.0)
+        if rng.random() < 0.6:
+            a = rng.uniform(0.0, 0.99)
+            if rng.random() < 0.2:
+                n = grids3[rng.integers(len(grids3))]
+            else:
+                n = grids2[rng.integers(len(grids2))] + (1,)
+            dom = torus.fm_torus(*n, ng=3, a=a, beta=beta, seed=int(rng.integers(1 << 30)))
+            kind = "torus"
+        else:
+            n = grids2[rng.integers(len(grids2))]
+            dom = bondi.bondi(*n, ng=3, beta=beta, seed=int(rng.integers(1 << 30)))
+            kind = "bondi"
+        out.append((kind, dom))
+    return out
+
+
+def bench_serving(count=12, tf=5.0, mean_gap_ms=40.0, seed=11, budget_bytes=32e9):
+    """Continuous batching: requests arrive on a seeded Poisson clock and go
+    through hgpu_server (admission by device footprint, overlapped solves),
+    against the same requests solved one at a time."""
+    import numpy as np
+
+    from harm_finalwham_b200.gpu import HarmGPU, HarmServer
+
+    reqs = serving_requests(count, seed)
+    rng = np.random.default_rng(seed + 1)
+    arrivals = np.cumsum(rng.exponential(mean_gap_ms / 1e3, count))
+    srv = HarmServer(max_device_bytes=int(budget_bytes), max_active=32, steps_per_chunk=8)
+    ids = {}
+    t0 = time.perf_counter()
+    done_at = {}
+    nsub = 0
+    while len(done_at) < count:
+        now = time.perf_counter() - t0
+        while nsub < count and arrivals[nsub] <= now:
+            ids[srv.submit(reqs[nsub][1], tf)] = nsub
+            nsub += 1
+        srv.poll()
+        for rid, q in ids.items():
+            if q not in done_at and srv.result(rid) is not None:
+                done_at[q] = time.perf_counter() - t0
+        if now > 600:
+            break
+    makespan = max(done_at.values())
+    zu = 0.0
+    lat = []
+    for rid, q in ids.items():
+        res = srv.result(rid)
+        if res is None:
+            continue
+        zu += float(np.prod(reqs[q][1].n)) * res[3]
+        lat.append((done_at[q] - arrivals[q]) * 1e3)
+    srv.close()
+    # the same requests one at a time (each alone, in arrival order)
+    inv = {0: "OUTFLOW", 4: "POLARAXIS", 7: "PERIODIC", 1000: "OUTFLOW_COPY"}
+    t1 = time.perf_counter()
+    zu1 = 0.0
+    for kind, dom in reqs:
+        g = HarmGPU(*dom.n, dom.ng, dom.dx, lim=dom.lim, flux=dom.flux, bc=tuple(inv[b] for b in dom.bc),
+                    gam=dom.gam, cour=dom.cour, tf=tf)
+        g.upload_geometry(dom.gcov, dom.gcon, dom.gcovpert, dom.gdet, dom.conn, dom.floors)
+        g.upload_state(dom.p, None, 0.0, 0.0)
+        g.init_dt()
+        n = 0
+        while n < 100000:
+            g.step_ch(8, stats=False)
+            n += 8
+            if g.time()[0] >= tf:
+                break
+        zu1 += float(np.prod(dom.n)) * n
+        g.close()
+    t_seq = time.perf_counter() - t1
+    return {"requests": count, "kinds": {k: sum(1 for kk, _ in reqs if kk == k) for k in ("torus", "bondi")},
+            "tf": tf, "value": zu / makespan, "unit": "zone-updates/s", "makespan_s": makespan,
+            "time_to_solution_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99))},
+            "one_at_a_time": {"value": zu1 / t_seq, "seconds": t_seq},
+            "speedup_vs_one_at_a_time": (zu / makespan) / (zu1 / t_seq),
+            "note": "wall clock; arrivals Poisson (mean gap %.0f ms); time-to-solution = finish - arrival; the "
+                    "one-at-a-time run steps each solve alone in chunks of 8 steps" % mean_gap_ms}
 
 
 def algorithmic_bytes(kernel, n1, n2, n3, lim="MC"):
@@ -423,6 +597,8 @@ def main():
     ap.add_argument("--workload", default=DEFAULT_WORKLOAD, choices=sorted(WORKLOADS))
     ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-batch", action="store_true",
+                    help="skip the batched 1D Riemann-problem measurement")
     ap.add_argument("--no-compare", action="store_true",
                     help="skip the run of the other precision mode (rate and error vs FP64)")
     ap.add_argument("--e2e-steps", type=int, default=5)

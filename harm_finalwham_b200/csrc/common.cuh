@@ -1,0 +1,468 @@
+// common.cuh -- device data layout and the reconstruction + Riemann-flux
+// kernels shared by the FP64 translation unit (harm_gpu.cu, built with
+// -fmad=false for bit-identity with the reference) and the FP32 one of the
+// mixed-precision path (flux_f32.cu, built with FMA contraction and fast
+// FP32 division/square root, which leave FP64 arithmetic untouched).
+#pragma once
+#include <cuda_runtime.h>
+
+#include "harm_device.cuh"
+#include "harmgpu.h"
+#include "weno5.cuh"
+
+namespace hg {
+
+// geometry component offsets
+constexpr int GLOC = 34;                  // per location: gcov 16, gcon 16, gcovpert_tt, gdet
+constexpr int G_FACE1 = 0, G_FACE2 = 1, G_FACE3 = 2, G_CENT = 3;
+constexpr int G_CORN = 4 * GLOC;          // CORN1, CORN2, CORN3 gdet
+constexpr int G_CONN = G_CORN + 3;        // 64
+constexpr int G_FLOOR = G_CONN + 64;      // 2
+constexpr int G_NCOMP = G_FLOOR + 2;      // 205
+
+// reference location ids (global.h:948-955)
+constexpr int R_FACE1 = 0, R_FACE2 = 1, R_FACE3 = 2, R_CORN1 = 3, R_CORN2 = 4, R_CORN3 = 5, R_CENT = 7;
+
+struct Dims {
+  int n1, n2, n3;
+  int g1, g2, g3;
+  int nt1, nt2, nt3;
+  int s1, s2, s3;
+  int gt1, gt2;
+  long long nz, nij;
+};
+
+// One instance of a batch: a 1D problem occupying the x1 cells
+// i0-ng .. i0+n+ng-1 of the concatenated line (its own ghosts included),
+// with its own gamma, dx, time and dt (step_ch's t, dt, tf per problem).
+struct Inst {
+  int i0, n;
+  double dx, gam, tf;
+  double t, dt;
+  unsigned long long ndtbits;  // x1 min of cour*dx/ctop as ordered bits
+  int done;                    // t reached tf: the instance no longer advances
+  int nsteps;                  // time steps this instance has taken
+};
+
+struct Params {
+  double gam, cour, gammamax, gammafail, rhominlimit, uuminlimit, defcon, safe, tf;
+  double dx1, dx2, dx3;
+  int lim, flux;
+  int bc[6];
+  // batch of independent 1D instances (nullptr: one domain)
+  const int *cell_inst;  // instance of every cell of the line
+  Inst *inst;
+  int ninst;
+};
+
+// device scalars
+struct Scalars {
+  double t, dt;
+  unsigned long long ndtbits[4];   // per-direction min of cour*dx/ctop as ordered bits
+  unsigned long long iters;        // Newton iterations
+  int err;
+  int nfail;                       // failures after Utoprimgen in the last stage
+  int ncand;                       // checksolution candidates
+  int nfixlist;                    // fixup_utoprim list length
+  int nfixed;
+  int overflow;
+  int done;                        // t reached tf: later steps leave the state unchanged
+  int nsteps;                      // time steps taken since the last upload
+  int nfloor;                      // zones raised to a floor by fixup1zone (per call)
+};
+
+__device__ __forceinline__ long long zix(const Dims &d, int i, int j, int k) {
+  return ((long long)(i + d.g1) * d.nt2 + (j + d.g2)) * d.nt3 + (k + d.g3);
+}
+__device__ __forceinline__ long long gix(const Dims &d, int i, int j) {
+  return (long long)(i + d.g1) * d.gt2 + (j + d.g2);
+}
+
+__device__ __forceinline__ void load_metric(const double *__restrict__ G, const Dims &d, long long ij, int slot,
+                                            Metric &m) {
+  const double *b = G + (long long)slot * GLOC * d.nij + ij;
+#pragma unroll
+  for (int q = 0; q < 16; q++) m.gcov[q] = __ldg(b + (long long)q * d.nij);
+#pragma unroll
+  for (int q = 0; q < 16; q++) m.gcon[q] = __ldg(b + (long long)(16 + q) * d.nij);
+  m.gcovpert_tt = __ldg(b + (long long)32 * d.nij);
+  m.g = __ldg(b + (long long)33 * d.nij);
+}
+
+__device__ __forceinline__ void load_prim(const double *__restrict__ P, const Dims &d, long long z, double *pr) {
+#pragma unroll
+  for (int v = 0; v < NPR; v++) pr[v] = P[(long long)v * d.nz + z];
+}
+__device__ __forceinline__ void store_prim(double *__restrict__ P, const Dims &d, long long z, const double *pr) {
+#pragma unroll
+  for (int v = 0; v < NPR; v++) P[(long long)v * d.nz + z] = pr[v];
+}
+
+// box iteration helper: flat index -> (i,j,k) with k fastest
+struct Box {
+  int i0, j0, k0, ni, nj, nk;
+  __host__ __device__ long long size() const { return (long long)ni * nj * nk; }
+};
+__device__ __forceinline__ void box_ijk(const Box &b, long long t, int &i, int &j, int &k) {
+  k = (int)(t % b.nk);
+  long long r = t / b.nk;
+  j = (int)(r % b.nj);
+  i = (int)(r / b.nj);
+  i += b.i0;
+  j += b.j0;
+  k += b.k0;
+}
+
+__device__ __forceinline__ void warp_min_atomic(unsigned long long *dst, double v, bool active) {
+  unsigned long long bits = active ? (unsigned long long)__double_as_longlong(v) : 0xFFFFFFFFFFFFFFFFull;
+  // NaN is never selected by the reference's `if (dtij < ndt)`: map it out
+  if (active && !(v == v)) bits = 0xFFFFFFFFFFFFFFFFull;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    unsigned long long ob = __shfl_xor_sync(0xffffffffu, bits, o);
+    bits = ob < bits ? ob : bits;
+  }
+  if ((threadIdx.x & 31) == 0 && bits != 0xFFFFFFFFFFFFFFFFull) atomicMin(dst, bits);
+}
+
+// MC / VANL / MINM / DONOR slopes (interppoint.c:387-443)
+template <typename T>
+__device__ __forceinline__ T slope3(int lim, T yl, T yc, T yr) {
+  if (lim == HGPU_LIM_MC) {
+    T Dqm = T(2.0) * (yc - yl);
+    T Dqp = T(2.0) * (yr - yc);
+    T Dqc = T(0.5) * (yr - yl);
+    T mm = ((Dqm) * (Dqp) <= T(0)) ? T(0.0) : ((fabs(Dqm) < fabs(Dqp)) ? (Dqm) : (Dqp));
+    return ((Dqc) * (mm) <= T(0)) ? T(0.0) : ((fabs(Dqc) < fabs(mm)) ? (Dqc) : (mm));
+  } else if (lim == HGPU_LIM_VANL) {
+    T Dqm = (yc - yl);
+    T Dqp = (yr - yc);
+    T s = Dqm * Dqp;
+    if (s <= T(0.)) return T(0.);
+    return (T(2.0) * s / (Dqm + Dqp));
+  } else if (lim == HGPU_LIM_MINM) {
+    T Dqm = T(1.0) * (yc - yl);
+    T Dqp = T(1.0) * (yr - yc);
+    T Dqc = T(0.5) * (yr - yl);
+    T mm = ((Dqm) * (Dqc) <= T(0)) ? T(0.0) : ((fabs(Dqm) < fabs(Dqc)) ? (Dqm) : (Dqc));
+    return ((mm) * (Dqp) <= T(0)) ? T(0.0) : ((fabs(mm) < fabs(Dqp)) ? (mm) : (Dqp));
+  }
+  return T(0.0);
+}
+
+// para4 (interppoint.c:736-869) with PARA2LIM=MC and JONPARAREDUCE=0: face
+// values of the cell at y[0] from y[-2..2]
+template <typename T>
+__device__ __forceinline__ void para4(const T *y, T *lout, T *rout) {
+  T dq[3];
+#pragma unroll
+  for (int mm = -1; mm <= 1; mm++) {
+    T Dqm = T(2.0) * (y[mm] - y[mm - 1]);
+    T Dqp = T(2.0) * (y[mm + 1] - y[mm]);
+    T Dqc = T(0.5) * (y[mm + 1] - y[mm - 1]);
+    T aDqm = fabs(Dqm), aDqp = fabs(Dqp), aDqc = fabs(Dqc);
+    T s = Dqm * Dqp;
+    T sg = (Dqc > T(0.0)) ? T(1.0) : ((Dqc < T(0.0)) ? T(-1.0) : T(0.0));
+    dq[mm + 1] = (s <= T(0.)) ? T(0.) : min_ref(aDqc, min_ref(aDqm, aDqp)) * sg;
+  }
+  T l = T(0.5) * (y[0] + y[-1]) - (dq[1] - dq[0]) / T(8.0);
+  T r = T(0.5) * (y[1] + y[0]) - (dq[2] - dq[1]) / T(8.0);
+  l = max_ref(min_ref(y[0], y[-1]), l);
+  l = min_ref(max_ref(y[0], y[-1]), l);
+  r = max_ref(min_ref(y[0], y[1]), r);
+  r = min_ref(max_ref(y[0], y[1]), r);
+  T qa = (r - y[0]) * (y[0] - l);
+  T qd = (r - l);
+  T qe = T(6.0) * (y[0] - T(0.5) * (l + r));
+  if (qa <= T(0.)) {
+    l = y[0];
+    r = y[0];
+  } else {
+    if (qd * (qd - qe) < T(0.0)) l = T(3.0) * y[0] - T(2.0) * r;
+    if (qd * (qd + qe) < T(0.0)) r = T(3.0) * y[0] - T(2.0) * l;
+  }
+  *lout = l;
+  *rout = r;
+}
+
+// ---------------------------------------------------------------------------
+// WENO5 line reconstruction (slope_lim_linetype_c2e, interpline.c:517-678) as
+// two cell-parallel passes; see weno5.cuh.  Scratch WA holds, per primitive
+// v, 4 planes: the SMONO code (indicator in [0,1], -1 at a cusp) and the
+// three unoptimised weights.
+// ---------------------------------------------------------------------------
+constexpr int W5_PLANES = 4;
+
+// Minimum resident 128-thread blocks per SM asked of the register allocator
+// for the FP64-heavy kernels (launch_bounds' second argument).  With 64K
+// registers per SM, B blocks cap a thread at 65536 / (128 B) registers:
+// 1-2 -> 255 (8 warps/SM), 3 -> 170 (12 warps), 4 -> 128 (16 warps), more
+// warps to hide FP64 latency at the price of spills to local memory.
+// Defaults from a B200 sweep (256x128x128 torus, 1/3/4/5 blocks for flux and
+// update, 1/5/6/8 for weno_b, 1/8/10 for weno_a): flux 4 (-11% WENO5, -21%
+// MC), weno_b 8 (-33%), weno_a 8 (-3%); update is fastest unconstrained.
+#ifndef HG_MINB_FLUX
+#define HG_MINB_FLUX 4
+#endif
+#ifndef HG_MINB_UPDATE
+#define HG_MINB_UPDATE 1
+#endif
+#ifndef HG_MINB_INVERT
+#define HG_MINB_INVERT 1
+#endif
+#ifndef HG_MINB_WENO_A
+#define HG_MINB_WENO_A 8
+#endif
+#ifndef HG_MINB_WENO_B
+#define HG_MINB_WENO_B 8
+#endif
+// the same for the FP32 kernels of the mixed-precision path (B200 sweep of
+// 4/6/8 for flux, 8/10/12 for weno_a/b: flux 8 -4%, the rest within 2%)
+#ifndef HG_MINB_FLUX_F32
+#define HG_MINB_FLUX_F32 8
+#endif
+#ifndef HG_MINB_WENO_A_F32
+#define HG_MINB_WENO_A_F32 12
+#endif
+#ifndef HG_MINB_WENO_B_F32
+#define HG_MINB_WENO_B_F32 8
+#endif
+template <typename T> struct MinBlocks;
+template <> struct MinBlocks<double> {
+  static constexpr int flux = HG_MINB_FLUX, weno_a = HG_MINB_WENO_A, weno_b = HG_MINB_WENO_B;
+};
+template <> struct MinBlocks<float> {
+  static constexpr int flux = HG_MINB_FLUX_F32, weno_a = HG_MINB_WENO_A_F32, weno_b = HG_MINB_WENO_B_F32;
+};
+
+template <int DIR>
+__device__ __forceinline__ long long dir_stride(const Dims &d) {
+  return (DIR == 1) ? (long long)d.nt2 * d.nt3 : ((DIR == 2) ? (long long)d.nt3 : 1);
+}
+
+// metric of one location converted to the arithmetic type of a kernel
+template <typename T>
+__device__ __forceinline__ void load_metric_t(const double *__restrict__ G, const Dims &d, long long ij, int slot,
+                                              MetricT<T> &m) {
+  const double *b = G + (long long)slot * GLOC * d.nij + ij;
+#pragma unroll
+  for (int q = 0; q < 16; q++) m.gcov[q] = (T)__ldg(b + (long long)q * d.nij);
+#pragma unroll
+  for (int q = 0; q < 16; q++) m.gcon[q] = (T)__ldg(b + (long long)(16 + q) * d.nij);
+  m.gcovpert_tt = (T)__ldg(b + (long long)32 * d.nij);
+  m.g = (T)__ldg(b + (long long)33 * d.nij);
+}
+
+// pass A over line cells -4..n+3: cusp test, SMONO indicator, unoptimised
+// weights.  T = double: the reference's arithmetic; T = float: mixed path.
+template <int DIR, typename T>
+__global__ void __launch_bounds__(128, MinBlocks<T>::weno_a) weno_a_kernel(Dims d, Box box, const double *__restrict__ pb,
+                                                                     T *__restrict__ WA) {
+  long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= box.size()) return;
+  int i, j, k;
+  box_ijk(box, t, i, j, k);
+  long long z = zix(d, i, j, k);
+  const long long o = dir_stride<DIR>(d);
+  for (int v = 0; v < NPR; v++) {
+    const double *q = pb + (long long)v * d.nz + z;
+    T ya[5] = {(T)__ldg(q - 2 * o), (T)__ldg(q - o), (T)__ldg(q), (T)__ldg(q + o), (T)__ldg(q + 2 * o)};
+    const T *y = ya + 2;
+    bool c = w5::cusp(y);
+    T m0 = c ? T(0.0) : w5::mono(y);
+    T w[3];
+    w5::unopt3(m0, y, w);
+    T *out = WA + (long long)v * W5_PLANES * d.nz + z;
+    out[0] = c ? T(-1.0) : m0;
+    out[d.nz] = w[0];
+    out[2 * d.nz] = w[1];
+    out[3 * d.nz] = w[2];
+  }
+}
+
+// pass B over line cells -1..n: dP/P, ratios, reduction, face values
+template <int DIR, typename T>
+__global__ void __launch_bounds__(128, MinBlocks<T>::weno_b) weno_b_kernel(Dims d, Params P, Box box,
+                                                                     const double *__restrict__ pb,
+                                                                     const double *__restrict__ G,
+                                                                     const T *__restrict__ WA, T *__restrict__ pL,
+                                                                     T *__restrict__ pR) {
+  long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= box.size()) return;
+  int i, j, k;
+  box_ijk(box, t, i, j, k);
+  long long z = zix(d, i, j, k);
+  const long long o = dir_stride<DIR>(d);
+  // compute_df_line_new (interpline.c:2148-2222): jump indicator from the
+  // primitives of the cells -1, 0, +1 along the line and their CENT metrics
+  T dP;
+  {
+    T pm[NPR], p0[NPR], pp[NPR];
+#pragma unroll
+    for (int v = 0; v < NPR; v++) {
+      pm[v] = (T)pb[(long long)v * d.nz + z - o];
+      p0[v] = (T)pb[(long long)v * d.nz + z];
+      pp[v] = (T)pb[(long long)v * d.nz + z + o];
+    }
+    StateT<T> ql, q, qr;
+    T a, b, c;
+    MetricT<T> m;
+    load_metric_t(G, d, gix(d, i - (DIR == 1), j - (DIR == 2)), G_CENT, m);
+    get_state(pm, m, ql);
+    a = compute_1plusud0(m, ql);
+    load_metric_t(G, d, gix(d, i, j), G_CENT, m);
+    get_state(p0, m, q);
+    b = compute_1plusud0(m, q);
+    load_metric_t(G, d, gix(d, i + (DIR == 1), j + (DIR == 2)), G_CENT, m);
+    get_state(pp, m, qr);
+    c = compute_1plusud0(m, qr);
+    T gam = (T)(P.cell_inst ? P.inst[P.cell_inst[z]].gam : P.gam);
+    T parl = a * (ql.ucon[0]);
+    T par = b * (q.ucon[0]);
+    T parr = c * (qr.ucon[0]);
+    T uparl = gam * pm[UU] * (ql.ucon[0] * ql.ucov[0]) + (gam - T(1.0)) * pm[UU];
+    T upar = gam * p0[UU] * (q.ucon[0] * q.ucov[0]) + (gam - T(1.0)) * p0[UU];
+    T uparr = gam * pp[UU] * (qr.ucon[0] * qr.ucov[0]) + (gam - T(1.0)) * pp[UU];
+    dP = (fabs(p0[RHO] * (parr - parl)) + fabs(uparr - uparl)) / (fabs(p0[RHO] * par) + fabs(upar) + w5::K<T>::tiny);
+  }
+  // apply_additional_reduction_to_weights (reconstructeno.c:650-700)
+  T ss = w5::wmin((fabs(dP) - T(0.5 * w5::kDpFrac)) / T(0.5 * w5::kDpFrac), T(1.));
+  for (int v = 0; v < NPR; v++) {
+    const T *wa = WA + (long long)v * W5_PLANES * d.nz + z;
+    // codes of cells -1, 0, +1 and weights of cells -3..+3 (w0 and w2 of the neighbours)
+    T cm = __ldg(wa - o), c0 = __ldg(wa), cp = __ldg(wa + o);
+    const T *w0p = wa + d.nz, *w1p = wa + 2 * d.nz, *w2p = wa + 3 * d.nz;
+    T wc[3] = {__ldg(w0p), __ldg(w1p), __ldg(w2p)};
+    T wm[3] = {__ldg(w0p - o), T(0.0), __ldg(w2p - o)};
+    T wp[3] = {__ldg(w0p + o), T(0.0), __ldg(w2p + o)};
+    T w_m3_0 = __ldg(w0p - 3 * o), w_m2_0 = __ldg(w0p - 2 * o);
+    T w_p2_2 = __ldg(w2p + 2 * o), w_p3_2 = __ldg(w2p + 3 * o);
+    T fd_m = w5::ratio_lof(wm, w_m3_0, __ldg(w2p + o), cm == T(-1.0) ? T(1.0) : T(0.0));
+    T fd_p = w5::ratio_lof(wp, __ldg(w0p - o), w_p3_2, cp == T(-1.0) ? T(1.0) : T(0.0));
+    T lof = w5::ratio_lof(wc, w_m2_0, w_p2_2, c0 == T(-1.0) ? T(1.0) : T(0.0));
+    lof = w5::wmax(lof, ss * fd_p);
+    lof = w5::wmax(lof, ss * fd_m);
+    const double *q = pb + (long long)v * d.nz + z;
+    T ya[5] = {(T)__ldg(q - 2 * o), (T)__ldg(q - o), (T)__ldg(q), (T)__ldg(q + o), (T)__ldg(q + 2 * o)};
+    bool cu = (c0 == T(-1.0));
+    T m0 = cu ? T(0.0) : c0;
+    T yl, yr;
+    w5::faces(ya + 2, m0, cu, wc, lof, &yl, &yr);
+    pL[(long long)v * d.nz + z] = yl;
+    pR[(long long)v * d.nz + z] = yr;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// face flux kernel (one per direction); RECON 0: MC-type slopes in the
+// kernel, RECON 1: Riemann states from the WENO5 face values pL/pR
+// ---------------------------------------------------------------------------
+template <int DIR, int RECON, typename T>
+__global__ void __launch_bounds__(128, MinBlocks<T>::flux) flux_kernel(Dims d, Params P, Box box,
+                                                                 const double *__restrict__ pb,
+                                                                 const T *__restrict__ pL, const T *__restrict__ pR,
+                                                                 const double *__restrict__ G, double *__restrict__ F,
+                                                                 Scalars *sc) {
+  long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  bool active = t < box.size();
+  double dtij = 0.0;
+  if (active) {
+    int i, j, k;
+    box_ijk(box, t, i, j, k);
+    long long z = zix(d, i, j, k);
+    const long long o = dir_stride<DIR>(d);
+    T p_l[NPR], p_r[NPR];
+    if (RECON == 1) {
+      // getp2interplr (flux.c:788-808), line-type branch
+#pragma unroll
+      for (int v = 0; v < NPR; v++) {
+        p_l[v] = __ldg(pR + (long long)v * d.nz + z - o);
+        p_r[v] = __ldg(pL + (long long)v * d.nz + z);
+      }
+    } else if (RECON == 2) {
+      // PARA: pright of the cell on the left, pleft of the cell on the right
+#pragma unroll
+      for (int v = 0; v < NPR; v++) {
+        const double *q = pb + (long long)v * d.nz + z;
+        T y[6];
+#pragma unroll
+        for (int l = 0; l < 6; l++) y[l] = (T)__ldg(q + (l - 3) * o);
+        T dummy;
+        para4(y + 2, &dummy, &p_l[v]);
+        para4(y + 3, &p_r[v], &dummy);
+      }
+    } else {
+#pragma unroll
+      for (int v = 0; v < NPR; v++) {
+        const double *q = pb + (long long)v * d.nz + z;
+        T ym2 = (T)__ldg(q - 2 * o), ym1 = (T)__ldg(q - o), y0 = (T)__ldg(q), yp1 = (T)__ldg(q + o);
+        T dqm = slope3(P.lim, ym2, ym1, y0);
+        T dq0 = slope3(P.lim, ym1, y0, yp1);
+        // getp2interplr (flux.c:788-808)
+        p_l[v] = ym1 + T(0.5) * dqm;
+        p_r[v] = y0 - T(0.5) * dq0;
+      }
+    }
+    // BDIRCONT (flux.c:629-633)
+    p_l[B1 + DIR - 1] = p_r[B1 + DIR - 1] = T(0.5) * (p_l[B1 + DIR - 1] + p_r[B1 + DIR - 1]);
+    MetricT<T> m;
+    load_metric_t(G, d, gix(d, i, j), DIR - 1, m);
+    StateT<T> ql, qr;
+    EMT<T> el, er;
+    T Fl[NPR], Fr[NPR], Ul[NPR], Ur[NPR];
+    int b = P.cell_inst ? P.cell_inst[z] : -1;
+    const T gam = (T)(b >= 0 ? P.inst[b].gam : P.gam);
+    int err = 0;
+    if (get_state(p_l, m, ql)) err |= ERR_UTCALC_DISCR;
+    em_prepare(p_l, m, ql, el);
+    primtoflux(p_l, ql, el, DIR, m, gam, Fl);
+    primtoflux(p_l, ql, el, 0, m, gam, Ul);
+    if (get_state(p_r, m, qr)) err |= ERR_UTCALC_DISCR;
+    em_prepare(p_r, m, qr, er);
+    primtoflux(p_r, qr, er, DIR, m, gam, Fr);
+    primtoflux(p_r, qr, er, 0, m, gam, Ur);
+    T cmaxl = T(0.), cminl = T(0.), cmaxr = T(0.), cminr = T(0.);
+    err |= vchar(p_l, ql, DIR, m, gam, &cmaxl, &cminl);
+    err |= vchar(p_r, qr, DIR, m, gam, &cmaxr, &cminr);
+    // cminmax_calc (wavespeeds.c:325-385)
+    T lmin = min_ref(cminl, cminr);
+    T lmax = max_ref(cmaxl, cmaxr);
+    lmin = fabs(max_ref(T(0.), -lmin));
+    lmax = fabs(max_ref(T(0.), lmax));
+    T cmin = lmin, cmax = lmax, ctop = max_ref(lmax, lmin);
+    double Fo[NPR];
+    if (P.flux == HGPU_FLUX_HLL && (cmax + cmin != T(0.0))) {
+#pragma unroll
+      for (int v = 0; v < NPR; v++)
+        Fo[v] = (double)(((cmax * Fl[v] + cmin * Fr[v]) - (cmax * cmin) * (Ur[v] - Ul[v])) / (cmax + cmin));
+    } else {
+#pragma unroll
+      for (int v = 0; v < NPR; v++) Fo[v] = (double)(T(0.5) * ((Fl[v] + Fr[v]) - ctop * (Ur[v] - Ul[v])));
+    }
+    // flux_ct gdet strip (fluxct.c:74-96), in FP64 in both precision modes
+    const double gface = __ldg(G + (long long)((DIR - 1) * GLOC + 33) * d.nij + gix(d, i, j));
+    Fo[B1] /= gface;
+    Fo[B2] /= gface;
+    Fo[B3] /= gface;
+    store_prim(F, d, z, Fo);
+    double dxd = (DIR == 1) ? P.dx1 : ((DIR == 2) ? P.dx2 : P.dx3);
+    if (b >= 0) {
+      // batch: faces 0..n of a running instance feed its own dt
+      const Inst &I = P.inst[b];
+      int loc = i - I.i0;
+      active = false;
+      if (loc >= 0 && loc <= I.n && !I.done) {
+        dtij = P.cour * I.dx / (double)ctop;
+        if (dtij == dtij) atomicMin(&P.inst[b].ndtbits, (unsigned long long)__double_as_longlong(dtij));
+        if (err) atomicOr(&sc->err, err);
+      }
+    } else {
+      dtij = P.cour * dxd / (double)ctop;
+      if (err) atomicOr(&sc->err, err);
+    }
+  }
+  warp_min_atomic(&sc->ndtbits[DIR], dtij, active);
+}
+
+
+}  // namespace hg

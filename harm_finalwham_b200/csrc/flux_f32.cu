@@ -1,0 +1,27 @@
+// flux_f32.cu -- the FP32 instantiations of the reconstruction and Riemann
+// kernels (mixed-precision path, HGPU_PREC_MIXED).  This translation unit is
+// compiled with FMA contraction and fast FP32 division and square root
+// (-fmad=true -prec-div=false -prec-sqrt=false -ftz=true): none of these
+// flags changes FP64 arithmetic, and the FP64 kernels live in harm_gpu.cu,
+// compiled with -fmad=false.  harm_gpu.cu launches these instantiations
+// (declared there as extern templates).
+#include "common.cuh"
+
+namespace hg {
+
+#define HG_F32_INSTANCES(DIR)                                                                                      \
+  template __global__ void weno_a_kernel<DIR, float>(Dims, Box, const double *, float *);                         \
+  template __global__ void weno_b_kernel<DIR, float>(Dims, Params, Box, const double *, const double *,           \
+                                                     const float *, float *, float *);                              \
+  template __global__ void flux_kernel<DIR, 0, float>(Dims, Params, Box, const double *, const float *,           \
+                                                      const float *, const double *, double *, Scalars *);          \
+  template __global__ void flux_kernel<DIR, 1, float>(Dims, Params, Box, const double *, const float *,           \
+                                                      const float *, const double *, double *, Scalars *);          \
+  template __global__ void flux_kernel<DIR, 2, float>(Dims, Params, Box, const double *, const float *,           \
+                                                      const float *, const double *, double *, Scalars *);
+
+HG_F32_INSTANCES(1)
+HG_F32_INSTANCES(2)
+HG_F32_INSTANCES(3)
+
+}  // namespace hg

@@ -11,14 +11,18 @@
 //
 // Work per RK substep (the reference's advance(), step_ch.c:94-186):
 //   weno_a/weno_b     WENO5 line reconstruction (interpline.c:517-678) in two
-//                     cell-parallel passes (lim = WENO5 only; weno5.cuh)
-//   flux_kernel<dir>  fluxcalc_standard (flux.c:469-680) fused with the MC
-//                     slopes, both Riemann states, vchar, HLL/LaxF, the gdet
-//                     strip of flux_ct and the dt-min
+//                     cell-parallel passes (lim = WENO5 only; weno5.cuh,
+//                     common.cuh)
+//   flux_kernel<dir>  fluxcalc_standard (flux.c:469-680) fused with the
+//                     MC/PARA reconstruction (or reading the WENO5 face
+//                     values), both Riemann states, vchar, HLL/LaxF, the gdet
+//                     strip of flux_ct and the dt-min (common.cuh; the FP32
+//                     instances of the mixed path are built in flux_f32.cu)
 //   emf_kernel        corner EMFs of flux_ct (fluxct.c:148-218)
-//   update_kernel     advance_standard zone loop (advance.c:143-213): U(pi),
+//   conserve_kernel   advance_standard zone loop (advance.c:143-213): U(pi),
 //                     source_conn, flux divergence (B fluxes rebuilt from the
-//                     EMFs, fluxct.c:724-781), dUtoU, Utoprimgen, fixup1zone
+//                     EMFs, fluxct.c:724-781), dUtoU
+//   invert_kernel     Utoprimgen and, on the final substep, fixup1zone
 //   bound kernels     bound_prim (bounds.fishmon.c:29-345)
 //   fixup kernels     post_fixup (fixup.c:37-96) in an order-independent
 //                     formulation that reproduces the reference's sequential
@@ -33,11 +37,30 @@
 #include <new>
 #include <vector>
 
+#include "common.cuh"
 #include "harm_device.cuh"
 #include "harmgpu.h"
 #include "weno5.cuh"
 
 using namespace hg;
+
+// FP32 instantiations of the reconstruction and flux kernels are compiled in
+// flux_f32.cu (FMA and fast FP32 division there; this unit keeps -fmad=false)
+namespace hg {
+#define HG_F32_EXTERN(DIR)                                                                                         \
+  extern template __global__ void weno_a_kernel<DIR, float>(Dims, Box, const double *, float *);                  \
+  extern template __global__ void weno_b_kernel<DIR, float>(Dims, Params, Box, const double *, const double *,    \
+                                                            const float *, float *, float *);                       \
+  extern template __global__ void flux_kernel<DIR, 0, float>(Dims, Params, Box, const double *, const float *,    \
+                                                             const float *, const double *, double *, Scalars *);   \
+  extern template __global__ void flux_kernel<DIR, 1, float>(Dims, Params, Box, const double *, const float *,    \
+                                                             const float *, const double *, double *, Scalars *);   \
+  extern template __global__ void flux_kernel<DIR, 2, float>(Dims, Params, Box, const double *, const float *,    \
+                                                             const float *, const double *, double *, Scalars *);
+HG_F32_EXTERN(1)
+HG_F32_EXTERN(2)
+HG_F32_EXTERN(3)
+}  // namespace hg
 
 namespace {
 
@@ -55,452 +78,6 @@ void set_err(const char *fmt, const char *a = "", int b = 0) {
       return HGPU_E_CUDA;                                                      \
     }                                                                          \
   } while (0)
-
-// geometry component offsets
-constexpr int GLOC = 34;                  // per location: gcov 16, gcon 16, gcovpert_tt, gdet
-constexpr int G_FACE1 = 0, G_FACE2 = 1, G_FACE3 = 2, G_CENT = 3;
-constexpr int G_CORN = 4 * GLOC;          // CORN1, CORN2, CORN3 gdet
-constexpr int G_CONN = G_CORN + 3;        // 64
-constexpr int G_FLOOR = G_CONN + 64;      // 2
-constexpr int G_NCOMP = G_FLOOR + 2;      // 205
-
-// reference location ids (global.h:948-955)
-constexpr int R_FACE1 = 0, R_FACE2 = 1, R_FACE3 = 2, R_CORN1 = 3, R_CORN2 = 4, R_CORN3 = 5, R_CENT = 7;
-
-struct Dims {
-  int n1, n2, n3;
-  int g1, g2, g3;
-  int nt1, nt2, nt3;
-  int s1, s2, s3;
-  int gt1, gt2;
-  long long nz, nij;
-};
-
-// One instance of a batch: a 1D problem occupying the x1 cells
-// i0-ng .. i0+n+ng-1 of the concatenated line (its own ghosts included),
-// with its own gamma, dx, time and dt (step_ch's t, dt, tf per problem).
-struct Inst {
-  int i0, n;
-  double dx, gam, tf;
-  double t, dt;
-  unsigned long long ndtbits;  // x1 min of cour*dx/ctop as ordered bits
-  int done;                    // t reached tf: the instance no longer advances
-  int nsteps;                  // time steps this instance has taken
-};
-
-struct Params {
-  double gam, cour, gammamax, gammafail, rhominlimit, uuminlimit, defcon, safe, tf;
-  double dx1, dx2, dx3;
-  int lim, flux;
-  int bc[6];
-  // batch of independent 1D instances (nullptr: one domain)
-  const int *cell_inst;  // instance of every cell of the line
-  Inst *inst;
-  int ninst;
-};
-
-// device scalars
-struct Scalars {
-  double t, dt;
-  unsigned long long ndtbits[4];   // per-direction min of cour*dx/ctop as ordered bits
-  unsigned long long iters;        // Newton iterations
-  int err;
-  int nfail;                       // failures after Utoprimgen in the last stage
-  int ncand;                       // checksolution candidates
-  int nfixlist;                    // fixup_utoprim list length
-  int nfixed;
-  int overflow;
-};
-
-__device__ __forceinline__ long long zix(const Dims &d, int i, int j, int k) {
-  return ((long long)(i + d.g1) * d.nt2 + (j + d.g2)) * d.nt3 + (k + d.g3);
-}
-__device__ __forceinline__ long long gix(const Dims &d, int i, int j) {
-  return (long long)(i + d.g1) * d.gt2 + (j + d.g2);
-}
-
-__device__ __forceinline__ void load_metric(const double *__restrict__ G, const Dims &d, long long ij, int slot,
-                                            Metric &m) {
-  const double *b = G + (long long)slot * GLOC * d.nij + ij;
-#pragma unroll
-  for (int q = 0; q < 16; q++) m.gcov[q] = __ldg(b + (long long)q * d.nij);
-#pragma unroll
-  for (int q = 0; q < 16; q++) m.gcon[q] = __ldg(b + (long long)(16 + q) * d.nij);
-  m.gcovpert_tt = __ldg(b + (long long)32 * d.nij);
-  m.g = __ldg(b + (long long)33 * d.nij);
-}
-
-__device__ __forceinline__ void load_prim(const double *__restrict__ P, const Dims &d, long long z, double *pr) {
-#pragma unroll
-  for (int v = 0; v < NPR; v++) pr[v] = P[(long long)v * d.nz + z];
-}
-__device__ __forceinline__ void store_prim(double *__restrict__ P, const Dims &d, long long z, const double *pr) {
-#pragma unroll
-  for (int v = 0; v < NPR; v++) P[(long long)v * d.nz + z] = pr[v];
-}
-
-// box iteration helper: flat index -> (i,j,k) with k fastest
-struct Box {
-  int i0, j0, k0, ni, nj, nk;
-  __host__ __device__ long long size() const { return (long long)ni * nj * nk; }
-};
-__device__ __forceinline__ void box_ijk(const Box &b, long long t, int &i, int &j, int &k) {
-  k = (int)(t % b.nk);
-  long long r = t / b.nk;
-  j = (int)(r % b.nj);
-  i = (int)(r / b.nj);
-  i += b.i0;
-  j += b.j0;
-  k += b.k0;
-}
-
-__device__ __forceinline__ void warp_min_atomic(unsigned long long *dst, double v, bool active) {
-  unsigned long long bits = active ? (unsigned long long)__double_as_longlong(v) : 0xFFFFFFFFFFFFFFFFull;
-  // NaN is never selected by the reference's `if (dtij < ndt)`: map it out
-  if (active && !(v == v)) bits = 0xFFFFFFFFFFFFFFFFull;
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) {
-    unsigned long long ob = __shfl_xor_sync(0xffffffffu, bits, o);
-    bits = ob < bits ? ob : bits;
-  }
-  if ((threadIdx.x & 31) == 0 && bits != 0xFFFFFFFFFFFFFFFFull) atomicMin(dst, bits);
-}
-
-// MC / VANL / MINM / DONOR slopes (interppoint.c:387-443)
-template <typename T>
-__device__ __forceinline__ T slope3(int lim, T yl, T yc, T yr) {
-  if (lim == HGPU_LIM_MC) {
-    T Dqm = T(2.0) * (yc - yl);
-    T Dqp = T(2.0) * (yr - yc);
-    T Dqc = T(0.5) * (yr - yl);
-    T mm = ((Dqm) * (Dqp) <= T(0)) ? T(0.0) : ((fabs(Dqm) < fabs(Dqp)) ? (Dqm) : (Dqp));
-    return ((Dqc) * (mm) <= T(0)) ? T(0.0) : ((fabs(Dqc) < fabs(mm)) ? (Dqc) : (mm));
-  } else if (lim == HGPU_LIM_VANL) {
-    T Dqm = (yc - yl);
-    T Dqp = (yr - yc);
-    T s = Dqm * Dqp;
-    if (s <= T(0.)) return T(0.);
-    return (T(2.0) * s / (Dqm + Dqp));
-  } else if (lim == HGPU_LIM_MINM) {
-    T Dqm = T(1.0) * (yc - yl);
-    T Dqp = T(1.0) * (yr - yc);
-    T Dqc = T(0.5) * (yr - yl);
-    T mm = ((Dqm) * (Dqc) <= T(0)) ? T(0.0) : ((fabs(Dqm) < fabs(Dqc)) ? (Dqm) : (Dqc));
-    return ((mm) * (Dqp) <= T(0)) ? T(0.0) : ((fabs(mm) < fabs(Dqp)) ? (mm) : (Dqp));
-  }
-  return T(0.0);
-}
-
-// para4 (interppoint.c:736-869) with PARA2LIM=MC and JONPARAREDUCE=0: face
-// values of the cell at y[0] from y[-2..2]
-template <typename T>
-__device__ __forceinline__ void para4(const T *y, T *lout, T *rout) {
-  T dq[3];
-#pragma unroll
-  for (int mm = -1; mm <= 1; mm++) {
-    T Dqm = T(2.0) * (y[mm] - y[mm - 1]);
-    T Dqp = T(2.0) * (y[mm + 1] - y[mm]);
-    T Dqc = T(0.5) * (y[mm + 1] - y[mm - 1]);
-    T aDqm = fabs(Dqm), aDqp = fabs(Dqp), aDqc = fabs(Dqc);
-    T s = Dqm * Dqp;
-    T sg = (Dqc > T(0.0)) ? T(1.0) : ((Dqc < T(0.0)) ? T(-1.0) : T(0.0));
-    dq[mm + 1] = (s <= T(0.)) ? T(0.) : min_ref(aDqc, min_ref(aDqm, aDqp)) * sg;
-  }
-  T l = T(0.5) * (y[0] + y[-1]) - (dq[1] - dq[0]) / T(8.0);
-  T r = T(0.5) * (y[1] + y[0]) - (dq[2] - dq[1]) / T(8.0);
-  l = max_ref(min_ref(y[0], y[-1]), l);
-  l = min_ref(max_ref(y[0], y[-1]), l);
-  r = max_ref(min_ref(y[0], y[1]), r);
-  r = min_ref(max_ref(y[0], y[1]), r);
-  T qa = (r - y[0]) * (y[0] - l);
-  T qd = (r - l);
-  T qe = T(6.0) * (y[0] - T(0.5) * (l + r));
-  if (qa <= T(0.)) {
-    l = y[0];
-    r = y[0];
-  } else {
-    if (qd * (qd - qe) < T(0.0)) l = T(3.0) * y[0] - T(2.0) * r;
-    if (qd * (qd + qe) < T(0.0)) r = T(3.0) * y[0] - T(2.0) * l;
-  }
-  *lout = l;
-  *rout = r;
-}
-
-// ---------------------------------------------------------------------------
-// WENO5 line reconstruction (slope_lim_linetype_c2e, interpline.c:517-678) as
-// two cell-parallel passes; see weno5.cuh.  Scratch WA holds, per primitive
-// v, 4 planes: the SMONO code (indicator in [0,1], -1 at a cusp) and the
-// three unoptimised weights.
-// ---------------------------------------------------------------------------
-constexpr int W5_PLANES = 4;
-
-// Minimum resident 128-thread blocks per SM asked of the register allocator
-// for the FP64-heavy kernels (launch_bounds' second argument).  With 64K
-// registers per SM, B blocks cap a thread at 65536 / (128 B) registers:
-// 1-2 -> 255 (8 warps/SM), 3 -> 170 (12 warps), 4 -> 128 (16 warps), more
-// warps to hide FP64 latency at the price of spills to local memory.
-// Defaults from a B200 sweep (256x128x128 torus, 1/3/4/5 blocks for flux and
-// update, 1/5/6/8 for weno_b, 1/8/10 for weno_a): flux 4 (-11% WENO5, -21%
-// MC), weno_b 8 (-33%), weno_a 8 (-3%); update is fastest unconstrained.
-#ifndef HG_MINB_FLUX
-#define HG_MINB_FLUX 4
-#endif
-#ifndef HG_MINB_UPDATE
-#define HG_MINB_UPDATE 1
-#endif
-#ifndef HG_MINB_WENO_A
-#define HG_MINB_WENO_A 8
-#endif
-#ifndef HG_MINB_WENO_B
-#define HG_MINB_WENO_B 8
-#endif
-// the same for the FP32 kernels of the mixed-precision path (B200 sweep of
-// 4/6/8 for flux, 8/10/12 for weno_a/b: flux 8 -4%, the rest within 2%)
-#ifndef HG_MINB_FLUX_F32
-#define HG_MINB_FLUX_F32 8
-#endif
-#ifndef HG_MINB_WENO_A_F32
-#define HG_MINB_WENO_A_F32 12
-#endif
-#ifndef HG_MINB_WENO_B_F32
-#define HG_MINB_WENO_B_F32 8
-#endif
-template <typename T> struct MinBlocks;
-template <> struct MinBlocks<double> {
-  static constexpr int flux = HG_MINB_FLUX, weno_a = HG_MINB_WENO_A, weno_b = HG_MINB_WENO_B;
-};
-template <> struct MinBlocks<float> {
-  static constexpr int flux = HG_MINB_FLUX_F32, weno_a = HG_MINB_WENO_A_F32, weno_b = HG_MINB_WENO_B_F32;
-};
-
-template <int DIR>
-__device__ __forceinline__ long long dir_stride(const Dims &d) {
-  return (DIR == 1) ? (long long)d.nt2 * d.nt3 : ((DIR == 2) ? (long long)d.nt3 : 1);
-}
-
-// metric of one location converted to the arithmetic type of a kernel
-template <typename T>
-__device__ __forceinline__ void load_metric_t(const double *__restrict__ G, const Dims &d, long long ij, int slot,
-                                              MetricT<T> &m) {
-  const double *b = G + (long long)slot * GLOC * d.nij + ij;
-#pragma unroll
-  for (int q = 0; q < 16; q++) m.gcov[q] = (T)__ldg(b + (long long)q * d.nij);
-#pragma unroll
-  for (int q = 0; q < 16; q++) m.gcon[q] = (T)__ldg(b + (long long)(16 + q) * d.nij);
-  m.gcovpert_tt = (T)__ldg(b + (long long)32 * d.nij);
-  m.g = (T)__ldg(b + (long long)33 * d.nij);
-}
-
-// pass A over line cells -4..n+3: cusp test, SMONO indicator, unoptimised
-// weights.  T = double: the reference's arithmetic; T = float: mixed path.
-template <int DIR, typename T>
-__global__ void __launch_bounds__(128, MinBlocks<T>::weno_a) weno_a_kernel(Dims d, Box box, const double *__restrict__ pb,
-                                                                     T *__restrict__ WA) {
-  long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= box.size()) return;
-  int i, j, k;
-  box_ijk(box, t, i, j, k);
-  long long z = zix(d, i, j, k);
-  const long long o = dir_stride<DIR>(d);
-  for (int v = 0; v < NPR; v++) {
-    const double *q = pb + (long long)v * d.nz + z;
-    T ya[5] = {(T)__ldg(q - 2 * o), (T)__ldg(q - o), (T)__ldg(q), (T)__ldg(q + o), (T)__ldg(q + 2 * o)};
-    const T *y = ya + 2;
-    bool c = w5::cusp(y);
-    T m0 = c ? T(0.0) : w5::mono(y);
-    T w[3];
-    w5::unopt3(m0, y, w);
-    T *out = WA + (long long)v * W5_PLANES * d.nz + z;
-    out[0] = c ? T(-1.0) : m0;
-    out[d.nz] = w[0];
-    out[2 * d.nz] = w[1];
-    out[3 * d.nz] = w[2];
-  }
-}
-
-// pass B over line cells -1..n: dP/P, ratios, reduction, face values
-template <int DIR, typename T>
-__global__ void __launch_bounds__(128, MinBlocks<T>::weno_b) weno_b_kernel(Dims d, Params P, Box box,
-                                                                     const double *__restrict__ pb,
-                                                                     const double *__restrict__ G,
-                                                                     const T *__restrict__ WA, T *__restrict__ pL,
-                                                                     T *__restrict__ pR) {
-  long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= box.size()) return;
-  int i, j, k;
-  box_ijk(box, t, i, j, k);
-  long long z = zix(d, i, j, k);
-  const long long o = dir_stride<DIR>(d);
-  // compute_df_line_new (interpline.c:2148-2222): jump indicator from the
-  // primitives of the cells -1, 0, +1 along the line and their CENT metrics
-  T dP;
-  {
-    T pm[NPR], p0[NPR], pp[NPR];
-#pragma unroll
-    for (int v = 0; v < NPR; v++) {
-      pm[v] = (T)pb[(long long)v * d.nz + z - o];
-      p0[v] = (T)pb[(long long)v * d.nz + z];
-      pp[v] = (T)pb[(long long)v * d.nz + z + o];
-    }
-    StateT<T> ql, q, qr;
-    T a, b, c;
-    MetricT<T> m;
-    load_metric_t(G, d, gix(d, i - (DIR == 1), j - (DIR == 2)), G_CENT, m);
-    get_state(pm, m, ql);
-    a = compute_1plusud0(m, ql);
-    load_metric_t(G, d, gix(d, i, j), G_CENT, m);
-    get_state(p0, m, q);
-    b = compute_1plusud0(m, q);
-    load_metric_t(G, d, gix(d, i + (DIR == 1), j + (DIR == 2)), G_CENT, m);
-    get_state(pp, m, qr);
-    c = compute_1plusud0(m, qr);
-    T gam = (T)(P.cell_inst ? P.inst[P.cell_inst[z]].gam : P.gam);
-    T parl = a * (ql.ucon[0]);
-    T par = b * (q.ucon[0]);
-    T parr = c * (qr.ucon[0]);
-    T uparl = gam * pm[UU] * (ql.ucon[0] * ql.ucov[0]) + (gam - T(1.0)) * pm[UU];
-    T upar = gam * p0[UU] * (q.ucon[0] * q.ucov[0]) + (gam - T(1.0)) * p0[UU];
-    T uparr = gam * pp[UU] * (qr.ucon[0] * qr.ucov[0]) + (gam - T(1.0)) * pp[UU];
-    dP = (fabs(p0[RHO] * (parr - parl)) + fabs(uparr - uparl)) / (fabs(p0[RHO] * par) + fabs(upar) + w5::K<T>::tiny);
-  }
-  // apply_additional_reduction_to_weights (reconstructeno.c:650-700)
-  T ss = w5::wmin((fabs(dP) - T(0.5 * w5::kDpFrac)) / T(0.5 * w5::kDpFrac), T(1.));
-  for (int v = 0; v < NPR; v++) {
-    const T *wa = WA + (long long)v * W5_PLANES * d.nz + z;
-    // codes of cells -1, 0, +1 and weights of cells -3..+3 (w0 and w2 of the neighbours)
-    T cm = __ldg(wa - o), c0 = __ldg(wa), cp = __ldg(wa + o);
-    const T *w0p = wa + d.nz, *w1p = wa + 2 * d.nz, *w2p = wa + 3 * d.nz;
-    T wc[3] = {__ldg(w0p), __ldg(w1p), __ldg(w2p)};
-    T wm[3] = {__ldg(w0p - o), T(0.0), __ldg(w2p - o)};
-    T wp[3] = {__ldg(w0p + o), T(0.0), __ldg(w2p + o)};
-    T w_m3_0 = __ldg(w0p - 3 * o), w_m2_0 = __ldg(w0p - 2 * o);
-    T w_p2_2 = __ldg(w2p + 2 * o), w_p3_2 = __ldg(w2p + 3 * o);
-    T fd_m = w5::ratio_lof(wm, w_m3_0, __ldg(w2p + o), cm == T(-1.0) ? T(1.0) : T(0.0));
-    T fd_p = w5::ratio_lof(wp, __ldg(w0p - o), w_p3_2, cp == T(-1.0) ? T(1.0) : T(0.0));
-    T lof = w5::ratio_lof(wc, w_m2_0, w_p2_2, c0 == T(-1.0) ? T(1.0) : T(0.0));
-    lof = w5::wmax(lof, ss * fd_p);
-    lof = w5::wmax(lof, ss * fd_m);
-    const double *q = pb + (long long)v * d.nz + z;
-    T ya[5] = {(T)__ldg(q - 2 * o), (T)__ldg(q - o), (T)__ldg(q), (T)__ldg(q + o), (T)__ldg(q + 2 * o)};
-    bool cu = (c0 == T(-1.0));
-    T m0 = cu ? T(0.0) : c0;
-    T yl, yr;
-    w5::faces(ya + 2, m0, cu, wc, lof, &yl, &yr);
-    pL[(long long)v * d.nz + z] = yl;
-    pR[(long long)v * d.nz + z] = yr;
-  }
-}
-
-// ---------------------------------------------------------------------------
-// face flux kernel (one per direction); RECON 0: MC-type slopes in the
-// kernel, RECON 1: Riemann states from the WENO5 face values pL/pR
-// ---------------------------------------------------------------------------
-template <int DIR, int RECON, typename T>
-__global__ void __launch_bounds__(128, MinBlocks<T>::flux) flux_kernel(Dims d, Params P, Box box,
-                                                                 const double *__restrict__ pb,
-                                                                 const T *__restrict__ pL, const T *__restrict__ pR,
-                                                                 const double *__restrict__ G, double *__restrict__ F,
-                                                                 Scalars *sc) {
-  long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  bool active = t < box.size();
-  double dtij = 0.0;
-  if (active) {
-    int i, j, k;
-    box_ijk(box, t, i, j, k);
-    long long z = zix(d, i, j, k);
-    const long long o = dir_stride<DIR>(d);
-    T p_l[NPR], p_r[NPR];
-    if (RECON == 1) {
-      // getp2interplr (flux.c:788-808), line-type branch
-#pragma unroll
-      for (int v = 0; v < NPR; v++) {
-        p_l[v] = __ldg(pR + (long long)v * d.nz + z - o);
-        p_r[v] = __ldg(pL + (long long)v * d.nz + z);
-      }
-    } else if (RECON == 2) {
-      // PARA: pright of the cell on the left, pleft of the cell on the right
-#pragma unroll
-      for (int v = 0; v < NPR; v++) {
-        const double *q = pb + (long long)v * d.nz + z;
-        T y[6];
-#pragma unroll
-        for (int l = 0; l < 6; l++) y[l] = (T)__ldg(q + (l - 3) * o);
-        T dummy;
-        para4(y + 2, &dummy, &p_l[v]);
-        para4(y + 3, &p_r[v], &dummy);
-      }
-    } else {
-#pragma unroll
-      for (int v = 0; v < NPR; v++) {
-        const double *q = pb + (long long)v * d.nz + z;
-        T ym2 = (T)__ldg(q - 2 * o), ym1 = (T)__ldg(q - o), y0 = (T)__ldg(q), yp1 = (T)__ldg(q + o);
-        T dqm = slope3(P.lim, ym2, ym1, y0);
-        T dq0 = slope3(P.lim, ym1, y0, yp1);
-        // getp2interplr (flux.c:788-808)
-        p_l[v] = ym1 + T(0.5) * dqm;
-        p_r[v] = y0 - T(0.5) * dq0;
-      }
-    }
-    // BDIRCONT (flux.c:629-633)
-    p_l[B1 + DIR - 1] = p_r[B1 + DIR - 1] = T(0.5) * (p_l[B1 + DIR - 1] + p_r[B1 + DIR - 1]);
-    MetricT<T> m;
-    load_metric_t(G, d, gix(d, i, j), DIR - 1, m);
-    StateT<T> ql, qr;
-    EMT<T> el, er;
-    T Fl[NPR], Fr[NPR], Ul[NPR], Ur[NPR];
-    int b = P.cell_inst ? P.cell_inst[z] : -1;
-    const T gam = (T)(b >= 0 ? P.inst[b].gam : P.gam);
-    int err = 0;
-    if (get_state(p_l, m, ql)) err |= ERR_UTCALC_DISCR;
-    em_prepare(p_l, m, ql, el);
-    primtoflux(p_l, ql, el, DIR, m, gam, Fl);
-    primtoflux(p_l, ql, el, 0, m, gam, Ul);
-    if (get_state(p_r, m, qr)) err |= ERR_UTCALC_DISCR;
-    em_prepare(p_r, m, qr, er);
-    primtoflux(p_r, qr, er, DIR, m, gam, Fr);
-    primtoflux(p_r, qr, er, 0, m, gam, Ur);
-    T cmaxl = T(0.), cminl = T(0.), cmaxr = T(0.), cminr = T(0.);
-    err |= vchar(p_l, ql, DIR, m, gam, &cmaxl, &cminl);
-    err |= vchar(p_r, qr, DIR, m, gam, &cmaxr, &cminr);
-    // cminmax_calc (wavespeeds.c:325-385)
-    T lmin = min_ref(cminl, cminr);
-    T lmax = max_ref(cmaxl, cmaxr);
-    lmin = fabs(max_ref(T(0.), -lmin));
-    lmax = fabs(max_ref(T(0.), lmax));
-    T cmin = lmin, cmax = lmax, ctop = max_ref(lmax, lmin);
-    double Fo[NPR];
-    if (P.flux == HGPU_FLUX_HLL && (cmax + cmin != T(0.0))) {
-#pragma unroll
-      for (int v = 0; v < NPR; v++)
-        Fo[v] = (double)(((cmax * Fl[v] + cmin * Fr[v]) - (cmax * cmin) * (Ur[v] - Ul[v])) / (cmax + cmin));
-    } else {
-#pragma unroll
-      for (int v = 0; v < NPR; v++) Fo[v] = (double)(T(0.5) * ((Fl[v] + Fr[v]) - ctop * (Ur[v] - Ul[v])));
-    }
-    // flux_ct gdet strip (fluxct.c:74-96), in FP64 in both precision modes
-    const double gface = __ldg(G + (long long)((DIR - 1) * GLOC + 33) * d.nij + gix(d, i, j));
-    Fo[B1] /= gface;
-    Fo[B2] /= gface;
-    Fo[B3] /= gface;
-    store_prim(F, d, z, Fo);
-    double dxd = (DIR == 1) ? P.dx1 : ((DIR == 2) ? P.dx2 : P.dx3);
-    if (b >= 0) {
-      // batch: faces 0..n of a running instance feed its own dt
-      const Inst &I = P.inst[b];
-      int loc = i - I.i0;
-      active = false;
-      if (loc >= 0 && loc <= I.n && !I.done) {
-        dtij = P.cour * I.dx / (double)ctop;
-        if (dtij == dtij) atomicMin(&P.inst[b].ndtbits, (unsigned long long)__double_as_longlong(dtij));
-        if (err) atomicOr(&sc->err, err);
-      }
-    } else {
-      dtij = P.cour * dxd / (double)ctop;
-      if (err) atomicOr(&sc->err, err);
-    }
-  }
-  warp_min_atomic(&sc->ndtbits[DIR], dtij, active);
-}
 
 // ---------------------------------------------------------------------------
 // corner EMFs (fluxct.c:104-218) on the corners the updated faces read
@@ -559,38 +136,45 @@ __global__ void __launch_bounds__(256) emf_kernel(Dims d, Box box, const double 
 }
 
 // ---------------------------------------------------------------------------
-// zone update: advance_standard's CZLOOP body (advance.c:143-213)
+// zone update: advance_standard's CZLOOP body (advance.c:143-213), split in
+// two kernels with the same arithmetic: the conserved update (U(pi), the
+// geometric source, the flux divergence, dUtoU) and the inversion with the
+// final-substep fixup1zone.  Each holds half the live state of the fused
+// loop body, so more warps fit per SM.
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(128, HG_MINB_UPDATE) update_kernel(Dims d, Params P, Box box, const double *pi, const double *pb,
-                                                     double *pf, double *__restrict__ uf, double *__restrict__ ucum,
-                                                     const double *__restrict__ F1, const double *__restrict__ F2,
-                                                     const double *__restrict__ F3, const double *__restrict__ E,
-                                                     const double *__restrict__ G, int *__restrict__ pflag,
-                                                     Scalars *sc, double CUf0, double CUf1, double CUf2,
-                                                     double Cunew0, double Cunew1, double Cunew2, int timeorder,
-                                                     int finalstep) {
+// per-zone step parameters: dt, gamma, dx1 of the domain or of the zone's
+// batch instance; false if the zone does not advance
+__device__ __forceinline__ bool zone_step(const Params &P, const Scalars *sc, long long z, int i, double &dt,
+                                          double &gam, double &dx1) {
+  dt = sc->dt;
+  gam = P.gam;
+  dx1 = P.dx1;
+  if (P.cell_inst) {
+    const Inst &I = P.inst[P.cell_inst[z]];
+    int loc = i - I.i0;
+    dt = I.dt;
+    gam = I.gam;
+    dx1 = I.dx;
+    return loc >= 0 && loc < I.n && !I.done;
+  }
+  return !sc->done;
+}
+
+__global__ void __launch_bounds__(128, HG_MINB_UPDATE) conserve_kernel(
+    Dims d, Params P, Box box, const double *pi, const double *pb, double *__restrict__ uf,
+    double *__restrict__ ucum, const double *__restrict__ F1, const double *__restrict__ F2,
+    const double *__restrict__ F3, const double *__restrict__ E, const double *__restrict__ G, Scalars *sc,
+    double CUf0, double CUf1, double CUf2, double Cunew0, double Cunew1, double Cunew2, int timeorder) {
   long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  unsigned long long my_iters = 0;
-  int my_fail = 0;
-  if (t < box.size()) {
-    int i, j, k;
-    box_ijk(box, t, i, j, k);
-    const long long z = zix(d, i, j, k);
-    const long long nz = d.nz;
-    const long long o1 = (long long)d.nt2 * d.nt3, o2 = d.nt3, o3 = 1;
-    const long long ij = gix(d, i, j);
-    double dt = sc->dt, gam = P.gam, dx1 = P.dx1;
-    bool run = true;
-    if (P.cell_inst) {
-      // batch: only the active cells of running instances advance
-      const Inst &I = P.inst[P.cell_inst[z]];
-      int loc = i - I.i0;
-      run = (loc >= 0 && loc < I.n && !I.done);
-      dt = I.dt;
-      gam = I.gam;
-      dx1 = I.dx;
-    }
-    if (run) {
+  if (t >= box.size()) return;
+  int i, j, k;
+  box_ijk(box, t, i, j, k);
+  const long long z = zix(d, i, j, k);
+  const long long nz = d.nz;
+  const long long o1 = (long long)d.nt2 * d.nt3, o2 = d.nt3, o3 = 1;
+  const long long ij = gix(d, i, j);
+  double dt, gam, dx1;
+  if (!zone_step(P, sc, z, i, dt, gam, dx1)) return;
     Metric m;
     load_metric(G, d, ij, G_CENT, m);
     int err = 0;
@@ -690,12 +274,40 @@ __global__ void __launch_bounds__(128, HG_MINB_UPDATE) update_kernel(Dims d, Par
       uf[pl * nz + z] = Uf[pl];
       ucum[pl * nz + z] = Ucum[pl];
     }
+    if (err) atomicOr(&sc->err, err);
+}
+
+__global__ void __launch_bounds__(128, HG_MINB_INVERT) invert_kernel(Dims d, Params P, Box box, const double *pb,
+                                                                     double *pf, const double *__restrict__ uf,
+                                                                     const double *__restrict__ ucum,
+                                                                     const double *__restrict__ G,
+                                                                     int *__restrict__ pflag, Scalars *sc,
+                                                                     int finalstep) {
+  long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  unsigned long long my_iters = 0;
+  int my_fail = 0;
+  if (t < box.size()) {
+    int i, j, k;
+    box_ijk(box, t, i, j, k);
+    const long long z = zix(d, i, j, k);
+    const long long nz = d.nz;
+    const long long ij = gix(d, i, j);
+    double dt, gam, dx1;
+    if (zone_step(P, sc, z, i, dt, gam, dx1)) {
+    Metric m;
+    load_metric(G, d, ij, G_CENT, m);
+    int err = 0;
+    double pbz[NPR], Uin[NPR];
+    load_prim(pb, d, z, pbz);
+    const double *src = finalstep ? ucum : uf;
+#pragma unroll
+    for (int pl = 0; pl < NPR; pl++) Uin[pl] = src[pl * nz + z];
     // guess = pb, invert (advance.c:188-205)
     double pr[NPR];
 #pragma unroll
     for (int v = 0; v < NPR; v++) pr[v] = pbz[v];
     int it = 0;
-    int flag = utoprimgen(finalstep ? Ucum : Uf, m, gam, P.gammafail, pr, &it);
+    int flag = utoprimgen(Uin, m, gam, P.gammafail, pr, &it);
     my_iters = (unsigned long long)it;
     my_fail = (flag != 0);
     if (finalstep) {
@@ -704,9 +316,11 @@ __global__ void __launch_bounds__(128, HG_MINB_UPDATE) update_kernel(Dims d, Par
       double fr = __ldg(fl), fu = __ldg(fl + d.nij);
       if (fr < P.rhominlimit) fr = P.rhominlimit;
       if (fu < P.uuminlimit) fu = P.uuminlimit;
+      bool floored = (fr > pr[RHO]) || (fu > pr[UU]);
       if (fr > pr[RHO]) pr[RHO] = fr;
       if (fu > pr[UU]) pr[UU] = fu;
       limit_gamma(P.gammamax, pr, m, &err);
+      if (floored) atomicAdd(&sc->nfloor, 1);
     }
     store_prim(pf, d, z, pr);
     pflag[z] = flag;
@@ -846,9 +460,10 @@ __global__ void bound_pole_kernel(Dims d, Params P, double *p) {
 }
 
 // bound_pflag_user (boundsint.c:6-266) as the same composition
-__global__ void bound_pflag_kernel(Dims d, Params P, int *pflag) {
+__global__ void bound_pflag_kernel(Dims d, Params P, int *pflag, const Scalars *sc) {
   long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= d.nz) return;
+  // a finished domain is frozen: its ghost flags keep the values of its last step
+  if (t >= d.nz || sc->done) return;
   int k = (int)(t % d.nt3) - d.g3;
   long long r = t / d.nt3;
   int j = (int)(r % d.nt2) - d.g2;
@@ -869,6 +484,8 @@ __global__ void bound_batch_kernel(Dims d, Params P, double *pv, int *pflag) {
   if (t >= d.nz) return;
   int i = (int)t - d.g1;  // the batch line is 1D
   const Inst &I = P.inst[P.cell_inst[t]];
+  // a finished instance is frozen: its ghosts keep the values of its last step
+  if (I.done) return;
   int loc = i - I.i0;
   int src;
   if (loc < 0) src = I.i0;
@@ -909,7 +526,7 @@ __global__ void checksol_gamma_kernel(Dims d, Params P, Box box, const double *_
     int loc = i - I.i0;
     activez = (loc >= 0 && loc < I.n && !I.done);
   }
-  if (activez && gamma >= 2.0) {
+  if (activez && gamma >= 2.0 && !sc->done) {
     int slot = atomicAdd(&sc->ncand, 1);
     if (slot < cap) cand[slot] = z;
     else atomicOr(&sc->overflow, 1);
@@ -1009,7 +626,7 @@ __global__ void fixup_collect_kernel(Dims d, Params P, Box box, const int *__res
     int loc = i - I.i0;
     if (!(loc >= 0 && loc < I.n && !I.done)) return;
   }
-  if (pflag[z] != 0) {
+  if (pflag[z] != 0 && !sc->done) {
     int slot = atomicAdd(&sc->nfixlist, 1);
     if (slot < cap) list[slot] = z;
     else atomicOr(&sc->overflow, 2);
@@ -1175,13 +792,16 @@ __global__ void finalize_kernel(Params P, Scalars *sc, int advance_time) {
   double n2 = __longlong_as_double((long long)sc->ndtbits[2]);
   double n3 = __longlong_as_double((long long)sc->ndtbits[3]);
   double ndt = P.defcon * 1. / (1. / n1 + 1. / n2 + 1. / n3);
-  if (advance_time) {
+  if (advance_time && !sc->done) {
     double dt = sc->dt;
     sc->t += dt;
     if (ndt > P.safe * dt) ndt = P.safe * dt;
     dt = ndt;
     if (sc->t + dt > P.tf) dt = P.tf - sc->t;
     sc->dt = dt;
+    // the reference's main loop runs while t < tf (main.c:33)
+    sc->nsteps++;
+    if (!(sc->t < P.tf)) sc->done = 1;
   }
   // keep the last ndt where the host can read it
   sc->ndtbits[0] = (unsigned long long)__double_as_longlong(ndt);
@@ -1285,12 +905,12 @@ inline unsigned grid_for(long long n, int block) { return (unsigned)((n + block 
 // ---------------------------------------------------------------------------
 enum KernelId {
   K_RESET, K_FLUX1, K_FLUX2, K_FLUX3, K_EMF, K_UPDATE, K_BOUND_GHOST, K_BOUND_POLE, K_BOUND_PFLAG, K_CHECK_GAMMA,
-  K_CHECK_RESOLVE, K_FIX_COLLECT, K_FIX_COMPUTE, K_FIX_SCATTER, K_FINALIZE, K_WENO_A, K_WENO_B, K_OTHER, K_NKERNELS
+  K_CHECK_RESOLVE, K_FIX_COLLECT, K_FIX_COMPUTE, K_FIX_SCATTER, K_FINALIZE, K_WENO_A, K_WENO_B, K_INVERT, K_OTHER, K_NKERNELS
 };
 static const char *kKernelNames[K_NKERNELS] = {
     "reset_stage",  "flux_x1",         "flux_x2",       "flux_x3",       "emf",           "update",
     "bound_ghost",  "bound_pole",      "bound_pflag",   "checksol_gamma", "checksol_resolve", "fixup_collect",
-    "fixup_compute", "fixup_scatter",  "finalize",      "weno_a",        "weno_b",        "other"};
+    "fixup_compute", "fixup_scatter",  "finalize",      "weno_a",        "weno_b",        "invert",        "other"};
 
 struct ProfEvent {
   int kid;
@@ -1321,6 +941,7 @@ struct hgpu_ctx {
   Scalars *sc = nullptr;
   double *staging = nullptr;  // AoS staging for uploads/downloads
   double *pL = nullptr, *pR = nullptr, *WA = nullptr;  // WENO5 face values and weights scratch
+  double *progress = nullptr;                          // 4 doubles for hg_progress_async
   Box wa_box[4], wb_box[4];
   int *istaging = nullptr;
   // batch of 1D instances (hgpu_create_batch)
@@ -1424,7 +1045,7 @@ void hgpu_destroy(hgpu_ctx *x) {
   for (cudaEvent_t e : x->freelist) cudaEventDestroy(e);
   void *ptrs[] = {x->p, x->pk, x->uf, x->ucum, x->F[1], x->F[2], x->F[3], x->E, x->G, x->pflag, x->gammacheck,
                   x->cand, x->fixlist, x->cand_orig, x->cand_dec, x->candmap, x->fixvals, x->sc, x->staging, x->istaging,
-                  x->pL, x->pR, x->WA, x->cell_inst, x->inst};
+                  x->pL, x->pR, x->WA, x->cell_inst, x->inst, x->progress};
   for (void *q : ptrs)
     if (q) cudaFree(q);
   cudaStreamDestroy(x->stream);
@@ -1804,15 +1425,16 @@ static void launch_stage(hgpu_ctx *x, int timeorder) {
   (void)s;
   launch_reset(x);
   launch_fluxes(x, pb);
-  LAUNCH(x, K_UPDATE, update_kernel, grid_for(x->active_box.size(), 128), 128, d, x->P, x->active_box, pi, pb, pf, x->uf,
-         x->ucum, x->F[1], x->F[2], x->F[3], x->E, x->G, x->pflag, x->sc, CUf0, CUf1, CUf2, Cn0, Cn1, Cn2, timeorder,
-         finalstep);
+  LAUNCH(x, K_UPDATE, conserve_kernel, grid_for(x->active_box.size(), 128), 128, d, x->P, x->active_box, pi, pb, x->uf,
+         x->ucum, x->F[1], x->F[2], x->F[3], x->E, x->G, x->sc, CUf0, CUf1, CUf2, Cn0, Cn1, Cn2, timeorder);
+  LAUNCH(x, K_INVERT, invert_kernel, grid_for(x->active_box.size(), 128), 128, d, x->P, x->active_box, pb, pf, x->uf,
+         x->ucum, x->G, x->pflag, x->sc, finalstep);
   launch_bound(x, pf);
   // post_fixup (fixup.c:37-96)
   if (x->P.cell_inst)
     LAUNCH(x, K_BOUND_PFLAG, bound_batch_kernel, grid_for(d.nz, 256), 256, d, x->P, (double *)nullptr, x->pflag);
   else
-    LAUNCH(x, K_BOUND_PFLAG, bound_pflag_kernel, grid_for(d.nz, 256), 256, d, x->P, x->pflag);
+    LAUNCH(x, K_BOUND_PFLAG, bound_pflag_kernel, grid_for(d.nz, 256), 256, d, x->P, x->pflag, x->sc);
   LAUNCH(x, K_CHECK_GAMMA, checksol_gamma_kernel, grid_for(x->dq_box.size(), 128), 128, d, x->P, x->dq_box, pf, x->G,
          x->gammacheck, x->cand, x->cap, x->sc);
   LAUNCH(x, K_CHECK_RESOLVE, checksol_resolve_kernel, 1, 1024, d, pf, x->gammacheck, x->pflag, x->cand, x->candmap,
@@ -1857,6 +1479,7 @@ static void clear_counters(hgpu_ctx *x) {
   cudaMemsetAsync(&x->sc->err, 0, sizeof(int), x->stream);
   cudaMemsetAsync(&x->sc->nfixed, 0, sizeof(int), x->stream);
   cudaMemsetAsync(&x->sc->overflow, 0, sizeof(int), x->stream);
+  cudaMemsetAsync(&x->sc->nfloor, 0, sizeof(int), x->stream);
 }
 
 int hgpu_step_ch(hgpu_ctx *x, int nsteps, hgpu_stats *stats) {
@@ -2036,6 +1659,119 @@ int hgpu_utoprim_batch(const double *U, const double *gcov, const double *gcon, 
   cudaFree(dpf);
   cudaFree(dit);
   return rc;
+}
+
+// ---------------------------------------------------------------------------
+// Diagnostics (dump_ener.c): integrals of the conserved quantities and the
+// flux-CT div B of the reference's divbmaxavg (dump_ener.c:482-520), over
+// the active zones, with a deterministic two-pass reduction.
+// ---------------------------------------------------------------------------
+constexpr int DIAG_VALS = 11;  // 8 integrals, divb sum, divb max, failed zones
+constexpr int DIAG_BLOCK = 256;
+
+// DIVBFLUXCT (global.h:1586-1645) at the corner (i,j,k): B*gdet(CENT)
+// averaged onto the corner and differenced, normalised; dims of size 1 use
+// the same zone on both sides (im1mac(i) = i)
+__device__ double divb_fluxct(const Dims &d, const Params &P, const double *__restrict__ p,
+                              const double *__restrict__ G, int i, int j, int k) {
+  const int s1 = d.s1, s2 = d.s2, s3 = d.s3;
+  auto Fg = [&](int ii, int jj, int kk, int pl) {
+    return p[(long long)pl * d.nz + zix(d, ii, jj, kk)] * __ldg(G + (long long)(G_CENT * GLOC + 33) * d.nij + gix(d, ii, jj));
+  };
+  auto avg1 = [&](int ii, int jj, int kk, int pl) { return 0.5 * (Fg(ii, jj, kk, pl) + Fg(ii - s1, jj, kk, pl)); };
+  auto avg2 = [&](int ii, int jj, int kk, int pl) { return 0.5 * (Fg(ii, jj, kk, pl) + Fg(ii, jj - s2, kk, pl)); };
+  auto for1 = [&](int ii, int jj, int kk) { return 0.5 * (avg2(ii, jj, kk, B1) + avg2(ii, jj, kk - s3, B1)); };
+  auto for2 = [&](int ii, int jj, int kk) { return 0.5 * (avg1(ii, jj, kk, B2) + avg1(ii, jj, kk - s3, B2)); };
+  auto for3 = [&](int ii, int jj, int kk) { return 0.5 * (avg2(ii, jj, kk, B3) + avg2(ii - s1, jj, kk, B3)); };
+  double dfx = for1(i, j, k) - for1(i - s1, j, k);
+  double dfy = for2(i, j, k) - for2(i, j - s2, k);
+  double dfz = for3(i, j, k) - for3(i, j, k - s3);
+  double nx = for1(i, j, k) + for1(i - s1, j, k);
+  double ny = for2(i, j, k) + for2(i, j - s2, k);
+  double nz = for3(i, j, k) + for3(i, j, k - s3);
+  // corner gdet: CORNT is not kept on the device; the metric does not depend
+  // on x3, so gdet at the true corner equals CORN3's
+  double gc = __ldg(G + (long long)(G_CORN + 2) * d.nij + gix(d, i, j));
+  double mx = max_ref(max_ref(P.dx1, P.dx2), P.dx3);
+  double norm = mx / ((1.0 / 3.0) * gc * fabs(nx + ny + nz) + 1.e-50);
+  return fabs((dfx / P.dx1 + dfy / P.dx2 + dfz / P.dx3) * norm);
+}
+
+__global__ void __launch_bounds__(DIAG_BLOCK) diag_kernel(Dims d, Params P, Box box, const double *__restrict__ p,
+                                                          const int *__restrict__ pflag, const double *__restrict__ G,
+                                                          double *__restrict__ part) {
+  __shared__ double sh[DIAG_VALS][DIAG_BLOCK];
+  long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  double v[DIAG_VALS];
+#pragma unroll
+  for (int q = 0; q < DIAG_VALS; q++) v[q] = 0.0;
+  if (t < box.size()) {
+    int i, j, k;
+    box_ijk(box, t, i, j, k);
+    long long z = zix(d, i, j, k);
+    Metric m;
+    load_metric(G, d, gix(d, i, j), G_CENT, m);
+    double pr[NPR], U[NPR];
+    load_prim(p, d, z, pr);
+    State q;
+    EM e;
+    get_state(pr, m, q);
+    em_prepare(pr, m, q, e);
+    primtoflux(pr, q, e, 0, m, P.gam, U);
+    double dV = P.dx1 * P.dx2 * P.dx3;
+#pragma unroll
+    for (int pl = 0; pl < NPR; pl++) v[pl] = U[pl] * dV;
+    double db = divb_fluxct(d, P, p, G, i, j, k);
+    v[8] = db;
+    v[9] = db;
+    v[10] = (pflag[z] > 0) ? 1.0 : 0.0;
+  }
+#pragma unroll
+  for (int q = 0; q < DIAG_VALS; q++) sh[q][threadIdx.x] = v[q];
+  __syncthreads();
+  for (int w = DIAG_BLOCK / 2; w > 0; w >>= 1) {
+    if (threadIdx.x < w) {
+#pragma unroll
+      for (int q = 0; q < DIAG_VALS; q++) {
+        double a = sh[q][threadIdx.x], b = sh[q][threadIdx.x + w];
+        sh[q][threadIdx.x] = (q == 9) ? max_ref(a, b) : a + b;
+      }
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x < DIAG_VALS) part[(long long)blockIdx.x * DIAG_VALS + threadIdx.x] = sh[threadIdx.x][0];
+}
+
+__global__ void __launch_bounds__(DIAG_BLOCK) diag_final_kernel(const double *__restrict__ part, int nblocks,
+                                                                double *__restrict__ out) {
+  __shared__ double sh[DIAG_BLOCK];
+  for (int q = 0; q < DIAG_VALS; q++) {
+    double a = 0.0;
+    for (int b = threadIdx.x; b < nblocks; b += DIAG_BLOCK) {
+      double x = part[(long long)b * DIAG_VALS + q];
+      a = (q == 9) ? max_ref(a, x) : a + x;
+    }
+    sh[threadIdx.x] = a;
+    __syncthreads();
+    for (int w = DIAG_BLOCK / 2; w > 0; w >>= 1) {
+      if (threadIdx.x < w) sh[threadIdx.x] = (q == 9) ? max_ref(sh[threadIdx.x], sh[threadIdx.x + w])
+                                                        : sh[threadIdx.x] + sh[threadIdx.x + w];
+      __syncthreads();
+    }
+    if (threadIdx.x == 0) out[q] = sh[0];
+    __syncthreads();
+  }
+}
+
+// progress of a context for a host that polls without blocking: t, dt,
+// done, steps
+__global__ void progress_kernel(const Scalars *sc, double *q) {
+  if (threadIdx.x == 0 && blockIdx.x == 0) {
+    q[0] = sc->t;
+    q[1] = sc->dt;
+    q[2] = sc->done;
+    q[3] = sc->nsteps;
+  }
 }
 
 __global__ void set_dt_kernel(Scalars *sc) {
@@ -2287,4 +2023,81 @@ extern "C" int hgpu_utoprim_batch_noalloc(const double *U, const double *gcov, c
   if (iters) *iters = (long long)it;
   return HGPU_OK;
 
+}
+
+// ---------------------------------------------------------------------------
+// Interfaces used by the serving loop (serve.cu)
+// ---------------------------------------------------------------------------
+cudaStream_t hg_stream(hgpu_ctx *x) { return x->stream; }
+
+// Enqueue on the context's stream a copy of (t, dt, done, steps) into host
+// memory dst[4] (pinned) and record ev after it; the host tests ev with
+// cudaEventQuery and reads dst once it has completed.
+int hg_progress_async(hgpu_ctx *x, double *dst, cudaEvent_t ev) {
+  if (!x->progress) CUDA_TRY(cudaMalloc(&x->progress, 4 * sizeof(double)));
+  progress_kernel<<<1, 32, 0, x->stream>>>(x->sc, x->progress);
+  CUDA_TRY(cudaMemcpyAsync(dst, x->progress, 4 * sizeof(double), cudaMemcpyDeviceToHost, x->stream));
+  CUDA_TRY(cudaEventRecord(ev, x->stream));
+  return HGPU_OK;
+}
+
+extern "C" size_t hgpu_context_bytes(const hgpu_config *c) {
+  if (!c || validate(c)) return 0;
+  auto tot = [&](int n) { return (size_t)(n > 1 ? n + 2 * c->ng : 1); };
+  size_t nt1 = tot(c->n1), nt2 = tot(c->n2), nt3 = tot(c->n3);
+  size_t nz = nt1 * nt2 * nt3;
+  size_t nij = (nt1 + (c->n1 > 1)) * (nt2 + (c->n2 > 1));
+  size_t zones = (size_t)c->n1 * c->n2 * c->n3;
+  size_t cap = zones < (1u << 22) ? zones : (1u << 22);
+  size_t plane = sizeof(double) * NPR * nz;
+  size_t b = 7 * plane                       // p, pk, uf, ucum, F1..F3
+             + sizeof(double) * 3 * nz        // corner EMFs
+             + sizeof(double) * G_NCOMP * nij // geometry
+             + sizeof(int) * 2 * nz           // pflag, candidate map
+             + sizeof(double) * nz            // gamma check
+             + cap * (2 * sizeof(long long) + 2 * sizeof(int) + 5 * sizeof(double))
+             + plane;                         // staging for uploads and downloads
+  if (c->lim == HGPU_LIM_WENO5) b += 2 * plane + W5_PLANES * plane;
+  return b;
+}
+
+extern "C" int hgpu_diagnostics(hgpu_ctx *x, hgpu_diag *out) {
+  if (!x || !out) return HGPU_E_INVALID;
+  const Box &box = x->active_box;
+  int nb = (int)grid_for(box.size(), DIAG_BLOCK);
+  double *part = nullptr;
+  CUDA_TRY(cudaMallocAsync(&part, sizeof(double) * ((size_t)nb * DIAG_VALS + DIAG_VALS), x->stream));
+  diag_kernel<<<nb, DIAG_BLOCK, 0, x->stream>>>(x->d, x->P, box, x->p, x->pflag, x->G, part);
+  diag_final_kernel<<<1, DIAG_BLOCK, 0, x->stream>>>(part, nb, part + (size_t)nb * DIAG_VALS);
+  double h[DIAG_VALS];
+  Scalars s;
+  cudaError_t e1 = cudaMemcpyAsync(h, part + (size_t)nb * DIAG_VALS, sizeof(h), cudaMemcpyDeviceToHost, x->stream);
+  cudaError_t e2 = cudaMemcpyAsync(&s, x->sc, sizeof(Scalars), cudaMemcpyDeviceToHost, x->stream);
+  cudaFreeAsync(part, x->stream);
+  CUDA_TRY(cudaStreamSynchronize(x->stream));
+  if (e1 != cudaSuccess || e2 != cudaSuccess) return HGPU_E_CUDA;
+  for (int q = 0; q < NPR; q++) out->integral[q] = h[q];
+  long long zones = (long long)x->d.n1 * x->d.n2 * x->d.n3;
+  out->divb_avg = h[8] / (double)zones;
+  out->divb_max = h[9];
+  out->nfail = (int)h[10];
+  out->t = s.t;
+  out->dt = s.dt;
+  out->nsteps = s.nsteps;
+  out->nfloor = s.nfloor;
+  return HGPU_OK;
+}
+
+// unew of the reference (the conserved state U^{n+1} = the last stage's ucum,
+// with gdet) in the reference's AoS layout, for restart dumps
+// (rdump_content, restart.c:244-250, writes p and unew per zone)
+extern "C" int hgpu_download_conserved(hgpu_ctx *x, double *unew) {
+  if (!x || !unew) return HGPU_E_INVALID;
+  long long nz = x->d.nz;
+  int rc = ensure_staging(x);
+  if (rc) return rc;
+  LAUNCH(x, K_OTHER, soa_to_aos_kernel, grid_for(nz * NPR, 256), 256, x->ucum, x->staging, nz);
+  CUDA_TRY(cudaMemcpyAsync(unew, x->staging, sizeof(double) * NPR * nz, cudaMemcpyDeviceToHost, x->stream));
+  CUDA_TRY(cudaStreamSynchronize(x->stream));
+  return HGPU_OK;
 }

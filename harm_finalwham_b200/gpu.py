@@ -39,6 +39,12 @@ class hgpu_config(ctypes.Structure):
                 ("gammamax", ctypes.c_double), ("gammafail", ctypes.c_double)]
 
 
+class hgpu_diag(ctypes.Structure):
+    _fields_ = [("t", ctypes.c_double), ("dt", ctypes.c_double), ("integral", ctypes.c_double * 8),
+                ("divb_max", ctypes.c_double), ("divb_avg", ctypes.c_double), ("nfail", ctypes.c_int),
+                ("nfloor", ctypes.c_int), ("nsteps", ctypes.c_longlong)]
+
+
 class hgpu_stats(ctypes.Structure):
     _fields_ = [("newton_iters", ctypes.c_longlong), ("err", ctypes.c_int), ("nfail", ctypes.c_int),
                 ("nfixed", ctypes.c_int)]
@@ -88,6 +94,19 @@ def load_library(path=None):
     L.hgpu_batch_layout.argtypes = [ctypes.c_void_p, _ip]
     L.hgpu_batch_status.argtypes = [ctypes.c_void_p, _dp, _dp, _ip, _ip]
     L.hgpu_step_graph.argtypes = [ctypes.c_void_p, ctypes.c_int, _P(hgpu_stats)]
+    L.hgpu_diagnostics.argtypes = [ctypes.c_void_p, _P(hgpu_diag)]
+    L.hgpu_download_conserved.argtypes = [ctypes.c_void_p, _dp]
+    L.hgpu_context_bytes.argtypes = [_P(hgpu_config)]
+    L.hgpu_context_bytes.restype = ctypes.c_size_t
+    L.hgpu_server_create.argtypes = [ctypes.c_size_t, ctypes.c_int, ctypes.c_int, _P(ctypes.c_void_p)]
+    L.hgpu_server_destroy.argtypes = [ctypes.c_void_p]
+    L.hgpu_server_destroy.restype = None
+    L.hgpu_server_submit.argtypes = [ctypes.c_void_p, _P(hgpu_config)] + [_dp] * 7 + [ctypes.c_double,
+                                                                                       _P(ctypes.c_longlong)]
+    L.hgpu_server_poll.argtypes = [ctypes.c_void_p, _ip, _ip, _ip]
+    L.hgpu_server_result.argtypes = [ctypes.c_void_p, ctypes.c_longlong, _dp, _ip, _dp, _P(ctypes.c_longlong), _dp,
+                                     _dp]
+    L.hgpu_server_release.argtypes = [ctypes.c_void_p, ctypes.c_longlong]
     L.hgpu_batch_run.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, _ip, _P(ctypes.c_float), _ip,
                                  _P(ctypes.c_float)]
     for name in ("hgpu_init_dt", "hgpu_step_ch_timed", "hgpu_set_profiling", "hgpu_kernel_times", "hgpu_alloc_pinned",
@@ -96,7 +115,8 @@ def load_library(path=None):
     for name in ("hgpu_create", "hgpu_upload_geometry", "hgpu_upload_state", "hgpu_download_state", "hgpu_step_ch",
                  "hgpu_advance_stage", "hgpu_fluxcalc", "hgpu_bound_prim", "hgpu_utoprim_batch",
                  "hgpu_device_prims", "hgpu_sync", "hgpu_create_batch", "hgpu_batch_layout", "hgpu_batch_status",
-                 "hgpu_step_graph", "hgpu_batch_run"):
+                 "hgpu_step_graph", "hgpu_batch_run", "hgpu_diagnostics", "hgpu_download_conserved", "hgpu_server_create", "hgpu_server_submit",
+                 "hgpu_server_poll", "hgpu_server_result", "hgpu_server_release"):
         getattr(L, name).restype = ctypes.c_int
     if path == _build.LIB:
         _lib = L
@@ -214,6 +234,19 @@ class HarmGPU:
         st = hgpu_stats()
         _check(self.L, self.L.hgpu_step_ch(self.h, int(nsteps), ctypes.byref(st) if stats else None))
         return st
+
+    def download_conserved(self):
+        """The conserved state after the last step (the reference's unew)."""
+        u = np.empty(self.nt + (NPR,))
+        _check(self.L, self.L.hgpu_download_conserved(self.h, _ptr(u)))
+        return u
+
+    def diagnostics(self):
+        """hgpu_diagnostics as a dict."""
+        dg = hgpu_diag()
+        _check(self.L, self.L.hgpu_diagnostics(self.h, ctypes.byref(dg)))
+        return {"t": dg.t, "dt": dg.dt, "integral": list(dg.integral), "divb_max": dg.divb_max,
+                "divb_avg": dg.divb_avg, "nfail": dg.nfail, "nfloor": dg.nfloor, "nsteps": dg.nsteps}
 
     def step_graph(self, nsteps=1, stats=True):
         """step_ch as replays of one captured CUDA graph per time step."""
@@ -388,3 +421,87 @@ class HarmBatch(HarmGPU):
         _check(self.L, self.L.hgpu_batch_run(self.h, int(check_every), int(max_steps), ctypes.byref(steps),
                                              ctypes.byref(ms), _ptr(per, ctypes.c_int), _ptr(fin, ctypes.c_float)))
         return steps.value, ms.value, per, fin
+
+
+def make_config(n, ng, dx, lim="MC", flux="HLL", bc=("OUTFLOW", "OUTFLOW", "POLARAXIS", "POLARAXIS", "PERIODIC",
+                "PERIODIC"), precision="fp64", gam=4.0 / 3.0, cour=0.8, safe=1.3, defcon=1.0, tf=2000.0,
+                rhominlimit=1e-20, uuminlimit=1e-20, gammamax=25.0, gammafail=2500.0):
+    c = hgpu_config()
+    c.n1, c.n2, c.n3 = n
+    c.ng = ng
+    c.lim = LIM[lim] if isinstance(lim, str) else int(lim)
+    c.fluxmethod = FLUX[flux] if isinstance(flux, str) else int(flux)
+    for i, b in enumerate(bc):
+        c.bc[i] = BC[b] if isinstance(b, str) else int(b)
+    c.precision = PREC[precision] if isinstance(precision, str) else int(precision)
+    for i in range(3):
+        c.dx[i + 1] = float(dx[i])
+    c.gam, c.cour, c.safe, c.defcon, c.tf = gam, cour, safe, defcon, tf
+    c.rhominlimit, c.uuminlimit, c.gammamax, c.gammafail = rhominlimit, uuminlimit, gammamax, gammafail
+    return c
+
+
+def context_bytes(cfg):
+    return int(load_library().hgpu_context_bytes(ctypes.byref(cfg)))
+
+
+class HarmServer:
+    """The serving loop (hgpu_server_*): submit solves at any time, call
+    poll() repeatedly, collect results of finished solves."""
+
+    def __init__(self, max_device_bytes, max_active=64, steps_per_chunk=8):
+        self.L = load_library()
+        h = ctypes.c_void_p()
+        _check(self.L, self.L.hgpu_server_create(int(max_device_bytes), int(max_active), int(steps_per_chunk),
+                                                 ctypes.byref(h)))
+        self.h = h
+        self.shapes = {}
+
+    def submit(self, dom, tf, precision="fp64"):
+        """dom: an object with the Domain/Problem attributes (n, ng, dx, lim, ...)."""
+        inv_bc = {v: k for k, v in BC.items()}
+        bc = tuple(inv_bc[b] if not isinstance(b, str) else b for b in dom.bc)
+        c = make_config(dom.n, dom.ng, dom.dx, lim=dom.lim, flux=dom.flux, bc=bc, precision=precision, gam=dom.gam,
+                        cour=dom.cour, safe=dom.safe, defcon=dom.defcon, tf=tf, rhominlimit=dom.rhominlimit,
+                        uuminlimit=dom.uuminlimit, gammamax=dom.gammamax, gammafail=dom.gammafail)
+        arrs = [_contig(a, np.float64) for a in (dom.gcov, dom.gcon, dom.gcovpert, dom.gdet, dom.conn, dom.floors,
+                                                 dom.p)]
+        rid = ctypes.c_longlong()
+        _check(self.L, self.L.hgpu_server_submit(self.h, ctypes.byref(c), *[_ptr(a) for a in arrs], float(tf),
+                                                 ctypes.byref(rid)))
+        self.shapes[rid.value] = dom.p.shape
+        return rid.value
+
+    def poll(self):
+        p, a, f = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        _check(self.L, self.L.hgpu_server_poll(self.h, ctypes.byref(p), ctypes.byref(a), ctypes.byref(f)))
+        return p.value, a.value, f.value
+
+    def result(self, rid):
+        """(p, pflag, t, steps, queue_ms, run_ms) of a finished solve, or None while it runs."""
+        shape = self.shapes[rid]
+        p = np.empty(shape)
+        pf = np.empty(shape[:-1], dtype=np.int32)
+        t, q, r = ctypes.c_double(), ctypes.c_double(), ctypes.c_double()
+        steps = ctypes.c_longlong()
+        rc = self.L.hgpu_server_result(self.h, rid, _ptr(p), _ptr(pf, ctypes.c_int), ctypes.byref(t),
+                                       ctypes.byref(steps), ctypes.byref(q), ctypes.byref(r))
+        if rc == 1:  # HGPU_E_INVALID: not finished
+            return None
+        _check(self.L, rc)
+        return p, pf, t.value, steps.value, q.value, r.value
+
+    def release(self, rid):
+        _check(self.L, self.L.hgpu_server_release(self.h, rid))
+        self.shapes.pop(rid, None)
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.L.hgpu_server_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -182,6 +182,57 @@ int hgpu_batch_run(hgpu_ctx *ctx, int check_every, int max_steps, int *steps, fl
    hgpu_step_ch. */
 int hgpu_step_graph(hgpu_ctx *ctx, int nsteps, hgpu_stats *stats);
 
+/* Diagnostics of the current state (the quantities dump_ener.c writes to
+   ener.out, computed on the device): integral[pl] = sum over active zones of
+   the conserved U (primtoU with gdet, UU without rest mass) times
+   dx1 dx2 dx3; divb_max / divb_avg = max and mean over active zones of the
+   flux-CT div B at each zone's lower corner (divbmaxavg, dump_ener.c:482;
+   DIVBFLUXCT, global.h:1586-1645); nfail = zones whose last inversion left
+   a failure code; nfloor = zones raised to a floor by fixup1zone during the
+   last hgpu_step_ch call; t, dt, nsteps since the last upload.  Sums are
+   deterministic (fixed-order two-pass reduction), not in the reference's
+   serial order. */
+typedef struct {
+  double t, dt;
+  double integral[8];
+  double divb_max, divb_avg;
+  int nfail, nfloor;
+  long long nsteps;
+} hgpu_diag;
+int hgpu_diagnostics(hgpu_ctx *ctx, hgpu_diag *out);
+
+/* The conserved state after the last full step (the reference's unew, with
+   gdet; defined on active zones), host layout as the primitives: with the
+   primitives it is what the reference's restart dump holds
+   (rdump_content, restart.c:244-250). */
+int hgpu_download_conserved(hgpu_ctx *ctx, double *unew);
+
+/* Device bytes a context of this configuration allocates (0 if invalid). */
+size_t hgpu_context_bytes(const hgpu_config *cfg);
+
+/* Serving loop (no counterpart in the reference, which runs one problem per
+   process).  Solves arrive at any time (hgpu_server_submit copies their
+   inputs); hgpu_server_poll is the request loop: it admits pending solves
+   first-fit in arrival order while their device footprint fits
+   max_device_bytes and fewer than max_active run, keeps steps_per_chunk
+   time steps in flight per running solve on its own CUDA stream (the work
+   of all running solves overlaps on the device), retires a solve when its t
+   has reached tf (cfg->tf is replaced by tf) and frees its memory for the
+   next admission.  Poll never blocks on running work.  A solve's result is
+   what running it alone gives.  Times are host wall-clock: queue_ms from
+   submit to admission, run_ms from admission to retirement. */
+typedef struct hgpu_server hgpu_server;
+int hgpu_server_create(size_t max_device_bytes, int max_active, int steps_per_chunk, hgpu_server **out);
+void hgpu_server_destroy(hgpu_server *srv);
+int hgpu_server_submit(hgpu_server *srv, const hgpu_config *cfg, const double *gcov, const double *gcon,
+                       const double *gcovpert, const double *gdet, const double *conn, const double *floors,
+                       const double *p, double tf, long long *id);
+int hgpu_server_poll(hgpu_server *srv, int *pending, int *active, int *finished);
+/* result of a finished solve (HGPU_E_INVALID while it runs); arrays in the layouts above */
+int hgpu_server_result(hgpu_server *srv, long long id, double *p, int *pflag, double *t, long long *steps,
+                       double *queue_ms, double *run_ms);
+int hgpu_server_release(hgpu_server *srv, long long id);
+
 /* Raw device pointers of the resident state for callers that keep data on
    the GPU (e.g. a graph-captured serving loop): primitive planes
    [8][nt1][nt2][nt3] of p (which=0) or pk (which=1). */

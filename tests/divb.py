@@ -44,3 +44,42 @@ def divb_max(p, gdet, ng, dx, n):
     dmax = max(dx[0], dx[1], dx[2] if n3 > 1 else 0.0)
     d = diff * (dmax / ((1.0 / 3.0) * gcorn * np.abs(norm) + SMALL))
     return float(np.max(np.abs(d)))
+
+
+def divb_maxavg(p, gdet, ng, dx, n):
+    """The reference's divbmaxavg (dump_ener.c:482-520): max and mean over all
+    active zones of |DIVBFLUXCT| at the zone's lower corner (dims of size 1
+    use the same zone on both sides); gdet at the corner from CORN3 (=CORNT,
+    the metric does not depend on x3)."""
+    n1, n2, n3 = n
+    s1, s2, s3 = int(n1 > 1), int(n2 > 1), int(n3 > 1)
+    g1, g2, g3 = ng * s1, ng * s2, ng * s3
+    gc = gdet[:p.shape[0], :p.shape[1], 7][:, :, None]
+    Fg = p[..., 5:8] * gc[..., None]
+    I, J, K = np.meshgrid(np.arange(n1) + g1, np.arange(n2) + g2, np.arange(n3) + g3, indexing="ij")
+
+    def avg1(a, b, c, q):
+        return 0.5 * (Fg[a, b, c, q] + Fg[a - s1, b, c, q])
+
+    def avg2(a, b, c, q):
+        return 0.5 * (Fg[a, b, c, q] + Fg[a, b - s2, c, q])
+
+    def for1(a, b, c):
+        return 0.5 * (avg2(a, b, c, 0) + avg2(a, b, c - s3, 0))
+
+    def for2(a, b, c):
+        return 0.5 * (avg1(a, b, c, 1) + avg1(a, b, c - s3, 1))
+
+    def for3(a, b, c):
+        return 0.5 * (avg2(a, b, c, 2) + avg2(a - s1, b, c, 2))
+
+    dfx = for1(I, J, K) - for1(I - s1, J, K)
+    dfy = for2(I, J, K) - for2(I, J - s2, K)
+    dfz = for3(I, J, K) - for3(I, J, K - s3)
+    nx = for1(I, J, K) + for1(I - s1, J, K)
+    ny = for2(I, J, K) + for2(I, J - s2, K)
+    nz = for3(I, J, K) + for3(I, J, K - s3)
+    mx = max(max(dx[0], dx[1]), dx[2])
+    norm = mx / ((1.0 / 3.0) * gdet[I, J, 5] * np.abs(nx + ny + nz) + SMALL)
+    d = np.abs((dfx / dx[0] + dfy / dx[1] + dfz / dx[2]) * norm)
+    return float(d.max()), float(d.mean())
