@@ -929,6 +929,7 @@ struct hgpu_ctx {
   Params P;
   cudaStream_t stream;
   double *p = nullptr, *pk = nullptr, *uf = nullptr, *ucum = nullptr;
+  double *pk1 = nullptr;  // second intermediate state of TIMEORDER 3 and 4
   double *F[4] = {nullptr, nullptr, nullptr, nullptr};
   double *E = nullptr;
   double *G = nullptr;
@@ -1027,6 +1028,7 @@ static int validate(const hgpu_config *c) {
   if (c->n3 > 1 && c->n3 < c->ng) return HGPU_E_INVALID;
   if (c->n1 > 1 && c->n1 < c->ng) return HGPU_E_INVALID;
   if (c->precision != HGPU_PREC_FP64 && c->precision != HGPU_PREC_MIXED) return HGPU_E_INVALID;
+  if (c->timeorder < 0 || c->timeorder > 4) return HGPU_E_INVALID;
   return HGPU_OK;
 }
 
@@ -1045,7 +1047,7 @@ void hgpu_destroy(hgpu_ctx *x) {
   for (cudaEvent_t e : x->freelist) cudaEventDestroy(e);
   void *ptrs[] = {x->p, x->pk, x->uf, x->ucum, x->F[1], x->F[2], x->F[3], x->E, x->G, x->pflag, x->gammacheck,
                   x->cand, x->fixlist, x->cand_orig, x->cand_dec, x->candmap, x->fixvals, x->sc, x->staging, x->istaging,
-                  x->pL, x->pR, x->WA, x->cell_inst, x->inst, x->progress};
+                  x->pL, x->pR, x->WA, x->cell_inst, x->inst, x->progress, x->pk1};
   for (void *q : ptrs)
     if (q) cudaFree(q);
   cudaStreamDestroy(x->stream);
@@ -1136,6 +1138,7 @@ int hgpu_create(const hgpu_config *cfg, hgpu_ctx **out) {
             cudaMalloc(&x->fixvals, sizeof(double) * 5 * x->cap) == cudaSuccess &&
             cudaMalloc(&x->sc, sizeof(Scalars)) == cudaSuccess;
   for (int dd = 1; dd <= 3 && ok; dd++) ok = cudaMalloc(&x->F[dd], pb) == cudaSuccess;
+  if (ok && cfg->timeorder >= 3) ok = cudaMalloc(&x->pk1, pb) == cudaSuccess && cudaMemset(x->pk1, 0, pb) == cudaSuccess;
   if (ok && cfg->lim == HGPU_LIM_WENO5)
     ok = cudaMalloc(&x->pL, pb) == cudaSuccess && cudaMalloc(&x->pR, pb) == cudaSuccess &&
          cudaMalloc(&x->WA, pb * W5_PLANES) == cudaSuccess;
@@ -1412,17 +1415,36 @@ static void launch_finalize(hgpu_ctx *x, int advance_time) {
     LAUNCH(x, K_FINALIZE, finalize_kernel, 1, 32, x->P, x->sc, advance_time);
 }
 
+// setup_rktimestep (step_ch.c:442-562): per stage of the TIMEORDER-stage
+// method, CUf (Ui, ulast, dU) and Cunew (Ui, dU, Uf), and the arrays read as
+// pb and written as pf (pi is always p): 0 = p, 1 = pk0, 2 = pk1
+struct RKStage {
+  double cuf[3], cun[3];
+  int pb, pf;
+};
+static const RKStage kRK1[1] = {{{1.0, 0.0, 1.0}, {0.0, 0.0, 1.0}, 0, 0}};
+static const RKStage kRK2[2] = {{{1.0, 0.0, 0.5}, {0.0, 0.0, 0.0}, 0, 1}, {{1.0, 0.0, 1.0}, {0.0, 0.0, 1.0}, 1, 0}};
+static const RKStage kRK3[3] = {{{1.0, 0.0, 1.0}, {0.0, 0.0, 0.0}, 0, 1},
+                                {{3.0 / 4.0, 1.0 / 4.0, 1.0 / 4.0}, {0.0, 0.0, 0.0}, 1, 2},
+                                {{1.0 / 3.0, 2.0 / 3.0, 2.0 / 3.0}, {0.0, 0.0, 1.0}, 2, 0}};
+static const RKStage kRK4[4] = {{{1.0, 0.0, 0.5}, {1.0, 1.0 / 6.0, 0.0}, 0, 1},
+                                {{1.0, 0.0, 0.5}, {0.0, 1.0 / 3.0, 0.0}, 1, 2},
+                                {{1.0, 0.0, 1.0}, {0.0, 1.0 / 3.0, 0.0}, 2, 1},
+                                {{1.0, 0.0, 1.0}, {0.0, 1.0 / 6.0, 0.0}, 1, 0}};
+
+static int num_orders(const hgpu_ctx *x) { return x->cfg.timeorder ? x->cfg.timeorder : 2; }
+
 static void launch_stage(hgpu_ctx *x, int timeorder) {
   const Dims &d = x->d;
-  cudaStream_t s = x->stream;
+  const int norders = num_orders(x);
+  const RKStage &S = (norders == 4 ? kRK4 : norders == 3 ? kRK3 : norders == 2 ? kRK2 : kRK1)[timeorder];
+  double *arr[3] = {x->p, x->pk, x->pk1};
   const double *pi = x->p;
-  const double *pb = (timeorder == 0) ? x->p : x->pk;
-  double *pf = (timeorder == 0) ? x->pk : x->p;
-  int finalstep = (timeorder == 1);
-  // midpoint tables (step_ch.c:504-524)
-  double CUf0 = 1.0, CUf1 = 0.0, CUf2 = (timeorder == 0) ? 0.5 : 1.0;
-  double Cn0 = 0.0, Cn1 = 0.0, Cn2 = (timeorder == 0) ? 0.0 : 1.0;
-  (void)s;
+  const double *pb = arr[S.pb];
+  double *pf = arr[S.pf];
+  int finalstep = (timeorder == norders - 1);
+  double CUf0 = S.cuf[0], CUf1 = S.cuf[1], CUf2 = S.cuf[2];
+  double Cn0 = S.cun[0], Cn1 = S.cun[1], Cn2 = S.cun[2];
   launch_reset(x);
   launch_fluxes(x, pb);
   LAUNCH(x, K_UPDATE, conserve_kernel, grid_for(x->active_box.size(), 128), 128, d, x->P, x->active_box, pi, pb, x->uf,
@@ -1486,8 +1508,7 @@ int hgpu_step_ch(hgpu_ctx *x, int nsteps, hgpu_stats *stats) {
   if (!x || nsteps < 0) return HGPU_E_INVALID;
   clear_counters(x);
   for (int n = 0; n < nsteps; n++) {
-    launch_stage(x, 0);
-    launch_stage(x, 1);
+    for (int o = 0; o < num_orders(x); o++) launch_stage(x, o);
     launch_finalize(x, 1);
   }
   CUDA_TRY(cudaGetLastError());
@@ -1508,8 +1529,7 @@ int hgpu_step_graph(hgpu_ctx *x, int nsteps, hgpu_stats *stats) {
     CUDA_TRY(cudaStreamSynchronize(x->stream));
     CUDA_TRY(cudaStreamBeginCapture(x->stream, cudaStreamCaptureModeThreadLocal));
     long long l0 = x->launches;
-    launch_stage(x, 0);
-    launch_stage(x, 1);
+    for (int o = 0; o < num_orders(x); o++) launch_stage(x, o);
     launch_finalize(x, 1);
     x->launches_per_step = x->launches - l0;
     x->launches = l0;
@@ -1537,7 +1557,7 @@ int hgpu_step_graph(hgpu_ctx *x, int nsteps, hgpu_stats *stats) {
 }
 
 int hgpu_advance_stage(hgpu_ctx *x, int timeorder, double *ndt, hgpu_stats *stats) {
-  if (!x || (timeorder != 0 && timeorder != 1)) return HGPU_E_INVALID;
+  if (!x || timeorder < 0 || timeorder >= num_orders(x)) return HGPU_E_INVALID;
   clear_counters(x);
   launch_stage(x, timeorder);
   launch_finalize(x, 0);
@@ -1800,8 +1820,7 @@ int hgpu_step_ch_timed(hgpu_ctx *x, int nsteps, float *ms, hgpu_stats *stats) {
   clear_counters(x);
   CUDA_TRY(cudaEventRecord(a, x->stream));
   for (int n = 0; n < nsteps; n++) {
-    launch_stage(x, 0);
-    launch_stage(x, 1);
+    for (int o = 0; o < num_orders(x); o++) launch_stage(x, o);
     launch_finalize(x, 1);
   }
   CUDA_TRY(cudaEventRecord(b, x->stream));

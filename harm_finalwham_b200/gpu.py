@@ -36,7 +36,7 @@ class hgpu_config(ctypes.Structure):
                 ("precision", ctypes.c_int), ("dx", ctypes.c_double * 4), ("gam", ctypes.c_double),
                 ("cour", ctypes.c_double), ("safe", ctypes.c_double), ("defcon", ctypes.c_double),
                 ("tf", ctypes.c_double), ("rhominlimit", ctypes.c_double), ("uuminlimit", ctypes.c_double),
-                ("gammamax", ctypes.c_double), ("gammafail", ctypes.c_double)]
+                ("gammamax", ctypes.c_double), ("gammafail", ctypes.c_double), ("timeorder", ctypes.c_int)]
 
 
 class hgpu_diag(ctypes.Structure):
@@ -146,9 +146,11 @@ class HarmGPU:
 
     def __init__(self, n1, n2, n3, ng, dx, lim="MC", flux="HLL", bc=("OUTFLOW", "OUTFLOW", "POLARAXIS",
                  "POLARAXIS", "PERIODIC", "PERIODIC"), precision="fp64", gam=4.0 / 3.0, cour=0.8, safe=1.3,
-                 defcon=1.0, tf=2000.0, rhominlimit=1e-20, uuminlimit=1e-20, gammamax=25.0, gammafail=2500.0):
+                 defcon=1.0, tf=2000.0, rhominlimit=1e-20, uuminlimit=1e-20, gammamax=25.0, gammafail=2500.0,
+                 timeorder=2):
         self.L = load_library()
         c = hgpu_config()
+        c.timeorder = int(timeorder)
         c.n1, c.n2, c.n3, c.ng = n1, n2, n3, ng
         c.lim = LIM[lim] if isinstance(lim, str) else int(lim)
         c.fluxmethod = FLUX[flux] if isinstance(flux, str) else int(flux)
@@ -177,7 +179,7 @@ class HarmGPU:
         o = cls(pr.n[0], pr.n[1], pr.n[2], pr.ng, pr.dx, lim=pr.lim, flux=pr.flux,
                 bc=tuple(inv_bc[b] for b in pr.bc), precision=precision, gam=pr.gam, cour=pr.cour, safe=pr.safe,
                 defcon=pr.defcon, tf=pr.tf, rhominlimit=pr.rhominlimit, uuminlimit=pr.uuminlimit,
-                gammamax=pr.gammamax, gammafail=pr.gammafail)
+                gammamax=pr.gammamax, gammafail=pr.gammafail, timeorder=getattr(pr, "timeorder", 2))
         o.upload_geometry(pr.gcov, pr.gcon, pr.gcovpert, pr.gdet, pr.conn, pr.floors)
         o.upload_state(pr.p, pr.pflag, pr.t, pr.dt)
         return o
@@ -425,8 +427,9 @@ class HarmBatch(HarmGPU):
 
 def make_config(n, ng, dx, lim="MC", flux="HLL", bc=("OUTFLOW", "OUTFLOW", "POLARAXIS", "POLARAXIS", "PERIODIC",
                 "PERIODIC"), precision="fp64", gam=4.0 / 3.0, cour=0.8, safe=1.3, defcon=1.0, tf=2000.0,
-                rhominlimit=1e-20, uuminlimit=1e-20, gammamax=25.0, gammafail=2500.0):
+                rhominlimit=1e-20, uuminlimit=1e-20, gammamax=25.0, gammafail=2500.0, timeorder=2):
     c = hgpu_config()
+    c.timeorder = int(timeorder)
     c.n1, c.n2, c.n3 = n
     c.ng = ng
     c.lim = LIM[lim] if isinstance(lim, str) else int(lim)

@@ -33,7 +33,7 @@
 extern "C" {
 #endif
 
-#define HGPU_ABI_VERSION 1
+#define HGPU_ABI_VERSION 2
 
 /* return codes */
 #define HGPU_OK 0
@@ -74,6 +74,8 @@ typedef struct {
   double dx[4];     /* dx[1..3] */
   double gam, cour, safe, defcon, tf;
   double rhominlimit, uuminlimit, gammamax, gammafail;
+  int timeorder;    /* TIMEORDER (setup_rktimestep, step_ch.c:442-562): 1 Euler,
+                       2 midpoint, 3 TVD RK3, 4 RK4; 0 means 2 */
 } hgpu_config;
 
 typedef struct hgpu_ctx hgpu_ctx;
@@ -108,10 +110,10 @@ int hgpu_download_state(hgpu_ctx *ctx, double *p, int *pflag, double *t, double 
    unless stats is non-NULL (then it synchronises and fills stats). */
 int hgpu_step_ch(hgpu_ctx *ctx, int nsteps, hgpu_stats *stats);
 
-/* advance (advance.c:16) for RK stage `timeorder` of the midpoint method,
+/* advance (advance.c:16) for RK stage `timeorder` (0 .. TIMEORDER-1),
    followed by the reference's per-stage bound_prim/post_fixup/bound_prim
-   sequence (step_ch.c:94-186).  Buffers: stage 0 reads p, writes pk;
-   stage 1 reads p and pk, writes p.  ndt receives the new dt estimate. */
+   sequence (step_ch.c:94-186), with the pi/pb/pf arrays of
+   setup_rktimestep.  ndt receives the new dt estimate. */
 int hgpu_advance_stage(hgpu_ctx *ctx, int timeorder, double *ndt, hgpu_stats *stats);
 
 /* fluxcalc (flux.c:7-318) including flux_ct (fluxct.c:10), on the current

@@ -22,7 +22,7 @@ Config overlay (settings only, no algorithm change): the FM torus problem
 file init.fishmon.c / init.fishmon.h / bounds.fishmon.c with
   EOMTYPE EOMGRMHD (init.fishmon.h:170 has EOMFFDE), defcoord=LOGRSINTH
   (init.fishmon.c:73 has 9), UTOPRIMVERSION=UTOPRIM2DFINAL
-  (init.fishmon.c:46), lim/fluxmethod/cour as requested, TIMEORDER=2,
+  (init.fishmon.c:46), lim/fluxmethod/cour as requested, TIMEORDER (2 unless asked),
   DOENOFLUX=NOENOFLUX, rescaletype=0 (r^-1.5 / r^-2.5 floors), N1/N2/N3.
 
 usage: python oracle/build_ref.py --n1 64 --n2 64 --n3 1 --lim MC --flux HLL
@@ -161,12 +161,12 @@ def overlay_init_h(text, n1, n2, n3, maxbnd):
     return text
 
 
-def overlay_init_c(text, lim, flux, cour):
+def overlay_init_c(text, lim, flux, cour, timeorder=2):
     w = "init.fishmon.c"
     text = sub_once(text, "  defcoord = 9;", "  defcoord = LOGRSINTH;", where=w)
     text = sub_once(text, "  UTOPRIMVERSION = UTOPRIMJONNONRELCOMPAT;", "  UTOPRIMVERSION = UTOPRIM2DFINAL;", where=w)
     text = sub_once(text, "  lim = PARA;", f"  lim = {LIMS[lim]};", where=w)
-    text = sub_once(text, "  TIMEORDER=4;", "  TIMEORDER=2;", where=w)
+    text = sub_once(text, "  TIMEORDER=4;", f"  TIMEORDER={int(timeorder)};", where=w)
     text = sub_once(text, "  DOENOFLUX = ENOFINITEVOLUME;", "  DOENOFLUX = NOENOFLUX;", count=2, where=w)
     text = sub_once(text, "  fluxmethod=HLLFLUX;", f"  fluxmethod={FLUXES[flux]};", where=w)
     text = sub_once(text, "  rescaletype=1;", "  rescaletype=0;", where=w)
@@ -185,9 +185,9 @@ int bound_prim_user_after_mpi(int boundstage, FTYPE prim[][N2M][N3M][NPR])
 """
 
 
-def build(ref, n1, n2, n3, lim, flux, cour, maxbnd, name=None, keep=False, verbose=False):
+def build(ref, n1, n2, n3, lim, flux, cour, maxbnd, name=None, keep=False, verbose=False, timeorder=2):
     os.makedirs(OUT, exist_ok=True)
-    name = name or f"harm_ref_{n1}x{n2}x{n3}_{lim}_{flux}"
+    name = name or (f"harm_ref_{n1}x{n2}x{n3}_{lim}_{flux}" + (f"_rk{timeorder}" if timeorder != 2 else ""))
     scratch = tempfile.mkdtemp(prefix="harmref_")
     try:
         for fn in os.listdir(ref):
@@ -222,7 +222,7 @@ def build(ref, n1, n2, n3, lim, flux, cour, maxbnd, name=None, keep=False, verbo
         with open(os.path.join(scratch, "init.h"), "w") as f:
             f.write(ih)
         with open(os.path.join(ref, "init.fishmon.c")) as f:
-            ic = overlay_init_c(f.read(), lim, flux, cour)
+            ic = overlay_init_c(f.read(), lim, flux, cour, timeorder)
         with open(os.path.join(scratch, "init.c"), "w") as f:
             f.write(ic)
         with open(os.path.join(ref, "bounds.fishmon.c")) as f:

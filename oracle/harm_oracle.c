@@ -1791,15 +1791,28 @@ typedef struct {
 } rkstage;
 
 /* midpoint method tables (step_ch.c:504-524) */
-static void rk2_stage(int timeorder, rkstage *s)
+/* setup_rktimestep (step_ch.c:442-562): CUf (Ui, ulast, dU) and Cunew (Ui,
+   dU, Uf) of stage `timeorder` of the TIMEORDER=`norders` method */
+static void rk_stage(int norders, int timeorder, rkstage *s)
 {
-  if (timeorder == 0) {
-    s->CUf[0] = 1.0; s->CUf[1] = 0.0; s->CUf[2] = 0.5; s->CUf[3] = 0.0;
-    s->Cunew[0] = 0.0; s->Cunew[1] = 0.0; s->Cunew[2] = 0.0; s->Cunew[3] = 0.0;
-  } else {
-    s->CUf[0] = 1.0; s->CUf[1] = 0.0; s->CUf[2] = 1.0; s->CUf[3] = 0.0;
-    s->Cunew[0] = 0.0; s->Cunew[1] = 0.0; s->Cunew[2] = 1.0; s->Cunew[3] = 0.0;
+  static const double cuf4[4][3] = {{1.0, 0.0, 0.5}, {1.0, 0.0, 0.5}, {1.0, 0.0, 1.0}, {1.0, 0.0, 1.0}};
+  static const double cun4[4][3] = {{1.0, 1.0 / 6.0, 0.0}, {0.0, 1.0 / 3.0, 0.0}, {0.0, 1.0 / 3.0, 0.0},
+                                    {0.0, 1.0 / 6.0, 0.0}};
+  static const double cuf3[3][3] = {{1.0, 0.0, 1.0}, {3.0 / 4.0, 1.0 / 4.0, 1.0 / 4.0}, {1.0 / 3.0, 2.0 / 3.0, 2.0 / 3.0}};
+  static const double cun3[3][3] = {{0.0, 0.0, 0.0}, {0.0, 0.0, 0.0}, {0.0, 0.0, 1.0}};
+  static const double cuf2[2][3] = {{1.0, 0.0, 0.5}, {1.0, 0.0, 1.0}};
+  static const double cun2[2][3] = {{0.0, 0.0, 0.0}, {0.0, 0.0, 1.0}};
+  static const double cuf1[1][3] = {{1.0, 0.0, 1.0}};
+  static const double cun1[1][3] = {{0.0, 0.0, 1.0}};
+  const double(*cuf)[3] = norders == 4 ? cuf4 : norders == 3 ? cuf3 : norders == 2 ? cuf2 : cuf1;
+  const double(*cun)[3] = norders == 4 ? cun4 : norders == 3 ? cun3 : norders == 2 ? cun2 : cun1;
+  int q;
+  for (q = 0; q < 3; q++) {
+    s->CUf[q] = cuf[timeorder][q];
+    s->Cunew[q] = cun[timeorder][q];
   }
+  s->CUf[3] = 0.0;
+  s->Cunew[3] = 0.0;
 }
 
 typedef struct {
@@ -1818,7 +1831,7 @@ static void advance(dom *d, const double *pi, const double *pb, double *pf, doub
   double idx1 = 1.0 / c->dx[1], idx2 = 1.0 / c->dx[2], idx3 = 1.0 / c->dx[3];
   long o1 = (long)d->nt[2] * d->nt[3], o2 = d->nt[3], o3 = 1;
   int finalstep = (timeorder == numtimeorders - 1);
-  rk2_stage(timeorder, &rk);
+  rk_stage(numtimeorders, timeorder, &rk);
 
   fluxcalc_dir(d, pb, 1, F1, sc->dq, &ndt1);
   fluxcalc_dir(d, pb, 2, F2, sc->dq, &ndt2);
@@ -1908,7 +1921,8 @@ int hgo_substep(const hgo_config *c, const hgo_geometry *g, const double *pi, co
   long iters = 0;
   dom_init(&d, c, g);
   if (alloc_scratch(&d, &sc)) return -1;
-  stage_with_fixups(&d, pi, pb, pf, uf, ucum, F1, F2, F3, pflag, dt, timeorder, 2, ndt, &sc, &iters);
+  stage_with_fixups(&d, pi, pb, pf, uf, ucum, F1, F2, F3, pflag, dt, timeorder, c->timeorder ? c->timeorder : 2,
+                    ndt, &sc, &iters);
   free_scratch(&sc);
   if (st) {
     st->newton_iters = iters;
@@ -1923,24 +1937,33 @@ int hgo_step(const hgo_config *c, const hgo_geometry *g, double *p, int *pflag, 
   dom d;
   scratch sc;
   long n, iters = 0;
-  double *pk, *uf, *ucum, *F1, *F2, *F3;
-  int s, z, nf = 0;
+  double *pk, *pk1, *uf, *ucum, *F1, *F2, *F3;
+  int s, z, nf = 0, norders = c->timeorder ? c->timeorder : 2, o;
   dom_init(&d, c, g);
   n = dom_ntot(&d);
   if (alloc_scratch(&d, &sc)) return -1;
   pk = (double *)calloc((size_t)n * NPR, sizeof(double));
+  pk1 = (double *)calloc((size_t)n * NPR, sizeof(double));
   uf = (double *)calloc((size_t)n * NPR, sizeof(double));
   ucum = (double *)calloc((size_t)n * NPR, sizeof(double));
   F1 = (double *)calloc((size_t)n * NPR, sizeof(double));
   F2 = (double *)calloc((size_t)n * NPR, sizeof(double));
   F3 = (double *)calloc((size_t)n * NPR, sizeof(double));
-  if (!pk || !uf || !ucum || !F1 || !F2 || !F3) return -1;
+  if (!pk || !pk1 || !uf || !ucum || !F1 || !F2 || !F3) return -1;
   for (s = 0; s < nsteps; s++) {
     double ndt;
-    /* pii/pbb/pff of the midpoint method: (p,p,pk0), (p,pk0,p) */
+    /* pii/pbb/pff of setup_rktimestep (step_ch.c:442-562): pi = p always;
+       (pb, pf): Euler (p,p); midpoint (p,pk0) (pk0,p); RK3 (p,pk0) (pk0,pk1)
+       (pk1,p); RK4 (p,pk0) (pk0,pk1) (pk1,pk0) (pk0,p) */
+    double *pb4[4] = {p, pk, pk1, pk}, *pf4[4] = {pk, pk1, pk, p};
+    double *pb3[3] = {p, pk, pk1}, *pf3[3] = {pk, pk1, p};
+    double *pb2[2] = {p, pk}, *pf2[2] = {pk, p};
+    double *pb1[1] = {p}, *pf1[1] = {p};
+    double **pbs = norders == 4 ? pb4 : norders == 3 ? pb3 : norders == 2 ? pb2 : pb1;
+    double **pfs = norders == 4 ? pf4 : norders == 3 ? pf3 : norders == 2 ? pf2 : pf1;
     memcpy(pk, p, sizeof(double) * NPR * n);
-    stage_with_fixups(&d, p, p, pk, uf, ucum, F1, F2, F3, pflag, *dt, 0, 2, &ndt, &sc, &iters);
-    stage_with_fixups(&d, p, pk, p, uf, ucum, F1, F2, F3, pflag, *dt, 1, 2, &ndt, &sc, &iters);
+    for (o = 0; o < norders; o++)
+      stage_with_fixups(&d, p, pbs[o], pfs[o], uf, ucum, F1, F2, F3, pflag, *dt, o, norders, &ndt, &sc, &iters);
     /* step_ch.c:236-247 */
     *t += *dt;
     if (ndt > c->safe * (*dt)) ndt = c->safe * (*dt);
@@ -1949,6 +1972,7 @@ int hgo_step(const hgo_config *c, const hgo_geometry *g, double *p, int *pflag, 
   }
   for (z = 0; z < n; z++) nf += (pflag[z] != 0);
   free(pk);
+  free(pk1);
   free(uf);
   free(ucum);
   free(F1);

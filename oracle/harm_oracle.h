@@ -54,6 +54,7 @@ typedef struct {
   double dx[4];
   double gam, cour, safe, defcon, tf;
   double rhominlimit, uuminlimit, gammamax, gammafail;
+  int timeorder;   /* TIMEORDER: 1 Euler, 2 midpoint, 3 TVD RK3, 4 RK4 (0 = 2) */
 } hgo_config;
 
 typedef struct {

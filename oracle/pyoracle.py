@@ -45,7 +45,7 @@ class hgo_config(ctypes.Structure):
                 ("dx", ctypes.c_double * 4), ("gam", ctypes.c_double), ("cour", ctypes.c_double),
                 ("safe", ctypes.c_double), ("defcon", ctypes.c_double), ("tf", ctypes.c_double),
                 ("rhominlimit", ctypes.c_double), ("uuminlimit", ctypes.c_double),
-                ("gammamax", ctypes.c_double), ("gammafail", ctypes.c_double)]
+                ("gammamax", ctypes.c_double), ("gammafail", ctypes.c_double), ("timeorder", ctypes.c_int)]
 
 
 class hgo_geometry(ctypes.Structure):
@@ -70,8 +70,9 @@ class Problem:
     def __init__(self, n1, n2, n3, ng, dx, gam=4.0 / 3.0, cour=0.8, lim="MC", flux="HLL",
                  bc=(BC_OUTFLOW, BC_OUTFLOW, BC_POLARAXIS, BC_POLARAXIS, BC_PERIODIC, BC_PERIODIC),
                  safe=1.3, defcon=1.0, tf=2000.0, rhominlimit=1e-20, uuminlimit=1e-20, gammamax=25.0,
-                 gammafail=2500.0):
+                 gammafail=2500.0, timeorder=2):
         self.n = (n1, n2, n3)
+        self.timeorder = timeorder
         self.ng = ng
         self.g = tuple(ng if n > 1 else 0 for n in self.n)
         self.s = tuple(1 if n > 1 else 0 for n in self.n)
@@ -114,6 +115,7 @@ class Problem:
         c.gam, c.cour, c.safe, c.defcon, c.tf = self.gam, self.cour, self.safe, self.defcon, self.tf
         c.rhominlimit, c.uuminlimit = self.rhominlimit, self.uuminlimit
         c.gammamax, c.gammafail = self.gammamax, self.gammafail
+        c.timeorder = getattr(self, "timeorder", 2)
         return c
 
     def copy(self):

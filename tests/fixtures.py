@@ -7,7 +7,8 @@ from oracle.pyoracle import Problem
 
 GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
 CASES = ["torus2d_16x16_mc_hll", "torus3d_12x12x6_mc_laxf", "torus2d_16x16_weno5_hll", "torus3d_12x12x6_weno5_laxf",
-         "torus2d_16x16_para_hll", "torus3d_12x12x6_para_laxf"]
+         "torus2d_16x16_para_hll", "torus3d_12x12x6_para_laxf", "torus2d_16x16_mc_hll_rk4",
+         "torus2d_16x16_mc_hll_rk1", "torus3d_12x12x6_weno5_laxf_rk3"]
 
 
 def load(name):
@@ -17,7 +18,8 @@ def load(name):
                  cour=float(d["cour"]), lim=str(d["lim"]), flux=str(d["flux"]), bc=tuple(int(x) for x in d["bc"]),
                  safe=float(d["safe"]), defcon=float(d["defcon"]), tf=float(d["tf"]),
                  rhominlimit=float(d["rhominlimit"]), uuminlimit=float(d["uuminlimit"]),
-                 gammamax=float(d["gammamax"]), gammafail=float(d["gammafail"]))
+                 gammamax=float(d["gammamax"]), gammafail=float(d["gammafail"]),
+                 timeorder=int(d["timeorder"]) if "timeorder" in d else 2)
     for k in ("gcov", "gcon", "gcovpert", "gdet", "conn", "floors"):
         getattr(pr, k)[...] = d[k]
     pr.p[...] = d["p_init"]

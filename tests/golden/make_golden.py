@@ -29,7 +29,7 @@ from oracle.pyoracle import RefDump  # noqa: E402
 # reference's MAXBND=11 line lengths) 6 per side
 NG = {"MC": 3, "PARA": 3, "WENO5": 6}
 
-# name: (n1, n2, n3, lim, flux, cour, nsteps, dump steps)
+# name: (n1, n2, n3, lim, flux, cour, nsteps, dump steps[, TIMEORDER])
 CASES = {
     "torus2d_16x16_mc_hll": (16, 16, 1, "MC", "HLL", 0.8, 5, [1, 5]),
     "torus3d_12x12x6_mc_laxf": (12, 12, 6, "MC", "LAXF", 0.8, 10, [1, 10]),
@@ -37,13 +37,17 @@ CASES = {
     "torus3d_12x12x6_weno5_laxf": (12, 12, 6, "WENO5", "LAXF", 0.8, 5, [1, 5]),
     "torus2d_16x16_para_hll": (16, 16, 1, "PARA", "HLL", 0.8, 5, [1, 5]),
     "torus3d_12x12x6_para_laxf": (12, 12, 6, "PARA", "LAXF", 0.8, 5, [1, 5]),
+    "torus2d_16x16_mc_hll_rk4": (16, 16, 1, "MC", "HLL", 0.8, 5, [1, 5], 4),
+    "torus2d_16x16_mc_hll_rk1": (16, 16, 1, "MC", "HLL", 0.8, 5, [1, 5], 1),
+    "torus3d_12x12x6_weno5_laxf_rk3": (12, 12, 6, "WENO5", "LAXF", 0.8, 3, [1, 3], 3),
 }
 
 
 def make(name, spec, ref):
-    n1, n2, n3, lim, flux, cour, nsteps, dumps = spec
+    n1, n2, n3, lim, flux, cour, nsteps, dumps = spec[:8]
+    timeorder = spec[8] if len(spec) > 8 else 2
     ng = NG[lim]
-    exe = build_ref.build(ref, n1, n2, n3, lim, flux, cour, 11)
+    exe = build_ref.build(ref, n1, n2, n3, lim, flux, cour, 11, timeorder=timeorder)
     with tempfile.TemporaryDirectory() as tmp:
         out = os.path.join(tmp, "out")
         subprocess.run([exe, out, str(nsteps)] + [str(s) for s in dumps], cwd=tmp, check=True,
@@ -55,7 +59,7 @@ def make(name, spec, ref):
                     tf=pr.tf, rhominlimit=pr.rhominlimit, uuminlimit=pr.uuminlimit, gammamax=pr.gammamax,
                     gammafail=pr.gammafail, gcov=pr.gcov, gcon=pr.gcon, gcovpert=pr.gcovpert, gdet=pr.gdet,
                     conn=pr.conn, floors=pr.floors, p_init=pr.p, pflag_init=pr.pflag, t_init=pr.t, dt_init=pr.dt,
-                    steps=np.array(dumps))
+                    steps=np.array(dumps), timeorder=np.array(timeorder))
         for s in dumps:
             m = rd.meta_of(f"s{s}")
             data[f"p_s{s}"] = rd.crop(rd.p(f"s{s}"), ng)

@@ -21,7 +21,8 @@ def test_library_builds_and_loads():
     path = hbuild.build()
     assert os.path.exists(path)
     L = load_library()
-    assert L.hgpu_abi_version() == 1
+    hdr = open(os.path.join(ROOT, "include", "harmgpu.h")).read()
+    assert L.hgpu_abi_version() == int(re.search(r"#define HGPU_ABI_VERSION (\d+)", hdr).group(1))
 
 
 def test_every_declared_symbol_is_exported():
