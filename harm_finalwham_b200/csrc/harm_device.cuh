@@ -585,4 +585,311 @@ __device__ __forceinline__ int utoprimgen(const double *U, const Metric &m, doub
   return lpflag;
 }
 
+// ---------------------------------------------------------------------------
+// Con-to-prim: Utoprimgen -> Utoprim_jon_nonrelcompat_inputnorestmass
+// (utoprim_jon.c:65-205, UTOPRIMVERSION=UTOPRIMJONNONRELCOMPAT, the FM torus
+// default set in init.fishmon.c:46): a 1-D Newton solve of E'(W') = 0 in
+// W' = W - D (WHICHHOTINVERTER 3, PRIMFROMVSQ 0, JONGENNEWTSTUFF 1,
+// USE_LINE_SEARCH -2), u2p_defs.h with PRECISEINVERSION 1, ideal gas.
+// ---------------------------------------------------------------------------
+struct JonU2P {
+  double Bsq, QdotB, QdotBsq, Qtsq, Qdotnp, D, wglobal, igammar, gammasq_too_big;
+};
+
+// utsq_calc (utoprim_jon.c:1294-1315)
+__device__ __forceinline__ double jon_utsq(const JonU2P &c, double W) {
+  double SoW = c.QdotB / W;
+  double top = c.Qtsq + (c.Bsq + 2.0 * W) * SoW * SoW;
+  double bottom = (c.Bsq * c.Bsq - c.Qtsq) + 2.0 * c.Bsq * W + W * W - SoW * SoW * (c.Bsq + 2.0 * W);
+  return top / bottom;
+}
+
+// coldgrhd (utoprim_jon.c:1402-1425)
+__device__ __forceinline__ int jon_coldgrhd(double Qtsq, double D, double *Wp) {
+  double det = D * D + Qtsq;
+  if (det < 0.0) return 1;
+  if (D > 0.0) *Wp = Qtsq / (D + sqrt(det));
+  else *Wp = Qtsq / (D - sqrt(det));
+  return 0;
+}
+
+__device__ __forceinline__ double jon_max(double a, double b) { return ((a) > (b)) ? (a) : (b); }  // global.h:750
+__device__ __forceinline__ double jon_sign(double a) {  // phys.c:1778
+  return (a > 0.0) ? 1.0 : ((a < 0.0) ? -1.0 : 0.0);
+}
+
+// func_Eprime (utoprim_jon.c:2258-2281): the Newton step -E'/(dE'/dW') from
+// Eprime_Wp (:1529-1554) and dEprimedWp (:1558-1587) with the ideal-gas EOS
+// pieces of utoprim_jon_eos.c (pressure_Wp_utsq :134, dpdWp_calc_utsq :262,
+// dpdvsq_calc2_Wp :391, wmrho0_compute_utsq :474) and eos.c:178-194.  Both
+// evaluate utsq_calc at the same W'; it is computed once here.
+__device__ __forceinline__ void jon_func(const JonU2P &c, double Wp, double *resid, double *dx) {
+  const double D = c.D;
+  const double W = Wp + D;
+  const double X = c.Bsq + W + 1.e-50;  // SMALL (global.h:1041)
+  double utsq = jon_utsq(c, W);
+  if (utsq < -0.1) utsq = 0.0;
+  const double gammasq = 1.0 + utsq;
+  const double gamma = sqrt(gammasq);
+  const double wmrho0 = (Wp - D * utsq / (1.0 + gamma)) / gammasq;
+  const double p_tmp = c.igammar * wmrho0;
+  const double X2 = X * X;
+  const double r = c.Qdotnp + Wp - p_tmp + 0.5 * c.Bsq + 0.5 * (c.Bsq * c.Qtsq - c.QdotBsq) / X2;
+  // dvsq_dW (:1378-1398)
+  const double Xv = c.Bsq + W;
+  const double Wsq = W * W;
+  const double W3 = Wsq * W;
+  const double X3v = Xv * Xv * Xv;
+  const double dvsq = -2. * (c.Qtsq / X3v + c.QdotBsq * (3.0 * W * Xv + c.Bsq * c.Bsq) / (W3 * X3v));
+  const double dp1 = 0.0 * 0.0 + (1.0 / gammasq) * c.igammar;
+  const double dp2 = (-D * gamma * 0.5) * 0.0 + (D * (gamma * 0.5 - 1.0) - Wp) * c.igammar;
+  const double dpdWp = dp1 + dp2 * dvsq;
+  const double X3 = X * X * X;
+  const double drdW = (1.0 - dpdWp) - (c.Bsq * c.Qtsq - c.QdotBsq) / X3;
+  *resid = r;
+  *dx = -r / drdW;
+}
+
+// Inversion of the evolved conserved vector U (includes gdet; U[UU] without
+// rest mass, as REMOVERESTMASSFROMUU 2 evolves it) with the guess in prim;
+// returns the pflag code and the Newton iteration count.  Flags follow the
+// reference: the non-B primitives are replaced whenever the Newton solve
+// returned 0 (UTOPRIMFAILCONVW, negative rho/u and a root equal to FAIL_VAL
+// come with new primitives, NaN components keep the guess with flag 8),
+// UTOPRIMFAILCONVRET keeps the guess.  A guess with u~^2 outside
+// [-MAXNEGUTSQ, UTSQ_TOO_BIG] or with no 4-velocity keeps the guess with
+// UTOPRIMFAILCONVGUESSUTSQ (the reference proceeds there with an unset W').
+__device__ __forceinline__ int utoprimgen_jon(const double *U, const Metric &m, double gam, double gammafail,
+                                              double *prim, int *iters) {
+  constexpr int MAX_NEWT_ITER = 200;
+  constexpr double NEWT_TOL = 1E3 * NUMEPSILON;
+  constexpr double NEWT_TOL_ULTRAREL = NUMEPSILON;
+  constexpr double MIN_NEWT_TOL = 1E-6;
+  constexpr int EXTRA_NEWT_ITER = 0;
+  constexpr int EXTRA_NEWT_ITER_ULTRAREL = 2;
+  constexpr double GAMMASQCHECKRESID = 1e2;
+  constexpr double MAXNEGUTSQ = 1E-10;
+  JonU2P c;
+  c.igammar = (gam - 1.0) / gam;
+  c.gammasq_too_big = gammafail * gammafail;
+  double Ut[NPR], pt[NPR];
+  // UtoU(UEVOLVE->UNOTHING); U[UU] stays without rest mass (utoprimgen.c:76-85)
+  double Ugf[NPR];
+#pragma unroll
+  for (int pl = 0; pl < NPR; pl++) Ugf[pl] = U[pl] / m.g;
+  prim[B1] = Ugf[B1];
+  prim[B2] = Ugf[B2];
+  prim[B3] = Ugf[B3];
+  const double alpha = 1.0 / sqrt(-GCON(m, 0, 0));
+#pragma unroll
+  for (int i = 0; i < NPR; i++) Ut[i] = alpha * Ugf[i];
+#pragma unroll
+  for (int i = 0; i < B1; i++) pt[i] = prim[i];
+#pragma unroll
+  for (int i = B1; i <= B3; i++) pt[i] = Ut[i];
+  // compute_setup_quantities (:494-636)
+  c.D = Ut[RHO];
+  double Bcon[4], Bcov[4], ncov[4], ncon[4], Qconp[4], Qcov[4], Qtcon[4];
+  Bcon[0] = 0.;
+  Bcon[1] = Ut[B1];
+  Bcon[2] = Ut[B2];
+  Bcon[3] = Ut[B3];
+#pragma unroll
+  for (int i = 0; i < 4; i++) {
+    double s = 0.;
+#pragma unroll
+    for (int j = 0; j < 4; j++) s += GCOV(m, i, j) * Bcon[j];
+    Bcov[i] = s;
+  }
+  double Bsq = 0.;
+#pragma unroll
+  for (int i = 1; i < 4; i++) Bsq += Bcon[i] * Bcov[i];
+  c.Bsq = Bsq;
+  const double lapse = sqrt(-1. / GCON(m, 0, 0));
+  ncov[0] = -lapse;
+  ncov[1] = 0.;
+  ncov[2] = 0.;
+  ncov[3] = 0.;
+#pragma unroll
+  for (int i = 0; i < 4; i++) {
+    double s = 0.;
+#pragma unroll
+    for (int j = 0; j < 4; j++) s += GCON(m, i, j) * ncov[j];
+    ncon[i] = s;
+  }
+#pragma unroll
+  for (int i = 0; i < 4; i++) {
+    double s = 0.;
+#pragma unroll
+    for (int j = 0; j < 4; j++) s += GCON(m, i, j) * Ut[UU + j];
+    Qconp[i] = s;
+  }
+  Qtcon[0] = 0.0;
+#pragma unroll
+  for (int j = 1; j < 4; j++) {
+    double s = 0.0;
+#pragma unroll
+    for (int i = 1; i < 4; i++) s += Ut[UU + i] * (GCON(m, i, j) + ncon[i] * ncon[j]);
+    Qtcon[j] = s;
+  }
+  double Qtsq = 0.;
+#pragma unroll
+  for (int i = 0; i < 4; i++) {
+    double s = 0.;
+#pragma unroll
+    for (int j = 0; j < 4; j++) s += GCOV(m, i, j) * Qtcon[j];
+    Qtsq += s * Qtcon[i];
+  }
+  c.Qtsq = Qtsq;
+#pragma unroll
+  for (int i = 0; i < 4; i++) Qcov[i] = (i == 0) ? Ut[UU] - c.D : Ut[UU + i];
+  double QdotB = 0.;
+#pragma unroll
+  for (int i = 1; i < 4; i++) QdotB += Qcov[i] * Bcon[i];
+  c.QdotB = QdotB;
+  c.QdotBsq = QdotB * QdotB;
+  c.Qdotnp = Qconp[0] * ncov[0] + c.D * (1.0 - 1.0 / fabs(ncov[TT]));
+  // set_guess_Wp (:640-745)
+  *iters = 0;
+  double utsq = 0.;
+#pragma unroll
+  for (int i = 1; i < 4; i++)
+#pragma unroll
+    for (int j = 1; j < 4; j++) utsq += GCOV(m, i, j) * pt[U1 + i - 1] * pt[U1 + j - 1];
+  if ((utsq < 0.) && (fabs(utsq) < MAXNEGUTSQ)) utsq = 0.0;
+  if (utsq < 0. || utsq > ((gammafail - 1.0) * (gammafail - 1.0))) return UTOPRIMFAILCONVGUESSUTSQ;
+  double gammasq = 1. + utsq;
+  double gamma = sqrt(gammasq);
+  double rho0 = c.D / gamma;
+  double u = pt[UU];
+  double p = (gam - 1.) * u;
+  double w = rho0 + u + p;
+  double bsq;
+  {
+    State q;
+    if (get_state(pt, m, q)) return UTOPRIMFAILCONVGUESSUTSQ;
+    bsq = dot4(q.bcon, q.bcov);
+  }
+  double Wp_last = c.D * utsq / (1.0 + gamma) + (u + p) * gammasq;
+  double W_last = Wp_last + c.D;
+  if ((w + bsq) * gammasq >= GAMMASQCHECKRESID) {
+    double Wpcoldhd;
+    if (jon_coldgrhd(c.Qtsq, c.D, &Wpcoldhd)) Wpcoldhd = Wp_last;
+    c.wglobal = 1E-5 * jon_max(jon_max(Wpcoldhd, Wp_last), w + bsq);
+    Wp_last = jon_max(jon_max(2.0 * Wpcoldhd, Wp_last), w + bsq);
+  } else {
+    c.wglobal = w + bsq;
+  }
+  // verify_Wlast (:752-812)
+  if (W_last < -c.D || Wp_last < 0) {
+    W_last = -c.D;
+    Wp_last = 0;
+  }
+  for (int i_increase = 0; i_increase < 10; i_increase++) {
+    if (!(W_last * W_last * W_last * (W_last + 2. * c.Bsq) - c.QdotBsq * (2. * W_last + c.Bsq) <=
+          W_last * W_last * (c.Qtsq - c.Bsq * c.Bsq)))
+      break;
+    Wp_last *= 10.;
+    W_last = Wp_last + c.D;
+  }
+  // general_newton_raphson (:2896-3424), n = 1, no line search
+  double x = Wp_last, x_old = x, x_older = x, dx = 0., dx_old = 1E30 * x, resid = 0.;
+  double errx = 1., xold0 = 0., residold = 0., damp = 1.0;
+  int n_iter = 0, doing_extra = 0, i_extra = 0;
+  const bool ultrarel_w = fabs(c.wglobal) > GAMMASQCHECKRESID;
+  bool keep = true;
+  while (keep) {
+    jon_func(c, x, &resid, &dx);
+    x_older = x_old;
+    x_old = x;
+    if (n_iter == 0) {
+      xold0 = x;
+      residold = resid;
+    } else if (jon_sign(residold) != jon_sign(resid)) {
+      if (fabs(xold0) > GAMMASQCHECKRESID || fabs(x_old) > GAMMASQCHECKRESID) {
+        damp = 0.5 * damp;
+        x = x_older;
+        dx = dx_old;
+      }
+    }
+    x += damp * dx;
+    errx = (c.wglobal == 0.) ? fabs(dx_old) : fabs(dx_old / jon_max(fabs(c.wglobal), fabs(x)));
+    // validate_Wp (:1726-1758)
+    if (x < -c.D && c.D > 0.0) {
+      double Wpc;
+      if (!jon_coldgrhd(c.Qtsq, c.D, &Wpc)) x = Wpc * 10.0;
+    }
+    x = (fabs(x / c.wglobal) > c.gammasq_too_big) ? 0.5 * (x_old + x) : x;
+    dx_old = dx;
+    // newt_errorcheck / newt_extracheck (:3430-3458)
+    const bool ur = ultrarel_w || (fabs(x) > GAMMASQCHECKRESID);
+    const bool conv = ur ? (fabs(errx) <= NEWT_TOL_ULTRAREL) : (fabs(errx) <= NEWT_TOL);
+    const int extra = ur ? EXTRA_NEWT_ITER_ULTRAREL : EXTRA_NEWT_ITER;
+    if (conv && (doing_extra == 0) && (extra > 0)) doing_extra = 1;
+    if (doing_extra == 1) i_extra++;
+    if ((conv && (doing_extra == 0)) || (i_extra > extra) || (n_iter >= (MAX_NEWT_ITER - 1))) keep = false;
+    n_iter++;
+  }
+  *iters = n_iter;
+  // f = resid^2/2 and df = -2 f are finite exactly when resid^2 is
+  int retval;
+  const double f = 0.5 * resid * resid;
+  if ((isfinite(f) == 0) || (isfinite(-2. * f) == 0) || (isfinite(x) == 0)) {
+    retval = 1;
+  } else {
+    x = x_old;
+    const bool ur = ultrarel_w || (fabs(x) > GAMMASQCHECKRESID);
+    const bool conv = ur ? (fabs(errx) <= NEWT_TOL_ULTRAREL) : (fabs(errx) <= NEWT_TOL);
+    retval = (conv || fabs(errx) <= MIN_NEWT_TOL) ? 0 : 1;
+  }
+  // check_Wp (:819-903)
+  const double Wp = x;
+  int lpflag = UTOPRIMNOFAIL;
+  if ((retval != 0) || (Wp == 1.e30)) {
+    lpflag = retval * 100 + 1;
+    if (retval != 0) return lpflag;
+  } else {
+    const double Wtest = Wp / c.wglobal;
+    if (!(Wtest <= 0.0) && (Wtest > c.gammasq_too_big)) lpflag = UTOPRIMFAILCONVW;
+  }
+  // Wp2prim (:949-1165), PRIMFROMVSQ 0
+  double pr0[NPR];
+#pragma unroll
+  for (int i = 0; i < NPR; i++) pr0[i] = pt[i];
+  const double W = Wp + c.D;
+  utsq = jon_utsq(c, W);
+  gammasq = 1.0 + utsq;
+  gamma = sqrt(gammasq);
+  const double wmrho0 = (Wp - c.D * utsq / (1.0 + gamma)) / gammasq;
+  rho0 = c.D / gamma;
+  p = c.igammar * wmrho0;
+  u = wmrho0 - p;
+  if ((rho0 <= 0.) || (u < 0.)) {
+    if ((rho0 <= 0.) && (u >= 0.)) lpflag = UTOPRIMFAILRHONEG;
+    if ((rho0 > 0.) && (u < 0.)) lpflag = UTOPRIMFAILUNEG;
+    if ((rho0 <= 0.) && (u < 0.)) lpflag = UTOPRIMFAILRHOUNEG;
+  }
+  pt[RHO] = rho0;
+  pt[UU] = u;
+#pragma unroll
+  for (int i = 1; i < 4; i++) pt[U1 + i - 1] = gamma / (W + c.Bsq) * (Qtcon[i] + QdotB * Bcon[i] / W);
+#pragma unroll
+  for (int i = 0; i < NPR; i++)
+    if (!isfinite(pt[i])) {
+      pt[i] = pr0[i];
+      lpflag = 8;  // UTOPRIMFAILNANRESULT
+    }
+#pragma unroll
+  for (int i = 0; i < B1; i++) prim[i] = pt[i];
+  return lpflag;
+}
+
+// Utoprimgen dispatch on UTOPRIMVERSION (0/6: UTOPRIM2DFINAL, 8: Jon)
+template <int UV>
+__device__ __forceinline__ int utoprimgen_v(const double *U, const Metric &m, double gam, double gammafail,
+                                            double *prim, int *iters) {
+  if (UV == 8) return utoprimgen_jon(U, m, gam, gammafail, prim, iters);
+  return utoprimgen(U, m, gam, gammafail, prim, iters);
+}
+
 }  // namespace hg

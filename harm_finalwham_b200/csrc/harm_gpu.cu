@@ -277,6 +277,7 @@ __global__ void __launch_bounds__(128, HG_MINB_UPDATE) conserve_kernel(
     if (err) atomicOr(&sc->err, err);
 }
 
+template <int UV>
 __global__ void __launch_bounds__(128, HG_MINB_INVERT) invert_kernel(Dims d, Params P, Box box, const double *pb,
                                                                      double *pf, const double *__restrict__ uf,
                                                                      const double *__restrict__ ucum,
@@ -307,7 +308,7 @@ __global__ void __launch_bounds__(128, HG_MINB_INVERT) invert_kernel(Dims d, Par
 #pragma unroll
     for (int v = 0; v < NPR; v++) pr[v] = pbz[v];
     int it = 0;
-    int flag = utoprimgen(Uin, m, gam, P.gammafail, pr, &it);
+    int flag = utoprimgen_v<UV>(Uin, m, gam, P.gammafail, pr, &it);
     my_iters = (unsigned long long)it;
     my_fail = (flag != 0);
     if (finalstep) {
@@ -863,7 +864,9 @@ __global__ void soa_to_aos_kernel(const double *__restrict__ s, double *__restri
   a[t] = s[(long long)v * nz + z];
 }
 
-// batched inversion on arbitrary per-zone metrics (hgpu_utoprim_batch)
+// batched inversion on arbitrary per-zone metrics (hgpu_utoprim_batch,
+// hgpu_utoprimgen_batch)
+template <int UV>
 __global__ void utoprim_batch_kernel(const double *__restrict__ U, const double *__restrict__ gcov,
                                      const double *__restrict__ gcon, const double *__restrict__ gdet, double *pr,
                                      int *pflag, long long n, double gam, double gammafail,
@@ -886,7 +889,7 @@ __global__ void utoprim_batch_kernel(const double *__restrict__ U, const double 
       p[v] = pr[t * NPR + v];
     }
     int it = 0;
-    pflag[t] = utoprimgen(u, m, gam, gammafail, p, &it);
+    pflag[t] = utoprimgen_v<UV>(u, m, gam, gammafail, p, &it);
 #pragma unroll
     for (int v = 0; v < NPR; v++) pr[t * NPR + v] = p[v];
     it_total = (unsigned long long)it;
@@ -1029,6 +1032,9 @@ static int validate(const hgpu_config *c) {
   if (c->n1 > 1 && c->n1 < c->ng) return HGPU_E_INVALID;
   if (c->precision != HGPU_PREC_FP64 && c->precision != HGPU_PREC_MIXED) return HGPU_E_INVALID;
   if (c->timeorder < 0 || c->timeorder > 4) return HGPU_E_INVALID;
+  if (c->utoprimversion != 0 && c->utoprimversion != HGPU_UTOPRIM2DFINAL &&
+      c->utoprimversion != HGPU_UTOPRIMJONNONRELCOMPAT)
+    return HGPU_E_INVALID;
   return HGPU_OK;
 }
 
@@ -1449,8 +1455,12 @@ static void launch_stage(hgpu_ctx *x, int timeorder) {
   launch_fluxes(x, pb);
   LAUNCH(x, K_UPDATE, conserve_kernel, grid_for(x->active_box.size(), 128), 128, d, x->P, x->active_box, pi, pb, x->uf,
          x->ucum, x->F[1], x->F[2], x->F[3], x->E, x->G, x->sc, CUf0, CUf1, CUf2, Cn0, Cn1, Cn2, timeorder);
-  LAUNCH(x, K_INVERT, invert_kernel, grid_for(x->active_box.size(), 128), 128, d, x->P, x->active_box, pb, pf, x->uf,
-         x->ucum, x->G, x->pflag, x->sc, finalstep);
+  if (x->cfg.utoprimversion == HGPU_UTOPRIMJONNONRELCOMPAT)
+    LAUNCH(x, K_INVERT, invert_kernel<8>, grid_for(x->active_box.size(), 128), 128, d, x->P, x->active_box, pb, pf,
+           x->uf, x->ucum, x->G, x->pflag, x->sc, finalstep);
+  else
+    LAUNCH(x, K_INVERT, invert_kernel<6>, grid_for(x->active_box.size(), 128), 128, d, x->P, x->active_box, pb, pf,
+           x->uf, x->ucum, x->G, x->pflag, x->sc, finalstep);
   launch_bound(x, pf);
   // post_fixup (fixup.c:37-96)
   if (x->P.cell_inst)
@@ -1630,9 +1640,10 @@ int hgpu_sync(hgpu_ctx *x) {
   return HGPU_OK;
 }
 
-int hgpu_utoprim_batch(const double *U, const double *gcov, const double *gcon, const double *gdet, double *pr,
-                       int *pflag, long long n, double gam, double gammafail, long long *iters) {
+static int utoprim_batch_impl(const double *U, const double *gcov, const double *gcon, const double *gdet, double *pr,
+                              int *pflag, long long n, double gam, double gammafail, int uv, long long *iters) {
   if (n < 0 || (n > 0 && (!U || !gcov || !gcon || !gdet || !pr || !pflag))) return HGPU_E_INVALID;
+  if (uv != 0 && uv != HGPU_UTOPRIM2DFINAL && uv != HGPU_UTOPRIMJONNONRELCOMPAT) return HGPU_E_INVALID;
   if (n == 0) {
     if (iters) *iters = 0;
     return HGPU_OK;
@@ -1657,7 +1668,10 @@ int hgpu_utoprim_batch(const double *U, const double *gcov, const double *gcon, 
     cudaMemcpy(dg, gdet, sizeof(double) * n, cudaMemcpyHostToDevice);
     cudaMemcpy(dpr, pr, sizeof(double) * 8 * n, cudaMemcpyHostToDevice);
     cudaMemset(dit, 0, sizeof(unsigned long long));
-    utoprim_batch_kernel<<<grid_for(n, 128), 128>>>(dU, dgcov, dgcon, dg, dpr, dpf, n, gam, gammafail, dit);
+    if (uv == HGPU_UTOPRIMJONNONRELCOMPAT)
+      utoprim_batch_kernel<8><<<grid_for(n, 128), 128>>>(dU, dgcov, dgcon, dg, dpr, dpf, n, gam, gammafail, dit);
+    else
+      utoprim_batch_kernel<6><<<grid_for(n, 128), 128>>>(dU, dgcov, dgcon, dg, dpr, dpf, n, gam, gammafail, dit);
     e = cudaGetLastError();
     if (e == cudaSuccess) e = cudaDeviceSynchronize();
     if (e == cudaSuccess) {
@@ -1679,6 +1693,17 @@ int hgpu_utoprim_batch(const double *U, const double *gcov, const double *gcon, 
   cudaFree(dpf);
   cudaFree(dit);
   return rc;
+}
+
+int hgpu_utoprim_batch(const double *U, const double *gcov, const double *gcon, const double *gdet, double *pr,
+                       int *pflag, long long n, double gam, double gammafail, long long *iters) {
+  return utoprim_batch_impl(U, gcov, gcon, gdet, pr, pflag, n, gam, gammafail, HGPU_UTOPRIM2DFINAL, iters);
+}
+
+int hgpu_utoprimgen_batch(const double *U, const double *gcov, const double *gcon, const double *gdet, double *pr,
+                          int *pflag, long long n, double gam, double gammafail, int utoprimversion,
+                          long long *iters) {
+  return utoprim_batch_impl(U, gcov, gcon, gdet, pr, pflag, n, gam, gammafail, utoprimversion, iters);
 }
 
 // ---------------------------------------------------------------------------
@@ -2032,7 +2057,7 @@ extern "C" int hgpu_utoprim_batch_noalloc(const double *U, const double *gcov, c
   CUDA_TRY(cudaMemcpy(dpr, pr, sizeof(double) * 8 * n, cudaMemcpyHostToDevice));
   // the counter keeps the previous call's value: clear it
   CUDA_TRY(cudaMemset(dit, 0, sizeof(unsigned long long)));
-  utoprim_batch_kernel<<<grid_for(n, 128), 128>>>(dU, dgcov, dgcon, dg, dpr, dpf, n, gam, gammafail, dit);
+  utoprim_batch_kernel<6><<<grid_for(n, 128), 128>>>(dU, dgcov, dgcon, dg, dpr, dpf, n, gam, gammafail, dit);
   CUDA_TRY(cudaGetLastError());
   CUDA_TRY(cudaDeviceSynchronize());
   unsigned long long it = 0;

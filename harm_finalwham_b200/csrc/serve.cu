@@ -6,8 +6,9 @@
 // their device footprint (hgpu_context_bytes) fits the server's byte budget
 // and the active-slot limit, gives every admitted request its own context
 // and CUDA stream with the state resident in HBM, keeps a chunk of time
-// steps in flight per request (so the work of all admitted requests
-// overlaps on the device), notices finished chunks without blocking
+// steps in flight per request as replays of the request's captured step
+// graph (so the work of all admitted requests overlaps on the device and
+// the host issues one launch per step), notices finished chunks without blocking
 // (cudaEventQuery on an event recorded after a progress copy), retires a
 // request when its t reached its end time (the step kernels freeze a
 // finished context, so a chunk that overruns the end leaves the state
@@ -120,7 +121,9 @@ static int admit(hgpu_server *s, Request *r) {
 }
 
 static void issue_chunk(hgpu_server *s, Request *r) {
-  int rc = hgpu_step_ch(r->ctx, s->chunk, nullptr);
+  // a chunk is `chunk` replays of the request's captured time step (one graph
+  // launch per step instead of one launch per kernel)
+  int rc = hgpu_step_graph(r->ctx, s->chunk, nullptr);
   if (!rc) rc = hg_progress_async(r->ctx, r->prog, r->ev);
   if (rc) {
     r->rc = rc;

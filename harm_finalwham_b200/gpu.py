@@ -20,6 +20,7 @@ LIM = {"DONOR": 0, "VANL": 1, "MINM": 2, "MC": 3, "PARA": 4, "WENO5": 9}
 FLUX = {"LAXF": 0, "HLL": 1}
 BC = {"OUTFLOW": 0, "POLARAXIS": 4, "PERIODIC": 7, "OUTFLOW_COPY": 1000}
 PREC = {"fp64": 0, "mixed": 1}
+UTOPRIM = {"2DFINAL": 6, "JON": 8, "JONNONRELCOMPAT": 8}
 
 _lib = None
 
@@ -36,7 +37,8 @@ class hgpu_config(ctypes.Structure):
                 ("precision", ctypes.c_int), ("dx", ctypes.c_double * 4), ("gam", ctypes.c_double),
                 ("cour", ctypes.c_double), ("safe", ctypes.c_double), ("defcon", ctypes.c_double),
                 ("tf", ctypes.c_double), ("rhominlimit", ctypes.c_double), ("uuminlimit", ctypes.c_double),
-                ("gammamax", ctypes.c_double), ("gammafail", ctypes.c_double), ("timeorder", ctypes.c_int)]
+                ("gammamax", ctypes.c_double), ("gammafail", ctypes.c_double), ("timeorder", ctypes.c_int),
+                ("utoprimversion", ctypes.c_int)]
 
 
 class hgpu_diag(ctypes.Structure):
@@ -79,6 +81,8 @@ def load_library(path=None):
     L.hgpu_bound_prim.argtypes = [ctypes.c_void_p, ctypes.c_int]
     L.hgpu_utoprim_batch.argtypes = [_dp, _dp, _dp, _dp, _dp, _ip, ctypes.c_longlong, ctypes.c_double,
                                      ctypes.c_double, _P(ctypes.c_longlong)]
+    L.hgpu_utoprimgen_batch.argtypes = [_dp, _dp, _dp, _dp, _dp, _ip, ctypes.c_longlong, ctypes.c_double,
+                                        ctypes.c_double, ctypes.c_int, _P(ctypes.c_longlong)]
     L.hgpu_device_prims.argtypes = [ctypes.c_void_p, ctypes.c_int, _P(ctypes.c_void_p)]
     L.hgpu_sync.argtypes = [ctypes.c_void_p]
     L.hgpu_init_dt.argtypes = [ctypes.c_void_p, _dp]
@@ -113,7 +117,7 @@ def load_library(path=None):
                  "hgpu_free_pinned", "hgpu_fp64_peak"):
         getattr(L, name).restype = ctypes.c_int
     for name in ("hgpu_create", "hgpu_upload_geometry", "hgpu_upload_state", "hgpu_download_state", "hgpu_step_ch",
-                 "hgpu_advance_stage", "hgpu_fluxcalc", "hgpu_bound_prim", "hgpu_utoprim_batch",
+                 "hgpu_advance_stage", "hgpu_fluxcalc", "hgpu_bound_prim", "hgpu_utoprim_batch", "hgpu_utoprimgen_batch",
                  "hgpu_device_prims", "hgpu_sync", "hgpu_create_batch", "hgpu_batch_layout", "hgpu_batch_status",
                  "hgpu_step_graph", "hgpu_batch_run", "hgpu_diagnostics", "hgpu_download_conserved", "hgpu_server_create", "hgpu_server_submit",
                  "hgpu_server_poll", "hgpu_server_result", "hgpu_server_release"):
@@ -147,10 +151,11 @@ class HarmGPU:
     def __init__(self, n1, n2, n3, ng, dx, lim="MC", flux="HLL", bc=("OUTFLOW", "OUTFLOW", "POLARAXIS",
                  "POLARAXIS", "PERIODIC", "PERIODIC"), precision="fp64", gam=4.0 / 3.0, cour=0.8, safe=1.3,
                  defcon=1.0, tf=2000.0, rhominlimit=1e-20, uuminlimit=1e-20, gammamax=25.0, gammafail=2500.0,
-                 timeorder=2):
+                 timeorder=2, utoprim="2DFINAL"):
         self.L = load_library()
         c = hgpu_config()
         c.timeorder = int(timeorder)
+        c.utoprimversion = UTOPRIM[utoprim] if isinstance(utoprim, str) else int(utoprim)
         c.n1, c.n2, c.n3, c.ng = n1, n2, n3, ng
         c.lim = LIM[lim] if isinstance(lim, str) else int(lim)
         c.fluxmethod = FLUX[flux] if isinstance(flux, str) else int(flux)
@@ -179,7 +184,8 @@ class HarmGPU:
         o = cls(pr.n[0], pr.n[1], pr.n[2], pr.ng, pr.dx, lim=pr.lim, flux=pr.flux,
                 bc=tuple(inv_bc[b] for b in pr.bc), precision=precision, gam=pr.gam, cour=pr.cour, safe=pr.safe,
                 defcon=pr.defcon, tf=pr.tf, rhominlimit=pr.rhominlimit, uuminlimit=pr.uuminlimit,
-                gammamax=pr.gammamax, gammafail=pr.gammafail, timeorder=getattr(pr, "timeorder", 2))
+                gammamax=pr.gammamax, gammafail=pr.gammafail, timeorder=getattr(pr, "timeorder", 2),
+                utoprim=getattr(pr, "utoprim", "2DFINAL"))
         o.upload_geometry(pr.gcov, pr.gcon, pr.gcovpert, pr.gdet, pr.conn, pr.floors)
         o.upload_state(pr.p, pr.pflag, pr.t, pr.dt)
         return o
@@ -325,8 +331,9 @@ class HarmGPU:
         return a[g[0]:g[0] + self.n[0], g[1]:g[1] + self.n[1], g[2]:g[2] + self.n[2]]
 
 
-def utoprim_batch(U, gcov, gcon, gdet, guess, gam, gammafail):
-    """Batched Utoprimgen on the GPU (hgpu_utoprim_batch)."""
+def utoprim_batch(U, gcov, gcon, gdet, guess, gam, gammafail, version="2DFINAL"):
+    """Batched Utoprimgen on the GPU (hgpu_utoprimgen_batch): version
+    "2DFINAL" (UTOPRIM2DFINAL) or "JON" (UTOPRIMJONNONRELCOMPAT)."""
     L = load_library()
     U = _contig(U, np.float64)
     gcov = _contig(gcov, np.float64)
@@ -336,8 +343,10 @@ def utoprim_batch(U, gcov, gcon, gdet, guess, gam, gammafail):
     n = U.shape[0]
     pflag = np.zeros(n, dtype=np.int32)
     it = ctypes.c_longlong(0)
-    _check(L, L.hgpu_utoprim_batch(_ptr(U), _ptr(gcov), _ptr(gcon), _ptr(gdet), _ptr(pr), _ptr(pflag, ctypes.c_int),
-                                   n, gam, gammafail, ctypes.byref(it)))
+    _check(L, L.hgpu_utoprimgen_batch(_ptr(U), _ptr(gcov), _ptr(gcon), _ptr(gdet), _ptr(pr),
+                                      _ptr(pflag, ctypes.c_int), n, gam, gammafail,
+                                      UTOPRIM[version] if isinstance(version, str) else int(version),
+                                      ctypes.byref(it)))
     return pr, pflag, it.value
 
 
@@ -427,9 +436,11 @@ class HarmBatch(HarmGPU):
 
 def make_config(n, ng, dx, lim="MC", flux="HLL", bc=("OUTFLOW", "OUTFLOW", "POLARAXIS", "POLARAXIS", "PERIODIC",
                 "PERIODIC"), precision="fp64", gam=4.0 / 3.0, cour=0.8, safe=1.3, defcon=1.0, tf=2000.0,
-                rhominlimit=1e-20, uuminlimit=1e-20, gammamax=25.0, gammafail=2500.0, timeorder=2):
+                rhominlimit=1e-20, uuminlimit=1e-20, gammamax=25.0, gammafail=2500.0, timeorder=2,
+                utoprim="2DFINAL"):
     c = hgpu_config()
     c.timeorder = int(timeorder)
+    c.utoprimversion = UTOPRIM[utoprim] if isinstance(utoprim, str) else int(utoprim)
     c.n1, c.n2, c.n3 = n
     c.ng = ng
     c.lim = LIM[lim] if isinstance(lim, str) else int(lim)

@@ -33,7 +33,7 @@
 extern "C" {
 #endif
 
-#define HGPU_ABI_VERSION 2
+#define HGPU_ABI_VERSION 3
 
 /* return codes */
 #define HGPU_OK 0
@@ -60,6 +60,11 @@ extern "C" {
    id 0 for both, the problem file decides, so the copy gets its own id. */
 #define HGPU_BC_OUTFLOW_COPY 1000
 
+/* con-to-prim inverters (UTOPRIMVERSION, global.h:283-287) */
+#define HGPU_UTOPRIM2DFINAL 6            /* 2D Newton on (W, v^2), utoprim_2d_final.c */
+#define HGPU_UTOPRIMJONNONRELCOMPAT 8    /* 1D Newton on E'(W'), utoprim_jon.c; the FM
+                                            torus default (init.fishmon.c:46) */
+
 /* precision modes */
 #define HGPU_PREC_FP64 0      /* bit-identical to the reference CPU build */
 #define HGPU_PREC_MIXED 1     /* FP32 reconstruction, wave speeds and Riemann flux */
@@ -76,6 +81,7 @@ typedef struct {
   double rhominlimit, uuminlimit, gammamax, gammafail;
   int timeorder;    /* TIMEORDER (setup_rktimestep, step_ch.c:442-562): 1 Euler,
                        2 midpoint, 3 TVD RK3, 4 RK4; 0 means 2 */
+  int utoprimversion; /* HGPU_UTOPRIM*; 0 means HGPU_UTOPRIM2DFINAL */
 } hgpu_config;
 
 typedef struct hgpu_ctx hgpu_ctx;
@@ -132,6 +138,14 @@ int hgpu_bound_prim(hgpu_ctx *ctx, int which);
    codes.  iters (may be NULL) receives the total Newton iterations. */
 int hgpu_utoprim_batch(const double *U, const double *gcov, const double *gcon, const double *gdet, double *pr,
                        int *pflag, long long n, double gam, double gammafail, long long *iters);
+
+/* The same with the inverter chosen: utoprimversion is HGPU_UTOPRIM2DFINAL
+   (what hgpu_utoprim_batch runs) or HGPU_UTOPRIMJONNONRELCOMPAT, the
+   reference's Utoprimgen_pick(UTOPRIMJONNONRELCOMPAT) (utoprimgen.c:687) ->
+   Utoprim_jon_nonrelcompat_inputnorestmass (utoprim_jon.c:65). */
+int hgpu_utoprimgen_batch(const double *U, const double *gcov, const double *gcon, const double *gdet, double *pr,
+                          int *pflag, long long n, double gam, double gammafail, int utoprimversion,
+                          long long *iters);
 
 /* Utoprimgen batch that allocates nothing (no counterpart in the reference).
    Same arguments and results as hgpu_utoprim_batch, for callers that cannot

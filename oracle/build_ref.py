@@ -21,8 +21,9 @@ Mechanical patches (the reference targets icc):
 Config overlay (settings only, no algorithm change): the FM torus problem
 file init.fishmon.c / init.fishmon.h / bounds.fishmon.c with
   EOMTYPE EOMGRMHD (init.fishmon.h:170 has EOMFFDE), defcoord=LOGRSINTH
-  (init.fishmon.c:73 has 9), UTOPRIMVERSION=UTOPRIM2DFINAL
-  (init.fishmon.c:46), lim/fluxmethod/cour as requested, TIMEORDER (2 unless asked),
+  (init.fishmon.c:73 has 9), UTOPRIMVERSION=UTOPRIM2DFINAL unless the Jon
+  inverter (UTOPRIMJONNONRELCOMPAT, init.fishmon.c:46) is asked for,
+  lim/fluxmethod/cour as requested, TIMEORDER (2 unless asked),
   DOENOFLUX=NOENOFLUX, rescaletype=0 (r^-1.5 / r^-2.5 floors), N1/N2/N3.
 
 usage: python oracle/build_ref.py --n1 64 --n2 64 --n3 1 --lim MC --flux HLL
@@ -161,10 +162,13 @@ def overlay_init_h(text, n1, n2, n3, maxbnd):
     return text
 
 
-def overlay_init_c(text, lim, flux, cour, timeorder=2):
+UTOPRIMS = {"2DFINAL": "UTOPRIM2DFINAL", "JON": "UTOPRIMJONNONRELCOMPAT"}
+
+
+def overlay_init_c(text, lim, flux, cour, timeorder=2, utoprim="2DFINAL"):
     w = "init.fishmon.c"
     text = sub_once(text, "  defcoord = 9;", "  defcoord = LOGRSINTH;", where=w)
-    text = sub_once(text, "  UTOPRIMVERSION = UTOPRIMJONNONRELCOMPAT;", "  UTOPRIMVERSION = UTOPRIM2DFINAL;", where=w)
+    text = sub_once(text, "  UTOPRIMVERSION = UTOPRIMJONNONRELCOMPAT;", f"  UTOPRIMVERSION = {UTOPRIMS[utoprim]};", where=w)
     text = sub_once(text, "  lim = PARA;", f"  lim = {LIMS[lim]};", where=w)
     text = sub_once(text, "  TIMEORDER=4;", f"  TIMEORDER={int(timeorder)};", where=w)
     text = sub_once(text, "  DOENOFLUX = ENOFINITEVOLUME;", "  DOENOFLUX = NOENOFLUX;", count=2, where=w)
@@ -185,9 +189,11 @@ int bound_prim_user_after_mpi(int boundstage, FTYPE prim[][N2M][N3M][NPR])
 """
 
 
-def build(ref, n1, n2, n3, lim, flux, cour, maxbnd, name=None, keep=False, verbose=False, timeorder=2):
+def build(ref, n1, n2, n3, lim, flux, cour, maxbnd, name=None, keep=False, verbose=False, timeorder=2,
+          utoprim="2DFINAL"):
     os.makedirs(OUT, exist_ok=True)
-    name = name or (f"harm_ref_{n1}x{n2}x{n3}_{lim}_{flux}" + (f"_rk{timeorder}" if timeorder != 2 else ""))
+    name = name or (f"harm_ref_{n1}x{n2}x{n3}_{lim}_{flux}" + (f"_rk{timeorder}" if timeorder != 2 else "")
+                    + ("_jon" if utoprim == "JON" else ""))
     scratch = tempfile.mkdtemp(prefix="harmref_")
     try:
         for fn in os.listdir(ref):
@@ -222,7 +228,7 @@ def build(ref, n1, n2, n3, lim, flux, cour, maxbnd, name=None, keep=False, verbo
         with open(os.path.join(scratch, "init.h"), "w") as f:
             f.write(ih)
         with open(os.path.join(ref, "init.fishmon.c")) as f:
-            ic = overlay_init_c(f.read(), lim, flux, cour, timeorder)
+            ic = overlay_init_c(f.read(), lim, flux, cour, timeorder, utoprim)
         with open(os.path.join(scratch, "init.c"), "w") as f:
             f.write(ic)
         with open(os.path.join(ref, "bounds.fishmon.c")) as f:
@@ -258,10 +264,13 @@ def main():
     ap.add_argument("--maxbnd", type=int, default=11)
     ap.add_argument("--name", default=None)
     ap.add_argument("--keep", action="store_true")
+    ap.add_argument("--timeorder", type=int, default=2, choices=[1, 2, 3, 4])
+    ap.add_argument("--utoprim", default="2DFINAL", choices=sorted(UTOPRIMS))
     a = ap.parse_args()
     if not os.path.isdir(a.ref):
         raise SystemExit(f"reference tree not found: {a.ref}")
-    build(a.ref, a.n1, a.n2, a.n3, a.lim, a.flux, a.cour, a.maxbnd, a.name, a.keep, verbose=True)
+    build(a.ref, a.n1, a.n2, a.n3, a.lim, a.flux, a.cour, a.maxbnd, a.name, a.keep, verbose=True,
+          timeorder=a.timeorder, utoprim=a.utoprim)
 
 
 if __name__ == "__main__":

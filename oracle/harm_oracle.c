@@ -1369,14 +1369,361 @@ static int utoprim_2d_final(const double *U, const geomref *g, const hgo_config 
   return lpflag;
 }
 
+/* ------------------------------------------------------------------ */
+/* con-to-prim: Utoprim_jon_nonrelcompat_inputnorestmass (utoprim_jon.c) */
+/* 1-D E'(W') Newton solve in W' = W - D (WHICHHOTINVERTER 3,             */
+/* PRIMFROMVSQ 0, USE_LINE_SEARCH -2, JONGENNEWTSTUFF 1; u2p_defs.h with   */
+/* PRECISEINVERSION 1 and OPTIMIZED 1), hot GRMHD, ideal-gas EOS.          */
+/* ------------------------------------------------------------------ */
+#define GAMMASQCHECKRESID (1e2)              /* u2p_defs.h:21 */
+#define NEWT_TOL_ULTRAREL (NUMEPSILON)       /* u2p_defs.h:29 */
+#define EXTRA_NEWT_ITER_ULTRAREL 2           /* u2p_defs.h:67 */
+
+typedef struct {
+  double Bsq, QdotB, QdotBsq, Qtsq, Qdotnp, D, wglobal, igammar, gammasq_too_big;
+  int iters;
+} jonctx;
+
+static inline double jon_sign(double a) { return (a > 0.0) ? 1.0 : ((a < 0.0) ? -1.0 : 0.0); } /* phys.c:1778 */
+static inline double jon_max(double a, double b) { return ((a) > (b)) ? (a) : (b); }           /* global.h:750 */
+
+/* utsq_calc (utoprim_jon.c:1294-1315) */
+static double jon_utsq(const jonctx *c, double W)
+{
+  double SoW = c->QdotB / W;
+  double top = c->Qtsq + (c->Bsq + 2.0 * W) * SoW * SoW;
+  double bottom = (c->Bsq * c->Bsq - c->Qtsq) + 2.0 * c->Bsq * W + W * W - SoW * SoW * (c->Bsq + 2.0 * W);
+  return top / bottom;
+}
+
+/* dvsq_dW (utoprim_jon.c:1378-1398) */
+static double jon_dvsq_dW(const jonctx *c, double W)
+{
+  double X = c->Bsq + W;
+  double Wsq = W * W;
+  double W3 = Wsq * W;
+  double X3 = X * X * X;
+  return (-2. * (c->Qtsq / X3 + c->QdotBsq * (3.0 * W * X + c->Bsq * c->Bsq) / (W3 * X3)));
+}
+
+/* wmrho0_compute_utsq (utoprim_jon_eos.c:474-478) */
+static inline double jon_wmrho0(double Wp, double D, double utsq, double gamma, double gammasq)
+{
+  return ((Wp - D * utsq / (1.0 + gamma)) / gammasq);
+}
+
+/* pressure_Wp_utsq (utoprim_jon_eos.c:134-152) with pressure_wmrho0_grmhd (eos.c:178-181) */
+static double jon_pressure(const jonctx *c, double Wp, double D, double utsq)
+{
+  double gammasq = 1.0 + utsq;
+  double gamma = sqrt(gammasq);
+  double wmrho0 = jon_wmrho0(Wp, D, utsq, gamma, gammasq);
+  return c->igammar * wmrho0;
+}
+
+/* Eprime_Wp (utoprim_jon.c:1529-1554) */
+static double jon_Eprime(const jonctx *c, double Wp)
+{
+  double W = Wp + c->D;
+  double X = c->Bsq + W + SMALL;
+  double X2 = X * X;
+  double utsq = jon_utsq(c, W);
+  double p_tmp;
+  if (utsq < -0.1) utsq = 0.0;
+  p_tmp = jon_pressure(c, Wp, c->D, utsq);
+  return c->Qdotnp + Wp - p_tmp + 0.5 * c->Bsq + 0.5 * (c->Bsq * c->Qtsq - c->QdotBsq) / X2;
+}
+
+/* dEprimedWp (utoprim_jon.c:1558-1587) with dpdWp_calc_utsq / dpdvsq_calc2_Wp
+   (utoprim_jon_eos.c:262-290, 391-426) and the ideal-gas derivatives
+   compute_idwmrho0dp_grmhd = (gam-1)/gam, compute_idrho0dp_grmhd = 0
+   (eos.c:184-194) */
+static double jon_dEprime(const jonctx *c, double Wp)
+{
+  double D = c->D;
+  double W = Wp + D;
+  double X = c->Bsq + W + SMALL;
+  double X3 = X * X * X;
+  double utsq = jon_utsq(c, W);
+  double dvsq, dp1, dp2, dpdWp, gammasq, gamma;
+  if (utsq < -0.1) utsq = 0.0;
+  dvsq = jon_dvsq_dW(c, W);
+  gammasq = 1.0 + utsq;
+  gamma = sqrt(gammasq);
+  dp1 = 0.0 * 0.0 + (1.0 / gammasq) * c->igammar;
+  dp2 = (-D * gamma * 0.5) * 0.0 + (D * (gamma * 0.5 - 1.0) - Wp) * c->igammar;
+  dpdWp = dp1 + dp2 * dvsq;
+  return (1.0 - dpdWp) - (c->Bsq * c->Qtsq - c->QdotBsq) / X3;
+}
+
+/* coldgrhd (utoprim_jon.c:1402-1425) */
+static int jon_coldgrhd(double Qtsq, double D, double *Wp)
+{
+  double det = D * D + Qtsq;
+  if (det < 0.0) return 1;
+  if (D > 0.0) *Wp = Qtsq / (D + sqrt(det));
+  else *Wp = Qtsq / (D - sqrt(det));
+  return 0;
+}
+
+/* validate_Wp (utoprim_jon.c:1726-1758).  The reference leaves Wp unset
+   when coldgrhd finds no root (D^2 + Qtsq < 0, which needs Qtsq < -D^2 < 0);
+   here the step is then left as it is. */
+static void jon_validate(const jonctx *c, double Wpold, double *Wpnew)
+{
+  double Wp;
+  if (*Wpnew < -c->D && c->D > 0.0) {
+    if (!jon_coldgrhd(c->Qtsq, c->D, &Wp)) *Wpnew = Wp * 10.0;
+  }
+  *Wpnew = (fabs(*Wpnew / c->wglobal) > c->gammasq_too_big) ? 0.5 * (Wpold + *Wpnew) : *Wpnew;
+}
+
+/* newt_errorcheck / newt_extracheck (utoprim_jon.c:3430-3458) */
+static int jon_ultrarel(double x0, double wglobal)
+{
+  return (fabs(wglobal) > fabs(GAMMASQCHECKRESID)) || (fabs(x0) > fabs(GAMMASQCHECKRESID));
+}
+static int jon_errorcheck(double errx, double x0, double wglobal)
+{
+  return jon_ultrarel(x0, wglobal) ? (fabs(errx) <= NEWT_TOL_ULTRAREL) : (fabs(errx) <= NEWT_TOL);
+}
+static int jon_extracheck(double x0, double wglobal)
+{
+  return jon_ultrarel(x0, wglobal) ? EXTRA_NEWT_ITER_ULTRAREL : EXTRA_NEWT_ITER;
+}
+
+/* general_newton_raphson (utoprim_jon.c:2896-3424) for n = 1 with func_Eprime
+   (utoprim_jon.c:2258-2281) and no line search: the step is damped by half and
+   restarted from the previous iterate when the residual changed sign against
+   the first one in the ultrarelativistic regime; errx is the relative size of
+   the previous step (the last evaluation only checks), and the returned root is
+   the last evaluated iterate.  The reference's final finite() test also reads
+   x[1] of a one-element array; only x[0] is tested here. */
+static int jon_newton(jonctx *c, double *xio)
+{
+  double x = *xio, x_old = x, x_older = x, dx = 0., dx_old = 1E30 * x;
+  double f = 1., df = 1., errx = 1., resid, drdW;
+  double xold0 = 0., residold = 0., damp = 1.0;
+  int n_iter = 0, keep_iterating = 1, doing_extra = 0, i_extra = 0;
+  while (keep_iterating) {
+    c->iters++;
+    resid = jon_Eprime(c, x);
+    drdW = jon_dEprime(c, x);
+    dx = -resid / drdW;
+    f = 0.5 * resid * resid;
+    df = -2. * f;
+    x_older = x_old;
+    x_old = x;
+    if (n_iter == 0) {
+      xold0 = x;
+      residold = resid;
+    } else if (jon_sign(residold) != jon_sign(resid)) {
+      if (fabs(xold0) > GAMMASQCHECKRESID || fabs(x_old) > GAMMASQCHECKRESID) {
+        damp = 0.5 * damp;
+        x = x_older;
+        dx = dx_old;
+      }
+    }
+    x += damp * dx;
+    errx = (c->wglobal == 0.) ? fabs(dx_old) : fabs(dx_old / jon_max(fabs(c->wglobal), fabs(x)));
+    jon_validate(c, x_old, &x);
+    dx_old = dx;
+    if (jon_errorcheck(errx, x, c->wglobal) && (doing_extra == 0) && (jon_extracheck(x, c->wglobal) > 0))
+      doing_extra = 1;
+    if (doing_extra == 1) i_extra++;
+    if ((jon_errorcheck(errx, x, c->wglobal) && (doing_extra == 0)) || (i_extra > jon_extracheck(x, c->wglobal)) ||
+        (n_iter >= (MAX_NEWT_ITER - 1)))
+      keep_iterating = 0;
+    n_iter++;
+  }
+  if ((isfinite(f) == 0) || (isfinite(df) == 0) || (isfinite(x) == 0)) {
+    *xio = x;
+    return 1;
+  }
+  x = x_old;
+  *xio = x;
+  if (jon_errorcheck(errx, x, c->wglobal)) return 0;
+  if (fabs(errx) <= MIN_NEWT_TOL) return 0;
+  return 1;
+}
+
+/* Utoprim_jon_nonrelcompat_inputnorestmass (utoprim_jon.c:65-205) with
+   Utoprim_new_body (:209-488), compute_setup_quantities (:494-636),
+   set_guess_Wp + verify_Wlast (:640-812), check_Wp (:819-903) and Wp2prim
+   (:949-1165).  U is geometry-free with no rest mass in U[UU]; prim holds
+   the guess on input.  Returns the pflag code.  The reference returns 0 and
+   reports through the flag; the non-B primitives are replaced whenever the
+   Newton solve returned 0, so a flag of UTOPRIMFAILCONVW, a negative density
+   or energy, or a flag of 1 (a root equal to FAIL_VAL) comes with new
+   primitives, while UTOPRIMFAILCONVRET leaves the guess.  When the guess has
+   u~^2 < -MAXNEGUTSQ or u~^2 > UTSQ_TOO_BIG the reference carries on with an
+   unset W' guess (its return value is ignored, utoprim_jon.c:281), and when
+   get_state fails on the guess its bsq_calc leaves b^2 unset; here the zone
+   then keeps its guess with flag UTOPRIMFAILCONVGUESSUTSQ. */
+static int utoprim_jon(const double *U, const geomref *g, const hgo_config *cfg, double *prim, int *iters)
+{
+  double U_tmp[NPR], prim_tmp[NPR], pr0[NPR], alpha;
+  double Bcon[4], Bcov[4], ncov[4], ncon[4], Qcovp[4], Qconp[4], Qcov[4], Qcon[4], Qtcon[4], Qtcov[4];
+  double utsq, gammasq, gamma, rho0, u, p, w, bsq, Wp_last, W_last, Wp, W, wmrho0, Wtest, lapse;
+  int i, j, lpflag, retval, i_increase;
+  jonctx c;
+
+  c.igammar = (cfg->gam - 1.0) / cfg->gam; /* IGAMMAR = GAMMAM1/GAMMA (eos.c:50-54) */
+  c.gammasq_too_big = cfg->gammafail * cfg->gammafail;
+  c.iters = 0;
+  *iters = 0;
+
+  for (i = B1; i <= B3; i++) prim[i] = U[i];
+  alpha = 1.0 / sqrt(-GCON(g, 0, 0));
+  for (i = RHO; i <= B3; i++) U_tmp[i] = alpha * U[i];
+  for (i = 0; i < B1; i++) prim_tmp[i] = prim[i];
+  for (i = B1; i <= B3; i++) prim_tmp[i] = alpha * prim[i];
+
+  lpflag = UTOPRIMNOFAIL;
+  /* compute_setup_quantities */
+  c.D = U_tmp[RHO];
+  for (i = B1; i <= B3; i++) prim_tmp[i] = U_tmp[i];
+  Bcon[0] = 0.;
+  for (i = 1; i < 4; i++) Bcon[i] = U_tmp[B1 + i - 1];
+  for (i = 0; i < 4; i++) {
+    Bcov[i] = 0.;
+    for (j = 0; j < 4; j++) Bcov[i] += GCOV(g, i, j) * Bcon[j];
+  }
+  c.Bsq = 0.;
+  for (i = 1; i < 4; i++) c.Bsq += Bcon[i] * Bcov[i];
+  lapse = sqrt(-1. / GCON(g, 0, 0));
+  ncov[0] = -lapse;
+  ncov[1] = 0.;
+  ncov[2] = 0.;
+  ncov[3] = 0.;
+  for (i = 0; i < 4; i++) {
+    ncon[i] = 0.;
+    for (j = 0; j < 4; j++) ncon[i] += GCON(g, i, j) * ncov[j];
+  }
+  for (i = 0; i < 4; i++) Qcovp[i] = U_tmp[UU + i];
+  for (i = 0; i < 4; i++) {
+    Qconp[i] = 0.;
+    for (j = 0; j < 4; j++) Qconp[i] += GCON(g, i, j) * Qcovp[j];
+  }
+  for (j = 0; j < 4; j++) Qtcon[j] = 0.0;
+  for (j = 1; j < 4; j++)
+    for (i = 1; i < 4; i++) Qtcon[j] += U_tmp[UU + i] * (GCON(g, i, j) + ncon[i] * ncon[j]);
+  for (i = 0; i < 4; i++) {
+    Qtcov[i] = 0.;
+    for (j = 0; j < 4; j++) Qtcov[i] += GCOV(g, i, j) * Qtcon[j];
+  }
+  c.Qtsq = 0.;
+  for (i = 0; i < 4; i++) c.Qtsq += Qtcov[i] * Qtcon[i];
+  for (i = 0; i < 4; i++) Qcov[i] = (i == 0) ? Qcovp[i] - c.D : Qcovp[i];
+  for (i = 0; i < 4; i++) {
+    Qcon[i] = 0.;
+    for (j = 0; j < 4; j++) Qcon[i] += GCON(g, i, j) * Qcov[j];
+  }
+  c.QdotB = 0.;
+  for (i = 1; i < 4; i++) c.QdotB += Qcov[i] * Bcon[i];
+  c.QdotBsq = c.QdotB * c.QdotB;
+  c.Qdotnp = Qconp[0] * ncov[0] + c.D * (1.0 - 1.0 / fabs(ncov[TT]));
+
+  /* set_guess_Wp */
+  utsq = 0.;
+  for (i = 1; i < 4; i++)
+    for (j = 1; j < 4; j++) utsq += GCOV(g, i, j) * prim_tmp[U1 + i - 1] * prim_tmp[U1 + j - 1];
+  if ((utsq < 0.) && (fabs(utsq) < MAXNEGUTSQ)) utsq = 0.0;
+  if (utsq < 0. || utsq > ((cfg->gammafail - 1.0) * (cfg->gammafail - 1.0))) return UTOPRIMFAILCONVGUESSUTSQ;
+  gammasq = 1. + utsq;
+  gamma = sqrt(gammasq);
+  rho0 = c.D / gamma;
+  u = prim_tmp[UU];
+  p = (cfg->gam - 1.) * u; /* pressure_rho0_u_grmhd (eos.c:58-65) */
+  w = rho0 + u + p;
+  {
+    /* bsq_calc (phys.c:755-763) on the guess with B^i -> alpha B^i */
+    zstate q;
+    if (get_state(prim_tmp, g, &q)) return UTOPRIMFAILCONVGUESSUTSQ;
+    bsq = dot4(q.bcon, q.bcov);
+  }
+  Wp_last = c.D * utsq / (1.0 + gamma) + (u + p) * gammasq;
+  W_last = Wp_last + c.D;
+  if ((w + bsq) * gammasq >= GAMMASQCHECKRESID) {
+    double Wpcoldhd;
+    if (jon_coldgrhd(c.Qtsq, c.D, &Wpcoldhd)) Wpcoldhd = Wp_last;
+    c.wglobal = 1E-5 * jon_max(jon_max(Wpcoldhd, Wp_last), w + bsq);
+    Wp_last = jon_max(jon_max(2.0 * Wpcoldhd, Wp_last), w + bsq);
+  } else {
+    c.wglobal = w + bsq;
+  }
+  /* verify_Wlast */
+  if (W_last < -c.D || Wp_last < 0) {
+    W_last = -c.D;
+    Wp_last = 0;
+  }
+  i_increase = 0;
+  while ((W_last * W_last * W_last * (W_last + 2. * c.Bsq) - c.QdotBsq * (2. * W_last + c.Bsq) <=
+          W_last * W_last * (c.Qtsq - c.Bsq * c.Bsq)) &&
+         (i_increase < 10)) {
+    Wp_last *= 10.;
+    W_last = Wp_last + c.D;
+    i_increase++;
+  }
+
+  /* find_root_1D_gen_Eprime (utoprim_jon.c:2704-2726) */
+  Wp = Wp_last;
+  retval = jon_newton(&c, &Wp);
+  *iters = c.iters;
+
+  /* check_Wp */
+  if ((retval != 0) || (Wp == FAIL_VAL)) {
+    lpflag = retval * 100 + 1;
+    if (retval != 0) return lpflag; /* Utoprim_new_body returns, guess kept */
+  } else {
+    Wtest = Wp / c.wglobal;
+    if (Wtest <= 0.0) {
+      /* check_Wp sets its own copy of Wp to SMALL and returns 0 */
+    } else if (Wtest > c.gammasq_too_big) {
+      lpflag = UTOPRIMFAILCONVW;
+    }
+  }
+
+  /* Wp2prim, PRIMFROMVSQ 0 */
+  for (i = B1; i <= B3; i++) prim_tmp[i] = U_tmp[i];
+  for (i = 0; i < NPR; i++) pr0[i] = prim_tmp[i];
+  W = Wp + c.D;
+  utsq = jon_utsq(&c, W);
+  gammasq = 1.0 + utsq;
+  gamma = sqrt(gammasq);
+  wmrho0 = jon_wmrho0(Wp, c.D, utsq, gamma, gammasq);
+  rho0 = c.D / gamma;
+  p = c.igammar * wmrho0; /* pressure_wmrho0_grmhd */
+  u = wmrho0 - p;
+  if ((rho0 <= 0.) || (u < 0.)) {
+    if ((rho0 <= 0.) && (u >= 0.)) lpflag = UTOPRIMFAILRHONEG;
+    if ((rho0 > 0.) && (u < 0.)) lpflag = UTOPRIMFAILUNEG;
+    if ((rho0 <= 0.) && (u < 0.)) lpflag = UTOPRIMFAILRHOUNEG;
+    /* UTOPRIMFAILRETURNTYPE==UTOPRIMRETURNADJUSTED: assign anyway */
+  }
+  prim_tmp[RHO] = rho0;
+  prim_tmp[UU] = u;
+  for (i = 1; i < 4; i++) prim_tmp[U1 + i - 1] = gamma / (W + c.Bsq) * (Qtcon[i] + c.QdotB * Bcon[i] / W);
+  for (i = 0; i < NPR; i++)
+    if (!isfinite(prim_tmp[i])) {
+      prim_tmp[i] = pr0[i];
+      lpflag = UTOPRIMFAILNANRESULT;
+    }
+  for (i = 0; i < B1; i++) prim[i] = prim_tmp[i];
+  return lpflag;
+}
+
 /* Utoprimgen (utoprimgen.c:23-436): geometry-free U, rest mass, inversion.
-   U is the evolved conserved vector (with gdet).  Returns pflag. */
+   U is the evolved conserved vector (with gdet).  Returns pflag.  The 2D
+   inverter wants the rest mass in U[UU] (utoprimgen.c:76-85); the Jon
+   inverter takes U[UU] without it, as evolved with REMOVERESTMASSFROMUU 2. */
 static int utoprimgen(const double *U, const geomref *g, const hgo_config *cfg, double *pr, int *iters)
 {
   double Ugf[NPR];
   int pl;
   for (pl = 0; pl < NPR; pl++) Ugf[pl] = U[pl] / g->g; /* UtoU UEVOLVE->UNOTHING */
-  Ugf[UU] -= Ugf[RHO];                                  /* REMOVERESTMASSFROMUU==2 (utoprimgen.c:76-85) */
+  if (cfg->utoprimversion == HGO_UTOPRIMJONNONRELCOMPAT) return utoprim_jon(Ugf, g, cfg, pr, iters);
+  Ugf[UU] -= Ugf[RHO];
   return utoprim_2d_final(Ugf, g, cfg, pr, iters);
 }
 
@@ -1998,12 +2345,19 @@ int hgo_bound_prim(const hgo_config *c, const hgo_geometry *g, double *p)
 int hgo_utoprim_batch(const double *U, const double *gcov, const double *gcon, const double *gdet, double *pr,
                       int *pflag, long n, double gam, double gammafail, long *iters)
 {
+  return hgo_utoprim_batch_v(U, gcov, gcon, gdet, pr, pflag, n, gam, gammafail, HGO_UTOPRIM2DFINAL, iters);
+}
+
+int hgo_utoprim_batch_v(const double *U, const double *gcov, const double *gcon, const double *gdet, double *pr,
+                        int *pflag, long n, double gam, double gammafail, int utoprimversion, long *iters)
+{
   hgo_config c;
   long z;
   long tot = 0;
   memset(&c, 0, sizeof(c));
   c.gam = gam;
   c.gammafail = gammafail;
+  c.utoprimversion = utoprimversion;
   for (z = 0; z < n; z++) {
     geomref g;
     int it = 0;
@@ -2018,4 +2372,4 @@ int hgo_utoprim_batch(const double *U, const double *gcov, const double *gcon, c
   return 0;
 }
 
-int hgo_abi_version(void) { return 1; }
+int hgo_abi_version(void) { return 2; }

@@ -55,7 +55,12 @@ typedef struct {
   double gam, cour, safe, defcon, tf;
   double rhominlimit, uuminlimit, gammamax, gammafail;
   int timeorder;   /* TIMEORDER: 1 Euler, 2 midpoint, 3 TVD RK3, 4 RK4 (0 = 2) */
+  int utoprimversion; /* UTOPRIMVERSION: HGO_UTOPRIM2DFINAL (0 also) or HGO_UTOPRIMJONNONRELCOMPAT */
 } hgo_config;
+
+/* inverter choices, numbered as global.h:283-287 */
+#define HGO_UTOPRIM2DFINAL 6
+#define HGO_UTOPRIMJONNONRELCOMPAT 8
 
 typedef struct {
   const double *gcov, *gcon, *gcovpert, *gdet, *conn, *floors;
@@ -87,6 +92,11 @@ int hgo_substep(const hgo_config *c, const hgo_geometry *g, const double *pi, co
    pr holds the guess on input and the solution on output. */
 int hgo_utoprim_batch(const double *U, const double *gcov, const double *gcon, const double *gdet, double *pr,
                       int *pflag, long n, double gam, double gammafail, long *iters);
+
+/* The same with the inverter chosen (HGO_UTOPRIM2DFINAL or
+   HGO_UTOPRIMJONNONRELCOMPAT). */
+int hgo_utoprim_batch_v(const double *U, const double *gcov, const double *gcon, const double *gdet, double *pr,
+                        int *pflag, long n, double gam, double gammafail, int utoprimversion, long *iters);
 
 /* Bound the primitives in place (bound_prim). */
 int hgo_bound_prim(const hgo_config *c, const hgo_geometry *g, double *p);

@@ -25,6 +25,7 @@ CENT = 7
 
 LIM = {"DONOR": 0, "VANL": 1, "MINM": 2, "MC": 3, "PARA": 4, "WENO5": 9}
 FLUX = {"LAXF": 0, "HLL": 1}
+UTOPRIM = {"2DFINAL": 6, "JON": 8, "JONNONRELCOMPAT": 8}   # global.h:283-287
 BC_OUTFLOW, BC_POLARAXIS, BC_PERIODIC, BC_OUTFLOW_COPY = 0, 4, 7, 1000
 
 
@@ -45,7 +46,8 @@ class hgo_config(ctypes.Structure):
                 ("dx", ctypes.c_double * 4), ("gam", ctypes.c_double), ("cour", ctypes.c_double),
                 ("safe", ctypes.c_double), ("defcon", ctypes.c_double), ("tf", ctypes.c_double),
                 ("rhominlimit", ctypes.c_double), ("uuminlimit", ctypes.c_double),
-                ("gammamax", ctypes.c_double), ("gammafail", ctypes.c_double), ("timeorder", ctypes.c_int)]
+                ("gammamax", ctypes.c_double), ("gammafail", ctypes.c_double), ("timeorder", ctypes.c_int),
+                ("utoprimversion", ctypes.c_int)]
 
 
 class hgo_geometry(ctypes.Structure):
@@ -70,9 +72,10 @@ class Problem:
     def __init__(self, n1, n2, n3, ng, dx, gam=4.0 / 3.0, cour=0.8, lim="MC", flux="HLL",
                  bc=(BC_OUTFLOW, BC_OUTFLOW, BC_POLARAXIS, BC_POLARAXIS, BC_PERIODIC, BC_PERIODIC),
                  safe=1.3, defcon=1.0, tf=2000.0, rhominlimit=1e-20, uuminlimit=1e-20, gammamax=25.0,
-                 gammafail=2500.0, timeorder=2):
+                 gammafail=2500.0, timeorder=2, utoprim="2DFINAL"):
         self.n = (n1, n2, n3)
         self.timeorder = timeorder
+        self.utoprim = utoprim
         self.ng = ng
         self.g = tuple(ng if n > 1 else 0 for n in self.n)
         self.s = tuple(1 if n > 1 else 0 for n in self.n)
@@ -116,6 +119,7 @@ class Problem:
         c.rhominlimit, c.uuminlimit = self.rhominlimit, self.uuminlimit
         c.gammamax, c.gammafail = self.gammamax, self.gammafail
         c.timeorder = getattr(self, "timeorder", 2)
+        c.utoprimversion = UTOPRIM[getattr(self, "utoprim", "2DFINAL")]
         return c
 
     def copy(self):
@@ -226,6 +230,10 @@ class Oracle:
                                         ctypes.c_long, ctypes.c_double, ctypes.c_double,
                                         ctypes.POINTER(ctypes.c_long)]
         L.hgo_utoprim_batch.restype = ctypes.c_int
+        L.hgo_utoprim_batch_v.argtypes = [ctypes.POINTER(ctypes.c_double)] * 5 + [ctypes.POINTER(ctypes.c_int),
+                                          ctypes.c_long, ctypes.c_double, ctypes.c_double, ctypes.c_int,
+                                          ctypes.POINTER(ctypes.c_long)]
+        L.hgo_utoprim_batch_v.restype = ctypes.c_int
 
     @staticmethod
     def geometry(pr):
@@ -250,7 +258,7 @@ class Oracle:
         pr.t, pr.dt = t.value, dt.value
         return st
 
-    def utoprim(self, U, gcov, gcon, gdet, guess, gam, gammafail):
+    def utoprim(self, U, gcov, gcon, gdet, guess, gam, gammafail, version="2DFINAL"):
         U = np.ascontiguousarray(U, dtype=np.float64)
         gcov = np.ascontiguousarray(gcov, dtype=np.float64)
         gcon = np.ascontiguousarray(gcon, dtype=np.float64)
@@ -259,6 +267,6 @@ class Oracle:
         n = U.shape[0]
         pflag = np.zeros(n, dtype=np.int32)
         it = ctypes.c_long(0)
-        self.lib.hgo_utoprim_batch(_dp(U), _dp(gcov), _dp(gcon), _dp(gdet), _dp(pr), _ip(pflag), n, gam, gammafail,
-                                   ctypes.byref(it))
+        self.lib.hgo_utoprim_batch_v(_dp(U), _dp(gcov), _dp(gcon), _dp(gdet), _dp(pr), _ip(pflag), n, gam, gammafail,
+                                     UTOPRIM[version], ctypes.byref(it))
         return pr, pflag, it.value

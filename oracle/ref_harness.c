@@ -15,6 +15,13 @@
  *          <outdir>/s<step>_* after each listed step (and always after nsteps)
  *   and prints the CLOCK_MONOTONIC start/end of every step to stderr (the
  *   CPU baseline's step-loop timing).  "-" as outdir writes no files.
+ *
+ * usage: harm_ref --invert <infile> <outfile>
+ *   runs the reference's Utoprimgen() (utoprimgen.c:20) zone by zone on
+ *   the records of <infile> (int64 n, then n x 49 doubles: evolved U[8]
+ *   with gdet, gcov[16], gcon[16], gdet, guess primitives[8]) after init(),
+ *   and writes <outfile>: n x 8 doubles (primitives), n int32 FLAGUTOPRIMFAIL
+ *   flags, n int32 Newton iteration counts (nstroke per zone).
  */
 #include "defs.h"  /* defines the reference globals, as the reference main.c does */
 #include <sys/stat.h>
@@ -111,11 +118,72 @@ static void dump_geometry(void)
   wbin("init", "conn", a_conn, sizeof(a_conn));
 }
 
+extern int Utoprimgen(int evolvetype, int inputtype, FTYPE *U, struct of_geom *ptrgeom, FTYPE *pr);
+
+static int invert_file(const char *in, const char *out)
+{
+  FILE *f = fopen(in, "rb");
+  long long n, z;
+  double *rec, *pout;
+  int *fout, *iout;
+  if (!f || fread(&n, sizeof(n), 1, f) != 1 || n < 0) { fprintf(stderr, "harness: bad %s\n", in); return 3; }
+  rec = (double *)malloc(sizeof(double) * 49 * (n > 0 ? n : 1));
+  pout = (double *)malloc(sizeof(double) * 8 * (n > 0 ? n : 1));
+  fout = (int *)malloc(sizeof(int) * (n > 0 ? n : 1));
+  iout = (int *)malloc(sizeof(int) * (n > 0 ? n : 1));
+  if (fread(rec, sizeof(double) * 49, (size_t)n, f) != (size_t)n) { fprintf(stderr, "harness: short %s\n", in); return 3; }
+  fclose(f);
+  for (z = 0; z < n; z++) {
+    const double *r = rec + 49 * z;
+    FTYPE U[NPR], pr[NPR], gcov[NDIM][NDIM], gcon[NDIM][NDIM], gcovpert[NDIM];
+    struct of_geom geom;
+    int a, b, pl;
+    for (pl = 0; pl < NPR; pl++) U[pl] = r[pl];
+    for (a = 0; a < NDIM; a++)
+      for (b = 0; b < NDIM; b++) {
+        gcov[a][b] = r[8 + 4 * a + b];
+        gcon[a][b] = r[24 + 4 * a + b];
+      }
+    for (a = 0; a < NDIM; a++) gcovpert[a] = 0.0;
+    for (pl = 0; pl < NPR; pl++) pr[pl] = r[41 + pl];
+    geom.gcov = gcov;
+    geom.gcon = gcon;
+    geom.gcovpert = gcovpert;
+    geom.g = r[40];
+    for (pl = 0; pl < NPR; pl++) geom.e[pl] = r[40]; /* WHICHEOM == WITHGDET */
+    geom.i = geom.j = geom.k = 0;
+    geom.p = CENT;
+    nstroke = 0;
+    Utoprimgen(EVOLVENOENTROPY, UEVOLVE, U, &geom, pr);
+    for (pl = 0; pl < NPR; pl++) pout[8 * z + pl] = pr[pl];
+    fout[z] = pflag[0][0][0][FLAGUTOPRIMFAIL];
+    iout[z] = nstroke;
+  }
+  f = fopen(out, "wb");
+  if (!f) { fprintf(stderr, "harness: cannot write %s\n", out); return 3; }
+  fwrite(pout, sizeof(double) * 8, (size_t)n, f);
+  fwrite(fout, sizeof(int), (size_t)n, f);
+  fwrite(iout, sizeof(int), (size_t)n, f);
+  fclose(f);
+  free(rec); free(pout); free(fout); free(iout);
+  return 0;
+}
+
 int main(int argc, char *argv[])
 {
   char *fakeargv[2];
   int nsteps, s, d, ndump = 0, nodump = 0;
   int dumps[64];
+
+  if (argc == 4 && strcmp(argv[1], "--invert") == 0) {
+    fakeargv[0] = argv[0];
+    fakeargv[1] = NULL;
+    if (init(1, fakeargv) >= 1) {
+      fprintf(stderr, "harness: init failed\n");
+      return 1;
+    }
+    return invert_file(argv[2], argv[3]);
+  }
 
   if (argc < 3) {
     fprintf(stderr, "usage: %s <outdir|-> <nsteps> [dumpstep ...]\n", argv[0]);

@@ -8,7 +8,8 @@ from oracle.pyoracle import Problem
 GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
 CASES = ["torus2d_16x16_mc_hll", "torus3d_12x12x6_mc_laxf", "torus2d_16x16_weno5_hll", "torus3d_12x12x6_weno5_laxf",
          "torus2d_16x16_para_hll", "torus3d_12x12x6_para_laxf", "torus2d_16x16_mc_hll_rk4",
-         "torus2d_16x16_mc_hll_rk1", "torus3d_12x12x6_weno5_laxf_rk3"]
+         "torus2d_16x16_mc_hll_rk1", "torus3d_12x12x6_weno5_laxf_rk3", "torus2d_16x16_mc_hll_jon",
+         "torus2d_16x16_para_hll_rk4_jon", "torus3d_12x12x6_weno5_laxf_jon"]
 
 
 def load(name):
@@ -19,7 +20,8 @@ def load(name):
                  safe=float(d["safe"]), defcon=float(d["defcon"]), tf=float(d["tf"]),
                  rhominlimit=float(d["rhominlimit"]), uuminlimit=float(d["uuminlimit"]),
                  gammamax=float(d["gammamax"]), gammafail=float(d["gammafail"]),
-                 timeorder=int(d["timeorder"]) if "timeorder" in d else 2)
+                 timeorder=int(d["timeorder"]) if "timeorder" in d else 2,
+                 utoprim=str(d["utoprim"]) if "utoprim" in d else "2DFINAL")
     for k in ("gcov", "gcon", "gcovpert", "gdet", "conn", "floors"):
         getattr(pr, k)[...] = d[k]
     pr.p[...] = d["p_init"]
@@ -37,3 +39,13 @@ def same(a, b):
     a = np.asarray(a)
     b = np.asarray(b)
     return a.shape == b.shape and bool(np.all((a == b) | (np.isnan(a) & np.isnan(b))))
+
+
+def load_zones():
+    """Zone-level inversion fixture (tests/golden/utoprim_zones.npz): inputs
+    and the reference's Utoprimgen outputs for both inverters."""
+    d = np.load(os.path.join(GOLDEN, "utoprim_zones.npz"))
+    z = {k: d[k] for k in d.files}
+    z["gam"] = float(d["gam"])
+    z["gammafail"] = float(d["gammafail"])
+    return z

@@ -29,7 +29,7 @@ from oracle.pyoracle import RefDump  # noqa: E402
 # reference's MAXBND=11 line lengths) 6 per side
 NG = {"MC": 3, "PARA": 3, "WENO5": 6}
 
-# name: (n1, n2, n3, lim, flux, cour, nsteps, dump steps[, TIMEORDER])
+# name: (n1, n2, n3, lim, flux, cour, nsteps, dump steps[, TIMEORDER[, inverter]])
 CASES = {
     "torus2d_16x16_mc_hll": (16, 16, 1, "MC", "HLL", 0.8, 5, [1, 5]),
     "torus3d_12x12x6_mc_laxf": (12, 12, 6, "MC", "LAXF", 0.8, 10, [1, 10]),
@@ -40,14 +40,18 @@ CASES = {
     "torus2d_16x16_mc_hll_rk4": (16, 16, 1, "MC", "HLL", 0.8, 5, [1, 5], 4),
     "torus2d_16x16_mc_hll_rk1": (16, 16, 1, "MC", "HLL", 0.8, 5, [1, 5], 1),
     "torus3d_12x12x6_weno5_laxf_rk3": (12, 12, 6, "WENO5", "LAXF", 0.8, 3, [1, 3], 3),
+    "torus2d_16x16_mc_hll_jon": (16, 16, 1, "MC", "HLL", 0.8, 5, [1, 5], 2, "JON"),
+    "torus2d_16x16_para_hll_rk4_jon": (16, 16, 1, "PARA", "HLL", 0.8, 5, [1, 5], 4, "JON"),
+    "torus3d_12x12x6_weno5_laxf_jon": (12, 12, 6, "WENO5", "LAXF", 0.8, 3, [1, 3], 2, "JON"),
 }
 
 
 def make(name, spec, ref):
     n1, n2, n3, lim, flux, cour, nsteps, dumps = spec[:8]
     timeorder = spec[8] if len(spec) > 8 else 2
+    utoprim = spec[9] if len(spec) > 9 else "2DFINAL"
     ng = NG[lim]
-    exe = build_ref.build(ref, n1, n2, n3, lim, flux, cour, 11, timeorder=timeorder)
+    exe = build_ref.build(ref, n1, n2, n3, lim, flux, cour, 11, timeorder=timeorder, utoprim=utoprim)
     with tempfile.TemporaryDirectory() as tmp:
         out = os.path.join(tmp, "out")
         subprocess.run([exe, out, str(nsteps)] + [str(s) for s in dumps], cwd=tmp, check=True,
@@ -59,7 +63,7 @@ def make(name, spec, ref):
                     tf=pr.tf, rhominlimit=pr.rhominlimit, uuminlimit=pr.uuminlimit, gammamax=pr.gammamax,
                     gammafail=pr.gammafail, gcov=pr.gcov, gcon=pr.gcon, gcovpert=pr.gcovpert, gdet=pr.gdet,
                     conn=pr.conn, floors=pr.floors, p_init=pr.p, pflag_init=pr.pflag, t_init=pr.t, dt_init=pr.dt,
-                    steps=np.array(dumps), timeorder=np.array(timeorder))
+                    steps=np.array(dumps), timeorder=np.array(timeorder), utoprim=np.array(utoprim))
         for s in dumps:
             m = rd.meta_of(f"s{s}")
             data[f"p_s{s}"] = rd.crop(rd.p(f"s{s}"), ng)
@@ -72,13 +76,103 @@ def make(name, spec, ref):
     print(f"wrote {path} ({os.path.getsize(path) / 1e6:.2f} MB)")
 
 
+CENT = 7
+
+
+def zone_inputs(nz=4096, seed=11):
+    """Seeded zone-level inversion inputs on the MKS torus metric of the 16x16
+    fixture: random primitives (rho log-uniform over 7 decades, u/rho over 6,
+    Lorentz factors up to 2000, b^2/rho up to 1e3), their evolved conserved
+    vector U (REMOVERESTMASSFROMUU 2: U[UU] = gdet (T^t_t + rho u^t)), a
+    perturbed guess, and for a quarter of the zones an energy perturbed
+    towards no physical solution."""
+    g = np.load(os.path.join(HERE, "torus2d_16x16_mc_hll.npz"))
+    gam = float(g["gam"])
+    gcov_all = g["gcov"][:, :, CENT].reshape(-1, 4, 4)
+    gcon_all = g["gcon"][:, :, CENT].reshape(-1, 4, 4)
+    gdet_all = g["gdet"][:, :, CENT].reshape(-1)
+    ok = np.abs(gdet_all) > 1e-8
+    gcov_all, gcon_all, gdet_all = gcov_all[ok], gcon_all[ok], gdet_all[ok]
+    rng = np.random.default_rng(seed)
+    pick = rng.integers(0, len(gdet_all), nz)
+    gcov, gcon, gdet = gcov_all[pick], gcon_all[pick], gdet_all[pick]
+    rho = 10.0 ** rng.uniform(-6, 1, nz)
+    uu = rho * 10.0 ** rng.uniform(-4, 2, nz)
+    lor = 10.0 ** (rng.uniform(0, 1, nz) ** 2 * np.log10(2000.0))
+    v = rng.normal(size=(nz, 3))
+    norm = np.einsum("zi,zij,zj->z", v, gcov[:, 1:, 1:], v)
+    ut = v * np.sqrt((lor * lor - 1.0) / norm)[:, None]
+    alpha = 1.0 / np.sqrt(-gcon[:, 0, 0])
+    ucon = np.zeros((nz, 4))
+    ucon[:, 0] = lor / alpha
+    ucon[:, 1:] = ut - ucon[:, :1] * gcon[:, 0, 1:] * (alpha * alpha)[:, None]
+    ucov = np.einsum("zij,zj->zi", gcov, ucon)
+    Bv = rng.normal(size=(nz, 3))
+    bt = np.einsum("zi,zi->z", Bv, ucov[:, 1:])
+    bcon = np.zeros((nz, 4))
+    bcon[:, 0] = bt
+    bcon[:, 1:] = (Bv + bt[:, None] * ucon[:, 1:]) / ucon[:, :1]
+    bsq = np.einsum("zi,zij,zj->z", bcon, gcov, bcon)
+    scale = np.sqrt(rho * 10.0 ** rng.uniform(-4, 3, nz) / bsq)
+    Bv *= scale[:, None]
+    bcon *= scale[:, None]
+    bsq *= scale * scale
+    bcov = np.einsum("zij,zj->zi", gcov, bcon)
+    p = (gam - 1.0) * uu
+    w = rho + uu + p
+    Tt = (w + bsq)[:, None] * ucon[:, :1] * ucov - bcon[:, :1] * bcov
+    Tt[:, 0] += p + 0.5 * bsq
+    U = np.zeros((nz, 8))
+    U[:, 0] = rho * ucon[:, 0]
+    U[:, 1] = Tt[:, 0] + U[:, 0]
+    U[:, 2:5] = Tt[:, 1:]
+    U[:, 5:8] = Bv
+    U *= gdet[:, None]
+    bad = rng.random(nz) < 0.25
+    U[bad, 1] *= 1.0 + rng.choice([-1.0, 1.0], bad.sum()) * 10.0 ** rng.uniform(-4, -0.3, bad.sum())
+    prim = np.concatenate([rho[:, None], uu[:, None], ut, Bv], axis=1)
+    guess = prim.copy()
+    guess[:, 0:2] *= np.exp(rng.normal(scale=0.2, size=(nz, 2)))
+    guess[:, 2:5] *= np.exp(rng.normal(scale=0.1, size=(nz, 1)))
+    return dict(U=U, gcov=gcov, gcon=gcon, gdet=gdet, guess=guess, gam=gam, gammafail=float(g["gammafail"]),
+                prim_true=prim)
+
+
+def make_zones(ref):
+    """Reference Utoprimgen outputs, both inverters, on zone_inputs()."""
+    z = zone_inputs()
+    n = len(z["gdet"])
+    rec = np.concatenate([z["U"], z["gcov"].reshape(n, 16), z["gcon"].reshape(n, 16), z["gdet"][:, None],
+                          z["guess"]], axis=1)
+    data = dict(z)
+    for inv in ("2DFINAL", "JON"):
+        exe = build_ref.build(ref, 16, 16, 1, "MC", "HLL", 0.8, 11, utoprim=inv)
+        with tempfile.TemporaryDirectory() as tmp:
+            fin, fout = os.path.join(tmp, "in.bin"), os.path.join(tmp, "out.bin")
+            with open(fin, "wb") as f:
+                f.write(np.int64(n).tobytes())
+                f.write(np.ascontiguousarray(rec).tobytes())
+            subprocess.run([exe, "--invert", fin, fout], cwd=tmp, check=True, stdout=subprocess.DEVNULL,
+                           stderr=subprocess.DEVNULL)
+            raw = open(fout, "rb").read()
+        data[f"pr_{inv}"] = np.frombuffer(raw[:n * 64], dtype=np.float64).reshape(n, 8).copy()
+        data[f"pflag_{inv}"] = np.frombuffer(raw[n * 64:n * 68], dtype=np.int32).copy()
+        data[f"iters_{inv}"] = np.frombuffer(raw[n * 68:n * 72], dtype=np.int32).copy()
+    path = os.path.join(HERE, "utoprim_zones.npz")
+    np.savez_compressed(path, **data)
+    print(f"wrote {path} ({os.path.getsize(path) / 1e6:.2f} MB)")
+
+
 def main():
     ref = os.environ.get("HARM_REFERENCE_DIR", "/root/reference")
     if not os.path.isdir(ref):
         raise SystemExit(f"reference tree not found: {ref}")
-    names = sys.argv[1:] or list(CASES)
+    names = sys.argv[1:] or list(CASES) + ["utoprim_zones"]
     for name in names:
-        make(name, CASES[name], ref)
+        if name == "utoprim_zones":
+            make_zones(ref)
+        else:
+            make(name, CASES[name], ref)
 
 
 if __name__ == "__main__":

@@ -93,3 +93,16 @@ def test_utoprim_batch_matches_oracle():
     assert np.array_equal(fa, fb)
     assert same(a, b)
     assert ia == ib
+
+
+@pytest.mark.parametrize("inv", ["2DFINAL", "JON"])
+def test_utoprim_zones_match_reference(inv):
+    # zone-level fixture: the reference's Utoprimgen on seeded zones with
+    # Lorentz factors up to 2000, b^2/rho up to 1e3 and perturbed energies
+    from tests.fixtures import load_zones
+    z = load_zones()
+    pr, pf, it = utoprim_batch(z["U"], z["gcov"], z["gcon"], z["gdet"], z["guess"], z["gam"], z["gammafail"],
+                               version=inv)
+    assert np.array_equal(pf, z[f"pflag_{inv}"])
+    assert same(pr, z[f"pr_{inv}"])
+    assert it == int(z[f"iters_{inv}"].sum())

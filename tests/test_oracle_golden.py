@@ -47,3 +47,19 @@ def test_divb_roundoff_in_reference_and_oracle(orc, name):
         assert divb_max(ref[s]["p"], pr.gdet, pr.ng, pr.dx, pr.n) < 1e-12
     orc.step(pr, 10)
     assert divb_max(pr.p, pr.gdet, pr.ng, pr.dx, pr.n) < 1e-12
+
+
+@pytest.mark.parametrize("inv", ["2DFINAL", "JON"])
+def test_oracle_utoprim_zones_match_reference(orc, inv):
+    # the reference's Utoprimgen run zone by zone through the harness
+    # (oracle/ref_harness.c --invert) on seeded zones, both inverters
+    from tests.fixtures import load_zones
+    z = load_zones()
+    pr, pf, it = orc.utoprim(z["U"], z["gcov"], z["gcon"], z["gdet"], z["guess"], z["gam"], z["gammafail"],
+                             version=inv)
+    assert np.array_equal(pf, z[f"pflag_{inv}"])
+    assert same(pr, z[f"pr_{inv}"])
+    assert it == int(z[f"iters_{inv}"].sum())
+    # the fixture covers converged, failed-Newton and negative-energy zones
+    flags = set(np.unique(pf).tolist())
+    assert {0, 101, 10} <= flags
