@@ -24,7 +24,9 @@ file init.fishmon.c / init.fishmon.h / bounds.fishmon.c with
   (init.fishmon.c:73 has 9), UTOPRIMVERSION=UTOPRIM2DFINAL unless the Jon
   inverter (UTOPRIMJONNONRELCOMPAT, init.fishmon.c:46) is asked for,
   lim/fluxmethod/cour as requested, TIMEORDER (2 unless asked),
-  DOENOFLUX=NOENOFLUX, rescaletype=0 (r^-1.5 / r^-2.5 floors), N1/N2/N3.
+  DOENOFLUX=NOENOFLUX unless the problem file's own ENOFINITEVOLUME
+  (init.fishmon.c:112, with its avgscheme=DONOR) is asked for,
+  rescaletype=0 (r^-1.5 / r^-2.5 floors), N1/N2/N3.
 
 usage: python oracle/build_ref.py --n1 64 --n2 64 --n3 1 --lim MC --flux HLL
 """
@@ -165,13 +167,14 @@ def overlay_init_h(text, n1, n2, n3, maxbnd):
 UTOPRIMS = {"2DFINAL": "UTOPRIM2DFINAL", "JON": "UTOPRIMJONNONRELCOMPAT"}
 
 
-def overlay_init_c(text, lim, flux, cour, timeorder=2, utoprim="2DFINAL"):
+def overlay_init_c(text, lim, flux, cour, timeorder=2, utoprim="2DFINAL", fv=False):
     w = "init.fishmon.c"
     text = sub_once(text, "  defcoord = 9;", "  defcoord = LOGRSINTH;", where=w)
     text = sub_once(text, "  UTOPRIMVERSION = UTOPRIMJONNONRELCOMPAT;", f"  UTOPRIMVERSION = {UTOPRIMS[utoprim]};", where=w)
     text = sub_once(text, "  lim = PARA;", f"  lim = {LIMS[lim]};", where=w)
     text = sub_once(text, "  TIMEORDER=4;", f"  TIMEORDER={int(timeorder)};", where=w)
-    text = sub_once(text, "  DOENOFLUX = ENOFINITEVOLUME;", "  DOENOFLUX = NOENOFLUX;", count=2, where=w)
+    if not fv:
+        text = sub_once(text, "  DOENOFLUX = ENOFINITEVOLUME;", "  DOENOFLUX = NOENOFLUX;", count=2, where=w)
     text = sub_once(text, "  fluxmethod=HLLFLUX;", f"  fluxmethod={FLUXES[flux]};", where=w)
     text = sub_once(text, "  rescaletype=1;", "  rescaletype=0;", where=w)
     text = sub_once(text, "  cour=0.8;", f"  cour={cour!r};", where=w)
@@ -190,10 +193,10 @@ int bound_prim_user_after_mpi(int boundstage, FTYPE prim[][N2M][N3M][NPR])
 
 
 def build(ref, n1, n2, n3, lim, flux, cour, maxbnd, name=None, keep=False, verbose=False, timeorder=2,
-          utoprim="2DFINAL"):
+          utoprim="2DFINAL", fv=False):
     os.makedirs(OUT, exist_ok=True)
     name = name or (f"harm_ref_{n1}x{n2}x{n3}_{lim}_{flux}" + (f"_rk{timeorder}" if timeorder != 2 else "")
-                    + ("_jon" if utoprim == "JON" else ""))
+                    + ("_jon" if utoprim == "JON" else "") + ("_fv" if fv else ""))
     scratch = tempfile.mkdtemp(prefix="harmref_")
     try:
         for fn in os.listdir(ref):
@@ -228,7 +231,7 @@ def build(ref, n1, n2, n3, lim, flux, cour, maxbnd, name=None, keep=False, verbo
         with open(os.path.join(scratch, "init.h"), "w") as f:
             f.write(ih)
         with open(os.path.join(ref, "init.fishmon.c")) as f:
-            ic = overlay_init_c(f.read(), lim, flux, cour, timeorder, utoprim)
+            ic = overlay_init_c(f.read(), lim, flux, cour, timeorder, utoprim, fv)
         with open(os.path.join(scratch, "init.c"), "w") as f:
             f.write(ic)
         with open(os.path.join(ref, "bounds.fishmon.c")) as f:
@@ -266,11 +269,12 @@ def main():
     ap.add_argument("--keep", action="store_true")
     ap.add_argument("--timeorder", type=int, default=2, choices=[1, 2, 3, 4])
     ap.add_argument("--utoprim", default="2DFINAL", choices=sorted(UTOPRIMS))
+    ap.add_argument("--fv", action="store_true", help="DOENOFLUX = ENOFINITEVOLUME (the problem file's own)")
     a = ap.parse_args()
     if not os.path.isdir(a.ref):
         raise SystemExit(f"reference tree not found: {a.ref}")
     build(a.ref, a.n1, a.n2, a.n3, a.lim, a.flux, a.cour, a.maxbnd, a.name, a.keep, verbose=True,
-          timeorder=a.timeorder, utoprim=a.utoprim)
+          timeorder=a.timeorder, utoprim=a.utoprim, fv=a.fv)
 
 
 if __name__ == "__main__":

@@ -924,13 +924,25 @@ static void fluxcalc_dir(dom *d, const double *pr, int dir, double *F, double *d
   *ndt = BIG;
   if (d->n[dir] == 1) return;
 
-  /* interp_loop_set (initbase.c:1010-1058), NOENOFLUX */
-  is = (dir == 1) ? 0 : -d->sh[1];
-  ie = (dir == 1) ? n1 - 1 + d->sh[1] : n1 - 1 + d->sh[1];
-  js = (dir == 2) ? 0 : -d->sh[2];
-  je = (dir == 2) ? n2 - 1 + d->sh[2] : n2 - 1 + d->sh[2];
-  ks = (dir == 3) ? 0 : -d->sh[3];
-  ke = (dir == 3) ? n3 - 1 + d->sh[3] : n3 - 1 + d->sh[3];
+  if (c->doenoflux == HGO_ENOFINITEVOLUME) {
+    /* interp_loop_set (initbase.c:952-994), ENOFINITEVOLUME with avgo = 0:
+       the faces along dir, every transverse zone including all ghosts
+       (INFULL..OUTFULL); the dt minimum runs over all of them */
+    is = (dir == 1) ? 0 : -d->ng[1];
+    ie = (dir == 1) ? n1 : n1 - 1 + d->ng[1];
+    js = (dir == 2) ? 0 : -d->ng[2];
+    je = (dir == 2) ? n2 : n2 - 1 + d->ng[2];
+    ks = (dir == 3) ? 0 : -d->ng[3];
+    ke = (dir == 3) ? n3 : n3 - 1 + d->ng[3];
+  } else {
+    /* interp_loop_set (initbase.c:1010-1058), NOENOFLUX */
+    is = (dir == 1) ? 0 : -d->sh[1];
+    ie = (dir == 1) ? n1 - 1 + d->sh[1] : n1 - 1 + d->sh[1];
+    js = (dir == 2) ? 0 : -d->sh[2];
+    je = (dir == 2) ? n2 - 1 + d->sh[2] : n2 - 1 + d->sh[2];
+    ks = (dir == 3) ? 0 : -d->sh[3];
+    ke = (dir == 3) ? n3 - 1 + d->sh[3] : n3 - 1 + d->sh[3];
+  }
 
   if (c->lim == HGO_LIM_WENO5) {
     weno5_faces(d, pr, dir, is, ie, js, je, ks, ke, dq, dq + dom_ntot(d) * NPR);
@@ -1755,17 +1767,63 @@ static int limit_gamma(double gammamax, double *pr, const geomref *g, int *err)
   return 0;
 }
 
-/* fixup1zone (fixup.c:341-447) with floors precomputed per zone */
-static void fixup1zone(double *pr, const geomref *g, const double *floor2, const hgo_config *c, int *err)
+/* fixup1zone (fixup.c:341-447) with floors precomputed per zone; returns
+   whether it changed the primitives (didchangeprim), 0 when limit_gamma
+   failed (the reference returns through FAILSTATEMENT before diag_fixup) */
+static int fixup1zone(double *pr, const geomref *g, const double *floor2, const hgo_config *c, int *err)
 {
   double prfloor[2];
+  int changed = 0, r;
   prfloor[RHO] = floor2[0];
   prfloor[UU] = floor2[1];
   if (prfloor[RHO] < c->rhominlimit) prfloor[RHO] = c->rhominlimit;
   if (prfloor[UU] < c->uuminlimit) prfloor[UU] = c->uuminlimit;
-  if (prfloor[RHO] > pr[RHO]) pr[RHO] = prfloor[RHO];
-  if (prfloor[UU] > pr[UU]) pr[UU] = prfloor[UU];
-  limit_gamma(c->gammamax, pr, g, err);
+  if (prfloor[RHO] > pr[RHO]) {
+    pr[RHO] = prfloor[RHO];
+    changed = 1;
+  }
+  if (prfloor[UU] > pr[UU]) {
+    pr[UU] = prfloor[UU];
+    changed = 1;
+  }
+  r = limit_gamma(c->gammamax, pr, g, err);
+  if (r >= 1) return 0;
+  if (r == -1) changed = 1;
+  return changed;
+}
+
+/* diag_fixup's correction of the evolved conserved state for
+   ENOFINITEVOLUME with DOENOFLUXMEMORY (fixup.c:196-252), on the final
+   substep: unew += UtoU(UDIAG->UEVOLVE, U(pr)) - UtoU(UDIAG->UEVOLVE, U(pr0))
+   with U = primtoU(UDIAG) (phys.c:225, UtoU phys.c:243-285: divide by gdet,
+   multiply by e = gdet).  It runs once per energy region (ENERREGIONLOOP,
+   NUMENERREGIONS = 3 with DOJETDIAG, global.h:435-439): the correctable
+   region (Uconsloop = the active zones for avgo = 0) holds in each, so an
+   active zone gets the difference added three times. */
+static void fv_diag_fixup(dom *d, const double *pr0, const double *pr, const geomref *g, double *unew)
+{
+  zstate q;
+  emstate e;
+  double Ui[NPR], Uf[NPR], Upre[NPR], Upost[NPR];
+  int pl, region;
+  if (get_state(pr0, g, &q)) {
+    d->err |= ERR_UTCALC_DISCR;
+    return;
+  }
+  em_prepare(pr0, g, &q, &e);
+  primtoflux(pr0, &q, &e, TT, g, d->c->gam, Ui);
+  if (get_state(pr, g, &q)) {
+    d->err |= ERR_UTCALC_DISCR;
+    return;
+  }
+  em_prepare(pr, g, &q, &e);
+  primtoflux(pr, &q, &e, TT, g, d->c->gam, Uf);
+  for (pl = 0; pl < NPR; pl++) {
+    Upre[pl] = (Ui[pl] / g->g) * g->g;
+    Upost[pl] = (Uf[pl] / g->g) * g->g;
+  }
+  for (region = 0; region < 3; region++)
+    for (pl = 0; pl < NPR; pl++) unew[pl] += Upost[pl] - Upre[pl];
 }
 
 /* inflow_check_rel4vel for dir 1 at a CENT ghost zone (fixup.c:2271-2400) */
@@ -1979,7 +2037,7 @@ static void fixup_checksolution(dom *d, const double *pv, int *pf, double *gamma
 /* fixup_utoprim (fixup.c:669-1470), GENERALAVERAGE=1, ORDERINDEPENDENT=1,
    HOWTOAVG_WHEN_U2AVG=MAXUPOSAVG, CAUSALAVG=0, TODONOGOOD=NOGOODAVERAGE,
    STEPOVERNEG*=-1, DOCOUNTNEG*=1, ADJUSTCONSERVEDQUANTITY=0 */
-static void fixup_utoprim(dom *d, double *pv, double *ptoavg, int *pf, int finalstep)
+static void fixup_utoprim(dom *d, double *pv, double *ptoavg, int *pf, int finalstep, double *unew)
 {
   int n1 = d->n[1], n2 = d->n[2], n3 = d->n[3];
   int s1 = d->sh[1], s2 = d->sh[2], s3 = d->sh[3];
@@ -2070,7 +2128,15 @@ static void fixup_utoprim(dom *d, double *pv, double *ptoavg, int *pf, int final
                  mypflag == UTOPRIMFAILU2AVG2 || mypflag == UTOPRIMFAILRHOUNEG)
           failtype = finalstep ? 1 : -1;
         else failtype = 1;
-        if (failtype != -1) pf[z] = UTOPRIMFAILFIXED;
+        if (failtype != -1) {
+          /* diag_fixup(pr0 = ptoavg, pv) (fixup.c:1428); pr0 is the zone's
+             pre-fixup state */
+          if (unew && finalstep) {
+            get_geometry(d, i, j, CENT, &g);
+            fv_diag_fixup(d, &ptoavg[z * NPR], &pv[z * NPR], &g, &unew[z * NPR]);
+          }
+          pf[z] = UTOPRIMFAILFIXED;
+        }
       }
 }
 
@@ -2169,7 +2235,7 @@ typedef struct {
 /* advance_standard (advance.c:58-238) for the midpoint RK2 stage `timeorder` */
 static void advance(dom *d, const double *pi, const double *pb, double *pf, double *uf, double *ucum, double *F1,
                     double *F2, double *F3, int *pflag, double dt, int timeorder, int numtimeorders, double *ndt,
-                    scratch *sc, long *iters)
+                    scratch *sc, long *iters, const double *ui)
 {
   const hgo_config *c = d->c;
   double ndt1, ndt2, ndt3;
@@ -2197,9 +2263,15 @@ static void advance(dom *d, const double *pi, const double *pb, double *pf, doub
         if (timeorder == 0)
           for (pl = 0; pl < NPR; pl++) uf[z * NPR + pl] = ucum[z * NPR + pl] = 0.0;
         get_geometry(d, i, j, CENT, &g);
-        if (get_state(&pi[z * NPR], &g, &q)) d->err |= ERR_UTCALC_DISCR;
-        em_prepare(&pi[z * NPR], &g, &q, &e);
-        primtoflux(&pi[z * NPR], &q, &e, TT, &g, c->gam, Ui);
+        if (ui) {
+          /* advance_finitevolume (advance.c:245-501): Ui is the stored
+             conserved state (ui = ucum of the last step, advance.c:330-343) */
+          for (pl = 0; pl < NPR; pl++) Ui[pl] = ui[z * NPR + pl];
+        } else {
+          if (get_state(&pi[z * NPR], &g, &q)) d->err |= ERR_UTCALC_DISCR;
+          em_prepare(&pi[z * NPR], &g, &q, &e);
+          primtoflux(&pi[z * NPR], &q, &e, TT, &g, c->gam, Ui);
+        }
         if ((r = source_conn(d, i, j, &pb[z * NPR], &g, dUgeom))) d->err |= r;
         /* flux2dUavg (advance.c:741-914) */
         for (pl = 0; pl < NPR; pl++) {
@@ -2221,7 +2293,12 @@ static void advance(dom *d, const double *pi, const double *pb, double *pf, doub
         if (finalstep) pflag[z] = utoprimgen(&ucum[z * NPR], &g, c, &pf[z * NPR], &it);
         else pflag[z] = utoprimgen(Uf, &g, c, &pf[z * NPR], &it);
         *iters += it;
-        if (finalstep) fixup1zone(&pf[z * NPR], &g, &d->floors[gidx(d, i, j) * 2], c, &d->err);
+        if (finalstep) {
+          double pr0[NPR];
+          for (pl = 0; pl < NPR; pl++) pr0[pl] = pf[z * NPR + pl];
+          if (fixup1zone(&pf[z * NPR], &g, &d->floors[gidx(d, i, j) * 2], c, &d->err) && ui)
+            fv_diag_fixup(d, pr0, &pf[z * NPR], &g, &ucum[z * NPR]); /* diag_fixup, fixup.c:443 */
+        }
       }
   *ndt = c->defcon * 1. / (1. / ndt1 + 1. / ndt2 + 1. / ndt3);
 }
@@ -2247,15 +2324,15 @@ static void free_scratch(scratch *sc)
 /* one RK stage with its boundary/fixup sequence (step_ch.c:94-186) */
 static void stage_with_fixups(dom *d, const double *pi, const double *pb, double *pf, double *uf, double *ucum,
                               double *F1, double *F2, double *F3, int *pflag, double dt, int timeorder,
-                              int numtimeorders, double *ndt, scratch *sc, long *iters)
+                              int numtimeorders, double *ndt, scratch *sc, long *iters, const double *ui)
 {
   int finalstep = (timeorder == numtimeorders - 1);
   /* pre_fixup: b^2 flags only (LIMADJUST=FLUXADJUST=0), no state change */
-  advance(d, pi, pb, pf, uf, ucum, F1, F2, F3, pflag, dt, timeorder, numtimeorders, ndt, sc, iters);
+  advance(d, pi, pb, pf, uf, ucum, F1, F2, F3, pflag, dt, timeorder, numtimeorders, ndt, sc, iters, ui);
   bound_prim(d, pf);
   bound_pflag(d, pflag);
   fixup_checksolution(d, pf, pflag, sc->gammacheck);
-  fixup_utoprim(d, pf, sc->ptoavg, pflag, finalstep);
+  fixup_utoprim(d, pf, sc->ptoavg, pflag, finalstep, ui ? ucum : NULL);
   bound_prim(d, pf);
 }
 
@@ -2269,7 +2346,7 @@ int hgo_substep(const hgo_config *c, const hgo_geometry *g, const double *pi, co
   dom_init(&d, c, g);
   if (alloc_scratch(&d, &sc)) return -1;
   stage_with_fixups(&d, pi, pb, pf, uf, ucum, F1, F2, F3, pflag, dt, timeorder, c->timeorder ? c->timeorder : 2,
-                    ndt, &sc, &iters);
+                    ndt, &sc, &iters, NULL);
   free_scratch(&sc);
   if (st) {
     st->newton_iters = iters;
@@ -2278,25 +2355,73 @@ int hgo_substep(const hgo_config *c, const hgo_geometry *g, const double *pi, co
   return d.err;
 }
 
+/* pi2Uavg (initbase.c:1833-1880), avgscheme=DONOR: U(p) over FULLLOOP */
+static void pi2u(dom *d, const double *p, double *u)
+{
+  int i, j, k;
+  for (i = -d->ng[1]; i < d->n[1] + d->ng[1]; i++)
+    for (j = -d->ng[2]; j < d->n[2] + d->ng[2]; j++)
+      for (k = -d->ng[3]; k < d->n[3] + d->ng[3]; k++) {
+        long z = zidx(d, i, j, k);
+        geomref g;
+        zstate q;
+        emstate e;
+        get_geometry(d, i, j, CENT, &g);
+        if (get_state(&p[z * NPR], &g, &q)) {
+          d->err |= ERR_UTCALC_DISCR;
+          continue;
+        }
+        em_prepare(&p[z * NPR], &g, &q, &e);
+        primtoflux(&p[z * NPR], &q, &e, TT, &g, d->c->gam, &u[z * NPR]);
+      }
+}
+
+int hgo_pi2u(const hgo_config *c, const hgo_geometry *g, const double *p, double *u)
+{
+  dom d;
+  dom_init(&d, c, g);
+  pi2u(&d, p, u);
+  return d.err;
+}
+
 int hgo_step(const hgo_config *c, const hgo_geometry *g, double *p, int *pflag, double *t, double *dt, int nsteps,
              hgo_stats *st)
+{
+  return hgo_step_u(c, g, p, pflag, NULL, t, dt, nsteps, st);
+}
+
+int hgo_step_u(const hgo_config *c, const hgo_geometry *g, double *p, int *pflag, double *u, double *t, double *dt,
+               int nsteps, hgo_stats *st)
 {
   dom d;
   scratch sc;
   long n, iters = 0;
-  double *pk, *pk1, *uf, *ucum, *F1, *F2, *F3;
+  double *pk, *pk1, *uf, *ucum, *F1, *F2, *F3, *ui = NULL, *uown = NULL;
   int s, z, nf = 0, norders = c->timeorder ? c->timeorder : 2, o;
+  int fv = (c->doenoflux == HGO_ENOFINITEVOLUME);
   dom_init(&d, c, g);
   n = dom_ntot(&d);
   if (alloc_scratch(&d, &sc)) return -1;
   pk = (double *)calloc((size_t)n * NPR, sizeof(double));
   pk1 = (double *)calloc((size_t)n * NPR, sizeof(double));
   uf = (double *)calloc((size_t)n * NPR, sizeof(double));
-  ucum = (double *)calloc((size_t)n * NPR, sizeof(double));
   F1 = (double *)calloc((size_t)n * NPR, sizeof(double));
   F2 = (double *)calloc((size_t)n * NPR, sizeof(double));
   F3 = (double *)calloc((size_t)n * NPR, sizeof(double));
-  if (!pk || !pk1 || !uf || !ucum || !F1 || !F2 || !F3) return -1;
+  if (fv) {
+    /* unew is the evolved state; ui receives it at the start of each step
+       (advance.c:330-343; at the first call uinitial = unew = U(p) from
+       init_conservatives, initbase.c:146-153) */
+    ui = (double *)calloc((size_t)n * NPR, sizeof(double));
+    if (!u) {
+      u = uown = (double *)calloc((size_t)n * NPR, sizeof(double));
+      if (uown) pi2u(&d, p, u);
+    }
+    ucum = u;
+  } else {
+    ucum = (double *)calloc((size_t)n * NPR, sizeof(double));
+  }
+  if (!pk || !pk1 || !uf || !ucum || !F1 || !F2 || !F3 || (fv && !ui)) return -1;
   for (s = 0; s < nsteps; s++) {
     double ndt;
     /* pii/pbb/pff of setup_rktimestep (step_ch.c:442-562): pi = p always;
@@ -2309,8 +2434,9 @@ int hgo_step(const hgo_config *c, const hgo_geometry *g, double *p, int *pflag, 
     double **pbs = norders == 4 ? pb4 : norders == 3 ? pb3 : norders == 2 ? pb2 : pb1;
     double **pfs = norders == 4 ? pf4 : norders == 3 ? pf3 : norders == 2 ? pf2 : pf1;
     memcpy(pk, p, sizeof(double) * NPR * n);
+    if (fv) memcpy(ui, ucum, sizeof(double) * NPR * n);
     for (o = 0; o < norders; o++)
-      stage_with_fixups(&d, p, pbs[o], pfs[o], uf, ucum, F1, F2, F3, pflag, *dt, o, norders, &ndt, &sc, &iters);
+      stage_with_fixups(&d, p, pbs[o], pfs[o], uf, ucum, F1, F2, F3, pflag, *dt, o, norders, &ndt, &sc, &iters, ui);
     /* step_ch.c:236-247 */
     *t += *dt;
     if (ndt > c->safe * (*dt)) ndt = c->safe * (*dt);
@@ -2321,7 +2447,9 @@ int hgo_step(const hgo_config *c, const hgo_geometry *g, double *p, int *pflag, 
   free(pk);
   free(pk1);
   free(uf);
-  free(ucum);
+  if (!fv) free(ucum);
+  free(ui);
+  free(uown);
   free(F1);
   free(F2);
   free(F3);
@@ -2372,4 +2500,4 @@ int hgo_utoprim_batch_v(const double *U, const double *gcov, const double *gcon,
   return 0;
 }
 
-int hgo_abi_version(void) { return 2; }
+int hgo_abi_version(void) { return 3; }

@@ -56,7 +56,13 @@ typedef struct {
   double rhominlimit, uuminlimit, gammamax, gammafail;
   int timeorder;   /* TIMEORDER: 1 Euler, 2 midpoint, 3 TVD RK3, 4 RK4 (0 = 2) */
   int utoprimversion; /* UTOPRIMVERSION: HGO_UTOPRIM2DFINAL (0 also) or HGO_UTOPRIMJONNONRELCOMPAT */
+  int doenoflux;      /* DOENOFLUX: HGO_NOENOFLUX (advance_standard) or HGO_ENOFINITEVOLUME
+                         (advance_finitevolume with avgscheme=DONOR, the FM torus setting) */
 } hgo_config;
+
+/* DOENOFLUX choices (global.h:188-191) */
+#define HGO_NOENOFLUX 0
+#define HGO_ENOFINITEVOLUME 3
 
 /* inverter choices, numbered as global.h:283-287 */
 #define HGO_UTOPRIM2DFINAL 6
@@ -77,6 +83,17 @@ typedef struct {
    error bitmask. */
 int hgo_step(const hgo_config *c, const hgo_geometry *g, double *p, int *pflag, double *t, double *dt, int nsteps,
              hgo_stats *st);
+
+/* hgo_step with the evolved conserved state u (the reference's unew, same
+   layout as p).  With DOENOFLUX = ENOFINITEVOLUME the scheme evolves u
+   itself (each step starts from ui = unew) and u is read and written; NULL
+   starts from U(p) as after init.  Ignored (may be NULL) otherwise. */
+int hgo_step_u(const hgo_config *c, const hgo_geometry *g, double *p, int *pflag, double *u, double *t, double *dt,
+               int nsteps, hgo_stats *st);
+
+/* pi2Uavg (initbase.c:1833) with avgscheme=DONOR: u = U(p) in every zone,
+   ghosts included. */
+int hgo_pi2u(const hgo_config *c, const hgo_geometry *g, const double *p, double *u);
 
 /* One substep of advance_standard() + bound_prim + post_fixup + bound_prim
    for RK stage `timeorder` of the midpoint method (for debugging/parity of

@@ -26,6 +26,7 @@ CENT = 7
 LIM = {"DONOR": 0, "VANL": 1, "MINM": 2, "MC": 3, "PARA": 4, "WENO5": 9}
 FLUX = {"LAXF": 0, "HLL": 1}
 UTOPRIM = {"2DFINAL": 6, "JON": 8, "JONNONRELCOMPAT": 8}   # global.h:283-287
+DOENOFLUX = {"NOENOFLUX": 0, "ENOFINITEVOLUME": 3}           # global.h:188-191
 BC_OUTFLOW, BC_POLARAXIS, BC_PERIODIC, BC_OUTFLOW_COPY = 0, 4, 7, 1000
 
 
@@ -47,7 +48,7 @@ class hgo_config(ctypes.Structure):
                 ("safe", ctypes.c_double), ("defcon", ctypes.c_double), ("tf", ctypes.c_double),
                 ("rhominlimit", ctypes.c_double), ("uuminlimit", ctypes.c_double),
                 ("gammamax", ctypes.c_double), ("gammafail", ctypes.c_double), ("timeorder", ctypes.c_int),
-                ("utoprimversion", ctypes.c_int)]
+                ("utoprimversion", ctypes.c_int), ("doenoflux", ctypes.c_int)]
 
 
 class hgo_geometry(ctypes.Structure):
@@ -72,10 +73,12 @@ class Problem:
     def __init__(self, n1, n2, n3, ng, dx, gam=4.0 / 3.0, cour=0.8, lim="MC", flux="HLL",
                  bc=(BC_OUTFLOW, BC_OUTFLOW, BC_POLARAXIS, BC_POLARAXIS, BC_PERIODIC, BC_PERIODIC),
                  safe=1.3, defcon=1.0, tf=2000.0, rhominlimit=1e-20, uuminlimit=1e-20, gammamax=25.0,
-                 gammafail=2500.0, timeorder=2, utoprim="2DFINAL"):
+                 gammafail=2500.0, timeorder=2, utoprim="2DFINAL", doenoflux="NOENOFLUX"):
         self.n = (n1, n2, n3)
         self.timeorder = timeorder
         self.utoprim = utoprim
+        self.doenoflux = doenoflux
+        self.u = None   # evolved conserved state (unew) of the finite-volume scheme
         self.ng = ng
         self.g = tuple(ng if n > 1 else 0 for n in self.n)
         self.s = tuple(1 if n > 1 else 0 for n in self.n)
@@ -120,6 +123,7 @@ class Problem:
         c.gammamax, c.gammafail = self.gammamax, self.gammafail
         c.timeorder = getattr(self, "timeorder", 2)
         c.utoprimversion = UTOPRIM[getattr(self, "utoprim", "2DFINAL")]
+        c.doenoflux = DOENOFLUX[getattr(self, "doenoflux", "NOENOFLUX")]
         return c
 
     def copy(self):
@@ -127,6 +131,8 @@ class Problem:
         q = copy.copy(self)
         q.p = self.p.copy()
         q.pflag = self.pflag.copy()
+        if getattr(self, "u", None) is not None:
+            q.u = self.u.copy()
         return q
 
 
@@ -169,6 +175,9 @@ class RefDump:
     def flux(self, tag, d):
         return self._f(tag, f"F{d}").reshape(self.NM + (NPR,))
 
+    def unew(self, tag):
+        return self._f(tag, "unew").reshape(self.NM + (NPR,))
+
     def pk(self, tag):
         return self._f(tag, "pk").reshape((2,) + self.NM + (NPR,))
 
@@ -189,10 +198,12 @@ class RefDump:
         lim = {v: k for k, v in LIM.items()}[m["lim"]]
         flux = {v: k for k, v in FLUX.items()}[m["fluxmethod"]]
         bc = tuple(m[f"BCtype{i}"] for i in range(6))
+        utoprim = {v: k for k, v in UTOPRIM.items() if k != "JONNONRELCOMPAT"}[m["UTOPRIMVERSION"]]
+        doenoflux = {v: k for k, v in DOENOFLUX.items()}[m["DOENOFLUX"]]
         pr = Problem(self.N[0], self.N[1], self.N[2], ng, (m["dx1"], m["dx2"], m["dx3"]), gam=m["gam"],
                      cour=m["cour"], lim=lim, flux=flux, bc=bc, safe=m["SAFE"], defcon=m["defcon"], tf=m["tf"],
                      rhominlimit=m["RHOMINLIMIT"], uuminlimit=m["UUMINLIMIT"], gammamax=m["GAMMAMAX"],
-                     gammafail=m["GAMMAFAIL"])
+                     gammafail=m["GAMMAFAIL"], timeorder=int(m["TIMEORDER"]), utoprim=utoprim, doenoflux=doenoflux)
         off = tuple(b - g for b, g in zip(self.bnd, pr.g))
         sl = tuple(slice(o, o + nt) for o, nt in zip(off, pr.nt))
         gsl = tuple(slice(o, o + gt) for o, gt in zip(off[:2], pr.gt))
@@ -206,6 +217,8 @@ class RefDump:
         pr.floors[:nconn.shape[0], :nconn.shape[1]] = fl[sl[0], sl[1], k0]
         pr.p[...] = self.p(tag)[sl]
         pr.pflag[...] = self.pflag(tag)[sl][..., 0]
+        if doenoflux == "ENOFINITEVOLUME":
+            pr.u = np.ascontiguousarray(self.unew(tag)[sl])
         mm = self.meta_of(tag)
         pr.t, pr.dt = mm["t"], mm["dt"]
         return pr
@@ -226,6 +239,14 @@ class Oracle:
                                ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double), ctypes.c_int,
                                ctypes.POINTER(hgo_stats)]
         L.hgo_step.restype = ctypes.c_int
+        L.hgo_step_u.argtypes = [ctypes.POINTER(hgo_config), ctypes.POINTER(hgo_geometry),
+                                 ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_int),
+                                 ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double),
+                                 ctypes.POINTER(ctypes.c_double), ctypes.c_int, ctypes.POINTER(hgo_stats)]
+        L.hgo_step_u.restype = ctypes.c_int
+        L.hgo_pi2u.argtypes = [ctypes.POINTER(hgo_config), ctypes.POINTER(hgo_geometry),
+                               ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double)]
+        L.hgo_pi2u.restype = ctypes.c_int
         L.hgo_utoprim_batch.argtypes = [ctypes.POINTER(ctypes.c_double)] * 5 + [ctypes.POINTER(ctypes.c_int),
                                         ctypes.c_long, ctypes.c_double, ctypes.c_double,
                                         ctypes.POINTER(ctypes.c_long)]
@@ -253,10 +274,22 @@ class Oracle:
         t = ctypes.c_double(pr.t)
         dt = ctypes.c_double(pr.dt)
         assert pr.p.flags.c_contiguous and pr.pflag.flags.c_contiguous
-        self.lib.hgo_step(ctypes.byref(c), ctypes.byref(g), _dp(pr.p), _ip(pr.pflag), ctypes.byref(t),
-                          ctypes.byref(dt), nsteps, ctypes.byref(st))
+        if c.doenoflux == DOENOFLUX["ENOFINITEVOLUME"]:
+            if getattr(pr, "u", None) is None:
+                pr.u = self.pi2u(pr)
+            self.lib.hgo_step_u(ctypes.byref(c), ctypes.byref(g), _dp(pr.p), _ip(pr.pflag), _dp(pr.u),
+                                ctypes.byref(t), ctypes.byref(dt), nsteps, ctypes.byref(st))
+        else:
+            self.lib.hgo_step(ctypes.byref(c), ctypes.byref(g), _dp(pr.p), _ip(pr.pflag), ctypes.byref(t),
+                              ctypes.byref(dt), nsteps, ctypes.byref(st))
         pr.t, pr.dt = t.value, dt.value
         return st
+
+    def pi2u(self, pr):
+        """pi2Uavg: the conserved state U(p) in every zone (init_conservatives)."""
+        u = np.zeros_like(pr.p)
+        self.lib.hgo_pi2u(ctypes.byref(pr.config()), ctypes.byref(self.geometry(pr)), _dp(pr.p), _dp(u))
+        return u
 
     def utoprim(self, U, gcov, gcon, gdet, guess, gam, gammafail, version="2DFINAL"):
         U = np.ascontiguousarray(U, dtype=np.float64)

@@ -80,6 +80,7 @@ static void dump_state(const char *tag, int with_fluxes)
   write_meta(tag);
   wbin(tag, "p", a_p, sizeof(a_p));
   wbin(tag, "pflag", a_pflag, sizeof(a_pflag));
+  if (!with_fluxes) wbin(tag, "unew", a_unew, sizeof(a_unew)); /* the conserved state after init */
   if (with_fluxes) {
     wbin(tag, "pk", a_pk, sizeof(a_pk));
     wbin(tag, "unew", a_unew, sizeof(a_unew));

@@ -9,7 +9,8 @@ GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
 CASES = ["torus2d_16x16_mc_hll", "torus3d_12x12x6_mc_laxf", "torus2d_16x16_weno5_hll", "torus3d_12x12x6_weno5_laxf",
          "torus2d_16x16_para_hll", "torus3d_12x12x6_para_laxf", "torus2d_16x16_mc_hll_rk4",
          "torus2d_16x16_mc_hll_rk1", "torus3d_12x12x6_weno5_laxf_rk3", "torus2d_16x16_mc_hll_jon",
-         "torus2d_16x16_para_hll_rk4_jon", "torus3d_12x12x6_weno5_laxf_jon"]
+         "torus2d_16x16_para_hll_rk4_jon", "torus3d_12x12x6_weno5_laxf_jon", "torus2d_16x16_para_hll_rk4_jon_fv",
+         "torus2d_16x16_mc_hll_fv", "torus3d_12x12x6_para_laxf_rk4_jon_fv"]
 
 
 def load(name):
@@ -21,16 +22,19 @@ def load(name):
                  rhominlimit=float(d["rhominlimit"]), uuminlimit=float(d["uuminlimit"]),
                  gammamax=float(d["gammamax"]), gammafail=float(d["gammafail"]),
                  timeorder=int(d["timeorder"]) if "timeorder" in d else 2,
-                 utoprim=str(d["utoprim"]) if "utoprim" in d else "2DFINAL")
+                 utoprim=str(d["utoprim"]) if "utoprim" in d else "2DFINAL",
+                 doenoflux=str(d["doenoflux"]) if "doenoflux" in d else "NOENOFLUX")
     for k in ("gcov", "gcon", "gcovpert", "gdet", "conn", "floors"):
         getattr(pr, k)[...] = d[k]
     pr.p[...] = d["p_init"]
     pr.pflag[...] = d["pflag_init"]
+    if "u_init" in d:
+        pr.u = np.ascontiguousarray(d["u_init"])
     pr.t = float(d["t_init"])
     pr.dt = float(d["dt_init"])
     steps = [int(s) for s in d["steps"]]
     ref = {s: dict(p=d[f"p_s{s}"], pflag=d[f"pflag_s{s}"], t=float(d[f"t_s{s}"]), dt=float(d[f"dt_s{s}"]),
-                   nstroke=float(d[f"nstroke_s{s}"])) for s in steps}
+                   nstroke=float(d[f"nstroke_s{s}"]), u=d[f"u_s{s}"] if f"u_s{s}" in d else None) for s in steps}
     return pr, ref
 
 

@@ -26,10 +26,12 @@ from oracle import build_ref  # noqa: E402
 from oracle.pyoracle import RefDump  # noqa: E402
 
 # ghost zones kept in the fixture: MC reads 2, PARA 3, WENO5 (with the
-# reference's MAXBND=11 line lengths) 6 per side
+# reference's MAXBND=11 line lengths) 6 per side.  The finite-volume cases
+# keep all MAXBND ghosts: their fluxes and dt minimum run over every
+# transverse ghost zone.
 NG = {"MC": 3, "PARA": 3, "WENO5": 6}
 
-# name: (n1, n2, n3, lim, flux, cour, nsteps, dump steps[, TIMEORDER[, inverter]])
+# name: (n1, n2, n3, lim, flux, cour, nsteps, dump steps[, TIMEORDER[, inverter[, finite volume, MAXBND]]])
 CASES = {
     "torus2d_16x16_mc_hll": (16, 16, 1, "MC", "HLL", 0.8, 5, [1, 5]),
     "torus3d_12x12x6_mc_laxf": (12, 12, 6, "MC", "LAXF", 0.8, 10, [1, 10]),
@@ -43,6 +45,11 @@ CASES = {
     "torus2d_16x16_mc_hll_jon": (16, 16, 1, "MC", "HLL", 0.8, 5, [1, 5], 2, "JON"),
     "torus2d_16x16_para_hll_rk4_jon": (16, 16, 1, "PARA", "HLL", 0.8, 5, [1, 5], 4, "JON"),
     "torus3d_12x12x6_weno5_laxf_jon": (12, 12, 6, "WENO5", "LAXF", 0.8, 3, [1, 3], 2, "JON"),
+    # the FM torus problem file's own scheme: PARA, HLL, RK4, Jon inverter,
+    # ENOFINITEVOLUME with avgscheme=DONOR, MAXBND 11
+    "torus2d_16x16_para_hll_rk4_jon_fv": (16, 16, 1, "PARA", "HLL", 0.8, 10, [1, 10], 4, "JON", True, 11),
+    "torus2d_16x16_mc_hll_fv": (16, 16, 1, "MC", "HLL", 0.8, 5, [1, 5], 2, "2DFINAL", True, 11),
+    "torus3d_12x12x6_para_laxf_rk4_jon_fv": (12, 12, 6, "PARA", "LAXF", 0.8, 3, [1, 3], 4, "JON", True, 3),
 }
 
 
@@ -50,8 +57,10 @@ def make(name, spec, ref):
     n1, n2, n3, lim, flux, cour, nsteps, dumps = spec[:8]
     timeorder = spec[8] if len(spec) > 8 else 2
     utoprim = spec[9] if len(spec) > 9 else "2DFINAL"
-    ng = NG[lim]
-    exe = build_ref.build(ref, n1, n2, n3, lim, flux, cour, 11, timeorder=timeorder, utoprim=utoprim)
+    fv = spec[10] if len(spec) > 10 else False
+    maxbnd = spec[11] if len(spec) > 11 else 11
+    ng = maxbnd if fv else NG[lim]
+    exe = build_ref.build(ref, n1, n2, n3, lim, flux, cour, maxbnd, timeorder=timeorder, utoprim=utoprim, fv=fv)
     with tempfile.TemporaryDirectory() as tmp:
         out = os.path.join(tmp, "out")
         subprocess.run([exe, out, str(nsteps)] + [str(s) for s in dumps], cwd=tmp, check=True,
@@ -63,7 +72,10 @@ def make(name, spec, ref):
                     tf=pr.tf, rhominlimit=pr.rhominlimit, uuminlimit=pr.uuminlimit, gammamax=pr.gammamax,
                     gammafail=pr.gammafail, gcov=pr.gcov, gcon=pr.gcon, gcovpert=pr.gcovpert, gdet=pr.gdet,
                     conn=pr.conn, floors=pr.floors, p_init=pr.p, pflag_init=pr.pflag, t_init=pr.t, dt_init=pr.dt,
-                    steps=np.array(dumps), timeorder=np.array(timeorder), utoprim=np.array(utoprim))
+                    steps=np.array(dumps), timeorder=np.array(timeorder), utoprim=np.array(utoprim),
+                    doenoflux=np.array("ENOFINITEVOLUME" if fv else "NOENOFLUX"))
+        if fv:
+            data["u_init"] = pr.u
         for s in dumps:
             m = rd.meta_of(f"s{s}")
             data[f"p_s{s}"] = rd.crop(rd.p(f"s{s}"), ng)
@@ -71,6 +83,8 @@ def make(name, spec, ref):
             data[f"t_s{s}"] = m["t"]
             data[f"dt_s{s}"] = m["dt"]
             data[f"nstroke_s{s}"] = m["nstroke"]
+            if fv:
+                data[f"u_s{s}"] = rd.crop(rd.unew(f"s{s}"), ng)
     path = os.path.join(HERE, name + ".npz")
     np.savez_compressed(path, **data)
     print(f"wrote {path} ({os.path.getsize(path) / 1e6:.2f} MB)")

@@ -23,6 +23,10 @@ def test_oracle_matches_reference(orc, name):
         assert same(pr.p, r["p"]), f"primitives differ after step {s}"
         assert np.array_equal(pr.pflag, r["pflag"]), f"pflag map differs after step {s}"
         assert pr.dt == r["dt"] and pr.t == r["t"]
+        if r["u"] is not None:
+            # the finite-volume scheme's evolved conserved state (unew) in the active zones
+            act = pr.active
+            assert same(act(pr.u), act(r["u"])), f"conserved state differs after step {s}"
 
 
 @pytest.mark.parametrize("name", CASES)
@@ -63,3 +67,9 @@ def test_oracle_utoprim_zones_match_reference(orc, inv):
     # the fixture covers converged, failed-Newton and negative-energy zones
     flags = set(np.unique(pf).tolist())
     assert {0, 101, 10} <= flags
+
+
+def test_oracle_pi2u_matches_reference_init():
+    # pi2Uavg (initbase.c:1833): the finite-volume scheme's initial unew
+    pr, _ = load("torus2d_16x16_para_hll_rk4_jon_fv")
+    assert same(Oracle().pi2u(pr), pr.u)
