@@ -160,11 +160,80 @@ __device__ __forceinline__ bool zone_step(const Params &P, const Scalars *sc, lo
   return !sc->done;
 }
 
+// diag_fixup's correction of the evolved conserved state under
+// ENOFINITEVOLUME with DOENOFLUXMEMORY (fixup.c:196-252), final substep only:
+// unew += UtoU(UDIAG->UEVOLVE, U(pr)) - UtoU(UDIAG->UEVOLVE, U(pr0)) where
+// U = primtoU(UDIAG) and UtoU divides by gdet and multiplies by e = gdet
+// (phys.c:243-285).  It runs once per energy region (NUMENERREGIONS = 3
+// with DOJETDIAG, global.h:435-439, every active zone being in the
+// correctable region), so the difference is added three times.
+__device__ __forceinline__ void fv_diag_fixup(const double *pr0, const double *pr, const Metric &m, double gam,
+                                              double *__restrict__ ucum, long long z, long long nz, int *err) {
+  double Ui[NPR], Uf[NPR];
+  {
+    State q;
+    EM e;
+    if (get_state(pr0, m, q)) {
+      *err |= ERR_UTCALC_DISCR;
+      return;
+    }
+    em_prepare(pr0, m, q, e);
+    primtoflux(pr0, q, e, 0, m, gam, Ui);
+  }
+  {
+    State q;
+    EM e;
+    if (get_state(pr, m, q)) {
+      *err |= ERR_UTCALC_DISCR;
+      return;
+    }
+    em_prepare(pr, m, q, e);
+    primtoflux(pr, q, e, 0, m, gam, Uf);
+  }
+#pragma unroll
+  for (int pl = 0; pl < NPR; pl++) {
+    const double upre = (Ui[pl] / m.g) * m.g;
+    const double upost = (Uf[pl] / m.g) * m.g;
+    double u = ucum[pl * nz + z];
+    u += upost - upre;
+    u += upost - upre;
+    u += upost - upre;
+    ucum[pl * nz + z] = u;
+  }
+}
+
+// pi2Uavg (initbase.c:1833-1880) with avgscheme=DONOR: the conserved state
+// U(p) in every zone, ghosts included
+__global__ void pi2u_kernel(Dims d, Params P, const double *__restrict__ p, const double *__restrict__ G,
+                            double *__restrict__ u, Scalars *sc) {
+  long long z = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (z >= d.nz) return;
+  int k = (int)(z % d.nt3) - d.g3;
+  long long r = z / d.nt3;
+  int j = (int)(r % d.nt2) - d.g2;
+  int i = (int)(r / d.nt2) - d.g1;
+  Metric m;
+  load_metric(G, d, gix(d, i, j), G_CENT, m);
+  double pr[NPR], U[NPR];
+  load_prim(p, d, z, pr);
+  State q;
+  EM e;
+  if (get_state(pr, m, q)) {
+    atomicOr(&sc->err, ERR_UTCALC_DISCR);
+    return;
+  }
+  em_prepare(pr, m, q, e);
+  primtoflux(pr, q, e, 0, m, P.gam, U);
+#pragma unroll
+  for (int pl = 0; pl < NPR; pl++) u[pl * d.nz + z] = U[pl];
+}
+
 __global__ void __launch_bounds__(128, HG_MINB_UPDATE) conserve_kernel(
     Dims d, Params P, Box box, const double *pi, const double *pb, double *__restrict__ uf,
     double *__restrict__ ucum, const double *__restrict__ F1, const double *__restrict__ F2,
     const double *__restrict__ F3, const double *__restrict__ E, const double *__restrict__ G, Scalars *sc,
-    double CUf0, double CUf1, double CUf2, double Cunew0, double Cunew1, double Cunew2, int timeorder) {
+    double CUf0, double CUf1, double CUf2, double Cunew0, double Cunew1, double Cunew2, int timeorder,
+    double *__restrict__ ui, int fv) {
   long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= box.size()) return;
   int i, j, k;
@@ -179,7 +248,21 @@ __global__ void __launch_bounds__(128, HG_MINB_UPDATE) conserve_kernel(
     load_metric(G, d, ij, G_CENT, m);
     int err = 0;
     double Ui[NPR], dUg[NPR], dUr[NPR];
-    {
+    if (fv) {
+      // advance_finitevolume (advance.c:245-501): Ui is the stored conserved
+      // state; the first substep takes the last step's ucum as ui
+      // (advance.c:330-343)
+      if (timeorder == 0) {
+#pragma unroll
+        for (int pl = 0; pl < NPR; pl++) {
+          Ui[pl] = ucum[pl * nz + z];
+          ui[pl * nz + z] = Ui[pl];
+        }
+      } else {
+#pragma unroll
+        for (int pl = 0; pl < NPR; pl++) Ui[pl] = ui[pl * nz + z];
+      }
+    } else {
       double pr[NPR];
       load_prim(pi, d, z, pr);
       State q;
@@ -283,7 +366,7 @@ __global__ void __launch_bounds__(128, HG_MINB_INVERT) invert_kernel(Dims d, Par
                                                                      const double *__restrict__ ucum,
                                                                      const double *__restrict__ G,
                                                                      int *__restrict__ pflag, Scalars *sc,
-                                                                     int finalstep) {
+                                                                     int finalstep, double *__restrict__ ufv) {
   long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   unsigned long long my_iters = 0;
   int my_fail = 0;
@@ -318,10 +401,15 @@ __global__ void __launch_bounds__(128, HG_MINB_INVERT) invert_kernel(Dims d, Par
       if (fr < P.rhominlimit) fr = P.rhominlimit;
       if (fu < P.uuminlimit) fu = P.uuminlimit;
       bool floored = (fr > pr[RHO]) || (fu > pr[UU]);
+      double pr0[NPR];
+#pragma unroll
+      for (int v = 0; v < NPR; v++) pr0[v] = pr[v];
       if (fr > pr[RHO]) pr[RHO] = fr;
       if (fu > pr[UU]) pr[UU] = fu;
-      limit_gamma(P.gammamax, pr, m, &err);
+      const int lg = limit_gamma(P.gammamax, pr, m, &err);
       if (floored) atomicAdd(&sc->nfloor, 1);
+      // diag_fixup (fixup.c:443) when fixup1zone changed the primitives
+      if (ufv && lg < 1 && (floored || lg == -1)) fv_diag_fixup(pr0, pr, m, gam, ufv, z, nz, &err);
     }
     store_prim(pf, d, z, pr);
     pflag[z] = flag;
@@ -744,16 +832,36 @@ __global__ void fixup_compute_kernel(Dims d, Params P, const double *__restrict_
   }
 }
 
-__global__ void fixup_scatter_kernel(Dims d, double *pv, int *pflag, const long long *__restrict__ list,
-                                     const double *__restrict__ outv, int cap, int finalstep, Scalars *sc) {
+__global__ void fixup_scatter_kernel(Dims d, Params P, double *pv, int *pflag, const long long *__restrict__ list,
+                                     const double *__restrict__ outv, int cap, int finalstep, Scalars *sc,
+                                     const double *__restrict__ G, double *__restrict__ ufv) {
   int n = sc->nfixlist;
   if (n > cap) n = cap;
   for (int a = blockIdx.x * blockDim.x + threadIdx.x; a < n; a += gridDim.x * blockDim.x) {
     long long z = list[a];
+    double pr0[NPR], pr[NPR];
+    if (ufv && finalstep) load_prim(pv, d, z, pr0);
 #pragma unroll
     for (int v = 0; v < 5; v++) pv[(long long)v * d.nz + z] = outv[(long long)a * 5 + v];
     int f = pflag[z];
     if (becomes_fixed(f, finalstep)) {
+      if (ufv && finalstep) {
+        // diag_fixup(pr0 = ptoavg, pv) (fixup.c:1428), pr0 = the zone before the fixup
+        int k = (int)(z % d.nt3) - d.g3;
+        long long r = z / d.nt3;
+        int j = (int)(r % d.nt2) - d.g2;
+        int i = (int)(r / d.nt2) - d.g1;
+        (void)k;
+        Metric m;
+        load_metric(G, d, gix(d, i, j), G_CENT, m);
+#pragma unroll
+        for (int v = 0; v < 5; v++) pr[v] = outv[(long long)a * 5 + v];
+#pragma unroll
+        for (int v = 5; v < NPR; v++) pr[v] = pr0[v];
+        int err = 0;
+        fv_diag_fixup(pr0, pr, m, P.gam, ufv, z, d.nz, &err);
+        if (err) atomicOr(&sc->err, err);
+      }
       pflag[z] = UTOPRIMFAILFIXED;
       atomicAdd(&sc->nfixed, 1);
     }
@@ -864,6 +972,37 @@ __global__ void soa_to_aos_kernel(const double *__restrict__ s, double *__restri
   a[t] = s[(long long)v * nz + z];
 }
 
+// geometry packing: the reference-layout arrays (per (i,j): gcov and gcon
+// [8 locations][16], gcovpert [8][4], gdet [8], conn [64], floors [2]) into
+// the SoA planes: FACE1/FACE2/FACE3/CENT x {gcov 16, gcon 16, 1+g_tt, gdet},
+// the three corner gdets, conn, floors
+constexpr int GRAW_WORDS = 128 + 128 + 32 + 8 + 64 + 2;
+__global__ void pack_geometry_kernel(const double *__restrict__ raw, long long nij, double *__restrict__ G) {
+  long long ij = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (ij >= nij) return;
+  const double *rcov = raw, *rcon = raw + 128 * nij, *rpert = raw + 256 * nij, *rgdet = raw + 288 * nij,
+               *rconn = raw + 296 * nij, *rfl = raw + 360 * nij;
+  const int locs[4] = {R_FACE1, R_FACE2, R_FACE3, R_CENT};
+#pragma unroll
+  for (int s = 0; s < 4; s++) {
+    const int L = locs[s];
+#pragma unroll
+    for (int q = 0; q < 16; q++) {
+      G[(long long)(s * GLOC + q) * nij + ij] = rcov[(ij * 8 + L) * 16 + q];
+      G[(long long)(s * GLOC + 16 + q) * nij + ij] = rcon[(ij * 8 + L) * 16 + q];
+    }
+    G[(long long)(s * GLOC + 32) * nij + ij] = rpert[(ij * 8 + L) * 4 + 0];
+    G[(long long)(s * GLOC + 33) * nij + ij] = rgdet[ij * 8 + L];
+  }
+  G[(long long)(G_CORN + 0) * nij + ij] = rgdet[ij * 8 + R_CORN1];
+  G[(long long)(G_CORN + 1) * nij + ij] = rgdet[ij * 8 + R_CORN2];
+  G[(long long)(G_CORN + 2) * nij + ij] = rgdet[ij * 8 + R_CORN3];
+#pragma unroll 8
+  for (int q = 0; q < 64; q++) G[(long long)(G_CONN + q) * nij + ij] = rconn[ij * 64 + q];
+  G[(long long)(G_FLOOR + 0) * nij + ij] = rfl[ij * 2 + 0];
+  G[(long long)(G_FLOOR + 1) * nij + ij] = rfl[ij * 2 + 1];
+}
+
 // batched inversion on arbitrary per-zone metrics (hgpu_utoprim_batch,
 // hgpu_utoprimgen_batch)
 template <int UV>
@@ -933,6 +1072,7 @@ struct hgpu_ctx {
   cudaStream_t stream;
   double *p = nullptr, *pk = nullptr, *uf = nullptr, *ucum = nullptr;
   double *pk1 = nullptr;  // second intermediate state of TIMEORDER 3 and 4
+  double *ui = nullptr;   // ENOFINITEVOLUME: the conserved state at the start of the step (uinitial)
   double *F[4] = {nullptr, nullptr, nullptr, nullptr};
   double *E = nullptr;
   double *G = nullptr;
@@ -1035,6 +1175,7 @@ static int validate(const hgpu_config *c) {
   if (c->utoprimversion != 0 && c->utoprimversion != HGPU_UTOPRIM2DFINAL &&
       c->utoprimversion != HGPU_UTOPRIMJONNONRELCOMPAT)
     return HGPU_E_INVALID;
+  if (c->doenoflux != HGPU_NOENOFLUX && c->doenoflux != HGPU_ENOFINITEVOLUME) return HGPU_E_INVALID;
   return HGPU_OK;
 }
 
@@ -1053,11 +1194,54 @@ void hgpu_destroy(hgpu_ctx *x) {
   for (cudaEvent_t e : x->freelist) cudaEventDestroy(e);
   void *ptrs[] = {x->p, x->pk, x->uf, x->ucum, x->F[1], x->F[2], x->F[3], x->E, x->G, x->pflag, x->gammacheck,
                   x->cand, x->fixlist, x->cand_orig, x->cand_dec, x->candmap, x->fixvals, x->sc, x->staging, x->istaging,
-                  x->pL, x->pR, x->WA, x->cell_inst, x->inst, x->progress, x->pk1};
+                  x->pL, x->pR, x->WA, x->cell_inst, x->inst, x->progress, x->pk1, x->ui};
   for (void *q : ptrs)
     if (q) cudaFree(q);
   cudaStreamDestroy(x->stream);
   delete x;
+}
+
+// the scalar parameters every kernel takes by value
+static void fill_params(Params &P, const hgpu_config *cfg) {
+  P.gam = cfg->gam;
+  P.cour = cfg->cour;
+  P.gammamax = cfg->gammamax;
+  P.gammafail = cfg->gammafail;
+  P.rhominlimit = cfg->rhominlimit;
+  P.uuminlimit = cfg->uuminlimit;
+  P.defcon = cfg->defcon;
+  P.safe = cfg->safe;
+  P.tf = cfg->tf;
+  P.dx1 = cfg->dx[1];
+  P.dx2 = cfg->dx[2];
+  P.dx3 = cfg->dx[3];
+  P.lim = cfg->lim;
+  P.flux = cfg->fluxmethod;
+  for (int f = 0; f < 6; f++) P.bc[f] = cfg->bc[f];
+}
+
+// Two configurations with the same allocation shape: the same device
+// buffers serve both (only the by-value parameters differ).
+bool hg_same_shape(const hgpu_config *a, const hgpu_config *b) {
+  return a->n1 == b->n1 && a->n2 == b->n2 && a->n3 == b->n3 && a->ng == b->ng && a->lim == b->lim &&
+         a->fluxmethod == b->fluxmethod && a->precision == b->precision &&
+         (a->timeorder >= 3) == (b->timeorder >= 3) && a->utoprimversion == b->utoprimversion &&
+         a->doenoflux == b->doenoflux;
+}
+
+// Give an idle context a new configuration of the same shape (a pool of
+// contexts reuses device memory across solves): new by-value parameters,
+// and the captured step graph, which holds the old ones, is dropped.
+int hg_reconfigure(hgpu_ctx *x, const hgpu_config *cfg) {
+  if (!x || validate(cfg) || !hg_same_shape(&x->cfg, cfg)) return HGPU_E_INVALID;
+  CUDA_TRY(cudaStreamSynchronize(x->stream));
+  if (x->graph_exec) cudaGraphExecDestroy(x->graph_exec);
+  if (x->graph) cudaGraphDestroy(x->graph);
+  x->graph_exec = nullptr;
+  x->graph = nullptr;
+  x->cfg = *cfg;
+  fill_params(x->P, cfg);
+  return HGPU_OK;
 }
 
 int hgpu_create(const hgpu_config *cfg, hgpu_ctx **out) {
@@ -1088,26 +1272,20 @@ int hgpu_create(const hgpu_config *cfg, hgpu_ctx **out) {
   d.gt2 = d.nt2 + d.s2;
   d.nz = (long long)d.nt1 * d.nt2 * d.nt3;
   d.nij = (long long)d.gt1 * d.gt2;
-  Params &P = x->P;
-  P.gam = cfg->gam;
-  P.cour = cfg->cour;
-  P.gammamax = cfg->gammamax;
-  P.gammafail = cfg->gammafail;
-  P.rhominlimit = cfg->rhominlimit;
-  P.uuminlimit = cfg->uuminlimit;
-  P.defcon = cfg->defcon;
-  P.safe = cfg->safe;
-  P.tf = cfg->tf;
-  P.dx1 = cfg->dx[1];
-  P.dx2 = cfg->dx[2];
-  P.dx3 = cfg->dx[3];
-  P.lim = cfg->lim;
-  P.flux = cfg->fluxmethod;
-  for (int f = 0; f < 6; f++) P.bc[f] = cfg->bc[f];
+  fill_params(x->P, cfg);
   // loop ranges (initbase.c:1010-1058 and fixup.c:477 DQZLOOP)
-  x->face_box[1] = Box{0, -d.s2, -d.s3, d.n1 + 1, d.n2 + 2 * d.s2, d.n3 + 2 * d.s3};
-  x->face_box[2] = Box{-d.s1, 0, -d.s3, d.n1 + 2 * d.s1, d.n2 + 1, d.n3 + 2 * d.s3};
-  x->face_box[3] = Box{-d.s1, -d.s2, 0, d.n1 + 2 * d.s1, d.n2 + 2 * d.s2, d.n3 + 1};
+  if (cfg->doenoflux == HGPU_ENOFINITEVOLUME) {
+    // ENOFINITEVOLUME with avgo = 0 (initbase.c:952-994): faces along the
+    // direction, every transverse zone including all ghosts; the dt minimum
+    // runs over all of them
+    x->face_box[1] = Box{0, -d.g2, -d.g3, d.n1 + 1, d.n2 + 2 * d.g2, d.n3 + 2 * d.g3};
+    x->face_box[2] = Box{-d.g1, 0, -d.g3, d.n1 + 2 * d.g1, d.n2 + 1, d.n3 + 2 * d.g3};
+    x->face_box[3] = Box{-d.g1, -d.g2, 0, d.n1 + 2 * d.g1, d.n2 + 2 * d.g2, d.n3 + 1};
+  } else {
+    x->face_box[1] = Box{0, -d.s2, -d.s3, d.n1 + 1, d.n2 + 2 * d.s2, d.n3 + 2 * d.s3};
+    x->face_box[2] = Box{-d.s1, 0, -d.s3, d.n1 + 2 * d.s1, d.n2 + 1, d.n3 + 2 * d.s3};
+    x->face_box[3] = Box{-d.s1, -d.s2, 0, d.n1 + 2 * d.s1, d.n2 + 2 * d.s2, d.n3 + 1};
+  }
   x->emf_box = Box{0, 0, 0, d.n1 + d.s1, d.n2 + d.s2, d.n3 + d.s3};
   x->active_box = Box{0, 0, 0, d.n1, d.n2, d.n3};
   x->dq_box = Box{-d.s1, -d.s2, -d.s3, d.n1 + 2 * d.s1, d.n2 + 2 * d.s2, d.n3 + 2 * d.s3};
@@ -1145,6 +1323,9 @@ int hgpu_create(const hgpu_config *cfg, hgpu_ctx **out) {
             cudaMalloc(&x->sc, sizeof(Scalars)) == cudaSuccess;
   for (int dd = 1; dd <= 3 && ok; dd++) ok = cudaMalloc(&x->F[dd], pb) == cudaSuccess;
   if (ok && cfg->timeorder >= 3) ok = cudaMalloc(&x->pk1, pb) == cudaSuccess && cudaMemset(x->pk1, 0, pb) == cudaSuccess;
+  if (ok && cfg->doenoflux == HGPU_ENOFINITEVOLUME)
+    ok = cudaMalloc(&x->ui, pb) == cudaSuccess && cudaMemset(x->ui, 0, pb) == cudaSuccess &&
+         cudaMemset(x->ucum, 0, pb) == cudaSuccess;
   if (ok && cfg->lim == HGPU_LIM_WENO5)
     ok = cudaMalloc(&x->pL, pb) == cudaSuccess && cudaMalloc(&x->pR, pb) == cudaSuccess &&
          cudaMalloc(&x->WA, pb * W5_PLANES) == cudaSuccess;
@@ -1181,6 +1362,10 @@ int hgpu_create_batch(const hgpu_config *cfg, int ninst, const int *n1, const do
   }
   if (cfg->bc[0] != HGPU_BC_OUTFLOW_COPY || cfg->bc[1] != HGPU_BC_OUTFLOW_COPY) {
     set_err("a batch needs HGPU_BC_OUTFLOW_COPY at both x1 ends");
+    return HGPU_E_INVALID;
+  }
+  if (cfg->doenoflux != HGPU_NOENOFLUX) {
+    set_err("a batch runs the standard (NOENOFLUX) scheme");
     return HGPU_E_INVALID;
   }
   long long total = 0;
@@ -1261,30 +1446,26 @@ int hgpu_batch_status(hgpu_ctx *x, double *t, double *dt, int *done, int *ndone)
 int hgpu_upload_geometry(hgpu_ctx *x, const double *gcov, const double *gcon, const double *gcovpert,
                          const double *gdet, const double *conn, const double *floors) {
   if (!x || !gcov || !gcon || !gcovpert || !gdet || !conn || !floors) return HGPU_E_INVALID;
-  const Dims &d = x->d;
-  long long nij = d.nij;
-  double *h = (double *)malloc(sizeof(double) * G_NCOMP * nij);
-  if (!h) return HGPU_E_NOMEM;
-  const int locs[4] = {R_FACE1, R_FACE2, R_FACE3, R_CENT};
-  for (long long ij = 0; ij < nij; ij++) {
-    for (int s = 0; s < 4; s++) {
-      int L = locs[s];
-      for (int q = 0; q < 16; q++) {
-        h[(long long)(s * GLOC + q) * nij + ij] = gcov[(ij * 8 + L) * 16 + q];
-        h[(long long)(s * GLOC + 16 + q) * nij + ij] = gcon[(ij * 8 + L) * 16 + q];
-      }
-      h[(long long)(s * GLOC + 32) * nij + ij] = gcovpert[(ij * 8 + L) * 4 + 0];
-      h[(long long)(s * GLOC + 33) * nij + ij] = gdet[ij * 8 + L];
-    }
-    h[(long long)(G_CORN + 0) * nij + ij] = gdet[ij * 8 + R_CORN1];
-    h[(long long)(G_CORN + 1) * nij + ij] = gdet[ij * 8 + R_CORN2];
-    h[(long long)(G_CORN + 2) * nij + ij] = gdet[ij * 8 + R_CORN3];
-    for (int q = 0; q < 64; q++) h[(long long)(G_CONN + q) * nij + ij] = conn[ij * 64 + q];
-    h[(long long)(G_FLOOR + 0) * nij + ij] = floors[ij * 2 + 0];
-    h[(long long)(G_FLOOR + 1) * nij + ij] = floors[ij * 2 + 1];
+  const long long nij = x->d.nij;
+  // the host arrays go up as they are (six large copies); the device packs
+  // them into the SoA planes of the library's layout
+  const long long words = nij * GRAW_WORDS;
+  double *raw = nullptr;
+  CUDA_TRY(cudaMallocAsync(&raw, sizeof(double) * words, x->stream));
+  double *rcov = raw, *rcon = raw + 128 * nij, *rpert = raw + 256 * nij, *rgdet = raw + 288 * nij,
+         *rconn = raw + 296 * nij, *rfl = raw + 360 * nij;
+  cudaError_t e = cudaMemcpyAsync(rcov, gcov, sizeof(double) * 128 * nij, cudaMemcpyHostToDevice, x->stream);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(rcon, gcon, sizeof(double) * 128 * nij, cudaMemcpyHostToDevice, x->stream);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(rpert, gcovpert, sizeof(double) * 32 * nij, cudaMemcpyHostToDevice, x->stream);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(rgdet, gdet, sizeof(double) * 8 * nij, cudaMemcpyHostToDevice, x->stream);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(rconn, conn, sizeof(double) * 64 * nij, cudaMemcpyHostToDevice, x->stream);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(rfl, floors, sizeof(double) * 2 * nij, cudaMemcpyHostToDevice, x->stream);
+  if (e == cudaSuccess) {
+    LAUNCH(x, K_OTHER, pack_geometry_kernel, grid_for(nij, 128), 128, raw, nij, x->G);
+    e = cudaGetLastError();
   }
-  cudaError_t e = cudaMemcpy(x->G, h, sizeof(double) * G_NCOMP * nij, cudaMemcpyHostToDevice);
-  free(h);
+  cudaFreeAsync(raw, x->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(x->stream);
   if (e != cudaSuccess) {
     set_err("geometry upload: %s", cudaGetErrorString(e));
     return HGPU_E_CUDA;
@@ -1310,6 +1491,9 @@ int hgpu_upload_state(hgpu_ctx *x, const double *p, const int *pflag, double t, 
   s.t = t;
   s.dt = dt;
   CUDA_TRY(cudaMemcpyAsync(x->sc, &s, sizeof(Scalars), cudaMemcpyHostToDevice, x->stream));
+  // the finite-volume scheme's conserved state: init_conservatives (pi2Uavg)
+  if (x->cfg.doenoflux == HGPU_ENOFINITEVOLUME)
+    LAUNCH(x, K_OTHER, pi2u_kernel, grid_for(nz, 128), 128, x->d, x->P, x->p, x->G, x->ucum, x->sc);
   CUDA_TRY(cudaStreamSynchronize(x->stream));
   CUDA_TRY(cudaGetLastError());
   return HGPU_OK;
@@ -1453,14 +1637,16 @@ static void launch_stage(hgpu_ctx *x, int timeorder) {
   double Cn0 = S.cun[0], Cn1 = S.cun[1], Cn2 = S.cun[2];
   launch_reset(x);
   launch_fluxes(x, pb);
+  const int fv = (x->cfg.doenoflux == HGPU_ENOFINITEVOLUME);
+  double *ufv = (fv && finalstep) ? x->ucum : nullptr;
   LAUNCH(x, K_UPDATE, conserve_kernel, grid_for(x->active_box.size(), 128), 128, d, x->P, x->active_box, pi, pb, x->uf,
-         x->ucum, x->F[1], x->F[2], x->F[3], x->E, x->G, x->sc, CUf0, CUf1, CUf2, Cn0, Cn1, Cn2, timeorder);
+         x->ucum, x->F[1], x->F[2], x->F[3], x->E, x->G, x->sc, CUf0, CUf1, CUf2, Cn0, Cn1, Cn2, timeorder, x->ui, fv);
   if (x->cfg.utoprimversion == HGPU_UTOPRIMJONNONRELCOMPAT)
     LAUNCH(x, K_INVERT, invert_kernel<8>, grid_for(x->active_box.size(), 128), 128, d, x->P, x->active_box, pb, pf,
-           x->uf, x->ucum, x->G, x->pflag, x->sc, finalstep);
+           x->uf, x->ucum, x->G, x->pflag, x->sc, finalstep, ufv);
   else
     LAUNCH(x, K_INVERT, invert_kernel<6>, grid_for(x->active_box.size(), 128), 128, d, x->P, x->active_box, pb, pf,
-           x->uf, x->ucum, x->G, x->pflag, x->sc, finalstep);
+           x->uf, x->ucum, x->G, x->pflag, x->sc, finalstep, ufv);
   launch_bound(x, pf);
   // post_fixup (fixup.c:37-96)
   if (x->P.cell_inst)
@@ -1478,8 +1664,8 @@ static void launch_stage(hgpu_ctx *x, int timeorder) {
   if (fixgrid > 296) fixgrid = 296;
   LAUNCH(x, K_FIX_COMPUTE, fixup_compute_kernel, fixgrid, 128, d, x->P, pf, x->pflag, x->G, x->fixlist, x->fixvals,
          x->cap, finalstep, x->sc);
-  LAUNCH(x, K_FIX_SCATTER, fixup_scatter_kernel, fixgrid, 128, d, pf, x->pflag, x->fixlist, x->fixvals, x->cap,
-         finalstep, x->sc);
+  LAUNCH(x, K_FIX_SCATTER, fixup_scatter_kernel, fixgrid, 128, d, x->P, pf, x->pflag, x->fixlist, x->fixvals, x->cap,
+         finalstep, x->sc, x->G, ufv);
   launch_bound(x, pf);
 }
 
@@ -2102,6 +2288,8 @@ extern "C" size_t hgpu_context_bytes(const hgpu_config *c) {
              + cap * (2 * sizeof(long long) + 2 * sizeof(int) + 5 * sizeof(double))
              + plane;                         // staging for uploads and downloads
   if (c->lim == HGPU_LIM_WENO5) b += 2 * plane + W5_PLANES * plane;
+  if (c->timeorder >= 3) b += plane;                     // pk1
+  if (c->doenoflux == HGPU_ENOFINITEVOLUME) b += plane;  // ui
   return b;
 }
 
@@ -2135,6 +2323,18 @@ extern "C" int hgpu_diagnostics(hgpu_ctx *x, hgpu_diag *out) {
 // unew of the reference (the conserved state U^{n+1} = the last stage's ucum,
 // with gdet) in the reference's AoS layout, for restart dumps
 // (rdump_content, restart.c:244-250, writes p and unew per zone)
+extern "C" int hgpu_upload_conserved(hgpu_ctx *x, const double *unew) {
+  if (!x || !unew || x->cfg.doenoflux != HGPU_ENOFINITEVOLUME) return HGPU_E_INVALID;
+  long long nz = x->d.nz;
+  int rc = ensure_staging(x);
+  if (rc) return rc;
+  CUDA_TRY(cudaMemcpyAsync(x->staging, unew, sizeof(double) * NPR * nz, cudaMemcpyHostToDevice, x->stream));
+  LAUNCH(x, K_OTHER, aos_to_soa_kernel, grid_for(nz * NPR, 256), 256, x->staging, x->ucum, nz);
+  CUDA_TRY(cudaStreamSynchronize(x->stream));
+  CUDA_TRY(cudaGetLastError());
+  return HGPU_OK;
+}
+
 extern "C" int hgpu_download_conserved(hgpu_ctx *x, double *unew) {
   if (!x || !unew) return HGPU_E_INVALID;
   long long nz = x->d.nz;

@@ -12,9 +12,13 @@
 // (cudaEventQuery on an event recorded after a progress copy), retires a
 // request when its t reached its end time (the step kernels freeze a
 // finished context, so a chunk that overruns the end leaves the state
-// unchanged), downloads its result and frees its memory for the next
-// admission.  A request's result is exactly what running it alone gives:
-// its kernels touch only its own context.
+// unchanged) and downloads its result.  A retired request's context goes
+// to an idle pool: the next admission of the same allocation shape reuses
+// its device memory, pinned progress word and event (no cudaMalloc/cudaFree
+// on the request path; cudaFree would also synchronize the whole device);
+// idle contexts are destroyed only when an admission needs their bytes.  A
+// request's result is exactly what running it alone gives: its kernels
+// touch only its own context.
 #include <cuda_runtime.h>
 #include <stdio.h>
 #include <string.h>
@@ -28,6 +32,10 @@
 
 cudaStream_t hg_stream(hgpu_ctx *x);
 int hg_progress_async(hgpu_ctx *x, double *dst, cudaEvent_t ev);
+extern "C" {
+bool hg_same_shape(const hgpu_config *a, const hgpu_config *b);
+int hg_reconfigure(hgpu_ctx *x, const hgpu_config *cfg);
+}
 
 namespace {
 
@@ -70,20 +78,41 @@ size_t geom_count(const hgpu_config &c) {
 
 }  // namespace
 
+// an idle context kept for reuse, with its progress word and event
+struct Slot {
+  hgpu_ctx *ctx = nullptr;
+  double *prog = nullptr;
+  cudaEvent_t ev = nullptr;
+  hgpu_config cfg;
+  size_t bytes = 0;
+};
+
 struct hgpu_server {
-  size_t max_bytes = 0, used = 0;
+  size_t max_bytes = 0, used = 0, idle_bytes = 0;
   int max_active = 0, chunk = 1, active = 0;
   long long next_id = 1;
   std::map<long long, Request *> reqs;  // ordered by id = arrival order
+  std::vector<Slot> idle;
   std::mutex m;
 };
 
+static void destroy_slot(Slot &q) {
+  if (q.ctx) hgpu_destroy(q.ctx);
+  if (q.ev) cudaEventDestroy(q.ev);
+  if (q.prog) cudaFreeHost(q.prog);
+  q.ctx = nullptr;
+  q.ev = nullptr;
+  q.prog = nullptr;
+}
+
 static void release_device(hgpu_server *s, Request *r) {
-  if (r->ctx) hgpu_destroy(r->ctx);
+  Slot q;
+  q.ctx = r->ctx;
+  q.prog = r->prog;
+  q.ev = r->ev;
+  destroy_slot(q);
   r->ctx = nullptr;
-  if (r->ev) cudaEventDestroy(r->ev);
   r->ev = nullptr;
-  if (r->prog) cudaFreeHost(r->prog);
   r->prog = nullptr;
   if (r->state == ACTIVE) {
     s->used -= r->bytes;
@@ -91,14 +120,54 @@ static void release_device(hgpu_server *s, Request *r) {
   }
 }
 
+// a finished request hands its context to the idle pool
+static void park(hgpu_server *s, Request *r) {
+  Slot q;
+  q.ctx = r->ctx;
+  q.prog = r->prog;
+  q.ev = r->ev;
+  q.cfg = r->cfg;
+  q.bytes = r->bytes;
+  r->ctx = nullptr;
+  r->prog = nullptr;
+  r->ev = nullptr;
+  s->used -= r->bytes;
+  s->active--;
+  s->idle.push_back(q);
+  s->idle_bytes += q.bytes;
+}
+
 static int admit(hgpu_server *s, Request *r) {
-  int rc = hgpu_create(&r->cfg, &r->ctx);
+  int rc = HGPU_OK;
+  // reuse an idle context of the same shape, else make room and create one
+  size_t pick = s->idle.size();
+  for (size_t q = 0; q < s->idle.size(); q++)
+    if (hg_same_shape(&s->idle[q].cfg, &r->cfg)) {
+      pick = q;
+      break;
+    }
+  if (pick < s->idle.size()) {
+    Slot q = s->idle[pick];
+    s->idle.erase(s->idle.begin() + (long)pick);
+    s->idle_bytes -= q.bytes;
+    r->ctx = q.ctx;
+    r->prog = q.prog;
+    r->ev = q.ev;
+    rc = hg_reconfigure(r->ctx, &r->cfg);
+  } else {
+    while (!s->idle.empty() && s->used + s->idle_bytes + r->bytes > s->max_bytes) {
+      s->idle_bytes -= s->idle.front().bytes;
+      destroy_slot(s->idle.front());
+      s->idle.erase(s->idle.begin());
+    }
+    rc = hgpu_create(&r->cfg, &r->ctx);
+    if (!rc && cudaMallocHost(&r->prog, 4 * sizeof(double)) != cudaSuccess) rc = HGPU_E_NOMEM;
+    if (!rc && cudaEventCreateWithFlags(&r->ev, cudaEventDisableTiming) != cudaSuccess) rc = HGPU_E_CUDA;
+  }
   if (!rc) rc = hgpu_upload_geometry(r->ctx, r->gcov.data(), r->gcon.data(), r->gcovpert.data(), r->gdet.data(),
                                      r->conn.data(), r->floors.data());
   if (!rc) rc = hgpu_upload_state(r->ctx, r->p.data(), nullptr, 0.0, 0.0);
   if (!rc) rc = hgpu_init_dt(r->ctx, nullptr);
-  if (!rc && cudaMallocHost(&r->prog, 4 * sizeof(double)) != cudaSuccess) rc = HGPU_E_NOMEM;
-  if (!rc && cudaEventCreateWithFlags(&r->ev, cudaEventDisableTiming) != cudaSuccess) rc = HGPU_E_CUDA;
   r->state = ACTIVE;
   s->used += r->bytes;
   s->active++;
@@ -141,7 +210,8 @@ static void retire(hgpu_server *s, Request *r) {
   r->pflag_out.resize(nz);
   double dt;
   int rc = hgpu_download_state(r->ctx, r->p_out.data(), r->pflag_out.data(), &r->t_out, &dt);
-  release_device(s, r);
+  if (rc) release_device(s, r);
+  else park(s, r);
   r->rc = rc;
   r->state = rc ? FAILED : FINISHED;
   r->t_finish = Clock::now();
@@ -167,6 +237,7 @@ void hgpu_server_destroy(hgpu_server *s) {
     release_device(s, r);
     delete r;
   }
+  for (Slot &q : s->idle) destroy_slot(q);
   delete s;
 }
 

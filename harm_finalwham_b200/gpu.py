@@ -21,6 +21,7 @@ FLUX = {"LAXF": 0, "HLL": 1}
 BC = {"OUTFLOW": 0, "POLARAXIS": 4, "PERIODIC": 7, "OUTFLOW_COPY": 1000}
 PREC = {"fp64": 0, "mixed": 1}
 UTOPRIM = {"2DFINAL": 6, "JON": 8, "JONNONRELCOMPAT": 8}
+DOENOFLUX = {"NOENOFLUX": 0, "ENOFINITEVOLUME": 3}
 
 _lib = None
 
@@ -38,7 +39,7 @@ class hgpu_config(ctypes.Structure):
                 ("cour", ctypes.c_double), ("safe", ctypes.c_double), ("defcon", ctypes.c_double),
                 ("tf", ctypes.c_double), ("rhominlimit", ctypes.c_double), ("uuminlimit", ctypes.c_double),
                 ("gammamax", ctypes.c_double), ("gammafail", ctypes.c_double), ("timeorder", ctypes.c_int),
-                ("utoprimversion", ctypes.c_int)]
+                ("utoprimversion", ctypes.c_int), ("doenoflux", ctypes.c_int)]
 
 
 class hgpu_diag(ctypes.Structure):
@@ -100,6 +101,7 @@ def load_library(path=None):
     L.hgpu_step_graph.argtypes = [ctypes.c_void_p, ctypes.c_int, _P(hgpu_stats)]
     L.hgpu_diagnostics.argtypes = [ctypes.c_void_p, _P(hgpu_diag)]
     L.hgpu_download_conserved.argtypes = [ctypes.c_void_p, _dp]
+    L.hgpu_upload_conserved.argtypes = [ctypes.c_void_p, _dp]
     L.hgpu_context_bytes.argtypes = [_P(hgpu_config)]
     L.hgpu_context_bytes.restype = ctypes.c_size_t
     L.hgpu_server_create.argtypes = [ctypes.c_size_t, ctypes.c_int, ctypes.c_int, _P(ctypes.c_void_p)]
@@ -119,7 +121,7 @@ def load_library(path=None):
     for name in ("hgpu_create", "hgpu_upload_geometry", "hgpu_upload_state", "hgpu_download_state", "hgpu_step_ch",
                  "hgpu_advance_stage", "hgpu_fluxcalc", "hgpu_bound_prim", "hgpu_utoprim_batch", "hgpu_utoprimgen_batch",
                  "hgpu_device_prims", "hgpu_sync", "hgpu_create_batch", "hgpu_batch_layout", "hgpu_batch_status",
-                 "hgpu_step_graph", "hgpu_batch_run", "hgpu_diagnostics", "hgpu_download_conserved", "hgpu_server_create", "hgpu_server_submit",
+                 "hgpu_step_graph", "hgpu_batch_run", "hgpu_diagnostics", "hgpu_download_conserved", "hgpu_upload_conserved", "hgpu_server_create", "hgpu_server_submit",
                  "hgpu_server_poll", "hgpu_server_result", "hgpu_server_release"):
         getattr(L, name).restype = ctypes.c_int
     if path == _build.LIB:
@@ -151,11 +153,12 @@ class HarmGPU:
     def __init__(self, n1, n2, n3, ng, dx, lim="MC", flux="HLL", bc=("OUTFLOW", "OUTFLOW", "POLARAXIS",
                  "POLARAXIS", "PERIODIC", "PERIODIC"), precision="fp64", gam=4.0 / 3.0, cour=0.8, safe=1.3,
                  defcon=1.0, tf=2000.0, rhominlimit=1e-20, uuminlimit=1e-20, gammamax=25.0, gammafail=2500.0,
-                 timeorder=2, utoprim="2DFINAL"):
+                 timeorder=2, utoprim="2DFINAL", doenoflux="NOENOFLUX"):
         self.L = load_library()
         c = hgpu_config()
         c.timeorder = int(timeorder)
         c.utoprimversion = UTOPRIM[utoprim] if isinstance(utoprim, str) else int(utoprim)
+        c.doenoflux = DOENOFLUX[doenoflux] if isinstance(doenoflux, str) else int(doenoflux)
         c.n1, c.n2, c.n3, c.ng = n1, n2, n3, ng
         c.lim = LIM[lim] if isinstance(lim, str) else int(lim)
         c.fluxmethod = FLUX[flux] if isinstance(flux, str) else int(flux)
@@ -185,9 +188,11 @@ class HarmGPU:
                 bc=tuple(inv_bc[b] for b in pr.bc), precision=precision, gam=pr.gam, cour=pr.cour, safe=pr.safe,
                 defcon=pr.defcon, tf=pr.tf, rhominlimit=pr.rhominlimit, uuminlimit=pr.uuminlimit,
                 gammamax=pr.gammamax, gammafail=pr.gammafail, timeorder=getattr(pr, "timeorder", 2),
-                utoprim=getattr(pr, "utoprim", "2DFINAL"))
+                utoprim=getattr(pr, "utoprim", "2DFINAL"), doenoflux=getattr(pr, "doenoflux", "NOENOFLUX"))
         o.upload_geometry(pr.gcov, pr.gcon, pr.gcovpert, pr.gdet, pr.conn, pr.floors)
         o.upload_state(pr.p, pr.pflag, pr.t, pr.dt)
+        if getattr(pr, "u", None) is not None and o.cfg.doenoflux == DOENOFLUX["ENOFINITEVOLUME"]:
+            o.upload_conserved(pr.u)
         return o
 
     def close(self):
@@ -242,6 +247,12 @@ class HarmGPU:
         st = hgpu_stats()
         _check(self.L, self.L.hgpu_step_ch(self.h, int(nsteps), ctypes.byref(st) if stats else None))
         return st
+
+    def upload_conserved(self, u):
+        """Set the finite-volume scheme's conserved state (restart's unew)."""
+        u = _contig(u, np.float64)
+        assert u.shape == self.nt + (NPR,)
+        _check(self.L, self.L.hgpu_upload_conserved(self.h, _ptr(u)))
 
     def download_conserved(self):
         """The conserved state after the last step (the reference's unew)."""
@@ -437,10 +448,11 @@ class HarmBatch(HarmGPU):
 def make_config(n, ng, dx, lim="MC", flux="HLL", bc=("OUTFLOW", "OUTFLOW", "POLARAXIS", "POLARAXIS", "PERIODIC",
                 "PERIODIC"), precision="fp64", gam=4.0 / 3.0, cour=0.8, safe=1.3, defcon=1.0, tf=2000.0,
                 rhominlimit=1e-20, uuminlimit=1e-20, gammamax=25.0, gammafail=2500.0, timeorder=2,
-                utoprim="2DFINAL"):
+                utoprim="2DFINAL", doenoflux="NOENOFLUX"):
     c = hgpu_config()
     c.timeorder = int(timeorder)
     c.utoprimversion = UTOPRIM[utoprim] if isinstance(utoprim, str) else int(utoprim)
+    c.doenoflux = DOENOFLUX[doenoflux] if isinstance(doenoflux, str) else int(doenoflux)
     c.n1, c.n2, c.n3 = n
     c.ng = ng
     c.lim = LIM[lim] if isinstance(lim, str) else int(lim)

@@ -33,7 +33,7 @@
 extern "C" {
 #endif
 
-#define HGPU_ABI_VERSION 3
+#define HGPU_ABI_VERSION 4
 
 /* return codes */
 #define HGPU_OK 0
@@ -65,6 +65,14 @@ extern "C" {
 #define HGPU_UTOPRIMJONNONRELCOMPAT 8    /* 1D Newton on E'(W'), utoprim_jon.c; the FM
                                             torus default (init.fishmon.c:46) */
 
+/* DOENOFLUX schemes (global.h:188-191) */
+#define HGPU_NOENOFLUX 0                 /* advance_standard (advance.c:58): Ui = U(pi) */
+#define HGPU_ENOFINITEVOLUME 3           /* advance_finitevolume (advance.c:245) with
+                                            avgscheme=DONOR, the FM torus problem's own
+                                            scheme (init.fishmon.c:97, 112): the conserved
+                                            state unew is evolved; needs ng = the
+                                            reference's MAXBND for its dt */
+
 /* precision modes */
 #define HGPU_PREC_FP64 0      /* bit-identical to the reference CPU build */
 #define HGPU_PREC_MIXED 1     /* FP32 reconstruction, wave speeds and Riemann flux */
@@ -82,6 +90,7 @@ typedef struct {
   int timeorder;    /* TIMEORDER (setup_rktimestep, step_ch.c:442-562): 1 Euler,
                        2 midpoint, 3 TVD RK3, 4 RK4; 0 means 2 */
   int utoprimversion; /* HGPU_UTOPRIM*; 0 means HGPU_UTOPRIM2DFINAL */
+  int doenoflux;    /* HGPU_NOENOFLUX or HGPU_ENOFINITEVOLUME */
 } hgpu_config;
 
 typedef struct hgpu_ctx hgpu_ctx;
@@ -222,6 +231,13 @@ int hgpu_diagnostics(hgpu_ctx *ctx, hgpu_diag *out);
    primitives it is what the reference's restart dump holds
    (rdump_content, restart.c:244-250). */
 int hgpu_download_conserved(hgpu_ctx *ctx, double *unew);
+
+/* Set the evolved conserved state of a HGPU_ENOFINITEVOLUME context from
+   the host (same layout), as the reference's restart reads unew and copies
+   it to uinitial (initbase.c:155-160).  hgpu_upload_state of such a context
+   sets it to U(p) in every zone, as init_conservatives/pi2Uavg does
+   (initbase.c:146-153, 1833). */
+int hgpu_upload_conserved(hgpu_ctx *ctx, const double *unew);
 
 /* Device bytes a context of this configuration allocates (0 if invalid). */
 size_t hgpu_context_bytes(const hgpu_config *cfg);
