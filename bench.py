@@ -51,16 +51,41 @@ WORKLOADS = {
     "torus3d_256x128x128_mc": (256, 128, 128, "MC", "HLL"),
     "torus3d_256x128x64_mc": (256, 128, 64, "MC", "HLL"),
     "torus2d_64x64": (64, 64, 1, "MC", "HLL"),
+    # the FM torus problem file's own scheme (init.fishmon.c:46, 97-127):
+    # PARA + HLL, RK4, Jon's inverter, finite volume with avgscheme=DONOR,
+    # all MAXBND=11 ghosts (its flux and dt loops cover them)
+    "torus3d_256x128x128_fishmon": (256, 128, 128, "PARA", "HLL"),
+    "torus3d_128x64x32_fishmon": (128, 64, 32, "PARA", "HLL"),
+}
+# scheme settings beyond the 2D Noble / midpoint / standard-update default
+SCHEMES = {
+    "torus3d_256x128x128_fishmon": {"timeorder": 4, "utoprim": "JON", "doenoflux": "ENOFINITEVOLUME", "ng": 11},
+    "torus3d_128x64x32_fishmon": {"timeorder": 4, "utoprim": "JON", "doenoflux": "ENOFINITEVOLUME", "ng": 11},
 }
 DEFAULT_WORKLOAD = "torus3d_256x128x128"
-# ghost zones kept on the device: MC reads 2 per side, WENO5 6 (the reference's
-# MAXBND=11 lines never truncate a WENO5 stencil, and 6 is what its stencils read)
-GHOSTS = {"MC": 3, "WENO5": 6}
+# ghost zones kept on the device: MC reads 2 per side, PARA 3, WENO5 6 (the
+# reference's MAXBND=11 lines never truncate a WENO5 stencil, and 6 is what
+# its stencils read)
+GHOSTS = {"MC": 3, "PARA": 3, "WENO5": 6}
 
 
-def cpu_sample(lim):
+def scheme_of(workload):
+    sc = {"timeorder": 2, "utoprim": "2DFINAL", "doenoflux": "NOENOFLUX", "ng": None}
+    sc.update(SCHEMES.get(workload, {}))
+    return sc
+
+
+def scheme_text(lim, flux, sc):
+    inv = "2D Noble" if sc["utoprim"] == "2DFINAL" else "Jon 1D E'(W')"
+    ti = {1: "Euler", 2: "midpoint RK2", 3: "TVD RK3", 4: "RK4"}[sc["timeorder"]]
+    fv = ", finite volume (avgscheme DONOR)" if sc["doenoflux"] == "ENOFINITEVOLUME" else ""
+    return f"{lim}+{flux}+flux-CT, {inv} inversion, {ti}{fv}"
+
+
+def cpu_sample(workload):
     """CPU sample for the reference build: same problem and scheme, 3D 64x32x32."""
-    return (64, 32, 32, lim, "HLL")
+    lim = WORKLOADS[workload][3]
+    return (64, 32, 32, lim, "HLL") + (scheme_of(workload),)
 
 METRIC = "zone-updates/s FP64 vs mixed on 3D Kerr torus at stated L1; batch p50/p99 latency"
 
@@ -159,8 +184,10 @@ def profile_traffic(workload, kernel):
 # reference CPU build
 # ---------------------------------------------------------------------------
 def ref_binary(sample):
-    n1, n2, n3, lim, flux = sample
-    return os.path.join(ROOT, "oracle", "_ref", f"harm_ref_{n1}x{n2}x{n3}_{lim}_{flux}")
+    n1, n2, n3, lim, flux, sc = sample
+    suffix = ((f"_rk{sc['timeorder']}" if sc["timeorder"] != 2 else "") + ("_jon" if sc["utoprim"] == "JON" else "")
+              + ("_fv" if sc["doenoflux"] == "ENOFINITEVOLUME" else ""))
+    return os.path.join(ROOT, "oracle", "_ref", f"harm_ref_{n1}x{n2}x{n3}_{lim}_{flux}{suffix}")
 
 
 def run_reference(sample, steps, warmup, procs):
@@ -207,15 +234,19 @@ def bench_ours(args, rank, world):
     from harm_finalwham_b200.gpu import HarmGPU, load_library
 
     n1, n2, n3, lim, flux = WORKLOADS[args.workload]
+    sc = scheme_of(args.workload)
+    if args.utoprim:
+        sc["utoprim"] = args.utoprim
     t_gen = time.time()
-    dom = torus.fm_torus(n1, n2, n3, ng=GHOSTS[lim], lim=lim, flux=flux, seed=7 + rank)
+    dom = torus.fm_torus(n1, n2, n3, ng=sc["ng"] or GHOSTS[lim], lim=lim, flux=flux, seed=7 + rank)
     t_gen = time.time() - t_gen
     L = load_library()
     g = HarmGPU(n1, n2, n3, dom.ng, dom.dx, lim=lim, flux=flux, precision=args.precision, gam=dom.gam,
-                cour=dom.cour, utoprim=args.utoprim)
+                cour=dom.cour, utoprim=sc["utoprim"], timeorder=sc["timeorder"], doenoflux=sc["doenoflux"])
     g.upload_geometry(dom.gcov, dom.gcon, dom.gcovpert, dom.gdet, dom.conn, dom.floors)
     g.upload_state(dom.p, dom.pflag, 0.0, 0.0)
     dt0 = g.init_dt()
+    tuning = g.autotune()
 
     dist = None
     if world > 1:
@@ -261,10 +292,11 @@ def bench_ours(args, rank, world):
         other_prec = "mixed" if args.precision == "fp64" else "fp64"
         p_this, _, _, _ = g.download_state()
         g2 = HarmGPU(n1, n2, n3, dom.ng, dom.dx, lim=lim, flux=flux, precision=other_prec, gam=dom.gam, cour=dom.cour,
-                     utoprim=args.utoprim)
+                     utoprim=sc["utoprim"], timeorder=sc["timeorder"], doenoflux=sc["doenoflux"])
         g2.upload_geometry(dom.gcov, dom.gcon, dom.gcovpert, dom.gdet, dom.conn, dom.floors)
         g2.upload_state(dom.p, dom.pflag, 0.0, 0.0)
         g2.init_dt()
+        g2.autotune()
         g2.step_ch(args.warmup)
         barrier()
         ms2, st2 = g2.step_ch_timed(args.steps)
@@ -316,7 +348,7 @@ def bench_ours(args, rank, world):
     dom_k = max(ktimes, key=lambda k: ktimes[k]["ms"])
     kt = ktimes[dom_k]
     avg_s = kt["ms"] / kt["launches"] / 1e3
-    alg = algorithmic_bytes(dom_k, n1, n2, n3, lim)
+    alg = algorithmic_bytes(dom_k, n1, n2, n3, lim, tx=dom.ng if sc["doenoflux"] == "ENOFINITEVOLUME" else 1)
     peaks, peaks_kind = measured_peaks()
     achieved = alg / avg_s / 1e9
     roof = {"kernel": dom_k, "bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
@@ -333,12 +365,11 @@ def bench_ours(args, rank, world):
         "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64" if args.precision == "fp64" else "f64+f32", "data": "synthetic",
         "config": {"workload": f"{args.workload}: 3D Fishbone-Moncrief torus a=0.9375 beta=100 MKS, "
-                               f"{lim}+{flux}+flux-CT, "
-                               f"{'2D Noble' if args.utoprim == '2DFINAL' else 'Jon 1D E(W)'} inversion, "
-                               f"midpoint RK2, {args.precision}",
+                               f"{scheme_text(lim, flux, sc)}, {args.precision}",
                    "zones": zones, "ghosts": dom.ng, "parallelism": f"replicas x{world}" if world > 1 else "single",
                    "l2": "inputs larger than L2 (300 MB per state array)", "init_dt": dt0,
-                   "newton_iters_per_zone_step": st.newton_iters / (zones * args.steps * 2.0)},
+                   "newton_iters_per_zone_step": st.newton_iters / (zones * args.steps * float(sc["timeorder"])),
+                   "autotune": tuning},
         "gpu_launches": launches,
         "roofline": roof,
         "kernels": {k: {"ms": round(v["ms"], 4), "launches": v["launches"]} for k, v in ktimes.items() if v["launches"]},
@@ -352,7 +383,7 @@ def bench_ours(args, rank, world):
         result["serving"] = bench_serving()
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         procs = min(host_cores(), args.cpu_procs)
-        cs = cpu_sample(lim)
+        cs = cpu_sample(args.workload)
         v, why = run_reference(cs, args.cpu_steps, 2, procs)
         result["cpu_baseline"] = ({"value": v, "unit": "zone-updates/s", "cores": procs, "kind": "reference",
                                    "sample": f"reference CPU build (gcc -O2 -ffp-contract=off), 3D torus "
@@ -472,7 +503,7 @@ def serving_requests(count, seed):
     return out
 
 
-def bench_serving(count=24, tf=5.0, mean_gap_ms=2.0, seed=11, budget_bytes=32e9):
+def bench_serving(count=24, tf=50.0, mean_gap_ms=2.0, seed=11, budget_bytes=32e9):
     """Continuous batching: requests arrive on a seeded Poisson clock fast
     enough to keep the GPU saturated and go through hgpu_server (admission by
     device footprint, overlapped solves, each solve's step replayed from its
@@ -547,12 +578,15 @@ def bench_serving(count=24, tf=5.0, mean_gap_ms=2.0, seed=11, budget_bytes=32e9)
                     "with plain launches or with its captured step graph" % mean_gap_ms}
 
 
-def algorithmic_bytes(kernel, n1, n2, n3, lim="MC"):
+def algorithmic_bytes(kernel, n1, n2, n3, lim="MC", tx=1):
     """Compulsory HBM bytes per launch (FP64, state resident; per-(i,j) metric
-    amortised over x3).  Units: faces for the flux kernels, zones otherwise."""
+    amortised over x3).  Units: faces for the flux kernels, zones otherwise.
+    tx: transverse zones beyond the grid that the flux loops cover (1; all
+    ghosts for the finite-volume scheme)."""
     zones = n1 * n2 * n3
-    faces = {"flux_x1": (n1 + 1) * (n2 + 2) * (n3 + 2), "flux_x2": (n1 + 2) * (n2 + 1) * (n3 + 2),
-             "flux_x3": (n1 + 2) * (n2 + 2) * (n3 + 1)}
+    t = 2 * tx
+    faces = {"flux_x1": (n1 + 1) * (n2 + t) * (n3 + t), "flux_x2": (n1 + t) * (n2 + 1) * (n3 + t),
+             "flux_x3": (n1 + t) * (n2 + t) * (n3 + 1)}
     if kernel in faces:
         if lim == "WENO5":
             return faces[kernel] * (128 + 64)     # read the two face states (16 doubles), write 8 fluxes
@@ -609,8 +643,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default=DEFAULT_WORKLOAD, choices=sorted(WORKLOADS))
     ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
-    ap.add_argument("--utoprim", default="2DFINAL", choices=["2DFINAL", "JON"],
-                    help="con-to-prim inverter: utoprim_2d_final.c or utoprim_jon.c")
+    ap.add_argument("--utoprim", default=None, choices=["2DFINAL", "JON"],
+                    help="con-to-prim inverter (default: the workload's): utoprim_2d_final.c or utoprim_jon.c")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-batch", action="store_true",
                     help="skip the batched 1D Riemann-problem measurement")
@@ -631,7 +665,7 @@ def main():
         if rank != 0:
             return 0
         procs = min(host_cores(), args.cpu_procs)
-        cs = cpu_sample(WORKLOADS[args.workload][3])
+        cs = cpu_sample(args.workload)
         # each step: one step of every process's bounded sample
         v, why = run_reference(cs, args.steps, args.warmup, procs)
         if v is None:

@@ -49,6 +49,9 @@ struct Params {
   double dx1, dx2, dx3;
   int lim, flux;
   int bc[6];
+  // finite-volume scheme: faces beyond one zone across the grid (its flux
+  // loops run over all transverse ghosts) feed only the dt minimum
+  int fvring;
   // batch of independent 1D instances (nullptr: one domain)
   const int *cell_inst;  // instance of every cell of the line
   Inst *inst;
@@ -235,6 +238,13 @@ template <> struct MinBlocks<float> {
   static constexpr int flux = HG_MINB_FLUX_F32, weno_a = HG_MINB_WENO_A_F32, weno_b = HG_MINB_WENO_B_F32;
 };
 
+// the FP64 variants the autotuner chooses between (resident 128-thread
+// blocks per SM for each heavy kernel; variant 0 is the default above)
+constexpr int kFluxMB[2] = {HG_MINB_FLUX, HG_MINB_FLUX + 1};
+constexpr int kWenoBMB[2] = {HG_MINB_WENO_B, HG_MINB_WENO_B + 2};
+constexpr int kConserveMB[2] = {HG_MINB_UPDATE, 3};
+constexpr int kInvertMB[2] = {HG_MINB_INVERT, 2};
+
 template <int DIR>
 __device__ __forceinline__ long long dir_stride(const Dims &d) {
   return (DIR == 1) ? (long long)d.nt2 * d.nt3 : ((DIR == 2) ? (long long)d.nt3 : 1);
@@ -281,8 +291,8 @@ __global__ void __launch_bounds__(128, MinBlocks<T>::weno_a) weno_a_kernel(Dims 
 }
 
 // pass B over line cells -1..n: dP/P, ratios, reduction, face values
-template <int DIR, typename T>
-__global__ void __launch_bounds__(128, MinBlocks<T>::weno_b) weno_b_kernel(Dims d, Params P, Box box,
+template <int DIR, typename T, int MB = MinBlocks<T>::weno_b>
+__global__ void __launch_bounds__(128, MB) weno_b_kernel(Dims d, Params P, Box box,
                                                                      const double *__restrict__ pb,
                                                                      const double *__restrict__ G,
                                                                      const T *__restrict__ WA, T *__restrict__ pL,
@@ -357,8 +367,8 @@ __global__ void __launch_bounds__(128, MinBlocks<T>::weno_b) weno_b_kernel(Dims 
 // face flux kernel (one per direction); RECON 0: MC-type slopes in the
 // kernel, RECON 1: Riemann states from the WENO5 face values pL/pR
 // ---------------------------------------------------------------------------
-template <int DIR, int RECON, typename T>
-__global__ void __launch_bounds__(128, MinBlocks<T>::flux) flux_kernel(Dims d, Params P, Box box,
+template <int DIR, int RECON, typename T, int MB = MinBlocks<T>::flux>
+__global__ void __launch_bounds__(128, MB) flux_kernel(Dims d, Params P, Box box,
                                                                  const double *__restrict__ pb,
                                                                  const T *__restrict__ pL, const T *__restrict__ pR,
                                                                  const double *__restrict__ G, double *__restrict__ F,
@@ -407,44 +417,63 @@ __global__ void __launch_bounds__(128, MinBlocks<T>::flux) flux_kernel(Dims d, P
     p_l[B1 + DIR - 1] = p_r[B1 + DIR - 1] = T(0.5) * (p_l[B1 + DIR - 1] + p_r[B1 + DIR - 1]);
     MetricT<T> m;
     load_metric_t(G, d, gix(d, i, j), DIR - 1, m);
-    StateT<T> ql, qr;
-    EMT<T> el, er;
-    T Fl[NPR], Fr[NPR], Ul[NPR], Ur[NPR];
     int b = P.cell_inst ? P.cell_inst[z] : -1;
     const T gam = (T)(b >= 0 ? P.inst[b].gam : P.gam);
     int err = 0;
-    if (get_state(p_l, m, ql)) err |= ERR_UTCALC_DISCR;
-    em_prepare(p_l, m, ql, el);
-    primtoflux(p_l, ql, el, DIR, m, gam, Fl);
-    primtoflux(p_l, ql, el, 0, m, gam, Ul);
-    if (get_state(p_r, m, qr)) err |= ERR_UTCALC_DISCR;
-    em_prepare(p_r, m, qr, er);
-    primtoflux(p_r, qr, er, DIR, m, gam, Fr);
-    primtoflux(p_r, qr, er, 0, m, gam, Ur);
+    // a face that only feeds the dt minimum needs the wave speeds alone
+    bool ring = false;
+    if (P.fvring) {
+      if (DIR != 1 && (i < -d.s1 || i > d.n1 - 1 + d.s1)) ring = true;
+      if (DIR != 2 && (j < -d.s2 || j > d.n2 - 1 + d.s2)) ring = true;
+      if (DIR != 3 && (k < -d.s3 || k > d.n3 - 1 + d.s3)) ring = true;
+    }
     T cmaxl = T(0.), cminl = T(0.), cmaxr = T(0.), cminr = T(0.);
-    err |= vchar(p_l, ql, DIR, m, gam, &cmaxl, &cminl);
-    err |= vchar(p_r, qr, DIR, m, gam, &cmaxr, &cminr);
+    T Fl[NPR], Fr[NPR], Ul[NPR], Ur[NPR];
+    {
+      StateT<T> q;
+      if (get_state(p_l, m, q)) err |= ERR_UTCALC_DISCR;
+      err |= vchar(p_l, q, DIR, m, gam, &cmaxl, &cminl);
+      if (!ring) {
+        EMT<T> e;
+        em_prepare(p_l, m, q, e);
+        primtoflux(p_l, q, e, DIR, m, gam, Fl);
+        primtoflux(p_l, q, e, 0, m, gam, Ul);
+      }
+    }
+    {
+      StateT<T> q;
+      if (get_state(p_r, m, q)) err |= ERR_UTCALC_DISCR;
+      err |= vchar(p_r, q, DIR, m, gam, &cmaxr, &cminr);
+      if (!ring) {
+        EMT<T> e;
+        em_prepare(p_r, m, q, e);
+        primtoflux(p_r, q, e, DIR, m, gam, Fr);
+        primtoflux(p_r, q, e, 0, m, gam, Ur);
+      }
+    }
     // cminmax_calc (wavespeeds.c:325-385)
     T lmin = min_ref(cminl, cminr);
     T lmax = max_ref(cmaxl, cmaxr);
     lmin = fabs(max_ref(T(0.), -lmin));
     lmax = fabs(max_ref(T(0.), lmax));
     T cmin = lmin, cmax = lmax, ctop = max_ref(lmax, lmin);
-    double Fo[NPR];
-    if (P.flux == HGPU_FLUX_HLL && (cmax + cmin != T(0.0))) {
+    if (!ring) {
+      double Fo[NPR];
+      if (P.flux == HGPU_FLUX_HLL && (cmax + cmin != T(0.0))) {
 #pragma unroll
-      for (int v = 0; v < NPR; v++)
-        Fo[v] = (double)(((cmax * Fl[v] + cmin * Fr[v]) - (cmax * cmin) * (Ur[v] - Ul[v])) / (cmax + cmin));
-    } else {
+        for (int v = 0; v < NPR; v++)
+          Fo[v] = (double)(((cmax * Fl[v] + cmin * Fr[v]) - (cmax * cmin) * (Ur[v] - Ul[v])) / (cmax + cmin));
+      } else {
 #pragma unroll
-      for (int v = 0; v < NPR; v++) Fo[v] = (double)(T(0.5) * ((Fl[v] + Fr[v]) - ctop * (Ur[v] - Ul[v])));
+        for (int v = 0; v < NPR; v++) Fo[v] = (double)(T(0.5) * ((Fl[v] + Fr[v]) - ctop * (Ur[v] - Ul[v])));
+      }
+      // flux_ct gdet strip (fluxct.c:74-96), in FP64 in both precision modes
+      const double gface = __ldg(G + (long long)((DIR - 1) * GLOC + 33) * d.nij + gix(d, i, j));
+      Fo[B1] /= gface;
+      Fo[B2] /= gface;
+      Fo[B3] /= gface;
+      store_prim(F, d, z, Fo);
     }
-    // flux_ct gdet strip (fluxct.c:74-96), in FP64 in both precision modes
-    const double gface = __ldg(G + (long long)((DIR - 1) * GLOC + 33) * d.nij + gix(d, i, j));
-    Fo[B1] /= gface;
-    Fo[B2] /= gface;
-    Fo[B3] /= gface;
-    store_prim(F, d, z, Fo);
     double dxd = (DIR == 1) ? P.dx1 : ((DIR == 2) ? P.dx2 : P.dx3);
     if (b >= 0) {
       // batch: faces 0..n of a running instance feed its own dt

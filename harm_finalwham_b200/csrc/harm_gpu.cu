@@ -228,7 +228,8 @@ __global__ void pi2u_kernel(Dims d, Params P, const double *__restrict__ p, cons
   for (int pl = 0; pl < NPR; pl++) u[pl * d.nz + z] = U[pl];
 }
 
-__global__ void __launch_bounds__(128, HG_MINB_UPDATE) conserve_kernel(
+template <int MB>
+__global__ void __launch_bounds__(128, MB) conserve_kernel(
     Dims d, Params P, Box box, const double *pi, const double *pb, double *__restrict__ uf,
     double *__restrict__ ucum, const double *__restrict__ F1, const double *__restrict__ F2,
     const double *__restrict__ F3, const double *__restrict__ E, const double *__restrict__ G, Scalars *sc,
@@ -281,17 +282,19 @@ __global__ void __launch_bounds__(128, HG_MINB_UPDATE) conserve_kernel(
       em_prepare(pbz, m, q, e);
       double dUconn[4] = {0., 0., 0., 0.};
       const double *conn = G + (long long)G_CONN * d.nij + ij;
-      double mhd[4][4];
+      // each T^jj_kk row is contracted as soon as it is formed; every
+      // dUconn[l] still adds its terms in the order jj, then kk
 #pragma unroll
-      for (int jj = 0; jj < 4; jj++) mhd_row(pbz, jj, gam, q, e, mhd[jj]);
+      for (int jj = 0; jj < 4; jj++) {
+        double row[4];
+        mhd_row(pbz, jj, gam, q, e, row);
 #pragma unroll
-      for (int l = 0; l < 4; l++) {
-        double s = dUconn[l];
+        for (int l = 0; l < 4; l++) {
+          double s = dUconn[l];
 #pragma unroll
-        for (int jj = 0; jj < 4; jj++)
-#pragma unroll
-          for (int kk = 0; kk < 4; kk++) s += mhd[jj][kk] * __ldg(conn + (long long)((kk * 4 + l) * 4 + jj) * d.nij);
-        dUconn[l] = s;
+          for (int kk = 0; kk < 4; kk++) s += row[kk] * __ldg(conn + (long long)((kk * 4 + l) * 4 + jj) * d.nij);
+          dUconn[l] = s;
+        }
       }
 #pragma unroll
       for (int l = 0; l < 4; l++) {
@@ -360,8 +363,8 @@ __global__ void __launch_bounds__(128, HG_MINB_UPDATE) conserve_kernel(
     if (err) atomicOr(&sc->err, err);
 }
 
-template <int UV>
-__global__ void __launch_bounds__(128, HG_MINB_INVERT) invert_kernel(Dims d, Params P, Box box, const double *pb,
+template <int UV, int MB>
+__global__ void __launch_bounds__(128, MB) invert_kernel(Dims d, Params P, Box box, const double *pb,
                                                                      double *pf, const double *__restrict__ uf,
                                                                      const double *__restrict__ ucum,
                                                                      const double *__restrict__ G,
@@ -1073,6 +1076,9 @@ struct hgpu_ctx {
   double *p = nullptr, *pk = nullptr, *uf = nullptr, *ucum = nullptr;
   double *pk1 = nullptr;  // second intermediate state of TIMEORDER 3 and 4
   double *ui = nullptr;   // ENOFINITEVOLUME: the conserved state at the start of the step (uinitial)
+  struct {
+    int flux = 0, weno_b = 0, conserve = 0, invert = 0;  // variant index per kernel family (hgpu_autotune)
+  } tune;
   double *F[4] = {nullptr, nullptr, nullptr, nullptr};
   double *E = nullptr;
   double *G = nullptr;
@@ -1218,6 +1224,7 @@ static void fill_params(Params &P, const hgpu_config *cfg) {
   P.lim = cfg->lim;
   P.flux = cfg->fluxmethod;
   for (int f = 0; f < 6; f++) P.bc[f] = cfg->bc[f];
+  P.fvring = (cfg->doenoflux == HGPU_ENOFINITEVOLUME);
 }
 
 // Two configurations with the same allocation shape: the same device
@@ -1520,55 +1527,35 @@ int hgpu_download_state(hgpu_ctx *x, double *p, int *pflag, double *t, double *d
 
 // one stage: fluxes, EMFs, update, bound, post_fixup, bound
 extern "C++" {
-template <typename T>
+// one direction's reconstruction + flux launches; FMB / BMB: resident
+// blocks per SM asked of the flux and weno_b kernels (autotuned variants)
+template <int DIR, typename T, int FMB, int BMB>
+static void launch_dir(hgpu_ctx *x, const double *pb) {
+  const Dims &d = x->d;
+  const Params &P = x->P;
+  T *WA = (T *)x->WA, *pL = (T *)x->pL, *pR = (T *)x->pR;
+  const int kid = (DIR == 1) ? K_FLUX1 : ((DIR == 2) ? K_FLUX2 : K_FLUX3);
+  unsigned gf = grid_for(x->face_box[DIR].size(), 128);
+  if (P.lim == HGPU_LIM_WENO5) {
+    unsigned ga = grid_for(x->wa_box[DIR].size(), 128), gb = grid_for(x->wb_box[DIR].size(), 128);
+    LAUNCH(x, K_WENO_A, (weno_a_kernel<DIR, T>), ga, 128, d, x->wa_box[DIR], pb, WA);
+    LAUNCH(x, K_WENO_B, (weno_b_kernel<DIR, T, BMB>), gb, 128, d, P, x->wb_box[DIR], pb, x->G, WA, pL, pR);
+    LAUNCH(x, kid, (flux_kernel<DIR, 1, T, FMB>), gf, 128, d, P, x->face_box[DIR], pb, pL, pR, x->G, x->F[DIR], x->sc);
+  } else if (P.lim == HGPU_LIM_PARA) {
+    LAUNCH(x, kid, (flux_kernel<DIR, 2, T, FMB>), gf, 128, d, P, x->face_box[DIR], pb, nullptr, nullptr, x->G,
+           x->F[DIR], x->sc);
+  } else {
+    LAUNCH(x, kid, (flux_kernel<DIR, 0, T, FMB>), gf, 128, d, P, x->face_box[DIR], pb, nullptr, nullptr, x->G,
+           x->F[DIR], x->sc);
+  }
+}
+
+template <typename T, int FMB, int BMB>
 static void launch_fluxes_t(hgpu_ctx *x, const double *pb) {
   const Dims &d = x->d;
-  const int nd[4] = {0, d.n1, d.n2, d.n3};
-  bool weno = x->P.lim == HGPU_LIM_WENO5;
-  T *WA = (T *)x->WA, *pL = (T *)x->pL, *pR = (T *)x->pR;
-  for (int q = 1; q <= 3; q++) {
-    if (nd[q] <= 1) continue;
-    unsigned gf = grid_for(x->face_box[q].size(), 128);
-    unsigned ga = grid_for(x->wa_box[q].size(), 128), gb = grid_for(x->wb_box[q].size(), 128);
-    const Params &P = x->P;
-    if (q == 1) {
-      if (weno) {
-        LAUNCH(x, K_WENO_A, (weno_a_kernel<1, T>), ga, 128, d, x->wa_box[1], pb, WA);
-        LAUNCH(x, K_WENO_B, (weno_b_kernel<1, T>), gb, 128, d, P, x->wb_box[1], pb, x->G, WA, pL, pR);
-        LAUNCH(x, K_FLUX1, (flux_kernel<1, 1, T>), gf, 128, d, P, x->face_box[1], pb, pL, pR, x->G, x->F[1], x->sc);
-      } else if (P.lim == HGPU_LIM_PARA) {
-        LAUNCH(x, K_FLUX1, (flux_kernel<1, 2, T>), gf, 128, d, P, x->face_box[1], pb, nullptr, nullptr, x->G, x->F[1],
-               x->sc);
-      } else {
-        LAUNCH(x, K_FLUX1, (flux_kernel<1, 0, T>), gf, 128, d, P, x->face_box[1], pb, nullptr, nullptr, x->G, x->F[1],
-               x->sc);
-      }
-    } else if (q == 2) {
-      if (weno) {
-        LAUNCH(x, K_WENO_A, (weno_a_kernel<2, T>), ga, 128, d, x->wa_box[2], pb, WA);
-        LAUNCH(x, K_WENO_B, (weno_b_kernel<2, T>), gb, 128, d, P, x->wb_box[2], pb, x->G, WA, pL, pR);
-        LAUNCH(x, K_FLUX2, (flux_kernel<2, 1, T>), gf, 128, d, P, x->face_box[2], pb, pL, pR, x->G, x->F[2], x->sc);
-      } else if (P.lim == HGPU_LIM_PARA) {
-        LAUNCH(x, K_FLUX2, (flux_kernel<2, 2, T>), gf, 128, d, P, x->face_box[2], pb, nullptr, nullptr, x->G, x->F[2],
-               x->sc);
-      } else {
-        LAUNCH(x, K_FLUX2, (flux_kernel<2, 0, T>), gf, 128, d, P, x->face_box[2], pb, nullptr, nullptr, x->G, x->F[2],
-               x->sc);
-      }
-    } else {
-      if (weno) {
-        LAUNCH(x, K_WENO_A, (weno_a_kernel<3, T>), ga, 128, d, x->wa_box[3], pb, WA);
-        LAUNCH(x, K_WENO_B, (weno_b_kernel<3, T>), gb, 128, d, P, x->wb_box[3], pb, x->G, WA, pL, pR);
-        LAUNCH(x, K_FLUX3, (flux_kernel<3, 1, T>), gf, 128, d, P, x->face_box[3], pb, pL, pR, x->G, x->F[3], x->sc);
-      } else if (P.lim == HGPU_LIM_PARA) {
-        LAUNCH(x, K_FLUX3, (flux_kernel<3, 2, T>), gf, 128, d, P, x->face_box[3], pb, nullptr, nullptr, x->G, x->F[3],
-               x->sc);
-      } else {
-        LAUNCH(x, K_FLUX3, (flux_kernel<3, 0, T>), gf, 128, d, P, x->face_box[3], pb, nullptr, nullptr, x->G, x->F[3],
-               x->sc);
-      }
-    }
-  }
+  if (d.n1 > 1) launch_dir<1, T, FMB, BMB>(x, pb);
+  if (d.n2 > 1) launch_dir<2, T, FMB, BMB>(x, pb);
+  if (d.n3 > 1) launch_dir<3, T, FMB, BMB>(x, pb);
 }
 }  // extern "C++"
 
@@ -1577,8 +1564,15 @@ static void launch_fluxes_t(hgpu_ctx *x, const double *pb) {
 // everything after them (flux-CT, update, inversion) stays FP64.
 static void launch_fluxes(hgpu_ctx *x, const double *pb) {
   const Dims &d = x->d;
-  if (x->cfg.precision == HGPU_PREC_MIXED) launch_fluxes_t<float>(x, pb);
-  else launch_fluxes_t<double>(x, pb);
+  if (x->cfg.precision == HGPU_PREC_MIXED) {
+    launch_fluxes_t<float, MinBlocks<float>::flux, MinBlocks<float>::weno_b>(x, pb);
+  } else {
+    const int fv = x->tune.flux, bv = x->tune.weno_b;
+    if (fv == 0 && bv == 0) launch_fluxes_t<double, kFluxMB[0], kWenoBMB[0]>(x, pb);
+    else if (fv == 0) launch_fluxes_t<double, kFluxMB[0], kWenoBMB[1]>(x, pb);
+    else if (bv == 0) launch_fluxes_t<double, kFluxMB[1], kWenoBMB[0]>(x, pb);
+    else launch_fluxes_t<double, kFluxMB[1], kWenoBMB[1]>(x, pb);
+  }
   LAUNCH(x, K_EMF, emf_kernel, grid_for(x->emf_box.size(), 256), 256, d, x->emf_box, x->F[1], x->F[2], x->F[3], x->G,
          x->E);
 }
@@ -1639,14 +1633,30 @@ static void launch_stage(hgpu_ctx *x, int timeorder) {
   launch_fluxes(x, pb);
   const int fv = (x->cfg.doenoflux == HGPU_ENOFINITEVOLUME);
   double *ufv = (fv && finalstep) ? x->ucum : nullptr;
-  LAUNCH(x, K_UPDATE, conserve_kernel, grid_for(x->active_box.size(), 128), 128, d, x->P, x->active_box, pi, pb, x->uf,
-         x->ucum, x->F[1], x->F[2], x->F[3], x->E, x->G, x->sc, CUf0, CUf1, CUf2, Cn0, Cn1, Cn2, timeorder, x->ui, fv);
-  if (x->cfg.utoprimversion == HGPU_UTOPRIMJONNONRELCOMPAT)
-    LAUNCH(x, K_INVERT, invert_kernel<8>, grid_for(x->active_box.size(), 128), 128, d, x->P, x->active_box, pb, pf,
-           x->uf, x->ucum, x->G, x->pflag, x->sc, finalstep, ufv);
+  if (x->tune.conserve)
+    LAUNCH(x, K_UPDATE, conserve_kernel<kConserveMB[1]>, grid_for(x->active_box.size(), 128), 128, d, x->P,
+           x->active_box, pi, pb, x->uf, x->ucum, x->F[1], x->F[2], x->F[3], x->E, x->G, x->sc, CUf0, CUf1, CUf2, Cn0,
+           Cn1, Cn2, timeorder, x->ui, fv);
   else
-    LAUNCH(x, K_INVERT, invert_kernel<6>, grid_for(x->active_box.size(), 128), 128, d, x->P, x->active_box, pb, pf,
-           x->uf, x->ucum, x->G, x->pflag, x->sc, finalstep, ufv);
+    LAUNCH(x, K_UPDATE, conserve_kernel<kConserveMB[0]>, grid_for(x->active_box.size(), 128), 128, d, x->P,
+           x->active_box, pi, pb, x->uf, x->ucum, x->F[1], x->F[2], x->F[3], x->E, x->G, x->sc, CUf0, CUf1, CUf2, Cn0,
+           Cn1, Cn2, timeorder, x->ui, fv);
+  {
+    const unsigned gi = grid_for(x->active_box.size(), 128);
+    const bool jon = x->cfg.utoprimversion == HGPU_UTOPRIMJONNONRELCOMPAT;
+    if (jon && x->tune.invert)
+      LAUNCH(x, K_INVERT, (invert_kernel<8, kInvertMB[1]>), gi, 128, d, x->P, x->active_box, pb, pf, x->uf, x->ucum,
+             x->G, x->pflag, x->sc, finalstep, ufv);
+    else if (jon)
+      LAUNCH(x, K_INVERT, (invert_kernel<8, kInvertMB[0]>), gi, 128, d, x->P, x->active_box, pb, pf, x->uf, x->ucum,
+             x->G, x->pflag, x->sc, finalstep, ufv);
+    else if (x->tune.invert)
+      LAUNCH(x, K_INVERT, (invert_kernel<6, kInvertMB[1]>), gi, 128, d, x->P, x->active_box, pb, pf, x->uf, x->ucum,
+             x->G, x->pflag, x->sc, finalstep, ufv);
+    else
+      LAUNCH(x, K_INVERT, (invert_kernel<6, kInvertMB[0]>), gi, 128, d, x->P, x->active_box, pb, pf, x->uf, x->ucum,
+             x->G, x->pflag, x->sc, finalstep, ufv);
+  }
   launch_bound(x, pf);
   // post_fixup (fixup.c:37-96)
   if (x->P.cell_inst)
@@ -2042,6 +2052,106 @@ int hgpu_step_ch_timed(hgpu_ctx *x, int nsteps, float *ms, hgpu_stats *stats) {
   cudaEventDestroy(b);
   if (ms) *ms = t;
   return read_stats(x, stats);
+}
+
+// Autotuner: for each FP64 kernel family (flux, weno_b, conserve, invert)
+// time both resident-block variants on the context's own state (one warm-up
+// step and one timed step each, kernel times from the profiling events, the
+// state restored before every trial) and keep the faster.  The variants
+// differ only in register allocation, so results are identical whichever
+// is chosen; the state is restored at the end.
+int hgpu_autotune(hgpu_ctx *x, hgpu_tuning *out) {
+  if (!x || x->P.cell_inst) return HGPU_E_INVALID;
+  if (x->profiling) {
+    set_err("hgpu_autotune: turn profiling off first");
+    return HGPU_E_INVALID;
+  }
+  const long long nz = x->d.nz;
+  const size_t pb = sizeof(double) * NPR * nz;
+  const bool fv = x->cfg.doenoflux == HGPU_ENOFINITEVOLUME;
+  double *sp = nullptr, *su = nullptr;
+  int *sf = nullptr;
+  Scalars *ss = nullptr;
+  CUDA_TRY(cudaStreamSynchronize(x->stream));
+  CUDA_TRY(cudaMallocAsync(&sp, pb, x->stream));
+  CUDA_TRY(cudaMallocAsync(&sf, sizeof(int) * nz, x->stream));
+  CUDA_TRY(cudaMallocAsync(&ss, sizeof(Scalars), x->stream));
+  if (fv) CUDA_TRY(cudaMallocAsync(&su, pb, x->stream));
+  CUDA_TRY(cudaMemcpyAsync(sp, x->p, pb, cudaMemcpyDeviceToDevice, x->stream));
+  CUDA_TRY(cudaMemcpyAsync(sf, x->pflag, sizeof(int) * nz, cudaMemcpyDeviceToDevice, x->stream));
+  CUDA_TRY(cudaMemcpyAsync(ss, x->sc, sizeof(Scalars), cudaMemcpyDeviceToDevice, x->stream));
+  if (fv) CUDA_TRY(cudaMemcpyAsync(su, x->ucum, pb, cudaMemcpyDeviceToDevice, x->stream));
+  auto restore = [&]() {
+    cudaMemcpyAsync(x->p, sp, pb, cudaMemcpyDeviceToDevice, x->stream);
+    cudaMemcpyAsync(x->pflag, sf, sizeof(int) * nz, cudaMemcpyDeviceToDevice, x->stream);
+    cudaMemcpyAsync(x->sc, ss, sizeof(Scalars), cudaMemcpyDeviceToDevice, x->stream);
+    if (fv) cudaMemcpyAsync(x->ucum, su, pb, cudaMemcpyDeviceToDevice, x->stream);
+  };
+  auto one_step = [&]() {
+    clear_counters(x);
+    for (int o = 0; o < num_orders(x); o++) launch_stage(x, o);
+    launch_finalize(x, 1);
+  };
+  const bool fp64 = x->cfg.precision == HGPU_PREC_FP64;
+  int *knob[4] = {&x->tune.flux, &x->tune.weno_b, &x->tune.conserve, &x->tune.invert};
+  const bool applies[4] = {fp64, fp64 && x->P.lim == HGPU_LIM_WENO5, true, true};
+  const int kids[4][3] = {{K_FLUX1, K_FLUX2, K_FLUX3}, {K_WENO_B, -1, -1}, {K_UPDATE, -1, -1}, {K_INVERT, -1, -1}};
+  float ms[4][2] = {{0.f, 0.f}, {0.f, 0.f}, {0.f, 0.f}, {0.f, 0.f}};
+  int rc = HGPU_OK;
+  x->profiling = true;
+  for (int f = 0; f < 4 && !rc; f++) {
+    if (!applies[f]) continue;
+    for (int v = 0; v < 2 && !rc; v++) {
+      *knob[f] = v;
+      for (int rep = 0; rep < 2; rep++) {
+        restore();
+        one_step();
+        if (cudaStreamSynchronize(x->stream) != cudaSuccess || cudaGetLastError() != cudaSuccess) {
+          rc = HGPU_E_CUDA;
+          break;
+        }
+        collect_profile(x);
+        double t = 0.0;
+        for (int q = 0; q < 3; q++)
+          if (kids[f][q] >= 0) t += x->kms[kids[f][q]];
+        if (rep == 1) ms[f][v] = (float)t;
+        for (int k = 0; k < K_NKERNELS; k++) {
+          x->kms[k] = 0.0;
+          x->kcount[k] = 0;
+        }
+      }
+    }
+    *knob[f] = (ms[f][1] < ms[f][0]) ? 1 : 0;
+  }
+  x->profiling = false;
+  restore();
+  cudaFreeAsync(sp, x->stream);
+  cudaFreeAsync(sf, x->stream);
+  cudaFreeAsync(ss, x->stream);
+  if (su) cudaFreeAsync(su, x->stream);
+  CUDA_TRY(cudaStreamSynchronize(x->stream));
+  // the captured step holds the old variants
+  if (x->graph_exec) cudaGraphExecDestroy(x->graph_exec);
+  if (x->graph) cudaGraphDestroy(x->graph);
+  x->graph_exec = nullptr;
+  x->graph = nullptr;
+  if (out) {
+    out->flux_minb = kFluxMB[x->tune.flux];
+    out->weno_b_minb = kWenoBMB[x->tune.weno_b];
+    out->update_minb = kConserveMB[x->tune.conserve];
+    out->invert_minb = kInvertMB[x->tune.invert];
+    for (int v = 0; v < 2; v++) {
+      out->flux_ms[v] = ms[0][v];
+      out->weno_b_ms[v] = ms[1][v];
+      out->update_ms[v] = ms[2][v];
+      out->invert_ms[v] = ms[3][v];
+      out->flux_cand[v] = kFluxMB[v];
+      out->weno_b_cand[v] = kWenoBMB[v];
+      out->update_cand[v] = kConserveMB[v];
+      out->invert_cand[v] = kInvertMB[v];
+    }
+  }
+  return rc;
 }
 
 int hgpu_set_profiling(hgpu_ctx *x, int on) {

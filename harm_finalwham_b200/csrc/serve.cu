@@ -51,13 +51,14 @@ struct Request {
   long long id = 0;
   hgpu_config cfg;
   std::vector<double> gcov, gcon, gcovpert, gdet, conn, floors, p;
+  const double *src[7] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};  // borrowed inputs
   double tf = 0.0;
   int state = PENDING;
   size_t bytes = 0;
   hgpu_ctx *ctx = nullptr;
-  double *prog = nullptr;  // pinned: t, dt, done, steps
-  cudaEvent_t ev = nullptr;
-  bool in_flight = false;
+  double *prog = nullptr;  // pinned, one slot per chunk in flight: t, dt, done, steps
+  cudaEvent_t ev[2] = {nullptr, nullptr};
+  long long issued = 0, noticed = 0;  // chunks issued / seen complete
   long long steps = 0;
   Clock::time_point t_submit, t_admit, t_finish;
   std::vector<double> p_out;
@@ -65,6 +66,10 @@ struct Request {
   double t_out = 0.0;
   int rc = 0;
 };
+
+// chunks kept in flight per solve: the next one is queued behind the
+// running one, so the solve's stream never waits for the host to notice
+constexpr int DEPTH = 2;
 
 size_t zone_count(const hgpu_config &c, int ng_ghosts) {
   auto tot = [&](int n) { return (size_t)(n > 1 ? n + 2 * ng_ghosts : 1); };
@@ -78,11 +83,11 @@ size_t geom_count(const hgpu_config &c) {
 
 }  // namespace
 
-// an idle context kept for reuse, with its progress word and event
+// an idle context kept for reuse, with its progress words and events
 struct Slot {
   hgpu_ctx *ctx = nullptr;
   double *prog = nullptr;
-  cudaEvent_t ev = nullptr;
+  cudaEvent_t ev[2] = {nullptr, nullptr};
   hgpu_config cfg;
   size_t bytes = 0;
 };
@@ -98,10 +103,11 @@ struct hgpu_server {
 
 static void destroy_slot(Slot &q) {
   if (q.ctx) hgpu_destroy(q.ctx);
-  if (q.ev) cudaEventDestroy(q.ev);
+  for (int e = 0; e < DEPTH; e++)
+    if (q.ev[e]) cudaEventDestroy(q.ev[e]);
   if (q.prog) cudaFreeHost(q.prog);
   q.ctx = nullptr;
-  q.ev = nullptr;
+  q.ev[0] = q.ev[1] = nullptr;
   q.prog = nullptr;
 }
 
@@ -109,10 +115,11 @@ static void release_device(hgpu_server *s, Request *r) {
   Slot q;
   q.ctx = r->ctx;
   q.prog = r->prog;
-  q.ev = r->ev;
+  q.ev[0] = r->ev[0];
+  q.ev[1] = r->ev[1];
   destroy_slot(q);
   r->ctx = nullptr;
-  r->ev = nullptr;
+  r->ev[0] = r->ev[1] = nullptr;
   r->prog = nullptr;
   if (r->state == ACTIVE) {
     s->used -= r->bytes;
@@ -125,12 +132,13 @@ static void park(hgpu_server *s, Request *r) {
   Slot q;
   q.ctx = r->ctx;
   q.prog = r->prog;
-  q.ev = r->ev;
+  q.ev[0] = r->ev[0];
+  q.ev[1] = r->ev[1];
   q.cfg = r->cfg;
   q.bytes = r->bytes;
   r->ctx = nullptr;
   r->prog = nullptr;
-  r->ev = nullptr;
+  r->ev[0] = r->ev[1] = nullptr;
   s->used -= r->bytes;
   s->active--;
   s->idle.push_back(q);
@@ -152,7 +160,8 @@ static int admit(hgpu_server *s, Request *r) {
     s->idle_bytes -= q.bytes;
     r->ctx = q.ctx;
     r->prog = q.prog;
-    r->ev = q.ev;
+    r->ev[0] = q.ev[0];
+    r->ev[1] = q.ev[1];
     rc = hg_reconfigure(r->ctx, &r->cfg);
   } else {
     while (!s->idle.empty() && s->used + s->idle_bytes + r->bytes > s->max_bytes) {
@@ -161,12 +170,17 @@ static int admit(hgpu_server *s, Request *r) {
       s->idle.erase(s->idle.begin());
     }
     rc = hgpu_create(&r->cfg, &r->ctx);
-    if (!rc && cudaMallocHost(&r->prog, 4 * sizeof(double)) != cudaSuccess) rc = HGPU_E_NOMEM;
-    if (!rc && cudaEventCreateWithFlags(&r->ev, cudaEventDisableTiming) != cudaSuccess) rc = HGPU_E_CUDA;
+    if (!rc && cudaMallocHost(&r->prog, 4 * DEPTH * sizeof(double)) != cudaSuccess) rc = HGPU_E_NOMEM;
+    for (int e = 0; e < DEPTH && !rc; e++)
+      if (cudaEventCreateWithFlags(&r->ev[e], cudaEventDisableTiming) != cudaSuccess) rc = HGPU_E_CUDA;
   }
-  if (!rc) rc = hgpu_upload_geometry(r->ctx, r->gcov.data(), r->gcon.data(), r->gcovpert.data(), r->gdet.data(),
-                                     r->conn.data(), r->floors.data());
-  if (!rc) rc = hgpu_upload_state(r->ctx, r->p.data(), nullptr, 0.0, 0.0);
+  const bool own = r->src[0] == nullptr;
+  if (!rc)
+    rc = hgpu_upload_geometry(r->ctx, own ? r->gcov.data() : r->src[0], own ? r->gcon.data() : r->src[1],
+                              own ? r->gcovpert.data() : r->src[2], own ? r->gdet.data() : r->src[3],
+                              own ? r->conn.data() : r->src[4], own ? r->floors.data() : r->src[5]);
+  if (!rc) rc = hgpu_upload_state(r->ctx, own ? r->p.data() : r->src[6], nullptr, 0.0, 0.0);
+  for (int q = 0; q < 7; q++) r->src[q] = nullptr;
   if (!rc) rc = hgpu_init_dt(r->ctx, nullptr);
   r->state = ACTIVE;
   s->used += r->bytes;
@@ -192,8 +206,9 @@ static int admit(hgpu_server *s, Request *r) {
 static void issue_chunk(hgpu_server *s, Request *r) {
   // a chunk is `chunk` replays of the request's captured time step (one graph
   // launch per step instead of one launch per kernel)
+  const int slot = (int)(r->issued % DEPTH);
   int rc = hgpu_step_graph(r->ctx, s->chunk, nullptr);
-  if (!rc) rc = hg_progress_async(r->ctx, r->prog, r->ev);
+  if (!rc) rc = hg_progress_async(r->ctx, r->prog + 4 * slot, r->ev[slot]);
   if (rc) {
     r->rc = rc;
     release_device(s, r);
@@ -201,7 +216,7 @@ static void issue_chunk(hgpu_server *s, Request *r) {
     r->t_finish = Clock::now();
     return;
   }
-  r->in_flight = true;
+  r->issued++;
 }
 
 static void retire(hgpu_server *s, Request *r) {
@@ -241,9 +256,9 @@ void hgpu_server_destroy(hgpu_server *s) {
   delete s;
 }
 
-int hgpu_server_submit(hgpu_server *s, const hgpu_config *cfg, const double *gcov, const double *gcon,
-                       const double *gcovpert, const double *gdet, const double *conn, const double *floors,
-                       const double *p, double tf, long long *id) {
+static int submit_common(hgpu_server *s, const hgpu_config *cfg, const double *gcov, const double *gcon,
+                         const double *gcovpert, const double *gdet, const double *conn, const double *floors,
+                         const double *p, double tf, long long *id, bool borrow) {
   if (!s || !cfg || !gcov || !gcon || !gcovpert || !gdet || !conn || !floors || !p || !id) return HGPU_E_INVALID;
   size_t bytes = hgpu_context_bytes(cfg);
   if (bytes == 0 || bytes > s->max_bytes) return HGPU_E_INVALID;
@@ -252,20 +267,37 @@ int hgpu_server_submit(hgpu_server *s, const hgpu_config *cfg, const double *gco
   r->cfg.tf = tf;
   r->tf = tf;
   r->bytes = bytes;
-  size_t nz = zone_count(*cfg, cfg->ng), nij = geom_count(*cfg);
-  r->gcov.assign(gcov, gcov + nij * 128);
-  r->gcon.assign(gcon, gcon + nij * 128);
-  r->gcovpert.assign(gcovpert, gcovpert + nij * 32);
-  r->gdet.assign(gdet, gdet + nij * 8);
-  r->conn.assign(conn, conn + nij * 64);
-  r->floors.assign(floors, floors + nij * 2);
-  r->p.assign(p, p + nz * 8);
+  if (borrow) {
+    const double *a[7] = {gcov, gcon, gcovpert, gdet, conn, floors, p};
+    for (int q = 0; q < 7; q++) r->src[q] = a[q];
+  } else {
+    size_t nz = zone_count(*cfg, cfg->ng), nij = geom_count(*cfg);
+    r->gcov.assign(gcov, gcov + nij * 128);
+    r->gcon.assign(gcon, gcon + nij * 128);
+    r->gcovpert.assign(gcovpert, gcovpert + nij * 32);
+    r->gdet.assign(gdet, gdet + nij * 8);
+    r->conn.assign(conn, conn + nij * 64);
+    r->floors.assign(floors, floors + nij * 2);
+    r->p.assign(p, p + nz * 8);
+  }
   r->t_submit = Clock::now();
   std::lock_guard<std::mutex> g(s->m);
   r->id = s->next_id++;
   s->reqs[r->id] = r;
   *id = r->id;
   return HGPU_OK;
+}
+
+int hgpu_server_submit(hgpu_server *s, const hgpu_config *cfg, const double *gcov, const double *gcon,
+                       const double *gcovpert, const double *gdet, const double *conn, const double *floors,
+                       const double *p, double tf, long long *id) {
+  return submit_common(s, cfg, gcov, gcon, gcovpert, gdet, conn, floors, p, tf, id, false);
+}
+
+int hgpu_server_submit_borrowed(hgpu_server *s, const hgpu_config *cfg, const double *gcov, const double *gcon,
+                                const double *gcovpert, const double *gdet, const double *conn,
+                                const double *floors, const double *p, double tf, long long *id) {
+  return submit_common(s, cfg, gcov, gcon, gcovpert, gdet, conn, floors, p, tf, id, true);
 }
 
 int hgpu_server_poll(hgpu_server *s, int *pending, int *active, int *finished) {
@@ -275,24 +307,35 @@ int hgpu_server_poll(hgpu_server *s, int *pending, int *active, int *finished) {
   for (auto &kv : s->reqs) {
     Request *r = kv.second;
     if (r->state != ACTIVE) continue;
-    if (r->in_flight) {
-      cudaError_t e = cudaEventQuery(r->ev);
-      if (e == cudaErrorNotReady) continue;
-      r->in_flight = false;
+    bool finished = false, failed = false;
+    while (r->noticed < r->issued) {
+      const int slot = (int)(r->noticed % DEPTH);
+      cudaError_t e = cudaEventQuery(r->ev[slot]);
+      if (e == cudaErrorNotReady) break;
       if (e != cudaSuccess) {
-        r->rc = HGPU_E_CUDA;
-        release_device(s, r);
-        r->state = FAILED;
-        r->t_finish = Clock::now();
-        continue;
+        failed = true;
+        break;
       }
-      r->steps = (long long)r->prog[3];
-      if (r->prog[2] != 0.0) {
-        retire(s, r);
-        continue;
+      r->noticed++;
+      r->steps = (long long)r->prog[4 * slot + 3];
+      if (r->prog[4 * slot + 2] != 0.0) {
+        finished = true;
+        break;
       }
     }
-    issue_chunk(s, r);
+    if (failed) {
+      r->rc = HGPU_E_CUDA;
+      release_device(s, r);
+      r->state = FAILED;
+      r->t_finish = Clock::now();
+      continue;
+    }
+    // a finished solve is frozen: chunks still queued behind leave it as it is
+    if (finished) {
+      retire(s, r);
+      continue;
+    }
+    while (r->state == ACTIVE && r->issued - r->noticed < DEPTH) issue_chunk(s, r);
   }
   // 2. admit pending requests first-fit in arrival order
   for (auto &kv : s->reqs) {
@@ -300,7 +343,8 @@ int hgpu_server_poll(hgpu_server *s, int *pending, int *active, int *finished) {
     if (r->state != PENDING) continue;
     if (s->active >= s->max_active) break;
     if (s->used + r->bytes > s->max_bytes) continue;
-    if (admit(s, r) == HGPU_OK) issue_chunk(s, r);
+    if (admit(s, r) == HGPU_OK)
+      while (r->state == ACTIVE && r->issued - r->noticed < DEPTH) issue_chunk(s, r);
   }
   int np = 0, na = 0, nf = 0;
   for (auto &kv : s->reqs) {

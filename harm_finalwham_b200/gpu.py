@@ -42,6 +42,12 @@ class hgpu_config(ctypes.Structure):
                 ("utoprimversion", ctypes.c_int), ("doenoflux", ctypes.c_int)]
 
 
+class hgpu_tuning(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_int) for n in ("flux_minb", "weno_b_minb", "update_minb", "invert_minb")] + \
+               [(n, ctypes.c_int * 2) for n in ("flux_cand", "weno_b_cand", "update_cand", "invert_cand")] + \
+               [(n, ctypes.c_float * 2) for n in ("flux_ms", "weno_b_ms", "update_ms", "invert_ms")]
+
+
 class hgpu_diag(ctypes.Structure):
     _fields_ = [("t", ctypes.c_double), ("dt", ctypes.c_double), ("integral", ctypes.c_double * 8),
                 ("divb_max", ctypes.c_double), ("divb_avg", ctypes.c_double), ("nfail", ctypes.c_int),
@@ -99,6 +105,7 @@ def load_library(path=None):
     L.hgpu_batch_layout.argtypes = [ctypes.c_void_p, _ip]
     L.hgpu_batch_status.argtypes = [ctypes.c_void_p, _dp, _dp, _ip, _ip]
     L.hgpu_step_graph.argtypes = [ctypes.c_void_p, ctypes.c_int, _P(hgpu_stats)]
+    L.hgpu_autotune.argtypes = [ctypes.c_void_p, _P(hgpu_tuning)]
     L.hgpu_diagnostics.argtypes = [ctypes.c_void_p, _P(hgpu_diag)]
     L.hgpu_download_conserved.argtypes = [ctypes.c_void_p, _dp]
     L.hgpu_upload_conserved.argtypes = [ctypes.c_void_p, _dp]
@@ -109,6 +116,7 @@ def load_library(path=None):
     L.hgpu_server_destroy.restype = None
     L.hgpu_server_submit.argtypes = [ctypes.c_void_p, _P(hgpu_config)] + [_dp] * 7 + [ctypes.c_double,
                                                                                        _P(ctypes.c_longlong)]
+    L.hgpu_server_submit_borrowed.argtypes = L.hgpu_server_submit.argtypes
     L.hgpu_server_poll.argtypes = [ctypes.c_void_p, _ip, _ip, _ip]
     L.hgpu_server_result.argtypes = [ctypes.c_void_p, ctypes.c_longlong, _dp, _ip, _dp, _P(ctypes.c_longlong), _dp,
                                      _dp]
@@ -121,7 +129,7 @@ def load_library(path=None):
     for name in ("hgpu_create", "hgpu_upload_geometry", "hgpu_upload_state", "hgpu_download_state", "hgpu_step_ch",
                  "hgpu_advance_stage", "hgpu_fluxcalc", "hgpu_bound_prim", "hgpu_utoprim_batch", "hgpu_utoprimgen_batch",
                  "hgpu_device_prims", "hgpu_sync", "hgpu_create_batch", "hgpu_batch_layout", "hgpu_batch_status",
-                 "hgpu_step_graph", "hgpu_batch_run", "hgpu_diagnostics", "hgpu_download_conserved", "hgpu_upload_conserved", "hgpu_server_create", "hgpu_server_submit",
+                 "hgpu_step_graph", "hgpu_autotune", "hgpu_batch_run", "hgpu_diagnostics", "hgpu_download_conserved", "hgpu_upload_conserved", "hgpu_server_create", "hgpu_server_submit", "hgpu_server_submit_borrowed",
                  "hgpu_server_poll", "hgpu_server_result", "hgpu_server_release"):
         getattr(L, name).restype = ctypes.c_int
     if path == _build.LIB:
@@ -272,6 +280,18 @@ class HarmGPU:
         st = hgpu_stats()
         _check(self.L, self.L.hgpu_step_graph(self.h, int(nsteps), ctypes.byref(st) if stats else None))
         return st
+
+    def autotune(self):
+        """hgpu_autotune: pick the resident-block variant of each heavy FP64
+        kernel on this state; returns {family: {"minb": chosen, "ms": {candidate: ms}}}."""
+        tu = hgpu_tuning()
+        _check(self.L, self.L.hgpu_autotune(self.h, ctypes.byref(tu)))
+        out = {}
+        for fam in ("flux", "weno_b", "update", "invert"):
+            cand = list(getattr(tu, fam + "_cand"))
+            ms = list(getattr(tu, fam + "_ms"))
+            out[fam] = {"minb": getattr(tu, fam + "_minb"), "ms": {str(c): round(m, 4) for c, m in zip(cand, ms)}}
+        return out
 
     def advance_stage(self, timeorder):
         st = hgpu_stats()
@@ -482,9 +502,12 @@ class HarmServer:
                                                  ctypes.byref(h)))
         self.h = h
         self.shapes = {}
+        self._held = {}
 
-    def submit(self, dom, tf, precision="fp64"):
-        """dom: an object with the Domain/Problem attributes (n, ng, dx, lim, ...)."""
+    def submit(self, dom, tf, precision="fp64", borrow=True):
+        """dom: an object with the Domain/Problem attributes (n, ng, dx, lim, ...).
+        borrow: the server reads dom's arrays at admission instead of copying
+        them now (they are held here until the result is released)."""
         inv_bc = {v: k for k, v in BC.items()}
         bc = tuple(inv_bc[b] if not isinstance(b, str) else b for b in dom.bc)
         c = make_config(dom.n, dom.ng, dom.dx, lim=dom.lim, flux=dom.flux, bc=bc, precision=precision, gam=dom.gam,
@@ -493,9 +516,11 @@ class HarmServer:
         arrs = [_contig(a, np.float64) for a in (dom.gcov, dom.gcon, dom.gcovpert, dom.gdet, dom.conn, dom.floors,
                                                  dom.p)]
         rid = ctypes.c_longlong()
-        _check(self.L, self.L.hgpu_server_submit(self.h, ctypes.byref(c), *[_ptr(a) for a in arrs], float(tf),
-                                                 ctypes.byref(rid)))
+        fn = self.L.hgpu_server_submit_borrowed if borrow else self.L.hgpu_server_submit
+        _check(self.L, fn(self.h, ctypes.byref(c), *[_ptr(a) for a in arrs], float(tf), ctypes.byref(rid)))
         self.shapes[rid.value] = dom.p.shape
+        if borrow:
+            self._held[rid.value] = arrs
         return rid.value
 
     def poll(self):
@@ -506,20 +531,24 @@ class HarmServer:
     def result(self, rid):
         """(p, pflag, t, steps, queue_ms, run_ms) of a finished solve, or None while it runs."""
         shape = self.shapes[rid]
-        p = np.empty(shape)
-        pf = np.empty(shape[:-1], dtype=np.int32)
         t, q, r = ctypes.c_double(), ctypes.c_double(), ctypes.c_double()
         steps = ctypes.c_longlong()
-        rc = self.L.hgpu_server_result(self.h, rid, _ptr(p), _ptr(pf, ctypes.c_int), ctypes.byref(t),
-                                       ctypes.byref(steps), ctypes.byref(q), ctypes.byref(r))
+        # a cheap check first: no arrays while the solve runs
+        rc = self.L.hgpu_server_result(self.h, rid, None, None, ctypes.byref(t), ctypes.byref(steps),
+                                       ctypes.byref(q), ctypes.byref(r))
         if rc == 1:  # HGPU_E_INVALID: not finished
             return None
         _check(self.L, rc)
+        p = np.empty(shape)
+        pf = np.empty(shape[:-1], dtype=np.int32)
+        _check(self.L, self.L.hgpu_server_result(self.h, rid, _ptr(p), _ptr(pf, ctypes.c_int), ctypes.byref(t),
+                                                 ctypes.byref(steps), ctypes.byref(q), ctypes.byref(r)))
         return p, pf, t.value, steps.value, q.value, r.value
 
     def release(self, rid):
         _check(self.L, self.L.hgpu_server_release(self.h, rid))
         self.shapes.pop(rid, None)
+        self._held.pop(rid, None)
 
     def close(self):
         if getattr(self, "h", None):

@@ -33,7 +33,7 @@
 extern "C" {
 #endif
 
-#define HGPU_ABI_VERSION 4
+#define HGPU_ABI_VERSION 5
 
 /* return codes */
 #define HGPU_OK 0
@@ -207,6 +207,20 @@ int hgpu_batch_run(hgpu_ctx *ctx, int check_every, int max_steps, int *steps, fl
    hgpu_step_ch. */
 int hgpu_step_graph(hgpu_ctx *ctx, int nsteps, hgpu_stats *stats);
 
+/* Autotuner (no counterpart in the reference): for the FP64 flux, weno_b,
+   update and inversion kernels, times two resident-blocks-per-SM variants
+   (registers per thread vs warps per SM) on this context's own state and
+   keeps the faster for later steps.  Results do not depend on the choice;
+   the state is left as it was.  *_ms: kernel milliseconds of one step per
+   candidate (0 where a family does not apply: weno_b without WENO5, flux and
+   weno_b in the mixed-precision mode). */
+typedef struct {
+  int flux_minb, weno_b_minb, update_minb, invert_minb;
+  int flux_cand[2], weno_b_cand[2], update_cand[2], invert_cand[2];
+  float flux_ms[2], weno_b_ms[2], update_ms[2], invert_ms[2];
+} hgpu_tuning;
+int hgpu_autotune(hgpu_ctx *ctx, hgpu_tuning *out);
+
 /* Diagnostics of the current state (the quantities dump_ener.c writes to
    ener.out, computed on the device): integral[pl] = sum over active zones of
    the conserved U (primtoU with gdet, UU without rest mass) times
@@ -259,6 +273,12 @@ void hgpu_server_destroy(hgpu_server *srv);
 int hgpu_server_submit(hgpu_server *srv, const hgpu_config *cfg, const double *gcov, const double *gcon,
                        const double *gcovpert, const double *gdet, const double *conn, const double *floors,
                        const double *p, double tf, long long *id);
+/* The same without copying: the server reads the caller's arrays when it
+   admits the solve, so they must stay valid and unchanged until
+   hgpu_server_poll no longer counts the solve as pending. */
+int hgpu_server_submit_borrowed(hgpu_server *srv, const hgpu_config *cfg, const double *gcov, const double *gcon,
+                                const double *gcovpert, const double *gdet, const double *conn,
+                                const double *floors, const double *p, double tf, long long *id);
 int hgpu_server_poll(hgpu_server *srv, int *pending, int *active, int *finished);
 /* result of a finished solve (HGPU_E_INVALID while it runs); arrays in the layouts above */
 int hgpu_server_result(hgpu_server *srv, long long id, double *p, int *pflag, double *t, long long *steps,
