@@ -56,11 +56,13 @@ WORKLOADS = {
     # all MAXBND=11 ghosts (its flux and dt loops cover them)
     "torus3d_256x128x128_fishmon": (256, 128, 128, "PARA", "HLL"),
     "torus3d_128x64x32_fishmon": (128, 64, 32, "PARA", "HLL"),
+    "torus3d_256x128x64_fishmon": (256, 128, 64, "PARA", "HLL"),
 }
 # scheme settings beyond the 2D Noble / midpoint / standard-update default
 SCHEMES = {
     "torus3d_256x128x128_fishmon": {"timeorder": 4, "utoprim": "JON", "doenoflux": "ENOFINITEVOLUME", "ng": 11},
     "torus3d_128x64x32_fishmon": {"timeorder": 4, "utoprim": "JON", "doenoflux": "ENOFINITEVOLUME", "ng": 11},
+    "torus3d_256x128x64_fishmon": {"timeorder": 4, "utoprim": "JON", "doenoflux": "ENOFINITEVOLUME", "ng": 11},
 }
 DEFAULT_WORKLOAD = "torus3d_256x128x128"
 # ghost zones kept on the device: MC reads 2 per side, PARA 3, WENO5 6 (the
@@ -246,7 +248,12 @@ def bench_ours(args, rank, world):
     g.upload_geometry(dom.gcov, dom.gcon, dom.gcovpert, dom.gdet, dom.conn, dom.floors)
     g.upload_state(dom.p, dom.pflag, 0.0, 0.0)
     dt0 = g.init_dt()
-    tuning = g.autotune()
+    if args.tuning:
+        # a known choice (e.g. for profiler runs that should not see the trials)
+        tuning = dict(zip(("flux", "weno_b", "update", "invert"), (int(v) for v in args.tuning.split(","))))
+        g.set_tuning(tuning)
+    else:
+        tuning = g.autotune()
 
     dist = None
     if world > 1:
@@ -296,7 +303,8 @@ def bench_ours(args, rank, world):
         g2.upload_geometry(dom.gcov, dom.gcon, dom.gcovpert, dom.gdet, dom.conn, dom.floors)
         g2.upload_state(dom.p, dom.pflag, 0.0, 0.0)
         g2.init_dt()
-        g2.autotune()
+        if not args.tuning:
+            g2.autotune()
         g2.step_ch(args.warmup)
         barrier()
         ms2, st2 = g2.step_ch_timed(args.steps)
@@ -654,6 +662,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-steps", type=int, default=3)
     ap.add_argument("--cpu-procs", type=int, default=16)
+    ap.add_argument("--tuning", default=None,
+                    help="blocks per SM for flux,weno_b,update,invert instead of running the autotuner")
     ap.add_argument("--kernels-only", action="store_true",
                     help="set-up, warm-up and the timed steps only (for profiler runs)")
     args = ap.parse_args()

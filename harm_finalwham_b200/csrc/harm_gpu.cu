@@ -2154,6 +2154,25 @@ int hgpu_autotune(hgpu_ctx *x, hgpu_tuning *out) {
   return rc;
 }
 
+// apply a known choice (e.g. from an earlier hgpu_autotune of the same shape)
+int hgpu_set_tuning(hgpu_ctx *x, const hgpu_tuning *t) {
+  if (!x || !t) return HGPU_E_INVALID;
+  auto pick = [](const int *cand, int minb) { return cand[1] == minb ? 1 : (cand[0] == minb ? 0 : -1); };
+  const int f = pick(kFluxMB, t->flux_minb), b = pick(kWenoBMB, t->weno_b_minb);
+  const int u = pick(kConserveMB, t->update_minb), v = pick(kInvertMB, t->invert_minb);
+  if (f < 0 || b < 0 || u < 0 || v < 0) return HGPU_E_INVALID;
+  CUDA_TRY(cudaStreamSynchronize(x->stream));
+  x->tune.flux = f;
+  x->tune.weno_b = b;
+  x->tune.conserve = u;
+  x->tune.invert = v;
+  if (x->graph_exec) cudaGraphExecDestroy(x->graph_exec);
+  if (x->graph) cudaGraphDestroy(x->graph);
+  x->graph_exec = nullptr;
+  x->graph = nullptr;
+  return HGPU_OK;
+}
+
 int hgpu_set_profiling(hgpu_ctx *x, int on) {
   if (!x) return HGPU_E_INVALID;
   CUDA_TRY(cudaStreamSynchronize(x->stream));

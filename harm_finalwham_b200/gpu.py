@@ -106,6 +106,7 @@ def load_library(path=None):
     L.hgpu_batch_status.argtypes = [ctypes.c_void_p, _dp, _dp, _ip, _ip]
     L.hgpu_step_graph.argtypes = [ctypes.c_void_p, ctypes.c_int, _P(hgpu_stats)]
     L.hgpu_autotune.argtypes = [ctypes.c_void_p, _P(hgpu_tuning)]
+    L.hgpu_set_tuning.argtypes = [ctypes.c_void_p, _P(hgpu_tuning)]
     L.hgpu_diagnostics.argtypes = [ctypes.c_void_p, _P(hgpu_diag)]
     L.hgpu_download_conserved.argtypes = [ctypes.c_void_p, _dp]
     L.hgpu_upload_conserved.argtypes = [ctypes.c_void_p, _dp]
@@ -129,7 +130,7 @@ def load_library(path=None):
     for name in ("hgpu_create", "hgpu_upload_geometry", "hgpu_upload_state", "hgpu_download_state", "hgpu_step_ch",
                  "hgpu_advance_stage", "hgpu_fluxcalc", "hgpu_bound_prim", "hgpu_utoprim_batch", "hgpu_utoprimgen_batch",
                  "hgpu_device_prims", "hgpu_sync", "hgpu_create_batch", "hgpu_batch_layout", "hgpu_batch_status",
-                 "hgpu_step_graph", "hgpu_autotune", "hgpu_batch_run", "hgpu_diagnostics", "hgpu_download_conserved", "hgpu_upload_conserved", "hgpu_server_create", "hgpu_server_submit", "hgpu_server_submit_borrowed",
+                 "hgpu_step_graph", "hgpu_autotune", "hgpu_set_tuning", "hgpu_batch_run", "hgpu_diagnostics", "hgpu_download_conserved", "hgpu_upload_conserved", "hgpu_server_create", "hgpu_server_submit", "hgpu_server_submit_borrowed",
                  "hgpu_server_poll", "hgpu_server_result", "hgpu_server_release"):
         getattr(L, name).restype = ctypes.c_int
     if path == _build.LIB:
@@ -292,6 +293,13 @@ class HarmGPU:
             ms = list(getattr(tu, fam + "_ms"))
             out[fam] = {"minb": getattr(tu, fam + "_minb"), "ms": {str(c): round(m, 4) for c, m in zip(cand, ms)}}
         return out
+
+    def set_tuning(self, minb):
+        """hgpu_set_tuning: {"flux": 4, "weno_b": 8, "update": 3, "invert": 1} (blocks per SM)."""
+        tu = hgpu_tuning()
+        tu.flux_minb, tu.weno_b_minb = int(minb["flux"]), int(minb["weno_b"])
+        tu.update_minb, tu.invert_minb = int(minb["update"]), int(minb["invert"])
+        _check(self.L, self.L.hgpu_set_tuning(self.h, ctypes.byref(tu)))
 
     def advance_stage(self, timeorder):
         st = hgpu_stats()

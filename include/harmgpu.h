@@ -220,6 +220,9 @@ typedef struct {
   float flux_ms[2], weno_b_ms[2], update_ms[2], invert_ms[2];
 } hgpu_tuning;
 int hgpu_autotune(hgpu_ctx *ctx, hgpu_tuning *out);
+/* Apply a choice found before (the *_minb fields; each must be one of the
+   candidates that hgpu_autotune reports), without timing anything. */
+int hgpu_set_tuning(hgpu_ctx *ctx, const hgpu_tuning *t);
 
 /* Diagnostics of the current state (the quantities dump_ener.c writes to
    ener.out, computed on the device): integral[pl] = sum over active zones of
