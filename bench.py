@@ -219,6 +219,22 @@ def run_reference(sample, steps, warmup, procs):
     return sum(zu / (e - s) for s, e in spans), None
 
 
+def replica_max(v, dist=None, device="cuda"):
+    """Max over ranks of a per-rank value (the timed region's device ms):
+    replicas advance independent tori, so the job's time is the slowest."""
+    if dist is None:
+        return v
+    import torch
+    t = torch.tensor([v], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def replica_value(zones, steps, world, ms_max):
+    """Whole-job zone-updates/s: every rank's zones over the slowest rank's time."""
+    return zones * steps * world / (ms_max / 1e3)
+
+
 def host_cores():
     try:
         return len(os.sched_getaffinity(0))
@@ -267,12 +283,7 @@ def bench_ours(args, rank, world):
             dist.barrier()
 
     def allmax(v):
-        if dist is None:
-            return v
-        import torch
-        t = torch.tensor([v], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+        return replica_max(v, dist, "cuda")
 
     # warm-up
     g.step_ch(args.warmup)
@@ -286,7 +297,7 @@ def bench_ours(args, rank, world):
     barrier()
     ms_max = allmax(ms)
     zones = n1 * n2 * n3
-    value = zones * args.steps * world / (ms_max / 1e3)
+    value = replica_value(zones, args.steps, world, ms_max)
     if args.kernels_only:
         g.close()
         return {"metric": METRIC, "value": value, "unit": "zone-updates/s", "note": "kernels-only run",
@@ -621,7 +632,7 @@ def fp64_roof(kt, kernel, args):
     """FP64 rate of the dominant kernel from the per-launch FP64 operation count
     measured with ncu (profiles/traffic.md) vs the FP64 peak measured here."""
     r = _traffic_row(args.workload, kernel)
-    if not r:
+    if not r or r[1] <= 0:
         return None
     ops_per_launch = r[1]
     avg_s = kt["ms"] / kt["launches"] / 1e3
