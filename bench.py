@@ -264,6 +264,7 @@ def bench_ours(args, rank, world):
     g.upload_geometry(dom.gcov, dom.gcon, dom.gcovpert, dom.gdet, dom.conn, dom.floors)
     g.upload_state(dom.p, dom.pflag, 0.0, 0.0)
     dt0 = g.init_dt()
+    diag0 = g.diagnostics()
     if args.tuning:
         # a known choice (e.g. for profiler runs that should not see the trials)
         tuning = dict(zip(("flux", "weno_b", "update", "invert"), (int(v) for v in args.tuning.split(","))))
@@ -308,6 +309,10 @@ def bench_ours(args, rank, world):
     other = None
     if not args.no_compare:
         other_prec = "mixed" if args.precision == "fp64" else "fp64"
+        # a longer comparison continues both runs untimed to --compare-steps
+        extra = max(0, args.compare_steps - (args.warmup + args.steps))
+        if extra:
+            g.step_ch(extra, stats=False)
         p_this, _, _, _ = g.download_state()
         g2 = HarmGPU(n1, n2, n3, dom.ng, dom.dx, lim=lim, flux=flux, precision=other_prec, gam=dom.gam, cour=dom.cour,
                      utoprim=sc["utoprim"], timeorder=sc["timeorder"], doenoflux=sc["doenoflux"])
@@ -321,16 +326,30 @@ def bench_ours(args, rank, world):
         ms2, st2 = g2.step_ch_timed(args.steps)
         barrier()
         ms2 = allmax(ms2)
+        if extra:
+            g2.step_ch(extra, stats=False)
         p_other, _, _, _ = g2.download_state()
+        diag_other = g2.diagnostics()
         g2.close()
+        diag_this = g.diagnostics()
         p64, p32 = (p_this, p_other) if args.precision == "fp64" else (p_other, p_this)
         a32, a64 = g.active(p32), g.active(p64)
         names = ["rho", "u", "u1", "u2", "u3", "B1", "B2", "B3"]
         err = {nm: float(np.abs(a32[..., q] - a64[..., q]).sum() / np.abs(a64[..., q]).sum())
                for q, nm in enumerate(names)}
+        d64, d32 = (diag_this, diag_other) if args.precision == "fp64" else (diag_other, diag_this)
+
+        def drift(dg, q):
+            a0 = diag0["integral"][q]
+            return (dg["integral"][q] - a0) / abs(a0) if a0 else None
+
+        cons = {prec: {"mass_drift": drift(dg, 0), "energy_drift": drift(dg, 1),
+                       "magnetic_flux_drift": [drift(dg, q) for q in (5, 6, 7)],
+                       "divb_max_interior": dg["divb_max_interior"], "failures_last_step": dg["nfail"]}
+                for prec, dg in (("fp64", d64), ("mixed", d32))}
         other = {"precision": other_prec, "value": zones * args.steps * world / (ms2 / 1e3),
-                 "ms_per_step": ms2 / args.steps, "steps_compared": args.warmup + args.steps,
-                 "rel_l1_mixed_vs_fp64": err,
+                 "ms_per_step": ms2 / args.steps, "steps_compared": args.warmup + args.steps + extra,
+                 "rel_l1_mixed_vs_fp64": err, "conservation": cons,
                  "note": "mixed = FP32 reconstruction, wave speeds and Riemann fluxes; FP64 flux-CT, conserved "
                          "update, con-to-prim and fixups; both runs from the same initial state"}
 
@@ -670,6 +689,8 @@ def main():
     ap.add_argument("--no-compare", action="store_true",
                     help="skip the run of the other precision mode (rate and error vs FP64)")
     ap.add_argument("--e2e-steps", type=int, default=5)
+    ap.add_argument("--compare-steps", type=int, default=0,
+                    help="steps of the FP64-vs-mixed comparison (default: warm-up + timed steps)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-steps", type=int, default=3)
     ap.add_argument("--cpu-procs", type=int, default=16)

@@ -71,7 +71,7 @@ struct Scalars {
   int overflow;
   int done;                        // t reached tf: later steps leave the state unchanged
   int nsteps;                      // time steps taken since the last upload
-  int nfloor;                      // zones raised to a floor by fixup1zone (per call)
+  unsigned long long nfloor;       // zone floorings by fixup1zone (summed over a call's final substeps)
 };
 
 __device__ __forceinline__ long long zix(const Dims &d, int i, int j, int k) {

@@ -410,7 +410,7 @@ __global__ void __launch_bounds__(128, MB) invert_kernel(Dims d, Params P, Box b
       if (fr > pr[RHO]) pr[RHO] = fr;
       if (fu > pr[UU]) pr[UU] = fu;
       const int lg = limit_gamma(P.gammamax, pr, m, &err);
-      if (floored) atomicAdd(&sc->nfloor, 1);
+      if (floored) atomicAdd(&sc->nfloor, 1ULL);
       // diag_fixup (fixup.c:443) when fixup1zone changed the primitives
       if (ufv && lg < 1 && (floored || lg == -1)) fv_diag_fixup(pr0, pr, m, gam, ufv, z, nz, &err);
     }
@@ -1707,7 +1707,7 @@ static void clear_counters(hgpu_ctx *x) {
   cudaMemsetAsync(&x->sc->err, 0, sizeof(int), x->stream);
   cudaMemsetAsync(&x->sc->nfixed, 0, sizeof(int), x->stream);
   cudaMemsetAsync(&x->sc->overflow, 0, sizeof(int), x->stream);
-  cudaMemsetAsync(&x->sc->nfloor, 0, sizeof(int), x->stream);
+  cudaMemsetAsync(&x->sc->nfloor, 0, sizeof(unsigned long long), x->stream);
 }
 
 int hgpu_step_ch(hgpu_ctx *x, int nsteps, hgpu_stats *stats) {
@@ -1907,7 +1907,8 @@ int hgpu_utoprimgen_batch(const double *U, const double *gcov, const double *gco
 // flux-CT div B of the reference's divbmaxavg (dump_ener.c:482-520), over
 // the active zones, with a deterministic two-pass reduction.
 // ---------------------------------------------------------------------------
-constexpr int DIAG_VALS = 11;  // 8 integrals, divb sum, divb max, failed zones
+constexpr int DIAG_VALS = 12;  // 8 integrals, divb sum, divb max, failed zones, interior divb max
+__device__ __forceinline__ bool diag_is_max(int q) { return q == 9 || q == 11; }
 constexpr int DIAG_BLOCK = 256;
 
 // DIVBFLUXCT (global.h:1586-1645) at the corner (i,j,k): B*gdet(CENT)
@@ -1966,6 +1967,12 @@ __global__ void __launch_bounds__(DIAG_BLOCK) diag_kernel(Dims d, Params P, Box 
     v[8] = db;
     v[9] = db;
     v[10] = (pflag[z] > 0) ? 1.0 : 0.0;
+    // corners constrained by flux-CT: x1 corners 1..n1-1, x2 corners
+    // 2..n2-2 (POLEDEATH resets B2 in the first and last rows, and gdet
+    // vanishes at the axis corners), all x3 corners
+    bool in1 = !d.s1 || (i >= 1 && i <= d.n1 - 1);
+    bool in2 = !d.s2 || (j >= 2 && j <= d.n2 - 2);
+    v[11] = (in1 && in2) ? db : 0.0;
   }
 #pragma unroll
   for (int q = 0; q < DIAG_VALS; q++) sh[q][threadIdx.x] = v[q];
@@ -1975,7 +1982,7 @@ __global__ void __launch_bounds__(DIAG_BLOCK) diag_kernel(Dims d, Params P, Box 
 #pragma unroll
       for (int q = 0; q < DIAG_VALS; q++) {
         double a = sh[q][threadIdx.x], b = sh[q][threadIdx.x + w];
-        sh[q][threadIdx.x] = (q == 9) ? max_ref(a, b) : a + b;
+        sh[q][threadIdx.x] = diag_is_max(q) ? max_ref(a, b) : a + b;
       }
     }
     __syncthreads();
@@ -1990,12 +1997,12 @@ __global__ void __launch_bounds__(DIAG_BLOCK) diag_final_kernel(const double *__
     double a = 0.0;
     for (int b = threadIdx.x; b < nblocks; b += DIAG_BLOCK) {
       double x = part[(long long)b * DIAG_VALS + q];
-      a = (q == 9) ? max_ref(a, x) : a + x;
+      a = diag_is_max(q) ? max_ref(a, x) : a + x;
     }
     sh[threadIdx.x] = a;
     __syncthreads();
     for (int w = DIAG_BLOCK / 2; w > 0; w >>= 1) {
-      if (threadIdx.x < w) sh[threadIdx.x] = (q == 9) ? max_ref(sh[threadIdx.x], sh[threadIdx.x + w])
+      if (threadIdx.x < w) sh[threadIdx.x] = diag_is_max(q) ? max_ref(sh[threadIdx.x], sh[threadIdx.x + w])
                                                         : sh[threadIdx.x] + sh[threadIdx.x + w];
       __syncthreads();
     }
@@ -2441,11 +2448,12 @@ extern "C" int hgpu_diagnostics(hgpu_ctx *x, hgpu_diag *out) {
   long long zones = (long long)x->d.n1 * x->d.n2 * x->d.n3;
   out->divb_avg = h[8] / (double)zones;
   out->divb_max = h[9];
+  out->divb_max_interior = h[11];
   out->nfail = (int)h[10];
   out->t = s.t;
   out->dt = s.dt;
   out->nsteps = s.nsteps;
-  out->nfloor = s.nfloor;
+  out->nfloor = (long long)s.nfloor;
   return HGPU_OK;
 }
 

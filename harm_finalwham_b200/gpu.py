@@ -51,7 +51,8 @@ class hgpu_tuning(ctypes.Structure):
 class hgpu_diag(ctypes.Structure):
     _fields_ = [("t", ctypes.c_double), ("dt", ctypes.c_double), ("integral", ctypes.c_double * 8),
                 ("divb_max", ctypes.c_double), ("divb_avg", ctypes.c_double), ("nfail", ctypes.c_int),
-                ("nfloor", ctypes.c_int), ("nsteps", ctypes.c_longlong)]
+                ("nfloor", ctypes.c_longlong), ("nsteps", ctypes.c_longlong),
+                ("divb_max_interior", ctypes.c_double)]
 
 
 class hgpu_stats(ctypes.Structure):
@@ -274,7 +275,8 @@ class HarmGPU:
         dg = hgpu_diag()
         _check(self.L, self.L.hgpu_diagnostics(self.h, ctypes.byref(dg)))
         return {"t": dg.t, "dt": dg.dt, "integral": list(dg.integral), "divb_max": dg.divb_max,
-                "divb_avg": dg.divb_avg, "nfail": dg.nfail, "nfloor": dg.nfloor, "nsteps": dg.nsteps}
+                "divb_avg": dg.divb_avg, "nfail": dg.nfail, "nfloor": dg.nfloor, "nsteps": dg.nsteps,
+                "divb_max_interior": dg.divb_max_interior}
 
     def step_graph(self, nsteps=1, stats=True):
         """step_ch as replays of one captured CUDA graph per time step."""

@@ -33,7 +33,7 @@
 extern "C" {
 #endif
 
-#define HGPU_ABI_VERSION 5
+#define HGPU_ABI_VERSION 6
 
 /* return codes */
 #define HGPU_OK 0
@@ -230,16 +230,20 @@ int hgpu_set_tuning(hgpu_ctx *ctx, const hgpu_tuning *t);
    dx1 dx2 dx3; divb_max / divb_avg = max and mean over active zones of the
    flux-CT div B at each zone's lower corner (divbmaxavg, dump_ener.c:482;
    DIVBFLUXCT, global.h:1586-1645); nfail = zones whose last inversion left
-   a failure code; nfloor = zones raised to a floor by fixup1zone during the
-   last hgpu_step_ch call; t, dt, nsteps since the last upload.  Sums are
+   a failure code; nfloor = zone floorings by fixup1zone summed over the last
+   stepping call; t, dt, nsteps since the last upload.  divb_max includes
+   the axis corners, where gdet vanishes and the reference's normalisation
+   divides by ~0; divb_max_interior leaves them out.  Sums are
    deterministic (fixed-order two-pass reduction), not in the reference's
    serial order. */
 typedef struct {
   double t, dt;
   double integral[8];
   double divb_max, divb_avg;
-  int nfail, nfloor;
+  int nfail;
+  long long nfloor;
   long long nsteps;
+  double divb_max_interior;  /* max over the corners flux-CT constrains (x1 1..n1-1, x2 2..n2-2) */
 } hgpu_diag;
 int hgpu_diagnostics(hgpu_ctx *ctx, hgpu_diag *out);
 

@@ -44,3 +44,22 @@ def test_mixed_tracks_fp64(lim):
     assert abs(t32 - t64) < 1e-5 * t64
     # failure maps: the same zones fail in both, up to a handful
     assert abs(int(np.count_nonzero(f32)) - int(np.count_nonzero(f64))) <= max(4, np.count_nonzero(f64) // 20)
+
+
+def test_mixed_finite_volume_default_scheme():
+    # the FM torus problem file's own scheme (PARA, RK4, Jon, finite volume
+    # over all 11 MAXBND ghosts) in mixed precision against FP64
+    from tests.fixtures import load
+    pr, _ = load("torus2d_16x16_para_hll_rk4_jon_fv")
+    out = {}
+    for prec in ("fp64", "mixed"):
+        with HarmGPU.from_problem(pr, precision=prec) as g:
+            st = g.step_ch(20)
+            p, pf, t, dt = g.download_state()
+            assert st.err == 0
+            out[prec] = (g.active(p), t)
+    p64, t64 = out["fp64"]
+    p32, t32 = out["mixed"]
+    assert np.all(np.isfinite(p32))
+    assert rel_l1(p32[..., 0], p64[..., 0]) < 1e-4
+    assert abs(t32 - t64) < 1e-4 * t64
