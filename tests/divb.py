@@ -46,11 +46,12 @@ def divb_max(p, gdet, ng, dx, n):
     return float(np.max(np.abs(d)))
 
 
-def divb_maxavg(p, gdet, ng, dx, n):
+def divb_maxavg(p, gdet, ng, dx, n, interior=False):
     """The reference's divbmaxavg (dump_ener.c:482-520): max and mean over all
     active zones of |DIVBFLUXCT| at the zone's lower corner (dims of size 1
     use the same zone on both sides); gdet at the corner from CORN3 (=CORNT,
-    the metric does not depend on x3)."""
+    the metric does not depend on x3).  interior: the max over the corners
+    flux-CT constrains only (x1 corners 1..n1-1, x2 corners 2..n2-2)."""
     n1, n2, n3 = n
     s1, s2, s3 = int(n1 > 1), int(n2 > 1), int(n3 > 1)
     g1, g2, g3 = ng * s1, ng * s2, ng * s3
@@ -82,4 +83,11 @@ def divb_maxavg(p, gdet, ng, dx, n):
     mx = max(max(dx[0], dx[1]), dx[2])
     norm = mx / ((1.0 / 3.0) * gdet[I, J, 5] * np.abs(nx + ny + nz) + SMALL)
     d = np.abs((dfx / dx[0] + dfy / dx[1] + dfz / dx[2]) * norm)
+    if interior:
+        m = np.ones(d.shape, dtype=bool)
+        if s1:
+            m &= (I - g1 >= 1) & (I - g1 <= n1 - 1)
+        if s2:
+            m &= (J - g2 >= 2) & (J - g2 <= n2 - 2)
+        return float(d[m].max())
     return float(d.max()), float(d.mean())
