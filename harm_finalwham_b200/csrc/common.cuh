@@ -240,8 +240,8 @@ template <> struct MinBlocks<float> {
 
 // the FP64 variants the autotuner chooses between (resident 128-thread
 // blocks per SM for each heavy kernel; variant 0 is the default above)
-constexpr int kFluxMB[2] = {HG_MINB_FLUX, HG_MINB_FLUX + 1};
-constexpr int kWenoBMB[2] = {HG_MINB_WENO_B, HG_MINB_WENO_B + 2};
+constexpr int kFluxMB[2] = {HG_MINB_FLUX, HG_MINB_FLUX - 1};
+constexpr int kWenoBMB[2] = {HG_MINB_WENO_B, HG_MINB_WENO_B - 2};
 constexpr int kConserveMB[2] = {HG_MINB_UPDATE, 3};
 constexpr int kInvertMB[2] = {HG_MINB_INVERT, 2};
 
@@ -307,33 +307,27 @@ __global__ void __launch_bounds__(128, MB) weno_b_kernel(Dims d, Params P, Box b
   // primitives of the cells -1, 0, +1 along the line and their CENT metrics
   T dP;
   {
-    T pm[NPR], p0[NPR], pp[NPR];
+    // one cell at a time (only its two scalars stay live): par = (1 + u_t) u^t,
+    // upar = gam u (u^t u_t) + (gam - 1) u
+    const T gam = (T)(P.cell_inst ? P.inst[P.cell_inst[z]].gam : P.gam);
+    auto cell = [&](int off, T *par, T *upar, T *rho) {
+      T pc[NPR];
 #pragma unroll
-    for (int v = 0; v < NPR; v++) {
-      pm[v] = (T)pb[(long long)v * d.nz + z - o];
-      p0[v] = (T)pb[(long long)v * d.nz + z];
-      pp[v] = (T)pb[(long long)v * d.nz + z + o];
-    }
-    StateT<T> ql, q, qr;
-    T a, b, c;
-    MetricT<T> m;
-    load_metric_t(G, d, gix(d, i - (DIR == 1), j - (DIR == 2)), G_CENT, m);
-    get_state(pm, m, ql);
-    a = compute_1plusud0(m, ql);
-    load_metric_t(G, d, gix(d, i, j), G_CENT, m);
-    get_state(p0, m, q);
-    b = compute_1plusud0(m, q);
-    load_metric_t(G, d, gix(d, i + (DIR == 1), j + (DIR == 2)), G_CENT, m);
-    get_state(pp, m, qr);
-    c = compute_1plusud0(m, qr);
-    T gam = (T)(P.cell_inst ? P.inst[P.cell_inst[z]].gam : P.gam);
-    T parl = a * (ql.ucon[0]);
-    T par = b * (q.ucon[0]);
-    T parr = c * (qr.ucon[0]);
-    T uparl = gam * pm[UU] * (ql.ucon[0] * ql.ucov[0]) + (gam - T(1.0)) * pm[UU];
-    T upar = gam * p0[UU] * (q.ucon[0] * q.ucov[0]) + (gam - T(1.0)) * p0[UU];
-    T uparr = gam * pp[UU] * (qr.ucon[0] * qr.ucov[0]) + (gam - T(1.0)) * pp[UU];
-    dP = (fabs(p0[RHO] * (parr - parl)) + fabs(uparr - uparl)) / (fabs(p0[RHO] * par) + fabs(upar) + w5::K<T>::tiny);
+      for (int v = 0; v < NPR; v++) pc[v] = (T)pb[(long long)v * d.nz + z + off * o];
+      MetricT<T> m;
+      load_metric_t(G, d, gix(d, i + off * (DIR == 1), j + off * (DIR == 2)), G_CENT, m);
+      StateT<T> q;
+      get_state(pc, m, q);
+      const T a = compute_1plusud0(m, q);
+      *par = a * (q.ucon[0]);
+      *upar = gam * pc[UU] * (q.ucon[0] * q.ucov[0]) + (gam - T(1.0)) * pc[UU];
+      *rho = pc[RHO];
+    };
+    T parl, uparl, par, upar, parr, uparr, rl, r0, rr;
+    cell(-1, &parl, &uparl, &rl);
+    cell(0, &par, &upar, &r0);
+    cell(1, &parr, &uparr, &rr);
+    dP = (fabs(r0 * (parr - parl)) + fabs(uparr - uparl)) / (fabs(r0 * par) + fabs(upar) + w5::K<T>::tiny);
   }
   // apply_additional_reduction_to_weights (reconstructeno.c:650-700)
   T ss = w5::wmin((fabs(dP) - T(0.5 * w5::kDpFrac)) / T(0.5 * w5::kDpFrac), T(1.));

@@ -31,7 +31,7 @@ def test_autotune_keeps_state_and_results(name):
 def test_set_tuning_applies_a_known_choice():
     pr, ref = load("torus2d_16x16_mc_hll")
     with HarmGPU.from_problem(pr) as g:
-        g.set_tuning({"flux": 5, "weno_b": 10, "update": 3, "invert": 2})
+        g.set_tuning({"flux": 3, "weno_b": 6, "update": 3, "invert": 2})
         s = sorted(ref)[-1]
         g.step_ch(s)
         p, pf, t, dt = g.download_state()
