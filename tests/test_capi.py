@@ -49,3 +49,27 @@ def test_invalid_config_is_rejected_without_gpu_work():
     import pytest
     with pytest.raises((HarmGPUError, ValueError)):
         HarmGPU(16, 16, 1, 1, (0.1, 0.1, 1.0))  # ng < 2 is invalid before any device call
+
+
+def test_configuration_validation_on_the_host():
+    # hgpu_context_bytes runs the same validation as hgpu_create and
+    # touches no device: 0 means rejected
+    from harm_finalwham_b200.gpu import context_bytes, make_config
+
+    def ok(**kw):
+        base = dict(n=(32, 32, 1), ng=3, dx=(0.1, 0.1, 1.0))
+        base.update(kw)
+        n, ng, dx = base.pop("n"), base.pop("ng"), base.pop("dx")
+        return context_bytes(make_config(n, ng, dx, **base)) > 0
+
+    assert ok()
+    assert ok(lim="PARA") and not ok(lim="PARA", ng=2)          # PARA reads 3 zones out
+    assert ok(lim="WENO5", ng=6) and not ok(lim="WENO5", ng=5)  # WENO5 reads 6
+    assert ok(timeorder=4) and ok(timeorder=1) and not ok(timeorder=5)
+    assert ok(utoprim="JON") and not ok(utoprim=7)
+    assert ok(doenoflux="ENOFINITEVOLUME", ng=11, n=(32, 32, 1)) and not ok(doenoflux=2)
+    assert not ok(n=(32, 2, 1))                                  # reflections need n2 >= ng
+    # the finite-volume scheme keeps a second conserved array; RK3/RK4 a second intermediate state
+    base = context_bytes(make_config((32, 32, 1), 3, (0.1, 0.1, 1.0)))
+    assert context_bytes(make_config((32, 32, 1), 3, (0.1, 0.1, 1.0), doenoflux="ENOFINITEVOLUME")) > base
+    assert context_bytes(make_config((32, 32, 1), 3, (0.1, 0.1, 1.0), timeorder=4)) > base
