@@ -1618,10 +1618,28 @@ static const RKStage kRK4[4] = {{{1.0, 0.0, 0.5}, {1.0, 1.0 / 6.0, 0.0}, 0, 1},
 
 static int num_orders(const hgpu_ctx *x) { return x->cfg.timeorder ? x->cfg.timeorder : 2; }
 
-static void launch_stage(hgpu_ctx *x, int timeorder) {
+static const RKStage &rk_stage(const hgpu_ctx *x, int timeorder) {
+  const int norders = num_orders(x);
+  return (norders == 4 ? kRK4 : norders == 3 ? kRK3 : norders == 2 ? kRK2 : kRK1)[timeorder];
+}
+
+// the array stage `timeorder` writes (pf); -1 names p itself
+static double *stage_output(hgpu_ctx *x, int timeorder) {
+  if (timeorder < 0) return x->p;
+  double *arr[3] = {x->p, x->pk, x->pk1};
+  return arr[rk_stage(x, timeorder).pf];
+}
+
+// One RK stage in two halves.  The first runs advance (fluxes, conserved
+// update, inversion, fixup1zone) and the bound_prim/bound_pflag that open
+// post_fixup; the second runs fixup_checksolution, fixup_utoprim and the
+// closing bound_prim.  A domain split along x3 exchanges the x3 ghost planes
+// of pf and pflag after the first half and of pf after the second, where the
+// reference's bound_prim and bound_pflag call bound_mpi / bound_mpi_int.
+static void launch_stage_advance(hgpu_ctx *x, int timeorder) {
   const Dims &d = x->d;
   const int norders = num_orders(x);
-  const RKStage &S = (norders == 4 ? kRK4 : norders == 3 ? kRK3 : norders == 2 ? kRK2 : kRK1)[timeorder];
+  const RKStage &S = rk_stage(x, timeorder);
   double *arr[3] = {x->p, x->pk, x->pk1};
   const double *pi = x->p;
   const double *pb = arr[S.pb];
@@ -1663,6 +1681,13 @@ static void launch_stage(hgpu_ctx *x, int timeorder) {
     LAUNCH(x, K_BOUND_PFLAG, bound_batch_kernel, grid_for(d.nz, 256), 256, d, x->P, (double *)nullptr, x->pflag);
   else
     LAUNCH(x, K_BOUND_PFLAG, bound_pflag_kernel, grid_for(d.nz, 256), 256, d, x->P, x->pflag, x->sc);
+}
+
+static void launch_stage_fixup(hgpu_ctx *x, int timeorder) {
+  const Dims &d = x->d;
+  double *pf = stage_output(x, timeorder);
+  const int finalstep = (timeorder == num_orders(x) - 1);
+  double *ufv = (x->cfg.doenoflux == HGPU_ENOFINITEVOLUME && finalstep) ? x->ucum : nullptr;
   LAUNCH(x, K_CHECK_GAMMA, checksol_gamma_kernel, grid_for(x->dq_box.size(), 128), 128, d, x->P, x->dq_box, pf, x->G,
          x->gammacheck, x->cand, x->cap, x->sc);
   LAUNCH(x, K_CHECK_RESOLVE, checksol_resolve_kernel, 1, 1024, d, pf, x->gammacheck, x->pflag, x->cand, x->candmap,
@@ -1677,6 +1702,11 @@ static void launch_stage(hgpu_ctx *x, int timeorder) {
   LAUNCH(x, K_FIX_SCATTER, fixup_scatter_kernel, fixgrid, 128, d, x->P, pf, x->pflag, x->fixlist, x->fixvals, x->cap,
          finalstep, x->sc, x->G, ufv);
   launch_bound(x, pf);
+}
+
+static void launch_stage(hgpu_ctx *x, int timeorder) {
+  launch_stage_advance(x, timeorder);
+  launch_stage_fixup(x, timeorder);
 }
 
 static int read_stats(hgpu_ctx *x, hgpu_stats *st) {
@@ -2480,5 +2510,146 @@ extern "C" int hgpu_download_conserved(hgpu_ctx *x, double *unew) {
   LAUNCH(x, K_OTHER, soa_to_aos_kernel, grid_for(nz * NPR, 256), 256, x->ucum, x->staging, nz);
   CUDA_TRY(cudaMemcpyAsync(unew, x->staging, sizeof(double) * NPR * nz, cudaMemcpyDeviceToHost, x->stream));
   CUDA_TRY(cudaStreamSynchronize(x->stream));
+  return HGPU_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Domain split along x3 (the reference's MPI decomposition with ncpux3 ranks,
+// boundmpi.c:6-180; pack / send-receive / unpack boundmpi.c:185-290).  A rank
+// owns n3 planes of the global domain; its x3 ghost planes are the
+// neighbours' edge planes.  The step runs as phases so that the caller can
+// move the planes between phases (NCCL between GPUs, or device copies
+// between domains on one GPU):
+//   hgpu_stats_clear
+//   per stage s: hgpu_stage_advance(s); exchange pf and pflag planes;
+//                hgpu_stage_fixup(s);   exchange pf planes
+//   exchange the per-direction ndt minima (minimum over ranks); hgpu_step_end(1)
+// Every kernel reads the x3 ghosts only after the exchange that fills them,
+// so the phases reproduce a whole-domain step bit for bit wherever the
+// per-rank loops of fixup_utoprim see the same "already visited" neighbours
+// (fixup.c:669-1470 counts an earlier failed neighbour that becomes fixed as
+// good; across a rank boundary that neighbour is a ghost zone).
+// Halo buffer of one face: [8 primitives][i][j][plane] doubles, then, with
+// pflag, [i][j][plane] ints; i and j run over the ghosts too, so the x1/x2
+// ghost corners travel with the planes.
+// ---------------------------------------------------------------------------
+__global__ void halo_x3_kernel(Dims d, double *p, int *pflag, unsigned char *buf, int side, int unpack,
+                               int with_pflag) {
+  const long long per_var = (long long)d.nt1 * d.nt2 * d.g3;
+  const long long nvals = per_var * (NPR + (with_pflag ? 1 : 0));
+  long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= nvals) return;
+  const int v = (int)(t / per_var);
+  const long long r = t % per_var;
+  // consecutive threads walk the planes of one (i,j) column, contiguous in k
+  const long long ij = r / d.g3;
+  const int layer = (int)(r % d.g3);
+  int k;
+  if (unpack) k = side == 0 ? layer - d.g3 : d.n3 + layer;
+  else k = side == 0 ? layer : d.n3 - d.g3 + layer;
+  const long long z = ij * d.nt3 + (k + d.g3);
+  double *vb = (double *)buf;
+  if (v < NPR) {
+    const long long b = (long long)v * per_var + r;
+    if (unpack) p[(long long)v * d.nz + z] = vb[b];
+    else vb[b] = p[(long long)v * d.nz + z];
+  } else {
+    int *fb = (int *)(vb + (long long)NPR * per_var);
+    if (unpack) pflag[z] = fb[r];
+    else fb[r] = pflag[z];
+  }
+}
+
+static int decomposable(const hgpu_ctx *x) { return x && !x->P.cell_inst && x->d.n3 > 1; }
+
+extern "C" int hgpu_halo_bytes(hgpu_ctx *x, size_t *bytes) {
+  if (!decomposable(x) || !bytes) return HGPU_E_INVALID;
+  *bytes = (size_t)x->d.nt1 * x->d.nt2 * x->d.g3 * (NPR * sizeof(double) + sizeof(int));
+  return HGPU_OK;
+}
+
+static int halo_io(hgpu_ctx *x, int stage, int side, int with_pflag, void *buf, int unpack) {
+  if (!decomposable(x) || !buf || (side != 0 && side != 1) || stage < -1 || stage >= num_orders(x))
+    return HGPU_E_INVALID;
+  const long long n = (long long)x->d.nt1 * x->d.nt2 * x->d.g3 * (NPR + (with_pflag ? 1 : 0));
+  LAUNCH(x, K_OTHER, halo_x3_kernel, grid_for(n, 256), 256, x->d, stage_output(x, stage), x->pflag,
+         (unsigned char *)buf, side, unpack, with_pflag ? 1 : 0);
+  CUDA_TRY(cudaGetLastError());
+  return HGPU_OK;
+}
+
+extern "C" int hgpu_halo_pack(hgpu_ctx *x, int stage, int side, int with_pflag, void *dev_buf) {
+  return halo_io(x, stage, side, with_pflag, dev_buf, 0);
+}
+
+extern "C" int hgpu_halo_unpack(hgpu_ctx *x, int stage, int side, int with_pflag, const void *dev_buf) {
+  return halo_io(x, stage, side, with_pflag, const_cast<void *>(dev_buf), 1);
+}
+
+extern "C" int hgpu_stats_clear(hgpu_ctx *x) {
+  if (!x) return HGPU_E_INVALID;
+  clear_counters(x);
+  CUDA_TRY(cudaGetLastError());
+  return HGPU_OK;
+}
+
+extern "C" int hgpu_stats_read(hgpu_ctx *x, hgpu_stats *stats) {
+  if (!x) return HGPU_E_INVALID;
+  return read_stats(x, stats);
+}
+
+extern "C" int hgpu_stage_advance(hgpu_ctx *x, int stage) {
+  if (!decomposable(x) || stage < 0 || stage >= num_orders(x)) return HGPU_E_INVALID;
+  launch_stage_advance(x, stage);
+  CUDA_TRY(cudaGetLastError());
+  return HGPU_OK;
+}
+
+extern "C" int hgpu_stage_fixup(hgpu_ctx *x, int stage) {
+  if (!decomposable(x) || stage < 0 || stage >= num_orders(x)) return HGPU_E_INVALID;
+  launch_stage_fixup(x, stage);
+  CUDA_TRY(cudaGetLastError());
+  return HGPU_OK;
+}
+
+// start-up ndt (set_dt, advance.c:957) of a split domain: the fluxes of p,
+// then the ndt exchange, then hgpu_step_end(x, 0)
+extern "C" int hgpu_dt_probe(hgpu_ctx *x) {
+  if (!decomposable(x)) return HGPU_E_INVALID;
+  launch_reset(x);
+  launch_fluxes(x, x->p);
+  CUDA_TRY(cudaGetLastError());
+  return HGPU_OK;
+}
+
+// advance_time 1: the dt update closing a step (step_ch.c:236-247);
+// 0: dt = ndt, the start-up value
+extern "C" int hgpu_step_end(hgpu_ctx *x, int advance_time) {
+  if (!decomposable(x)) return HGPU_E_INVALID;
+  launch_finalize(x, advance_time ? 1 : 0);
+  if (!advance_time) LAUNCH(x, K_OTHER, set_dt_kernel, 1, 32, x->sc);
+  CUDA_TRY(cudaGetLastError());
+  return HGPU_OK;
+}
+
+// the three per-direction minima of cour*dx/ctop as order-preserving 64-bit
+// patterns (positive doubles compare as integers), for a minimum over ranks
+extern "C" int hgpu_ndt_pack(hgpu_ctx *x, unsigned long long *dev3) {
+  if (!decomposable(x) || !dev3) return HGPU_E_INVALID;
+  CUDA_TRY(cudaMemcpyAsync(dev3, &x->sc->ndtbits[1], 3 * sizeof(unsigned long long), cudaMemcpyDeviceToDevice,
+                           x->stream));
+  return HGPU_OK;
+}
+
+extern "C" int hgpu_ndt_unpack(hgpu_ctx *x, const unsigned long long *dev3) {
+  if (!decomposable(x) || !dev3) return HGPU_E_INVALID;
+  CUDA_TRY(cudaMemcpyAsync(&x->sc->ndtbits[1], dev3, 3 * sizeof(unsigned long long), cudaMemcpyDeviceToDevice,
+                           x->stream));
+  return HGPU_OK;
+}
+
+extern "C" int hgpu_stream(hgpu_ctx *x, void **stream) {
+  if (!x || !stream) return HGPU_E_INVALID;
+  *stream = (void *)x->stream;
   return HGPU_OK;
 }

@@ -125,6 +125,19 @@ def load_library(path=None):
     L.hgpu_server_release.argtypes = [ctypes.c_void_p, ctypes.c_longlong]
     L.hgpu_batch_run.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, _ip, _P(ctypes.c_float), _ip,
                                  _P(ctypes.c_float)]
+    _v = ctypes.c_void_p
+    L.hgpu_halo_bytes.argtypes = [_v, _P(ctypes.c_size_t)]
+    L.hgpu_halo_pack.argtypes = [_v, ctypes.c_int, ctypes.c_int, ctypes.c_int, _v]
+    L.hgpu_halo_unpack.argtypes = [_v, ctypes.c_int, ctypes.c_int, ctypes.c_int, _v]
+    L.hgpu_stats_clear.argtypes = [_v]
+    L.hgpu_stats_read.argtypes = [_v, _P(hgpu_stats)]
+    L.hgpu_stage_advance.argtypes = [_v, ctypes.c_int]
+    L.hgpu_stage_fixup.argtypes = [_v, ctypes.c_int]
+    L.hgpu_dt_probe.argtypes = [_v]
+    L.hgpu_step_end.argtypes = [_v, ctypes.c_int]
+    L.hgpu_ndt_pack.argtypes = [_v, _v]
+    L.hgpu_ndt_unpack.argtypes = [_v, _v]
+    L.hgpu_stream.argtypes = [_v, _P(_v)]
     for name in ("hgpu_init_dt", "hgpu_step_ch_timed", "hgpu_set_profiling", "hgpu_kernel_times", "hgpu_alloc_pinned",
                  "hgpu_free_pinned", "hgpu_fp64_peak"):
         getattr(L, name).restype = ctypes.c_int
@@ -132,7 +145,9 @@ def load_library(path=None):
                  "hgpu_advance_stage", "hgpu_fluxcalc", "hgpu_bound_prim", "hgpu_utoprim_batch", "hgpu_utoprimgen_batch",
                  "hgpu_device_prims", "hgpu_sync", "hgpu_create_batch", "hgpu_batch_layout", "hgpu_batch_status",
                  "hgpu_step_graph", "hgpu_autotune", "hgpu_set_tuning", "hgpu_batch_run", "hgpu_diagnostics", "hgpu_download_conserved", "hgpu_upload_conserved", "hgpu_server_create", "hgpu_server_submit", "hgpu_server_submit_borrowed",
-                 "hgpu_server_poll", "hgpu_server_result", "hgpu_server_release"):
+                 "hgpu_server_poll", "hgpu_server_result", "hgpu_server_release", "hgpu_halo_bytes", "hgpu_halo_pack",
+                 "hgpu_halo_unpack", "hgpu_stats_clear", "hgpu_stats_read", "hgpu_stage_advance", "hgpu_stage_fixup",
+                 "hgpu_dt_probe", "hgpu_step_end", "hgpu_ndt_pack", "hgpu_ndt_unpack", "hgpu_stream"):
         getattr(L, name).restype = ctypes.c_int
     if path == _build.LIB:
         _lib = L

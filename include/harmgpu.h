@@ -33,7 +33,7 @@
 extern "C" {
 #endif
 
-#define HGPU_ABI_VERSION 6
+#define HGPU_ABI_VERSION 7
 
 /* return codes */
 #define HGPU_OK 0
@@ -259,6 +259,46 @@ int hgpu_download_conserved(hgpu_ctx *ctx, double *unew);
    sets it to U(p) in every zone, as init_conservatives/pi2Uavg does
    (initbase.c:146-153, 1833). */
 int hgpu_upload_conserved(hgpu_ctx *ctx, const double *unew);
+
+/* ---- Domain split along x3 ----------------------------------------------
+   The reference decomposes the grid over MPI ranks (ncpux1..3,
+   mpi_init.c:226) and fills each rank's ghost zones from its neighbours in
+   bound_prim and bound_pflag (bound_mpi boundmpi.c:6-180, bound_mpi_int
+   boundmpiint.c:4), and takes the minimum of dt over ranks (mpifmin,
+   step_ch.c:243, mpi_fileio.c:1905).  Here a context holds one rank's
+   n3 planes of an x3-periodic domain (n3 > 1) and one step runs as phases,
+   with the plane exchange and the dt minimum done by the caller between
+   them (NCCL send/recv and all-reduce between GPUs, device copies between
+   contexts on one GPU):
+     hgpu_stats_clear
+     for each stage s of TIMEORDER:
+       hgpu_stage_advance(s)   advance + bound_prim + bound_pflag
+       exchange: hgpu_halo_pack(s, side, 1) -> neighbour -> hgpu_halo_unpack
+       hgpu_stage_fixup(s)     post_fixup + bound_prim
+       exchange: the same with with_pflag = 0
+     ndt: hgpu_ndt_pack -> elementwise minimum over ranks -> hgpu_ndt_unpack
+     hgpu_step_end(1); hgpu_stats_read
+   The minimum is taken per direction before the three are combined, so a
+   split run reproduces the whole-domain dt (the reference combines per rank
+   first, step_ch.c:243).  Start-up dt: hgpu_dt_probe, the ndt exchange,
+   hgpu_step_end(0).  All calls are asynchronous on the context's stream
+   (hgpu_stream) except hgpu_stats_read.
+   Halo buffers live in device memory; side 0 is the lower x3 face, 1 the
+   upper.  Pack side 1 of rank r is unpacked as side 0 of rank r+1 (mod P),
+   and pack side 0 of rank r as side 1 of rank r-1.  stage -1 names the
+   state itself (the exchange after an upload, before the first step). */
+int hgpu_halo_bytes(hgpu_ctx *ctx, size_t *bytes);
+int hgpu_halo_pack(hgpu_ctx *ctx, int stage, int side, int with_pflag, void *dev_buf);
+int hgpu_halo_unpack(hgpu_ctx *ctx, int stage, int side, int with_pflag, const void *dev_buf);
+int hgpu_stats_clear(hgpu_ctx *ctx);
+int hgpu_stats_read(hgpu_ctx *ctx, hgpu_stats *stats);
+int hgpu_stage_advance(hgpu_ctx *ctx, int stage);
+int hgpu_stage_fixup(hgpu_ctx *ctx, int stage);
+int hgpu_dt_probe(hgpu_ctx *ctx);
+int hgpu_step_end(hgpu_ctx *ctx, int advance_time);
+int hgpu_ndt_pack(hgpu_ctx *ctx, unsigned long long *dev3);
+int hgpu_ndt_unpack(hgpu_ctx *ctx, const unsigned long long *dev3);
+int hgpu_stream(hgpu_ctx *ctx, void **stream);
 
 /* Device bytes a context of this configuration allocates (0 if invalid). */
 size_t hgpu_context_bytes(const hgpu_config *cfg);
