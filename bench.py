@@ -28,6 +28,9 @@ host core on the bounded sample, aggregate zone-updates/s.
 
 Multi-GPU: replicas (each rank advances its own torus; no data-path
 collective), weak scaling; value = all ranks' zone-updates / max time.
+--decomp x3 instead splits one torus of n3 x N planes along x3 (each rank
+owns n3 planes; ghost planes exchanged over NCCL twice per stage, the ndt
+minima all-reduced once per step).
 """
 import argparse
 import json
@@ -153,6 +156,86 @@ class ClockSampler:
         return {"sm_mhz": statistics.median(loaded), "sm_max_mhz": smax, "reasons": sorted(reasons),
                 "samples": len(rows), "power_w_max": max(float(r[3]) for r in rows if r[3].strip()
                                                            .replace('.', '', 1).isdigit()) if rows else None}
+
+
+def bench_decomp(args, rank, world):
+    """--decomp x3: one torus of n3 x world planes split along x3, rank r
+    owning planes r*n3 .. (r+1)*n3-1 (weak scaling).  Each step runs the
+    phase entry points with the x3 ghost planes sent to the neighbours over
+    NCCL after each half-stage and the per-direction ndt minima all-reduced;
+    with one rank the planes wrap onto the same context, which measures the
+    cost of the phase-driven step against the one-call step."""
+    import datetime
+
+    import torch
+
+    from harm_finalwham_b200 import torus
+    from harm_finalwham_b200.decomp import CollectiveTransport, SplitRun, _Sub, split_x3
+    from harm_finalwham_b200.gpu import HarmGPU, load_library
+
+    n1, n2, n3, lim, flux = WORKLOADS[args.workload]
+    sc = scheme_of(args.workload)
+    if args.utoprim:
+        sc["utoprim"] = args.utoprim
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+        torch.cuda.set_device(0)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    dom = torus.fm_torus(n1, n2, n3 * world, ng=sc["ng"] or GHOSTS[lim], lim=lim, flux=flux, seed=7)
+    dom.timeorder, dom.utoprim, dom.doenoflux = sc["timeorder"], sc["utoprim"], sc["doenoflux"]
+    slab = split_x3(dom, world, rank)
+    del dom
+    L = load_library()
+    g = HarmGPU.from_problem(slab, precision=args.precision)
+    if args.tuning:
+        g.set_tuning(dict(zip(("flux", "weno_b", "update", "invert"), (int(v) for v in args.tuning.split(",")))))
+    else:
+        g.autotune()
+    sub = _Sub(g)
+    run = SplitRun([g], CollectiveTransport(sub))
+    run.start(init_dt=True)
+    run.step(args.warmup, stats=False)
+    if dist is not None:
+        dist.barrier()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    launches0 = L.hgpu_launch_count(g.h)
+    clocks = ClockSampler()
+    clocks.start()
+    e0.record(sub.stream)
+    run.step(args.steps, stats=False)
+    e1.record(sub.stream)
+    e1.synchronize()
+    clk = clocks.stop()
+    launches = L.hgpu_launch_count(g.h) - launches0
+    st = run.stats()
+    ms = e0.elapsed_time(e1)
+    if dist is not None:
+        dist.barrier()
+    ms_max = replica_max(ms, dist, "cuda")
+    zones = n1 * n2 * n3
+    norders = sc["timeorder"] or 2
+    out = {"metric": METRIC, "value": replica_value(zones, args.steps, world, ms_max), "unit": "zone-updates/s",
+           "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_max / args.steps,
+           "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+           "dtype": "f64" if args.precision == "fp64" else "f64+f32", "data": "synthetic",
+           "config": {"workload": f"{args.workload} per rank, x3 split of {n1}x{n2}x{n3 * world}",
+                      "scheme": scheme_text(lim, flux, sc), "precision": args.precision,
+                      "parallelism": f"x3 split over {world} ranks" + (" (NCCL halos)" if world > 1 else
+                                                                         " (planes wrap onto the one rank)"),
+                      "l2": "state larger than L2"},
+           "halo": {"bytes_per_face_exchange": sub.nbytes, "exchanges_per_step": 2 * norders,
+                    "bytes_sent_per_step": 2 * 2 * norders * sub.nbytes},
+           "gpu_launches": launches, "clocks": clk, "newton_fail_err": st.err}
+    if world == 1:
+        # the same slab through the one-call step, for the phase-driven overhead
+        ms1, _ = g.step_ch_timed(args.steps)
+        out["one_call_ms_per_step"] = ms1 / args.steps
+    run.close()
+    if dist is not None:
+        dist.destroy_process_group()
+    return out
 
 
 def measured_peaks():
@@ -698,6 +781,8 @@ def main():
                     help="blocks per SM for flux,weno_b,update,invert instead of running the autotuner")
     ap.add_argument("--kernels-only", action="store_true",
                     help="set-up, warm-up and the timed steps only (for profiler runs)")
+    ap.add_argument("--decomp", default=None, choices=["x3"],
+                    help="split one torus along x3 over the ranks (NCCL halo exchange) instead of replicas")
     args = ap.parse_args()
     rank, world, local = rank_info()
     if args.warmup < 3:
@@ -728,7 +813,7 @@ def main():
         return 0
 
     pin_device(local, world)
-    res = bench_ours(args, rank, world)
+    res = bench_decomp(args, rank, world) if args.decomp else bench_ours(args, rank, world)
     if rank == 0:
         print(json.dumps(res))
     return 0

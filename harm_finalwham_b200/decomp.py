@@ -165,8 +165,10 @@ class CollectiveTransport:
         self.dist = dist
         self.sub = sub
         self.group = group
-        self.rank = dist.get_rank(group)
-        self.world = dist.get_world_size(group)
+        # without a process group the one slab's planes wrap onto itself
+        up = dist.is_available() and dist.is_initialized()
+        self.rank = dist.get_rank(group) if up else 0
+        self.world = dist.get_world_size(group) if up else 1
         dev = getattr(sub, "device", torch.device("cpu"))
         self.send_lo = torch.empty(sub.nbytes, dtype=torch.uint8, device=dev)
         self.send_hi = torch.empty_like(self.send_lo)
@@ -265,8 +267,11 @@ class SplitRun:
                 self.t.exchange(s, False)
             self.t.ndt_min()
             self._all("hgpu_step_end", 1)
-        if not stats:
-            return None
+        return self.stats() if stats else None
+
+    def stats(self):
+        """Statistics since the last step call, summed over the slabs held here
+        (synchronises)."""
         tot = hgpu_stats()
         for c in self.ctxs:
             st = hgpu_stats()

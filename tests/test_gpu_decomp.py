@@ -59,3 +59,27 @@ def test_split_run_matches_whole_domain(name, kw, nslabs):
     assert st_s.newton_iters == st_w.newton_iters
     assert st_s.err == st_w.err == 0
 
+
+
+def test_collective_transport_on_one_rank_matches_whole_domain():
+    """The multi-GPU transport with one rank (no process group): the planes
+    wrap onto the same context on its own stream, no host synchronisation."""
+    from harm_finalwham_b200.decomp import CollectiveTransport, _Sub
+    dom = _torus(n=(32, 16, 16), ng=3, lim="PARA", flux="HLL", timeorder=4, utoprim="JON",
+                 doenoflux="ENOFINITEVOLUME")
+    with HarmGPU.from_problem(dom) as whole:
+        whole.bound_prim(0)
+        whole.init_dt()
+        whole.step_ch(5)
+        p_w, f_w, t_w, dt_w = whole.download_state()
+    g = HarmGPU.from_problem(dom)
+    run = SplitRun([g], CollectiveTransport(_Sub(g)))
+    try:
+        run.start(init_dt=True)
+        run.step(5)
+        p_s, f_s, t_s, dt_s = run.download()
+    finally:
+        run.close()
+    assert (t_s, dt_s) == (t_w, dt_w)
+    assert _same_bits(p_s, p_w[3:-3, 3:-3, 3:-3])
+    assert np.array_equal(f_s, f_w[3:-3, 3:-3, 3:-3])
