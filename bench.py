@@ -594,13 +594,15 @@ def bench_riemann_batch(ninst=256, seed=2024, sample_single=12, check_every=25):
 
 
 def serving_requests(count, seed):
-    """A seeded request stream: 60% Kerr torus, 40% Bondi (Schwarzschild,
-    r_s = 8M, monopole field), grids from {32x32, 64x64, 128x128, 256x128}
-    (2D) or {64x32x16, 96x48x32} (3D tori), spin a ~ U(0, 0.99), beta ~
-    logU[10, 1000], 4% internal-energy noise; arrival gaps exponential."""
+    """A seeded request stream of (kind, domain, end time): 45% Kerr torus,
+    30% Bondi (Schwarzschild, r_s = 8M, monopole field), both to t = 50 on
+    grids from {32x32, 64x64, 128x128, 256x128} (2D) or {64x32x16, 96x48x32}
+    (3D tori), spin a ~ U(0, 0.99), beta ~ logU[10, 1000], 4% internal-energy
+    noise; 25% 1D relativistic-MHD shock tubes (MC + HLL, CFL 0.5, N ~
+    U{200..2000}, seeded states) to t = 0.4; arrival gaps exponential."""
     import numpy as np
 
-    from harm_finalwham_b200 import bondi, torus
+    from harm_finalwham_b200 import bondi, riemann, torus
 
     rng = np.random.default_rng(seed)
     grids2 = [(32, 32), (64, 64), (128, 128), (256, 128)]
@@ -608,7 +610,12 @@ def serving_requests(count, seed):
     out = []
     for q in range(count):
         beta = 10.0 ** rng.uniform(1.0, 3.0)
-        if rng.random() < 0.6:
+        u = rng.random()
+        if u < 0.25:
+            prob = riemann.draw(1, seed=int(rng.integers(1 << 30)))[0]
+            out.append(("shock tube", riemann.domain(prob), 0.4))
+            continue
+        if u < 0.25 + 0.45:
             a = rng.uniform(0.0, 0.99)
             if rng.random() < 0.2:
                 n = grids3[rng.integers(len(grids3))]
@@ -620,11 +627,12 @@ def serving_requests(count, seed):
             n = grids2[rng.integers(len(grids2))]
             dom = bondi.bondi(*n, ng=3, beta=beta, seed=int(rng.integers(1 << 30)))
             kind = "bondi"
-        out.append((kind, dom))
+        out.append((kind, dom, 50.0))
     return out
 
 
-def bench_serving(count=24, tf=50.0, mean_gap_ms=2.0, seed=11, budget_bytes=32e9):
+def bench_serving(count=32, mean_gap_ms=2.0, seed=11, budget_bytes=32e9, max_active=64, steps_per_chunk=8,
+                  one_at_a_time=True):
     """Continuous batching: requests arrive on a seeded Poisson clock fast
     enough to keep the GPU saturated and go through hgpu_server (admission by
     device footprint, overlapped solves, each solve's step replayed from its
@@ -636,7 +644,7 @@ def bench_serving(count=24, tf=50.0, mean_gap_ms=2.0, seed=11, budget_bytes=32e9
     reqs = serving_requests(count, seed)
     rng = np.random.default_rng(seed + 1)
     arrivals = np.cumsum(rng.exponential(mean_gap_ms / 1e3, count))
-    srv = HarmServer(max_device_bytes=int(budget_bytes), max_active=32, steps_per_chunk=8)
+    srv = HarmServer(max_device_bytes=int(budget_bytes), max_active=max_active, steps_per_chunk=steps_per_chunk)
     ids = {}
     t0 = time.perf_counter()
     done_at = {}
@@ -644,7 +652,7 @@ def bench_serving(count=24, tf=50.0, mean_gap_ms=2.0, seed=11, budget_bytes=32e9
     while len(done_at) < count:
         now = time.perf_counter() - t0
         while nsub < count and arrivals[nsub] <= now:
-            ids[srv.submit(reqs[nsub][1], tf)] = nsub
+            ids[srv.submit(reqs[nsub][1], reqs[nsub][2])] = nsub
             nsub += 1
         srv.poll()
         for rid, q in ids.items():
@@ -666,10 +674,10 @@ def bench_serving(count=24, tf=50.0, mean_gap_ms=2.0, seed=11, budget_bytes=32e9
     # launches (the one-solve-at-a-time baseline) and graph replays
     inv = {0: "OUTFLOW", 4: "POLARAXIS", 7: "PERIODIC", 1000: "OUTFLOW_COPY"}
     alone = {}
-    for mode in ("plain_launches", "graph"):
+    for mode in (("plain_launches", "graph") if one_at_a_time else ()):
         t1 = time.perf_counter()
         zu1 = 0.0
-        for kind, dom in reqs:
+        for kind, dom, tf in reqs:
             g = HarmGPU(*dom.n, dom.ng, dom.dx, lim=dom.lim, flux=dom.flux, bc=tuple(inv[b] for b in dom.bc),
                         gam=dom.gam, cour=dom.cour, tf=tf)
             g.upload_geometry(dom.gcov, dom.gcon, dom.gcovpert, dom.gdet, dom.conn, dom.floors)
@@ -689,11 +697,12 @@ def bench_serving(count=24, tf=50.0, mean_gap_ms=2.0, seed=11, budget_bytes=32e9
             g.close()
         t_seq = time.perf_counter() - t1
         alone[mode] = {"value": zu1 / t_seq, "seconds": t_seq}
-    return {"requests": count, "kinds": {k: sum(1 for kk, _ in reqs if kk == k) for k in ("torus", "bondi")},
-            "tf": tf, "value": zu / makespan, "unit": "zone-updates/s", "makespan_s": makespan,
+    return {"requests": count, "kinds": {k: sum(1 for r in reqs if r[0] == k) for k in ("torus", "bondi", "shock tube")},
+            "tf": {"torus": 50.0, "bondi": 50.0, "shock tube": 0.4}, "value": zu / makespan, "unit": "zone-updates/s", "makespan_s": makespan,
             "time_to_solution_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99))},
             "one_at_a_time": alone,
             "speedup_vs_one_at_a_time": {m: (zu / makespan) / v["value"] for m, v in alone.items()},
+            "slots": max_active, "steps_per_chunk": steps_per_chunk,
             "note": "wall clock; arrivals Poisson (mean gap %.0f ms, saturating); time-to-solution = finish - "
                     "arrival; one at a time = each solve alone in arrival order, 8 steps per host check, "
                     "with plain launches or with its captured step graph" % mean_gap_ms}

@@ -89,3 +89,17 @@ def minkowski_geometry(nt1):
     conn = np.zeros((gt1, 1, 4, 4, 4))
     floors = np.zeros((gt1, 1, 2))
     return gcov, gcon, gcovpert, gdet, conn, floors
+
+
+def domain(prob, ng=3, cour=0.5):
+    """One problem as a single-solve domain (the reference's own 1D run:
+    MC + HLL, bounds.c OUTFLOW copies at both ends), with the attributes the
+    context and the serving loop read."""
+    from .torus import Domain
+    n = prob.n
+    dom = Domain(n=(n, 1, 1), ng=ng, dx=(prob.dx, 1.0, 1.0), lim="MC", flux="HLL",
+                 bc=(1000, 1000, 0, 0, 0, 0), gam=prob.gam, cour=cour)
+    dom.gcov, dom.gcon, dom.gcovpert, dom.gdet, dom.conn, dom.floors = minkowski_geometry(n + 2 * ng)
+    dom.p = primitives(prob, ng)
+    dom.meta = dict(kind="shock tube", n=n, gam=prob.gam)
+    return dom

@@ -1,10 +1,11 @@
-"""Serving loop (hgpu_server_*): solves of different kinds and sizes that
+"""Serving loop (hgpu_server_*): solves of different kinds (Kerr tori in 2D
+and 3D, Bondi accretion, 1D shock tubes) and sizes that
 arrive while others run are admitted as memory frees up, run overlapped on
 the device, and each result is bit-identical to running that solve alone."""
 import numpy as np
 import pytest
 
-from harm_finalwham_b200 import bondi, torus
+from harm_finalwham_b200 import bondi, riemann, torus
 from harm_finalwham_b200.gpu import HarmGPU, HarmServer, context_bytes, make_config
 from tests.fixtures import same
 
@@ -19,7 +20,8 @@ def requests():
             torus.fm_torus(16, 16, 8, ng=3, a=0.9, beta=200.0, seed=3),
             torus.fm_torus(24, 16, 1, ng=6, lim="WENO5", seed=4),
             bondi.bondi(48, 32, ng=3, beta=300.0, seed=5),
-            torus.fm_torus(32, 16, 1, ng=3, a=0.2, seed=6)]
+            torus.fm_torus(32, 16, 1, ng=3, a=0.2, seed=6)] + \
+        [riemann.domain(p) for p in riemann.draw(2, seed=9, nmin=100, nmax=300)]
 
 
 def run_alone(dom, tf):
@@ -41,7 +43,9 @@ def run_alone(dom, tf):
 
 def test_serve_matches_alone():
     reqs = requests()
-    sizes = [context_bytes(make_config(d.n, d.ng, d.dx, lim=d.lim)) for d in reqs]
+    inv = {0: "OUTFLOW", 4: "POLARAXIS", 7: "PERIODIC", 1000: "OUTFLOW_COPY"}
+    sizes = [context_bytes(make_config(d.n, d.ng, d.dx, lim=d.lim, bc=tuple(inv[b] for b in d.bc))) for d in reqs]
+    assert min(sizes) > 0
     # room for about two solves at a time: the rest queue and are admitted as memory frees up
     srv = HarmServer(max_device_bytes=int(2.2 * max(sizes)), max_active=4, steps_per_chunk=3)
     try:
