@@ -544,6 +544,7 @@ def bench_riemann_batch(ninst=256, seed=2024, sample_single=12, check_every=25):
     w.run(check_every)
     w.close()
     b = batch_of(probs)
+    tuning = b.autotune()
     steps, ms, per, fin = b.run(check_every)
     b.close()
     zu = float(np.sum(np.array([p.n for p in probs]) * per))
@@ -553,6 +554,7 @@ def bench_riemann_batch(ninst=256, seed=2024, sample_single=12, check_every=25):
            "time_to_solution_ms": {"p50": float(np.percentile(fin, 50)), "p99": float(np.percentile(fin, 99)),
                                    "resolution_steps": check_every},
            "scheme": "MC + HLL + flux-CT, CFL 0.5, t = 0.4, N ~ U{200..2000}, seeded states",
+           "autotune": tuning,
            "timing": "device time (CUDA events) of the whole run incl. the done-flag polls"}
     # one solve at a time: (a) the plain host loop, one step_ch(1) and a time read per step;
     # (b) the same graph machinery on a batch of one

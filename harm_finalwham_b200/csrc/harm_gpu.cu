@@ -2098,7 +2098,7 @@ int hgpu_step_ch_timed(hgpu_ctx *x, int nsteps, float *ms, hgpu_stats *stats) {
 // differ only in register allocation, so results are identical whichever
 // is chosen; the state is restored at the end.
 int hgpu_autotune(hgpu_ctx *x, hgpu_tuning *out) {
-  if (!x || x->P.cell_inst) return HGPU_E_INVALID;
+  if (!x) return HGPU_E_INVALID;
   if (x->profiling) {
     set_err("hgpu_autotune: turn profiling off first");
     return HGPU_E_INVALID;
@@ -2109,8 +2109,14 @@ int hgpu_autotune(hgpu_ctx *x, hgpu_tuning *out) {
   double *sp = nullptr, *su = nullptr;
   int *sf = nullptr;
   Scalars *ss = nullptr;
+  Inst *si = nullptr;  // a batch's per-instance t, dt, done, step count
+  const size_t ib = sizeof(Inst) * (size_t)x->ninst;
   CUDA_TRY(cudaStreamSynchronize(x->stream));
   CUDA_TRY(cudaMallocAsync(&sp, pb, x->stream));
+  if (ib) {
+    CUDA_TRY(cudaMallocAsync(&si, ib, x->stream));
+    CUDA_TRY(cudaMemcpyAsync(si, x->inst, ib, cudaMemcpyDeviceToDevice, x->stream));
+  }
   CUDA_TRY(cudaMallocAsync(&sf, sizeof(int) * nz, x->stream));
   CUDA_TRY(cudaMallocAsync(&ss, sizeof(Scalars), x->stream));
   if (fv) CUDA_TRY(cudaMallocAsync(&su, pb, x->stream));
@@ -2123,6 +2129,7 @@ int hgpu_autotune(hgpu_ctx *x, hgpu_tuning *out) {
     cudaMemcpyAsync(x->pflag, sf, sizeof(int) * nz, cudaMemcpyDeviceToDevice, x->stream);
     cudaMemcpyAsync(x->sc, ss, sizeof(Scalars), cudaMemcpyDeviceToDevice, x->stream);
     if (fv) cudaMemcpyAsync(x->ucum, su, pb, cudaMemcpyDeviceToDevice, x->stream);
+    if (ib) cudaMemcpyAsync(x->inst, si, ib, cudaMemcpyDeviceToDevice, x->stream);
   };
   auto one_step = [&]() {
     clear_counters(x);
@@ -2166,6 +2173,7 @@ int hgpu_autotune(hgpu_ctx *x, hgpu_tuning *out) {
   cudaFreeAsync(sf, x->stream);
   cudaFreeAsync(ss, x->stream);
   if (su) cudaFreeAsync(su, x->stream);
+  if (si) cudaFreeAsync(si, x->stream);
   CUDA_TRY(cudaStreamSynchronize(x->stream));
   // the captured step holds the old variants
   if (x->graph_exec) cudaGraphExecDestroy(x->graph_exec);

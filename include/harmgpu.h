@@ -211,7 +211,8 @@ int hgpu_step_graph(hgpu_ctx *ctx, int nsteps, hgpu_stats *stats);
    update and inversion kernels, times two resident-blocks-per-SM variants
    (registers per thread vs warps per SM) on this context's own state and
    keeps the faster for later steps.  Results do not depend on the choice;
-   the state is left as it was.  *_ms: kernel milliseconds of one step per
+   the state is left as it was (for a batch context, every instance's t,
+   dt, done flag and step count too).  *_ms: kernel milliseconds of one step per
    candidate (0 where a family does not apply: weno_b without WENO5, flux and
    weno_b in the mixed-precision mode). */
 typedef struct {

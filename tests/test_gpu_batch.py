@@ -91,3 +91,25 @@ def test_single_context_with_outflow_copy_matches_oracle():
     pr = oracle_problem(pb, ng, "MC", "HLL", 0.4, dt0)
     Oracle().step(pr, 10)
     assert same(p, pr.p) and t == pr.t and dt == pr.dt
+
+
+def test_batch_autotune_keeps_state_and_results():
+    probs = riemann.draw(5, seed=21, nmin=40, nmax=90)
+    tfs = [0.4, 0.1, 0.4, 0.25, 0.4]
+    b1 = make_batch(probs, 3, "MC", "HLL", tfs)
+    b2 = make_batch(probs, 3, "MC", "HLL", tfs)
+    try:
+        before = b2.status()
+        tun = b2.autotune()
+        after = b2.status()
+        for x, y in zip(before, after):
+            assert np.array_equal(np.asarray(x), np.asarray(y))
+        assert set(tun) >= {"flux", "update", "invert"}
+        r1 = b1.run(check_every=5)
+        r2 = b2.run(check_every=5)
+        assert r1[0] == r2[0] and np.array_equal(r1[2], r2[2])
+        assert same(b1.download_state()[0], b2.download_state()[0])
+        assert np.array_equal(b1.status()[0], b2.status()[0])
+    finally:
+        b1.close()
+        b2.close()
