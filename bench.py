@@ -595,13 +595,14 @@ def bench_riemann_batch(ninst=256, seed=2024, sample_single=12, check_every=25):
     return out
 
 
-def serving_requests(count, seed):
-    """A seeded request stream of (kind, domain, end time): 45% Kerr torus,
-    30% Bondi (Schwarzschild, r_s = 8M, monopole field), both to t = 50 on
+def serving_requests(count, seed, shock_tubes=0.0):
+    """A seeded request stream of (kind, domain, end time): 60% Kerr torus,
+    40% Bondi (Schwarzschild, r_s = 8M, monopole field), both to t = 50 on
     grids from {32x32, 64x64, 128x128, 256x128} (2D) or {64x32x16, 96x48x32}
     (3D tori), spin a ~ U(0, 0.99), beta ~ logU[10, 1000], 4% internal-energy
-    noise; 25% 1D relativistic-MHD shock tubes (MC + HLL, CFL 0.5, N ~
-    U{200..2000}, seeded states) to t = 0.4; arrival gaps exponential."""
+    noise; arrival gaps exponential.  With shock_tubes > 0 that fraction of
+    the requests are 1D relativistic-MHD shock tubes instead (MC + HLL, CFL
+    0.5, N ~ U{200..2000}, seeded states, to t = 0.4)."""
     import numpy as np
 
     from harm_finalwham_b200 import bondi, riemann, torus
@@ -612,12 +613,11 @@ def serving_requests(count, seed):
     out = []
     for q in range(count):
         beta = 10.0 ** rng.uniform(1.0, 3.0)
-        u = rng.random()
-        if u < 0.25:
+        if shock_tubes and rng.random() < shock_tubes:
             prob = riemann.draw(1, seed=int(rng.integers(1 << 30)))[0]
             out.append(("shock tube", riemann.domain(prob), 0.4))
             continue
-        if u < 0.25 + 0.45:
+        if rng.random() < 0.6:
             a = rng.uniform(0.0, 0.99)
             if rng.random() < 0.2:
                 n = grids3[rng.integers(len(grids3))]
@@ -633,8 +633,8 @@ def serving_requests(count, seed):
     return out
 
 
-def bench_serving(count=32, mean_gap_ms=2.0, seed=11, budget_bytes=32e9, max_active=64, steps_per_chunk=8,
-                  one_at_a_time=True):
+def bench_serving(count=24, mean_gap_ms=2.0, seed=11, budget_bytes=32e9, max_active=32, steps_per_chunk=8,
+                  one_at_a_time=True, shock_tubes=0.0):
     """Continuous batching: requests arrive on a seeded Poisson clock fast
     enough to keep the GPU saturated and go through hgpu_server (admission by
     device footprint, overlapped solves, each solve's step replayed from its
@@ -643,7 +643,7 @@ def bench_serving(count=32, mean_gap_ms=2.0, seed=11, budget_bytes=32e9, max_act
 
     from harm_finalwham_b200.gpu import HarmGPU, HarmServer
 
-    reqs = serving_requests(count, seed)
+    reqs = serving_requests(count, seed, shock_tubes)
     rng = np.random.default_rng(seed + 1)
     arrivals = np.cumsum(rng.exponential(mean_gap_ms / 1e3, count))
     srv = HarmServer(max_device_bytes=int(budget_bytes), max_active=max_active, steps_per_chunk=steps_per_chunk)
