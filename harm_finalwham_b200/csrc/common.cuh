@@ -208,7 +208,7 @@ constexpr int W5_PLANES = 4;
 #define HG_MINB_FLUX 4
 #endif
 #ifndef HG_MINB_UPDATE
-#define HG_MINB_UPDATE 1
+#define HG_MINB_UPDATE 4
 #endif
 #ifndef HG_MINB_INVERT
 #define HG_MINB_INVERT 1

@@ -228,6 +228,47 @@ __global__ void pi2u_kernel(Dims d, Params P, const double *__restrict__ p, cons
   for (int pl = 0; pl < NPR; pl++) u[pl * d.nz + z] = U[pl];
 }
 
+// source() -> source_conn() (phys.c:578-752): the connection contraction of
+// T^mu_nu for the state pbz (q, e formed from it), times gdet
+__device__ __forceinline__ void source_conn(const Dims &d, const double *__restrict__ G, long long ij,
+                                            const double *pbz, const State &q, const EM &e, const Metric &m,
+                                            double gam, double *dUg) {
+  double dUconn[4] = {0., 0., 0., 0.};
+  const double *conn = G + (long long)G_CONN * d.nij + ij;
+  // each T^jj_kk row is contracted as soon as it is formed; every
+  // dUconn[l] still adds its terms in the order jj, then kk
+#pragma unroll
+  for (int jj = 0; jj < 4; jj++) {
+    double row[4];
+    mhd_row(pbz, jj, gam, q, e, row);
+#pragma unroll
+    for (int l = 0; l < 4; l++) {
+      double s = dUconn[l];
+#pragma unroll
+      for (int kk = 0; kk < 4; kk++) s += row[kk] * __ldg(conn + (long long)((kk * 4 + l) * 4 + jj) * d.nij);
+      dUconn[l] = s;
+    }
+  }
+#pragma unroll
+  for (int l = 0; l < 4; l++) {
+    double s = dUconn[l];
+#pragma unroll
+    for (int jj = 0; jj < 4; jj++) s += -pbz[RHO] * q.ucon[jj] * __ldg(conn + (long long)((0 * 4 + l) * 4 + jj) * d.nij);
+    dUconn[l] = s;
+  }
+  // dU = sum of the NUMSOURCES components; only GEOMSOURCE is nonzero
+  double full[NPR] = {0., dUconn[0], dUconn[1], dUconn[2], dUconn[3], 0., 0., 0.};
+#pragma unroll
+  for (int pl = 0; pl < NPR; pl++) {
+    double comp0 = 0. + m.g * full[pl];
+    double acc = 0.;
+    acc += comp0;
+#pragma unroll
+    for (int l = 1; l < 7; l++) acc += 0.0;
+    dUg[pl] = acc;
+  }
+}
+
 template <int MB>
 __global__ void __launch_bounds__(128, MB) conserve_kernel(
     Dims d, Params P, Box box, const double *pi, const double *pb, double *__restrict__ uf,
@@ -245,76 +286,9 @@ __global__ void __launch_bounds__(128, MB) conserve_kernel(
   const long long ij = gix(d, i, j);
   double dt, gam, dx1;
   if (!zone_step(P, sc, z, i, dt, gam, dx1)) return;
-    Metric m;
-    load_metric(G, d, ij, G_CENT, m);
-    int err = 0;
     double Ui[NPR], dUg[NPR], dUr[NPR];
-    if (fv) {
-      // advance_finitevolume (advance.c:245-501): Ui is the stored conserved
-      // state; the first substep takes the last step's ucum as ui
-      // (advance.c:330-343)
-      if (timeorder == 0) {
-#pragma unroll
-        for (int pl = 0; pl < NPR; pl++) {
-          Ui[pl] = ucum[pl * nz + z];
-          ui[pl * nz + z] = Ui[pl];
-        }
-      } else {
-#pragma unroll
-        for (int pl = 0; pl < NPR; pl++) Ui[pl] = ui[pl * nz + z];
-      }
-    } else {
-      double pr[NPR];
-      load_prim(pi, d, z, pr);
-      State q;
-      EM e;
-      if (get_state(pr, m, q)) err |= ERR_UTCALC_DISCR;
-      em_prepare(pr, m, q, e);
-      primtoflux(pr, q, e, 0, m, gam, Ui);
-    }
-    double pbz[NPR];
-    load_prim(pb, d, z, pbz);
-    {
-      // source() -> source_conn() (phys.c:578-752)
-      State q;
-      EM e;
-      if (get_state(pbz, m, q)) err |= ERR_UTCALC_DISCR;
-      em_prepare(pbz, m, q, e);
-      double dUconn[4] = {0., 0., 0., 0.};
-      const double *conn = G + (long long)G_CONN * d.nij + ij;
-      // each T^jj_kk row is contracted as soon as it is formed; every
-      // dUconn[l] still adds its terms in the order jj, then kk
-#pragma unroll
-      for (int jj = 0; jj < 4; jj++) {
-        double row[4];
-        mhd_row(pbz, jj, gam, q, e, row);
-#pragma unroll
-        for (int l = 0; l < 4; l++) {
-          double s = dUconn[l];
-#pragma unroll
-          for (int kk = 0; kk < 4; kk++) s += row[kk] * __ldg(conn + (long long)((kk * 4 + l) * 4 + jj) * d.nij);
-          dUconn[l] = s;
-        }
-      }
-#pragma unroll
-      for (int l = 0; l < 4; l++) {
-        double s = dUconn[l];
-#pragma unroll
-        for (int jj = 0; jj < 4; jj++) s += -pbz[RHO] * q.ucon[jj] * __ldg(conn + (long long)((0 * 4 + l) * 4 + jj) * d.nij);
-        dUconn[l] = s;
-      }
-      // dU = sum of the NUMSOURCES components; only GEOMSOURCE is nonzero
-      double full[NPR] = {0., dUconn[0], dUconn[1], dUconn[2], dUconn[3], 0., 0., 0.};
-#pragma unroll
-      for (int pl = 0; pl < NPR; pl++) {
-        double comp0 = 0. + m.g * full[pl];
-        double acc = 0.;
-        acc += comp0;
-#pragma unroll
-        for (int l = 1; l < 7; l++) acc += 0.0;
-        dUg[pl] = acc;
-      }
-    }
+    // the flux differences first: their ~50 independent loads are in flight
+    // together before the arithmetic of U(pi) and the source term
     // flux2dUavg (advance.c:741-914) with the B fluxes of flux_ct (fluxct.c:724-781)
     {
       const double idx1 = 1.0 / dx1, idx2 = 1.0 / P.dx2, idx3 = 1.0 / P.dx3;
@@ -348,6 +322,59 @@ __global__ void __launch_bounds__(128, MB) conserve_kernel(
         }
         dUr[pl] = a1 + a2 + a3;
       }
+    }
+    Metric m;
+    load_metric(G, d, ij, G_CENT, m);
+    int err = 0;
+    if (fv) {
+      // advance_finitevolume (advance.c:245-501): Ui is the stored conserved
+      // state; the first substep takes the last step's ucum as ui
+      // (advance.c:330-343)
+      if (timeorder == 0) {
+#pragma unroll
+        for (int pl = 0; pl < NPR; pl++) {
+          Ui[pl] = ucum[pl * nz + z];
+          ui[pl * nz + z] = Ui[pl];
+        }
+      } else {
+#pragma unroll
+        for (int pl = 0; pl < NPR; pl++) Ui[pl] = ui[pl * nz + z];
+      }
+      double pbz[NPR];
+      load_prim(pb, d, z, pbz);
+      State q;
+      EM e;
+      if (get_state(pbz, m, q)) err |= ERR_UTCALC_DISCR;
+      em_prepare(pbz, m, q, e);
+      source_conn(d, G, ij, pbz, q, e, m, gam, dUg);
+    } else if (pi == pb) {
+      // a first substep: U(pi) and the source read the same state, whose
+      // get_state and field terms are formed once
+      double pbz[NPR];
+      load_prim(pb, d, z, pbz);
+      State q;
+      EM e;
+      if (get_state(pbz, m, q)) err |= ERR_UTCALC_DISCR;
+      em_prepare(pbz, m, q, e);
+      primtoflux(pbz, q, e, 0, m, gam, Ui);
+      source_conn(d, G, ij, pbz, q, e, m, gam, dUg);
+    } else {
+      {
+        double pr[NPR];
+        load_prim(pi, d, z, pr);
+        State qi;
+        EM ei;
+        if (get_state(pr, m, qi)) err |= ERR_UTCALC_DISCR;
+        em_prepare(pr, m, qi, ei);
+        primtoflux(pr, qi, ei, 0, m, gam, Ui);
+      }
+      double pbz[NPR];
+      load_prim(pb, d, z, pbz);
+      State q;
+      EM e;
+      if (get_state(pbz, m, q)) err |= ERR_UTCALC_DISCR;
+      em_prepare(pbz, m, q, e);
+      source_conn(d, G, ij, pbz, q, e, m, gam, dUg);
     }
     // dUtoU (advance.c:922-949)
     double Uf[NPR], Ucum[NPR];
