@@ -91,3 +91,36 @@ def divb_maxavg(p, gdet, ng, dx, n, interior=False):
             m &= (J - g2 >= 2) & (J - g2 <= n2 - 2)
         return float(d[m].max())
     return float(d.max()), float(d.mean())
+
+
+def divb_scaled_max(p, gdet, ng, dx, n):
+    """The flux-CT corner divergence of divb_max without the local
+    normalisation (which divides by the signed sum of the corner averages and
+    spikes where that sum nearly cancels): max |div(gdet B)| times max(dx)
+    over max |gdet B| on the grid, a round-off measure that does not depend
+    on the grid size."""
+    n1, n2, n3 = n
+    g1, g2, g3 = (ng if n1 > 1 else 0), (ng if n2 > 1 else 0), (ng if n3 > 1 else 0)
+    gc = gdet[:p.shape[0], :p.shape[1], 7][:, :, None]
+    Fg = p[..., 5:8] * gc[..., None]
+    i = np.arange(1, n1) + g1
+    j = np.arange(2, n2 - 1) + g2
+    k = (np.arange(0, n3) if n3 > 1 else np.array([0])) + g3
+    I, J, K = np.meshgrid(i, j, k, indexing="ij")
+    km = K - (1 if n3 > 1 else 0)
+
+    def for1(a):
+        return 0.5 * (0.5 * (Fg[a, J, K, 0] + Fg[a, J - 1, K, 0]) + 0.5 * (Fg[a, J, km, 0] + Fg[a, J - 1, km, 0]))
+
+    def for2(b):
+        return 0.5 * (0.5 * (Fg[I, b, K, 1] + Fg[I - 1, b, K, 1]) + 0.5 * (Fg[I, b, km, 1] + Fg[I - 1, b, km, 1]))
+
+    def for3(c):
+        return 0.5 * (0.5 * (Fg[I, J, c, 2] + Fg[I, J - 1, c, 2]) + 0.5 * (Fg[I - 1, J, c, 2] + Fg[I - 1, J - 1, c, 2]))
+
+    dxs = (dx[0] if n1 > 1 else 1.0, dx[1] if n2 > 1 else 1.0, dx[2] if n3 > 1 else 1.0)
+    diff = (for1(I) - for1(I - 1)) / dxs[0] + (for2(J) - for2(J - 1)) / dxs[1]
+    if n3 > 1:
+        diff = diff + (for3(K) - for3(km)) / dxs[2]
+    dmax = max(dx[0], dx[1], dx[2] if n3 > 1 else 0.0)
+    return float(np.max(np.abs(diff)) * dmax / (np.max(np.abs(Fg)) + SMALL))
