@@ -33,6 +33,7 @@ owns n3 planes; ghost planes exchanged over NCCL twice per stage, the ndt
 minima all-reduced once per step).
 """
 import argparse
+import datetime
 import json
 import os
 import re
@@ -165,12 +166,10 @@ def bench_decomp(args, rank, world):
     NCCL after each half-stage and the per-direction ndt minima all-reduced;
     with one rank the planes wrap onto the same context, which measures the
     cost of the phase-driven step against the one-call step."""
-    import datetime
-
     import torch
 
     from harm_finalwham_b200 import torus
-    from harm_finalwham_b200.decomp import CollectiveTransport, SplitRun, _Sub, split_x3
+    from harm_finalwham_b200.decomp import CollectiveTransport, SplitRun, SlabContext, split_x3
     from harm_finalwham_b200.gpu import HarmGPU, load_library
 
     n1, n2, n3, lim, flux = WORKLOADS[args.workload]
@@ -192,7 +191,7 @@ def bench_decomp(args, rank, world):
         g.set_tuning(dict(zip(("flux", "weno_b", "update", "invert"), (int(v) for v in args.tuning.split(",")))))
     else:
         g.autotune()
-    sub = _Sub(g)
+    sub = SlabContext(g)
     run = SplitRun([g], CollectiveTransport(sub))
     run.start(init_dt=True)
     run.step(args.warmup, stats=False)
@@ -360,7 +359,7 @@ def bench_ours(args, rank, world):
         import torch
         import torch.distributed as dist
         torch.cuda.set_device(0)
-        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=300))
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
 
     def barrier():
         if dist is not None:

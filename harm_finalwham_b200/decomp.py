@@ -67,7 +67,7 @@ def join_x3(parts):
     return np.concatenate(parts, axis=2)
 
 
-class _Sub:
+class SlabContext:
     """What a transport needs from one subdomain (a HarmGPU context)."""
 
     def __init__(self, ctx):
@@ -234,7 +234,7 @@ class SplitRun:
     def local(cls, dom, nslabs, precision="fp64", init_dt=False):
         """All `nslabs` slabs of `dom` as contexts on the current device."""
         ctxs = [HarmGPU.from_problem(split_x3(dom, nslabs, r), precision=precision) for r in range(nslabs)]
-        run = cls(ctxs, LocalTransport([_Sub(c) for c in ctxs]))
+        run = cls(ctxs, LocalTransport([SlabContext(c) for c in ctxs]))
         run.start(init_dt=init_dt)
         return run
 

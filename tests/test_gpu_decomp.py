@@ -64,7 +64,7 @@ def test_split_run_matches_whole_domain(name, kw, nslabs):
 def test_collective_transport_on_one_rank_matches_whole_domain():
     """The multi-GPU transport with one rank (no process group): the planes
     wrap onto the same context on its own stream, no host synchronisation."""
-    from harm_finalwham_b200.decomp import CollectiveTransport, _Sub
+    from harm_finalwham_b200.decomp import CollectiveTransport, SlabContext
     dom = _torus(n=(32, 16, 16), ng=3, lim="PARA", flux="HLL", timeorder=4, utoprim="JON",
                  doenoflux="ENOFINITEVOLUME")
     with HarmGPU.from_problem(dom) as whole:
@@ -73,7 +73,7 @@ def test_collective_transport_on_one_rank_matches_whole_domain():
         whole.step_ch(5)
         p_w, f_w, t_w, dt_w = whole.download_state()
     g = HarmGPU.from_problem(dom)
-    run = SplitRun([g], CollectiveTransport(_Sub(g)))
+    run = SplitRun([g], CollectiveTransport(SlabContext(g)))
     try:
         run.start(init_dt=True)
         run.step(5)
