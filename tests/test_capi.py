@@ -73,3 +73,27 @@ def test_configuration_validation_on_the_host():
     base = context_bytes(make_config((32, 32, 1), 3, (0.1, 0.1, 1.0)))
     assert context_bytes(make_config((32, 32, 1), 3, (0.1, 0.1, 1.0), doenoflux="ENOFINITEVOLUME")) > base
     assert context_bytes(make_config((32, 32, 1), 3, (0.1, 0.1, 1.0), timeorder=4)) > base
+
+
+def test_split_entry_points_reject_bad_arguments_without_gpu_work():
+    # every x3-split entry point validates its arguments before touching the
+    # device: a NULL context (or NULL output) is HGPU_E_INVALID
+    HGPU_E_INVALID = 1
+    L = load_library()
+    buf = ctypes.create_string_buffer(64)
+    nb = ctypes.c_size_t()
+    st = ctypes.c_void_p()
+    assert L.hgpu_halo_bytes(None, ctypes.byref(nb)) == HGPU_E_INVALID
+    for side in (0, 1):
+        assert L.hgpu_halo_pack(None, 0, side, 1, ctypes.addressof(buf)) == HGPU_E_INVALID
+        assert L.hgpu_halo_unpack(None, 0, side, 0, ctypes.addressof(buf)) == HGPU_E_INVALID
+    assert L.hgpu_stats_clear(None) == HGPU_E_INVALID
+    assert L.hgpu_stats_read(None, None) == HGPU_E_INVALID
+    assert L.hgpu_stage_advance(None, 0) == HGPU_E_INVALID
+    assert L.hgpu_stage_fixup(None, 0) == HGPU_E_INVALID
+    assert L.hgpu_dt_probe(None) == HGPU_E_INVALID
+    assert L.hgpu_step_end(None, 1) == HGPU_E_INVALID
+    assert L.hgpu_ndt_pack(None, ctypes.addressof(buf)) == HGPU_E_INVALID
+    assert L.hgpu_ndt_unpack(None, ctypes.addressof(buf)) == HGPU_E_INVALID
+    assert L.hgpu_stream(None, ctypes.byref(st)) == HGPU_E_INVALID
+    assert L.hgpu_autotune(None, None) == HGPU_E_INVALID
