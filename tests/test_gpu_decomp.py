@@ -27,17 +27,29 @@ SCHEMES = [
     ("para_laxf_rk4_jon_fv", dict(n=(32, 16, 16), ng=3, lim="PARA", flux="LAXF", timeorder=4, utoprim="JON",
                                   doenoflux="ENOFINITEVOLUME")),
     ("weno5_hll_rk3", dict(n=(24, 16, 24), ng=6, lim="WENO5", flux="HLL", timeorder=3)),
+    # the FM torus problem file's own scheme with all MAXBND = 11 ghosts
+    ("fishmon_maxbnd11", dict(n=(24, 16, 44), ng=11, lim="PARA", flux="HLL", timeorder=4, utoprim="JON",
+                              doenoflux="ENOFINITEVOLUME")),
 ]
 
 
 @pytest.mark.parametrize("name,kw", SCHEMES, ids=[s[0] for s in SCHEMES])
 @pytest.mark.parametrize("nslabs", [1, 2, 4])
 def test_split_run_matches_whole_domain(name, kw, nslabs):
+    _split_vs_whole(kw, nslabs, "fp64")
+
+
+@pytest.mark.parametrize("nslabs", [2, 4])
+def test_split_run_matches_whole_domain_mixed_precision(nslabs):
+    _split_vs_whole(SCHEMES[2][1], nslabs, "mixed")
+
+
+def _split_vs_whole(kw, nslabs, precision):
     dom = _torus(**kw)
     if dom.n[2] // nslabs < dom.g[2]:
         pytest.skip("slab thinner than the ghost planes")
     nsteps = 6
-    with HarmGPU.from_problem(dom) as whole:
+    with HarmGPU.from_problem(dom, precision=precision) as whole:
         # the generator's ghost planes are evaluated, not copied: start both
         # runs from bound_prim, as the reference's init does
         whole.bound_prim(0)
@@ -45,7 +57,7 @@ def test_split_run_matches_whole_domain(name, kw, nslabs):
         st_w = whole.step_ch(nsteps)
         p_w, f_w, t_w, dt_w = whole.download_state()
         p_w, f_w = whole.active(p_w), whole.active(f_w)
-    run = SplitRun.local(dom, nslabs, init_dt=True)
+    run = SplitRun.local(dom, nslabs, precision=precision, init_dt=True)
     try:
         _, _, _, dt_s0 = run.download()
         assert dt_s0 == dt0
