@@ -159,7 +159,7 @@ class CollectiveTransport:
     without a host synchronisation.
     """
 
-    def __init__(self, sub, group=None):
+    def __init__(self, sub, group=None, host_staging=None):
         import torch
         import torch.distributed as dist
         self.dist = dist
@@ -175,6 +175,17 @@ class CollectiveTransport:
         self.recv_lo = torch.empty_like(self.send_lo)
         self.recv_hi = torch.empty_like(self.send_lo)
         self.ndt = torch.empty(3, dtype=torch.int64, device=dev)
+        # a backend that cannot move device memory (gloo) gets the planes
+        # through host copies, as a non-CUDA-aware MPI would (blocking copies
+        # on the context's stream; pageable buffers, so that no host-allocator
+        # events outlive the context)
+        if host_staging is None:
+            host_staging = up and dev.type == "cuda" and dist.get_backend(group) != "nccl"
+        self.staged = bool(host_staging)
+        if self.staged:
+            self.h = {k: torch.empty(sub.nbytes, dtype=torch.uint8) for k in ("send_lo", "send_hi", "recv_lo",
+                                                                               "recv_hi")}
+            self.h_ndt = torch.empty(3, dtype=torch.int64)
 
     def _on_stream(self):
         import torch
@@ -200,19 +211,33 @@ class CollectiveTransport:
             # upper ghosts; tag 1: its upper edge, the right neighbour's lower
             # ghosts.  The issue order is the same on every rank, which is
             # what NCCL matches sends and receives by.
-            ops = [dist.P2POp(dist.isend, self.send_lo[:nb], left, self.group, 0),
-                   dist.P2POp(dist.irecv, self.recv_hi[:nb], right, self.group, 0),
-                   dist.P2POp(dist.isend, self.send_hi[:nb], right, self.group, 1),
-                   dist.P2POp(dist.irecv, self.recv_lo[:nb], left, self.group, 1)]
+            if self.staged:
+                h = self.h
+                h["send_lo"][:nb].copy_(self.send_lo[:nb])
+                h["send_hi"][:nb].copy_(self.send_hi[:nb])
+                bufs = (h["send_lo"], h["recv_hi"], h["send_hi"], h["recv_lo"])
+            else:
+                bufs = (self.send_lo, self.recv_hi, self.send_hi, self.recv_lo)
+            ops = [dist.P2POp(dist.isend, bufs[0][:nb], left, self.group, 0),
+                   dist.P2POp(dist.irecv, bufs[1][:nb], right, self.group, 0),
+                   dist.P2POp(dist.isend, bufs[2][:nb], right, self.group, 1),
+                   dist.P2POp(dist.irecv, bufs[3][:nb], left, self.group, 1)]
             for w in dist.batch_isend_irecv(ops):
                 w.wait()
+            if self.staged:
+                self.recv_lo[:nb].copy_(self.h["recv_lo"][:nb])
+                self.recv_hi[:nb].copy_(self.h["recv_hi"][:nb])
             s.unpack(stage, 0, with_pflag, self.recv_lo)
             s.unpack(stage, 1, with_pflag, self.recv_hi)
 
     def ndt_min(self):
         with self._on_stream():
             self.sub.ndt_pack(self.ndt)
-            if self.world > 1:
+            if self.world > 1 and self.staged:
+                self.h_ndt.copy_(self.ndt)
+                self.dist.all_reduce(self.h_ndt, op=self.dist.ReduceOp.MIN, group=self.group)
+                self.ndt.copy_(self.h_ndt)
+            elif self.world > 1:
                 self.dist.all_reduce(self.ndt, op=self.dist.ReduceOp.MIN, group=self.group)
             self.sub.ndt_unpack(self.ndt)
 

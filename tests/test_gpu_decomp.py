@@ -95,3 +95,65 @@ def test_collective_transport_on_one_rank_matches_whole_domain():
     assert (t_s, dt_s) == (t_w, dt_w)
     assert _same_bits(p_s, p_w[3:-3, 3:-3, 3:-3])
     assert np.array_equal(f_s, f_w[3:-3, 3:-3, 3:-3])
+
+
+def _gloo_rank(rank, world, port, kw, nsteps, out):
+    import datetime
+    import os
+
+    import torch.distributed as dist
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=120))
+    try:
+        from harm_finalwham_b200.decomp import CollectiveTransport, SlabContext, split_x3
+        dom = _torus(**kw)
+        g = HarmGPU.from_problem(split_x3(dom, world, rank))
+        tr = CollectiveTransport(SlabContext(g))
+        assert tr.staged and tr.world == world
+        run = SplitRun([g], tr)
+        try:
+            run.start(init_dt=True)
+            st = run.step(nsteps)
+            p, f, t, dt = run.download()
+        finally:
+            run.close()
+        out[rank] = (p, f, t, dt, st.newton_iters)
+        dist.barrier()
+    finally:
+        dist.destroy_process_group()
+
+
+def test_two_processes_through_the_collective_transport_match_whole_domain():
+    """Two ranks (processes) on one GPU, each with its own slab context; the
+    planes and the ndt minima go through torch.distributed (gloo, through
+    pinned host copies), so no kernel ever waits on the other process."""
+    import socket
+
+    import torch.multiprocessing as mp
+    kw, nsteps, world = SCHEMES[0][1], 4, 2
+    dom = _torus(**kw)
+    with HarmGPU.from_problem(dom) as whole:
+        whole.bound_prim(0)
+        whole.init_dt()
+        st_w = whole.step_ch(nsteps)
+        p_w, f_w, t_w, dt_w = whole.download_state()
+        p_w, f_w = whole.active(p_w), whole.active(f_w)
+    sock = socket.socket()
+    sock.bind(("127.0.0.1", 0))
+    port = sock.getsockname()[1]
+    sock.close()
+    ctx = mp.get_context("spawn")
+    out = ctx.Manager().dict()
+    procs = [ctx.Process(target=_gloo_rank, args=(r, world, port, kw, nsteps, out)) for r in range(world)]
+    for pr in procs:
+        pr.start()
+    for pr in procs:
+        pr.join(300)
+        assert pr.exitcode == 0
+    p_s = np.concatenate([out[r][0] for r in range(world)], axis=2)
+    f_s = np.concatenate([out[r][1] for r in range(world)], axis=2)
+    assert all((out[r][2], out[r][3]) == (t_w, dt_w) for r in range(world))
+    assert _same_bits(p_s, p_w)
+    assert np.array_equal(f_s, f_w)
+    assert sum(out[r][4] for r in range(world)) == st_w.newton_iters
