@@ -502,7 +502,7 @@ def bench_ours(args, rank, world):
         result["batch_riemann1d"] = bench_riemann_batch()
         result["serving"] = bench_serving()
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        procs = min(host_cores(), args.cpu_procs)
+        procs = min(host_cores(), args.cpu_procs) if args.cpu_procs > 0 else host_cores()
         cs = cpu_sample(args.workload)
         v, why = run_reference(cs, args.cpu_steps, 2, procs)
         result["cpu_baseline"] = ({"value": v, "unit": "zone-updates/s", "cores": procs, "kind": "reference",
@@ -786,7 +786,8 @@ def main():
                     help="steps of the FP64-vs-mixed comparison (default: warm-up + timed steps)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-steps", type=int, default=3)
-    ap.add_argument("--cpu-procs", type=int, default=16)
+    ap.add_argument("--cpu-procs", type=int, default=0,
+                    help="processes of the reference CPU build (default: every host core this process may use)")
     ap.add_argument("--tuning", default=None,
                     help="blocks per SM for flux,weno_b,update,invert instead of running the autotuner")
     ap.add_argument("--kernels-only", action="store_true",
@@ -801,7 +802,7 @@ def main():
     if args.impl == "reference":
         if rank != 0:
             return 0
-        procs = min(host_cores(), args.cpu_procs)
+        procs = min(host_cores(), args.cpu_procs) if args.cpu_procs > 0 else host_cores()
         cs = cpu_sample(args.workload)
         # each step: one step of every process's bounded sample
         v, why = run_reference(cs, args.steps, args.warmup, procs)
