@@ -40,7 +40,10 @@ import tempfile
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 OUT = os.path.join(HERE, "_ref")
-DEFAULT_REF = "/root/reference"
+# the reference source tree: HARM_REFERENCE_DIR, else a checkout named
+# "reference" beside this repository
+DEFAULT_REF = os.environ.get("HARM_REFERENCE_DIR",
+                             os.path.normpath(os.path.join(HERE, os.pardir, os.pardir, "reference")))
 
 HOIST_FILES = ["utoprim_jon.c", "utoprim_jon_eos.c", "u2p_util.c", "utoprim_2d_final.c",
                "utoprim_1d_final.c", "utoprim_5d2_final.c", "dudp_calc.c"]
@@ -192,11 +195,20 @@ int bound_prim_user_after_mpi(int boundstage, FTYPE prim[][N2M][N3M][NPR])
 """
 
 
+REPO = os.path.dirname(HERE)
+SHIM = os.path.join(REPO, "harm_finalwham_b200", "dropin", "step_ch_gpu.c")
+GPULIB = os.path.join(REPO, "harm_finalwham_b200", "lib")
+
+
 def build(ref, n1, n2, n3, lim, flux, cour, maxbnd, name=None, keep=False, verbose=False, timeorder=2,
-          utoprim="2DFINAL", fv=False):
+          utoprim="2DFINAL", fv=False, gpu_shim=False):
+    """gpu_shim: link the drop-in GPU step_ch (harm_finalwham_b200/dropin/step_ch_gpu.c
+    against lib/libharmgpu.so) in place of the reference's own, which is kept
+    as harm_cpu_step_ch (the only change to step_ch.c: the name at :16)."""
     os.makedirs(OUT, exist_ok=True)
     name = name or (f"harm_ref_{n1}x{n2}x{n3}_{lim}_{flux}" + (f"_rk{timeorder}" if timeorder != 2 else "")
-                    + ("_jon" if utoprim == "JON" else "") + ("_fv" if fv else ""))
+                    + ("_jon" if utoprim == "JON" else "") + ("_fv" if fv else "")
+                    + ("_gpushim" if gpu_shim else ""))
     scratch = tempfile.mkdtemp(prefix="harmref_")
     try:
         for fn in os.listdir(ref):
@@ -240,9 +252,21 @@ def build(ref, n1, n2, n3, lim, flux, cour, maxbnd, name=None, keep=False, verbo
             f.write(bc)
         shutil.copy(os.path.join(HERE, "ref_harness.c"), os.path.join(scratch, "ref_harness.c"))
         srcs = SOURCES + ["ref_harness.c"]
+        extra = []
+        if gpu_shim:
+            p = os.path.join(scratch, "step_ch.c")
+            with open(p) as f:
+                t = f.read()
+            t = sub_once(t, "int step_ch(void)\n{", "int harm_cpu_step_ch(void)\n{", where="step_ch.c")
+            with open(p, "w") as f:
+                f.write(t)
+            shutil.copy(SHIM, os.path.join(scratch, "step_ch_gpu.c"))
+            srcs = srcs + ["step_ch_gpu.c"]
+            extra = ["-I" + os.path.join(REPO, "include"), "-L" + GPULIB, "-lharmgpu",
+                     "-Wl,-rpath,$ORIGIN/../../harm_finalwham_b200/lib"]
         exe = os.path.join(OUT, name)
         cmd = ["gcc", "-O2", "-ffp-contract=off", "-fno-fast-math", "-fcommon", "-w",
-               "-mcmodel=medium", "-o", exe] + srcs + ["-lm"]
+               "-mcmodel=medium", "-o", exe] + srcs + extra + ["-lm"]
         r = subprocess.run(cmd, cwd=scratch, capture_output=True, text=True)
         if r.returncode != 0:
             sys.stderr.write(r.stderr[-6000:])
@@ -257,7 +281,7 @@ def build(ref, n1, n2, n3, lim, flux, cour, maxbnd, name=None, keep=False, verbo
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--ref", default=os.environ.get("HARM_REFERENCE_DIR", DEFAULT_REF))
+    ap.add_argument("--ref", default=DEFAULT_REF)
     ap.add_argument("--n1", type=int, default=64)
     ap.add_argument("--n2", type=int, default=64)
     ap.add_argument("--n3", type=int, default=1)
@@ -270,11 +294,13 @@ def main():
     ap.add_argument("--timeorder", type=int, default=2, choices=[1, 2, 3, 4])
     ap.add_argument("--utoprim", default="2DFINAL", choices=sorted(UTOPRIMS))
     ap.add_argument("--fv", action="store_true", help="DOENOFLUX = ENOFINITEVOLUME (the problem file's own)")
+    ap.add_argument("--gpu-shim", action="store_true",
+                    help="link the drop-in GPU step_ch (harm_finalwham_b200/dropin) in place of the CPU one")
     a = ap.parse_args()
     if not os.path.isdir(a.ref):
         raise SystemExit(f"reference tree not found: {a.ref}")
     build(a.ref, a.n1, a.n2, a.n3, a.lim, a.flux, a.cour, a.maxbnd, a.name, a.keep, verbose=True,
-          timeorder=a.timeorder, utoprim=a.utoprim, fv=a.fv)
+          timeorder=a.timeorder, utoprim=a.utoprim, fv=a.fv, gpu_shim=a.gpu_shim)
 
 
 if __name__ == "__main__":

@@ -182,14 +182,20 @@ class RefDump:
         return self._f(tag, "pk").reshape((2,) + self.NM + (NPR,))
 
     def geom(self, name):
+        """Geometry array, x3 extent 1 when the harness wrote only the first
+        x3 plane (--geomplane)."""
         gm = tuple(n + s for n, s in zip(self.NM, self.sh))
+        nm = self.NM
+        if self.meta.get("GEOMPLANE", 0):
+            gm = gm[:2] + (1,)
+            nm = nm[:2] + (1,)
         shapes = {"gcov": (LOCS, 4, 4), "gcon": (LOCS, 4, 4), "gcovpert": (LOCS, 4), "gdet": (LOCS,)}
         if name in shapes:
             return self._f("init", name).reshape(gm + shapes[name])
         if name == "conn":
-            return self._f("init", name).reshape(self.NM + (4, 4, 4))
+            return self._f("init", name).reshape(nm + (4, 4, 4))
         if name == "floors":
-            return self._f("init", name).reshape(self.NM + (2,))
+            return self._f("init", name).reshape(nm + (2,))
         raise KeyError(name)
 
     def to_problem(self, ng, tag="init"):

@@ -16,6 +16,20 @@
  *   and prints the CLOCK_MONOTONIC start/end of every step to stderr (the
  *   CPU baseline's step-loop timing).  "-" as outdir writes no files.
  *
+ * options (before <outdir>):
+ *   --phimodes <seed>  multiplies rho of every active zone by
+ *                      1 + 0.02 sum_{m=1..4} A_m cos(m phi + phi_m), A_m ~ U(0,1),
+ *                      phi_m ~ U(0,2pi) drawn from <seed> (splitmix64), after
+ *                      the reference's init() and before its first step, then
+ *                      repeats init's own closing sequence on the perturbed
+ *                      state (initbase.c:107-160: fixup, bound_prim,
+ *                      pre_fixup, set_dt, init_conservatives).  phi is the
+ *                      reference's own Boyer-Lindquist azimuth of the zone
+ *                      centre (coord + bl_coord, coord.c:1195, :389).
+ *   --geomplane        writes the geometry of the first x3 plane only (the
+ *                      metric does not depend on x3): keeps the init dump of
+ *                      large 3D grids small.
+ *
  * usage: harm_ref --invert <infile> <outfile>
  *   runs the reference's Utoprimgen() (utoprimgen.c:20) zone by zone on
  *   the records of <infile> (int64 n, then n x 49 doubles: evolved U[8]
@@ -33,6 +47,55 @@ extern int error_check(int wherefrom);
 extern int set_density_floors(struct of_geom *ptrgeom, FTYPE *pr, FTYPE *prfloor);
 
 static char outdir[1024];
+static int geomplane = 0;
+
+/* splitmix64 (Steele, Lea and Flood, OOPSLA 2014): a small seeded generator
+   for the azimuthal mode amplitudes and phases */
+static unsigned long long sm_state;
+static double sm_uniform(void)
+{
+  unsigned long long z = (sm_state += 0x9E3779B97F4A7C15ULL);
+  z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ULL;
+  z = (z ^ (z >> 27)) * 0x94D049BB133111EBULL;
+  z = z ^ (z >> 31);
+  return (double)(z >> 11) * (1.0 / 9007199254740992.0);
+}
+
+extern int fixup(int stage, FTYPE (*pv)[N2M][N3M][NPR], int finalstep);
+extern int pre_fixup(int stage, FTYPE (*pv)[N2M][N3M][NPR]);
+extern int bound_prim(int boundstage, FTYPE prim[][N2M][N3M][NPR]);
+extern int set_dt(FTYPE (*prim)[N2M][N3M][NPR], SFTYPE *dt);
+extern int init_conservatives(FTYPE p[][N2M][N3M][NPR], FTYPE Utemp[][N2M][N3M][NPR], FTYPE U[][N2M][N3M][NPR]);
+extern void coord(int i, int j, int k, int loc, FTYPE *X);
+extern void bl_coord(FTYPE *X, FTYPE *V);
+
+/* density modes along the azimuth on top of the reference's initial data,
+   then init's closing sequence again (initbase.c:107-160) */
+static int apply_phi_modes(unsigned long long seed, double amp)
+{
+  double Am[4], phm[4];
+  int i, j, k, m;
+  sm_state = seed;
+  for (m = 0; m < 4; m++) Am[m] = sm_uniform();
+  for (m = 0; m < 4; m++) phm[m] = 2.0 * M_PI * sm_uniform();
+  ZLOOP {
+    FTYPE X[NDIM], V[NDIM];
+    double pert = 0.0;
+    coord(i, j, k, CENT, X);
+    bl_coord(X, V);
+    for (m = 0; m < 4; m++) pert += Am[m] * cos((m + 1) * V[3] + phm[m]);
+    p[i][j][k][RHO] *= 1.0 + amp * pert;
+  }
+#if(FIXUPAFTERINIT)
+  if (fixup(STAGEM1, p, 0) >= 1) return 1;
+#endif
+  if (bound_prim(STAGEM1, p) >= 1) return 1;
+  if (pre_fixup(STAGEM1, p) >= 1) return 1;
+  set_dt(p, &dt);
+  if (DOENOFLUXMEMORY) init_conservatives(p, ulast, uinitial);
+  else init_conservatives(p, ulast, unew);
+  return 0;
+}
 
 static void wbin(const char *tag, const char *name, const void *ptr, size_t nbytes)
 {
@@ -72,6 +135,7 @@ static void write_meta(const char *tag)
   fprintf(f, "rescaletype %d\ndefcoord %d\n", rescaletype, defcoord);
   for (pl = 0; pl < 6; pl++) fprintf(f, "BCtype%d %d\n", pl, BCtype[pl]);
   fprintf(f, "failed %d\nnstroke %.17g\n", failed, (double)nstroke);
+  fprintf(f, "GEOMPLANE %d\n", geomplane);
   fclose(f);
 }
 
@@ -111,12 +175,38 @@ static void dump_geometry(void)
     floors[i + N1BND][j + N2BND][k + N3BND][0] = prfloor[RHO];
     floors[i + N1BND][j + N2BND][k + N3BND][1] = prfloor[UU];
   }
-  wbin("init", "floors", floors, sizeof(floors));
-  wbin("init", "gcov", a_gcov, sizeof(a_gcov));
-  wbin("init", "gcon", a_gcon, sizeof(a_gcon));
-  wbin("init", "gcovpert", a_gcovpert, sizeof(a_gcovpert));
-  wbin("init", "gdet", a_gdet, sizeof(a_gdet));
-  wbin("init", "conn", a_conn, sizeof(a_conn));
+  if (!geomplane) {
+    wbin("init", "floors", floors, sizeof(floors));
+    wbin("init", "gcov", a_gcov, sizeof(a_gcov));
+    wbin("init", "gcon", a_gcon, sizeof(a_gcon));
+    wbin("init", "gcovpert", a_gcovpert, sizeof(a_gcovpert));
+    wbin("init", "gdet", a_gdet, sizeof(a_gdet));
+    wbin("init", "conn", a_conn, sizeof(a_conn));
+    return;
+  }
+  /* first x3 plane of every array, same element order with the x3 extent 1 */
+  {
+    const int n1 = N1M + SHIFT1, n2 = N2M + SHIFT2, n3 = N3M + SHIFT3;
+    int ii, jj;
+#define PLANE(arr, name, n1_, n2_, n3_)                                                        \
+    do {                                                                                        \
+      size_t per = sizeof(arr) / ((size_t)(n1_) * (n2_) * (n3_));                                \
+      char *buf = (char *)malloc(per * (size_t)(n1_) * (n2_));                                   \
+      for (ii = 0; ii < (n1_); ii++)                                                             \
+        for (jj = 0; jj < (n2_); jj++)                                                           \
+          memcpy(buf + per * ((size_t)ii * (n2_) + jj),                                          \
+                 (char *)(arr) + per * (((size_t)ii * (n2_) + jj) * (n3_)), per);                 \
+      wbin("init", name, buf, per * (size_t)(n1_) * (n2_));                                     \
+      free(buf);                                                                                \
+    } while (0)
+    PLANE(floors, "floors", N1M, N2M, N3M);
+    PLANE(a_gcov, "gcov", n1, n2, n3);
+    PLANE(a_gcon, "gcon", n1, n2, n3);
+    PLANE(a_gcovpert, "gcovpert", n1, n2, n3);
+    PLANE(a_gdet, "gdet", n1, n2, n3);
+    PLANE(a_conn, "conn", N1M, N2M, N3M);
+#undef PLANE
+  }
 }
 
 extern int Utoprimgen(int evolvetype, int inputtype, FTYPE *U, struct of_geom *ptrgeom, FTYPE *pr);
@@ -174,6 +264,7 @@ int main(int argc, char *argv[])
 {
   char *fakeargv[2];
   int nsteps, s, d, ndump = 0, nodump = 0;
+  long long phiseed = -1;
   int dumps[64];
 
   if (argc == 4 && strcmp(argv[1], "--invert") == 0) {
@@ -186,8 +277,22 @@ int main(int argc, char *argv[])
     return invert_file(argv[2], argv[3]);
   }
 
+  while (argc >= 2 && strncmp(argv[1], "--", 2) == 0) {
+    if (strcmp(argv[1], "--phimodes") == 0 && argc >= 3) {
+      phiseed = strtoll(argv[2], NULL, 10);
+      argv += 2;
+      argc -= 2;
+    } else if (strcmp(argv[1], "--geomplane") == 0) {
+      geomplane = 1;
+      argv += 1;
+      argc -= 1;
+    } else {
+      fprintf(stderr, "harness: unknown option %s\n", argv[1]);
+      return 2;
+    }
+  }
   if (argc < 3) {
-    fprintf(stderr, "usage: %s <outdir|-> <nsteps> [dumpstep ...]\n", argv[0]);
+    fprintf(stderr, "usage: %s [--phimodes seed] [--geomplane] <outdir|-> <nsteps> [dumpstep ...]\n", argv[0]);
     return 2;
   }
   /* outdir "-" runs the steps for timing only and writes nothing */
@@ -201,6 +306,10 @@ int main(int argc, char *argv[])
   fakeargv[1] = NULL;
   if (init(1, fakeargv) >= 1) {
     fprintf(stderr, "harness: init failed\n");
+    return 1;
+  }
+  if (phiseed >= 0 && apply_phi_modes((unsigned long long)phiseed, 0.02)) {
+    fprintf(stderr, "harness: init after the azimuthal modes failed\n");
     return 1;
   }
   if (!nodump) {

@@ -1,4 +1,7 @@
-"""Load the committed golden fixtures (tests/golden/*.npz) into oracle Problems."""
+"""Load the committed golden fixtures (tests/golden/*.npz) into oracle Problems,
+and summarise states into the compact records kept for the configurations
+too large to store whole (tests/golden/records/*.npz)."""
+import hashlib
 import os
 
 import numpy as np
@@ -10,7 +13,8 @@ CASES = ["torus2d_16x16_mc_hll", "torus3d_12x12x6_mc_laxf", "torus2d_16x16_weno5
          "torus2d_16x16_para_hll", "torus3d_12x12x6_para_laxf", "torus2d_16x16_mc_hll_rk4",
          "torus2d_16x16_mc_hll_rk1", "torus3d_12x12x6_weno5_laxf_rk3", "torus2d_16x16_mc_hll_jon",
          "torus2d_16x16_para_hll_rk4_jon", "torus3d_12x12x6_weno5_laxf_jon", "torus2d_16x16_para_hll_rk4_jon_fv",
-         "torus2d_16x16_mc_hll_fv", "torus3d_12x12x6_para_laxf_rk4_jon_fv"]
+         "torus2d_16x16_mc_hll_fv", "torus3d_12x12x6_para_laxf_rk4_jon_fv", "torus3d_12x12x6_weno5_hll",
+         "torus3d_12x12x6_mc_hll"]
 
 
 def load(name):
@@ -53,3 +57,33 @@ def load_zones():
     z["gam"] = float(d["gam"])
     z["gammafail"] = float(d["gammafail"])
     return z
+
+
+RECORDS = os.path.join(GOLDEN, "records")
+
+
+def sha(a):
+    """SHA-256 of an array's bytes in C order (little-endian)."""
+    return hashlib.sha256(np.ascontiguousarray(a).tobytes()).hexdigest()
+
+
+def lattice(n, stride):
+    """Sample indices of the active zones: every stride-th zone per axis,
+    offset to the middle of the first stride."""
+    return tuple(np.arange(min(st // 2, nn - 1), nn, st) for nn, st in zip(n, stride))
+
+
+def summarise(p_active, pflag_active, stride):
+    """Compact record of a state: hashes of the primitives and of the
+    failure-flag map, per-primitive sums of |p|, and the primitives on a
+    sparse lattice (for a relative-L1 estimate when the hashes differ)."""
+    idx = lattice(p_active.shape[:3], stride)
+    sample = p_active[np.ix_(*idx)]
+    return dict(sha_p=sha(p_active), sha_pflag=sha(pflag_active.astype(np.int32)),
+                l1=np.abs(p_active).reshape(-1, p_active.shape[-1]).sum(axis=0), sample=sample,
+                nfail=int((pflag_active > 0).sum()))
+
+
+def load_record(name):
+    d = np.load(os.path.join(RECORDS, name + ".npz"))
+    return {k: d[k] for k in d.files}

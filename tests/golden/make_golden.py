@@ -5,9 +5,19 @@ Builds the reference (oracle/build_ref.py: the reference's own C sources plus
 the FM-torus config overlay, compiled with gcc) for small grids, runs it
 through oracle/ref_harness.c, and stores the reference's geometry, initial
 state and the states after the listed steps, cropped to NG ghost zones, as
-compressed .npz files.  Needs the reference tree (HARM_REFERENCE_DIR or
-/root/reference); the fixtures themselves are committed so that tests run
-without it.
+compressed .npz files.
+
+The benchmark configurations at their own sizes and step counts are too
+large to store whole; for them (RECORDS) the reference's run is summarised
+into tests/golden/records/<name>.npz: SHA-256 of the active primitives and
+failure flags at init and after the listed steps, per-primitive sums of |p|,
+the primitives on a sparse lattice, t and dt (tests/fixtures.summarise).
+The GPU tests regenerate the initial state with the same reference binary
+(built by __graft_entry__.build) and compare their run with the record.
+
+Needs the reference tree (HARM_REFERENCE_DIR, else "reference" beside this
+repository); the fixtures and records themselves are committed so that tests
+run without it.
 
 usage: python tests/golden/make_golden.py [case ...]
 """
@@ -24,6 +34,8 @@ sys.path.insert(0, ROOT)
 
 from oracle import build_ref  # noqa: E402
 from oracle.pyoracle import RefDump  # noqa: E402
+from tests.fixtures import RECORDS as RECORD_DIR  # noqa: E402
+from tests.fixtures import summarise  # noqa: E402
 
 # ghost zones kept in the fixture: MC reads 2, PARA 3, WENO5 (with the
 # reference's MAXBND=11 line lengths) 6 per side.  The finite-volume cases
@@ -32,6 +44,7 @@ from oracle.pyoracle import RefDump  # noqa: E402
 NG = {"MC": 3, "PARA": 3, "WENO5": 6}
 
 # name: (n1, n2, n3, lim, flux, cour, nsteps, dump steps[, TIMEORDER[, inverter[, finite volume, MAXBND]]])
+# [, {"phimodes": seed}] (the harness's azimuthal density modes)
 CASES = {
     "torus2d_16x16_mc_hll": (16, 16, 1, "MC", "HLL", 0.8, 5, [1, 5]),
     "torus3d_12x12x6_mc_laxf": (12, 12, 6, "MC", "LAXF", 0.8, 10, [1, 10]),
@@ -50,6 +63,25 @@ CASES = {
     "torus2d_16x16_para_hll_rk4_jon_fv": (16, 16, 1, "PARA", "HLL", 0.8, 10, [1, 10], 4, "JON", True, 11),
     "torus2d_16x16_mc_hll_fv": (16, 16, 1, "MC", "HLL", 0.8, 5, [1, 5], 2, "2DFINAL", True, 11),
     "torus3d_12x12x6_para_laxf_rk4_jon_fv": (12, 12, 6, "PARA", "LAXF", 0.8, 3, [1, 3], 4, "JON", True, 3),
+    # 3D with the HLL flux in all three directions, on a torus with azimuthal
+    # density modes (x3 gradients in every primitive)
+    "torus3d_12x12x6_weno5_hll": (12, 12, 6, "WENO5", "HLL", 0.8, 5, [1, 5], 2, "2DFINAL", False, 11,
+                                  {"phimodes": 1}),
+    "torus3d_12x12x6_mc_hll": (12, 12, 6, "MC", "HLL", 0.8, 10, [1, 10], 2, "2DFINAL", False, 11, {"phimodes": 1}),
+}
+
+# Benchmark configurations run by the reference at their own sizes and step
+# counts: name -> (n1, n2, n3, lim, flux, cour, nsteps, dump steps, harness
+# options, lattice stride of the sample, keep the whole active state)
+RECORDS = {
+    # the 2D FM torus 64x64, MC + HLL + flux-CT, RK2, CFL 0.8, 200 steps
+    "torus2d_64x64_mc_hll_200": (64, 64, 1, "MC", "HLL", 0.8, 200, [1, 200], [], (1, 1, 1), True),
+    # the 3D torus 128x64x32 with azimuthal density modes, WENO5 + HLL, 500 steps
+    "torus3d_128x64x32_weno5_hll_500": (128, 64, 32, "WENO5", "HLL", 0.8, 500, [1, 500],
+                                        ["--phimodes", "1"], (8, 8, 4), False),
+    # the precision-at-scale torus 256x128x128, WENO5 + HLL, first 5 steps
+    "torus3d_256x128x128_weno5_hll_5": (256, 128, 128, "WENO5", "HLL", 0.8, 5, [1, 5],
+                                        ["--phimodes", "1", "--geomplane"], (8, 8, 8), False),
 }
 
 
@@ -59,11 +91,13 @@ def make(name, spec, ref):
     utoprim = spec[9] if len(spec) > 9 else "2DFINAL"
     fv = spec[10] if len(spec) > 10 else False
     maxbnd = spec[11] if len(spec) > 11 else 11
+    opts = spec[12] if len(spec) > 12 else {}
+    hargs = ["--phimodes", str(opts["phimodes"])] if "phimodes" in opts else []
     ng = maxbnd if fv else NG[lim]
     exe = build_ref.build(ref, n1, n2, n3, lim, flux, cour, maxbnd, timeorder=timeorder, utoprim=utoprim, fv=fv)
     with tempfile.TemporaryDirectory() as tmp:
         out = os.path.join(tmp, "out")
-        subprocess.run([exe, out, str(nsteps)] + [str(s) for s in dumps], cwd=tmp, check=True,
+        subprocess.run([exe] + hargs + [out, str(nsteps)] + [str(s) for s in dumps], cwd=tmp, check=True,
                        stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL)
         rd = RefDump(out)
         pr = rd.to_problem(ng, "init")
@@ -177,14 +211,51 @@ def make_zones(ref):
     print(f"wrote {path} ({os.path.getsize(path) / 1e6:.2f} MB)")
 
 
+def record_binary(ref, name):
+    """Reference binary of a record (the one __graft_entry__.build also builds)."""
+    n1, n2, n3, lim, flux, cour = RECORDS[name][:6]
+    return build_ref.build(ref, n1, n2, n3, lim, flux, cour, 11)
+
+
+def make_record(name, ref, workdir=None):
+    n1, n2, n3, lim, flux, cour, nsteps, dumps, hargs, stride, whole = RECORDS[name]
+    exe = record_binary(ref, name)
+    os.makedirs(RECORD_DIR, exist_ok=True)
+    with tempfile.TemporaryDirectory(dir=workdir) as tmp:
+        out = os.path.join(tmp, "out")
+        subprocess.run([exe] + hargs + [out, str(nsteps)] + [str(s) for s in dumps], cwd=tmp, check=True,
+                       stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL)
+        rd = RefDump(out)
+        data = dict(n=np.array((n1, n2, n3)), steps=np.array(dumps), stride=np.array(stride),
+                    harness_args=np.array(" ".join(hargs)))
+        for tag in ["init"] + [f"s{s}" for s in dumps]:
+            p = rd.crop(rd.p(tag), 0)
+            f = rd.crop(rd.pflag(tag), 0)[..., 0]
+            m = rd.meta_of(tag)
+            rec = summarise(p, f, stride)
+            for k, v in rec.items():
+                data[f"{tag}_{k}"] = np.array(v)
+            data[f"{tag}_t"] = m["t"]
+            data[f"{tag}_dt"] = m["dt"]
+            data[f"{tag}_nstroke"] = m["nstroke"]
+            if whole and tag != "init":
+                data[f"{tag}_p"] = p
+                data[f"{tag}_pflag"] = f
+    path = os.path.join(RECORD_DIR, name + ".npz")
+    np.savez_compressed(path, **data)
+    print(f"wrote {path} ({os.path.getsize(path) / 1e6:.2f} MB)")
+
+
 def main():
-    ref = os.environ.get("HARM_REFERENCE_DIR", "/root/reference")
+    ref = build_ref.DEFAULT_REF
     if not os.path.isdir(ref):
-        raise SystemExit(f"reference tree not found: {ref}")
-    names = sys.argv[1:] or list(CASES) + ["utoprim_zones"]
+        raise SystemExit(f"reference tree not found at {ref}: set HARM_REFERENCE_DIR")
+    names = sys.argv[1:] or list(CASES) + ["utoprim_zones"] + list(RECORDS)
     for name in names:
         if name == "utoprim_zones":
             make_zones(ref)
+        elif name in RECORDS:
+            make_record(name, ref)
         else:
             make(name, CASES[name], ref)
 

@@ -1,0 +1,68 @@
+"""The reference's own program driving the GPU through the drop-in step_ch.
+
+oracle/_ref/harm_ref_*_gpushim is the reference's C sources (its init, its
+arrays, the step loop of oracle/ref_harness.c that main.c:33-49 runs) with
+harm_finalwham_b200/dropin/step_ch_gpu.c linked in place of its CPU step_ch
+(step_ch.c:16).  Its dumps must equal the reference's own CPU run bit for
+bit: the 64x64 torus configuration for its 200 steps (the record of the
+reference's run), the 3D WENO5 + HLL torus with azimuthal modes and the
+finite-volume scheme (PARA, RK4, Jon's inverter) against their golden
+fixtures."""
+import os
+import subprocess
+import tempfile
+
+import numpy as np
+import pytest
+
+from oracle.pyoracle import LIBDIR, RefDump
+from tests.fixtures import load, load_record, same
+
+pytestmark = pytest.mark.gpu
+
+
+def run_shim(binary, nsteps, dumps, args=()):
+    exe = os.path.join(LIBDIR, binary)
+    assert os.path.exists(exe), f"{exe} is missing: __graft_entry__.build() builds it"
+    tmp = tempfile.TemporaryDirectory()
+    out = os.path.join(tmp.name, "out")
+    r = subprocess.run([exe] + list(args) + [out, str(nsteps)] + [str(d) for d in dumps], cwd=tmp.name,
+                       capture_output=True, text=True)
+    assert r.returncode == 0, f"{binary} failed: {r.stderr[-2000:]}"
+    return tmp, RefDump(out)
+
+
+def test_reference_loop_on_gpu_matches_reference_run_64x64():
+    rec = load_record("torus2d_64x64_mc_hll_200")
+    tmp, rd = run_shim("harm_ref_64x64x1_MC_HLL_gpushim", 200, [1])
+    with tmp:
+        for s in (1, 200):
+            tag = f"s{s}"
+            p = rd.crop(rd.p(tag), 0)
+            f = rd.crop(rd.pflag(tag), 0)[..., 0]
+            m = rd.meta_of(tag)
+            assert same(p, rec[f"{tag}_p"]), f"primitives differ from the reference's run after step {s}"
+            assert np.array_equal(f, rec[f"{tag}_pflag"]), f"failure flags differ after step {s}"
+            assert m["t"] == float(rec[f"{tag}_t"]) and m["dt"] == float(rec[f"{tag}_dt"])
+            assert m["nstroke"] == float(rec[f"{tag}_nstroke"])
+
+
+@pytest.mark.parametrize("binary,fixture,args", [
+    ("harm_ref_12x12x6_WENO5_HLL_gpushim", "torus3d_12x12x6_weno5_hll", ["--phimodes", "1"]),
+    ("harm_ref_16x16x1_PARA_HLL_rk4_jon_fv_gpushim", "torus2d_16x16_para_hll_rk4_jon_fv", []),
+])
+def test_reference_loop_on_gpu_matches_golden(binary, fixture, args):
+    pr, ref = load(fixture)
+    steps = sorted(ref)
+    tmp, rd = run_shim(binary, steps[-1], steps[:-1], args)
+    with tmp:
+        for s in steps:
+            tag = f"s{s}"
+            r = ref[s]
+            assert same(rd.crop(rd.p(tag), pr.ng), r["p"]), f"primitives differ after step {s}"
+            assert np.array_equal(rd.crop(rd.pflag(tag), pr.ng)[..., 0], r["pflag"])
+            m = rd.meta_of(tag)
+            assert m["t"] == r["t"] and m["dt"] == r["dt"] and m["nstroke"] == r["nstroke"]
+            if r["u"] is not None:
+                act = pr.active
+                assert same(act(rd.crop(rd.unew(tag), pr.ng)), act(r["u"])), f"unew differs after step {s}"

@@ -73,3 +73,31 @@ def test_oracle_pi2u_matches_reference_init():
     # pi2Uavg (initbase.c:1833): the finite-volume scheme's initial unew
     pr, _ = load("torus2d_16x16_para_hll_rk4_jon_fv")
     assert same(Oracle().pi2u(pr), pr.u)
+
+
+def test_oracle_matches_reference_run_of_the_64x64_torus(orc):
+    # the 2D FM torus 64x64 configuration (MC + HLL + flux-CT, RK2, CFL 0.8)
+    # for its 200 steps, against the record of the reference's own run; the
+    # initial state comes from the same reference binary
+    import os
+    import subprocess
+    import tempfile
+
+    from oracle.pyoracle import LIBDIR, RefDump
+    from tests.fixtures import load_record, summarise
+    exe = os.path.join(LIBDIR, "harm_ref_64x64x1_MC_HLL")
+    if not os.path.exists(exe):
+        pytest.skip("reference binary not built (__graft_entry__.build builds it where the reference tree is)")
+    rec = load_record("torus2d_64x64_mc_hll_200")
+    with tempfile.TemporaryDirectory() as tmp:
+        out = os.path.join(tmp, "init")
+        subprocess.run([exe, out, "0"], cwd=tmp, check=True, stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL)
+        pr = RefDump(out).to_problem(3, "init")
+    assert summarise(pr.active(pr.p), pr.active(pr.pflag), (1, 1, 1))["sha_p"] == str(rec["init_sha_p"])
+    done = 0
+    for s in [int(x) for x in rec["steps"]]:
+        orc.step(pr, s - done)
+        done = s
+        assert same(pr.active(pr.p), rec[f"s{s}_p"]), f"primitives differ after step {s}"
+        assert np.array_equal(pr.active(pr.pflag), rec[f"s{s}_pflag"])
+        assert pr.t == float(rec[f"s{s}_t"]) and pr.dt == float(rec[f"s{s}_dt"])
