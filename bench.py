@@ -188,7 +188,7 @@ def bench_decomp(args, rank, world):
     L = load_library()
     g = HarmGPU.from_problem(slab, precision=args.precision)
     if args.tuning:
-        g.set_tuning(dict(zip(("flux", "weno_b", "update", "invert"), (int(v) for v in args.tuning.split(",")))))
+        g.set_tuning(dict(zip(("flux", "weno", "update", "invert"), (int(v) for v in args.tuning.split(",")))))
     else:
         g.autotune()
     sub = SlabContext(g)
@@ -349,7 +349,7 @@ def bench_ours(args, rank, world):
     diag0 = g.diagnostics()
     if args.tuning:
         # a known choice (e.g. for profiler runs that should not see the trials)
-        tuning = dict(zip(("flux", "weno_b", "update", "invert"), (int(v) for v in args.tuning.split(","))))
+        tuning = dict(zip(("flux", "weno", "update", "invert"), (int(v) for v in args.tuning.split(","))))
         g.set_tuning(tuning)
     else:
         tuning = g.autotune()
@@ -789,7 +789,7 @@ def main():
     ap.add_argument("--cpu-procs", type=int, default=0,
                     help="processes of the reference CPU build (default: every host core this process may use)")
     ap.add_argument("--tuning", default=None,
-                    help="blocks per SM for flux,weno_b,update,invert instead of running the autotuner")
+                    help="blocks per SM for flux,weno,update,invert instead of running the autotuner")
     ap.add_argument("--kernels-only", action="store_true",
                     help="set-up, warm-up and the timed steps only (for profiler runs)")
     ap.add_argument("--decomp", default=None, choices=["x3"],

@@ -188,22 +188,14 @@ __device__ __forceinline__ void para4(const T *y, T *lout, T *rout) {
   *rout = r;
 }
 
-// ---------------------------------------------------------------------------
-// WENO5 line reconstruction (slope_lim_linetype_c2e, interpline.c:517-678) as
-// two cell-parallel passes; see weno5.cuh.  Scratch WA holds, per primitive
-// v, 4 planes: the SMONO code (indicator in [0,1], -1 at a cusp) and the
-// three unoptimised weights.
-// ---------------------------------------------------------------------------
-constexpr int W5_PLANES = 4;
-
-// Minimum resident 128-thread blocks per SM asked of the register allocator
-// for the FP64-heavy kernels (launch_bounds' second argument).  With 64K
-// registers per SM, B blocks cap a thread at 65536 / (128 B) registers:
+// Minimum resident blocks per SM asked of the register allocator for the
+// FP64-heavy kernels (launch_bounds' second argument).  With 64K registers
+// per SM, B blocks of 128 threads cap a thread at 65536 / (128 B) registers:
 // 1-2 -> 255 (8 warps/SM), 3 -> 170 (12 warps), 4 -> 128 (16 warps), more
 // warps to hide FP64 latency at the price of spills to local memory.
 // Defaults from a B200 sweep (256x128x128 torus, 1/3/4/5 blocks for flux and
-// update, 1/5/6/8 for weno_b, 1/8/10 for weno_a): flux 4 (-11% WENO5, -21%
-// MC), weno_b 8 (-33%), weno_a 8 (-3%); update is fastest unconstrained.
+// update): flux 4 (-11% WENO5, -21% MC); update is fastest unconstrained.
+// The WENO5 kernel runs blocks of 256 threads (W5_THREADS).
 #ifndef HG_MINB_FLUX
 #define HG_MINB_FLUX 4
 #endif
@@ -213,35 +205,29 @@ constexpr int W5_PLANES = 4;
 #ifndef HG_MINB_INVERT
 #define HG_MINB_INVERT 1
 #endif
-#ifndef HG_MINB_WENO_A
-#define HG_MINB_WENO_A 8
-#endif
-#ifndef HG_MINB_WENO_B
-#define HG_MINB_WENO_B 8
+#ifndef HG_MINB_WENO
+#define HG_MINB_WENO 3
 #endif
 // the same for the FP32 kernels of the mixed-precision path (B200 sweep of
-// 4/6/8 for flux, 8/10/12 for weno_a/b: flux 8 -4%, the rest within 2%)
+// 4/6/8 for flux: 8 -4%)
 #ifndef HG_MINB_FLUX_F32
 #define HG_MINB_FLUX_F32 8
 #endif
-#ifndef HG_MINB_WENO_A_F32
-#define HG_MINB_WENO_A_F32 12
-#endif
-#ifndef HG_MINB_WENO_B_F32
-#define HG_MINB_WENO_B_F32 8
+#ifndef HG_MINB_WENO_F32
+#define HG_MINB_WENO_F32 3
 #endif
 template <typename T> struct MinBlocks;
 template <> struct MinBlocks<double> {
-  static constexpr int flux = HG_MINB_FLUX, weno_a = HG_MINB_WENO_A, weno_b = HG_MINB_WENO_B;
+  static constexpr int flux = HG_MINB_FLUX, weno = HG_MINB_WENO;
 };
 template <> struct MinBlocks<float> {
-  static constexpr int flux = HG_MINB_FLUX_F32, weno_a = HG_MINB_WENO_A_F32, weno_b = HG_MINB_WENO_B_F32;
+  static constexpr int flux = HG_MINB_FLUX_F32, weno = HG_MINB_WENO_F32;
 };
 
-// the FP64 variants the autotuner chooses between (resident 128-thread
-// blocks per SM for each heavy kernel; variant 0 is the default above)
+// the FP64 variants the autotuner chooses between (resident blocks per SM
+// for each heavy kernel; variant 0 is the default above)
 constexpr int kFluxMB[2] = {HG_MINB_FLUX, HG_MINB_FLUX - 1};
-constexpr int kWenoBMB[2] = {HG_MINB_WENO_B, HG_MINB_WENO_B - 2};
+constexpr int kWenoMB[2] = {HG_MINB_WENO, HG_MINB_WENO + 1};
 constexpr int kConserveMB[2] = {HG_MINB_UPDATE, 3};
 constexpr int kInvertMB[2] = {HG_MINB_INVERT, 2};
 
@@ -263,97 +249,190 @@ __device__ __forceinline__ void load_metric_t(const double *__restrict__ G, cons
   m.g = (T)__ldg(b + (long long)33 * d.nij);
 }
 
-// pass A over line cells -4..n+3: cusp test, SMONO indicator, unoptimised
-// weights.  T = double: the reference's arithmetic; T = float: mixed path.
-template <int DIR, typename T>
-__global__ void __launch_bounds__(128, MinBlocks<T>::weno_a) weno_a_kernel(Dims d, Box box, const double *__restrict__ pb,
-                                                                     T *__restrict__ WA) {
+// ---------------------------------------------------------------------------
+// WENO5 line reconstruction (slope_lim_linetype_c2e, interpline.c:517-678),
+// one kernel per direction.  The reference sweeps whole lines serially; here
+// a block owns a tile: `lb` consecutive output cells along the direction on
+// `w` lines, and stages what the cells of the tile share in shared memory so
+// that every per-cell quantity is computed once:
+//   S  per output cell: the post/pre-shock reduction factor of
+//      apply_additional_reduction_to_weights (reconstructeno.c:650-700) from
+//      the dP/P jump of compute_df_line_new (interpline.c:2148-2222) over
+//      cells -1, 0, +1, whose state pieces w5_state_kernel formed once per
+//      zone for all three directions
+//   for each primitive v:
+//   Y  the line of v, cells -5..lb+4
+//   A  per cell -3..lb+2: SMONO cusp test and indicator, unoptimised order-3
+//      weights (compute_cf_stencil_weights + mono_adjust_unoptimized_weights)
+//   R  per cell -1..lb: lower-order fraction of compute_weights_ratios
+//   F  per output cell: the final fraction (the cell's own, and the shock
+//      factor times its neighbours'), optimised and order-2 weights and the
+//      two face values -> pL, pR
+// The output cells of a direction are the line cells -1..n (the box), every
+// line across it that the flux loop covers.  Every quantity is formed by the
+// same device functions, in the same operation order, as before tiling, so
+// the FP64 results stay bit-identical to the reference.
+// ---------------------------------------------------------------------------
+constexpr int W5_THREADS = 256;
+
+struct W5Tile {
+  Box box;      // output cells
+  int lb;       // output cells per tile along the direction
+  int w;        // lines per tile (a power of two, at most 32)
+  int wshift;   // log2(w)
+  int nseg;     // tiles along the direction
+  int ntile;    // tiles across (ceil(nlines / w))
+  int nlines;   // lines of the box
+  int fast_s;   // 1: threads walk along the line (its cells are contiguous in memory), 0: across lines
+};
+
+// The dP/P pieces of compute_df_line_new (interpline.c:2148-2222) of one
+// zone, (1 + u_t) u^t and gam u (u^t u_t) + (gam - 1) u, into PU[0][z] and
+// PU[1][z]: they depend on the zone's state only, so one pass serves the
+// WENO5 reconstruction of every direction.
+template <typename T>
+__global__ void __launch_bounds__(128) w5_state_kernel(Dims d, Params P, Box box, const double *__restrict__ pb,
+                                                       const double *__restrict__ G, T *__restrict__ PU) {
   long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= box.size()) return;
   int i, j, k;
   box_ijk(box, t, i, j, k);
-  long long z = zix(d, i, j, k);
-  const long long o = dir_stride<DIR>(d);
-  for (int v = 0; v < NPR; v++) {
-    const double *q = pb + (long long)v * d.nz + z;
-    T ya[5] = {(T)__ldg(q - 2 * o), (T)__ldg(q - o), (T)__ldg(q), (T)__ldg(q + o), (T)__ldg(q + 2 * o)};
-    const T *y = ya + 2;
-    bool c = w5::cusp(y);
-    T m0 = c ? T(0.0) : w5::mono(y);
-    T w[3];
-    w5::unopt3(m0, y, w);
-    T *out = WA + (long long)v * W5_PLANES * d.nz + z;
-    out[0] = c ? T(-1.0) : m0;
-    out[d.nz] = w[0];
-    out[2 * d.nz] = w[1];
-    out[3 * d.nz] = w[2];
-  }
+  const long long z = zix(d, i, j, k);
+  const T gam = (T)(P.cell_inst ? P.inst[P.cell_inst[z]].gam : P.gam);
+  T pc[NPR];
+#pragma unroll
+  for (int v = 0; v < NPR; v++) pc[v] = (T)pb[(long long)v * d.nz + z];
+  MetricT<T> m;
+  load_metric_t(G, d, gix(d, i, j), G_CENT, m);
+  StateT<T> q;
+  get_state(pc, m, q);
+  const T a = compute_1plusud0(m, q);
+  PU[z] = a * (q.ucon[0]);
+  PU[d.nz + z] = gam * pc[UU] * (q.ucon[0] * q.ucov[0]) + (gam - T(1.0)) * pc[UU];
 }
 
-// pass B over line cells -1..n: dP/P, ratios, reduction, face values
-template <int DIR, typename T, int MB = MinBlocks<T>::weno_b>
-__global__ void __launch_bounds__(128, MB) weno_b_kernel(Dims d, Params P, Box box,
-                                                                     const double *__restrict__ pb,
-                                                                     const double *__restrict__ G,
-                                                                     const T *__restrict__ WA, T *__restrict__ pL,
-                                                                     T *__restrict__ pR) {
-  long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= box.size()) return;
-  int i, j, k;
-  box_ijk(box, t, i, j, k);
-  long long z = zix(d, i, j, k);
-  const long long o = dir_stride<DIR>(d);
-  // compute_df_line_new (interpline.c:2148-2222): jump indicator from the
-  // primitives of the cells -1, 0, +1 along the line and their CENT metrics
-  T dP;
-  {
-    // one cell at a time (only its two scalars stay live): par = (1 + u_t) u^t,
-    // upar = gam u (u^t u_t) + (gam - 1) u
-    const T gam = (T)(P.cell_inst ? P.inst[P.cell_inst[z]].gam : P.gam);
-    auto cell = [&](int off, T *par, T *upar, T *rho) {
-      T pc[NPR];
-#pragma unroll
-      for (int v = 0; v < NPR; v++) pc[v] = (T)pb[(long long)v * d.nz + z + off * o];
-      MetricT<T> m;
-      load_metric_t(G, d, gix(d, i + off * (DIR == 1), j + off * (DIR == 2)), G_CENT, m);
-      StateT<T> q;
-      get_state(pc, m, q);
-      const T a = compute_1plusud0(m, q);
-      *par = a * (q.ucon[0]);
-      *upar = gam * pc[UU] * (q.ucon[0] * q.ucov[0]) + (gam - T(1.0)) * pc[UU];
-      *rho = pc[RHO];
-    };
-    T parl, uparl, par, upar, parr, uparr, rl, r0, rr;
-    cell(-1, &parl, &uparl, &rl);
-    cell(0, &par, &upar, &r0);
-    cell(1, &parr, &uparr, &rr);
-    dP = (fabs(r0 * (parr - parl)) + fabs(uparr - uparl)) / (fabs(r0 * par) + fabs(upar) + w5::K<T>::tiny);
+// shared-memory elements of a tile with lb output cells on w lines:
+// Y (lb+10) + A 4 (lb+6) + R (lb+2) + the shock factor lb, per line
+__host__ __device__ inline long long w5_smem_elems(int lb, int w) { return (long long)w * (7LL * lb + 36); }
+
+// zone index of cell 0 of line `line` of box b (along the line the index
+// steps by dir_stride)
+template <int DIR>
+__device__ __forceinline__ long long w5_line(const Dims &d, const Box &b, int line) {
+  int i = 0, j = 0, k = 0;
+  if (DIR == 1) {
+    j = b.j0 + line / b.nk;
+    k = b.k0 + line % b.nk;
+  } else if (DIR == 2) {
+    i = b.i0 + line / b.nk;
+    k = b.k0 + line % b.nk;
+  } else {
+    i = b.i0 + line / b.nj;
+    j = b.j0 + line % b.nj;
   }
-  // apply_additional_reduction_to_weights (reconstructeno.c:650-700)
-  T ss = w5::wmin((fabs(dP) - T(0.5 * w5::kDpFrac)) / T(0.5 * w5::kDpFrac), T(1.));
+  return zix(d, i, j, k);
+}
+
+template <int DIR, bool FS, typename T, int MB = MinBlocks<T>::weno>
+__global__ void __launch_bounds__(W5_THREADS, MB) weno5_kernel(Dims d, Params P, W5Tile tl,
+                                                               const double *__restrict__ pb,
+                                                               const T *__restrict__ PU, T *__restrict__ pL,
+                                                               T *__restrict__ pR) {
+  extern __shared__ __align__(16) unsigned char w5_smem[];
+  __shared__ long long zb[32];
+  T *sm = reinterpret_cast<T *>(w5_smem);
+  const int W = tl.w;
+  const int seg = blockIdx.x % tl.nseg;
+  const int line0 = (blockIdx.x / tl.nseg) * W;
+  const int nl = min(W, tl.nlines - line0);
+  const int nout = (DIR == 1) ? tl.box.ni : ((DIR == 2) ? tl.box.nj : tl.box.nk);
+  const int c0 = ((DIR == 1) ? tl.box.i0 : ((DIR == 2) ? tl.box.j0 : tl.box.k0)) + seg * tl.lb;
+  const int nv = min(tl.lb, nout - seg * tl.lb);  // output cells of this tile
+  const int NS = nv + 10, NA = nv + 6, NL = nv + 2;
+  const long long o = dir_stride<DIR>(d);
+  // this thread's line w and first cell r; it steps along the line by TL
+  const int TL = W5_THREADS >> tl.wshift;
+  const int w = FS ? (int)(threadIdx.x / TL) : (int)(threadIdx.x & (W - 1));
+  const int r = FS ? (int)(threadIdx.x & (TL - 1)) : (int)(threadIdx.x >> tl.wshift);
+  const bool on = w < nl;
+  if (threadIdx.x < nl) zb[threadIdx.x] = w5_line<DIR>(d, tl.box, line0 + threadIdx.x);
+  T *Y = sm;                        // cells -5 .. nv+4
+  T *A = Y + (long long)NS * W;     // 4 planes, cells -3 .. nv+2: code (indicator, -1 at a cusp), w0, w1, w2
+  T *R = A + 4LL * NA * W;          // cells -1 .. nv: lower-order fraction
+  T *SS = R + (long long)NL * W;    // output cells: shock reduction factor
+  // element s of this thread's line in a plane with n cells per line
+  auto at = [&](T *plane, int n, int s) -> T & { return FS ? plane[w * n + s] : plane[s * W + w]; };
+  __syncthreads();
+  const long long zl = on ? zb[w] : 0;
+
+  // S: the reduction factor of each output cell from the state pieces of
+  // cells -1, 0, +1 (no barrier needed before stage Y: different planes)
+  if (on)
+    for (int s = r; s < nv; s += TL) {
+      const long long z = zl + (long long)(c0 + s) * o;
+      const T parl = __ldg(PU + z - o), par = __ldg(PU + z), parr = __ldg(PU + z + o);
+      const T uparl = __ldg(PU + d.nz + z - o), upar = __ldg(PU + d.nz + z), uparr = __ldg(PU + d.nz + z + o);
+      const T r0 = (T)__ldg(pb + z);
+      const T dP =
+          (fabs(r0 * (parr - parl)) + fabs(uparr - uparl)) / (fabs(r0 * par) + fabs(upar) + w5::K<T>::tiny);
+      // (x / 0.25 is the exact multiplication by 4)
+      at(SS, nv, s) = w5::wmin((fabs(dP) - T(0.5 * w5::kDpFrac)) * T(1.0 / (0.5 * w5::kDpFrac)), T(1.));
+    }
+
+  T *CODE = A, *W0 = A + (long long)NA * W, *W1 = A + 2LL * NA * W, *W2 = A + 3LL * NA * W;
   for (int v = 0; v < NPR; v++) {
-    const T *wa = WA + (long long)v * W5_PLANES * d.nz + z;
-    // codes of cells -1, 0, +1 and weights of cells -3..+3 (w0 and w2 of the neighbours)
-    T cm = __ldg(wa - o), c0 = __ldg(wa), cp = __ldg(wa + o);
-    const T *w0p = wa + d.nz, *w1p = wa + 2 * d.nz, *w2p = wa + 3 * d.nz;
-    T wc[3] = {__ldg(w0p), __ldg(w1p), __ldg(w2p)};
-    T wm[3] = {__ldg(w0p - o), T(0.0), __ldg(w2p - o)};
-    T wp[3] = {__ldg(w0p + o), T(0.0), __ldg(w2p + o)};
-    T w_m3_0 = __ldg(w0p - 3 * o), w_m2_0 = __ldg(w0p - 2 * o);
-    T w_p2_2 = __ldg(w2p + 2 * o), w_p3_2 = __ldg(w2p + 3 * o);
-    T fd_m = w5::ratio_lof(wm, w_m3_0, __ldg(w2p + o), cm == T(-1.0) ? T(1.0) : T(0.0));
-    T fd_p = w5::ratio_lof(wp, __ldg(w0p - o), w_p3_2, cp == T(-1.0) ? T(1.0) : T(0.0));
-    T lof = w5::ratio_lof(wc, w_m2_0, w_p2_2, c0 == T(-1.0) ? T(1.0) : T(0.0));
-    lof = w5::wmax(lof, ss * fd_p);
-    lof = w5::wmax(lof, ss * fd_m);
-    const double *q = pb + (long long)v * d.nz + z;
-    T ya[5] = {(T)__ldg(q - 2 * o), (T)__ldg(q - o), (T)__ldg(q), (T)__ldg(q + o), (T)__ldg(q + 2 * o)};
-    bool cu = (c0 == T(-1.0));
-    T m0 = cu ? T(0.0) : c0;
-    T yl, yr;
-    w5::faces(ya + 2, m0, cu, wc, lof, &yl, &yr);
-    pL[(long long)v * d.nz + z] = yl;
-    pR[(long long)v * d.nz + z] = yr;
+    const double *pv = pb + (long long)v * d.nz + zl;
+    // Y: the line of primitive v
+    if (on)
+      for (int s = r; s < NS; s += TL) at(Y, NS, s) = (T)__ldg(pv + (long long)(c0 - 5 + s) * o);
+    __syncthreads();
+    // A: cusp test, SMONO indicator, unoptimised weights of cells -3..nv+2
+    if (on)
+      for (int s = r; s < NA; s += TL) {
+        T ya[5];
+#pragma unroll
+        for (int q = 0; q < 5; q++) ya[q] = at(Y, NS, s + q);
+        const T *y = ya + 2;
+        const bool c = w5::cusp(y);
+        const T m0 = c ? T(0.0) : w5::mono(y);
+        T wt[3];
+        w5::unopt3(m0, y, wt);
+        at(CODE, NA, s) = c ? T(-1.0) : m0;
+        at(W0, NA, s) = wt[0];
+        at(W1, NA, s) = wt[1];
+        at(W2, NA, s) = wt[2];
+      }
+    __syncthreads();
+    // R: lower-order fraction of cells -1..nv from the weights of cells -3..nv+2
+    if (on)
+      for (int s = r; s < NL; s += TL) {
+        const int a = s + 2;  // cell s-1 in the A planes
+        const T wc[3] = {at(W0, NA, a), T(0.0), at(W2, NA, a)};
+        at(R, NL, s) =
+            w5::ratio_lof(wc, at(W0, NA, a - 2), at(W2, NA, a + 2), at(CODE, NA, a) == T(-1.0) ? T(1.0) : T(0.0));
+      }
+    __syncthreads();
+    // F: face values of the output cells
+    if (on)
+      for (int s = r; s < nv; s += TL) {
+        const T ss = at(SS, nv, s);
+        T lof = at(R, NL, s + 1);
+        lof = w5::wmax(lof, ss * at(R, NL, s + 2));
+        lof = w5::wmax(lof, ss * at(R, NL, s));
+        const int a = s + 3;
+        const T c0v = at(CODE, NA, a);
+        const T wc[3] = {at(W0, NA, a), at(W1, NA, a), at(W2, NA, a)};
+        T ya[5];
+#pragma unroll
+        for (int q = 0; q < 5; q++) ya[q] = at(Y, NS, s + 3 + q);
+        const bool cu = (c0v == T(-1.0));
+        T yl, yr;
+        w5::faces(ya + 2, cu ? T(0.0) : c0v, cu, wc, lof, &yl, &yr);
+        const long long z = zl + (long long)(c0 + s) * o + (long long)v * d.nz;
+        pL[z] = yl;
+        pR[z] = yr;
+      }
+    __syncthreads();
   }
 }
 

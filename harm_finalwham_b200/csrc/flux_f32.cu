@@ -10,9 +10,10 @@
 namespace hg {
 
 #define HG_F32_INSTANCES(DIR)                                                                                      \
-  template __global__ void weno_a_kernel<DIR, float>(Dims, Box, const double *, float *);                         \
-  template __global__ void weno_b_kernel<DIR, float>(Dims, Params, Box, const double *, const double *,           \
-                                                     const float *, float *, float *);                              \
+  template __global__ void weno5_kernel<DIR, true, float>(Dims, Params, W5Tile, const double *, const float *,    \
+                                                          float *, float *);                                        \
+  template __global__ void weno5_kernel<DIR, false, float>(Dims, Params, W5Tile, const double *, const float *,   \
+                                                           float *, float *);                                       \
   template __global__ void flux_kernel<DIR, 0, float>(Dims, Params, Box, const double *, const float *,           \
                                                       const float *, const double *, double *, Scalars *);          \
   template __global__ void flux_kernel<DIR, 1, float>(Dims, Params, Box, const double *, const float *,           \
@@ -23,5 +24,6 @@ namespace hg {
 HG_F32_INSTANCES(1)
 HG_F32_INSTANCES(2)
 HG_F32_INSTANCES(3)
+template __global__ void w5_state_kernel<float>(Dims, Params, Box, const double *, const double *, float *);
 
 }  // namespace hg

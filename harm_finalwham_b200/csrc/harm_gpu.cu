@@ -10,9 +10,9 @@
 //     CORN1..3 gdet, conn[64] at CENT, floors[2].
 //
 // Work per RK substep (the reference's advance(), step_ch.c:94-186):
-//   weno_a/weno_b     WENO5 line reconstruction (interpline.c:517-678) in two
-//                     cell-parallel passes (lim = WENO5 only; weno5.cuh,
-//                     common.cuh)
+//   weno5_kernel<dir> WENO5 line reconstruction (interpline.c:517-678), one
+//                     kernel per direction over tiles staged in shared
+//                     memory (lim = WENO5 only; weno5.cuh, common.cuh)
 //   flux_kernel<dir>  fluxcalc_standard (flux.c:469-680) fused with the
 //                     MC/PARA reconstruction (or reading the WENO5 face
 //                     values), both Riemann states, vchar, HLL/LaxF, the gdet
@@ -48,9 +48,10 @@ using namespace hg;
 // flux_f32.cu (FMA and fast FP32 division there; this unit keeps -fmad=false)
 namespace hg {
 #define HG_F32_EXTERN(DIR)                                                                                         \
-  extern template __global__ void weno_a_kernel<DIR, float>(Dims, Box, const double *, float *);                  \
-  extern template __global__ void weno_b_kernel<DIR, float>(Dims, Params, Box, const double *, const double *,    \
-                                                            const float *, float *, float *);                       \
+  extern template __global__ void weno5_kernel<DIR, true, float>(Dims, Params, W5Tile, const double *,            \
+                                                                 const float *, float *, float *);                \
+  extern template __global__ void weno5_kernel<DIR, false, float>(Dims, Params, W5Tile, const double *,           \
+                                                                  const float *, float *, float *);               \
   extern template __global__ void flux_kernel<DIR, 0, float>(Dims, Params, Box, const double *, const float *,    \
                                                              const float *, const double *, double *, Scalars *);   \
   extern template __global__ void flux_kernel<DIR, 1, float>(Dims, Params, Box, const double *, const float *,    \
@@ -60,6 +61,7 @@ namespace hg {
 HG_F32_EXTERN(1)
 HG_F32_EXTERN(2)
 HG_F32_EXTERN(3)
+extern template __global__ void w5_state_kernel<float>(Dims, Params, Box, const double *, const double *, float *);
 }  // namespace hg
 
 namespace {
@@ -1070,6 +1072,93 @@ __global__ void utoprim_batch_kernel(const double *__restrict__ U, const double 
 
 inline unsigned grid_for(long long n, int block) { return (unsigned)((n + block - 1) / block); }
 
+// Dynamic shared memory the WENO5 kernel may use per block (its tilings are
+// sized to fit, for FP64 elements)
+constexpr size_t W5_SMEM_MAX = 72 * 1024;
+
+// Cost of a WENO5 tiling in thread rounds (256-thread sweeps over a stage's
+// items), weighted by each stage's work per item: D (state, dP/P) once, then
+// per primitive A (SMONO + weights), R (ratios), F (face values).
+double w5_cost(int nout, long long nlines, int lb, int w) {
+  const int nseg = (nout + lb - 1) / lb;
+  const long long ntile = (nlines + w - 1) / w;
+  double per = 0.0;
+  for (int sgi = 0; sgi < 2; sgi++) {
+    const int nv = sgi == 0 ? lb : nout - (nseg - 1) * lb;  // full tiles, then the last one
+    const double count = sgi == 0 ? (double)(nseg - 1) : 1.0;
+    auto rounds = [&](int n) { return (double)((n * (long long)w + W5_THREADS - 1) / W5_THREADS); };
+    per += count * (3.0 * rounds(nv + 2) + 8.0 * (2.0 * rounds(nv + 6) + 0.3 * rounds(nv + 2) + 1.5 * rounds(nv)));
+  }
+  return per * (double)ntile;
+}
+
+// WENO5 tiling of the output box b along direction dir: lines whose cells
+// are contiguous in memory (x3, or any direction of a domain flat across
+// it) are walked along by consecutive threads, the others across
+// (consecutive threads on neighbouring lines, x3 fastest); the tile length
+// and line count are chosen by w5_cost within the shared-memory budget.
+W5Tile w5_tiling(const Dims &d, const Box &b, int dir) {
+  W5Tile t;
+  t.box = b;
+  const int nout = dir == 1 ? b.ni : (dir == 2 ? b.nj : b.nk);
+  const long long nlines = dir == 1 ? (long long)b.nj * b.nk : (dir == 2 ? (long long)b.ni * b.nk : (long long)b.ni * b.nj);
+  const long long stride = dir == 1 ? (long long)d.nt2 * d.nt3 : (dir == 2 ? (long long)d.nt3 : 1LL);
+  t.nlines = (int)nlines;
+  t.fast_s = stride == 1;
+  const long long cap = (long long)(W5_SMEM_MAX / sizeof(double));
+  double best = -1.0;
+  t.lb = 1;
+  t.w = 1;
+  const int ws[] = {1, 2, 4, 8, 16, 32};
+  for (int w : ws) {
+    if (w > nlines && w > 1) break;
+    // coalescing across lines wants at least 8 neighbouring lines (64 B rows)
+    if (!t.fast_s && w < 8 && nlines >= 8) continue;
+    for (int nseg = 1; nseg <= nout; nseg++) {
+      const int lb = (nout + nseg - 1) / nseg;
+      if (w5_smem_elems(lb, w) > cap) continue;
+      if (lb < 8 && nseg > 1) break;
+      const double c = w5_cost(nout, nlines, lb, w);
+      if (best < 0.0 || c < best) {
+        best = c;
+        t.lb = lb;
+        t.w = w;
+      }
+      if (nseg > 64 && lb < 256) break;
+    }
+  }
+  t.nseg = (nout + t.lb - 1) / t.lb;
+  t.ntile = (int)((nlines + t.w - 1) / t.w);
+  t.wshift = 0;
+  while ((1 << t.wshift) < t.w) t.wshift++;
+  return t;
+}
+
+// the WENO5 kernels may use up to W5_SMEM_MAX of dynamic shared memory
+void w5_allow_smem_all() {
+  static std::once_flag once;
+  std::call_once(once, [] {
+    const int m = (int)W5_SMEM_MAX;
+    const cudaFuncAttribute a = cudaFuncAttributeMaxDynamicSharedMemorySize;
+    cudaFuncSetAttribute(weno5_kernel<1, false, double, kWenoMB[0]>, a, m);
+    cudaFuncSetAttribute(weno5_kernel<1, true, double, kWenoMB[0]>, a, m);
+    cudaFuncSetAttribute(weno5_kernel<2, false, double, kWenoMB[0]>, a, m);
+    cudaFuncSetAttribute(weno5_kernel<2, true, double, kWenoMB[0]>, a, m);
+    cudaFuncSetAttribute(weno5_kernel<3, true, double, kWenoMB[0]>, a, m);
+    cudaFuncSetAttribute(weno5_kernel<1, false, double, kWenoMB[1]>, a, m);
+    cudaFuncSetAttribute(weno5_kernel<1, true, double, kWenoMB[1]>, a, m);
+    cudaFuncSetAttribute(weno5_kernel<2, false, double, kWenoMB[1]>, a, m);
+    cudaFuncSetAttribute(weno5_kernel<2, true, double, kWenoMB[1]>, a, m);
+    cudaFuncSetAttribute(weno5_kernel<3, true, double, kWenoMB[1]>, a, m);
+    cudaFuncSetAttribute(weno5_kernel<1, false, float>, a, m);
+    cudaFuncSetAttribute(weno5_kernel<1, true, float>, a, m);
+    cudaFuncSetAttribute(weno5_kernel<2, false, float>, a, m);
+    cudaFuncSetAttribute(weno5_kernel<2, true, float>, a, m);
+    cudaFuncSetAttribute(weno5_kernel<3, true, float>, a, m);
+    cudaGetLastError();
+  });
+}
+
 }  // namespace
 
 // ---------------------------------------------------------------------------
@@ -1077,12 +1166,12 @@ inline unsigned grid_for(long long n, int block) { return (unsigned)((n + block 
 // ---------------------------------------------------------------------------
 enum KernelId {
   K_RESET, K_FLUX1, K_FLUX2, K_FLUX3, K_EMF, K_UPDATE, K_BOUND_GHOST, K_BOUND_POLE, K_BOUND_PFLAG, K_CHECK_GAMMA,
-  K_CHECK_RESOLVE, K_FIX_COLLECT, K_FIX_COMPUTE, K_FIX_SCATTER, K_FINALIZE, K_WENO_A, K_WENO_B, K_INVERT, K_OTHER, K_NKERNELS
+  K_CHECK_RESOLVE, K_FIX_COLLECT, K_FIX_COMPUTE, K_FIX_SCATTER, K_FINALIZE, K_WENO5, K_W5STATE, K_INVERT, K_OTHER, K_NKERNELS
 };
 static const char *kKernelNames[K_NKERNELS] = {
     "reset_stage",  "flux_x1",         "flux_x2",       "flux_x3",       "emf",           "update",
     "bound_ghost",  "bound_pole",      "bound_pflag",   "checksol_gamma", "checksol_resolve", "fixup_collect",
-    "fixup_compute", "fixup_scatter",  "finalize",      "weno_a",        "weno_b",        "invert",        "other"};
+    "fixup_compute", "fixup_scatter",  "finalize",      "weno5",         "w5_state",      "invert",        "other"};
 
 struct ProfEvent {
   int kid;
@@ -1104,7 +1193,7 @@ struct hgpu_ctx {
   double *pk1 = nullptr;  // second intermediate state of TIMEORDER 3 and 4
   double *ui = nullptr;   // ENOFINITEVOLUME: the conserved state at the start of the step (uinitial)
   struct {
-    int flux = 0, weno_b = 0, conserve = 0, invert = 0;  // variant index per kernel family (hgpu_autotune)
+    int flux = 0, weno = 0, conserve = 0, invert = 0;  // variant index per kernel family (hgpu_autotune)
   } tune;
   double *F[4] = {nullptr, nullptr, nullptr, nullptr};
   double *E = nullptr;
@@ -1117,9 +1206,11 @@ struct hgpu_ctx {
   int cap = 0;
   Scalars *sc = nullptr;
   double *staging = nullptr;  // AoS staging for uploads/downloads
-  double *pL = nullptr, *pR = nullptr, *WA = nullptr;  // WENO5 face values and weights scratch
+  double *pL = nullptr, *pR = nullptr;  // WENO5 face values
+  double *w5pu = nullptr;               // WENO5: per-zone dP/P state pieces (2 planes)
   double *progress = nullptr;                          // 4 doubles for hg_progress_async
-  Box wa_box[4], wb_box[4];
+  W5Tile w5[4];  // WENO5 tiling per direction
+  Box w5_state_box;  // zones whose dP/P state pieces some direction reads
   int *istaging = nullptr;
   // batch of 1D instances (hgpu_create_batch)
   int *cell_inst = nullptr;
@@ -1227,7 +1318,7 @@ void hgpu_destroy(hgpu_ctx *x) {
   for (cudaEvent_t e : x->freelist) cudaEventDestroy(e);
   void *ptrs[] = {x->p, x->pk, x->uf, x->ucum, x->F[1], x->F[2], x->F[3], x->E, x->G, x->pflag, x->gammacheck,
                   x->cand, x->fixlist, x->cand_orig, x->cand_dec, x->candmap, x->fixvals, x->sc, x->staging, x->istaging,
-                  x->pL, x->pR, x->WA, x->cell_inst, x->inst, x->progress, x->pk1, x->ui};
+                  x->pL, x->pR, x->w5pu, x->cell_inst, x->inst, x->progress, x->pk1, x->ui};
   for (void *q : ptrs)
     if (q) cudaFree(q);
   cudaStreamDestroy(x->stream);
@@ -1323,17 +1414,25 @@ int hgpu_create(const hgpu_config *cfg, hgpu_ctx **out) {
   x->emf_box = Box{0, 0, 0, d.n1 + d.s1, d.n2 + d.s2, d.n3 + d.s3};
   x->active_box = Box{0, 0, 0, d.n1, d.n2, d.n3};
   x->dq_box = Box{-d.s1, -d.s2, -d.s3, d.n1 + 2 * d.s1, d.n2 + 2 * d.s2, d.n3 + 2 * d.s3};
-  // WENO5 passes: line cells -4..n+3 (A) and -1..n (B) along the direction,
-  // the flux loop's transverse ranges across it
+  // WENO5: output cells -1..n along the direction, the flux loop's
+  // transverse ranges across it
   for (int q = 1; q <= 3; q++) {
-    Box a = x->face_box[q], b = x->face_box[q];
+    Box b = x->face_box[q];
     int n = (q == 1) ? d.n1 : ((q == 2) ? d.n2 : d.n3);
-    if (q == 1) { a.i0 = -4; a.ni = n + 8; b.i0 = -1; b.ni = n + 2; }
-    if (q == 2) { a.j0 = -4; a.nj = n + 8; b.j0 = -1; b.nj = n + 2; }
-    if (q == 3) { a.k0 = -4; a.nk = n + 8; b.k0 = -1; b.nk = n + 2; }
-    x->wa_box[q] = a;
-    x->wb_box[q] = b;
+    if (q == 1) { b.i0 = -1; b.ni = n + 2; }
+    if (q == 2) { b.j0 = -1; b.nj = n + 2; }
+    if (q == 3) { b.k0 = -1; b.nk = n + 2; }
+    x->w5[q] = w5_tiling(d, b, q);
   }
+  // the state pieces are read at cells -2..n+1 along each direction, across
+  // it over the flux loop's transverse range (every ghost for the
+  // finite-volume scheme)
+  {
+    const int fvg = cfg->doenoflux == HGPU_ENOFINITEVOLUME;
+    const int e1 = fvg ? d.g1 : 2 * d.s1, e2 = fvg ? d.g2 : 2 * d.s2, e3 = fvg ? d.g3 : 2 * d.s3;
+    x->w5_state_box = Box{-e1, -e2, -e3, d.n1 + 2 * e1, d.n2 + 2 * e2, d.n3 + 2 * e3};
+  }
+  if (cfg->lim == HGPU_LIM_WENO5) w5_allow_smem_all();
   long long nz = d.nz;
   x->cap = (int)((long long)d.n1 * d.n2 * d.n3 < (1LL << 22) ? (long long)d.n1 * d.n2 * d.n3 : (1LL << 22));
   if (cudaStreamCreateWithFlags(&x->stream, cudaStreamNonBlocking) != cudaSuccess) {
@@ -1362,7 +1461,7 @@ int hgpu_create(const hgpu_config *cfg, hgpu_ctx **out) {
          cudaMemset(x->ucum, 0, pb) == cudaSuccess;
   if (ok && cfg->lim == HGPU_LIM_WENO5)
     ok = cudaMalloc(&x->pL, pb) == cudaSuccess && cudaMalloc(&x->pR, pb) == cudaSuccess &&
-         cudaMalloc(&x->WA, pb * W5_PLANES) == cudaSuccess;
+         cudaMalloc(&x->w5pu, sizeof(double) * 2 * nz) == cudaSuccess;
   if (!ok) {
     hgpu_destroy(x);
     set_err("device allocation failed");
@@ -1555,18 +1654,30 @@ int hgpu_download_state(hgpu_ctx *x, double *p, int *pflag, double *t, double *d
 // one stage: fluxes, EMFs, update, bound, post_fixup, bound
 extern "C++" {
 // one direction's reconstruction + flux launches; FMB / BMB: resident
-// blocks per SM asked of the flux and weno_b kernels (autotuned variants)
+// blocks per SM asked of the flux and WENO5 kernels (autotuned variants)
 template <int DIR, typename T, int FMB, int BMB>
 static void launch_dir(hgpu_ctx *x, const double *pb) {
   const Dims &d = x->d;
   const Params &P = x->P;
-  T *WA = (T *)x->WA, *pL = (T *)x->pL, *pR = (T *)x->pR;
+  T *pL = (T *)x->pL, *pR = (T *)x->pR;
+  const T *PU = (const T *)x->w5pu;
   const int kid = (DIR == 1) ? K_FLUX1 : ((DIR == 2) ? K_FLUX2 : K_FLUX3);
   unsigned gf = grid_for(x->face_box[DIR].size(), 128);
   if (P.lim == HGPU_LIM_WENO5) {
-    unsigned ga = grid_for(x->wa_box[DIR].size(), 128), gb = grid_for(x->wb_box[DIR].size(), 128);
-    LAUNCH(x, K_WENO_A, (weno_a_kernel<DIR, T>), ga, 128, d, x->wa_box[DIR], pb, WA);
-    LAUNCH(x, K_WENO_B, (weno_b_kernel<DIR, T, BMB>), gb, 128, d, P, x->wb_box[DIR], pb, x->G, WA, pL, pR);
+    const W5Tile &tl = x->w5[DIR];
+    const size_t smem = sizeof(T) * (size_t)w5_smem_elems(tl.lb, tl.w);
+    {
+      ProfScope ps__(x, K_WENO5);
+      const unsigned grid = (unsigned)tl.nseg * tl.ntile;
+      if constexpr (DIR == 3) {
+        weno5_kernel<3, true, T, BMB><<<grid, W5_THREADS, smem, x->stream>>>(d, P, tl, pb, PU, pL, pR);
+      } else {
+        if (tl.fast_s)
+          weno5_kernel<DIR, true, T, BMB><<<grid, W5_THREADS, smem, x->stream>>>(d, P, tl, pb, PU, pL, pR);
+        else
+          weno5_kernel<DIR, false, T, BMB><<<grid, W5_THREADS, smem, x->stream>>>(d, P, tl, pb, PU, pL, pR);
+      }
+    }
     LAUNCH(x, kid, (flux_kernel<DIR, 1, T, FMB>), gf, 128, d, P, x->face_box[DIR], pb, pL, pR, x->G, x->F[DIR], x->sc);
   } else if (P.lim == HGPU_LIM_PARA) {
     LAUNCH(x, kid, (flux_kernel<DIR, 2, T, FMB>), gf, 128, d, P, x->face_box[DIR], pb, nullptr, nullptr, x->G,
@@ -1580,6 +1691,9 @@ static void launch_dir(hgpu_ctx *x, const double *pb) {
 template <typename T, int FMB, int BMB>
 static void launch_fluxes_t(hgpu_ctx *x, const double *pb) {
   const Dims &d = x->d;
+  if (x->P.lim == HGPU_LIM_WENO5)
+    LAUNCH(x, K_W5STATE, w5_state_kernel<T>, grid_for(x->w5_state_box.size(), 128), 128, d, x->P, x->w5_state_box, pb,
+           x->G, (T *)x->w5pu);
   if (d.n1 > 1) launch_dir<1, T, FMB, BMB>(x, pb);
   if (d.n2 > 1) launch_dir<2, T, FMB, BMB>(x, pb);
   if (d.n3 > 1) launch_dir<3, T, FMB, BMB>(x, pb);
@@ -1592,13 +1706,13 @@ static void launch_fluxes_t(hgpu_ctx *x, const double *pb) {
 static void launch_fluxes(hgpu_ctx *x, const double *pb) {
   const Dims &d = x->d;
   if (x->cfg.precision == HGPU_PREC_MIXED) {
-    launch_fluxes_t<float, MinBlocks<float>::flux, MinBlocks<float>::weno_b>(x, pb);
+    launch_fluxes_t<float, MinBlocks<float>::flux, MinBlocks<float>::weno>(x, pb);
   } else {
-    const int fv = x->tune.flux, bv = x->tune.weno_b;
-    if (fv == 0 && bv == 0) launch_fluxes_t<double, kFluxMB[0], kWenoBMB[0]>(x, pb);
-    else if (fv == 0) launch_fluxes_t<double, kFluxMB[0], kWenoBMB[1]>(x, pb);
-    else if (bv == 0) launch_fluxes_t<double, kFluxMB[1], kWenoBMB[0]>(x, pb);
-    else launch_fluxes_t<double, kFluxMB[1], kWenoBMB[1]>(x, pb);
+    const int fv = x->tune.flux, bv = x->tune.weno;
+    if (fv == 0 && bv == 0) launch_fluxes_t<double, kFluxMB[0], kWenoMB[0]>(x, pb);
+    else if (fv == 0) launch_fluxes_t<double, kFluxMB[0], kWenoMB[1]>(x, pb);
+    else if (bv == 0) launch_fluxes_t<double, kFluxMB[1], kWenoMB[0]>(x, pb);
+    else launch_fluxes_t<double, kFluxMB[1], kWenoMB[1]>(x, pb);
   }
   LAUNCH(x, K_EMF, emf_kernel, grid_for(x->emf_box.size(), 256), 256, d, x->emf_box, x->F[1], x->F[2], x->F[3], x->G,
          x->E);
@@ -2118,7 +2232,7 @@ int hgpu_step_ch_timed(hgpu_ctx *x, int nsteps, float *ms, hgpu_stats *stats) {
   return read_stats(x, stats);
 }
 
-// Autotuner: for each FP64 kernel family (flux, weno_b, conserve, invert)
+// Autotuner: for each FP64 kernel family (flux, WENO5, conserve, invert)
 // time both resident-block variants on the context's own state (one warm-up
 // step and one timed step each, kernel times from the profiling events, the
 // state restored before every trial) and keep the faster.  The variants
@@ -2164,9 +2278,9 @@ int hgpu_autotune(hgpu_ctx *x, hgpu_tuning *out) {
     launch_finalize(x, 1);
   };
   const bool fp64 = x->cfg.precision == HGPU_PREC_FP64;
-  int *knob[4] = {&x->tune.flux, &x->tune.weno_b, &x->tune.conserve, &x->tune.invert};
+  int *knob[4] = {&x->tune.flux, &x->tune.weno, &x->tune.conserve, &x->tune.invert};
   const bool applies[4] = {fp64, fp64 && x->P.lim == HGPU_LIM_WENO5, true, true};
-  const int kids[4][3] = {{K_FLUX1, K_FLUX2, K_FLUX3}, {K_WENO_B, -1, -1}, {K_UPDATE, -1, -1}, {K_INVERT, -1, -1}};
+  const int kids[4][3] = {{K_FLUX1, K_FLUX2, K_FLUX3}, {K_WENO5, -1, -1}, {K_UPDATE, -1, -1}, {K_INVERT, -1, -1}};
   float ms[4][2] = {{0.f, 0.f}, {0.f, 0.f}, {0.f, 0.f}, {0.f, 0.f}};
   int rc = HGPU_OK;
   x->profiling = true;
@@ -2209,16 +2323,16 @@ int hgpu_autotune(hgpu_ctx *x, hgpu_tuning *out) {
   x->graph = nullptr;
   if (out) {
     out->flux_minb = kFluxMB[x->tune.flux];
-    out->weno_b_minb = kWenoBMB[x->tune.weno_b];
+    out->weno_minb = kWenoMB[x->tune.weno];
     out->update_minb = kConserveMB[x->tune.conserve];
     out->invert_minb = kInvertMB[x->tune.invert];
     for (int v = 0; v < 2; v++) {
       out->flux_ms[v] = ms[0][v];
-      out->weno_b_ms[v] = ms[1][v];
+      out->weno_ms[v] = ms[1][v];
       out->update_ms[v] = ms[2][v];
       out->invert_ms[v] = ms[3][v];
       out->flux_cand[v] = kFluxMB[v];
-      out->weno_b_cand[v] = kWenoBMB[v];
+      out->weno_cand[v] = kWenoMB[v];
       out->update_cand[v] = kConserveMB[v];
       out->invert_cand[v] = kInvertMB[v];
     }
@@ -2230,12 +2344,12 @@ int hgpu_autotune(hgpu_ctx *x, hgpu_tuning *out) {
 int hgpu_set_tuning(hgpu_ctx *x, const hgpu_tuning *t) {
   if (!x || !t) return HGPU_E_INVALID;
   auto pick = [](const int *cand, int minb) { return cand[1] == minb ? 1 : (cand[0] == minb ? 0 : -1); };
-  const int f = pick(kFluxMB, t->flux_minb), b = pick(kWenoBMB, t->weno_b_minb);
+  const int f = pick(kFluxMB, t->flux_minb), b = pick(kWenoMB, t->weno_minb);
   const int u = pick(kConserveMB, t->update_minb), v = pick(kInvertMB, t->invert_minb);
   if (f < 0 || b < 0 || u < 0 || v < 0) return HGPU_E_INVALID;
   CUDA_TRY(cudaStreamSynchronize(x->stream));
   x->tune.flux = f;
-  x->tune.weno_b = b;
+  x->tune.weno = b;
   x->tune.conserve = u;
   x->tune.invert = v;
   if (x->graph_exec) cudaGraphExecDestroy(x->graph_exec);
@@ -2488,7 +2602,7 @@ extern "C" size_t hgpu_context_bytes(const hgpu_config *c) {
              + sizeof(double) * nz            // gamma check
              + cap * (2 * sizeof(long long) + 2 * sizeof(int) + 5 * sizeof(double))
              + plane;                         // staging for uploads and downloads
-  if (c->lim == HGPU_LIM_WENO5) b += 2 * plane + W5_PLANES * plane;
+  if (c->lim == HGPU_LIM_WENO5) b += 2 * plane + sizeof(double) * 2 * nz;  // pL, pR, dP/P state pieces
   if (c->timeorder >= 3) b += plane;                     // pk1
   if (c->doenoflux == HGPU_ENOFINITEVOLUME) b += plane;  // ui
   return b;

@@ -9,11 +9,12 @@
 // The reference reconstructs whole lines; every quantity of one output cell
 // c depends only on the line from c-5 to c+5 (for the reference's MAXBND=11
 // lines no stencil reaches a line end, so its boundary-truncation branches
-// are dead).  The GPU splits the line work into two cell-parallel passes:
-//   pass A (per cell, per primitive): SMONO cusp test and indicator, and the
+// are dead).  These are the per-cell pieces; weno5_kernel (common.cuh)
+// stages them over tiles of a line in shared memory:
+//   per cell, per primitive: SMONO cusp test and indicator, and the
 //          unoptimised order-3 weights (compute_cf_stencil_weights +
 //          mono_adjust_unoptimized_weights)
-//   pass B (per output cell): weight ratios of c-1..c+1 (compute_weights_ratios),
+//   per output cell: weight ratios of c-1..c+1 (compute_weights_ratios),
 //          dP/P reduction (apply_additional_reduction_to_weights), optimised
 //          weights, order-2 weights when reduced (choose_weno_order) and the
 //          face values (eno_cvt + the SMONO blend).
@@ -84,6 +85,28 @@ __device__ __forceinline__ T sum5(const T *a) {
   return s;
 }
 
+// x / 12 rounded to nearest without a division instruction.  q = RN(x r)
+// with r = RN(1/12) is within 2 ulp of x/12, so e = x - 12 q is exact (a
+// small multiple of 4 ulp(q)), and q + e r, rounded once by the FMA, differs
+// from x/12 by at most 2^-52 ulp.  x/12 = (x/3)/4, and x/3 has a significand
+// fraction of 0, 1/3 or 2/3 ulp, so x/12 lies at least 1/6 ulp from every
+// rounding midpoint (or is a float): the result is RN(x/12), the bits of
+// the IEEE division.  Magnitudes outside [2^-960, 2^1000] (where the steps
+// could underflow or overflow), zeros, infinities and NaN take the division.
+// The FP32 kernels of the mixed-precision path are built with approximate
+// division and keep it.
+template <typename T>
+__device__ __forceinline__ T div12(T x) { return x / T(12.); }
+template <>
+__device__ __forceinline__ double div12<double>(double x) {
+  const double ax = fabs(x);
+  if (!(ax >= 0x1p-960 && ax <= 0x1p1000)) return x / 12.0;
+  const double r = 1.0 / 12.0;
+  const double q = x * r;
+  const double e = fma(-q, 12.0, x);
+  return fma(e, r, q);
+}
+
 // check_for_cusp_new (smonointerp.c:439-476); y points at the cell (y[-2..2] valid)
 template <typename T>
 __device__ __forceinline__ bool cusp(const T *y) {
@@ -115,12 +138,13 @@ __device__ __forceinline__ bool cusp(const T *y) {
 // compute_mono_indicator_point_eno5 (smonointerp.c:296-425) + transition_function (:428-437)
 template <typename T>
 __device__ __forceinline__ T mono(const T *y) {
-  T l1 = (((-3 * y[-2] + y[2]) + (-10 * y[-1] - 6 * y[1])) + 18 * y[0]) / T(12.);
-  T l2 = (((11 * y[-2] - y[2]) + (-20 * y[-1] + 4 * y[1])) + 6 * y[0]) / T(12.);
-  T l3 = (((-3 * y[-2] - y[2]) + (10 * y[-1] + 6 * y[1])) - 12 * y[0]) / T(2.);
-  T r1 = (((-y[-2] + 3 * y[2]) + (6 * y[-1] + 10 * y[1])) - 18 * y[0]) / T(12.);
-  T r2 = (((-y[-2] + 11 * y[2]) + (4 * y[-1] - 20 * y[1])) + 6 * y[0]) / T(12.);
-  T r3 = (((y[-2] + 3 * y[2]) - (6 * y[-1] + 10 * y[1])) + 12 * y[0]) / T(2.);
+  // (division by 2 is the exact multiplication by 1/2)
+  T l1 = div12((((-3 * y[-2] + y[2]) + (-10 * y[-1] - 6 * y[1])) + 18 * y[0]));
+  T l2 = div12((((11 * y[-2] - y[2]) + (-20 * y[-1] + 4 * y[1])) + 6 * y[0]));
+  T l3 = (((-3 * y[-2] - y[2]) + (10 * y[-1] + 6 * y[1])) - 12 * y[0]) * T(0.5);
+  T r1 = div12((((-y[-2] + 3 * y[2]) + (6 * y[-1] + 10 * y[1])) - 18 * y[0]));
+  T r2 = div12((((-y[-2] + 11 * y[2]) + (4 * y[-1] - 20 * y[1])) + 6 * y[0]));
+  T r3 = (((y[-2] + 3 * y[2]) - (6 * y[-1] + 10 * y[1])) + 12 * y[0]) * T(0.5);
   l1 = minmod(l1, y[-1] - y[-2]);
   r1 = minmod(r1, y[2] - y[1]);
   T minabs = K<T>::big;

@@ -43,9 +43,9 @@ class hgpu_config(ctypes.Structure):
 
 
 class hgpu_tuning(ctypes.Structure):
-    _fields_ = [(n, ctypes.c_int) for n in ("flux_minb", "weno_b_minb", "update_minb", "invert_minb")] + \
-               [(n, ctypes.c_int * 2) for n in ("flux_cand", "weno_b_cand", "update_cand", "invert_cand")] + \
-               [(n, ctypes.c_float * 2) for n in ("flux_ms", "weno_b_ms", "update_ms", "invert_ms")]
+    _fields_ = [(n, ctypes.c_int) for n in ("flux_minb", "weno_minb", "update_minb", "invert_minb")] + \
+               [(n, ctypes.c_int * 2) for n in ("flux_cand", "weno_cand", "update_cand", "invert_cand")] + \
+               [(n, ctypes.c_float * 2) for n in ("flux_ms", "weno_ms", "update_ms", "invert_ms")]
 
 
 class hgpu_diag(ctypes.Structure):
@@ -305,16 +305,16 @@ class HarmGPU:
         tu = hgpu_tuning()
         _check(self.L, self.L.hgpu_autotune(self.h, ctypes.byref(tu)))
         out = {}
-        for fam in ("flux", "weno_b", "update", "invert"):
+        for fam in ("flux", "weno", "update", "invert"):
             cand = list(getattr(tu, fam + "_cand"))
             ms = list(getattr(tu, fam + "_ms"))
             out[fam] = {"minb": getattr(tu, fam + "_minb"), "ms": {str(c): round(m, 4) for c, m in zip(cand, ms)}}
         return out
 
     def set_tuning(self, minb):
-        """hgpu_set_tuning: {"flux": 4, "weno_b": 8, "update": 3, "invert": 1} (blocks per SM)."""
+        """hgpu_set_tuning: {"flux": 4, "weno": 2, "update": 3, "invert": 1} (blocks per SM)."""
         tu = hgpu_tuning()
-        tu.flux_minb, tu.weno_b_minb = int(minb["flux"]), int(minb["weno_b"])
+        tu.flux_minb, tu.weno_minb = int(minb["flux"]), int(minb["weno"])
         tu.update_minb, tu.invert_minb = int(minb["update"]), int(minb["invert"])
         _check(self.L, self.L.hgpu_set_tuning(self.h, ctypes.byref(tu)))
 

@@ -33,7 +33,7 @@
 extern "C" {
 #endif
 
-#define HGPU_ABI_VERSION 7
+#define HGPU_ABI_VERSION 8
 
 /* return codes */
 #define HGPU_OK 0
@@ -167,9 +167,12 @@ int hgpu_utoprimgen_batch(const double *U, const double *gcov, const double *gco
    n is rejected with HGPU_E_INVALID and a message), held by every GPU that
    loads the library until the process exits.  The first call on a device
    looks up the array's device address (cudaGetSymbolAddress) with that device
-   current; make that first call before any stream capture.  All calls share
-   the array and each call overwrites it, so calls that overlap on the GPU
-   (other host threads, other streams) race: serialise them. */
+   current; make that first call before any stream capture.  That address is
+   kept for the life of the process: after cudaDeviceReset (or anything else
+   that destroys the device's primary context) it is stale, so do not call
+   this entry point again in that process.  All calls share the array and
+   each call overwrites it, so calls that overlap on the GPU (other host
+   threads, other streams) race: serialise them. */
 #define HGPU_NOALLOC_MAX_ZONES 16384
 int hgpu_utoprim_batch_noalloc(const double *U, const double *gcov, const double *gcon, const double *gdet,
                                double *pr, int *pflag, long long n, double gam, double gammafail, long long *iters);
@@ -207,18 +210,18 @@ int hgpu_batch_run(hgpu_ctx *ctx, int check_every, int max_steps, int *steps, fl
    hgpu_step_ch. */
 int hgpu_step_graph(hgpu_ctx *ctx, int nsteps, hgpu_stats *stats);
 
-/* Autotuner (no counterpart in the reference): for the FP64 flux, weno_b,
-   update and inversion kernels, times two resident-blocks-per-SM variants
+/* Autotuner (no counterpart in the reference): for the FP64 flux, WENO5
+   reconstruction, update and inversion kernels, times two resident-blocks-per-SM variants
    (registers per thread vs warps per SM) on this context's own state and
    keeps the faster for later steps.  Results do not depend on the choice;
    the state is left as it was (for a batch context, every instance's t,
    dt, done flag and step count too).  *_ms: kernel milliseconds of one step per
-   candidate (0 where a family does not apply: weno_b without WENO5, flux and
-   weno_b in the mixed-precision mode). */
+   candidate (0 where a family does not apply: weno without WENO5, flux and
+   weno in the mixed-precision mode). */
 typedef struct {
-  int flux_minb, weno_b_minb, update_minb, invert_minb;
-  int flux_cand[2], weno_b_cand[2], update_cand[2], invert_cand[2];
-  float flux_ms[2], weno_b_ms[2], update_ms[2], invert_ms[2];
+  int flux_minb, weno_minb, update_minb, invert_minb;
+  int flux_cand[2], weno_cand[2], update_cand[2], invert_cand[2];
+  float flux_ms[2], weno_ms[2], update_ms[2], invert_ms[2];
 } hgpu_tuning;
 int hgpu_autotune(hgpu_ctx *ctx, hgpu_tuning *out);
 /* Apply a choice found before (the *_minb fields; each must be one of the

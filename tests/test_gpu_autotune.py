@@ -31,11 +31,11 @@ def test_autotune_keeps_state_and_results(name):
 def test_set_tuning_applies_a_known_choice():
     pr, ref = load("torus2d_16x16_mc_hll")
     with HarmGPU.from_problem(pr) as g:
-        g.set_tuning({"flux": 3, "weno_b": 6, "update": 3, "invert": 2})
+        g.set_tuning({"flux": 3, "weno": 3, "update": 3, "invert": 2})
         s = sorted(ref)[-1]
         g.step_ch(s)
         p, pf, t, dt = g.download_state()
         with pytest.raises(Exception):
-            g.set_tuning({"flux": 7, "weno_b": 8, "update": 1, "invert": 1})
+            g.set_tuning({"flux": 7, "weno": 8, "update": 1, "invert": 1})
     r = ref[s]
     assert same(p, r["p"]) and np.array_equal(pf, r["pflag"]) and t == r["t"] and dt == r["dt"]

@@ -75,6 +75,22 @@ def test_noalloc_matches_allocating_entry_point_twice():
         assert ia == ib
 
 
+def test_noalloc_takes_no_device_memory():
+    # the device's free memory is the same before and after further calls
+    # (the first call, which looks up the scratch array, comes first)
+    import torch
+    U, gcov, gcon, gdet, guess, gam, gfail = inputs(13, 0.1)
+    rc, *_ = noalloc(U, gcov, gcon, gdet, guess, gam, gfail)
+    assert rc == 0, load_library().hgpu_last_error()
+    torch.cuda.synchronize()
+    free0 = torch.cuda.mem_get_info()[0]
+    for _ in range(3):
+        rc, *_ = noalloc(U, gcov, gcon, gdet, guess, gam, gfail)
+        assert rc == 0, load_library().hgpu_last_error()
+    torch.cuda.synchronize()
+    assert torch.cuda.mem_get_info()[0] == free0
+
+
 def test_noalloc_rejects_oversized_batch():
     n = MAX_ZONES + 1
     z = np.zeros((n, 8))
