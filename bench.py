@@ -246,8 +246,10 @@ def measured_peaks():
 
 
 def _traffic_row(workload, kernel):
-    """(DRAM bytes, FP64 flop) per launch of `kernel` on `workload` from the
-    committed ncu summary profiles/traffic.md, or None."""
+    """(DRAM bytes, FP64 instructions) per launch of `kernel` on `workload`
+    from the committed ncu summary profiles/traffic.md, or None.  FP64
+    instructions = DADD + DMUL + DFMA executed (thread-level), the unit of the
+    FP64 issue-rate peak."""
     path = os.path.join(ROOT, "profiles", "traffic.md")
     try:
         txt = open(path).read()
@@ -256,6 +258,18 @@ def _traffic_row(workload, kernel):
     m = re.search(rf"^\|\s*{re.escape(workload)}\s*\|\s*{re.escape(kernel)}\s*\|\s*([0-9.eE+]+)\s*\|\s*([0-9.eE+]+)\s*\|",
                   txt, re.M)
     return (float(m.group(1)), float(m.group(2))) if m else None
+
+
+def step_dram_bytes(workload):
+    """ncu DRAM bytes (read + write) of one whole time step of `workload`, from
+    profiles/traffic.md, or None."""
+    path = os.path.join(ROOT, "profiles", "traffic.md")
+    try:
+        txt = open(path).read()
+    except OSError:
+        return None
+    m = re.search(rf"^\|\s*{re.escape(workload)}\s*\|\s*step\s*\|\s*([0-9.eE+]+)\s*\|", txt, re.M)
+    return float(m.group(1)) if m else None
 
 
 def profile_traffic(workload, kernel):
@@ -425,15 +439,18 @@ def bench_ours(args, rank, world):
             a0 = diag0["integral"][q]
             return (dg["integral"][q] - a0) / abs(a0) if a0 else None
 
+        # the torus's single field loop has zero net magnetic flux: its
+        # drift is reported as the absolute change of the integral
         cons = {prec: {"mass_drift": drift(dg, 0), "energy_drift": drift(dg, 1),
-                       "magnetic_flux_drift": [drift(dg, q) for q in (5, 6, 7)],
+                       "magnetic_flux_change": [dg["integral"][q] - diag0["integral"][q] for q in (5, 6, 7)],
                        "divb_max_interior": dg["divb_max_interior"], "failures_last_step": dg["nfail"]}
                 for prec, dg in (("fp64", d64), ("mixed", d32))}
         other = {"precision": other_prec, "value": zones * args.steps * world / (ms2 / 1e3),
                  "ms_per_step": ms2 / args.steps, "steps_compared": args.warmup + args.steps + extra,
                  "rel_l1_mixed_vs_fp64": err, "conservation": cons,
-                 "note": "mixed = FP32 reconstruction, wave speeds and Riemann fluxes; FP64 flux-CT, conserved "
-                         "update, con-to-prim and fixups; both runs from the same initial state"}
+                 "note": "mixed = FP32 WENO5 reconstruction (on differences from each cell's value, FP64 "
+                         "epsilons; MC/PARA: FP32 Riemann kernel); FP64 Riemann fluxes, flux-CT, conserved update, "
+                         "con-to-prim and fixups; both runs from the same initial state"}
 
     # per-kernel device times for the roofline (a separate profiled pass)
     g.set_profiling(True)
@@ -479,6 +496,17 @@ def bench_ours(args, rank, world):
     fp64 = fp64_roof(kt, dom_k, args)
     if fp64:
         roof["fp64"] = fp64
+    # the whole step against the path's compulsory bytes: 392 B per
+    # zone-update (2 substeps x [read p_b 64 + read p^n 64 + write p_f 64 +
+    # pflag 4], state resident, metric per (i,j) amortised over x3), beside
+    # the DRAM bytes ncu counted for one step
+    step_s = ms_max / args.steps / 1e3
+    step_alg = 392.0 * zones
+    sdb = step_dram_bytes(args.workload)
+    roof["step"] = {"algorithmic_bytes": step_alg, "achieved_gbs": step_alg / step_s / 1e9,
+                    "frac": step_alg / step_s / 1e9 / peaks["hbm_gbs"], "dram_bytes_ncu": sdb,
+                    "dram_over_algorithmic": (sdb / step_alg) if sdb else None,
+                    "dram_gbs": (sdb / step_s / 1e9) if sdb else None}
 
     result = {
         "metric": METRIC, "value": value, "unit": "zone-updates/s", "n_gpus": world, "steps": args.steps,
@@ -724,11 +752,17 @@ def algorithmic_bytes(kernel, n1, n2, n3, lim="MC", tx=1):
         return faces[kernel] * (64 + 64)          # read one zone's 8 primitives, write 8 face fluxes
     # the WENO5 passes run once per direction under one name: mean cells per launch
     nd = [n for n in (n1, n2, n3) if n > 1]
-    if kernel in ("weno_a", "weno_b"):
-        ext = 8 if kernel == "weno_a" else 2
-        cells = sum(zones / n * (n + ext) for n in nd) / len(nd)
-        # A: read 8 primitives, write 4 planes x 8; B: read 8 primitives + 4x8 planes, write 16 face values
-        return cells * ((64 + 256) if kernel == "weno_a" else (64 + 256 + 128))
+    if kernel == "weno5":
+        # output cells -1..n along the direction (mean over the directions):
+        # read 8 primitives and the 2 dP/P state pieces, write 16 face values
+        cells = sum(zones / n * (n + 2) for n in nd) / len(nd)
+        return cells * (64 + 16 + 128)
+    if kernel == "w5_state":
+        # zones -2..n+1: read 8 primitives, write 2 state pieces
+        ext = 1.0
+        for n in (n1, n2, n3):
+            ext *= (n + 4) / n if n > 1 else 1.0
+        return zones * ext * (64 + 16)
     if kernel == "update":
         # mean of the two substeps: p(64) [+pk 64] + 5 F comps x3 dirs (120) + 3 EMFs (24)
         # + uf/ucum write (128) [+read 128] + pf (64) + pflag (4)
@@ -741,18 +775,23 @@ def algorithmic_bytes(kernel, n1, n2, n3, lim="MC", tx=1):
 
 
 def fp64_roof(kt, kernel, args):
-    """FP64 rate of the dominant kernel from the per-launch FP64 operation count
-    measured with ncu (profiles/traffic.md) vs the FP64 peak measured here."""
+    """FP64 issue rate of the dominant kernel: FP64 instructions per launch
+    (DADD + DMUL + DFMA, ncu, profiles/traffic.md) over its CUDA-event time,
+    against the FP64 instruction issue rate measured here (hgpu_fp64_peak:
+    independent DADD/DMUL streams; a DFMA issues at the same rate).  Both
+    numbers count instructions, one per FP64 operation issued."""
     r = _traffic_row(args.workload, kernel)
     if not r or r[1] <= 0:
         return None
-    ops_per_launch = r[1]
+    inst_per_launch = r[1]
     avg_s = kt["ms"] / kt["launches"] / 1e3
-    achieved = ops_per_launch / avg_s / 1e12
+    achieved = inst_per_launch / avg_s / 1e12
     peak = measure_fp64_peak()
-    return {"achieved_tflops": achieved, "peak_tflops": peak, "frac": achieved / peak if peak else None,
-            "note": "FP64 DADD+DMUL+2*DFMA per launch from ncu; peak = measured DADD/DMUL issue rate (no FMA: "
-                    "the FP64 path is built with -fmad=false for bit-identity)"}
+    return {"achieved_tinst_s": achieved, "peak_tinst_s": peak, "frac": achieved / peak if peak else None,
+            "unit": "T FP64 instructions/s",
+            "note": "DADD+DMUL+DFMA instructions per launch from ncu over the CUDA-event launch time; peak = "
+                    "measured FP64 issue rate of this GPU (the FP64 path is built with -fmad=false for "
+                    "bit-identity, so its FMAs are those inside the IEEE division/sqrt sequences)"}
 
 
 _FP64_PEAK = None
@@ -782,8 +821,9 @@ def main():
     ap.add_argument("--no-compare", action="store_true",
                     help="skip the run of the other precision mode (rate and error vs FP64)")
     ap.add_argument("--e2e-steps", type=int, default=5)
-    ap.add_argument("--compare-steps", type=int, default=0,
-                    help="steps of the FP64-vs-mixed comparison (default: warm-up + timed steps)")
+    ap.add_argument("--compare-steps", type=int, default=1000,
+                    help="steps of the FP64-vs-mixed comparison (the precision-at-scale configuration runs 1000; "
+                         "0: warm-up + timed steps)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-steps", type=int, default=3)
     ap.add_argument("--cpu-procs", type=int, default=0,

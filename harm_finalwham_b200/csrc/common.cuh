@@ -214,7 +214,7 @@ __device__ __forceinline__ void para4(const T *y, T *lout, T *rout) {
 #define HG_MINB_FLUX_F32 8
 #endif
 #ifndef HG_MINB_WENO_F32
-#define HG_MINB_WENO_F32 3
+#define HG_MINB_WENO_F32 4
 #endif
 template <typename T> struct MinBlocks;
 template <> struct MinBlocks<double> {
@@ -271,7 +271,11 @@ __device__ __forceinline__ void load_metric_t(const double *__restrict__ G, cons
 // The output cells of a direction are the line cells -1..n (the box), every
 // line across it that the flux loop covers.  Every quantity is formed by the
 // same device functions, in the same operation order, as before tiling, so
-// the FP64 results stay bit-identical to the reference.
+// the FP64 results stay bit-identical to the reference.  T = float is the
+// reconstruction of the mixed-precision path: its line is kept in FP64, it
+// works on differences from each cell's own value and writes FP64 face
+// values (the cell's value plus the FP32 offset), which the FP64 Riemann
+// kernel reads.
 // ---------------------------------------------------------------------------
 constexpr int W5_THREADS = 256;
 
@@ -311,9 +315,12 @@ __global__ void __launch_bounds__(128) w5_state_kernel(Dims d, Params P, Box box
   PU[d.nz + z] = gam * pc[UU] * (q.ucon[0] * q.ucov[0]) + (gam - T(1.0)) * pc[UU];
 }
 
-// shared-memory elements of a tile with lb output cells on w lines:
-// Y (lb+10) + A 4 (lb+6) + R (lb+2) + the shock factor lb, per line
-__host__ __device__ inline long long w5_smem_elems(int lb, int w) { return (long long)w * (7LL * lb + 36); }
+// shared-memory bytes of a tile with lb output cells on w lines: per line
+// Y (lb+10) in FP64, and in the arithmetic type (tsize bytes) A 4 (lb+6),
+// R (lb+2) and the shock factor lb
+__host__ __device__ inline long long w5_smem_bytes(int lb, int w, int tsize) {
+  return (long long)w * (8LL * (lb + 10) + (long long)tsize * (6LL * lb + 26));
+}
 
 // zone index of cell 0 of line `line` of box b (along the line the index
 // steps by dir_stride)
@@ -336,11 +343,10 @@ __device__ __forceinline__ long long w5_line(const Dims &d, const Box &b, int li
 template <int DIR, bool FS, typename T, int MB = MinBlocks<T>::weno>
 __global__ void __launch_bounds__(W5_THREADS, MB) weno5_kernel(Dims d, Params P, W5Tile tl,
                                                                const double *__restrict__ pb,
-                                                               const T *__restrict__ PU, T *__restrict__ pL,
-                                                               T *__restrict__ pR) {
+                                                               const T *__restrict__ PU, double *__restrict__ pL,
+                                                               double *__restrict__ pR) {
   extern __shared__ __align__(16) unsigned char w5_smem[];
   __shared__ long long zb[32];
-  T *sm = reinterpret_cast<T *>(w5_smem);
   const int W = tl.w;
   const int seg = blockIdx.x % tl.nseg;
   const int line0 = (blockIdx.x / tl.nseg) * W;
@@ -356,12 +362,30 @@ __global__ void __launch_bounds__(W5_THREADS, MB) weno5_kernel(Dims d, Params P,
   const int r = FS ? (int)(threadIdx.x & (TL - 1)) : (int)(threadIdx.x >> tl.wshift);
   const bool on = w < nl;
   if (threadIdx.x < nl) zb[threadIdx.x] = w5_line<DIR>(d, tl.box, line0 + threadIdx.x);
-  T *Y = sm;                        // cells -5 .. nv+4
-  T *A = Y + (long long)NS * W;     // 4 planes, cells -3 .. nv+2: code (indicator, -1 at a cusp), w0, w1, w2
+  double *Y = reinterpret_cast<double *>(w5_smem);                  // cells -5 .. nv+4
+  T *A = reinterpret_cast<T *>(Y + (long long)NS * W);  // 4 planes, cells -3 .. nv+2: code (indicator, -1 at a cusp), w0, w1, w2
   T *R = A + 4LL * NA * W;          // cells -1 .. nv: lower-order fraction
   T *SS = R + (long long)NL * W;    // output cells: shock reduction factor
   // element s of this thread's line in a plane with n cells per line
   auto at = [&](T *plane, int n, int s) -> T & { return FS ? plane[w * n + s] : plane[s * W + w]; };
+  auto aty = [&](int s) -> double & { return FS ? Y[w * NS + s] : Y[s * W + w]; };
+  // the stencil of the cell at Y index sc: yd[] for differences and linear
+  // combinations, yn[] for magnitudes (the same values in FP64; in FP32 the
+  // offsets from the cell's own value and the values)
+  auto stencil = [&](int sc, T *yd, T *yn, double &yc) {
+    yc = aty(sc);
+#pragma unroll
+    for (int q = 0; q < 5; q++) {
+      const double yq = aty(sc - 2 + q);
+      if constexpr (sizeof(T) == 4) {
+        yd[q] = (T)(yq - yc);
+        yn[q] = (T)yq;
+      } else {
+        yd[q] = yq;
+        yn[q] = yq;
+      }
+    }
+  };
   __syncthreads();
   const long long zl = on ? zb[w] : 0;
 
@@ -384,19 +408,19 @@ __global__ void __launch_bounds__(W5_THREADS, MB) weno5_kernel(Dims d, Params P,
     const double *pv = pb + (long long)v * d.nz + zl;
     // Y: the line of primitive v
     if (on)
-      for (int s = r; s < NS; s += TL) at(Y, NS, s) = (T)__ldg(pv + (long long)(c0 - 5 + s) * o);
+      for (int s = r; s < NS; s += TL) aty(s) = __ldg(pv + (long long)(c0 - 5 + s) * o);
     __syncthreads();
     // A: cusp test, SMONO indicator, unoptimised weights of cells -3..nv+2
     if (on)
       for (int s = r; s < NA; s += TL) {
-        T ya[5];
-#pragma unroll
-        for (int q = 0; q < 5; q++) ya[q] = at(Y, NS, s + q);
-        const T *y = ya + 2;
-        const bool c = w5::cusp(y);
-        const T m0 = c ? T(0.0) : w5::mono(y);
+        T ya[5], yb[5];
+        double yc;
+        stencil(s + 2, ya, yb, yc);
+        const T *y = ya + 2, *yn = yb + 2;
+        const bool c = w5::cusp(y, yn);
+        const T m0 = c ? T(0.0) : w5::mono(y, yn);
         T wt[3];
-        w5::unopt3(m0, y, wt);
+        w5::unopt3(m0, y, yn, wt);
         at(CODE, NA, s) = c ? T(-1.0) : m0;
         at(W0, NA, s) = wt[0];
         at(W1, NA, s) = wt[1];
@@ -422,15 +446,20 @@ __global__ void __launch_bounds__(W5_THREADS, MB) weno5_kernel(Dims d, Params P,
         const int a = s + 3;
         const T c0v = at(CODE, NA, a);
         const T wc[3] = {at(W0, NA, a), at(W1, NA, a), at(W2, NA, a)};
-        T ya[5];
-#pragma unroll
-        for (int q = 0; q < 5; q++) ya[q] = at(Y, NS, s + 3 + q);
+        T ya[5], yb[5];
+        double yc;
+        stencil(s + 5, ya, yb, yc);
         const bool cu = (c0v == T(-1.0));
         T yl, yr;
-        w5::faces(ya + 2, cu ? T(0.0) : c0v, cu, wc, lof, &yl, &yr);
+        w5::faces(ya + 2, yb + 2, cu ? T(0.0) : c0v, cu, wc, lof, &yl, &yr);
         const long long z = zl + (long long)(c0 + s) * o + (long long)v * d.nz;
-        pL[z] = yl;
-        pR[z] = yr;
+        if constexpr (sizeof(T) == 4) {
+          pL[z] = yc + (double)yl;
+          pR[z] = yc + (double)yr;
+        } else {
+          pL[z] = yl;
+          pR[z] = yr;
+        }
       }
     __syncthreads();
   }
@@ -438,12 +467,13 @@ __global__ void __launch_bounds__(W5_THREADS, MB) weno5_kernel(Dims d, Params P,
 
 // ---------------------------------------------------------------------------
 // face flux kernel (one per direction); RECON 0: MC-type slopes in the
-// kernel, RECON 1: Riemann states from the WENO5 face values pL/pR
+// kernel, RECON 1: Riemann states from the WENO5 face values pL/pR (stored
+// as TR), RECON 2: PARA
 // ---------------------------------------------------------------------------
-template <int DIR, int RECON, typename T, int MB = MinBlocks<T>::flux>
+template <int DIR, int RECON, typename T, int MB = MinBlocks<T>::flux, typename TR = T>
 __global__ void __launch_bounds__(128, MB) flux_kernel(Dims d, Params P, Box box,
                                                                  const double *__restrict__ pb,
-                                                                 const T *__restrict__ pL, const T *__restrict__ pR,
+                                                                 const TR *__restrict__ pL, const TR *__restrict__ pR,
                                                                  const double *__restrict__ G, double *__restrict__ F,
                                                                  Scalars *sc) {
   long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -459,8 +489,8 @@ __global__ void __launch_bounds__(128, MB) flux_kernel(Dims d, Params P, Box box
       // getp2interplr (flux.c:788-808), line-type branch
 #pragma unroll
       for (int v = 0; v < NPR; v++) {
-        p_l[v] = __ldg(pR + (long long)v * d.nz + z - o);
-        p_r[v] = __ldg(pL + (long long)v * d.nz + z);
+        p_l[v] = (T)__ldg(pR + (long long)v * d.nz + z - o);
+        p_r[v] = (T)__ldg(pL + (long long)v * d.nz + z);
       }
     } else if (RECON == 2) {
       // PARA: pright of the cell on the left, pleft of the cell on the right

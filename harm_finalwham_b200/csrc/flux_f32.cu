@@ -11,12 +11,10 @@ namespace hg {
 
 #define HG_F32_INSTANCES(DIR)                                                                                      \
   template __global__ void weno5_kernel<DIR, true, float>(Dims, Params, W5Tile, const double *, const float *,    \
-                                                          float *, float *);                                        \
+                                                          double *, double *);                                      \
   template __global__ void weno5_kernel<DIR, false, float>(Dims, Params, W5Tile, const double *, const float *,   \
-                                                           float *, float *);                                       \
+                                                           double *, double *);                                     \
   template __global__ void flux_kernel<DIR, 0, float>(Dims, Params, Box, const double *, const float *,           \
-                                                      const float *, const double *, double *, Scalars *);          \
-  template __global__ void flux_kernel<DIR, 1, float>(Dims, Params, Box, const double *, const float *,           \
                                                       const float *, const double *, double *, Scalars *);          \
   template __global__ void flux_kernel<DIR, 2, float>(Dims, Params, Box, const double *, const float *,           \
                                                       const float *, const double *, double *, Scalars *);

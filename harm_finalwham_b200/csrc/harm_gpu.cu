@@ -35,6 +35,7 @@
 
 #include <mutex>
 #include <new>
+#include <utility>
 #include <vector>
 
 #include "common.cuh"
@@ -49,12 +50,10 @@ using namespace hg;
 namespace hg {
 #define HG_F32_EXTERN(DIR)                                                                                         \
   extern template __global__ void weno5_kernel<DIR, true, float>(Dims, Params, W5Tile, const double *,            \
-                                                                 const float *, float *, float *);                \
+                                                                 const float *, double *, double *);              \
   extern template __global__ void weno5_kernel<DIR, false, float>(Dims, Params, W5Tile, const double *,           \
-                                                                  const float *, float *, float *);               \
+                                                                  const float *, double *, double *);             \
   extern template __global__ void flux_kernel<DIR, 0, float>(Dims, Params, Box, const double *, const float *,    \
-                                                             const float *, const double *, double *, Scalars *);   \
-  extern template __global__ void flux_kernel<DIR, 1, float>(Dims, Params, Box, const double *, const float *,    \
                                                              const float *, const double *, double *, Scalars *);   \
   extern template __global__ void flux_kernel<DIR, 2, float>(Dims, Params, Box, const double *, const float *,    \
                                                              const float *, const double *, double *, Scalars *);
@@ -1076,62 +1075,88 @@ inline unsigned grid_for(long long n, int block) { return (unsigned)((n + block 
 // sized to fit, for FP64 elements)
 constexpr size_t W5_SMEM_MAX = 72 * 1024;
 
-// Cost of a WENO5 tiling in thread rounds (256-thread sweeps over a stage's
-// items), weighted by each stage's work per item: D (state, dP/P) once, then
-// per primitive A (SMONO + weights), R (ratios), F (face values).
-double w5_cost(int nout, long long nlines, int lb, int w) {
+// Cost of a WENO5 tiling in block rounds (a stage's items over the 256
+// threads, whole rounds), weighted by each stage's work per item, plus the
+// barriers: S (shock factor) once, then per primitive Y (line loads), A
+// (SMONO + weights), R (ratios), F (face values) and four barriers.
+double w5_cost(int nout, long long nlines, int lb, int w, bool fs) {
   const int nseg = (nout + lb - 1) / lb;
   const long long ntile = (nlines + w - 1) / w;
+  const int tl = W5_THREADS / w;
+  auto rounds = [&](int n) {
+    return fs ? (double)((n + tl - 1) / tl) : (double)(((long long)n * w + W5_THREADS - 1) / W5_THREADS);
+  };
   double per = 0.0;
   for (int sgi = 0; sgi < 2; sgi++) {
     const int nv = sgi == 0 ? lb : nout - (nseg - 1) * lb;  // full tiles, then the last one
     const double count = sgi == 0 ? (double)(nseg - 1) : 1.0;
-    auto rounds = [&](int n) { return (double)((n * (long long)w + W5_THREADS - 1) / W5_THREADS); };
-    per += count * (3.0 * rounds(nv + 2) + 8.0 * (2.0 * rounds(nv + 6) + 0.3 * rounds(nv + 2) + 1.5 * rounds(nv)));
+    per += count * (rounds(nv) +
+                    8.0 * (0.3 * rounds(nv + 10) + 2.0 * rounds(nv + 6) + 0.3 * rounds(nv + 2) + 1.5 * rounds(nv) + 2.0));
   }
   return per * (double)ntile;
 }
 
-// WENO5 tiling of the output box b along direction dir: lines whose cells
-// are contiguous in memory (x3, or any direction of a domain flat across
-// it) are walked along by consecutive threads, the others across
-// (consecutive threads on neighbouring lines, x3 fastest); the tile length
-// and line count are chosen by w5_cost within the shared-memory budget.
-W5Tile w5_tiling(const Dims &d, const Box &b, int dir) {
-  W5Tile t;
-  t.box = b;
+// WENO5 tilings of the output box b along direction dir, best first (at
+// most `max` of them, one per line count).  Lines whose cells are contiguous
+// in memory (x3, or any direction of a domain flat across it) are walked
+// along by consecutive threads, a warp or more per line; the others across,
+// consecutive threads on neighbouring lines (x3 fastest), at least 8 of them
+// for 64-byte rows.  Every tiling fits the shared-memory budget.
+int w5_candidates(const Dims &d, const Box &b, int dir, W5Tile *out, int max) {
   const int nout = dir == 1 ? b.ni : (dir == 2 ? b.nj : b.nk);
   const long long nlines = dir == 1 ? (long long)b.nj * b.nk : (dir == 2 ? (long long)b.ni * b.nk : (long long)b.ni * b.nj);
   const long long stride = dir == 1 ? (long long)d.nt2 * d.nt3 : (dir == 2 ? (long long)d.nt3 : 1LL);
-  t.nlines = (int)nlines;
-  t.fast_s = stride == 1;
-  const long long cap = (long long)(W5_SMEM_MAX / sizeof(double));
-  double best = -1.0;
-  t.lb = 1;
-  t.w = 1;
+  const bool fs = stride == 1;
+  double cost[6];
+  W5Tile cand[6];
+  int n = 0;
   const int ws[] = {1, 2, 4, 8, 16, 32};
   for (int w : ws) {
     if (w > nlines && w > 1) break;
-    // coalescing across lines wants at least 8 neighbouring lines (64 B rows)
-    if (!t.fast_s && w < 8 && nlines >= 8) continue;
+    if (!fs && w < 8 && nlines >= 8) continue;
+    if (fs && w > 8 && nout >= 32) continue;
+    double best = -1.0;
+    int blb = 0;
     for (int nseg = 1; nseg <= nout; nseg++) {
       const int lb = (nout + nseg - 1) / nseg;
-      if (w5_smem_elems(lb, w) > cap) continue;
+      if (w5_smem_bytes(lb, w, 8) > (long long)W5_SMEM_MAX) continue;
       if (lb < 8 && nseg > 1) break;
-      const double c = w5_cost(nout, nlines, lb, w);
+      const double c = w5_cost(nout, nlines, lb, w, fs);
       if (best < 0.0 || c < best) {
         best = c;
-        t.lb = lb;
-        t.w = w;
+        blb = lb;
       }
       if (nseg > 64 && lb < 256) break;
     }
+    if (blb == 0) continue;
+    W5Tile t;
+    t.box = b;
+    t.nlines = (int)nlines;
+    t.fast_s = fs;
+    t.lb = blb;
+    t.w = w;
+    t.nseg = (nout + blb - 1) / blb;
+    t.ntile = (int)((nlines + w - 1) / w);
+    t.wshift = 0;
+    while ((1 << t.wshift) < w) t.wshift++;
+    cost[n] = best;
+    cand[n++] = t;
   }
-  t.nseg = (nout + t.lb - 1) / t.lb;
-  t.ntile = (int)((nlines + t.w - 1) / t.w);
-  t.wshift = 0;
-  while ((1 << t.wshift) < t.w) t.wshift++;
-  return t;
+  // best first
+  for (int i = 1; i < n; i++)
+    for (int j = i; j > 0 && cost[j] < cost[j - 1]; j--) {
+      std::swap(cost[j], cost[j - 1]);
+      std::swap(cand[j], cand[j - 1]);
+    }
+  if (n > max) n = max;
+  for (int i = 0; i < n; i++) out[i] = cand[i];
+  return n;
+}
+
+W5Tile w5_tiling(const Dims &d, const Box &b, int dir) {
+  W5Tile t[1];
+  w5_candidates(d, b, dir, t, 1);
+  return t[0];
 }
 
 // the WENO5 kernels may use up to W5_SMEM_MAX of dynamic shared memory
@@ -1653,66 +1678,101 @@ int hgpu_download_state(hgpu_ctx *x, double *p, int *pflag, double *t, double *d
 
 // one stage: fluxes, EMFs, update, bound, post_fixup, bound
 extern "C++" {
-// one direction's reconstruction + flux launches; FMB / BMB: resident
-// blocks per SM asked of the flux and WENO5 kernels (autotuned variants)
-template <int DIR, typename T, int FMB, int BMB>
+// one direction's reconstruction + flux launches.  TW: arithmetic of the
+// WENO5 reconstruction, TF: of the Riemann kernel (the MC/PARA
+// reconstruction happens inside it); FMB / BMB: resident blocks per SM asked
+// of the flux and WENO5 kernels (autotuned variants)
+// the WENO5 reconstruction of one direction with the context's tiling
+template <int DIR, typename TW, int BMB>
+static void launch_w5(hgpu_ctx *x, const double *pb) {
+  const Dims &d = x->d;
+  const Params &P = x->P;
+  const W5Tile &tl = x->w5[DIR];
+  const size_t smem = (size_t)w5_smem_bytes(tl.lb, tl.w, (int)sizeof(TW));
+  const TW *PU = (const TW *)x->w5pu;
+  double *pL = x->pL, *pR = x->pR;
+  ProfScope ps__(x, K_WENO5);
+  const unsigned grid = (unsigned)tl.nseg * tl.ntile;
+  if constexpr (DIR == 3) {
+    weno5_kernel<3, true, TW, BMB><<<grid, W5_THREADS, smem, x->stream>>>(d, P, tl, pb, PU, pL, pR);
+  } else {
+    if (tl.fast_s)
+      weno5_kernel<DIR, true, TW, BMB><<<grid, W5_THREADS, smem, x->stream>>>(d, P, tl, pb, PU, pL, pR);
+    else
+      weno5_kernel<DIR, false, TW, BMB><<<grid, W5_THREADS, smem, x->stream>>>(d, P, tl, pb, PU, pL, pR);
+  }
+}
+
+template <int DIR, typename TW, typename TF, int FMB, int BMB>
 static void launch_dir(hgpu_ctx *x, const double *pb) {
   const Dims &d = x->d;
   const Params &P = x->P;
-  T *pL = (T *)x->pL, *pR = (T *)x->pR;
-  const T *PU = (const T *)x->w5pu;
   const int kid = (DIR == 1) ? K_FLUX1 : ((DIR == 2) ? K_FLUX2 : K_FLUX3);
   unsigned gf = grid_for(x->face_box[DIR].size(), 128);
   if (P.lim == HGPU_LIM_WENO5) {
-    const W5Tile &tl = x->w5[DIR];
-    const size_t smem = sizeof(T) * (size_t)w5_smem_elems(tl.lb, tl.w);
-    {
-      ProfScope ps__(x, K_WENO5);
-      const unsigned grid = (unsigned)tl.nseg * tl.ntile;
-      if constexpr (DIR == 3) {
-        weno5_kernel<3, true, T, BMB><<<grid, W5_THREADS, smem, x->stream>>>(d, P, tl, pb, PU, pL, pR);
-      } else {
-        if (tl.fast_s)
-          weno5_kernel<DIR, true, T, BMB><<<grid, W5_THREADS, smem, x->stream>>>(d, P, tl, pb, PU, pL, pR);
-        else
-          weno5_kernel<DIR, false, T, BMB><<<grid, W5_THREADS, smem, x->stream>>>(d, P, tl, pb, PU, pL, pR);
-      }
-    }
-    LAUNCH(x, kid, (flux_kernel<DIR, 1, T, FMB>), gf, 128, d, P, x->face_box[DIR], pb, pL, pR, x->G, x->F[DIR], x->sc);
+    launch_w5<DIR, TW, BMB>(x, pb);
+    LAUNCH(x, kid, (flux_kernel<DIR, 1, TF, FMB, double>), gf, 128, d, P, x->face_box[DIR], pb, x->pL, x->pR, x->G,
+           x->F[DIR], x->sc);
   } else if (P.lim == HGPU_LIM_PARA) {
-    LAUNCH(x, kid, (flux_kernel<DIR, 2, T, FMB>), gf, 128, d, P, x->face_box[DIR], pb, nullptr, nullptr, x->G,
+    LAUNCH(x, kid, (flux_kernel<DIR, 2, TF, FMB, TF>), gf, 128, d, P, x->face_box[DIR], pb, nullptr, nullptr, x->G,
            x->F[DIR], x->sc);
   } else {
-    LAUNCH(x, kid, (flux_kernel<DIR, 0, T, FMB>), gf, 128, d, P, x->face_box[DIR], pb, nullptr, nullptr, x->G,
+    LAUNCH(x, kid, (flux_kernel<DIR, 0, TF, FMB, TF>), gf, 128, d, P, x->face_box[DIR], pb, nullptr, nullptr, x->G,
            x->F[DIR], x->sc);
   }
 }
 
-template <typename T, int FMB, int BMB>
+template <typename TW, typename TF, int FMB, int BMB>
 static void launch_fluxes_t(hgpu_ctx *x, const double *pb) {
   const Dims &d = x->d;
   if (x->P.lim == HGPU_LIM_WENO5)
-    LAUNCH(x, K_W5STATE, w5_state_kernel<T>, grid_for(x->w5_state_box.size(), 128), 128, d, x->P, x->w5_state_box, pb,
-           x->G, (T *)x->w5pu);
-  if (d.n1 > 1) launch_dir<1, T, FMB, BMB>(x, pb);
-  if (d.n2 > 1) launch_dir<2, T, FMB, BMB>(x, pb);
-  if (d.n3 > 1) launch_dir<3, T, FMB, BMB>(x, pb);
+    LAUNCH(x, K_W5STATE, w5_state_kernel<TW>, grid_for(x->w5_state_box.size(), 128), 128, d, x->P, x->w5_state_box,
+           pb, x->G, (TW *)x->w5pu);
+  if (d.n1 > 1) launch_dir<1, TW, TF, FMB, BMB>(x, pb);
+  if (d.n2 > 1) launch_dir<2, TW, TF, FMB, BMB>(x, pb);
+  if (d.n3 > 1) launch_dir<3, TW, TF, FMB, BMB>(x, pb);
+}
+// the WENO5 state pieces and one direction's reconstruction with the
+// context's precision and WENO5 variant (for timing tilings)
+template <int DIR>
+static void launch_w5_any(hgpu_ctx *x, const double *pb, bool state) {
+  const Dims &d = x->d;
+  if (x->cfg.precision == HGPU_PREC_MIXED) {
+    if (state)
+      w5_state_kernel<float><<<grid_for(x->w5_state_box.size(), 128), 128, 0, x->stream>>>(d, x->P, x->w5_state_box,
+                                                                                          pb, x->G, (float *)x->w5pu);
+    launch_w5<DIR, float, MinBlocks<float>::weno>(x, pb);
+  } else {
+    if (state)
+      w5_state_kernel<double><<<grid_for(x->w5_state_box.size(), 128), 128, 0, x->stream>>>(d, x->P, x->w5_state_box,
+                                                                                           pb, x->G, x->w5pu);
+    if (x->tune.weno == 0) launch_w5<DIR, double, kWenoMB[0]>(x, pb);
+    else launch_w5<DIR, double, kWenoMB[1]>(x, pb);
+  }
 }
 }  // extern "C++"
 
-// fluxcalc + the EMFs of flux_ct.  HGPU_PREC_MIXED runs reconstruction, wave
-// speeds and the Riemann flux in FP32; the fluxes are stored in FP64 and
-// everything after them (flux-CT, update, inversion) stays FP64.
+// fluxcalc + the EMFs of flux_ct.  HGPU_PREC_MIXED runs the WENO5
+// reconstruction in FP32 (on differences from each cell's value, face values
+// returned in FP64) and the Riemann kernel in FP64: in a torus near
+// equilibrium the flux divergence cancels most of each face flux, so FP32
+// rounding of the fluxes themselves would dominate the error.  With MC/PARA,
+// whose reconstruction runs inside the Riemann kernel, that kernel runs in
+// FP32.  The fluxes are stored in FP64 and everything after them (flux-CT,
+// update, inversion) stays FP64.
 static void launch_fluxes(hgpu_ctx *x, const double *pb) {
   const Dims &d = x->d;
+  const int fv = x->tune.flux, bv = x->tune.weno;
   if (x->cfg.precision == HGPU_PREC_MIXED) {
-    launch_fluxes_t<float, MinBlocks<float>::flux, MinBlocks<float>::weno>(x, pb);
+    constexpr int WMB = MinBlocks<float>::weno;
+    if (x->P.lim != HGPU_LIM_WENO5) launch_fluxes_t<float, float, MinBlocks<float>::flux, WMB>(x, pb);
+    else if (fv == 0) launch_fluxes_t<float, double, kFluxMB[0], WMB>(x, pb);
+    else launch_fluxes_t<float, double, kFluxMB[1], WMB>(x, pb);
   } else {
-    const int fv = x->tune.flux, bv = x->tune.weno;
-    if (fv == 0 && bv == 0) launch_fluxes_t<double, kFluxMB[0], kWenoMB[0]>(x, pb);
-    else if (fv == 0) launch_fluxes_t<double, kFluxMB[0], kWenoMB[1]>(x, pb);
-    else if (bv == 0) launch_fluxes_t<double, kFluxMB[1], kWenoMB[0]>(x, pb);
-    else launch_fluxes_t<double, kFluxMB[1], kWenoMB[1]>(x, pb);
+    if (fv == 0 && bv == 0) launch_fluxes_t<double, double, kFluxMB[0], kWenoMB[0]>(x, pb);
+    else if (fv == 0) launch_fluxes_t<double, double, kFluxMB[0], kWenoMB[1]>(x, pb);
+    else if (bv == 0) launch_fluxes_t<double, double, kFluxMB[1], kWenoMB[0]>(x, pb);
+    else launch_fluxes_t<double, double, kFluxMB[1], kWenoMB[1]>(x, pb);
   }
   LAUNCH(x, K_EMF, emf_kernel, grid_for(x->emf_box.size(), 256), 256, d, x->emf_box, x->F[1], x->F[2], x->F[3], x->G,
          x->E);
@@ -2279,7 +2339,9 @@ int hgpu_autotune(hgpu_ctx *x, hgpu_tuning *out) {
   };
   const bool fp64 = x->cfg.precision == HGPU_PREC_FP64;
   int *knob[4] = {&x->tune.flux, &x->tune.weno, &x->tune.conserve, &x->tune.invert};
-  const bool applies[4] = {fp64, fp64 && x->P.lim == HGPU_LIM_WENO5, true, true};
+  // the mixed-precision path runs the FP64 Riemann kernel after a WENO5
+  // reconstruction (its FP32 kernels have fixed variants)
+  const bool applies[4] = {fp64 || x->P.lim == HGPU_LIM_WENO5, fp64 && x->P.lim == HGPU_LIM_WENO5, true, true};
   const int kids[4][3] = {{K_FLUX1, K_FLUX2, K_FLUX3}, {K_WENO5, -1, -1}, {K_UPDATE, -1, -1}, {K_INVERT, -1, -1}};
   float ms[4][2] = {{0.f, 0.f}, {0.f, 0.f}, {0.f, 0.f}, {0.f, 0.f}};
   int rc = HGPU_OK;
@@ -2310,6 +2372,55 @@ int hgpu_autotune(hgpu_ctx *x, hgpu_tuning *out) {
   }
   x->profiling = false;
   restore();
+  // WENO5 tile shapes: per direction, the candidates of the cost model timed
+  // on the current state (the face values are scratch: nothing else changes)
+  float tile_ms[4] = {0.f, 0.f, 0.f, 0.f};
+  if (!rc && x->P.lim == HGPU_LIM_WENO5) {
+    const Dims &d = x->d;
+    const int nd[4] = {0, d.n1, d.n2, d.n3};
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    for (int dir = 1; dir <= 3 && !rc; dir++) {
+      if (nd[dir] <= 1) continue;
+      W5Tile cand[4];
+      const int nc = w5_candidates(d, x->w5[dir].box, dir, cand, 4);
+      float best = -1.f;
+      W5Tile bt = x->w5[dir];
+      for (int c = 0; c < nc; c++) {
+        x->w5[dir] = cand[c];
+        auto go = [&](bool state) {
+          if (dir == 1) launch_w5_any<1>(x, x->p, state);
+          else if (dir == 2) launch_w5_any<2>(x, x->p, state);
+          else launch_w5_any<3>(x, x->p, state);
+        };
+        go(true);  // warm-up, with the state pieces
+        cudaEventRecord(e0, x->stream);
+        go(false);
+        go(false);
+        cudaEventRecord(e1, x->stream);
+        if (cudaEventSynchronize(e1) != cudaSuccess || cudaGetLastError() != cudaSuccess) {
+          rc = HGPU_E_CUDA;
+          break;
+        }
+        float t = 0.f;
+        cudaEventElapsedTime(&t, e0, e1);
+        t *= 0.5f;
+        if (best < 0.f || t < best) {
+          best = t;
+          bt = cand[c];
+        }
+      }
+      x->w5[dir] = bt;
+      tile_ms[dir] = best;
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    for (int k = 0; k < K_NKERNELS; k++) {
+      x->kms[k] = 0.0;
+      x->kcount[k] = 0;
+    }
+  }
   cudaFreeAsync(sp, x->stream);
   cudaFreeAsync(sf, x->stream);
   cudaFreeAsync(ss, x->stream);
@@ -2326,6 +2437,12 @@ int hgpu_autotune(hgpu_ctx *x, hgpu_tuning *out) {
     out->weno_minb = kWenoMB[x->tune.weno];
     out->update_minb = kConserveMB[x->tune.conserve];
     out->invert_minb = kInvertMB[x->tune.invert];
+    for (int q = 0; q < 4; q++) {
+      const bool on = q >= 1 && x->P.lim == HGPU_LIM_WENO5;
+      out->weno_lb[q] = on ? x->w5[q].lb : 0;
+      out->weno_lines[q] = on ? x->w5[q].w : 0;
+      out->weno_tile_ms[q] = tile_ms[q];
+    }
     for (int v = 0; v < 2; v++) {
       out->flux_ms[v] = ms[0][v];
       out->weno_ms[v] = ms[1][v];
@@ -2347,7 +2464,27 @@ int hgpu_set_tuning(hgpu_ctx *x, const hgpu_tuning *t) {
   const int f = pick(kFluxMB, t->flux_minb), b = pick(kWenoMB, t->weno_minb);
   const int u = pick(kConserveMB, t->update_minb), v = pick(kInvertMB, t->invert_minb);
   if (f < 0 || b < 0 || u < 0 || v < 0) return HGPU_E_INVALID;
+  // WENO5 tilings (0: keep the current one)
+  W5Tile w5[4];
+  for (int q = 1; q <= 3; q++) {
+    w5[q] = x->w5[q];
+    const int lb = t->weno_lb[q], w = t->weno_lines[q];
+    if (lb <= 0 || x->P.lim != HGPU_LIM_WENO5) continue;
+    const Box &bx = x->w5[q].box;
+    const int nout = q == 1 ? bx.ni : (q == 2 ? bx.nj : bx.nk);
+    if (w < 1 || w > 32 || (w & (w - 1)) || lb > nout || w5_smem_bytes(lb, w, 8) > (long long)W5_SMEM_MAX) {
+      set_err("hgpu_set_tuning: invalid WENO5 tiling");
+      return HGPU_E_INVALID;
+    }
+    w5[q].lb = lb;
+    w5[q].w = w;
+    w5[q].nseg = (nout + lb - 1) / lb;
+    w5[q].ntile = (w5[q].nlines + w - 1) / w;
+    w5[q].wshift = 0;
+    while ((1 << w5[q].wshift) < w) w5[q].wshift++;
+  }
   CUDA_TRY(cudaStreamSynchronize(x->stream));
+  for (int q = 1; q <= 3; q++) x->w5[q] = w5[q];
   x->tune.flux = f;
   x->tune.weno = b;
   x->tune.conserve = u;

@@ -26,10 +26,12 @@ namespace hg {
 namespace w5 {
 
 // Constants of the scheme per arithmetic type.  FP64: the reference's own.
-// FP32 (mixed precision path): the epsilons are raised so that they stay
-// above FP32 round-off and (eps)^2 stays a normal number; DBL_MIN becomes
-// FLT_MIN.  The FP32 path is not bit-compatible with the reference; its error
-// against the FP64 path is measured and stated instead.
+// FP32 (mixed-precision path): the same WENO and SMONO epsilons -- the FP32
+// path reconstructs on differences from the cell's own value (exact zeros
+// where the line is flat, as in FP64) and forms the nonlinear weights from
+// ratios to the smallest smoothness term (no 1/eps^2 overflow); BIG, SMALL
+// and DBL_MIN become FP32-range values.  The FP32 path is not bit-compatible
+// with the reference; its error against the FP64 path is measured and stated.
 template <typename T> struct K;
 template <> struct K<double> {
   static constexpr double eps = 1.e-26;       // WENO_EPSILON = REDUCEEPSILON (reconstructeno.h:195-200)
@@ -39,8 +41,8 @@ template <> struct K<double> {
   static constexpr double tiny = 2.2250738585072014e-308;  // DBL_MIN
 };
 template <> struct K<float> {
-  static constexpr float eps = 1.e-12f;
-  static constexpr float smono = 1.e-5f;
+  static constexpr float eps = 1.e-26f;
+  static constexpr float smono = 1.e-13f;
   static constexpr float big = 1.e+30f;
   static constexpr float small = 1.e-30f;
   static constexpr float tiny = 1.17549435e-38f;  // FLT_MIN
@@ -107,12 +109,20 @@ __device__ __forceinline__ double div12<double>(double x) {
   return fma(e, r, q);
 }
 
-// check_for_cusp_new (smonointerp.c:439-476); y points at the cell (y[-2..2] valid)
+// The routines below take the line at the cell twice: y (y[-2..2] valid)
+// for every difference and linear combination, and yn for the magnitudes
+// that scale the epsilons.  The FP64 path passes the primitives as both; the
+// FP32 path passes y[k] = y_k - y_0 (formed in FP64) and the primitives as
+// yn, and adds y_0 back to the face values in FP64.  The stencil formulas
+// used on y are differences or rows summing to one, so both forms agree in
+// exact arithmetic.
+
+// check_for_cusp_new (smonointerp.c:439-476)
 template <typename T>
-__device__ __forceinline__ bool cusp(const T *y) {
+__device__ __forceinline__ bool cusp(const T *y, const T *yn) {
   T df_m1 = y[-1] - y[-2], df0 = y[0] - y[-1], df1 = y[1] - y[0], df2 = y[2] - y[1];
   T ddf_m1 = df0 - df_m1, ddf0 = df1 - df0, ddf1 = df2 - df1;
-  T norm = (fabs(y[-2]) + fabs(y[-1]) + fabs(y[0]) + fabs(y[1]) + fabs(y[2]) + K<T>::small);
+  T norm = (fabs(yn[-2]) + fabs(yn[-1]) + fabs(yn[0]) + fabs(yn[1]) + fabs(yn[2]) + K<T>::small);
   norm = norm * K<T>::smono;
   T s0 = sgn(df0);
   T f1a = fabs(df0) - norm;
@@ -137,7 +147,7 @@ __device__ __forceinline__ bool cusp(const T *y) {
 
 // compute_mono_indicator_point_eno5 (smonointerp.c:296-425) + transition_function (:428-437)
 template <typename T>
-__device__ __forceinline__ T mono(const T *y) {
+__device__ __forceinline__ T mono(const T *y, const T *yn) {
   // (division by 2 is the exact multiplication by 1/2)
   T l1 = div12((((-3 * y[-2] + y[2]) + (-10 * y[-1] - 6 * y[1])) + 18 * y[0]));
   T l2 = div12((((11 * y[-2] - y[2]) + (-20 * y[-1] + 4 * y[1])) + 6 * y[0]));
@@ -151,7 +161,7 @@ __device__ __forceinline__ T mono(const T *y) {
   minabs = wmin(minabs, fabs(minmod(l1, r1)));
   minabs = wmin(minabs, fabs(minmod(l2, r2)));
   minabs = wmin(minabs, fabs(minmod(l3, r3)));
-  T norm = fabs(y[0]) + ((fabs(y[-1]) + fabs(y[1])) + (fabs(y[-2]) + fabs(y[2])));
+  T norm = fabs(yn[0]) + ((fabs(yn[-1]) + fabs(yn[1])) + (fabs(yn[-2]) + fabs(yn[2])));
   T cut = norm * K<T>::smono + K<T>::tiny;
   T v = (minabs - T(0.0)) / (cut - T(0.0));
   return wmax(T(0.), wmin(T(1.), v));
@@ -184,7 +194,7 @@ __device__ __forceinline__ T eno5(bool right, const T *y) {
 // by mono_adjust_unoptimized_weights (:702-728).  m0 is monoindicator[0]
 // (0 at a cusp); the cusp's lower_order_fraction=1 is kept by the caller.
 template <typename T>
-__device__ __forceinline__ void unopt3(T m0, const T *u, T w[3]) {
+__device__ __forceinline__ void unopt3(T m0, const T *u, const T *un, T w[3]) {
   if (m0 == 1) {
     w[0] = w[1] = w[2] = T(1.0) / 3;
     return;
@@ -198,7 +208,7 @@ __device__ __forceinline__ void unopt3(T m0, const T *u, T w[3]) {
   T si0 = T(13.) / T(12.) * sd0 * sd0 + T(1.) / T(4.) * fd0 * fd0;
   T si1 = T(13.) / T(12.) * sd1 * sd1 + T(1.) / T(4.) * fd1 * fd1;
   T si2 = T(13.) / T(12.) * sd2 * sd2 + T(1.) / T(4.) * fd2 * fd2;
-  T u2[5] = {u[-2] * u[-2], u[-1] * u[-1], u[0] * u[0], u[1] * u[1], u[2] * u[2]};
+  T u2[5] = {un[-2] * un[-2], un[-1] * un[-1], un[0] * un[0], un[1] * un[1], un[2] * un[2]};
   T e = sum5(u2) * K<T>::eps;
   si0 += e;
   si1 += e;
@@ -208,12 +218,23 @@ __device__ __forceinline__ void unopt3(T m0, const T *u, T w[3]) {
   si1 /= (s + K<T>::tiny);
   si2 /= (s + K<T>::tiny);
   T t0 = si0 + K<T>::eps / T(1.), t1 = si1 + K<T>::eps / T(1.), t2 = si2 + K<T>::eps / T(1.);
-  t0 *= t0;
-  t1 *= t1;
-  t2 *= t2;
-  w[0] = T(1.) / t0;
-  w[1] = T(1.) / t1;
-  w[2] = T(1.) / t2;
+  if constexpr (sizeof(T) == 4) {
+    // 1/t^2 normalised, formed as (tmin/t)^2 (each in (0, 1])
+    const T tm = wmin(t0, wmin(t1, t2));
+    t0 = tm / t0;
+    t1 = tm / t1;
+    t2 = tm / t2;
+    w[0] = t0 * t0;
+    w[1] = t1 * t1;
+    w[2] = t2 * t2;
+  } else {
+    t0 *= t0;
+    t1 *= t1;
+    t2 *= t2;
+    w[0] = T(1.) / t0;
+    w[1] = T(1.) / t1;
+    w[2] = T(1.) / t2;
+  }
   s = sum3(w[0], w[1], w[2]);
   w[0] /= (s + T(0.0));
   w[1] /= (s + T(0.0));
@@ -228,7 +249,7 @@ __device__ __forceinline__ void unopt3(T m0, const T *u, T w[3]) {
 
 // order-2 unoptimised weights (compute_cf_stencil_weights with order 2)
 template <typename T>
-__device__ __forceinline__ void unopt2(T m0, const T *u, T w[2]) {
+__device__ __forceinline__ void unopt2(T m0, const T *u, const T *un, T w[2]) {
   if (m0 == 1) {
     w[0] = w[1] = T(1.0) / 2;
     return;
@@ -236,17 +257,25 @@ __device__ __forceinline__ void unopt2(T m0, const T *u, T w[2]) {
   T fd0 = u[1] - u[0];
   T fd1 = u[0] - u[-1];
   T si0 = fd0 * fd0, si1 = fd1 * fd1;
-  T e = sum3(u[-1] * u[-1], u[0] * u[0], u[1] * u[1]) * K<T>::eps;
+  T e = sum3(un[-1] * un[-1], un[0] * un[0], un[1] * un[1]) * K<T>::eps;
   si0 += e;
   si1 += e;
   T s = sum2(si0, si1);
   si0 /= (s + K<T>::tiny);
   si1 /= (s + K<T>::tiny);
   T t0 = si0 + K<T>::eps / T(1.), t1 = si1 + K<T>::eps / T(1.);
-  t0 *= t0;
-  t1 *= t1;
-  w[0] = T(1.) / t0;
-  w[1] = T(1.) / t1;
+  if constexpr (sizeof(T) == 4) {
+    const T tm = wmin(t0, t1);
+    t0 = tm / t0;
+    t1 = tm / t1;
+    w[0] = t0 * t0;
+    w[1] = t1 * t1;
+  } else {
+    t0 *= t0;
+    t1 *= t1;
+    w[0] = T(1.) / t0;
+    w[1] = T(1.) / t1;
+  }
   s = sum2(w[0], w[1]);
   w[0] /= (s + T(0.0));
   w[1] /= (s + T(0.0));
@@ -309,7 +338,7 @@ __device__ __forceinline__ T cvt2(bool right, const T *wo, const T *u) {
 // u: the line at the cell (u[-2..2]); m0: SMONO indicator (0 at a cusp);
 // is_cusp; w: unoptimised order-3 weights; lof: final lower-order fraction.
 template <typename T>
-__device__ __forceinline__ void faces(const T *u, T m0, bool is_cusp, const T w[3], T lof,
+__device__ __forceinline__ void faces(const T *u, const T *un, T m0, bool is_cusp, const T w[3], T lof,
                                       T *yl, T *yr) {
   // optimised order-3 weights, left face then right face (c2e_optimal_weights_*face[1])
   T wl[3], wr[3];
@@ -338,7 +367,7 @@ __device__ __forceinline__ void faces(const T *u, T m0, bool is_cusp, const T w[
     wr[1] *= f;
     wr[2] *= f;
     T w2[2];
-    unopt2(m0, u, w2);
+    unopt2(m0, u, un, w2);
     // order-2 optimised weights (c2e_optimal_weights_*face[0]), then scaled by lof
     ll[0] = w2[0] * (T(1.) / T(4.));
     ll[1] = w2[1] * (T(3.) / 4);

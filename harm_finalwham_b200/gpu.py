@@ -45,7 +45,8 @@ class hgpu_config(ctypes.Structure):
 class hgpu_tuning(ctypes.Structure):
     _fields_ = [(n, ctypes.c_int) for n in ("flux_minb", "weno_minb", "update_minb", "invert_minb")] + \
                [(n, ctypes.c_int * 2) for n in ("flux_cand", "weno_cand", "update_cand", "invert_cand")] + \
-               [(n, ctypes.c_float * 2) for n in ("flux_ms", "weno_ms", "update_ms", "invert_ms")]
+               [(n, ctypes.c_float * 2) for n in ("flux_ms", "weno_ms", "update_ms", "invert_ms")] + \
+               [("weno_lb", ctypes.c_int * 4), ("weno_lines", ctypes.c_int * 4), ("weno_tile_ms", ctypes.c_float * 4)]
 
 
 class hgpu_diag(ctypes.Structure):
@@ -301,7 +302,9 @@ class HarmGPU:
 
     def autotune(self):
         """hgpu_autotune: pick the resident-block variant of each heavy FP64
-        kernel on this state; returns {family: {"minb": chosen, "ms": {candidate: ms}}}."""
+        kernel and the WENO5 tile shape per direction on this state; returns
+        {family: {"minb": chosen, "ms": {candidate: ms}}, "weno_tiles": {dir:
+        {"lb": cells, "lines": lines, "ms": per launch}}}."""
         tu = hgpu_tuning()
         _check(self.L, self.L.hgpu_autotune(self.h, ctypes.byref(tu)))
         out = {}
@@ -309,13 +312,18 @@ class HarmGPU:
             cand = list(getattr(tu, fam + "_cand"))
             ms = list(getattr(tu, fam + "_ms"))
             out[fam] = {"minb": getattr(tu, fam + "_minb"), "ms": {str(c): round(m, 4) for c, m in zip(cand, ms)}}
+        out["weno_tiles"] = {str(q): {"lb": tu.weno_lb[q], "lines": tu.weno_lines[q],
+                                      "ms": round(tu.weno_tile_ms[q], 4)} for q in (1, 2, 3) if tu.weno_lb[q] > 0}
         return out
 
     def set_tuning(self, minb):
-        """hgpu_set_tuning: {"flux": 4, "weno": 2, "update": 3, "invert": 1} (blocks per SM)."""
+        """hgpu_set_tuning: {"flux": 4, "weno": 3, "update": 3, "invert": 1} (blocks per SM), optionally
+        "weno_tiles": {dir: (cells per tile, lines per tile)}."""
         tu = hgpu_tuning()
         tu.flux_minb, tu.weno_minb = int(minb["flux"]), int(minb["weno"])
         tu.update_minb, tu.invert_minb = int(minb["update"]), int(minb["invert"])
+        for q, (lb, lines) in (minb.get("weno_tiles") or {}).items():
+            tu.weno_lb[int(q)], tu.weno_lines[int(q)] = int(lb), int(lines)
         _check(self.L, self.L.hgpu_set_tuning(self.h, ctypes.byref(tu)))
 
     def advance_stage(self, timeorder):

@@ -33,7 +33,7 @@
 extern "C" {
 #endif
 
-#define HGPU_ABI_VERSION 8
+#define HGPU_ABI_VERSION 9
 
 /* return codes */
 #define HGPU_OK 0
@@ -216,12 +216,20 @@ int hgpu_step_graph(hgpu_ctx *ctx, int nsteps, hgpu_stats *stats);
    keeps the faster for later steps.  Results do not depend on the choice;
    the state is left as it was (for a batch context, every instance's t,
    dt, done flag and step count too).  *_ms: kernel milliseconds of one step per
-   candidate (0 where a family does not apply: weno without WENO5, flux and
-   weno in the mixed-precision mode). */
+   candidate (0 where a family does not apply: weno without WENO5; in the
+   mixed-precision mode weno, and flux unless the scheme is WENO5, whose
+   Riemann kernel stays FP64). */
 typedef struct {
   int flux_minb, weno_minb, update_minb, invert_minb;
   int flux_cand[2], weno_cand[2], update_cand[2], invert_cand[2];
   float flux_ms[2], weno_ms[2], update_ms[2], invert_ms[2];
+  /* WENO5 tile shape per direction d = 1..3 (index 0 unused): output cells
+     per tile along the direction and lines per tile (a power of two); the
+     autotuner times up to four candidate shapes of its cost model per
+     direction (weno_tile_ms: the chosen one's time per launch).  In
+     hgpu_set_tuning, 0 keeps the current shape. */
+  int weno_lb[4], weno_lines[4];
+  float weno_tile_ms[4];
 } hgpu_tuning;
 int hgpu_autotune(hgpu_ctx *ctx, hgpu_tuning *out);
 /* Apply a choice found before (the *_minb fields; each must be one of the

@@ -1,7 +1,10 @@
-"""Mixed precision (HGPU_PREC_MIXED: FP32 reconstruction, wave speeds and
-Riemann fluxes; FP64 flux-CT, conserved update and inversion) against the
-FP64 path, which is bit-identical to the reference.  The mixed path is not
-bit-compatible by design; these tests state and bound its error."""
+"""Mixed precision (HGPU_PREC_MIXED) against the FP64 path, which is
+bit-identical to the reference.  With WENO5 the reconstruction runs in FP32
+(on differences from each cell's own value, with the FP64 epsilons) and the
+Riemann fluxes in FP64; with MC/PARA the Riemann kernel, which reconstructs
+too, runs in FP32.  Flux-CT, the conserved update and the inversion stay
+FP64.  The mixed path is not bit-compatible by design; these tests state and
+bound its error."""
 import numpy as np
 import pytest
 
@@ -63,3 +66,18 @@ def test_mixed_finite_volume_default_scheme():
     assert np.all(np.isfinite(p32))
     assert rel_l1(p32[..., 0], p64[..., 0]) < 1e-4
     assert abs(t32 - t64) < 1e-4 * t64
+
+
+def test_mixed_weno5_within_1e5_of_fp64_at_scale():
+    # the precision-at-scale torus 256x128x128 (WENO5 + HLL + flux-CT), 200
+    # steps: the benchmark's bound is relative L1(rho) <= 1e-5 against FP64
+    dom = torus.fm_torus(256, 128, 128, ng=6, lim="WENO5", flux="HLL", seed=7)
+    p64, f64, t64, s64, d64 = run(dom, "fp64", 200)
+    p32, f32, t32, s32, d32 = run(dom, "mixed", 200)
+    assert s64.err == 0 and s32.err == 0
+    errs = {name: rel_l1(p32[..., q], p64[..., q]) for name, q in (("rho", 0), ("u", 1), ("B1", 5), ("B2", 6),
+                                                                     ("B3", 7))}
+    print("WENO5 mixed vs fp64 after 200 steps at 256x128x128, relative L1:",
+          {k: f"{v:.2e}" for k, v in errs.items()})
+    assert all(v <= 1e-5 for v in errs.values()), errs
+    assert d32 < 1e-12
