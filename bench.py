@@ -26,11 +26,11 @@ Our arm:
 Reference arm (--impl reference): the reference CPU build, one process per
 host core on the bounded sample, aggregate zone-updates/s.
 
-Multi-GPU: replicas (each rank advances its own torus; no data-path
-collective), weak scaling; value = all ranks' zone-updates / max time.
---decomp x3 instead splits one torus of n3 x N planes along x3 (each rank
-owns n3 planes; ghost planes exchanged over NCCL twice per stage, the ndt
-minima all-reduced once per step).
+Multi-GPU (N > 1): one torus of n3 x N planes split along x3 (each rank
+owns n3 planes, the reference's MPI decomposition with ncpux3 = N; ghost
+planes exchanged over NCCL twice per stage, the ndt minima all-reduced once
+per step), weak scaling; value = all ranks' zone-updates / max time.
+--replicas instead runs N independent tori (no data-path collective).
 """
 import argparse
 import datetime
@@ -833,7 +833,9 @@ def main():
     ap.add_argument("--kernels-only", action="store_true",
                     help="set-up, warm-up and the timed steps only (for profiler runs)")
     ap.add_argument("--decomp", default=None, choices=["x3"],
-                    help="split one torus along x3 over the ranks (NCCL halo exchange) instead of replicas")
+                    help="split one torus along x3 over the ranks (NCCL halo exchange); the default for N > 1")
+    ap.add_argument("--replicas", action="store_true",
+                    help="N > 1: independent tori per rank instead of the x3 split")
     args = ap.parse_args()
     rank, world, local = rank_info()
     if args.warmup < 3:
@@ -864,6 +866,8 @@ def main():
         return 0
 
     pin_device(local, world)
+    if world > 1 and not args.replicas and not args.decomp:
+        args.decomp = "x3"
     res = bench_decomp(args, rank, world) if args.decomp else bench_ours(args, rank, world)
     if rank == 0:
         print(json.dumps(res))

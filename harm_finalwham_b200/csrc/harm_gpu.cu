@@ -580,6 +580,45 @@ __global__ void bound_pole_kernel(Dims d, Params P, double *p) {
 }
 
 // bound_pflag_user (boundsint.c:6-266) as the same composition
+// get_bsqflags (fixup.c:1751-1849), which pre_fixup runs on the stage's
+// input state at the start of every RK stage (step_ch.c:117-120): per zone,
+// with the CENT metric, b^2/rho against BSQORHOLIMIT and b^2/u against
+// BSQOULIMIT (initbase.c:465-466), 2 above the limit, 1 above 0.9 of it,
+// else 0: the FLAGBSQORHO and FLAGBSQOU slots of pflag, packed as
+// FLAGBSQORHO | FLAGBSQOU << 2.  With LIMADJUST = FLUXADJUST = 0 they change
+// no state; the last stage's values are what the reference leaves in pflag.
+// A state whose u^t has no real solution sets ERR_UTCALC_DISCR, as the
+// reference's FAILSTATEMENT ends the step.
+constexpr double BSQORHOLIMIT = 20.0, BSQOULIMIT = 100.0;
+__global__ void bsqflags_kernel(Dims d, const double *__restrict__ pv, const double *__restrict__ G,
+                                unsigned char *__restrict__ bf, Scalars *sc) {
+  const long long z = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (z >= d.nz) return;
+  const int k = (int)(z % d.nt3) - d.g3;
+  const long long r = z / d.nt3;
+  const int j = (int)(r % d.nt2) - d.g2;
+  const int i = (int)(r / d.nt2) - d.g1;
+  double pr[NPR];
+  load_prim(pv, d, z, pr);
+  Metric m;
+  load_metric(G, d, gix(d, i, j), G_CENT, m);
+  State q;
+  if (get_state(pr, m, q)) {
+    atomicOr(&sc->err, ERR_UTCALC_DISCR);
+    bf[z] = 0;
+    return;
+  }
+  const double bsq = dot4(q.bcon, q.bcov);
+  int f0, f3;
+  if (bsq / pr[RHO] > BSQORHOLIMIT) f0 = 2;
+  else if (bsq / pr[RHO] > 0.9 * BSQORHOLIMIT) f0 = 1;
+  else f0 = 0;
+  if (bsq / pr[UU] > BSQOULIMIT) f3 = 2;
+  else if (bsq / pr[UU] > 0.9 * BSQOULIMIT) f3 = 1;
+  else f3 = 0;
+  bf[z] = (unsigned char)(f0 | (f3 << 2));
+}
+
 __global__ void bound_pflag_kernel(Dims d, Params P, int *pflag, const Scalars *sc) {
   long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   // a finished domain is frozen: its ghost flags keep the values of its last step
@@ -1233,6 +1272,7 @@ struct hgpu_ctx {
   double *staging = nullptr;  // AoS staging for uploads/downloads
   double *pL = nullptr, *pR = nullptr;  // WENO5 face values
   double *w5pu = nullptr;               // WENO5: per-zone dP/P state pieces (2 planes)
+  unsigned char *bsqf = nullptr;        // FLAGBSQORHO | FLAGBSQOU << 2 per zone
   double *progress = nullptr;                          // 4 doubles for hg_progress_async
   W5Tile w5[4];  // WENO5 tiling per direction
   Box w5_state_box;  // zones whose dP/P state pieces some direction reads
@@ -1343,7 +1383,7 @@ void hgpu_destroy(hgpu_ctx *x) {
   for (cudaEvent_t e : x->freelist) cudaEventDestroy(e);
   void *ptrs[] = {x->p, x->pk, x->uf, x->ucum, x->F[1], x->F[2], x->F[3], x->E, x->G, x->pflag, x->gammacheck,
                   x->cand, x->fixlist, x->cand_orig, x->cand_dec, x->candmap, x->fixvals, x->sc, x->staging, x->istaging,
-                  x->pL, x->pR, x->w5pu, x->cell_inst, x->inst, x->progress, x->pk1, x->ui};
+                  x->pL, x->pR, x->w5pu, x->bsqf, x->cell_inst, x->inst, x->progress, x->pk1, x->ui};
   for (void *q : ptrs)
     if (q) cudaFree(q);
   cudaStreamDestroy(x->stream);
@@ -1478,7 +1518,8 @@ int hgpu_create(const hgpu_config *cfg, hgpu_ctx **out) {
             cudaMalloc(&x->cand_dec, sizeof(int) * x->cap) == cudaSuccess &&
             cudaMalloc(&x->candmap, sizeof(int) * nz) == cudaSuccess &&
             cudaMalloc(&x->fixvals, sizeof(double) * 5 * x->cap) == cudaSuccess &&
-            cudaMalloc(&x->sc, sizeof(Scalars)) == cudaSuccess;
+            cudaMalloc(&x->sc, sizeof(Scalars)) == cudaSuccess &&
+            cudaMalloc(&x->bsqf, nz) == cudaSuccess && cudaMemset(x->bsqf, 0, nz) == cudaSuccess;
   for (int dd = 1; dd <= 3 && ok; dd++) ok = cudaMalloc(&x->F[dd], pb) == cudaSuccess;
   if (ok && cfg->timeorder >= 3) ok = cudaMalloc(&x->pk1, pb) == cudaSuccess && cudaMemset(x->pk1, 0, pb) == cudaSuccess;
   if (ok && cfg->doenoflux == HGPU_ENOFINITEVOLUME)
@@ -1849,6 +1890,9 @@ static void launch_stage_advance(hgpu_ctx *x, int timeorder) {
   double CUf0 = S.cuf[0], CUf1 = S.cuf[1], CUf2 = S.cuf[2];
   double Cn0 = S.cun[0], Cn1 = S.cun[1], Cn2 = S.cun[2];
   launch_reset(x);
+  // pre_fixup: only the last stage's flags survive the step
+  if (finalstep && !x->P.cell_inst)
+    LAUNCH(x, K_OTHER, bsqflags_kernel, grid_for(d.nz, 256), 256, d, pi, x->G, x->bsqf, x->sc);
   launch_fluxes(x, pb);
   const int fv = (x->cfg.doenoflux == HGPU_ENOFINITEVOLUME);
   double *ufv = (fv && finalstep) ? x->ucum : nullptr;
@@ -2736,6 +2780,7 @@ extern "C" size_t hgpu_context_bytes(const hgpu_config *c) {
              + sizeof(double) * 3 * nz        // corner EMFs
              + sizeof(double) * G_NCOMP * nij // geometry
              + sizeof(int) * 2 * nz           // pflag, candidate map
+             + (size_t)nz                     // b^2 flags
              + sizeof(double) * nz            // gamma check
              + cap * (2 * sizeof(long long) + 2 * sizeof(int) + 5 * sizeof(double))
              + plane;                         // staging for uploads and downloads
@@ -2785,6 +2830,19 @@ extern "C" int hgpu_upload_conserved(hgpu_ctx *x, const double *unew) {
   LAUNCH(x, K_OTHER, aos_to_soa_kernel, grid_for(nz * NPR, 256), 256, x->staging, x->ucum, nz);
   CUDA_TRY(cudaStreamSynchronize(x->stream));
   CUDA_TRY(cudaGetLastError());
+  return HGPU_OK;
+}
+
+extern "C" int hgpu_download_bsqflags(hgpu_ctx *x, int *flags) {
+  if (!x || !flags) return HGPU_E_INVALID;
+  const long long nz = x->d.nz;
+  std::vector<unsigned char> h((size_t)nz);
+  CUDA_TRY(cudaMemcpyAsync(h.data(), x->bsqf, (size_t)nz, cudaMemcpyDeviceToHost, x->stream));
+  CUDA_TRY(cudaStreamSynchronize(x->stream));
+  for (long long z = 0; z < nz; z++) {
+    flags[2 * z] = h[z] & 3;
+    flags[2 * z + 1] = (h[z] >> 2) & 3;
+  }
   return HGPU_OK;
 }
 

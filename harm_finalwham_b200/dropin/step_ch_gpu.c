@@ -29,8 +29,8 @@
  * The device keeps the ghost zones the scheme reads (MC 3, PARA 3, WENO5 6;
  * the finite-volume scheme all MAXBND: its flux and dt loops cover every
  * transverse ghost); the reference's ghost zones beyond those are left as
- * they were.  Only the failure-flag slot FLAGUTOPRIMFAIL of pflag is
- * produced.
+ * they were.  Of pflag, the slots FLAGUTOPRIMFAIL (the inversion and
+ * fixups) and FLAGBSQORHO / FLAGBSQOU (pre_fixup's b^2 flags) are produced.
  *
  * Environment:
  *   HARMGPU_PRECISION=mixed   the mixed-precision path instead of FP64
@@ -52,7 +52,7 @@ extern int set_density_floors(struct of_geom *ptrgeom, FTYPE *pr, FTYPE *prfloor
 static hgpu_ctx *g_ctx;
 static int g_ng, g_g[4], g_nt[4], g_gt[3];
 static double *g_p, *g_u;
-static int *g_pflag;
+static int *g_pflag, *g_bsq;
 static int g_resident, g_uploaded;
 
 #define CHECK(call)                                                                            \
@@ -202,6 +202,7 @@ static int setup(void)
   CHECK(hgpu_create(&cfg, &g_ctx));
   if (hgpu_alloc_pinned((size_t)nz * NPR * sizeof(double), (void **)&g_p) != HGPU_OK ||
       hgpu_alloc_pinned((size_t)nz * sizeof(int), (void **)&g_pflag) != HGPU_OK ||
+      hgpu_alloc_pinned((size_t)nz * 2 * sizeof(int), (void **)&g_bsq) != HGPU_OK ||
       (DOENOFLUX == ENOFINITEVOLUME &&
        hgpu_alloc_pinned((size_t)nz * NPR * sizeof(double), (void **)&g_u) != HGPU_OK)) {
     dualfprintf(fail_file, "step_ch_gpu: pinned host buffers: %s\n", hgpu_last_error());
@@ -236,6 +237,16 @@ int step_ch(void)
   CHECK(hgpu_download_state(g_ctx, g_p, g_pflag, &tt, &dtt));
   window(p, g_p, 1);
   flag_window(1);
+  CHECK(hgpu_download_bsqflags(g_ctx, g_bsq));
+  {
+    int i, j, k;
+    for (i = -g_g[1]; i < N1 + g_g[1]; i++)
+      for (j = -g_g[2]; j < N2 + g_g[2]; j++)
+        for (k = -g_g[3]; k < N3 + g_g[3]; k++) {
+          pflag[i][j][k][FLAGBSQORHO] = g_bsq[2 * zone_index(i, j, k)];
+          pflag[i][j][k][FLAGBSQOU] = g_bsq[2 * zone_index(i, j, k) + 1];
+        }
+  }
   if (DOENOFLUX == ENOFINITEVOLUME) {
     /* unew is defined on the active zones only */
     int i, j, k, pl;

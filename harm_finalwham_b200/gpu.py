@@ -111,6 +111,7 @@ def load_library(path=None):
     L.hgpu_set_tuning.argtypes = [ctypes.c_void_p, _P(hgpu_tuning)]
     L.hgpu_diagnostics.argtypes = [ctypes.c_void_p, _P(hgpu_diag)]
     L.hgpu_download_conserved.argtypes = [ctypes.c_void_p, _dp]
+    L.hgpu_download_bsqflags.argtypes = [ctypes.c_void_p, _ip]
     L.hgpu_upload_conserved.argtypes = [ctypes.c_void_p, _dp]
     L.hgpu_context_bytes.argtypes = [_P(hgpu_config)]
     L.hgpu_context_bytes.restype = ctypes.c_size_t
@@ -279,6 +280,13 @@ class HarmGPU:
         u = _contig(u, np.float64)
         assert u.shape == self.nt + (NPR,)
         _check(self.L, self.L.hgpu_upload_conserved(self.h, _ptr(u)))
+
+    def download_bsqflags(self):
+        """hgpu_download_bsqflags: the FLAGBSQORHO and FLAGBSQOU pflag slots,
+        int32 [n1+2g][n2+2g][n3+2g][2]."""
+        f = np.zeros(self.nt + (2,), dtype=np.int32)
+        _check(self.L, self.L.hgpu_download_bsqflags(self.h, _ptr(f, ctypes.c_int)))
+        return f
 
     def download_conserved(self):
         """The conserved state after the last step (the reference's unew)."""

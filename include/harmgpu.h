@@ -265,6 +265,14 @@ int hgpu_diagnostics(hgpu_ctx *ctx, hgpu_diag *out);
    (rdump_content, restart.c:244-250). */
 int hgpu_download_conserved(hgpu_ctx *ctx, double *unew);
 
+/* The pflag slots FLAGBSQORHO and FLAGBSQOU (global.h:867-868) that
+   pre_fixup -> get_bsqflags (fixup.c:25, :1751) sets at the start of each RK
+   stage (step_ch.c:117-120) from b^2/rho and b^2/u of the stage's input
+   state: flags[z][0] = FLAGBSQORHO, flags[z][1] = FLAGBSQOU (0, 1 or 2) per
+   zone of the host zone layout, as the last stage of the last step left
+   them (0 before the first step).  Not produced for batches of 1D problems. */
+int hgpu_download_bsqflags(hgpu_ctx *ctx, int *flags);
+
 /* Set the evolved conserved state of a HGPU_ENOFINITEVOLUME context from
    the host (same layout), as the reference's restart reads unew and copies
    it to uinitial (initbase.c:155-160).  hgpu_upload_state of such a context

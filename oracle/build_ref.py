@@ -170,8 +170,11 @@ def overlay_init_h(text, n1, n2, n3, maxbnd):
 UTOPRIMS = {"2DFINAL": "UTOPRIM2DFINAL", "JON": "UTOPRIMJONNONRELCOMPAT"}
 
 
-def overlay_init_c(text, lim, flux, cour, timeorder=2, utoprim="2DFINAL", fv=False):
+def overlay_init_c(text, lim, flux, cour, timeorder=2, utoprim="2DFINAL", fv=False, beta=None):
     w = "init.fishmon.c"
+    if beta is not None:
+        # plasma beta of the field normalisation (init.fishmon.c:384)
+        text = sub_once(text, "  beta = 1.e2 ;", f"  beta = {float(beta)!r} ;", where=w)
     text = sub_once(text, "  defcoord = 9;", "  defcoord = LOGRSINTH;", where=w)
     text = sub_once(text, "  UTOPRIMVERSION = UTOPRIMJONNONRELCOMPAT;", f"  UTOPRIMVERSION = {UTOPRIMS[utoprim]};", where=w)
     text = sub_once(text, "  lim = PARA;", f"  lim = {LIMS[lim]};", where=w)
@@ -201,14 +204,14 @@ GPULIB = os.path.join(REPO, "harm_finalwham_b200", "lib")
 
 
 def build(ref, n1, n2, n3, lim, flux, cour, maxbnd, name=None, keep=False, verbose=False, timeorder=2,
-          utoprim="2DFINAL", fv=False, gpu_shim=False):
+          utoprim="2DFINAL", fv=False, gpu_shim=False, beta=None):
     """gpu_shim: link the drop-in GPU step_ch (harm_finalwham_b200/dropin/step_ch_gpu.c
     against lib/libharmgpu.so) in place of the reference's own, which is kept
     as harm_cpu_step_ch (the only change to step_ch.c: the name at :16)."""
     os.makedirs(OUT, exist_ok=True)
     name = name or (f"harm_ref_{n1}x{n2}x{n3}_{lim}_{flux}" + (f"_rk{timeorder}" if timeorder != 2 else "")
                     + ("_jon" if utoprim == "JON" else "") + ("_fv" if fv else "")
-                    + ("_gpushim" if gpu_shim else ""))
+                    + (f"_beta{beta:g}" if beta is not None else "") + ("_gpushim" if gpu_shim else ""))
     scratch = tempfile.mkdtemp(prefix="harmref_")
     try:
         for fn in os.listdir(ref):
@@ -243,7 +246,7 @@ def build(ref, n1, n2, n3, lim, flux, cour, maxbnd, name=None, keep=False, verbo
         with open(os.path.join(scratch, "init.h"), "w") as f:
             f.write(ih)
         with open(os.path.join(ref, "init.fishmon.c")) as f:
-            ic = overlay_init_c(f.read(), lim, flux, cour, timeorder, utoprim, fv)
+            ic = overlay_init_c(f.read(), lim, flux, cour, timeorder, utoprim, fv, beta)
         with open(os.path.join(scratch, "init.c"), "w") as f:
             f.write(ic)
         with open(os.path.join(ref, "bounds.fishmon.c")) as f:

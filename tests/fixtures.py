@@ -14,7 +14,7 @@ CASES = ["torus2d_16x16_mc_hll", "torus3d_12x12x6_mc_laxf", "torus2d_16x16_weno5
          "torus2d_16x16_mc_hll_rk1", "torus3d_12x12x6_weno5_laxf_rk3", "torus2d_16x16_mc_hll_jon",
          "torus2d_16x16_para_hll_rk4_jon", "torus3d_12x12x6_weno5_laxf_jon", "torus2d_16x16_para_hll_rk4_jon_fv",
          "torus2d_16x16_mc_hll_fv", "torus3d_12x12x6_para_laxf_rk4_jon_fv", "torus3d_12x12x6_weno5_hll",
-         "torus3d_12x12x6_mc_hll"]
+         "torus3d_12x12x6_mc_hll", "torus2d_16x16_mc_hll_beta1e-4"]
 
 
 def load(name):
@@ -38,7 +38,8 @@ def load(name):
     pr.dt = float(d["dt_init"])
     steps = [int(s) for s in d["steps"]]
     ref = {s: dict(p=d[f"p_s{s}"], pflag=d[f"pflag_s{s}"], t=float(d[f"t_s{s}"]), dt=float(d[f"dt_s{s}"]),
-                   nstroke=float(d[f"nstroke_s{s}"]), u=d[f"u_s{s}"] if f"u_s{s}" in d else None) for s in steps}
+                   nstroke=float(d[f"nstroke_s{s}"]), u=d[f"u_s{s}"] if f"u_s{s}" in d else None,
+                   bsq=d[f"bsq_s{s}"] if f"bsq_s{s}" in d else None) for s in steps}
     return pr, ref
 
 

@@ -68,6 +68,10 @@ CASES = {
     "torus3d_12x12x6_weno5_hll": (12, 12, 6, "WENO5", "HLL", 0.8, 5, [1, 5], 2, "2DFINAL", False, 11,
                                   {"phimodes": 1}),
     "torus3d_12x12x6_mc_hll": (12, 12, 6, "MC", "HLL", 0.8, 10, [1, 10], 2, "2DFINAL", False, 11, {"phimodes": 1}),
+    # a strongly magnetised torus (plasma beta 1e-4): b^2/rho and b^2/u above
+    # the reference's flag limits in part of the grid, high-sigma inversions
+    "torus2d_16x16_mc_hll_beta1e-4": (16, 16, 1, "MC", "HLL", 0.8, 5, [1, 5], 2, "2DFINAL", False, 11,
+                                       {"beta": 1e-4}),
 }
 
 # Benchmark configurations run by the reference at their own sizes and step
@@ -94,7 +98,8 @@ def make(name, spec, ref):
     opts = spec[12] if len(spec) > 12 else {}
     hargs = ["--phimodes", str(opts["phimodes"])] if "phimodes" in opts else []
     ng = maxbnd if fv else NG[lim]
-    exe = build_ref.build(ref, n1, n2, n3, lim, flux, cour, maxbnd, timeorder=timeorder, utoprim=utoprim, fv=fv)
+    exe = build_ref.build(ref, n1, n2, n3, lim, flux, cour, maxbnd, timeorder=timeorder, utoprim=utoprim, fv=fv,
+                          beta=opts.get("beta"))
     with tempfile.TemporaryDirectory() as tmp:
         out = os.path.join(tmp, "out")
         subprocess.run([exe] + hargs + [out, str(nsteps)] + [str(s) for s in dumps], cwd=tmp, check=True,
@@ -114,6 +119,8 @@ def make(name, spec, ref):
             m = rd.meta_of(f"s{s}")
             data[f"p_s{s}"] = rd.crop(rd.p(f"s{s}"), ng)
             data[f"pflag_s{s}"] = rd.crop(rd.pflag(f"s{s}"), ng)[..., 0]
+            # the b^2/rho and b^2/u flags of pre_fixup (FLAGBSQORHO, FLAGBSQOU)
+            data[f"bsq_s{s}"] = rd.crop(rd.pflag(f"s{s}"), ng)[..., 2:4]
             data[f"t_s{s}"] = m["t"]
             data[f"dt_s{s}"] = m["dt"]
             data[f"nstroke_s{s}"] = m["nstroke"]

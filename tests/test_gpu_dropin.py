@@ -5,9 +5,9 @@ arrays, the step loop of oracle/ref_harness.c that main.c:33-49 runs) with
 harm_finalwham_b200/dropin/step_ch_gpu.c linked in place of its CPU step_ch
 (step_ch.c:16).  Its dumps must equal the reference's own CPU run bit for
 bit: the 64x64 torus configuration for its 200 steps (the record of the
-reference's run), the 3D WENO5 + HLL torus with azimuthal modes and the
-finite-volume scheme (PARA, RK4, Jon's inverter) against their golden
-fixtures."""
+reference's run), the 3D WENO5 + HLL torus with azimuthal modes, a strongly
+magnetised torus (failed inversions, b^2 flags) and the finite-volume scheme
+(PARA, RK4, Jon's inverter) against their golden fixtures."""
 import os
 import subprocess
 import tempfile
@@ -49,6 +49,7 @@ def test_reference_loop_on_gpu_matches_reference_run_64x64():
 
 @pytest.mark.parametrize("binary,fixture,args", [
     ("harm_ref_12x12x6_WENO5_HLL_gpushim", "torus3d_12x12x6_weno5_hll", ["--phimodes", "1"]),
+    ("harm_ref_16x16x1_MC_HLL_beta0.0001_gpushim", "torus2d_16x16_mc_hll_beta1e-4", []),
     ("harm_ref_16x16x1_PARA_HLL_rk4_jon_fv_gpushim", "torus2d_16x16_para_hll_rk4_jon_fv", []),
 ])
 def test_reference_loop_on_gpu_matches_golden(binary, fixture, args):
@@ -61,6 +62,7 @@ def test_reference_loop_on_gpu_matches_golden(binary, fixture, args):
             r = ref[s]
             assert same(rd.crop(rd.p(tag), pr.ng), r["p"]), f"primitives differ after step {s}"
             assert np.array_equal(rd.crop(rd.pflag(tag), pr.ng)[..., 0], r["pflag"])
+            assert np.array_equal(rd.crop(rd.pflag(tag), pr.ng)[..., 2:4], r["bsq"])
             m = rd.meta_of(tag)
             assert m["t"] == r["t"] and m["dt"] == r["dt"] and m["nstroke"] == r["nstroke"]
             if r["u"] is not None:

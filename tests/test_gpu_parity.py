@@ -110,3 +110,19 @@ def test_utoprim_zones_match_reference(inv):
     assert np.array_equal(pf, z[f"pflag_{inv}"])
     assert same(pr, z[f"pr_{inv}"])
     assert it == int(z[f"iters_{inv}"].sum())
+
+
+@pytest.mark.parametrize("name", [c for c in CASES if c.startswith("torus")])
+def test_bsq_flags_match_reference(name):
+    # pre_fixup's b^2/rho and b^2/u flags (pflag slots FLAGBSQORHO and
+    # FLAGBSQOU, get_bsqflags fixup.c:1751) as the reference leaves them
+    pr, ref = load(name)
+    with HarmGPU.from_problem(pr) as g:
+        done = 0
+        for s in sorted(ref):
+            g.step_ch(s - done)
+            done = s
+            bsq = ref[s]["bsq"]
+            assert bsq is not None, "fixture lacks the b^2 flags"
+            got = g.download_bsqflags()
+            assert np.array_equal(got, bsq), f"{int(np.count_nonzero(got != bsq))} flags differ after step {s}"
