@@ -2214,9 +2214,12 @@ __device__ double divb_fluxct(const Dims &d, const Params &P, const double *__re
   return fabs((dfx / P.dx1 + dfy / P.dx2 + dfz / P.dx3) * norm);
 }
 
+// ufv: the evolved conserved state of the finite-volume scheme, which the
+// reference's constotal integrates directly (dump_ener.c:611-619); nullptr:
+// U(p) (dump_ener.c:622-630)
 __global__ void __launch_bounds__(DIAG_BLOCK) diag_kernel(Dims d, Params P, Box box, const double *__restrict__ p,
                                                           const int *__restrict__ pflag, const double *__restrict__ G,
-                                                          double *__restrict__ part) {
+                                                          const double *__restrict__ ufv, double *__restrict__ part) {
   __shared__ double sh[DIAG_VALS][DIAG_BLOCK];
   long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   double v[DIAG_VALS];
@@ -2229,12 +2232,16 @@ __global__ void __launch_bounds__(DIAG_BLOCK) diag_kernel(Dims d, Params P, Box 
     Metric m;
     load_metric(G, d, gix(d, i, j), G_CENT, m);
     double pr[NPR], U[NPR];
-    load_prim(p, d, z, pr);
-    State q;
-    EM e;
-    get_state(pr, m, q);
-    em_prepare(pr, m, q, e);
-    primtoflux(pr, q, e, 0, m, P.gam, U);
+    if (ufv) {
+      load_prim(ufv, d, z, U);
+    } else {
+      load_prim(p, d, z, pr);
+      State q;
+      EM e;
+      get_state(pr, m, q);
+      em_prepare(pr, m, q, e);
+      primtoflux(pr, q, e, 0, m, P.gam, U);
+    }
     double dV = P.dx1 * P.dx2 * P.dx3;
 #pragma unroll
     for (int pl = 0; pl < NPR; pl++) v[pl] = U[pl] * dV;
@@ -2796,7 +2803,8 @@ extern "C" int hgpu_diagnostics(hgpu_ctx *x, hgpu_diag *out) {
   int nb = (int)grid_for(box.size(), DIAG_BLOCK);
   double *part = nullptr;
   CUDA_TRY(cudaMallocAsync(&part, sizeof(double) * ((size_t)nb * DIAG_VALS + DIAG_VALS), x->stream));
-  diag_kernel<<<nb, DIAG_BLOCK, 0, x->stream>>>(x->d, x->P, box, x->p, x->pflag, x->G, part);
+  const double *ufv = x->cfg.doenoflux == HGPU_ENOFINITEVOLUME ? x->ucum : nullptr;
+  diag_kernel<<<nb, DIAG_BLOCK, 0, x->stream>>>(x->d, x->P, box, x->p, x->pflag, x->G, ufv, part);
   diag_final_kernel<<<1, DIAG_BLOCK, 0, x->stream>>>(part, nb, part + (size_t)nb * DIAG_VALS);
   double h[DIAG_VALS];
   Scalars s;

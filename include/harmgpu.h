@@ -238,7 +238,8 @@ int hgpu_set_tuning(hgpu_ctx *ctx, const hgpu_tuning *t);
 
 /* Diagnostics of the current state (the quantities dump_ener.c writes to
    ener.out, computed on the device): integral[pl] = sum over active zones of
-   the conserved U (primtoU with gdet, UU without rest mass) times
+   the conserved U (primtoU with gdet, UU without rest mass; the evolved unew
+   for HGPU_ENOFINITEVOLUME, as constotal dump_ener.c:596-635) times
    dx1 dx2 dx3; divb_max / divb_avg = max and mean over active zones of the
    flux-CT div B at each zone's lower corner (divbmaxavg, dump_ener.c:482;
    DIVBFLUXCT, global.h:1586-1645); nfail = zones whose last inversion left

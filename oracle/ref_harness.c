@@ -29,6 +29,11 @@
  *   --geomplane        writes the geometry of the first x3 plane only (the
  *                      metric does not depend on x3): keeps the init dump of
  *                      large 3D grids small.
+ *   --ener             calls the reference's own dump_ener (dump_ener.c:3)
+ *                      after init and after every dumped step, which appends
+ *                      a line to ener.out in the working directory (t,
+ *                      realnstep, the conserved integrals, ..., divbmax,
+ *                      divbavg).
  *
  * usage: harm_ref --invert <infile> <outfile>
  *   runs the reference's Utoprimgen() (utoprimgen.c:20) zone by zone on
@@ -48,6 +53,8 @@ extern int set_density_floors(struct of_geom *ptrgeom, FTYPE *pr, FTYPE *prfloor
 
 static char outdir[1024];
 static int geomplane = 0;
+static int do_ener = 0;
+extern int dump_ener(int doener, int dordump, int call_code);
 
 /* splitmix64 (Steele, Lea and Flood, OOPSLA 2014): a small seeded generator
    for the azimuthal mode amplitudes and phases */
@@ -286,6 +293,10 @@ int main(int argc, char *argv[])
       geomplane = 1;
       argv += 1;
       argc -= 1;
+    } else if (strcmp(argv[1], "--ener") == 0) {
+      do_ener = 1;
+      argv += 1;
+      argc -= 1;
     } else {
       fprintf(stderr, "harness: unknown option %s\n", argv[1]);
       return 2;
@@ -316,6 +327,10 @@ int main(int argc, char *argv[])
     dump_geometry();
     dump_state("init", 0);
   }
+  if (do_ener && dump_ener(1, 0, INIT_OUT) >= 1) {
+    fprintf(stderr, "harness: dump_ener failed at init\n");
+    return 1;
+  }
 
   for (s = 1; s <= nsteps; s++) {
     char tag[64];
@@ -333,6 +348,10 @@ int main(int argc, char *argv[])
     if (want) {
       snprintf(tag, sizeof(tag), "s%d", s);
       dump_state(tag, 1);
+      if (do_ener && dump_ener(1, 0, DUMP_OUT) >= 1) {
+        fprintf(stderr, "harness: dump_ener failed at step %d\n", s);
+        return 1;
+      }
     }
   }
   fprintf(stderr, "harness: done %d steps t=%.17g dt=%.17g\n", nsteps, (double)t, (double)dt);

@@ -102,10 +102,15 @@ def make(name, spec, ref):
                           beta=opts.get("beta"))
     with tempfile.TemporaryDirectory() as tmp:
         out = os.path.join(tmp, "out")
-        subprocess.run([exe] + hargs + [out, str(nsteps)] + [str(s) for s in dumps], cwd=tmp, check=True,
-                       stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL)
+        subprocess.run([exe, "--ener"] + hargs + [out, str(nsteps)] + [str(s) for s in dumps], cwd=tmp,
+                       check=True, stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL)
         rd = RefDump(out)
         pr = rd.to_problem(ng, "init")
+        # the reference's own ener.out (dump_ener.c:287-295), one line at init
+        # and one after every dumped step: t, realnstep, the conserved
+        # integrals U_tot[8], ..., divbmax, divbavg
+        with open(os.path.join(tmp, "ener.out")) as f:
+            ener = [np.array([float(v) for v in line.split()]) for line in f if line.strip()]
         data = dict(n=np.array(pr.n), ng=np.array(ng), dx=np.array(pr.dx), gam=pr.gam, cour=pr.cour,
                     lim=np.array(lim), flux=np.array(flux), bc=np.array(pr.bc), safe=pr.safe, defcon=pr.defcon,
                     tf=pr.tf, rhominlimit=pr.rhominlimit, uuminlimit=pr.uuminlimit, gammamax=pr.gammamax,
@@ -115,6 +120,9 @@ def make(name, spec, ref):
                     doenoflux=np.array("ENOFINITEVOLUME" if fv else "NOENOFLUX"))
         if fv:
             data["u_init"] = pr.u
+        data["ener_init"] = ener[0]
+        for n_, s in enumerate(sorted(set(dumps) | {nsteps})):
+            data[f"ener_s{s}"] = ener[1 + n_]
         for s in dumps:
             m = rd.meta_of(f"s{s}")
             data[f"p_s{s}"] = rd.crop(rd.p(f"s{s}"), ng)

@@ -43,3 +43,37 @@ def test_diagnostics(name):
     # unew (the conserved state the step produced) inverts to p: its mass integral agrees
     umass = float(np.sum(g.active(unew)[..., 0]) * pr.dx[0] * pr.dx[1] * pr.dx[2])
     assert umass == pytest.approx(mass, rel=1e-3)  # floors and fixups change p after the inversion
+
+
+@pytest.mark.parametrize("name", ["torus2d_16x16_mc_hll", "torus3d_12x12x6_weno5_hll", "torus2d_16x16_mc_hll_beta1e-4",
+                                  "torus2d_16x16_para_hll_rk4_jon_fv"])
+def test_diagnostics_match_reference_ener_out(name):
+    # the reference's own ener.out (dump_ener.c:287-295, written by its
+    # dump_ener through the harness at init and after each dumped step):
+    # t, realnstep, the conserved integrals U_tot (constotal dump_ener.c:596,
+    # U with gdet times dx1 dx2 dx3 over the active zones; unew for the
+    # finite-volume scheme), ..., divbmax, divbavg (divbmaxavg :482).  The
+    # file prints 15 significant digits and sums in loop order, the device
+    # in a fixed tree order: integrals agree to 1e-13 of the mass integral's
+    # scale, the div B maximum to the print precision.
+    pr, ref = load(name)
+    assert pr.ener_init is not None, "fixture lacks the reference's ener.out"
+    npr = 8
+    ncol = 2 + npr + 2 * 6 * npr + 2 * npr
+
+    def check(dg, line, step):
+        assert line[0] == pytest.approx(dg["t"], rel=1e-14, abs=1e-300)
+        scale = abs(line[2])
+        for q in range(npr):
+            assert dg["integral"][q] == pytest.approx(line[2 + q], rel=1e-13, abs=1e-13 * scale), \
+                f"step {step}: integral {q}: {dg['integral'][q]!r} vs ener.out {line[2 + q]!r}"
+        assert dg["divb_max"] == pytest.approx(line[ncol], rel=1e-13, abs=1e-300)
+        assert dg["divb_avg"] == pytest.approx(line[ncol + 1], rel=1e-12, abs=1e-300)
+
+    with HarmGPU.from_problem(pr) as g:
+        check(g.diagnostics(), pr.ener_init, 0)
+        done = 0
+        for s in sorted(ref):
+            g.step_ch(s - done)
+            done = s
+            check(g.diagnostics(), ref[s]["ener"], s)
