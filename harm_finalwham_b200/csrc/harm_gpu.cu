@@ -1434,6 +1434,12 @@ int hg_reconfigure(hgpu_ctx *x, const hgpu_config *cfg) {
   return HGPU_OK;
 }
 
+int hgpu_reconfigure(hgpu_ctx *x, const hgpu_config *cfg) {
+  const int rc = hg_reconfigure(x, cfg);
+  if (rc == HGPU_E_INVALID) set_err("hgpu_reconfigure: configuration invalid or of another allocation shape");
+  return rc;
+}
+
 int hgpu_create(const hgpu_config *cfg, hgpu_ctx **out) {
   if (!out) return HGPU_E_INVALID;
   *out = nullptr;

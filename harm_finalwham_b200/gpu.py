@@ -112,6 +112,7 @@ def load_library(path=None):
     L.hgpu_diagnostics.argtypes = [ctypes.c_void_p, _P(hgpu_diag)]
     L.hgpu_download_conserved.argtypes = [ctypes.c_void_p, _dp]
     L.hgpu_download_bsqflags.argtypes = [ctypes.c_void_p, _ip]
+    L.hgpu_reconfigure.argtypes = [ctypes.c_void_p, _P(hgpu_config)]
     L.hgpu_upload_conserved.argtypes = [ctypes.c_void_p, _dp]
     L.hgpu_context_bytes.argtypes = [_P(hgpu_config)]
     L.hgpu_context_bytes.restype = ctypes.c_size_t
@@ -206,6 +207,22 @@ class HarmGPU:
         h = ctypes.c_void_p()
         _check(self.L, self.L.hgpu_create(ctypes.byref(c), ctypes.byref(h)))
         self.h = h
+
+    def reconfigure(self, dx=None, gam=None, cour=None, tf=None):
+        """hgpu_reconfigure: the same context for another solve of the same
+        allocation shape (upload geometry and state afterwards)."""
+        c = hgpu_config.from_buffer_copy(self.cfg)
+        if dx is not None:
+            for i in range(3):
+                c.dx[i + 1] = float(dx[i])
+        if gam is not None:
+            c.gam = float(gam)
+        if cour is not None:
+            c.cour = float(cour)
+        if tf is not None:
+            c.tf = float(tf)
+        _check(self.L, self.L.hgpu_reconfigure(self.h, ctypes.byref(c)))
+        self.cfg = c
 
     @classmethod
     def from_problem(cls, pr, precision="fp64"):

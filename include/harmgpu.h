@@ -110,6 +110,16 @@ int hgpu_abi_version(void);
 int hgpu_create(const hgpu_config *cfg, hgpu_ctx **out);
 void hgpu_destroy(hgpu_ctx *ctx);
 
+/* Reuse a context for another solve of the same allocation shape (no
+   counterpart in the reference, which runs one problem per process): the
+   by-value parameters of cfg (dx, gam, cour, safe, defcon, tf, floor limits,
+   gammamax, gammafail, boundary ids) replace the context's; grid size,
+   ghosts, scheme, inverter, time order and precision must be unchanged
+   (else HGPU_E_INVALID).  Upload the geometry and the state after it.  No
+   device memory is allocated or freed, as the serving loop does for its
+   idle contexts. */
+int hgpu_reconfigure(hgpu_ctx *ctx, const hgpu_config *cfg);
+
 /* Upload the precomputed geometry (set_grid.c:7-151) and floors
    (set_density_floors, fixup.c:1542-1654); host layouts above. */
 int hgpu_upload_geometry(hgpu_ctx *ctx, const double *gcov, const double *gcon, const double *gcovpert,

@@ -261,14 +261,34 @@ def make_record(name, ref, workdir=None):
     print(f"wrote {path} ({os.path.getsize(path) / 1e6:.2f} MB)")
 
 
+def make_bondigrid(ref):
+    """The reference's tabulated Bondi solutions (bondigrid{N}.dat, read by
+    readin_bondi_solution init.c:350-460): per table its header constants
+    and the rows i, x, r, rho, u^r, u (the ghost rows included)."""
+    data = {}
+    for n in (32, 64, 128, 256):
+        with open(os.path.join(ref, f"bondigrid{n}.dat")) as f:
+            lines = f.read().splitlines()
+        head = " ".join(lines[:2]).replace("#", " ").replace("=", " ").split()
+        kv = {head[i]: float(head[i + 1]) for i in range(0, len(head) - 1, 2)}
+        rows = np.array([[float(v) for v in ln.split()] for ln in lines[3:] if ln.strip()])
+        data[f"n{n}_rows"] = rows
+        data[f"n{n}_head"] = np.array([kv[k] for k in ("Gamma", "Rcr", "uu1cr", "rhocr", "Nx", "Rin", "Rout")])
+    path = os.path.join(HERE, "bondigrid.npz")
+    np.savez_compressed(path, **data)
+    print(f"wrote {path} ({os.path.getsize(path) / 1e6:.2f} MB)")
+
+
 def main():
     ref = build_ref.DEFAULT_REF
     if not os.path.isdir(ref):
         raise SystemExit(f"reference tree not found at {ref}: set HARM_REFERENCE_DIR")
-    names = sys.argv[1:] or list(CASES) + ["utoprim_zones"] + list(RECORDS)
+    names = sys.argv[1:] or list(CASES) + ["utoprim_zones", "bondigrid"] + list(RECORDS)
     for name in names:
         if name == "utoprim_zones":
             make_zones(ref)
+        elif name == "bondigrid":
+            make_bondigrid(ref)
         elif name in RECORDS:
             make_record(name, ref)
         else:

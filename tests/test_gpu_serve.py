@@ -88,3 +88,40 @@ def test_context_frozen_after_end_time():
     finally:
         g.close()
     assert same(a[0], b[0]) and np.array_equal(a[1], b[1]) and a[2] == b[2] and a[2] >= TF
+
+
+def test_reconfigured_context_equals_fresh_context():
+    # hgpu_reconfigure: a context reused for another solve of the same
+    # allocation shape (another spin, so another dx, and another end time)
+    # gives the fresh context's result bit for bit, in plain and graph steps
+    a = torus.fm_torus(32, 32, 1, ng=3, a=0.5, beta=50.0, seed=1)
+    b = torus.fm_torus(32, 32, 1, ng=3, a=0.9, beta=200.0, seed=7)
+    assert a.dx != b.dx
+    ref = run_alone(b, 0.3)
+    inv = {0: "OUTFLOW", 4: "POLARAXIS", 7: "PERIODIC", 1000: "OUTFLOW_COPY"}
+    g = HarmGPU(*a.n, a.ng, a.dx, lim=a.lim, flux=a.flux, bc=tuple(inv[q] for q in a.bc), gam=a.gam, cour=a.cour,
+                tf=TF)
+    try:
+        for use_graph in (False, True):
+            for dom, tf in ((a, TF), (b, 0.3)):
+                g.reconfigure(dx=dom.dx, gam=dom.gam, cour=dom.cour, tf=tf)
+                g.upload_geometry(dom.gcov, dom.gcon, dom.gcovpert, dom.gdet, dom.conn, dom.floors)
+                g.upload_state(dom.p, None, 0.0, 0.0)
+                g.init_dt()
+                for _ in range(2000):
+                    if use_graph:
+                        g.step_graph(1, stats=False)
+                    else:
+                        g.step_ch(1, stats=False)
+                    if g.time()[0] >= tf:
+                        break
+            p, pf, t, dt = g.download_state()
+            assert same(p, ref[0]) and np.array_equal(pf, ref[1]) and t == ref[2] and dt == ref[3]
+        # another allocation shape is refused
+        import ctypes
+        from harm_finalwham_b200.gpu import hgpu_config
+        c = hgpu_config.from_buffer_copy(g.cfg)
+        c.n1 = 64
+        assert g.L.hgpu_reconfigure(g.h, ctypes.byref(c)) != 0
+    finally:
+        g.close()
