@@ -2,8 +2,8 @@
 
     python -m harm_finalwham_b200.build
 
-nvcc compiles csrc/harm_gpu.cu (kernels and C ABI) and csrc/serve.cu (the
-serving loop, host code) for sm_100a only (-gencode
+nvcc compiles csrc/harm_gpu.cu (kernels and C ABI), csrc/serve.cu (the
+serving loop, host code), csrc/rdump.cu (restart dumps, host code) for sm_100a only (-gencode
 arch=compute_100a,code=sm_100a) with -fmad=false so that the FP64 path keeps
 the reference's floating-point operation order (the reference CPU build uses
 -ffp-contract=off), and csrc/flux_f32.cu (the FP32 kernels of the mixed
@@ -20,7 +20,7 @@ ROOT = os.path.dirname(PKG)
 CSRC = os.path.join(PKG, "csrc")
 LIBDIR = os.path.join(PKG, "lib")
 LIB = os.path.join(LIBDIR, "libharmgpu.so")
-SOURCES = ["harm_gpu.cu", "serve.cu", "flux_f32.cu"]
+SOURCES = ["harm_gpu.cu", "serve.cu", "rdump.cu", "flux_f32.cu"]
 HEADERS = ["harm_device.cuh", "weno5.cuh", "common.cuh", os.path.join(ROOT, "include", "harmgpu.h")]
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]

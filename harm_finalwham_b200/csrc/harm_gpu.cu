@@ -1374,6 +1374,9 @@ int hgpu_abi_version(void) { return HGPU_ABI_VERSION; }
 
 const char *hgpu_last_error(void) { return g_errbuf; }
 
+// error text of a failing call made elsewhere in the library (host code)
+void hg_set_error(const char *msg) { snprintf(g_errbuf, sizeof(g_errbuf), "%s", msg); }
+
 void hgpu_destroy(hgpu_ctx *x) {
   if (!x) return;
   cudaStreamSynchronize(x->stream);
@@ -2769,6 +2772,13 @@ extern "C" int hgpu_utoprim_batch_noalloc(const double *U, const double *gcov, c
 // ---------------------------------------------------------------------------
 cudaStream_t hg_stream(hgpu_ctx *x) { return x->stream; }
 
+// Configuration of a context and whether it is a batch of 1D instances
+// (host code elsewhere in the library: the restart dump writer).
+const hgpu_config *hg_config(const hgpu_ctx *x, int *is_batch) {
+  if (is_batch) *is_batch = x->ninst > 0;
+  return &x->cfg;
+}
+
 // Enqueue on the context's stream a copy of (t, dt, done, steps) into host
 // memory dst[4] (pinned) and record ev after it; the host tests ev with
 // cudaEventQuery and reads dst once it has completed.
@@ -2836,7 +2846,7 @@ extern "C" int hgpu_diagnostics(hgpu_ctx *x, hgpu_diag *out) {
 // with gdet) in the reference's AoS layout, for restart dumps
 // (rdump_content, restart.c:244-250, writes p and unew per zone)
 extern "C" int hgpu_upload_conserved(hgpu_ctx *x, const double *unew) {
-  if (!x || !unew || x->cfg.doenoflux != HGPU_ENOFINITEVOLUME) return HGPU_E_INVALID;
+  if (!x || !unew || x->ninst > 0) return HGPU_E_INVALID;
   long long nz = x->d.nz;
   int rc = ensure_staging(x);
   if (rc) return rc;

@@ -39,6 +39,12 @@
  *                             loops that never modify p between steps);
  *                             results are still copied back every step
  *
+ * Restart dumps: the reference's restart_write (restart.c:206) is kept as
+ * harm_cpu_restart_write (a one-token rename of restart.c:206, done by the
+ * same build step) and wrapped below: unew, which the host arrays do not
+ * receive after every step for the non-finite-volume schemes, is copied
+ * from the device first, so the file holds what a CPU run writes.
+ *
  * Errors: a failing hgpu_* call prints hgpu_last_error() to the reference's
  * fail_file and step_ch returns 1, which the reference's MYFUN/error_check
  * turn into its own failure path.  HGPU_E_PHYSICS marks the conditions where
@@ -259,4 +265,19 @@ int step_ch(void)
   tstepparti = tsteppartf = t;
   realnstep++;
   return 0;
+}
+
+extern int harm_cpu_restart_write(long dump_cnt);
+
+/* restart_write (restart.c:206-235) with the device's unew (the conserved
+   state after the last step; rdump_content writes p and unew) */
+int restart_write(long dump_cnt)
+{
+  if (g_ctx && DOENOFLUX != ENOFINITEVOLUME) {
+    int i, j, k, pl;
+    CHECK(hgpu_download_conserved(g_ctx, g_p));
+    ZLOOP for (pl = 0; pl < NPR; pl++) unew[i][j][k][pl] = g_p[NPR * zone_index(i, j, k) + pl];
+    /* g_p held the primitives of the last step, which p already has */
+  }
+  return harm_cpu_restart_write(dump_cnt);
 }

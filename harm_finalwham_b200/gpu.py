@@ -114,6 +114,9 @@ def load_library(path=None):
     L.hgpu_download_bsqflags.argtypes = [ctypes.c_void_p, _ip]
     L.hgpu_reconfigure.argtypes = [ctypes.c_void_p, _P(hgpu_config)]
     L.hgpu_upload_conserved.argtypes = [ctypes.c_void_p, _dp]
+    L.hgpu_write_rdump.argtypes = [ctypes.c_void_p, ctypes.c_char_p, ctypes.c_void_p, ctypes.c_size_t, ctypes.c_int]
+    L.hgpu_read_rdump.argtypes = [ctypes.c_void_p, ctypes.c_char_p, ctypes.c_size_t, ctypes.c_int, ctypes.c_double,
+                                  ctypes.c_double]
     L.hgpu_context_bytes.argtypes = [_P(hgpu_config)]
     L.hgpu_context_bytes.restype = ctypes.c_size_t
     L.hgpu_server_create.argtypes = [ctypes.c_size_t, ctypes.c_int, ctypes.c_int, _P(ctypes.c_void_p)]
@@ -147,7 +150,8 @@ def load_library(path=None):
     for name in ("hgpu_create", "hgpu_upload_geometry", "hgpu_upload_state", "hgpu_download_state", "hgpu_step_ch",
                  "hgpu_advance_stage", "hgpu_fluxcalc", "hgpu_bound_prim", "hgpu_utoprim_batch", "hgpu_utoprimgen_batch",
                  "hgpu_device_prims", "hgpu_sync", "hgpu_create_batch", "hgpu_batch_layout", "hgpu_batch_status",
-                 "hgpu_step_graph", "hgpu_autotune", "hgpu_set_tuning", "hgpu_batch_run", "hgpu_diagnostics", "hgpu_download_conserved", "hgpu_upload_conserved", "hgpu_server_create", "hgpu_server_submit", "hgpu_server_submit_borrowed",
+                 "hgpu_step_graph", "hgpu_autotune", "hgpu_set_tuning", "hgpu_batch_run", "hgpu_diagnostics", "hgpu_download_conserved", "hgpu_upload_conserved",
+                 "hgpu_write_rdump", "hgpu_read_rdump", "hgpu_server_create", "hgpu_server_submit", "hgpu_server_submit_borrowed",
                  "hgpu_server_poll", "hgpu_server_result", "hgpu_server_release", "hgpu_halo_bytes", "hgpu_halo_pack",
                  "hgpu_halo_unpack", "hgpu_stats_clear", "hgpu_stats_read", "hgpu_stage_advance", "hgpu_stage_fixup",
                  "hgpu_dt_probe", "hgpu_step_end", "hgpu_ndt_pack", "hgpu_ndt_unpack", "hgpu_stream"):
@@ -293,7 +297,8 @@ class HarmGPU:
         return st
 
     def upload_conserved(self, u):
-        """Set the finite-volume scheme's conserved state (restart's unew)."""
+        """Set the conserved state unew (restart's unew; evolved by the
+        finite-volume scheme, reported until the next step otherwise)."""
         u = _contig(u, np.float64)
         assert u.shape == self.nt + (NPR,)
         _check(self.L, self.L.hgpu_upload_conserved(self.h, _ptr(u)))
@@ -304,6 +309,17 @@ class HarmGPU:
         f = np.zeros(self.nt + (2,), dtype=np.int32)
         _check(self.L, self.L.hgpu_download_bsqflags(self.h, _ptr(f, ctypes.c_int)))
         return f
+
+    def write_rdump(self, path, header=b"", binary=False):
+        """hgpu_write_rdump: the reference's restart dump of the current state
+        (header bytes, then p[0..7] and unew[0..7] of every active zone)."""
+        header = bytes(header)
+        _check(self.L, self.L.hgpu_write_rdump(self.h, os.fsencode(path), header, len(header), int(bool(binary))))
+
+    def read_rdump(self, path, t, dt, header_bytes=0, binary=False):
+        """hgpu_read_rdump: state from a restart dump, ghosts by bound_prim."""
+        _check(self.L, self.L.hgpu_read_rdump(self.h, os.fsencode(path), int(header_bytes), int(bool(binary)),
+                                              float(t), float(dt)))
 
     def download_conserved(self):
         """The conserved state after the last step (the reference's unew)."""

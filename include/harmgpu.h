@@ -33,7 +33,7 @@
 extern "C" {
 #endif
 
-#define HGPU_ABI_VERSION 9
+#define HGPU_ABI_VERSION 10
 
 /* return codes */
 #define HGPU_OK 0
@@ -284,12 +284,37 @@ int hgpu_download_conserved(hgpu_ctx *ctx, double *unew);
    them (0 before the first step).  Not produced for batches of 1D problems. */
 int hgpu_download_bsqflags(hgpu_ctx *ctx, int *flags);
 
-/* Set the evolved conserved state of a HGPU_ENOFINITEVOLUME context from
-   the host (same layout), as the reference's restart reads unew and copies
-   it to uinitial (initbase.c:155-160).  hgpu_upload_state of such a context
-   sets it to U(p) in every zone, as init_conservatives/pi2Uavg does
-   (initbase.c:146-153, 1833). */
+/* Set the conserved state unew from the host (same layout), as the
+   reference's restart reads unew (restart.c:256-270).  A HGPU_ENOFINITEVOLUME
+   context evolves it: the next step starts from it, as the reference copies
+   it to uinitial (initbase.c:155-160), and hgpu_upload_state of such a
+   context sets it to U(p) in every zone, as init_conservatives/pi2Uavg does
+   (initbase.c:146-153, 1833).  Any other context only reports it through
+   hgpu_download_conserved until its next step, which rewrites unew without
+   reading it (advance_standard, advance.c:58-240).  Not for batches. */
 int hgpu_upload_conserved(hgpu_ctx *ctx, const double *unew);
+
+/* The reference's restart dump (restart_write restart.c:206-235, body
+   rdump_content :240-245 through dump_gen dumpgen.c:245-283 and myfwrite
+   mpi_fileio.c:2073-2150, one process): `header` (header_bytes bytes: the
+   caller's write_restart_header output, restart.c:640-800, which holds host
+   state such as t, nstep, the options and the cumulative diagnostics; may
+   be empty) and then every active zone, k outermost and i fastest
+   (DUMPGENLOOP, global.h:1411-1432), as p[0..7] followed by unew[0..7] (the
+   context's state after its last step): binary = 0 writes each value as
+   "%21.15g " and a newline after each zone (TEXTOUTPUT, the reference's
+   format without MPI, initbase.c:237), binary = 1 the 16 doubles of each
+   zone in host byte order (BINARYOUTPUT).  HGPU_E_INVALID with a message on
+   an I/O error.  Not for batches. */
+int hgpu_write_rdump(hgpu_ctx *ctx, const char *path, const void *header, size_t header_bytes, int binary);
+
+/* Reads such a dump (its first header_bytes bytes skipped) into the
+   context: the primitives and unew of the active zones, then bound_prim for
+   the ghost zones, as restart_init does after restart_read (restart.c:1-150);
+   t and dt are the caller's (the header's t; the reference then resets dt
+   with set_dt).  pflag is cleared.  HGPU_E_INVALID with a message on a
+   missing, short or malformed file. */
+int hgpu_read_rdump(hgpu_ctx *ctx, const char *path, size_t header_bytes, int binary, double t, double dt);
 
 /* ---- Domain split along x3 ----------------------------------------------
    The reference decomposes the grid over MPI ranks (ncpux1..3,

@@ -34,6 +34,10 @@
  *                      a line to ener.out in the working directory (t,
  *                      realnstep, the conserved integrals, ..., divbmax,
  *                      divbavg).
+ *   --rdump            calls the reference's own restart_write(0)
+ *                      (restart.c:206) after the last step, which writes
+ *                      dumps/rdump-0 in the working directory (its header,
+ *                      then p and unew of every active zone).
  *
  * usage: harm_ref --invert <infile> <outfile>
  *   runs the reference's Utoprimgen() (utoprimgen.c:20) zone by zone on
@@ -54,6 +58,8 @@ extern int set_density_floors(struct of_geom *ptrgeom, FTYPE *pr, FTYPE *prfloor
 static char outdir[1024];
 static int geomplane = 0;
 static int do_ener = 0;
+static int do_rdump = 0;
+extern int restart_write(long dump_cnt);
 extern int dump_ener(int doener, int dordump, int call_code);
 
 /* splitmix64 (Steele, Lea and Flood, OOPSLA 2014): a small seeded generator
@@ -297,13 +303,17 @@ int main(int argc, char *argv[])
       do_ener = 1;
       argv += 1;
       argc -= 1;
+    } else if (strcmp(argv[1], "--rdump") == 0) {
+      do_rdump = 1;
+      argv += 1;
+      argc -= 1;
     } else {
       fprintf(stderr, "harness: unknown option %s\n", argv[1]);
       return 2;
     }
   }
   if (argc < 3) {
-    fprintf(stderr, "usage: %s [--phimodes seed] [--geomplane] <outdir|-> <nsteps> [dumpstep ...]\n", argv[0]);
+    fprintf(stderr, "usage: %s [--phimodes seed] [--geomplane] [--ener] [--rdump] <outdir|-> <nsteps> [dumpstep ...]\n", argv[0]);
     return 2;
   }
   /* outdir "-" runs the steps for timing only and writes nothing */
@@ -353,6 +363,10 @@ int main(int argc, char *argv[])
         return 1;
       }
     }
+  }
+  if (do_rdump) {
+    mkdir("dumps", 0755);
+    if (restart_write(0) != 0) { fprintf(stderr, "harness: restart_write failed\n"); return 1; }
   }
   fprintf(stderr, "harness: done %d steps t=%.17g dt=%.17g\n", nsteps, (double)t, (double)dt);
   return 0;

@@ -74,6 +74,12 @@ CASES = {
                                        {"beta": 1e-4}),
 }
 
+# cases whose fixture also holds the reference's restart dump after the last
+# step (restart_write(0) through the harness's --rdump: header line, then p
+# and unew of every active zone as text), from a run without dump_ener
+RDUMP = {"torus2d_16x16_mc_hll", "torus2d_16x16_mc_hll_beta1e-4", "torus2d_16x16_para_hll_rk4_jon_fv",
+         "torus3d_12x12x6_weno5_hll"}
+
 # Benchmark configurations run by the reference at their own sizes and step
 # counts: name -> (n1, n2, n3, lim, flux, cour, nsteps, dump steps, harness
 # options, lattice stride of the sample, keep the whole active state)
@@ -134,6 +140,18 @@ def make(name, spec, ref):
             data[f"nstroke_s{s}"] = m["nstroke"]
             if fv:
                 data[f"u_s{s}"] = rd.crop(rd.unew(f"s{s}"), ng)
+            else:
+                # unew of the other schemes: the last stage's conserved
+                # update (what the restart dump holds beside p)
+                data[f"unew_s{s}"] = rd.crop(rd.unew(f"s{s}"), ng)
+        if name in RDUMP:
+            # a run of its own without dump_ener, whose integrals would fill
+            # the header's cumulative diagnostics (dump_ener.c:160-230)
+            with tempfile.TemporaryDirectory() as tmp2:
+                subprocess.run([exe, "--rdump"] + hargs + ["-", str(nsteps)], cwd=tmp2, check=True,
+                               stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL)
+                with open(os.path.join(tmp2, "dumps", "rdump-0"), "rb") as f:
+                    data["rdump"] = np.frombuffer(f.read(), dtype=np.uint8)
     path = os.path.join(HERE, name + ".npz")
     np.savez_compressed(path, **data)
     print(f"wrote {path} ({os.path.getsize(path) / 1e6:.2f} MB)")

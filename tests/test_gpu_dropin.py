@@ -7,7 +7,9 @@ harm_finalwham_b200/dropin/step_ch_gpu.c linked in place of its CPU step_ch
 bit: the 64x64 torus configuration for its 200 steps (the record of the
 reference's run), the 3D WENO5 + HLL torus with azimuthal modes, a strongly
 magnetised torus (failed inversions, b^2 flags) and the finite-volume scheme
-(PARA, RK4, Jon's inverter) against their golden fixtures."""
+(PARA, RK4, Jon's inverter) against their golden fixtures, and the restart
+dump the reference's restart_write makes from the GPU state equals the one
+of its CPU run byte for byte."""
 import os
 import subprocess
 import tempfile
@@ -55,8 +57,12 @@ def test_reference_loop_on_gpu_matches_reference_run_64x64():
 def test_reference_loop_on_gpu_matches_golden(binary, fixture, args):
     pr, ref = load(fixture)
     steps = sorted(ref)
-    tmp, rd = run_shim(binary, steps[-1], steps[:-1], args)
+    # --rdump: the reference's own restart_write after the last step, through
+    # the shim's wrapper that brings unew from the device
+    tmp, rd = run_shim(binary, steps[-1], steps[:-1], ["--rdump"] + list(args))
     with tmp:
+        with open(os.path.join(tmp.name, "dumps", "rdump-0"), "rb") as f:
+            assert f.read() == pr.rdump, "the restart dump differs from the reference's"
         for s in steps:
             tag = f"s{s}"
             r = ref[s]
