@@ -56,7 +56,28 @@ struct Params {
   const int *cell_inst;  // instance of every cell of the line
   Inst *inst;
   int ninst;
+  // failure and floor counters per zone, NFFC planes of nz (failfloorcount,
+  // fixup.c:206): incremented where the reference's diag_fixup counts
+  unsigned int *ffc;
 };
+
+// counter categories (global.h:769-779)
+enum {
+  CNT_UTOPRIMFAILCONV = 0,
+  CNT_FLOORACT = 1,
+  CNT_LIMITGAMMAACT = 2,
+  CNT_INFLOWACT = 3,
+  CNT_UTOPRIMFAILRHONEG = 4,
+  CNT_UTOPRIMFAILUNEG = 5,
+  CNT_UTOPRIMFAILRHOUNEG = 6,
+  CNT_GAMMAPERC = 7,
+  CNT_UPERC = 8,
+  NFFC = 9
+};
+
+__device__ __forceinline__ void ffc_count(const Params &P, long long nz, long long z, int what) {
+  if (P.ffc) P.ffc[(long long)what * nz + z] += 1u;
+}
 
 // device scalars
 struct Scalars {

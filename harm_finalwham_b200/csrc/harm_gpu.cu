@@ -439,6 +439,11 @@ __global__ void __launch_bounds__(128, MB) invert_kernel(Dims d, Params P, Box b
       if (fu > pr[UU]) pr[UU] = fu;
       const int lg = limit_gamma(P.gammamax, pr, m, &err);
       if (floored) atomicAdd(&sc->nfloor, 1ULL);
+      // diag_fixup's counts: limit_gamma's own when it rescaled
+      // (fixup.c:1913), fixup1zone's when floors or the gamma limit changed
+      // the zone (fixup.c:443; a failed limit_gamma returns before either)
+      if (lg == -1) ffc_count(P, nz, z, CNT_LIMITGAMMAACT);
+      if (lg < 1 && (floored || lg == -1)) ffc_count(P, nz, z, CNT_FLOORACT);
       // diag_fixup (fixup.c:443) when fixup1zone changed the primitives
       if (ufv && lg < 1 && (floored || lg == -1)) fv_diag_fixup(pr0, pr, m, gam, ufv, z, nz, &err);
     }
@@ -792,6 +797,17 @@ __global__ void fixup_collect_kernel(Dims d, Params P, Box box, const int *__res
   }
 }
 
+// counter of a failure code that becomes fixed (fixup.c:1340-1425, with the
+// reference's settings STEPOVERNEG*=-1 and DOCOUNTNEG*=1)
+__device__ __forceinline__ int failure_counter(int f) {
+  if (f == UTOPRIMFAILRHONEG) return CNT_UTOPRIMFAILRHONEG;
+  if (f == UTOPRIMFAILUNEG || f == UTOPRIMFAILU2AVG1 || f == UTOPRIMFAILU2AVG2) return CNT_UTOPRIMFAILUNEG;
+  if (f == UTOPRIMFAILRHOUNEG) return CNT_UTOPRIMFAILRHOUNEG;
+  if (f == UTOPRIMFAILGAMMAPERC) return CNT_GAMMAPERC;
+  if (f == UTOPRIMFAILUPERC) return CNT_UPERC;
+  return CNT_UTOPRIMFAILCONV;  // the non-convergence and NaN codes
+}
+
 __device__ __forceinline__ bool becomes_fixed(int f, int finalstep) {
   // accounting branch of fixup.c:1399-1470: which codes are reset to
   // UTOPRIMFAILFIXED (STEPOVERNEG*=-1, DOCOUNTNEG*=1)
@@ -894,7 +910,9 @@ __global__ void fixup_compute_kernel(Dims d, Params P, const double *__restrict_
         pr[pl] = 0.5 * (a41 + a42);
       }
     }
-    limit_gamma(gamma, pr, m, &err);
+    // the averaged state's gamma limited to the zone's own (fixup.c:1326),
+    // counted by limit_gamma when it rescaled (fixup.c:1913)
+    if (limit_gamma(gamma, pr, m, &err) == -1) ffc_count(P, d.nz, z, CNT_LIMITGAMMAACT);
   }
 #pragma unroll
   for (int v = 0; v < 5; v++) outv[(long long)a * 5 + v] = pr[v];
@@ -932,6 +950,8 @@ __global__ void fixup_scatter_kernel(Dims d, Params P, double *pv, int *pflag, c
         fv_diag_fixup(pr0, pr, m, P.gam, ufv, z, d.nz, &err);
         if (err) atomicOr(&sc->err, err);
       }
+      // diag_fixup's count of the failure type (fixup.c:1428)
+      if (f > 0) ffc_count(P, d.nz, z, failure_counter(f));
       pflag[z] = UTOPRIMFAILFIXED;
       atomicAdd(&sc->nfixed, 1);
     }
@@ -1273,6 +1293,7 @@ struct hgpu_ctx {
   double *pL = nullptr, *pR = nullptr;  // WENO5 face values
   double *w5pu = nullptr;               // WENO5: per-zone dP/P state pieces (2 planes)
   unsigned char *bsqf = nullptr;        // FLAGBSQORHO | FLAGBSQOU << 2 per zone
+  unsigned int *ffc = nullptr;          // failure/floor counters, NFFC planes
   double *progress = nullptr;                          // 4 doubles for hg_progress_async
   W5Tile w5[4];  // WENO5 tiling per direction
   Box w5_state_box;  // zones whose dP/P state pieces some direction reads
@@ -1386,7 +1407,7 @@ void hgpu_destroy(hgpu_ctx *x) {
   for (cudaEvent_t e : x->freelist) cudaEventDestroy(e);
   void *ptrs[] = {x->p, x->pk, x->uf, x->ucum, x->F[1], x->F[2], x->F[3], x->E, x->G, x->pflag, x->gammacheck,
                   x->cand, x->fixlist, x->cand_orig, x->cand_dec, x->candmap, x->fixvals, x->sc, x->staging, x->istaging,
-                  x->pL, x->pR, x->w5pu, x->bsqf, x->cell_inst, x->inst, x->progress, x->pk1, x->ui};
+                  x->pL, x->pR, x->w5pu, x->bsqf, x->ffc, x->cell_inst, x->inst, x->progress, x->pk1, x->ui};
   for (void *q : ptrs)
     if (q) cudaFree(q);
   cudaStreamDestroy(x->stream);
@@ -1434,6 +1455,7 @@ int hg_reconfigure(hgpu_ctx *x, const hgpu_config *cfg) {
   x->graph = nullptr;
   x->cfg = *cfg;
   fill_params(x->P, cfg);
+  CUDA_TRY(cudaMemsetAsync(x->ffc, 0, sizeof(unsigned int) * NFFC * x->d.nz, x->stream));
   return HGPU_OK;
 }
 
@@ -1528,7 +1550,9 @@ int hgpu_create(const hgpu_config *cfg, hgpu_ctx **out) {
             cudaMalloc(&x->candmap, sizeof(int) * nz) == cudaSuccess &&
             cudaMalloc(&x->fixvals, sizeof(double) * 5 * x->cap) == cudaSuccess &&
             cudaMalloc(&x->sc, sizeof(Scalars)) == cudaSuccess &&
-            cudaMalloc(&x->bsqf, nz) == cudaSuccess && cudaMemset(x->bsqf, 0, nz) == cudaSuccess;
+            cudaMalloc(&x->bsqf, nz) == cudaSuccess && cudaMemset(x->bsqf, 0, nz) == cudaSuccess &&
+            cudaMalloc(&x->ffc, sizeof(unsigned int) * NFFC * nz) == cudaSuccess &&
+            cudaMemset(x->ffc, 0, sizeof(unsigned int) * NFFC * nz) == cudaSuccess;
   for (int dd = 1; dd <= 3 && ok; dd++) ok = cudaMalloc(&x->F[dd], pb) == cudaSuccess;
   if (ok && cfg->timeorder >= 3) ok = cudaMalloc(&x->pk1, pb) == cudaSuccess && cudaMemset(x->pk1, 0, pb) == cudaSuccess;
   if (ok && cfg->doenoflux == HGPU_ENOFINITEVOLUME)
@@ -1542,6 +1566,7 @@ int hgpu_create(const hgpu_config *cfg, hgpu_ctx **out) {
     set_err("device allocation failed");
     return HGPU_E_NOMEM;
   }
+  x->P.ffc = x->ffc;
   cudaMemsetAsync(x->p, 0, pb, x->stream);
   cudaMemsetAsync(x->pk, 0, pb, x->stream);
   cudaMemsetAsync(x->uf, 0, pb, x->stream);
@@ -2804,6 +2829,7 @@ extern "C" size_t hgpu_context_bytes(const hgpu_config *c) {
              + sizeof(double) * G_NCOMP * nij // geometry
              + sizeof(int) * 2 * nz           // pflag, candidate map
              + (size_t)nz                     // b^2 flags
+             + sizeof(unsigned int) * NFFC * nz  // failure/floor counters
              + sizeof(double) * nz            // gamma check
              + cap * (2 * sizeof(long long) + 2 * sizeof(int) + 5 * sizeof(double))
              + plane;                         // staging for uploads and downloads
@@ -2867,6 +2893,18 @@ extern "C" int hgpu_download_bsqflags(hgpu_ctx *x, int *flags) {
     flags[2 * z] = h[z] & 3;
     flags[2 * z + 1] = (h[z] >> 2) & 3;
   }
+  return HGPU_OK;
+}
+
+extern "C" int hgpu_download_failfloorcount(hgpu_ctx *x, long long *counts, int clear) {
+  if (!x || !counts) return HGPU_E_INVALID;
+  const long long nz = x->d.nz;
+  std::vector<unsigned int> h((size_t)(NFFC * nz));
+  CUDA_TRY(cudaMemcpyAsync(h.data(), x->ffc, sizeof(unsigned int) * NFFC * nz, cudaMemcpyDeviceToHost, x->stream));
+  if (clear) CUDA_TRY(cudaMemsetAsync(x->ffc, 0, sizeof(unsigned int) * NFFC * nz, x->stream));
+  CUDA_TRY(cudaStreamSynchronize(x->stream));
+  for (long long z = 0; z < nz; z++)
+    for (int c = 0; c < NFFC; c++) counts[z * NFFC + c] = (long long)h[(size_t)(c * nz + z)];
   return HGPU_OK;
 }
 

@@ -39,11 +39,16 @@
  *                             loops that never modify p between steps);
  *                             results are still copied back every step
  *
- * Restart dumps: the reference's restart_write (restart.c:206) is kept as
- * harm_cpu_restart_write (a one-token rename of restart.c:206, done by the
- * same build step) and wrapped below: unew, which the host arrays do not
- * receive after every step for the non-finite-volume schemes, is copied
- * from the device first, so the file holds what a CPU run writes.
+ * Restart dumps and diagnostics: the reference's restart_write
+ * (restart.c:206), diag (diag.c:9) and dump_ener (dump_ener.c:3) are kept as
+ * harm_cpu_restart_write, harm_cpu_diag and harm_cpu_dump_ener (one-token
+ * renames, done by the same build step) and wrapped below.  Before any of
+ * them runs, the device's failure and floor counters since the last call
+ * are added to the reference's failfloorcount (every time scale, as
+ * diag_fixup increments them, fixup.c:206), and restart_write first copies
+ * unew from the device (the host arrays do not receive it after every step
+ * for the non-finite-volume schemes), so dumps, ener.out's counters and
+ * the restart file hold what a CPU run writes.
  *
  * Errors: a failing hgpu_* call prints hgpu_last_error() to the reference's
  * fail_file and step_ch returns 1, which the reference's MYFUN/error_check
@@ -59,6 +64,7 @@ static hgpu_ctx *g_ctx;
 static int g_ng, g_g[4], g_nt[4], g_gt[3];
 static double *g_p, *g_u;
 static int *g_pflag, *g_bsq;
+static long long *g_ffc;
 static int g_resident, g_uploaded;
 
 #define CHECK(call)                                                                            \
@@ -214,6 +220,13 @@ static int setup(void)
     dualfprintf(fail_file, "step_ch_gpu: pinned host buffers: %s\n", hgpu_last_error());
     return 1;
   }
+#if(DODEBUG)
+  g_ffc = (long long *)malloc(sizeof(long long) * 9 * (size_t)nz);
+  if (!g_ffc) {
+    dualfprintf(fail_file, "step_ch_gpu: out of host memory for the counters\n");
+    return 1;
+  }
+#endif
   if (upload_geometry()) return 1;
   g_resident = res && atoi(res) != 0;
   trifprintf("step_ch_gpu: %dx%dx%d zones, %d ghosts on the device, %s\n", N1, N2, N3, g_ng,
@@ -268,11 +281,45 @@ int step_ch(void)
 }
 
 extern int harm_cpu_restart_write(long dump_cnt);
+extern int harm_cpu_diag(int call_code);
+extern int harm_cpu_dump_ener(int doener, int dordump, int call_code);
+
+/* the device's failure and floor counters since the last call, added to
+   failfloorcount of every time scale (the device's categories are the
+   reference's, global.h:769-779; active zones) and cleared on the device */
+static int sync_counters(void)
+{
+#if(DODEBUG)
+  int i, j, k, c, tscale;
+  if (!g_ctx || !g_ffc) return 0;
+  CHECK(hgpu_download_failfloorcount(g_ctx, g_ffc, 1));
+  ZLOOP {
+    const long long *n = g_ffc + 9 * zone_index(i, j, k);
+    for (c = 0; c < NUMFAILFLOORFLAGS && c < 9; c++)
+      if (n[c]) TSCALELOOP(tscale) failfloorcount[i][j][k][tscale][c] += (CTYPE)n[c];
+  }
+#endif
+  return 0;
+}
+
+/* diag (diag.c:9) and dump_ener (dump_ener.c:3) with the device's counters */
+int diag(int call_code)
+{
+  if (sync_counters()) return 1;
+  return harm_cpu_diag(call_code);
+}
+
+int dump_ener(int doener, int dordump, int call_code)
+{
+  if (sync_counters()) return 1;
+  return harm_cpu_dump_ener(doener, dordump, call_code);
+}
 
 /* restart_write (restart.c:206-235) with the device's unew (the conserved
    state after the last step; rdump_content writes p and unew) */
 int restart_write(long dump_cnt)
 {
+  if (sync_counters()) return 1;
   if (g_ctx && DOENOFLUX != ENOFINITEVOLUME) {
     int i, j, k, pl;
     CHECK(hgpu_download_conserved(g_ctx, g_p));

@@ -114,6 +114,7 @@ def load_library(path=None):
     L.hgpu_download_bsqflags.argtypes = [ctypes.c_void_p, _ip]
     L.hgpu_reconfigure.argtypes = [ctypes.c_void_p, _P(hgpu_config)]
     L.hgpu_upload_conserved.argtypes = [ctypes.c_void_p, _dp]
+    L.hgpu_download_failfloorcount.argtypes = [ctypes.c_void_p, _P(ctypes.c_longlong), ctypes.c_int]
     L.hgpu_write_rdump.argtypes = [ctypes.c_void_p, ctypes.c_char_p, ctypes.c_void_p, ctypes.c_size_t, ctypes.c_int]
     L.hgpu_read_rdump.argtypes = [ctypes.c_void_p, ctypes.c_char_p, ctypes.c_size_t, ctypes.c_int, ctypes.c_double,
                                   ctypes.c_double]
@@ -151,7 +152,7 @@ def load_library(path=None):
                  "hgpu_advance_stage", "hgpu_fluxcalc", "hgpu_bound_prim", "hgpu_utoprim_batch", "hgpu_utoprimgen_batch",
                  "hgpu_device_prims", "hgpu_sync", "hgpu_create_batch", "hgpu_batch_layout", "hgpu_batch_status",
                  "hgpu_step_graph", "hgpu_autotune", "hgpu_set_tuning", "hgpu_batch_run", "hgpu_diagnostics", "hgpu_download_conserved", "hgpu_upload_conserved",
-                 "hgpu_write_rdump", "hgpu_read_rdump", "hgpu_server_create", "hgpu_server_submit", "hgpu_server_submit_borrowed",
+                 "hgpu_write_rdump", "hgpu_read_rdump", "hgpu_download_failfloorcount", "hgpu_server_create", "hgpu_server_submit", "hgpu_server_submit_borrowed",
                  "hgpu_server_poll", "hgpu_server_result", "hgpu_server_release", "hgpu_halo_bytes", "hgpu_halo_pack",
                  "hgpu_halo_unpack", "hgpu_stats_clear", "hgpu_stats_read", "hgpu_stage_advance", "hgpu_stage_fixup",
                  "hgpu_dt_probe", "hgpu_step_end", "hgpu_ndt_pack", "hgpu_ndt_unpack", "hgpu_stream"):
@@ -309,6 +310,13 @@ class HarmGPU:
         f = np.zeros(self.nt + (2,), dtype=np.int32)
         _check(self.L, self.L.hgpu_download_bsqflags(self.h, _ptr(f, ctypes.c_int)))
         return f
+
+    def download_failfloorcount(self, clear=False):
+        """hgpu_download_failfloorcount: int64 [n1+2g][n2+2g][n3+2g][9], the
+        reference's failfloorcount categories per zone."""
+        c = np.zeros(self.nt + (9,), dtype=np.int64)
+        _check(self.L, self.L.hgpu_download_failfloorcount(self.h, _ptr(c, ctypes.c_longlong), int(bool(clear))))
+        return c
 
     def write_rdump(self, path, header=b"", binary=False):
         """hgpu_write_rdump: the reference's restart dump of the current state

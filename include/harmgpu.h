@@ -33,7 +33,7 @@
 extern "C" {
 #endif
 
-#define HGPU_ABI_VERSION 10
+#define HGPU_ABI_VERSION 11
 
 /* return codes */
 #define HGPU_OK 0
@@ -283,6 +283,25 @@ int hgpu_download_conserved(hgpu_ctx *ctx, double *unew);
    zone of the host zone layout, as the last stage of the last step left
    them (0 before the first step).  Not produced for batches of 1D problems. */
 int hgpu_download_bsqflags(hgpu_ctx *ctx, int *flags);
+
+/* Failure and floor counters per zone (the reference's failfloorcount,
+   fixup.c:206, incremented by diag_fixup): counts[z*9 + c], zones in the
+   primitives' host layout, c the categories COUNTUTOPRIMFAILCONV 0,
+   COUNTFLOORACT 1, COUNTLIMITGAMMAACT 2, COUNTINFLOWACT 3,
+   COUNTUTOPRIMFAILRHONEG 4, COUNTUTOPRIMFAILUNEG 5, COUNTUTOPRIMFAILRHOUNEG 6,
+   COUNTGAMMAPERC 7, COUNTUPERC 8 (global.h:769-779): the number of times
+   since hgpu_create / hgpu_reconfigure or the last clearing download
+   (uploading a state does not reset them: a host that uploads before every
+   step, as the drop-in step_ch does, accumulates them over its steps) that
+   fixup1zone
+   floored the zone or limited its Lorentz factor (fixup.c:408, 443, 1913),
+   that fixup_utoprim limited the averaged state's Lorentz factor
+   (fixup.c:1326) and that it reset a failure of each type to fixed
+   (fixup.c:1340-1428).  Active zones only: the inflow checks of the
+   boundaries (COUNTINFLOWACT) and the limit_gamma there count ghost zones,
+   which no output of the reference reads, and are not kept.  clear != 0
+   zeroes the counters after the copy. */
+int hgpu_download_failfloorcount(hgpu_ctx *ctx, long long *counts, int clear);
 
 /* Set the conserved state unew from the host (same layout), as the
    reference's restart reads unew (restart.c:256-270).  A HGPU_ENOFINITEVOLUME

@@ -208,8 +208,9 @@ def build(ref, n1, n2, n3, lim, flux, cour, maxbnd, name=None, keep=False, verbo
     """gpu_shim: link the drop-in GPU step_ch (harm_finalwham_b200/dropin/step_ch_gpu.c
     against lib/libharmgpu.so) in place of the reference's own, which is kept
     as harm_cpu_step_ch (the only change to step_ch.c: the name at :16); the
-    shim's restart_write wraps the reference's, kept as
-    harm_cpu_restart_write (the name at restart.c:206)."""
+    shim's restart_write, diag and dump_ener wrap the reference's, kept as
+    harm_cpu_restart_write, harm_cpu_diag and harm_cpu_dump_ener (the names
+    at restart.c:206, diag.c:9, dump_ener.c:3)."""
     os.makedirs(OUT, exist_ok=True)
     name = name or (f"harm_ref_{n1}x{n2}x{n3}_{lim}_{flux}" + (f"_rk{timeorder}" if timeorder != 2 else "")
                     + ("_jon" if utoprim == "JON" else "") + ("_fv" if fv else "")
@@ -265,15 +266,20 @@ def build(ref, n1, n2, n3, lim, flux, cour, maxbnd, name=None, keep=False, verbo
             t = sub_once(t, "int step_ch(void)\n{", "int harm_cpu_step_ch(void)\n{", where="step_ch.c")
             with open(p, "w") as f:
                 f.write(t)
-            # restart_write (restart.c:206) too: the shim's restart_write
-            # brings unew from the device first, then calls it
-            p = os.path.join(scratch, "restart.c")
-            with open(p) as f:
-                t = f.read()
-            t = sub_once(t, "int restart_write(long dump_cnt)\n{", "int harm_cpu_restart_write(long dump_cnt)\n{",
-                         where="restart.c")
-            with open(p, "w") as f:
-                f.write(t)
+            # restart_write (restart.c:206), diag (diag.c:9) and dump_ener
+            # (dump_ener.c:3) too: the shim's versions bring unew and the
+            # failure/floor counters from the device first, then call them
+            for fname, old, new in (
+                    ("restart.c", "int restart_write(long dump_cnt)\n{", "int harm_cpu_restart_write(long dump_cnt)\n{"),
+                    ("diag.c", "int diag(int call_code)\n{", "int harm_cpu_diag(int call_code)\n{"),
+                    ("dump_ener.c", "int dump_ener(int doener, int dordump, int call_code)\n{",
+                     "int harm_cpu_dump_ener(int doener, int dordump, int call_code)\n{")):
+                p = os.path.join(scratch, fname)
+                with open(p) as f:
+                    t = f.read()
+                t = sub_once(t, old, new, where=fname)
+                with open(p, "w") as f:
+                    f.write(t)
             shutil.copy(SHIM, os.path.join(scratch, "step_ch_gpu.c"))
             srcs = srcs + ["step_ch_gpu.c"]
             extra = ["-I" + os.path.join(REPO, "include"), "-L" + GPULIB, "-lharmgpu",

@@ -178,6 +178,10 @@ class RefDump:
     def unew(self, tag):
         return self._f(tag, "unew").reshape(self.NM + (NPR,))
 
+    def ffc(self, tag):
+        """failfloorcount of the first time scale: [N1M][N2M][N3M][9]."""
+        return self._f(tag, "ffc").reshape(self.NM + (9,))
+
     def pk(self, tag):
         return self._f(tag, "pk").reshape((2,) + self.NM + (NPR,))
 

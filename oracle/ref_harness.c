@@ -34,6 +34,10 @@
  *                      a line to ener.out in the working directory (t,
  *                      realnstep, the conserved integrals, ..., divbmax,
  *                      divbavg).
+ *   --ffc              with every state dump also writes the reference's
+ *                      failure and floor counters per zone (failfloorcount
+ *                      of the first time scale, fixup.c:206; all zones with
+ *                      ghosts, 9 categories, doubles as CTYPE is).
  *   --rdump            calls the reference's own restart_write(0)
  *                      (restart.c:206) after the last step, which writes
  *                      dumps/rdump-0 in the working directory (its header,
@@ -59,6 +63,7 @@ static char outdir[1024];
 static int geomplane = 0;
 static int do_ener = 0;
 static int do_rdump = 0;
+static int do_ffc = 0;
 extern int restart_write(long dump_cnt);
 extern int dump_ener(int doener, int dordump, int call_code);
 
@@ -157,6 +162,18 @@ static void dump_state(const char *tag, int with_fluxes)
   write_meta(tag);
   wbin(tag, "p", a_p, sizeof(a_p));
   wbin(tag, "pflag", a_pflag, sizeof(a_pflag));
+  if (do_ffc) {
+    /* time scale 0 of failfloorcount[N1M][N2M][N3M][NUMTSCALES][NUMFAILFLOORFLAGS] */
+    const size_t nzone = (size_t)N1M * N2M * N3M;
+    double *buf = (double *)malloc(sizeof(double) * NUMFAILFLOORFLAGS * nzone);
+    const CTYPE *src = &a_failfloorcount[0][0][0][0][0];
+    size_t z;
+    int c;
+    for (z = 0; z < nzone; z++)
+      for (c = 0; c < NUMFAILFLOORFLAGS; c++) buf[z * NUMFAILFLOORFLAGS + c] = (double)src[z * NUMTSCALES * NUMFAILFLOORFLAGS + c];
+    wbin(tag, "ffc", buf, sizeof(double) * NUMFAILFLOORFLAGS * nzone);
+    free(buf);
+  }
   if (!with_fluxes) wbin(tag, "unew", a_unew, sizeof(a_unew)); /* the conserved state after init */
   if (with_fluxes) {
     wbin(tag, "pk", a_pk, sizeof(a_pk));
@@ -303,6 +320,10 @@ int main(int argc, char *argv[])
       do_ener = 1;
       argv += 1;
       argc -= 1;
+    } else if (strcmp(argv[1], "--ffc") == 0) {
+      do_ffc = 1;
+      argv += 1;
+      argc -= 1;
     } else if (strcmp(argv[1], "--rdump") == 0) {
       do_rdump = 1;
       argv += 1;
@@ -313,7 +334,7 @@ int main(int argc, char *argv[])
     }
   }
   if (argc < 3) {
-    fprintf(stderr, "usage: %s [--phimodes seed] [--geomplane] [--ener] [--rdump] <outdir|-> <nsteps> [dumpstep ...]\n", argv[0]);
+    fprintf(stderr, "usage: %s [--phimodes seed] [--geomplane] [--ener] [--rdump] [--ffc] <outdir|-> <nsteps> [dumpstep ...]\n", argv[0]);
     return 2;
   }
   /* outdir "-" runs the steps for timing only and writes nothing */
@@ -357,11 +378,12 @@ int main(int argc, char *argv[])
     for (d = 0; d < ndump; d++) if (dumps[d] == s) want = 1;
     if (want) {
       snprintf(tag, sizeof(tag), "s%d", s);
-      dump_state(tag, 1);
+      /* dump_ener reads the state and the counters and writes ener.out only */
       if (do_ener && dump_ener(1, 0, DUMP_OUT) >= 1) {
         fprintf(stderr, "harness: dump_ener failed at step %d\n", s);
         return 1;
       }
+      dump_state(tag, 1);
     }
   }
   if (do_rdump) {

@@ -41,9 +41,12 @@ def load(name):
                    nstroke=float(d[f"nstroke_s{s}"]), u=d[f"u_s{s}"] if f"u_s{s}" in d else None,
                    unew=d[f"u_s{s}"] if f"u_s{s}" in d else (d[f"unew_s{s}"] if f"unew_s{s}" in d else None),
                    bsq=d[f"bsq_s{s}"] if f"bsq_s{s}" in d else None,
+                   ffc=d[f"ffc_s{s}"] if f"ffc_s{s}" in d else None,
                    ener=d[f"ener_s{s}"] if f"ener_s{s}" in d else None) for s in steps}
     # the reference's ener.out line at init (dump_ener.c:287-295)
     pr.ener_init = d["ener_init"] if "ener_init" in d else None
+    # the reference's failure and floor counters per zone at init
+    pr.ffc_init = d["ffc_init"] if "ffc_init" in d else None
     # the reference's restart dump after the last step (restart_write), bytes
     pr.rdump = d["rdump"].tobytes() if "rdump" in d else None
     return pr, ref

@@ -108,7 +108,7 @@ def make(name, spec, ref):
                           beta=opts.get("beta"))
     with tempfile.TemporaryDirectory() as tmp:
         out = os.path.join(tmp, "out")
-        subprocess.run([exe, "--ener"] + hargs + [out, str(nsteps)] + [str(s) for s in dumps], cwd=tmp,
+        subprocess.run([exe, "--ener", "--ffc"] + hargs + [out, str(nsteps)] + [str(s) for s in dumps], cwd=tmp,
                        check=True, stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL)
         rd = RefDump(out)
         pr = rd.to_problem(ng, "init")
@@ -127,6 +127,9 @@ def make(name, spec, ref):
         if fv:
             data["u_init"] = pr.u
         data["ener_init"] = ener[0]
+        # the reference's failure and floor counters per zone (failfloorcount,
+        # fixup.c:206): at init (fixup at init counts too) and after each dump
+        data["ffc_init"] = rd.crop(rd.ffc("init"), ng).astype(np.int32)
         for n_, s in enumerate(sorted(set(dumps) | {nsteps})):
             data[f"ener_s{s}"] = ener[1 + n_]
         for s in dumps:
@@ -135,6 +138,7 @@ def make(name, spec, ref):
             data[f"pflag_s{s}"] = rd.crop(rd.pflag(f"s{s}"), ng)[..., 0]
             # the b^2/rho and b^2/u flags of pre_fixup (FLAGBSQORHO, FLAGBSQOU)
             data[f"bsq_s{s}"] = rd.crop(rd.pflag(f"s{s}"), ng)[..., 2:4]
+            data[f"ffc_s{s}"] = rd.crop(rd.ffc(f"s{s}"), ng).astype(np.int32)
             data[f"t_s{s}"] = m["t"]
             data[f"dt_s{s}"] = m["dt"]
             data[f"nstroke_s{s}"] = m["nstroke"]

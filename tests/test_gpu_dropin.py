@@ -58,19 +58,26 @@ def test_reference_loop_on_gpu_matches_golden(binary, fixture, args):
     pr, ref = load(fixture)
     steps = sorted(ref)
     # --rdump: the reference's own restart_write after the last step, through
-    # the shim's wrapper that brings unew from the device
-    tmp, rd = run_shim(binary, steps[-1], steps[:-1], ["--rdump"] + list(args))
+    # the shim's wrapper that brings unew from the device (a run without
+    # dump_ener, as the fixture's dump was made)
+    tmp, rd = run_shim(binary, steps[-1], [], ["--rdump"] + list(args))
     with tmp:
         with open(os.path.join(tmp.name, "dumps", "rdump-0"), "rb") as f:
             assert f.read() == pr.rdump, "the restart dump differs from the reference's"
+    # --ener --ffc: dump_ener, whose wrapper adds the device's failure and
+    # floor counters to the reference's failfloorcount, before every dump
+    tmp, rd = run_shim(binary, steps[-1], steps[:-1], ["--ener", "--ffc"] + list(args))
+    with tmp:
         for s in steps:
             tag = f"s{s}"
             r = ref[s]
             assert same(rd.crop(rd.p(tag), pr.ng), r["p"]), f"primitives differ after step {s}"
             assert np.array_equal(rd.crop(rd.pflag(tag), pr.ng)[..., 0], r["pflag"])
             assert np.array_equal(rd.crop(rd.pflag(tag), pr.ng)[..., 2:4], r["bsq"])
+            act = pr.active
+            assert np.array_equal(act(rd.crop(rd.ffc(tag), pr.ng)), act(r["ffc"])), \
+                f"failure/floor counters differ after step {s}"
             m = rd.meta_of(tag)
             assert m["t"] == r["t"] and m["dt"] == r["dt"] and m["nstroke"] == r["nstroke"]
             if r["u"] is not None:
-                act = pr.active
                 assert same(act(rd.crop(rd.unew(tag), pr.ng)), act(r["u"])), f"unew differs after step {s}"

@@ -35,6 +35,24 @@ def test_step_ch_bit_identical_to_reference(name):
 
 
 @pytest.mark.parametrize("name", CASES)
+def test_failure_floor_counters_match_reference(name):
+    # failfloorcount (fixup.c:206) per zone and category: the reference's
+    # counts after each dumped step less its counts at init (init's own
+    # fixup counts too; the device starts from zero at upload)
+    pr, ref = load(name)
+    with HarmGPU.from_problem(pr) as g:
+        done = 0
+        for s in sorted(ref):
+            g.step_ch(s - done)
+            done = s
+            c = g.active(g.download_failfloorcount())
+            want = g.active(ref[s]["ffc"]) - g.active(pr.ffc_init)
+            bad = np.argwhere(c != want)
+            assert bad.size == 0, (f"{len(bad)} counters differ after step {s}, first (i, j, k, category) "
+                                   f"{tuple(bad[0])}: {c[tuple(bad[0])]} vs {want[tuple(bad[0])]}")
+
+
+@pytest.mark.parametrize("name", CASES)
 def test_newton_iterations_match_reference(name):
     pr, ref = load(name)
     with HarmGPU.from_problem(pr) as g:
