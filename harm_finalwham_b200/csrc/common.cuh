@@ -59,6 +59,8 @@ struct Params {
   // failure and floor counters per zone, NFFC planes of nz (failfloorcount,
   // fixup.c:206): incremented where the reference's diag_fixup counts
   unsigned int *ffc;
+  // Bondi-integral x1 boundaries: [2][g1+1][n2][49] coordinate data (nullptr: none)
+  const double *bondi;
 };
 
 // counter categories (global.h:769-779)

@@ -45,6 +45,7 @@ constexpr int ERR_VCHAR_DISCR = 8;
 constexpr int ERR_VSQ_NEG = 16;
 constexpr int ERR_NONFINITE_SPEED = 32;
 constexpr int ERR_PREF_NEG = 64;
+constexpr int ERR_BONDI = 128;  // bondi_invert_integrals' myexit (bounds.c:1040-1066)
 
 // Tolerances of the reference's round-off guards, per arithmetic type.  The
 // FP64 values are the reference's own (NUMEPSILON = DBL_EPSILON, global.h);

@@ -469,15 +469,24 @@ __global__ void __launch_bounds__(128, MB) invert_kernel(Dims d, Params P, Box b
 // ---------------------------------------------------------------------------
 // boundaries: bound_prim_user (bounds.fishmon.c:29-345)
 // ---------------------------------------------------------------------------
+__device__ __forceinline__ bool is_polar(int bc) { return bc == HGPU_BC_POLARAXIS || bc == HGPU_BC_POLARAXIS_FLIP; }
+__device__ __forceinline__ bool is_bondi(int bc) {
+  return bc == HGPU_BC_BONDIINTOUTFLOW || bc == HGPU_BC_BONDIMDOTOUTFLOW;
+}
+
+// Source index of a ghost zone along one direction.  The Bondi-integral
+// ghosts are computed (bondi_bc_kernel), so they are their own source.
 __device__ __forceinline__ int map_idx(int i, int n, int bcdn, int bcup) {
   if (i < 0) {
     if (bcdn == HGPU_BC_PERIODIC) return i + n;
-    if (bcdn == HGPU_BC_POLARAXIS) return -i - 1;
+    if (is_polar(bcdn)) return -i - 1;
+    if (is_bondi(bcdn)) return i;
     return 0;  // OUTFLOW
   }
   if (i >= n) {
     if (bcup == HGPU_BC_PERIODIC) return i - n;
-    if (bcup == HGPU_BC_POLARAXIS) return (n - 1) + ((n - 1) - i + 1);
+    if (is_polar(bcup)) return (n - 1) + ((n - 1) - i + 1);
+    if (is_bondi(bcup)) return i;
     return n - 1;
   }
   return i;
@@ -524,11 +533,120 @@ __device__ __forceinline__ void inflow_check_x1(const Dims &d, const Params &P, 
   pr[U3] *= gamma;
 }
 
+// Bondi-integral x1 boundaries (bounds.c:140-156, 295-308): one thread per
+// ghost zone (i, j, k) of active j, k.  The edge zone's integrals
+// (bondi_compute_integrals, bounds.c:788-836: its relative 4-velocity to
+// u^mu, metptomet to Kerr-Schild u^r, transforms.c:51-84, 310-328), carried
+// unchanged to the ghost (interpn of order 1), then the ghost's primitives
+// (bondi_generate_solution, bounds.c:839-888).  Runs before
+// bound_ghost_kernel, which takes these zones as the sources of the x2/x3
+// ghost corners.
+__device__ __forceinline__ void mat4_vec(const double *M, const double *u, double *out) {
+#pragma unroll
+  for (int j = 0; j < 4; j++) {
+    double t = 0.;
+#pragma unroll
+    for (int k = 0; k < 4; k++) t += M[4 * j + k] * u[k];
+    out[j] = t;
+  }
+}
+
+__global__ void bondi_bc_kernel(Dims d, Params P, double *p, const double *__restrict__ G, Scalars *sc) {
+  const long long per_side = (long long)d.g1 * d.n2 * d.n3;
+  long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= 2 * per_side || sc->done) return;
+  const int side = (int)(t / per_side);
+  long long r = t % per_side;
+  const int k = (int)(r % d.n3);
+  r /= d.n3;
+  const int j = (int)(r % d.n2);
+  const int q = 1 + (int)(r / d.n2);
+  if (side == 0 && P.bc[1] != HGPU_BC_BONDIINTOUTFLOW) return;
+  if (side == 1 && P.bc[0] != HGPU_BC_BONDIMDOTOUTFLOW) return;
+  const int i0 = side == 0 ? 0 : d.n1 - 1;
+  const int i = side == 0 ? -q : d.n1 - 1 + q;
+  const double *e = P.bondi + ((long long)(side * (d.g1 + 1)) * d.n2 + j) * 49;
+  const double *g = P.bondi + ((long long)(side * (d.g1 + 1) + q) * d.n2 + j) * 49;
+  const double gam = P.gam;
+  const double n = 1 / (gam - 1);
+  int err = 0;
+  // the edge zone's integrals
+  double pr0[NPR];
+  load_prim(p, d, zix(d, i0, j, k), pr0);
+  Metric m0;
+  load_metric(G, d, gix(d, i0, j), G_CENT, m0);
+  double ucp[4], uks[4];
+  if (ucon_calc(pr0, m0, ucp)) err |= ERR_UTCALC_DISCR;
+  mat4_vec(e + 1, ucp, uks);
+  const double pres = (gam - 1) * pr0[UU];
+  const double T = pres / pr0[RHO];
+  const double re = e[0];
+  double C1 = pow(T, n) * uks[1] * re * re;
+  double C2 = pow(1 + (1 + n) * T, 2.) * (1 - 2. / re + uks[1] * uks[1]);
+  double K = pres / pow(pr0[RHO], gam);
+  if (side == 1) {
+    C2 = 1.373125;  // bounds.c:48-49 (bondigrid4acc.nb)
+    K = 1.;
+  }
+  // bondi_invert_integrals at the ghost's radius
+  const double rg = g[0];
+  double T0 = 0.2, T1 = 0.1;
+  int it = 0;
+  if (rg > 0.35 && rg < 2.5) {
+    for (; it < 250 && fabs((T0 - T1) / T1) > 1.0e-15; it++) {
+      T0 = T1;
+      const double u1 = C1 / (rg * rg * pow(T0, n));
+      T1 = T0 + 0.02 * (T0 - (sqrt(C2 / (1 - 2 / rg + u1 * u1)) - 1) / (1 + n));
+    }
+  } else if (rg > 9) {
+    for (; it < 250 && (T0 - T1) / T1 > 1.0e-15; it++) {
+      T0 = T1;
+      const double u1 = C1 / (rg * rg * pow(T0, n));
+      T1 = (sqrt(C2 / (1 - 2 / rg + u1 * u1)) - 1) / (1 + n);
+    }
+    if (T1 > T0) err |= ERR_BONDI;
+  } else {
+    err |= ERR_BONDI;
+  }
+  if (err & ERR_BONDI) {
+    atomicOr(&sc->err, err);
+    return;
+  }
+  double pr[NPR];
+#pragma unroll
+  for (int v = 0; v < NPR; v++) pr[v] = 0.0;
+  pr[RHO] = pow(T1 / K, n);
+  pr[UU] = pr[RHO] * T1 * n;
+  // u^t from the Kerr-Schild metric (pr2ucon VEL4: get_4velterms, phys.c:1192-1262)
+  const double *gk = g + 33;
+  double uc[4] = {0., C1 / (pow(T1, n) * rg * rg), 0., 0.};
+  const double AA = gk[0];
+  const double BB = 2. * (gk[1] * uc[1] + gk[2] * uc[2] + gk[3] * uc[3]);
+  const double CCM1 = gk[5] * uc[1] * uc[1] + gk[10] * uc[2] * uc[2] + gk[15] * uc[3] * uc[3] +
+                      2. * (gk[6] * uc[1] * uc[2] + gk[7] * uc[1] * uc[3] + gk[11] * uc[2] * uc[3]);
+  const double discr = BB * BB - 4. * AA * (CCM1 + 1.0);
+  if (discr < 0.) err |= ERR_UTCALC_DISCR;
+  uc[0] = (-BB - sqrt(discr)) / (2. * AA);
+  // to the internal coordinates (mettometpface) and the relative 4-velocity (ucon2pr VELREL4)
+  double ucp2[4];
+  mat4_vec(g + 17, uc, ucp2);
+  Metric mg;
+  load_metric(G, d, gix(d, i, j), G_CENT, mg);
+  const double alphasq = 1. / (-GCON(mg, 0, 0));
+  pr[U1] = ucp2[1] + (alphasq * GCON(mg, 0, 1)) * ucp2[0];
+  pr[U2] = ucp2[2] + (alphasq * GCON(mg, 0, 2)) * ucp2[0];
+  pr[U3] = ucp2[3] + (alphasq * GCON(mg, 0, 3)) * ucp2[0];
+  store_prim(p, d, zix(d, i, j, k), pr);
+  if (err) atomicOr(&sc->err, err);
+}
+
 // Every ghost zone of the full box as the composition of the reference's
 // sequential fills: x1 (active j,k: copy + inflow check + gamma limit with the
-// ghost's own metric), then x2 (full i, active k: reflection, POLEDEATH
-// zeroing of u~2 and B2), then x3 (full i, full j: periodic copy).  Reads only
-// active zones, which this kernel does not write.
+// ghost's own metric; the Bondi-integral ghosts come from bondi_bc_kernel),
+// then x2 (full i, active k: reflection, and either POLEDEATH zeroing of u~2
+// and B2 (bounds.fishmon.c) or their negation (the generic bounds.c,
+// HGPU_BC_POLARAXIS_FLIP)), then x3 (full i, full j: periodic copy).  Reads
+// only zones this kernel does not write.
 __global__ void __launch_bounds__(128) bound_ghost_kernel(Dims d, Params P, double *p, const double *__restrict__ G,
                                                           Scalars *sc) {
   long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -539,12 +657,19 @@ __global__ void __launch_bounds__(128) bound_ghost_kernel(Dims d, Params P, doub
   int i = (int)(r / d.nt2) - d.g1;
   bool gi = (i < 0 || i >= d.n1), gj = (j < 0 || j >= d.n2), gk = (k < 0 || k >= d.n3);
   if (!(gi || gj || gk)) return;
+  // x1 ghosts of active j, k on a Bondi-integral side: bondi_bc_kernel's
+  if (gi && !gj && !gk && is_bondi(i < 0 ? P.bc[1] : P.bc[0])) return;
   int si = map_idx(i, d.n1, P.bc[1], P.bc[0]);
   int sj = map_idx(j, d.n2, P.bc[3], P.bc[2]);
   int sk = map_idx(k, d.n3, P.bc[5], P.bc[4]);
   double pr[NPR];
   load_prim(p, d, zix(d, si, sj, sk), pr);
   int err = 0;
+  // the generic bounds.c's polar reflection (bounds.c:477-489)
+  if (gj && ((j < 0 && P.bc[3] == HGPU_BC_POLARAXIS_FLIP) || (j >= d.n2 && P.bc[2] == HGPU_BC_POLARAXIS_FLIP))) {
+    pr[U2] *= -1.;
+    pr[B2] *= -1.;
+  }
   if (gi && (P.bc[1] == HGPU_BC_OUTFLOW || P.bc[0] == HGPU_BC_OUTFLOW) &&
       ((i < 0 && P.bc[1] == HGPU_BC_OUTFLOW) || (i >= d.n1 && P.bc[0] == HGPU_BC_OUTFLOW))) {
     Metric m;
@@ -1294,6 +1419,7 @@ struct hgpu_ctx {
   double *w5pu = nullptr;               // WENO5: per-zone dP/P state pieces (2 planes)
   unsigned char *bsqf = nullptr;        // FLAGBSQORHO | FLAGBSQOU << 2 per zone
   unsigned int *ffc = nullptr;          // failure/floor counters, NFFC planes
+  double *bondi_tab = nullptr;          // Bondi-integral boundaries' coordinate data
   double *progress = nullptr;                          // 4 doubles for hg_progress_async
   W5Tile w5[4];  // WENO5 tiling per direction
   Box w5_state_box;  // zones whose dP/P state pieces some direction reads
@@ -1374,8 +1500,12 @@ static int validate(const hgpu_config *c) {
   if (c->fluxmethod != HGPU_FLUX_HLL && c->fluxmethod != HGPU_FLUX_LAXF) return HGPU_E_INVALID;
   for (int f = 0; f < 6; f++)
     if (c->bc[f] != HGPU_BC_OUTFLOW && c->bc[f] != HGPU_BC_POLARAXIS && c->bc[f] != HGPU_BC_PERIODIC &&
-        c->bc[f] != HGPU_BC_OUTFLOW_COPY)
+        c->bc[f] != HGPU_BC_OUTFLOW_COPY && c->bc[f] != HGPU_BC_POLARAXIS_FLIP &&
+        !(f == 0 && c->bc[f] == HGPU_BC_BONDIMDOTOUTFLOW) && !(f == 1 && c->bc[f] == HGPU_BC_BONDIINTOUTFLOW))
       return HGPU_E_INVALID;
+  // the Bondi-integral boundaries: x1 ghosts exist, and the edge zone's
+  // integrals come from the zone itself
+  if ((c->bc[0] == HGPU_BC_BONDIMDOTOUTFLOW || c->bc[1] == HGPU_BC_BONDIINTOUTFLOW) && c->n1 < 2) return HGPU_E_INVALID;
   // reflections and periodic wraps read inside the active range
   if (c->n2 > 1 && c->n2 < c->ng) return HGPU_E_INVALID;
   if (c->n3 > 1 && c->n3 < c->ng) return HGPU_E_INVALID;
@@ -1407,7 +1537,7 @@ void hgpu_destroy(hgpu_ctx *x) {
   for (cudaEvent_t e : x->freelist) cudaEventDestroy(e);
   void *ptrs[] = {x->p, x->pk, x->uf, x->ucum, x->F[1], x->F[2], x->F[3], x->E, x->G, x->pflag, x->gammacheck,
                   x->cand, x->fixlist, x->cand_orig, x->cand_dec, x->candmap, x->fixvals, x->sc, x->staging, x->istaging,
-                  x->pL, x->pR, x->w5pu, x->bsqf, x->ffc, x->cell_inst, x->inst, x->progress, x->pk1, x->ui};
+                  x->pL, x->pR, x->w5pu, x->bsqf, x->ffc, x->bondi_tab, x->cell_inst, x->inst, x->progress, x->pk1, x->ui};
   for (void *q : ptrs)
     if (q) cudaFree(q);
   cudaStreamDestroy(x->stream);
@@ -1859,6 +1989,10 @@ static void launch_bound(hgpu_ctx *x, double *pv) {
     LAUNCH(x, K_BOUND_GHOST, bound_batch_kernel, grid_for(d.nz, 128), 128, d, x->P, pv, (int *)nullptr);
     return;
   }
+  if (x->P.bondi) {
+    const long long nb = 2LL * d.g1 * d.n2 * d.n3;
+    LAUNCH(x, K_BOUND_GHOST, bondi_bc_kernel, grid_for(nb, 128), 128, d, x->P, pv, x->G, x->sc);
+  }
   LAUNCH(x, K_BOUND_GHOST, bound_ghost_kernel, grid_for(d.nz, 128), 128, d, x->P, pv, x->G, x->sc);
   if (d.n2 > 1) LAUNCH(x, K_BOUND_POLE, bound_pole_kernel, grid_for(2LL * d.n1 * d.n3, 128), 128, d, x->P, pv);
 }
@@ -2019,8 +2153,19 @@ static void clear_counters(hgpu_ctx *x) {
   cudaMemsetAsync(&x->sc->nfloor, 0, sizeof(unsigned long long), x->stream);
 }
 
+// the Bondi-integral boundaries need their coordinate data before any bound
+static int boundaries_ready(const hgpu_ctx *x) {
+  const bool bondi = x->cfg.bc[0] == HGPU_BC_BONDIMDOTOUTFLOW || x->cfg.bc[1] == HGPU_BC_BONDIINTOUTFLOW;
+  if (bondi && !x->P.bondi) {
+    set_err("Bondi-integral boundaries: call hgpu_set_bondi_boundaries first");
+    return HGPU_E_INVALID;
+  }
+  return HGPU_OK;
+}
+
 int hgpu_step_ch(hgpu_ctx *x, int nsteps, hgpu_stats *stats) {
   if (!x || nsteps < 0) return HGPU_E_INVALID;
+  if (boundaries_ready(x)) return HGPU_E_INVALID;
   clear_counters(x);
   for (int n = 0; n < nsteps; n++) {
     for (int o = 0; o < num_orders(x); o++) launch_stage(x, o);
@@ -2036,6 +2181,7 @@ int hgpu_step_ch(hgpu_ctx *x, int nsteps, hgpu_stats *stats) {
 // dt and every bound from device memory, so the same graph advances any state.
 int hgpu_step_graph(hgpu_ctx *x, int nsteps, hgpu_stats *stats) {
   if (!x || nsteps < 0) return HGPU_E_INVALID;
+  if (boundaries_ready(x)) return HGPU_E_INVALID;
   if (x->profiling) {
     set_err("hgpu_step_graph: turn profiling off first");
     return HGPU_E_INVALID;
@@ -2073,6 +2219,7 @@ int hgpu_step_graph(hgpu_ctx *x, int nsteps, hgpu_stats *stats) {
 
 int hgpu_advance_stage(hgpu_ctx *x, int timeorder, double *ndt, hgpu_stats *stats) {
   if (!x || timeorder < 0 || timeorder >= num_orders(x)) return HGPU_E_INVALID;
+  if (boundaries_ready(x)) return HGPU_E_INVALID;
   clear_counters(x);
   launch_stage(x, timeorder);
   launch_finalize(x, 0);
@@ -2126,6 +2273,7 @@ int hgpu_fluxcalc(hgpu_ctx *x, int which, double *F1, double *F2, double *F3, do
 
 int hgpu_bound_prim(hgpu_ctx *x, int which) {
   if (!x || (which != 0 && which != 1)) return HGPU_E_INVALID;
+  if (boundaries_ready(x)) return HGPU_E_INVALID;
   launch_bound(x, which ? x->pk : x->p);
   CUDA_TRY(cudaGetLastError());
   CUDA_TRY(cudaStreamSynchronize(x->stream));
@@ -2358,6 +2506,7 @@ int hgpu_init_dt(hgpu_ctx *x, double *dt) {
 
 int hgpu_step_ch_timed(hgpu_ctx *x, int nsteps, float *ms, hgpu_stats *stats) {
   if (!x || nsteps < 0) return HGPU_E_INVALID;
+  if (boundaries_ready(x)) return HGPU_E_INVALID;
   cudaEvent_t a, b;
   CUDA_TRY(cudaEventCreate(&a));
   CUDA_TRY(cudaEventCreate(&b));
@@ -2836,6 +2985,8 @@ extern "C" size_t hgpu_context_bytes(const hgpu_config *c) {
   if (c->lim == HGPU_LIM_WENO5) b += 2 * plane + sizeof(double) * 2 * nz;  // pL, pR, dP/P state pieces
   if (c->timeorder >= 3) b += plane;                     // pk1
   if (c->doenoflux == HGPU_ENOFINITEVOLUME) b += plane;  // ui
+  if (c->bc[0] == HGPU_BC_BONDIMDOTOUTFLOW || c->bc[1] == HGPU_BC_BONDIINTOUTFLOW)
+    b += sizeof(double) * 2 * (size_t)((c->n1 > 1 ? c->ng : 0) + 1) * c->n2 * 49;  // Bondi boundary table
   return b;
 }
 
@@ -2893,6 +3044,21 @@ extern "C" int hgpu_download_bsqflags(hgpu_ctx *x, int *flags) {
     flags[2 * z] = h[z] & 3;
     flags[2 * z + 1] = (h[z] >> 2) & 3;
   }
+  return HGPU_OK;
+}
+
+extern "C" int hgpu_set_bondi_boundaries(hgpu_ctx *x, const double *table) {
+  if (!x || !table || x->ninst > 0) return HGPU_E_INVALID;
+  const size_t n = (size_t)2 * (x->d.g1 + 1) * x->d.n2 * 49;
+  if (!x->bondi_tab) CUDA_TRY(cudaMalloc(&x->bondi_tab, sizeof(double) * n));
+  CUDA_TRY(cudaMemcpyAsync(x->bondi_tab, table, sizeof(double) * n, cudaMemcpyHostToDevice, x->stream));
+  CUDA_TRY(cudaStreamSynchronize(x->stream));
+  x->P.bondi = x->bondi_tab;
+  // a captured step holds the parameters by value
+  if (x->graph_exec) cudaGraphExecDestroy(x->graph_exec);
+  if (x->graph) cudaGraphDestroy(x->graph);
+  x->graph_exec = nullptr;
+  x->graph = nullptr;
   return HGPU_OK;
 }
 
@@ -3006,6 +3172,7 @@ extern "C" int hgpu_stats_read(hgpu_ctx *x, hgpu_stats *stats) {
 
 extern "C" int hgpu_stage_advance(hgpu_ctx *x, int stage) {
   if (!decomposable(x) || stage < 0 || stage >= num_orders(x)) return HGPU_E_INVALID;
+  if (boundaries_ready(x)) return HGPU_E_INVALID;
   launch_stage_advance(x, stage);
   CUDA_TRY(cudaGetLastError());
   return HGPU_OK;
@@ -3013,6 +3180,7 @@ extern "C" int hgpu_stage_advance(hgpu_ctx *x, int stage) {
 
 extern "C" int hgpu_stage_fixup(hgpu_ctx *x, int stage) {
   if (!decomposable(x) || stage < 0 || stage >= num_orders(x)) return HGPU_E_INVALID;
+  if (boundaries_ready(x)) return HGPU_E_INVALID;
   launch_stage_fixup(x, stage);
   CUDA_TRY(cudaGetLastError());
   return HGPU_OK;

@@ -18,7 +18,8 @@ from . import build as _build
 NPR = 8
 LIM = {"DONOR": 0, "VANL": 1, "MINM": 2, "MC": 3, "PARA": 4, "WENO5": 9}
 FLUX = {"LAXF": 0, "HLL": 1}
-BC = {"OUTFLOW": 0, "POLARAXIS": 4, "PERIODIC": 7, "OUTFLOW_COPY": 1000}
+BC = {"OUTFLOW": 0, "POLARAXIS": 4, "PERIODIC": 7, "OUTFLOW_COPY": 1000, "POLARAXIS_FLIP": 1001,
+      "BONDIMDOTOUTFLOW": 109, "BONDIINTOUTFLOW": 110}
 PREC = {"fp64": 0, "mixed": 1}
 UTOPRIM = {"2DFINAL": 6, "JON": 8, "JONNONRELCOMPAT": 8}
 DOENOFLUX = {"NOENOFLUX": 0, "ENOFINITEVOLUME": 3}
@@ -114,6 +115,7 @@ def load_library(path=None):
     L.hgpu_download_bsqflags.argtypes = [ctypes.c_void_p, _ip]
     L.hgpu_reconfigure.argtypes = [ctypes.c_void_p, _P(hgpu_config)]
     L.hgpu_upload_conserved.argtypes = [ctypes.c_void_p, _dp]
+    L.hgpu_set_bondi_boundaries.argtypes = [ctypes.c_void_p, _dp]
     L.hgpu_download_failfloorcount.argtypes = [ctypes.c_void_p, _P(ctypes.c_longlong), ctypes.c_int]
     L.hgpu_write_rdump.argtypes = [ctypes.c_void_p, ctypes.c_char_p, ctypes.c_void_p, ctypes.c_size_t, ctypes.c_int]
     L.hgpu_read_rdump.argtypes = [ctypes.c_void_p, ctypes.c_char_p, ctypes.c_size_t, ctypes.c_int, ctypes.c_double,
@@ -152,7 +154,7 @@ def load_library(path=None):
                  "hgpu_advance_stage", "hgpu_fluxcalc", "hgpu_bound_prim", "hgpu_utoprim_batch", "hgpu_utoprimgen_batch",
                  "hgpu_device_prims", "hgpu_sync", "hgpu_create_batch", "hgpu_batch_layout", "hgpu_batch_status",
                  "hgpu_step_graph", "hgpu_autotune", "hgpu_set_tuning", "hgpu_batch_run", "hgpu_diagnostics", "hgpu_download_conserved", "hgpu_upload_conserved",
-                 "hgpu_write_rdump", "hgpu_read_rdump", "hgpu_download_failfloorcount", "hgpu_server_create", "hgpu_server_submit", "hgpu_server_submit_borrowed",
+                 "hgpu_write_rdump", "hgpu_read_rdump", "hgpu_download_failfloorcount", "hgpu_set_bondi_boundaries", "hgpu_server_create", "hgpu_server_submit", "hgpu_server_submit_borrowed",
                  "hgpu_server_poll", "hgpu_server_result", "hgpu_server_release", "hgpu_halo_bytes", "hgpu_halo_pack",
                  "hgpu_halo_unpack", "hgpu_stats_clear", "hgpu_stats_read", "hgpu_stage_advance", "hgpu_stage_fixup",
                  "hgpu_dt_probe", "hgpu_step_end", "hgpu_ndt_pack", "hgpu_ndt_unpack", "hgpu_stream"):
@@ -239,6 +241,8 @@ class HarmGPU:
                 gammamax=pr.gammamax, gammafail=pr.gammafail, timeorder=getattr(pr, "timeorder", 2),
                 utoprim=getattr(pr, "utoprim", "2DFINAL"), doenoflux=getattr(pr, "doenoflux", "NOENOFLUX"))
         o.upload_geometry(pr.gcov, pr.gcon, pr.gcovpert, pr.gdet, pr.conn, pr.floors)
+        if getattr(pr, "bondi_bc", None) is not None:
+            o.set_bondi_boundaries(pr.bondi_bc)
         o.upload_state(pr.p, pr.pflag, pr.t, pr.dt)
         if getattr(pr, "u", None) is not None and o.cfg.doenoflux == DOENOFLUX["ENOFINITEVOLUME"]:
             o.upload_conserved(pr.u)
@@ -310,6 +314,15 @@ class HarmGPU:
         f = np.zeros(self.nt + (2,), dtype=np.int32)
         _check(self.L, self.L.hgpu_download_bsqflags(self.h, _ptr(f, ctypes.c_int)))
         return f
+
+    def set_bondi_boundaries(self, table):
+        """hgpu_set_bondi_boundaries: [2][ng+1][n2][49] coordinate data (r,
+        dx/dx', its inverse, the Kerr-Schild metric) of the x1 edge and ghost
+        zones, for the Bondi-integral boundaries."""
+        table = _contig(table, np.float64)
+        g1 = self.g[0]
+        assert table.shape == (2, g1 + 1, self.n[1], 49)
+        _check(self.L, self.L.hgpu_set_bondi_boundaries(self.h, _ptr(table)))
 
     def download_failfloorcount(self, clear=False):
         """hgpu_download_failfloorcount: int64 [n1+2g][n2+2g][n3+2g][9], the

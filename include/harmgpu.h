@@ -33,7 +33,7 @@
 extern "C" {
 #endif
 
-#define HGPU_ABI_VERSION 11
+#define HGPU_ABI_VERSION 12
 
 /* return codes */
 #define HGPU_OK 0
@@ -59,6 +59,25 @@ extern "C" {
    bounds.fishmon.c (copy + inflow check + gamma limit); the reference uses
    id 0 for both, the problem file decides, so the copy gets its own id. */
 #define HGPU_BC_OUTFLOW_COPY 1000
+/* The generic bounds.c (the reference's test problems) gives POLARAXIS
+   another meaning than bounds.fishmon.c: the x2 ghosts mirror the active
+   zones with u~2 and B2 negated (bounds.c:477-489, POLEDEATH 0), where the
+   FM torus file zeroes them and the first/last active rows.  That variant
+   has its own id. */
+#define HGPU_BC_POLARAXIS_FLIP 1001
+/* Bondi-integral radial boundaries of the generic bounds.c (definit.h:329-330,
+   the Bondi flow, init.c's TESTNUMBER 153): each x1 ghost zone holds the
+   Bondi solution whose integrals C1 = T^n u^r r^2, C2 = (1 + (1+n) T)^2
+   (1 - 2/r + (u^r)^2), K = p / rho^gam (n = 1/(gam-1), T = p/rho, Kerr-Schild
+   u^r) are those of the first active zone (inner, BONDIINTOUTFLOW,
+   bounds.c:140-156) or C1 of the last active zone with C2 = 1.373125 and
+   K = 1 (outer, BONDIMDOTOUTFLOW, bounds.c:295-308); temperature by the
+   reference's fixed-point iteration (bounds.c:1013-1083), the field zero.
+   They need hgpu_set_bondi_boundaries.  The ghost zones agree with the
+   reference's to a few ulp, not bit for bit: the integrals use pow, whose
+   CUDA implementation rounds differently from the C library's. */
+#define HGPU_BC_BONDIMDOTOUTFLOW 109  /* x1 outer */
+#define HGPU_BC_BONDIINTOUTFLOW 110   /* x1 inner */
 
 /* con-to-prim inverters (UTOPRIMVERSION, global.h:283-287) */
 #define HGPU_UTOPRIM2DFINAL 6            /* 2D Newton on (W, v^2), utoprim_2d_final.c */
@@ -283,6 +302,18 @@ int hgpu_download_conserved(hgpu_ctx *ctx, double *unew);
    zone of the host zone layout, as the last stage of the last step left
    them (0 before the first step).  Not produced for batches of 1D problems. */
 int hgpu_download_bsqflags(hgpu_ctx *ctx, int *flags);
+
+/* Coordinate data of the Bondi-integral boundaries (HGPU_BC_BONDI*), which
+   the device does not derive from the metric it holds: table[s][q][j][49]
+   for side s (0: x1 inner, zones i = 0, -1, ..., -ng; 1: x1 outer,
+   i = n1-1, n1, ..., n1-1+ng; q = 0 is the active edge zone), active j
+   (the metric does not depend on x3), each at the zone centre: the
+   Boyer-Lindquist radius r (coord + bl_coord, coord.c:1195, 389), dx/dx'
+   [4][4] (dxdxprim, coord.c:596), its inverse [4][4] (matrix_inverse,
+   metric.c:1346) and the Kerr-Schild metric g_{mu nu} [4][4]
+   (gcov_func(0, KSCOORDS), metric.c:11).  Copied; a captured step graph is
+   dropped (it held the previous table). */
+int hgpu_set_bondi_boundaries(hgpu_ctx *ctx, const double *table);
 
 /* Failure and floor counters per zone (the reference's failfloorcount,
    fixup.c:206, incremented by diag_fixup): counts[z*9 + c], zones in the

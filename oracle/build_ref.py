@@ -187,6 +187,63 @@ def overlay_init_c(text, lim, flux, cour, timeorder=2, utoprim="2DFINAL", fv=Fal
     return text
 
 
+def overlay_bondi_h(text, n1, n2):
+    """Generic init.h (the 1D/2D test-problem header) set to the Bondi flow,
+    TESTNUMBER 153 (init.h:578-582: 16x16 by default; the resolution must be
+    one of the reference's bondigrid<N1>.dat tables)."""
+    w = "init.h"
+    text = sub_once(text, "#define TESTNUMBER 49", "#define TESTNUMBER 153", where=w)
+    i = text.index("#elif( TESTNUMBER == 153 )  // 1D Bondi problem")
+    j = text.index("#elif", i + 5)
+    block = sub_once(text[i:j], "#define NXTEST 16", f"#define NXTEST {n1}", where=w)
+    block = sub_once(block, "#define NYTEST 16", f"#define NYTEST {n2}", where=w)
+    text = text[:i] + block + text[j:]
+    # the step's scheme settings of the FM torus problem file (init.fishmon.h),
+    # which the test problems' header sets otherwise for non-FFDE tests
+    # (init.h:209-220, 274, 283-293): primitives reconstructed as they are
+    # (no rescaling, no extra interpolated quantities), checksolution on with
+    # its limits, fixup1zone on
+    k = text.rindex("#endif")
+    return text[:k] + BONDI_SCHEME_SETTINGS + text[k:]
+
+
+BONDI_SCHEME_SETTINGS = """
+/* settings overlay (oracle/build_ref.py): the FM torus file's scheme */
+#undef VARTOINTERP
+#define VARTOINTERP PRIMTOINTERP
+#undef RESCALEINTERP
+#define RESCALEINTERP 0
+#undef DOEXTRAINTERP
+#define DOEXTRAINTERP 0
+#undef CHECKSOLUTION
+#define CHECKSOLUTION 1
+#undef GAMMAPERCDIFFMAX
+#define GAMMAPERCDIFFMAX 2.0
+#undef UPERCDIFFMAX
+#define UPERCDIFFMAX 10.0
+#undef FIXUPZONES
+#define FIXUPZONES FIXUP1ZONE
+"""
+
+
+def overlay_bondi_c(text, lim, flux, cour, timeorder=2, utoprim="2DFINAL"):
+    """Generic init.c's GRMHD scheme block (init.c:915-934: WENO5BND finite
+    volume, RK4, Jon's inverter) set to a point scheme, as the FM torus
+    overlay does; everything else (grid from the bondigrid table, a = 0,
+    LOGRSINTH with hslope 1, the Bondi-integral x1 boundaries, polar x2,
+    periodic x3) is the reference's own TESTNUMBER 153 set-up."""
+    w = "init.c"
+    text = sub_once(text, "  avgscheme=WENO5BND;\n  //avgscheme=DONOR;", "  avgscheme=DONOR;\n  //avgscheme=DONOR;", where=w)
+    text = sub_once(text, "  lim = WENO5BND;\n  //lim = WENO3;", f"  lim = {LIMS[lim]};\n  //lim = WENO3;", where=w)
+    text = sub_once(text, "  TIMEORDER=4;\n  DOENOFLUX = ENOFINITEVOLUME;\n  //DOENOFLUX = NOENOFLUX;\n  fluxmethod= HLLFLUX; //LAXFFLUX;",
+                    f"  TIMEORDER={int(timeorder)};\n  DOENOFLUX = NOENOFLUX;\n  //DOENOFLUX = NOENOFLUX;\n"
+                    f"  fluxmethod= {FLUXES[flux]}; //LAXFFLUX;", where=w)
+    text = sub_once(text, "  //UTOPRIMVERSION=UTOPRIM5D1;\n \tUTOPRIMVERSION = UTOPRIMJONNONRELCOMPAT;",
+                    f"  //UTOPRIMVERSION=UTOPRIM5D1;\n \tUTOPRIMVERSION = {UTOPRIMS[utoprim]};", where=w)
+    text = sub_once(text, "  SAFE=1.3;\n  cour = 0.5;", f"  SAFE=1.3;\n  cour = {cour!r};", where=w)
+    return text
+
+
 AFTER_MPI_STUB = """
 
 /* bounds.fishmon.c has no bound_prim_user_after_mpi(); step_ch.c:bound_prim()
@@ -204,15 +261,22 @@ GPULIB = os.path.join(REPO, "harm_finalwham_b200", "lib")
 
 
 def build(ref, n1, n2, n3, lim, flux, cour, maxbnd, name=None, keep=False, verbose=False, timeorder=2,
-          utoprim="2DFINAL", fv=False, gpu_shim=False, beta=None):
+          utoprim="2DFINAL", fv=False, gpu_shim=False, beta=None, problem="fmtorus"):
     """gpu_shim: link the drop-in GPU step_ch (harm_finalwham_b200/dropin/step_ch_gpu.c
     against lib/libharmgpu.so) in place of the reference's own, which is kept
     as harm_cpu_step_ch (the only change to step_ch.c: the name at :16); the
     shim's restart_write, diag and dump_ener wrap the reference's, kept as
     harm_cpu_restart_write, harm_cpu_diag and harm_cpu_dump_ener (the names
-    at restart.c:206, diag.c:9, dump_ener.c:3)."""
+    at restart.c:206, diag.c:9, dump_ener.c:3).
+
+    problem: "fmtorus" (init.fishmon.c / init.fishmon.h / bounds.fishmon.c)
+    or "bondi" (the generic init.c / init.h / bounds.c at TESTNUMBER 153,
+    the Bondi flow with the Bondi-integral x1 boundaries, bounds.c:140-156,
+    295-308; n3 must be 1 and n1 x n2 a bondigrid table's size; the binary
+    reads bondigrid<n1>.dat from its working directory)."""
     os.makedirs(OUT, exist_ok=True)
-    name = name or (f"harm_ref_{n1}x{n2}x{n3}_{lim}_{flux}" + (f"_rk{timeorder}" if timeorder != 2 else "")
+    name = name or (("harm_bondi_" if problem == "bondi" else "harm_ref_")
+                    + f"{n1}x{n2}x{n3}_{lim}_{flux}" + (f"_rk{timeorder}" if timeorder != 2 else "")
                     + ("_jon" if utoprim == "JON" else "") + ("_fv" if fv else "")
                     + (f"_beta{beta:g}" if beta is not None else "") + ("_gpushim" if gpu_shim else ""))
     scratch = tempfile.mkdtemp(prefix="harmref_")
@@ -244,18 +308,30 @@ def build(ref, n1, n2, n3, lim, flux, cour, maxbnd, name=None, keep=False, verbo
         with open(p, "w") as f:
             f.write(t)
         # problem overlay
-        with open(os.path.join(ref, "init.fishmon.h")) as f:
-            ih = overlay_init_h(f.read(), n1, n2, n3, maxbnd)
-        with open(os.path.join(scratch, "init.h"), "w") as f:
-            f.write(ih)
-        with open(os.path.join(ref, "init.fishmon.c")) as f:
-            ic = overlay_init_c(f.read(), lim, flux, cour, timeorder, utoprim, fv, beta)
-        with open(os.path.join(scratch, "init.c"), "w") as f:
-            f.write(ic)
-        with open(os.path.join(ref, "bounds.fishmon.c")) as f:
-            bc = f.read() + AFTER_MPI_STUB
-        with open(os.path.join(scratch, "bounds.c"), "w") as f:
-            f.write(bc)
+        if problem == "bondi":
+            if n3 != 1 or fv or beta is not None:
+                raise SystemExit("the Bondi problem is 2D, point scheme, unmagnetised")
+            with open(os.path.join(ref, "init.h")) as f:
+                ih = overlay_bondi_h(f.read(), n1, n2)
+            with open(os.path.join(scratch, "init.h"), "w") as f:
+                f.write(ih)
+            with open(os.path.join(ref, "init.c")) as f:
+                ic = overlay_bondi_c(f.read(), lim, flux, cour, timeorder, utoprim)
+            with open(os.path.join(scratch, "init.c"), "w") as f:
+                f.write(ic)
+        else:
+            with open(os.path.join(ref, "init.fishmon.h")) as f:
+                ih = overlay_init_h(f.read(), n1, n2, n3, maxbnd)
+            with open(os.path.join(scratch, "init.h"), "w") as f:
+                f.write(ih)
+            with open(os.path.join(ref, "init.fishmon.c")) as f:
+                ic = overlay_init_c(f.read(), lim, flux, cour, timeorder, utoprim, fv, beta)
+            with open(os.path.join(scratch, "init.c"), "w") as f:
+                f.write(ic)
+            with open(os.path.join(ref, "bounds.fishmon.c")) as f:
+                bc = f.read() + AFTER_MPI_STUB
+            with open(os.path.join(scratch, "bounds.c"), "w") as f:
+                f.write(bc)
         shutil.copy(os.path.join(HERE, "ref_harness.c"), os.path.join(scratch, "ref_harness.c"))
         srcs = SOURCES + ["ref_harness.c"]
         extra = []

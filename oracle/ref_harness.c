@@ -38,6 +38,13 @@
  *                      failure and floor counters per zone (failfloorcount
  *                      of the first time scale, fixup.c:206; all zones with
  *                      ghosts, 9 categories, doubles as CTYPE is).
+ *   --bcgeom           writes init_bcgeom.bin: per (i,j) of the first x3
+ *                      plane, all zones with ghosts, at CENT, 49 doubles:
+ *                      the Boyer-Lindquist r (coord + bl_coord, coord.c:1195,
+ *                      389), dx/dx' (dxdxprim, coord.c:596), its inverse
+ *                      (matrix_inverse, metric.c:1346) and the Kerr-Schild
+ *                      metric g_{mu nu} (gcov_func(0, KSCOORDS), metric.c:11):
+ *                      what the Bondi-integral boundaries use (bounds.c:788-1000).
  *   --rdump            calls the reference's own restart_write(0)
  *                      (restart.c:206) after the last step, which writes
  *                      dumps/rdump-0 in the working directory (its header,
@@ -64,6 +71,10 @@ static int geomplane = 0;
 static int do_ener = 0;
 static int do_rdump = 0;
 static int do_ffc = 0;
+static int do_bcgeom = 0;
+extern void dxdxprim(FTYPE *X, FTYPE *V, FTYPE (*dxdxp)[NDIM]);
+extern void matrix_inverse(FTYPE gcov[][NDIM], FTYPE gcon[][NDIM]);
+extern void gcov_func(int getprim, int whichcoord, FTYPE *X, FTYPE gcov[][NDIM], FTYPE *gcovpert);
 extern int restart_write(long dump_cnt);
 extern int dump_ener(int doener, int dordump, int call_code);
 
@@ -239,6 +250,33 @@ static void dump_geometry(void)
   }
 }
 
+/* coordinate data of the Bondi-integral boundaries, first x3 plane */
+static void dump_bcgeom(void)
+{
+  const int n1 = N1M, n2 = N2M;
+  double *buf = (double *)malloc(sizeof(double) * 49 * (size_t)n1 * n2);
+  int i, j, a, b;
+  for (i = -N1BND; i < N1 + N1BND; i++)
+    for (j = -N2BND; j < N2 + N2BND; j++) {
+      double *o = buf + 49 * ((size_t)(i + N1BND) * n2 + (j + N2BND));
+      FTYPE X[NDIM], V[NDIM], dxdxp[NDIM][NDIM], idxdxp[NDIM][NDIM], gks[NDIM][NDIM], gpert[NDIM];
+      coord(i, j, 0, CENT, X);
+      bl_coord(X, V);
+      dxdxprim(X, V, dxdxp);
+      matrix_inverse(dxdxp, idxdxp);
+      gcov_func(0, KSCOORDS, X, gks, gpert);
+      o[0] = V[1];
+      for (a = 0; a < NDIM; a++)
+        for (b = 0; b < NDIM; b++) {
+          o[1 + 4 * a + b] = dxdxp[a][b];
+          o[17 + 4 * a + b] = idxdxp[a][b];
+          o[33 + 4 * a + b] = gks[a][b];
+        }
+    }
+  wbin("init", "bcgeom", buf, sizeof(double) * 49 * (size_t)n1 * n2);
+  free(buf);
+}
+
 extern int Utoprimgen(int evolvetype, int inputtype, FTYPE *U, struct of_geom *ptrgeom, FTYPE *pr);
 
 static int invert_file(const char *in, const char *out)
@@ -320,6 +358,10 @@ int main(int argc, char *argv[])
       do_ener = 1;
       argv += 1;
       argc -= 1;
+    } else if (strcmp(argv[1], "--bcgeom") == 0) {
+      do_bcgeom = 1;
+      argv += 1;
+      argc -= 1;
     } else if (strcmp(argv[1], "--ffc") == 0) {
       do_ffc = 1;
       argv += 1;
@@ -334,7 +376,7 @@ int main(int argc, char *argv[])
     }
   }
   if (argc < 3) {
-    fprintf(stderr, "usage: %s [--phimodes seed] [--geomplane] [--ener] [--rdump] [--ffc] <outdir|-> <nsteps> [dumpstep ...]\n", argv[0]);
+    fprintf(stderr, "usage: %s [--phimodes seed] [--geomplane] [--ener] [--rdump] [--ffc] [--bcgeom] <outdir|-> <nsteps> [dumpstep ...]\n", argv[0]);
     return 2;
   }
   /* outdir "-" runs the steps for timing only and writes nothing */
@@ -356,6 +398,7 @@ int main(int argc, char *argv[])
   }
   if (!nodump) {
     dump_geometry();
+    if (do_bcgeom) dump_bcgeom();
     dump_state("init", 0);
   }
   if (do_ener && dump_ener(1, 0, INIT_OUT) >= 1) {

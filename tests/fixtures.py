@@ -47,6 +47,10 @@ def load(name):
     pr.ener_init = d["ener_init"] if "ener_init" in d else None
     # the reference's failure and floor counters per zone at init
     pr.ffc_init = d["ffc_init"] if "ffc_init" in d else None
+    # Bondi-integral boundaries: the x1 edge/ghost coordinate table and the
+    # per-zone coordinate data (r, dx/dx', inverse, Kerr-Schild metric)
+    pr.bondi_bc = np.ascontiguousarray(d["bondi_bc"]) if "bondi_bc" in d else None
+    pr.bcgeom = d["bcgeom"] if "bcgeom" in d else None
     # the reference's restart dump after the last step (restart_write), bytes
     pr.rdump = d["rdump"].tobytes() if "rdump" in d else None
     return pr, ref

@@ -22,6 +22,7 @@ run without it.
 usage: python tests/golden/make_golden.py [case ...]
 """
 import os
+import shutil
 import subprocess
 import sys
 import tempfile
@@ -74,6 +75,15 @@ CASES = {
                                        {"beta": 1e-4}),
 }
 
+# The Bondi flow of the generic init.c (TESTNUMBER 153: the reference's
+# bondigrid16.dat table on 16x16 zones, a = 0, its Bondi-integral x1
+# boundaries, polar x2) with the MC + HLL point scheme and RK2 (its own
+# inverter, Jon's); checked with a tolerance, not by the bit (pow).
+BONDI_CASES = {
+    "bondi2d_16x16_mc_hll": (16, 16, 1, "MC", "HLL", 0.5, 100, [1, 10, 100], 2, "JON", False, 11,
+                             {"problem": "bondi"}),
+}
+
 # cases whose fixture also holds the reference's restart dump after the last
 # step (restart_write(0) through the harness's --rdump: header line, then p
 # and unew of every active zone as text), from a run without dump_ener
@@ -103,15 +113,24 @@ def make(name, spec, ref):
     maxbnd = spec[11] if len(spec) > 11 else 11
     opts = spec[12] if len(spec) > 12 else {}
     hargs = ["--phimodes", str(opts["phimodes"])] if "phimodes" in opts else []
+    problem = opts.get("problem", "fmtorus")
+    if problem == "bondi":
+        hargs = hargs + ["--bcgeom"]
     ng = maxbnd if fv else NG[lim]
     exe = build_ref.build(ref, n1, n2, n3, lim, flux, cour, maxbnd, timeorder=timeorder, utoprim=utoprim, fv=fv,
-                          beta=opts.get("beta"))
+                          beta=opts.get("beta"), problem=problem)
     with tempfile.TemporaryDirectory() as tmp:
         out = os.path.join(tmp, "out")
+        if problem == "bondi":
+            # the analytic solution the reference's init reads (init.c:350-460)
+            shutil.copy(os.path.join(ref, f"bondigrid{n1}.dat"), tmp)
         subprocess.run([exe, "--ener", "--ffc"] + hargs + [out, str(nsteps)] + [str(s) for s in dumps], cwd=tmp,
                        check=True, stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL)
         rd = RefDump(out)
         pr = rd.to_problem(ng, "init")
+        if problem == "bondi":
+            # the generic bounds.c's POLARAXIS (u~2, B2 negated) has its own id here
+            pr.bc = tuple(1001 if b == 4 else b for b in pr.bc)
         # the reference's own ener.out (dump_ener.c:287-295), one line at init
         # and one after every dumped step: t, realnstep, the conserved
         # integrals U_tot[8], ..., divbmax, divbavg
@@ -148,6 +167,17 @@ def make(name, spec, ref):
                 # unew of the other schemes: the last stage's conserved
                 # update (what the restart dump holds beside p)
                 data[f"unew_s{s}"] = rd.crop(rd.unew(f"s{s}"), ng)
+        if problem == "bondi":
+            # coordinate data of the x1 edge and ghost zones (hgpu_set_bondi_boundaries'
+            # table: [side][q][j][49], q = 0 the edge zone, q >= 1 the ghosts)
+            g = np.fromfile(os.path.join(out, "init_bcgeom.bin")).reshape(rd.NM[0], rd.NM[1], 49)
+            b1, b2 = rd.bnd[0], rd.bnd[1]
+            tab = np.zeros((2, ng + 1, n2, 49))
+            for q in range(ng + 1):
+                tab[0, q] = g[b1 - q, b2:b2 + n2]
+                tab[1, q] = g[b1 + n1 - 1 + q, b2:b2 + n2]
+            data["bondi_bc"] = tab
+            data["bcgeom"] = rd.crop(g[:, :, None, :], ng)[:, :, 0, :]
         if name in RDUMP:
             # a run of its own without dump_ener, whose integrals would fill
             # the header's cumulative diagnostics (dump_ener.c:160-230)
@@ -305,7 +335,7 @@ def main():
     ref = build_ref.DEFAULT_REF
     if not os.path.isdir(ref):
         raise SystemExit(f"reference tree not found at {ref}: set HARM_REFERENCE_DIR")
-    names = sys.argv[1:] or list(CASES) + ["utoprim_zones", "bondigrid"] + list(RECORDS)
+    names = sys.argv[1:] or list(CASES) + list(BONDI_CASES) + ["utoprim_zones", "bondigrid"] + list(RECORDS)
     for name in names:
         if name == "utoprim_zones":
             make_zones(ref)
@@ -313,6 +343,8 @@ def main():
             make_bondigrid(ref)
         elif name in RECORDS:
             make_record(name, ref)
+        elif name in BONDI_CASES:
+            make(name, BONDI_CASES[name], ref)
         else:
             make(name, CASES[name], ref)
 
