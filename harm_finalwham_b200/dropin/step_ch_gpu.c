@@ -32,6 +32,15 @@
  * they were.  Of pflag, the slots FLAGUTOPRIMFAIL (the inversion and
  * fixups) and FLAGBSQORHO / FLAGBSQOU (pre_fixup's b^2 flags) are produced.
  *
+ * Boundary meanings: the FM torus file's bounds.fishmon.c is the default.
+ * Built with -DHARMGPU_GENERIC_BOUNDS (the reference's generic bounds.c, as
+ * its test problems use), OUTFLOW is the plain copy (HGPU_BC_OUTFLOW_COPY)
+ * and POLARAXIS the reflection with u~2 and B2 negated
+ * (HGPU_BC_POLARAXIS_FLIP); with the Bondi-integral x1 boundaries
+ * (BONDIINTOUTFLOW / BONDIMDOTOUTFLOW, bounds.c:140-156, 295-308) the
+ * coordinate data they need comes from the reference's own coord,
+ * bl_coord, dxdxprim, matrix_inverse and gcov_func(KSCOORDS).
+ *
  * Environment:
  *   HARMGPU_PRECISION=mixed   the mixed-precision path instead of FP64
  *   HARMGPU_RESIDENT=1        upload the state on the first call only and
@@ -166,6 +175,49 @@ static int upload_geometry(void)
   return 0;
 }
 
+extern void dxdxprim(FTYPE *X, FTYPE *V, FTYPE (*dxdxp)[NDIM]);
+extern void matrix_inverse(FTYPE gcov[][NDIM], FTYPE gcon[][NDIM]);
+extern void gcov_func(int getprim, int whichcoord, FTYPE *X, FTYPE gcov[][NDIM], FTYPE *gcovpert);
+
+/* hgpu_set_bondi_boundaries' table: per x1 side, edge zone and ghost zones,
+   active j, at CENT of the first x3 plane: r, dx/dx', its inverse, the
+   Kerr-Schild metric */
+static int upload_bondi_table(void)
+{
+  const int nq = g_g[1] + 1;
+  double *tab;
+  int side, q, j, a, b, rc;
+  if (BCtype[X1UP] != HGPU_BC_BONDIMDOTOUTFLOW && BCtype[X1DN] != HGPU_BC_BONDIINTOUTFLOW) return 0;
+  tab = (double *)calloc((size_t)2 * nq * N2 * 49, sizeof(double));
+  if (!tab) {
+    dualfprintf(fail_file, "step_ch_gpu: out of host memory for the Bondi boundary table\n");
+    return 1;
+  }
+  for (side = 0; side < 2; side++)
+    for (q = 0; q < nq; q++)
+      for (j = 0; j < N2; j++) {
+        const int i = side == 0 ? -q : N1 - 1 + q;
+        double *o = tab + ((size_t)(side * nq + q) * N2 + j) * 49;
+        FTYPE X[NDIM], V[NDIM], dxdxp[NDIM][NDIM], idxdxp[NDIM][NDIM], gks[NDIM][NDIM], gpert[NDIM];
+        coord(i, j, 0, CENT, X);
+        bl_coord(X, V);
+        dxdxprim(X, V, dxdxp);
+        matrix_inverse(dxdxp, idxdxp);
+        gcov_func(0, KSCOORDS, X, gks, gpert);
+        o[0] = V[1];
+        for (a = 0; a < NDIM; a++)
+          for (b = 0; b < NDIM; b++) {
+            o[1 + 4 * a + b] = dxdxp[a][b];
+            o[17 + 4 * a + b] = idxdxp[a][b];
+            o[33 + 4 * a + b] = gks[a][b];
+          }
+      }
+  rc = hgpu_set_bondi_boundaries(g_ctx, tab);
+  free(tab);
+  CHECK(rc);
+  return 0;
+}
+
 static int setup(void)
 {
   hgpu_config cfg;
@@ -188,6 +240,12 @@ static int setup(void)
   cfg.lim = lim;
   cfg.fluxmethod = fluxmethod;
   for (d = 0; d < 6; d++) cfg.bc[d] = BCtype[d];
+#ifdef HARMGPU_GENERIC_BOUNDS
+  for (d = 0; d < 6; d++) {
+    if (cfg.bc[d] == POLARAXIS) cfg.bc[d] = HGPU_BC_POLARAXIS_FLIP;  /* bounds.c:477-489 */
+    if (cfg.bc[d] == OUTFLOW) cfg.bc[d] = HGPU_BC_OUTFLOW_COPY;      /* bounds.c:84-135 */
+  }
+#endif
   cfg.precision = (prec && strcmp(prec, "mixed") == 0) ? HGPU_PREC_MIXED : HGPU_PREC_FP64;
   for (d = 1; d <= 3; d++) cfg.dx[d] = dx[d];
   cfg.gam = gam;
@@ -228,6 +286,7 @@ static int setup(void)
   }
 #endif
   if (upload_geometry()) return 1;
+  if (upload_bondi_table()) return 1;
   g_resident = res && atoi(res) != 0;
   trifprintf("step_ch_gpu: %dx%dx%d zones, %d ghosts on the device, %s\n", N1, N2, N3, g_ng,
              cfg.precision == HGPU_PREC_FP64 ? "FP64" : "mixed precision");

@@ -360,6 +360,9 @@ def build(ref, n1, n2, n3, lim, flux, cour, maxbnd, name=None, keep=False, verbo
             srcs = srcs + ["step_ch_gpu.c"]
             extra = ["-I" + os.path.join(REPO, "include"), "-L" + GPULIB, "-lharmgpu",
                      "-Wl,-rpath,$ORIGIN/../../harm_finalwham_b200/lib"]
+            if problem == "bondi":
+                # the shim maps the generic bounds.c's boundary meanings
+                extra.append("-DHARMGPU_GENERIC_BOUNDS")
         exe = os.path.join(OUT, name)
         cmd = ["gcc", "-O2", "-ffp-contract=off", "-fno-fast-math", "-fcommon", "-w",
                "-mcmodel=medium", "-o", exe] + srcs + extra + ["-lm"]

@@ -51,6 +51,8 @@ def load(name):
     # per-zone coordinate data (r, dx/dx', inverse, Kerr-Schild metric)
     pr.bondi_bc = np.ascontiguousarray(d["bondi_bc"]) if "bondi_bc" in d else None
     pr.bcgeom = d["bcgeom"] if "bcgeom" in d else None
+    # the reference's bondigrid<N1>.dat the Bondi flow's init reads
+    pr.bondigrid_dat = d["bondigrid_dat"].tobytes() if "bondigrid_dat" in d else None
     # the reference's restart dump after the last step (restart_write), bytes
     pr.rdump = d["rdump"].tobytes() if "rdump" in d else None
     return pr, ref

@@ -178,6 +178,9 @@ def make(name, spec, ref):
                 tab[1, q] = g[b1 + n1 - 1 + q, b2:b2 + n2]
             data["bondi_bc"] = tab
             data["bcgeom"] = rd.crop(g[:, :, None, :], ng)[:, :, 0, :]
+            # the table file itself, for runs of the reference program
+            with open(os.path.join(ref, f"bondigrid{n1}.dat"), "rb") as f:
+                data["bondigrid_dat"] = np.frombuffer(f.read(), dtype=np.uint8)
         if name in RDUMP:
             # a run of its own without dump_ener, whose integrals would fill
             # the header's cumulative diagnostics (dump_ener.c:160-230)

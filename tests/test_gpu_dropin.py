@@ -81,3 +81,32 @@ def test_reference_loop_on_gpu_matches_golden(binary, fixture, args):
             assert m["t"] == r["t"] and m["dt"] == r["dt"] and m["nstroke"] == r["nstroke"]
             if r["u"] is not None:
                 assert same(act(rd.crop(rd.unew(tag), pr.ng)), act(r["u"])), f"unew differs after step {s}"
+
+
+def test_reference_bondi_flow_on_gpu_tracks_its_cpu_run():
+    # the generic init.c's Bondi flow (TESTNUMBER 153) with its Bondi-integral
+    # x1 boundaries and the generic polar axis, through the drop-in built
+    # with -DHARMGPU_GENERIC_BOUNDS; pow in the boundaries makes the bar a
+    # tolerance (the device's own runs: tests/test_gpu_bondi_bc.py)
+    pr, ref = load("bondi2d_16x16_mc_hll")
+    exe = os.path.join(LIBDIR, "harm_bondi_16x16x1_MC_HLL_jon_gpushim")
+    assert os.path.exists(exe), f"{exe} is missing: __graft_entry__.build() builds it"
+    steps = sorted(ref)
+    with tempfile.TemporaryDirectory() as tmp:
+        with open(os.path.join(tmp, "bondigrid16.dat"), "wb") as f:
+            f.write(pr.bondigrid_dat)
+        out = os.path.join(tmp, "out")
+        r = subprocess.run([exe, out, str(steps[-1])] + [str(s) for s in steps[:-1]], cwd=tmp,
+                           capture_output=True, text=True)
+        assert r.returncode == 0, r.stderr[-2000:]
+        rd = RefDump(out)
+        act = pr.active
+        for s in steps:
+            p = act(rd.crop(rd.p(f"s{s}"), pr.ng))
+            want = act(ref[s]["p"])
+            for q, tol in ((0, 1e-13), (1, 1e-13), (2, 1e-13), (3, 1e-11)):
+                l1 = float(np.sum(np.abs(p[..., q] - want[..., q])) / np.sum(np.abs(want[..., q])))
+                assert l1 < tol, f"primitive {q}: relative L1 {l1:.3e} after {s} steps"
+            m = rd.meta_of(f"s{s}")
+            assert abs(m["t"] - ref[s]["t"]) <= 1e-13 * ref[s]["t"]
+
