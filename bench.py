@@ -14,10 +14,15 @@ Our arm:
   value       zone-updates/s with the state resident in HBM, timed with CUDA
               events on the library's stream (max over ranks); the state
               arrays (300 MB each) exceed L2, so no flush is needed.
-  e2e         the same metric through the C ABI with host-owned arrays, as a
-              drop-in step_ch() on reference-owned memory does: every step
-              uploads the primitives from pinned host memory, steps, and
-              downloads primitives and flags (wall clock incl. copies).
+  e2e         the same metric through the C ABI with host-owned arrays
+              (wall clock incl. copies from/to pinned host memory): every
+              step uploads the active zones' primitives
+              (hgpu_upload_active; the device rebuilds the ghosts with
+              bound_prim), steps, and downloads primitives and flags
+              (hgpu_download_active); e2e.full_arrays is the same with the
+              arrays including ghost zones, as the drop-in step_ch() moves
+              them (the finite-volume scheme, whose unew must travel too,
+              reports that path).
   roofline    dominant kernel: algorithmic bytes per launch / its average
               CUDA-event duration vs the measured HBM peak, plus its FP64
               operation rate vs the FP64 peak measured in this run.
@@ -462,24 +467,47 @@ def bench_ours(args, rank, world):
     # e2e through the C ABI with host-owned arrays
     e2e = None
     if not args.no_e2e:
-        p_host, pf_host = g.pinned_state_buffers()
-        p_host[...] = dom.p
-        pf_host[...] = 0
-        t_now, dt_now = g.time()
-        barrier()
         e2e_steps = max(1, min(args.steps, args.e2e_steps))
+        fv = sc["doenoflux"] == "ENOFINITEVOLUME"
+        # (a) arrays with ghosts, as the drop-in step_ch moves them: p + pflag
+        # up and down every step (the finite-volume scheme's unew too)
+        p_host, pf_host = g.pinned_state_buffers()
+        u_host = g.download_conserved() if fv else None
+        _, _, t_now, dt_now = g.download_state(out=(p_host, pf_host))
+        barrier()
         t0 = time.perf_counter()
         for _ in range(e2e_steps):
             g.upload_state(p_host, pf_host, t_now, dt_now)
+            if fv:
+                g.upload_conserved(u_host)
             g.step_ch(1)
             _, _, t_now, dt_now = g.download_state(out=(p_host, pf_host))
-        el = time.perf_counter() - t0
-        el = allmax(el)
-        h2d = p_host.nbytes + pf_host.nbytes
-        d2h = p_host.nbytes + pf_host.nbytes
-        e2e = {"value": zones * e2e_steps * world / el, "unit": "zone-updates/s", "h2d_bytes_per_step": h2d,
-               "d2h_bytes_per_step": d2h, "steps": e2e_steps,
-               "mode": "host-owned arrays: upload p+pflag, step_ch(1), download p+pflag every step"}
+            if fv:
+                u_host = g.download_conserved()
+        el_full = allmax(time.perf_counter() - t0)
+        nb_full = p_host.nbytes + pf_host.nbytes + (2 * u_host.nbytes if fv else 0)
+        full = {"value": zones * e2e_steps * world / el_full, "h2d_bytes_per_step": nb_full,
+                "d2h_bytes_per_step": nb_full,
+                "mode": "arrays with ghosts: upload p+pflag, step_ch(1), download p+pflag every step"}
+        if fv:
+            e2e = dict(full, unit="zone-updates/s", steps=e2e_steps)
+        else:
+            # (b) active zones only (hgpu_upload_active / hgpu_download_active:
+            # the ghosts rebuilt by bound_prim on the device)
+            pa_host, fa_host = g.pinned_active_buffers()
+            _, _, t_now, dt_now = g.download_active(out=(pa_host, fa_host))
+            barrier()
+            t0 = time.perf_counter()
+            for _ in range(e2e_steps):
+                g.upload_active(pa_host, t_now, dt_now)
+                g.step_ch(1)
+                _, _, t_now, dt_now = g.download_active(out=(pa_host, fa_host))
+            el = allmax(time.perf_counter() - t0)
+            e2e = {"value": zones * e2e_steps * world / el, "unit": "zone-updates/s",
+                   "h2d_bytes_per_step": pa_host.nbytes, "d2h_bytes_per_step": pa_host.nbytes + fa_host.nbytes,
+                   "steps": e2e_steps,
+                   "mode": "host-owned active-zone arrays: upload p, step_ch(1), download p+pflag every step",
+                   "full_arrays": full}
 
     # roofline on the dominant kernel
     dom_k = max(ktimes, key=lambda k: ktimes[k]["ms"])

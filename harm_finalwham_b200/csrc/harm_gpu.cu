@@ -1172,6 +1172,37 @@ __global__ void reset_stage_kernel(Scalars *sc) {
 }
 
 // reference AoS [zone][8] <-> device SoA [8][zone]
+// Active zones only, host layout [n1][n2][n3][8] (and [n1][n2][n3] for the
+// flags) <-> the device's planes with ghosts: thread per (zone, primitive),
+// so the host-layout side is read/written contiguously.
+__global__ void active_scatter_kernel(Dims d, const double *__restrict__ a, double *__restrict__ s) {
+  const long long na = (long long)d.n1 * d.n2 * d.n3;
+  long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= na * NPR) return;
+  const long long z = t / NPR;
+  const int pl = (int)(t % NPR);
+  const int k = (int)(z % d.n3), j = (int)((z / d.n3) % d.n2), i = (int)(z / ((long long)d.n2 * d.n3));
+  s[(long long)pl * d.nz + zix(d, i, j, k)] = a[t];
+}
+
+__global__ void active_gather_kernel(Dims d, const double *__restrict__ s, double *__restrict__ a) {
+  const long long na = (long long)d.n1 * d.n2 * d.n3;
+  long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= na * NPR) return;
+  const long long z = t / NPR;
+  const int pl = (int)(t % NPR);
+  const int k = (int)(z % d.n3), j = (int)((z / d.n3) % d.n2), i = (int)(z / ((long long)d.n2 * d.n3));
+  a[t] = s[(long long)pl * d.nz + zix(d, i, j, k)];
+}
+
+__global__ void active_gather_flags_kernel(Dims d, const int *__restrict__ f, int *__restrict__ a) {
+  const long long na = (long long)d.n1 * d.n2 * d.n3;
+  long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= na) return;
+  const int k = (int)(t % d.n3), j = (int)((t / d.n3) % d.n2), i = (int)(t / ((long long)d.n2 * d.n3));
+  a[t] = f[zix(d, i, j, k)];
+}
+
 __global__ void aos_to_soa_kernel(const double *__restrict__ a, double *__restrict__ s, long long nz) {
   long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= nz * NPR) return;
@@ -2173,6 +2204,55 @@ int hgpu_step_ch(hgpu_ctx *x, int nsteps, hgpu_stats *stats) {
   }
   CUDA_TRY(cudaGetLastError());
   if (stats) return read_stats(x, stats);
+  return HGPU_OK;
+}
+
+// The active zones from / to host arrays; the ghost zones are the device's
+// bound_prim of them (what the end of every step leaves there).
+int hgpu_upload_active(hgpu_ctx *x, const double *p, double t, double dt) {
+  if (!x || !p || x->ninst > 0) return HGPU_E_INVALID;
+  if (boundaries_ready(x)) return HGPU_E_INVALID;
+  int rc = ensure_staging(x);
+  if (rc) return rc;
+  const Dims &d = x->d;
+  const long long na = (long long)d.n1 * d.n2 * d.n3;
+  CUDA_TRY(cudaMemcpyAsync(x->staging, p, sizeof(double) * NPR * na, cudaMemcpyHostToDevice, x->stream));
+  LAUNCH(x, K_OTHER, active_scatter_kernel, grid_for(na * NPR, 256), 256, d, x->staging, x->p);
+  Scalars s;
+  memset(&s, 0, sizeof(s));
+  s.t = t;
+  s.dt = dt;
+  CUDA_TRY(cudaMemcpyAsync(x->sc, &s, sizeof(Scalars), cudaMemcpyHostToDevice, x->stream));
+  launch_bound(x, x->p);
+  if (x->cfg.doenoflux == HGPU_ENOFINITEVOLUME)
+    LAUNCH(x, K_OTHER, pi2u_kernel, grid_for(d.nz, 128), 128, d, x->P, x->p, x->G, x->ucum, x->sc);
+  CUDA_TRY(cudaStreamSynchronize(x->stream));
+  CUDA_TRY(cudaGetLastError());
+  return HGPU_OK;
+}
+
+int hgpu_download_active(hgpu_ctx *x, double *p, int *pflag, double *t, double *dt) {
+  if (!x || x->ninst > 0) return HGPU_E_INVALID;
+  int rc = ensure_staging(x);
+  if (rc) return rc;
+  const Dims &d = x->d;
+  const long long na = (long long)d.n1 * d.n2 * d.n3;
+  if (p) {
+    LAUNCH(x, K_OTHER, active_gather_kernel, grid_for(na * NPR, 256), 256, d, x->p, x->staging);
+    CUDA_TRY(cudaMemcpyAsync(p, x->staging, sizeof(double) * NPR * na, cudaMemcpyDeviceToHost, x->stream));
+  }
+  if (pflag) {
+    // the flags follow the primitives in the staging buffer (it holds 8 nz doubles)
+    int *fs = (int *)(x->staging + NPR * na);
+    LAUNCH(x, K_OTHER, active_gather_flags_kernel, grid_for(na, 256), 256, d, x->pflag, fs);
+    CUDA_TRY(cudaMemcpyAsync(pflag, fs, sizeof(int) * na, cudaMemcpyDeviceToHost, x->stream));
+  }
+  Scalars s;
+  CUDA_TRY(cudaMemcpyAsync(&s, x->sc, sizeof(Scalars), cudaMemcpyDeviceToHost, x->stream));
+  CUDA_TRY(cudaStreamSynchronize(x->stream));
+  CUDA_TRY(cudaGetLastError());
+  if (t) *t = s.t;
+  if (dt) *dt = s.dt;
   return HGPU_OK;
 }
 

@@ -116,6 +116,8 @@ def load_library(path=None):
     L.hgpu_reconfigure.argtypes = [ctypes.c_void_p, _P(hgpu_config)]
     L.hgpu_upload_conserved.argtypes = [ctypes.c_void_p, _dp]
     L.hgpu_set_bondi_boundaries.argtypes = [ctypes.c_void_p, _dp]
+    L.hgpu_upload_active.argtypes = [ctypes.c_void_p, _dp, ctypes.c_double, ctypes.c_double]
+    L.hgpu_download_active.argtypes = [ctypes.c_void_p, _dp, _ip, _dp, _dp]
     L.hgpu_download_failfloorcount.argtypes = [ctypes.c_void_p, _P(ctypes.c_longlong), ctypes.c_int]
     L.hgpu_write_rdump.argtypes = [ctypes.c_void_p, ctypes.c_char_p, ctypes.c_void_p, ctypes.c_size_t, ctypes.c_int]
     L.hgpu_read_rdump.argtypes = [ctypes.c_void_p, ctypes.c_char_p, ctypes.c_size_t, ctypes.c_int, ctypes.c_double,
@@ -154,7 +156,7 @@ def load_library(path=None):
                  "hgpu_advance_stage", "hgpu_fluxcalc", "hgpu_bound_prim", "hgpu_utoprim_batch", "hgpu_utoprimgen_batch",
                  "hgpu_device_prims", "hgpu_sync", "hgpu_create_batch", "hgpu_batch_layout", "hgpu_batch_status",
                  "hgpu_step_graph", "hgpu_autotune", "hgpu_set_tuning", "hgpu_batch_run", "hgpu_diagnostics", "hgpu_download_conserved", "hgpu_upload_conserved",
-                 "hgpu_write_rdump", "hgpu_read_rdump", "hgpu_download_failfloorcount", "hgpu_set_bondi_boundaries", "hgpu_server_create", "hgpu_server_submit", "hgpu_server_submit_borrowed",
+                 "hgpu_write_rdump", "hgpu_read_rdump", "hgpu_download_failfloorcount", "hgpu_set_bondi_boundaries", "hgpu_upload_active", "hgpu_download_active", "hgpu_server_create", "hgpu_server_submit", "hgpu_server_submit_borrowed",
                  "hgpu_server_poll", "hgpu_server_result", "hgpu_server_release", "hgpu_halo_bytes", "hgpu_halo_pack",
                  "hgpu_halo_unpack", "hgpu_stats_clear", "hgpu_stats_read", "hgpu_stage_advance", "hgpu_stage_fixup",
                  "hgpu_dt_probe", "hgpu_step_end", "hgpu_ndt_pack", "hgpu_ndt_unpack", "hgpu_stream"):
@@ -315,6 +317,28 @@ class HarmGPU:
         _check(self.L, self.L.hgpu_download_bsqflags(self.h, _ptr(f, ctypes.c_int)))
         return f
 
+    def upload_active(self, p, t, dt):
+        """hgpu_upload_active: active-zone primitives [n1][n2][n3][8]; the
+        ghosts by bound_prim on the device."""
+        p = _contig(p, np.float64)
+        assert p.shape == tuple(self.n) + (NPR,)
+        _check(self.L, self.L.hgpu_upload_active(self.h, _ptr(p), float(t), float(dt)))
+
+    def download_active(self, out=None):
+        """hgpu_download_active: (p [n1][n2][n3][8], pflag [n1][n2][n3], t, dt)."""
+        if out is None:
+            out = (np.empty(tuple(self.n) + (NPR,)), np.empty(tuple(self.n), dtype=np.int32))
+        p, f = out
+        t, dt = ctypes.c_double(), ctypes.c_double()
+        _check(self.L, self.L.hgpu_download_active(self.h, _ptr(p), _ptr(f, ctypes.c_int), ctypes.byref(t),
+                                                   ctypes.byref(dt)))
+        return p, f, t.value, dt.value
+
+    def pinned_active_buffers(self):
+        """Page-locked host arrays for the active-zone transfers."""
+        n = tuple(self.n)
+        return self._pinned_array(n + (NPR,), np.float64), self._pinned_array(n, np.int32)
+
     def set_bondi_boundaries(self, table):
         """hgpu_set_bondi_boundaries: [2][ng+1][n2][49] coordinate data (r,
         dx/dx', its inverse, the Kerr-Schild metric) of the x1 edge and ghost
@@ -434,17 +458,18 @@ class HarmGPU:
     def launch_count(self):
         return self.L.hgpu_launch_count(self.h)
 
+    def _pinned_array(self, shape, dtype):
+        """A page-locked host array owned by this object."""
+        nbytes = int(np.prod(shape)) * np.dtype(dtype).itemsize
+        ptr = ctypes.c_void_p()
+        _check(self.L, self.L.hgpu_alloc_pinned(nbytes, ctypes.byref(ptr)))
+        self._pinned = getattr(self, "_pinned", []) + [ptr]
+        arr = np.ctypeslib.as_array(ctypes.cast(ptr, ctypes.POINTER(ctypes.c_byte)), shape=(nbytes,))
+        return arr.view(dtype).reshape(shape)
+
     def pinned_state_buffers(self):
         """Primitive and flag arrays in page-locked host memory (owned by this object)."""
-        nz = int(np.prod(self.nt))
-        bufs = []
-        for nbytes, dtype, shape in ((nz * NPR * 8, np.float64, self.nt + (NPR,)), (nz * 4, np.int32, self.nt)):
-            ptr = ctypes.c_void_p()
-            _check(self.L, self.L.hgpu_alloc_pinned(nbytes, ctypes.byref(ptr)))
-            self._pinned = getattr(self, "_pinned", []) + [ptr]
-            arr = np.ctypeslib.as_array(ctypes.cast(ptr, ctypes.POINTER(ctypes.c_byte)), shape=(nbytes,))
-            bufs.append(arr.view(dtype).reshape(shape))
-        return bufs[0], bufs[1]
+        return self._pinned_array(self.nt + (NPR,), np.float64), self._pinned_array(self.nt, np.int32)
 
     def bound_prim(self, which=0):
         _check(self.L, self.L.hgpu_bound_prim(self.h, int(which)))
