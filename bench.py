@@ -454,8 +454,9 @@ def bench_ours(args, rank, world):
                  "ms_per_step": ms2 / args.steps, "steps_compared": args.warmup + args.steps + extra,
                  "rel_l1_mixed_vs_fp64": err, "conservation": cons,
                  "note": "mixed = FP32 WENO5 reconstruction (on differences from each cell's value, FP64 "
-                         "epsilons; MC/PARA: FP32 Riemann kernel); FP64 Riemann fluxes, flux-CT, conserved update, "
-                         "con-to-prim and fixups; both runs from the same initial state"}
+                         "epsilons; MC/PARA: FP32 Riemann kernel); WENO5's Riemann fluxes FP64 with FP32 wave speeds; "
+                         "flux-CT, conserved update, con-to-prim and fixups FP64; both runs from the same "
+                         "initial state"}
 
     # per-kernel device times for the roofline (a separate profiled pass)
     g.set_profiling(True)

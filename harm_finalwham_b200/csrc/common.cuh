@@ -493,7 +493,10 @@ __global__ void __launch_bounds__(W5_THREADS, MB) weno5_kernel(Dims d, Params P,
 // kernel, RECON 1: Riemann states from the WENO5 face values pL/pR (stored
 // as TR), RECON 2: PARA
 // ---------------------------------------------------------------------------
-template <int DIR, int RECON, typename T, int MB = MinBlocks<T>::flux, typename TR = T>
+// MIX = 1: the mixed-precision variant of the FP64 kernel (wave speeds in
+// FP32, vchar_f32; instantiated only in flux_f32.cu, whose FP64 arithmetic
+// may contract a*b+c into FMA)
+template <int DIR, int RECON, typename T, int MB = MinBlocks<T>::flux, typename TR = T, int MIX = 0>
 __global__ void __launch_bounds__(128, MB) flux_kernel(Dims d, Params P, Box box,
                                                                  const double *__restrict__ pb,
                                                                  const TR *__restrict__ pL, const TR *__restrict__ pR,
@@ -558,7 +561,8 @@ __global__ void __launch_bounds__(128, MB) flux_kernel(Dims d, Params P, Box box
     {
       StateT<T> q;
       if (get_state(p_l, m, q)) err |= ERR_UTCALC_DISCR;
-      err |= vchar(p_l, q, DIR, m, gam, &cmaxl, &cminl);
+      if constexpr (MIX != 0) err |= vchar_f32(p_l, q, DIR, m, gam, &cmaxl, &cminl);
+      else err |= vchar(p_l, q, DIR, m, gam, &cmaxl, &cminl);
       if (!ring) {
         EMT<T> e;
         em_prepare(p_l, m, q, e);
@@ -569,7 +573,8 @@ __global__ void __launch_bounds__(128, MB) flux_kernel(Dims d, Params P, Box box
     {
       StateT<T> q;
       if (get_state(p_r, m, q)) err |= ERR_UTCALC_DISCR;
-      err |= vchar(p_r, q, DIR, m, gam, &cmaxr, &cminr);
+      if constexpr (MIX != 0) err |= vchar_f32(p_r, q, DIR, m, gam, &cmaxr, &cminr);
+      else err |= vchar(p_r, q, DIR, m, gam, &cmaxr, &cminr);
       if (!ring) {
         EMT<T> e;
         em_prepare(p_r, m, q, e);

@@ -354,6 +354,33 @@ __device__ __forceinline__ int vchar(const T *pr, const StateT<T> &q, int dir, c
   return simplefast(dir, m, q, cms2, vmin, vmax);
 }
 
+// vchar with FP32 arithmetic on an FP64 state (the mixed-precision Riemann
+// kernel of WENO5: fluxes and states stay FP64, the wave speeds, which only
+// scale the HLL dissipation and the CFL limit, are formed in FP32).  Reads
+// what vchar reads: rho, u, b^mu, b_mu, u^mu and g^{mu nu}.
+template <typename T>
+__device__ __forceinline__ int vchar_f32(const T *pr, const StateT<T> &q, int dir, const MetricT<T> &m, T gam,
+                                         T *vmax, T *vmin) {
+  float prf[NPR];
+  prf[RHO] = (float)pr[RHO];
+  prf[UU] = (float)pr[UU];
+  StateT<float> qf;
+  MetricT<float> mf;
+#pragma unroll
+  for (int a = 0; a < 4; a++) {
+    qf.ucon[a] = (float)q.ucon[a];
+    qf.bcon[a] = (float)q.bcon[a];
+    qf.bcov[a] = (float)q.bcov[a];
+  }
+#pragma unroll
+  for (int a = 0; a < 16; a++) mf.gcon[a] = (float)m.gcon[a];
+  float vmx = 0.f, vmn = 0.f;
+  const int r = vchar<float>(prf, qf, dir, mf, (float)gam, &vmx, &vmn);
+  *vmax = (T)vmx;
+  *vmin = (T)vmn;
+  return r;
+}
+
 template <typename T>
 __device__ __forceinline__ T max_ref(T a, T b) { return (a > b) ? a : b; }  // phys.c:1797
 template <typename T>

@@ -56,7 +56,11 @@ namespace hg {
   extern template __global__ void flux_kernel<DIR, 0, float>(Dims, Params, Box, const double *, const float *,    \
                                                              const float *, const double *, double *, Scalars *);   \
   extern template __global__ void flux_kernel<DIR, 2, float>(Dims, Params, Box, const double *, const float *,    \
-                                                             const float *, const double *, double *, Scalars *);
+                                                             const float *, const double *, double *, Scalars *);   \
+  extern template __global__ void flux_kernel<DIR, 1, double, kFluxMB[0], double, 1>(                             \
+      Dims, Params, Box, const double *, const double *, const double *, const double *, double *, Scalars *);      \
+  extern template __global__ void flux_kernel<DIR, 1, double, kFluxMB[1], double, 1>(                             \
+      Dims, Params, Box, const double *, const double *, const double *, const double *, double *, Scalars *);
 HG_F32_EXTERN(1)
 HG_F32_EXTERN(2)
 HG_F32_EXTERN(3)
@@ -1939,7 +1943,7 @@ static void launch_w5(hgpu_ctx *x, const double *pb) {
   }
 }
 
-template <int DIR, typename TW, typename TF, int FMB, int BMB>
+template <int DIR, typename TW, typename TF, int FMB, int BMB, int MIX = 0>
 static void launch_dir(hgpu_ctx *x, const double *pb) {
   const Dims &d = x->d;
   const Params &P = x->P;
@@ -1947,7 +1951,7 @@ static void launch_dir(hgpu_ctx *x, const double *pb) {
   unsigned gf = grid_for(x->face_box[DIR].size(), 128);
   if (P.lim == HGPU_LIM_WENO5) {
     launch_w5<DIR, TW, BMB>(x, pb);
-    LAUNCH(x, kid, (flux_kernel<DIR, 1, TF, FMB, double>), gf, 128, d, P, x->face_box[DIR], pb, x->pL, x->pR, x->G,
+    LAUNCH(x, kid, (flux_kernel<DIR, 1, TF, FMB, double, MIX>), gf, 128, d, P, x->face_box[DIR], pb, x->pL, x->pR, x->G,
            x->F[DIR], x->sc);
   } else if (P.lim == HGPU_LIM_PARA) {
     LAUNCH(x, kid, (flux_kernel<DIR, 2, TF, FMB, TF>), gf, 128, d, P, x->face_box[DIR], pb, nullptr, nullptr, x->G,
@@ -1958,15 +1962,15 @@ static void launch_dir(hgpu_ctx *x, const double *pb) {
   }
 }
 
-template <typename TW, typename TF, int FMB, int BMB>
+template <typename TW, typename TF, int FMB, int BMB, int MIX = 0>
 static void launch_fluxes_t(hgpu_ctx *x, const double *pb) {
   const Dims &d = x->d;
   if (x->P.lim == HGPU_LIM_WENO5)
     LAUNCH(x, K_W5STATE, w5_state_kernel<TW>, grid_for(x->w5_state_box.size(), 128), 128, d, x->P, x->w5_state_box,
            pb, x->G, (TW *)x->w5pu);
-  if (d.n1 > 1) launch_dir<1, TW, TF, FMB, BMB>(x, pb);
-  if (d.n2 > 1) launch_dir<2, TW, TF, FMB, BMB>(x, pb);
-  if (d.n3 > 1) launch_dir<3, TW, TF, FMB, BMB>(x, pb);
+  if (d.n1 > 1) launch_dir<1, TW, TF, FMB, BMB, MIX>(x, pb);
+  if (d.n2 > 1) launch_dir<2, TW, TF, FMB, BMB, MIX>(x, pb);
+  if (d.n3 > 1) launch_dir<3, TW, TF, FMB, BMB, MIX>(x, pb);
 }
 // the WENO5 state pieces and one direction's reconstruction with the
 // context's precision and WENO5 variant (for timing tilings)
@@ -2002,8 +2006,8 @@ static void launch_fluxes(hgpu_ctx *x, const double *pb) {
   if (x->cfg.precision == HGPU_PREC_MIXED) {
     constexpr int WMB = MinBlocks<float>::weno;
     if (x->P.lim != HGPU_LIM_WENO5) launch_fluxes_t<float, float, MinBlocks<float>::flux, WMB>(x, pb);
-    else if (fv == 0) launch_fluxes_t<float, double, kFluxMB[0], WMB>(x, pb);
-    else launch_fluxes_t<float, double, kFluxMB[1], WMB>(x, pb);
+    else if (fv == 0) launch_fluxes_t<float, double, kFluxMB[0], WMB, 1>(x, pb);
+    else launch_fluxes_t<float, double, kFluxMB[1], WMB, 1>(x, pb);
   } else {
     if (fv == 0 && bv == 0) launch_fluxes_t<double, double, kFluxMB[0], kWenoMB[0]>(x, pb);
     else if (fv == 0) launch_fluxes_t<double, double, kFluxMB[0], kWenoMB[1]>(x, pb);
