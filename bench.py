@@ -108,13 +108,26 @@ def rank_info():
     return r, w, lr
 
 
-def pin_device(local_rank, world):
-    """One process per GPU: expose only this rank's GPU to the CUDA runtime."""
+# the physical index of this process's GPU (for nvidia-smi)
+PHYS_GPU = "0"
+
+
+def select_device(local_rank, world):
+    """One process per GPU: this rank's GPU (its local rank) for torch and
+    for the library, whose statically linked CUDA runtime keeps its own
+    current device.  Every GPU stays visible, so NCCL can reach its peers
+    over NVLink."""
+    global PHYS_GPU
+    vis = os.environ.get("CUDA_VISIBLE_DEVICES")
+    devs = vis.split(",") if vis else None
+    PHYS_GPU = devs[local_rank % len(devs)].strip() if devs else str(local_rank)
     if world <= 1:
         return
-    vis = os.environ.get("CUDA_VISIBLE_DEVICES")
-    devs = vis.split(",") if vis else [str(i) for i in range(64)]
-    os.environ["CUDA_VISIBLE_DEVICES"] = devs[local_rank % len(devs)]
+    import torch
+
+    from harm_finalwham_b200.gpu import set_device
+    torch.cuda.set_device(local_rank)
+    set_device(local_rank)
 
 
 class ClockSampler:
@@ -146,8 +159,7 @@ class ClockSampler:
         self.out.seek(0)
         rows = [r.split(",") for r in self.out.read().strip().splitlines() if r.strip()]
         os.unlink(self.out.name)
-        dev = os.environ.get("CUDA_VISIBLE_DEVICES", "0").split(",")[0]
-        rows = [r for r in rows if len(r) >= 9 and r[0].strip() == dev] or [r for r in rows if len(r) >= 9]
+        rows = [r for r in rows if len(r) >= 9 and r[0].strip() == PHYS_GPU] or [r for r in rows if len(r) >= 9]
         if not rows:
             return None
         sm = [float(r[1]) for r in rows]
@@ -184,7 +196,6 @@ def bench_decomp(args, rank, world):
     dist = None
     if world > 1:
         import torch.distributed as dist
-        torch.cuda.set_device(0)
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
     dom = torus.fm_torus(n1, n2, n3 * world, ng=sc["ng"] or GHOSTS[lim], lim=lim, flux=flux, seed=7)
     dom.timeorder, dom.utoprim, dom.doenoflux = sc["timeorder"], sc["utoprim"], sc["doenoflux"]
@@ -377,7 +388,6 @@ def bench_ours(args, rank, world):
     if world > 1:
         import torch
         import torch.distributed as dist
-        torch.cuda.set_device(0)
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
 
     def barrier():
@@ -911,7 +921,7 @@ def main():
         print(json.dumps(out))
         return 0
 
-    pin_device(local, world)
+    select_device(local, world)
     if world > 1 and not args.replicas and not args.decomp:
         args.decomp = "x3"
     res = bench_decomp(args, rank, world) if args.decomp else bench_ours(args, rank, world)

@@ -1558,6 +1558,11 @@ extern "C" {
 
 int hgpu_abi_version(void) { return HGPU_ABI_VERSION; }
 
+int hgpu_set_device(int device) {
+  CUDA_TRY(cudaSetDevice(device));
+  return HGPU_OK;
+}
+
 const char *hgpu_last_error(void) { return g_errbuf; }
 
 // error text of a failing call made elsewhere in the library (host code)

@@ -78,6 +78,8 @@ def load_library(path=None):
             path = _build.build()
     L = ctypes.CDLL(path)
     L.hgpu_abi_version.restype = ctypes.c_int
+    L.hgpu_set_device.argtypes = [ctypes.c_int]
+    L.hgpu_set_device.restype = ctypes.c_int
     L.hgpu_last_error.restype = ctypes.c_char_p
     L.hgpu_create.argtypes = [_P(hgpu_config), _P(ctypes.c_void_p)]
     L.hgpu_destroy.argtypes = [ctypes.c_void_p]
@@ -164,6 +166,14 @@ def load_library(path=None):
     if path == _build.LIB:
         _lib = L
     return L
+
+
+def set_device(device):
+    """hgpu_set_device: the CUDA device the library uses on this thread (its
+    runtime is linked statically, so torch.cuda.set_device does not reach
+    it); call before creating contexts."""
+    L = load_library()
+    _check(L, L.hgpu_set_device(int(device)))
 
 
 def _check(L, rc):

@@ -33,7 +33,7 @@
 extern "C" {
 #endif
 
-#define HGPU_ABI_VERSION 13
+#define HGPU_ABI_VERSION 14
 
 /* return codes */
 #define HGPU_OK 0
@@ -123,6 +123,14 @@ typedef struct {
 
 /* Library/ABI identification. */
 int hgpu_abi_version(void);
+
+/* Select the CUDA device that this host thread's later calls use
+   (cudaSetDevice in the library's own CUDA runtime, which is linked
+   statically, so a device chosen through another runtime, e.g. a Python
+   framework's, does not reach it).  One process per GPU calls it with its
+   local rank before hgpu_create; contexts keep the device they were created
+   on.  HGPU_E_CUDA for a device that does not exist. */
+int hgpu_set_device(int device);
 
 /* Create a device context on the current CUDA device (init-time set_arrays.c / set_grid.c
    storage).  Returns HGPU_OK and *out, or an error code. */
