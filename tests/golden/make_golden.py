@@ -102,6 +102,11 @@ RECORDS = {
     # the precision-at-scale torus 256x128x128, WENO5 + HLL, first 5 steps
     "torus3d_256x128x128_weno5_hll_5": (256, 128, 128, "WENO5", "HLL", 0.8, 5, [1, 5],
                                         ["--phimodes", "1", "--geomplane"], (8, 8, 8), False),
+    # the FM torus problem file's own scheme (PARA + HLL, RK4, Jon's inverter,
+    # finite volume with avgscheme=DONOR, MAXBND 11) on the 3D torus 64x32x32
+    # with azimuthal density modes, 20 steps
+    "torus3d_64x32x32_para_hll_rk4_jon_fv_20": (64, 32, 32, "PARA", "HLL", 0.8, 20, [1, 20], ["--phimodes", "1"],
+                                                (4, 4, 4), False, {"timeorder": 4, "utoprim": "JON", "fv": True}),
 }
 
 
@@ -284,11 +289,12 @@ def make_zones(ref):
 def record_binary(ref, name):
     """Reference binary of a record (the one __graft_entry__.build also builds)."""
     n1, n2, n3, lim, flux, cour = RECORDS[name][:6]
-    return build_ref.build(ref, n1, n2, n3, lim, flux, cour, 11)
+    kw = RECORDS[name][11] if len(RECORDS[name]) > 11 else {}
+    return build_ref.build(ref, n1, n2, n3, lim, flux, cour, 11, **kw)
 
 
 def make_record(name, ref, workdir=None):
-    n1, n2, n3, lim, flux, cour, nsteps, dumps, hargs, stride, whole = RECORDS[name]
+    n1, n2, n3, lim, flux, cour, nsteps, dumps, hargs, stride, whole = RECORDS[name][:11]
     exe = record_binary(ref, name)
     os.makedirs(RECORD_DIR, exist_ok=True)
     with tempfile.TemporaryDirectory(dir=workdir) as tmp:

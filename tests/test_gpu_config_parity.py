@@ -38,6 +38,9 @@ CONFIGS = {
     "torus3d_128x64x32_weno5_hll_500": ("harm_ref_128x64x32_WENO5_HLL", 6),
     # precision-at-scale torus 256x128x128, WENO5 + HLL, first 5 steps
     "torus3d_256x128x128_weno5_hll_5": ("harm_ref_256x128x128_WENO5_HLL", 6),
+    # the FM torus problem file's own scheme (PARA, RK4, Jon, finite volume,
+    # all 11 MAXBND ghosts) on the 3D torus 64x32x32, 20 steps
+    "torus3d_64x32x32_para_hll_rk4_jon_fv_20": ("harm_ref_64x32x32_PARA_HLL_rk4_jon_fv", 11),
 }
 
 
