@@ -1846,6 +1846,22 @@ int hgpu_batch_status(hgpu_ctx *x, double *t, double *dt, int *done, int *ndone)
   return HGPU_OK;
 }
 
+int hgpu_batch_set_time(hgpu_ctx *x, const double *t, const double *dt) {
+  if (!x || !x->inst || !t || !dt) return HGPU_E_INVALID;
+  std::vector<Inst> hi(x->ninst);
+  CUDA_TRY(cudaMemcpyAsync(hi.data(), x->inst, sizeof(Inst) * x->ninst, cudaMemcpyDeviceToHost, x->stream));
+  CUDA_TRY(cudaStreamSynchronize(x->stream));
+  for (int b = 0; b < x->ninst; b++) {
+    hi[b].t = t[b];
+    hi[b].dt = dt[b];
+    hi[b].done = !(t[b] < hi[b].tf);
+    hi[b].nsteps = 0;
+  }
+  CUDA_TRY(cudaMemcpyAsync(x->inst, hi.data(), sizeof(Inst) * x->ninst, cudaMemcpyHostToDevice, x->stream));
+  CUDA_TRY(cudaStreamSynchronize(x->stream));
+  return HGPU_OK;
+}
+
 int hgpu_upload_geometry(hgpu_ctx *x, const double *gcov, const double *gcon, const double *gcovpert,
                          const double *gdet, const double *conn, const double *floors) {
   if (!x || !gcov || !gcon || !gcovpert || !gdet || !conn || !floors) return HGPU_E_INVALID;

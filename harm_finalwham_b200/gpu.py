@@ -109,6 +109,7 @@ def load_library(path=None):
     L.hgpu_create_batch.argtypes = [_P(hgpu_config), ctypes.c_int, _ip, _dp, _dp, _dp, _P(ctypes.c_void_p)]
     L.hgpu_batch_layout.argtypes = [ctypes.c_void_p, _ip]
     L.hgpu_batch_status.argtypes = [ctypes.c_void_p, _dp, _dp, _ip, _ip]
+    L.hgpu_batch_set_time.argtypes = [ctypes.c_void_p, _dp, _dp]
     L.hgpu_step_graph.argtypes = [ctypes.c_void_p, ctypes.c_int, _P(hgpu_stats)]
     L.hgpu_autotune.argtypes = [ctypes.c_void_p, _P(hgpu_tuning)]
     L.hgpu_set_tuning.argtypes = [ctypes.c_void_p, _P(hgpu_tuning)]
@@ -156,7 +157,7 @@ def load_library(path=None):
         getattr(L, name).restype = ctypes.c_int
     for name in ("hgpu_create", "hgpu_upload_geometry", "hgpu_upload_state", "hgpu_download_state", "hgpu_step_ch",
                  "hgpu_advance_stage", "hgpu_fluxcalc", "hgpu_bound_prim", "hgpu_utoprim_batch", "hgpu_utoprimgen_batch",
-                 "hgpu_device_prims", "hgpu_sync", "hgpu_create_batch", "hgpu_batch_layout", "hgpu_batch_status",
+                 "hgpu_device_prims", "hgpu_sync", "hgpu_create_batch", "hgpu_batch_layout", "hgpu_batch_status", "hgpu_batch_set_time",
                  "hgpu_step_graph", "hgpu_autotune", "hgpu_set_tuning", "hgpu_batch_run", "hgpu_diagnostics", "hgpu_download_conserved", "hgpu_upload_conserved",
                  "hgpu_write_rdump", "hgpu_read_rdump", "hgpu_download_failfloorcount", "hgpu_set_bondi_boundaries", "hgpu_upload_active", "hgpu_download_active", "hgpu_server_create", "hgpu_server_submit", "hgpu_server_submit_borrowed",
                  "hgpu_server_poll", "hgpu_server_result", "hgpu_server_release", "hgpu_halo_bytes", "hgpu_halo_pack",
@@ -528,7 +529,8 @@ class HarmBatch(HarmGPU):
     with their own ng ghosts."""
 
     def __init__(self, n1s, dx1s, gams, tfs, ng=3, lim="MC", flux="HLL", precision="fp64", cour=0.5, safe=1.3,
-                 defcon=1.0, rhominlimit=1e-20, uuminlimit=1e-20, gammamax=25.0, gammafail=2500.0):
+                 defcon=1.0, rhominlimit=1e-20, uuminlimit=1e-20, gammamax=25.0, gammafail=2500.0, utoprim="2DFINAL",
+                 timeorder=2):
         self.L = load_library()
         n1s = np.ascontiguousarray(n1s, dtype=np.int32)
         self.ninst = len(n1s)
@@ -542,6 +544,8 @@ class HarmBatch(HarmGPU):
         c.dx[1] = c.dx[2] = c.dx[3] = 1.0
         c.gam, c.cour, c.safe, c.defcon, c.tf = 4.0 / 3.0, cour, safe, defcon, 0.0
         c.rhominlimit, c.uuminlimit, c.gammamax, c.gammafail = rhominlimit, uuminlimit, gammamax, gammafail
+        c.utoprimversion = UTOPRIM[utoprim] if isinstance(utoprim, str) else int(utoprim)
+        c.timeorder = int(timeorder)
         self.cfg = c
         self.n = (c.n1, 1, 1)
         self.g = (ng, 0, 0)
@@ -567,6 +571,10 @@ class HarmBatch(HarmGPU):
         _check(self.L, self.L.hgpu_batch_status(self.h, _ptr(t), _ptr(dt), _ptr(done, ctypes.c_int),
                                                 ctypes.byref(nd)))
         return t, dt, done, nd.value
+
+    def set_time(self, t, dt):
+        """hgpu_batch_set_time: every instance's t and dt."""
+        _check(self.L, self.L.hgpu_batch_set_time(self.h, _ptr(_contig(t, np.float64)), _ptr(_contig(dt, np.float64))))
 
     def split(self, line):
         """Per-instance views (own ghosts included) of a line array [nt1, ...]."""

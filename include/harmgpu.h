@@ -33,7 +33,7 @@
 extern "C" {
 #endif
 
-#define HGPU_ABI_VERSION 14
+#define HGPU_ABI_VERSION 15
 
 /* return codes */
 #define HGPU_OK 0
@@ -241,6 +241,10 @@ int hgpu_create_batch(const hgpu_config *cfg, int ninst, const int *n1, const do
 int hgpu_batch_layout(hgpu_ctx *ctx, int *i0);
 /* per-instance t, dt, done flag (each may be NULL) and the number of finished instances */
 int hgpu_batch_status(hgpu_ctx *ctx, double *t, double *dt, int *done, int *ndone);
+/* set every instance's t and dt (e.g. an instance's own start-up dt, the
+   reference's set_dt of its initial state); an instance with t >= its tf is
+   marked done; the per-instance step counts restart from zero */
+int hgpu_batch_set_time(hgpu_ctx *ctx, const double *t, const double *dt);
 
 /* Advance a batch until every instance has reached its end time (or
    max_steps batch steps): CUDA-graph replays of check_every steps between

@@ -187,16 +187,27 @@ def overlay_init_c(text, lim, flux, cour, timeorder=2, utoprim="2DFINAL", fv=Fal
     return text
 
 
-def overlay_bondi_h(text, n1, n2):
-    """Generic init.h (the 1D/2D test-problem header) set to the Bondi flow,
-    TESTNUMBER 153 (init.h:578-582: 16x16 by default; the resolution must be
-    one of the reference's bondigrid<N1>.dat tables)."""
+# generic test problems (init.c / init.h / bounds.c) this recipe builds:
+# problem name -> (TESTNUMBER, the marker line of its grid block in init.h)
+GENERIC_PROBLEMS = {
+    "bondi": (153, "#elif( TESTNUMBER == 153 )  // 1D Bondi problem"),
+    "ram101": (101, "#elif( TESTNUMBER == 101 )  // 1D Riemann problem #1 from RAM paper"),
+}
+
+
+def overlay_bondi_h(text, n1, n2, problem="bondi"):
+    """Generic init.h (the 1D/2D test-problem header) set to one of its test
+    problems: the Bondi flow, TESTNUMBER 153 (init.h:578-582: 16x16 by
+    default; the resolution must be one of the reference's bondigrid<N1>.dat
+    tables), or the RAM paper's first relativistic shock tube, TESTNUMBER 101
+    (init.h:515-520, 400 zones; init.c:2396-2411)."""
     w = "init.h"
-    text = sub_once(text, "#define TESTNUMBER 49", "#define TESTNUMBER 153", where=w)
-    i = text.index("#elif( TESTNUMBER == 153 )  // 1D Bondi problem")
+    num, marker = GENERIC_PROBLEMS[problem]
+    text = sub_once(text, "#define TESTNUMBER 49", f"#define TESTNUMBER {num}", where=w)
+    i = text.index(marker)
     j = text.index("#elif", i + 5)
-    block = sub_once(text[i:j], "#define NXTEST 16", f"#define NXTEST {n1}", where=w)
-    block = sub_once(block, "#define NYTEST 16", f"#define NYTEST {n2}", where=w)
+    block = re.sub(r"#define NXTEST \d+", f"#define NXTEST {n1}", text[i:j], count=1)
+    block = re.sub(r"#define NYTEST \d+", f"#define NYTEST {n2}", block, count=1)
     text = text[:i] + block + text[j:]
     # the step's scheme settings of the FM torus problem file (init.fishmon.h),
     # which the test problems' header sets otherwise for non-FFDE tests
@@ -269,13 +280,16 @@ def build(ref, n1, n2, n3, lim, flux, cour, maxbnd, name=None, keep=False, verbo
     harm_cpu_restart_write, harm_cpu_diag and harm_cpu_dump_ener (the names
     at restart.c:206, diag.c:9, dump_ener.c:3).
 
-    problem: "fmtorus" (init.fishmon.c / init.fishmon.h / bounds.fishmon.c)
-    or "bondi" (the generic init.c / init.h / bounds.c at TESTNUMBER 153,
-    the Bondi flow with the Bondi-integral x1 boundaries, bounds.c:140-156,
-    295-308; n3 must be 1 and n1 x n2 a bondigrid table's size; the binary
-    reads bondigrid<n1>.dat from its working directory)."""
+    problem: "fmtorus" (init.fishmon.c / init.fishmon.h / bounds.fishmon.c),
+    or one of the generic init.c / init.h / bounds.c's test problems
+    (GENERIC_PROBLEMS) with the FM torus file's scheme settings: "bondi"
+    (TESTNUMBER 153, the Bondi flow with the Bondi-integral x1 boundaries,
+    bounds.c:140-156, 295-308; n3 must be 1 and n1 x n2 a bondigrid table's
+    size; the binary reads bondigrid<n1>.dat from its working directory) or
+    "ram101" (TESTNUMBER 101, the first relativistic shock tube of the RAM
+    paper on the Minkowski line, OUTFLOW copies at both ends)."""
     os.makedirs(OUT, exist_ok=True)
-    name = name or (("harm_bondi_" if problem == "bondi" else "harm_ref_")
+    name = name or ((f"harm_{problem}_" if problem in GENERIC_PROBLEMS else "harm_ref_")
                     + f"{n1}x{n2}x{n3}_{lim}_{flux}" + (f"_rk{timeorder}" if timeorder != 2 else "")
                     + ("_jon" if utoprim == "JON" else "") + ("_fv" if fv else "")
                     + (f"_beta{beta:g}" if beta is not None else "") + ("_gpushim" if gpu_shim else ""))
@@ -308,11 +322,11 @@ def build(ref, n1, n2, n3, lim, flux, cour, maxbnd, name=None, keep=False, verbo
         with open(p, "w") as f:
             f.write(t)
         # problem overlay
-        if problem == "bondi":
+        if problem in GENERIC_PROBLEMS:
             if n3 != 1 or fv or beta is not None:
-                raise SystemExit("the Bondi problem is 2D, point scheme, unmagnetised")
+                raise SystemExit("the generic test problems here are 1D/2D, point scheme, as the reference sets them")
             with open(os.path.join(ref, "init.h")) as f:
-                ih = overlay_bondi_h(f.read(), n1, n2)
+                ih = overlay_bondi_h(f.read(), n1, n2, problem)
             with open(os.path.join(scratch, "init.h"), "w") as f:
                 f.write(ih)
             with open(os.path.join(ref, "init.c")) as f:
@@ -360,7 +374,7 @@ def build(ref, n1, n2, n3, lim, flux, cour, maxbnd, name=None, keep=False, verbo
             srcs = srcs + ["step_ch_gpu.c"]
             extra = ["-I" + os.path.join(REPO, "include"), "-L" + GPULIB, "-lharmgpu",
                      "-Wl,-rpath,$ORIGIN/../../harm_finalwham_b200/lib"]
-            if problem == "bondi":
+            if problem in GENERIC_PROBLEMS:
                 # the shim maps the generic bounds.c's boundary meanings
                 extra.append("-DHARMGPU_GENERIC_BOUNDS")
         exe = os.path.join(OUT, name)

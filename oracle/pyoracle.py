@@ -193,11 +193,16 @@ class RefDump:
         if self.meta.get("GEOMPLANE", 0):
             gm = gm[:2] + (1,)
             nm = nm[:2] + (1,)
-        shapes = {"gcov": (LOCS, 4, 4), "gcon": (LOCS, 4, 4), "gcovpert": (LOCS, 4), "gdet": (LOCS,)}
+        shapes = {"gcov": (LOCS, 4, 4), "gcon": (LOCS, 4, 4), "gcovpert": (LOCS, 4), "gdet": (LOCS,),
+                  "conn": (4, 4, 4)}
         if name in shapes:
-            return self._f("init", name).reshape(gm + shapes[name])
-        if name == "conn":
-            return self._f("init", name).reshape(nm + (4, 4, 4))
+            a = self._f("init", name)
+            full = (nm if name == "conn" else gm) + shapes[name]
+            if a.size == int(np.prod(shapes[name])):
+                # a constant metric (CARTMINKMETRIC: the reference stores one
+                # point, defs.h:214) holds everywhere
+                return np.broadcast_to(a.reshape((1, 1, 1) + shapes[name]), full).copy()
+            return a.reshape(full)
         if name == "floors":
             return self._f("init", name).reshape(nm + (2,))
         raise KeyError(name)

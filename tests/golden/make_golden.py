@@ -82,6 +82,11 @@ CASES = {
 BONDI_CASES = {
     "bondi2d_16x16_mc_hll": (16, 16, 1, "MC", "HLL", 0.5, 100, [1, 10, 100], 2, "JON", False, 11,
                              {"problem": "bondi"}),
+    # the RAM paper's first relativistic shock tube (TESTNUMBER 101: 400 zones
+    # on [0, 1], rho 10 | 1, p 13.33 | 1e-8, Gamma 5/3, CFL 0.5, to t = 0.4)
+    # on the Minkowski line with the generic bounds.c's OUTFLOW copies
+    "ram101_400_mc_hll": (400, 1, 1, "MC", "HLL", 0.5, 200, [1, 50, 200], 2, "JON", False, 11,
+                          {"problem": "ram101"}),
 }
 
 # cases whose fixture also holds the reference's restart dump after the last
@@ -133,9 +138,10 @@ def make(name, spec, ref):
                        check=True, stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL)
         rd = RefDump(out)
         pr = rd.to_problem(ng, "init")
-        if problem == "bondi":
-            # the generic bounds.c's POLARAXIS (u~2, B2 negated) has its own id here
-            pr.bc = tuple(1001 if b == 4 else b for b in pr.bc)
+        if problem != "fmtorus":
+            # the generic bounds.c's POLARAXIS (u~2, B2 negated) and OUTFLOW
+            # (a plain copy) have their own ids here
+            pr.bc = tuple({4: 1001, 0: 1000}.get(b, b) for b in pr.bc)
         # the reference's own ener.out (dump_ener.c:287-295), one line at init
         # and one after every dumped step: t, realnstep, the conserved
         # integrals U_tot[8], ..., divbmax, divbavg
