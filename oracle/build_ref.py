@@ -192,6 +192,9 @@ def overlay_init_c(text, lim, flux, cour, timeorder=2, utoprim="2DFINAL", fv=Fal
 GENERIC_PROBLEMS = {
     "bondi": (153, "#elif( TESTNUMBER == 153 )  // 1D Bondi problem"),
     "ram101": (101, "#elif( TESTNUMBER == 101 )  // 1D Riemann problem #1 from RAM paper"),
+    "ram102": (102, "#elif( TESTNUMBER == 102 )  // 1D Riemann problem #2 from RAM paper"),
+    "ram103": (103, "#elif( TESTNUMBER == 103 )  // 1D Riemann problem #3 from RAM paper"),
+    "ram106": (106, "#elif( TESTNUMBER == 106 )  // 1D Riemann problem #6.1 from RAM paper (Hard test)"),
 }
 
 

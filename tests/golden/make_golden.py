@@ -87,6 +87,11 @@ BONDI_CASES = {
     # on the Minkowski line with the generic bounds.c's OUTFLOW copies
     "ram101_400_mc_hll": (400, 1, 1, "MC", "HLL", 0.5, 200, [1, 50, 200], 2, "JON", False, 11,
                           {"problem": "ram101"}),
+    # its problems 2 (p 1000 | 0.01, a blast wave), 3 (a flow at v = 0.9 into
+    # a denser, hotter state, Gamma 4/3) and 6.1 (the hard test), 400 zones
+    "ram102_400_mc_hll": (400, 1, 1, "MC", "HLL", 0.5, 150, [1, 150], 2, "JON", False, 11, {"problem": "ram102"}),
+    "ram103_400_mc_hll": (400, 1, 1, "MC", "HLL", 0.5, 150, [1, 150], 2, "JON", False, 11, {"problem": "ram103"}),
+    "ram106_400_mc_hll": (400, 1, 1, "MC", "HLL", 0.5, 150, [1, 150], 2, "JON", False, 11, {"problem": "ram106"}),
 }
 
 # cases whose fixture also holds the reference's restart dump after the last
