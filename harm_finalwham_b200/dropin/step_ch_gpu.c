@@ -125,6 +125,14 @@ static void flag_window(int to_ref)
       }
 }
 
+/* index of a zone in the reference's metric arrays: a constant metric
+   (CARTMINKMETRIC) is stored once (defs.h:214, get_geometry phys.c:869-877) */
+#if(MCOORD!=CARTMINKMETRIC)
+#define MIDX(a) (a)
+#else
+#define MIDX(a) 0
+#endif
+
 /* geometry of the first x3 plane, per (i,j), in the C ABI's layout */
 static int upload_geometry(void)
 {
@@ -150,19 +158,19 @@ static int upload_geometry(void)
       for (loc = 0; loc < NPG; loc++) {
         for (a = 0; a < NDIM; a++) {
           for (b = 0; b < NDIM; b++) {
-            gcv[(ij * NPG + loc) * 16 + 4 * a + b] = gcov[i][j][k][loc][a][b];
-            gcn[(ij * NPG + loc) * 16 + 4 * a + b] = gcon[i][j][k][loc][a][b];
+            gcv[(ij * NPG + loc) * 16 + 4 * a + b] = gcov[MIDX(i)][MIDX(j)][MIDX(k)][loc][a][b];
+            gcn[(ij * NPG + loc) * 16 + 4 * a + b] = gcon[MIDX(i)][MIDX(j)][MIDX(k)][loc][a][b];
           }
-          gpt[(ij * NPG + loc) * 4 + a] = gcovpert[i][j][k][loc][a];
+          gpt[(ij * NPG + loc) * 4 + a] = gcovpert[MIDX(i)][MIDX(j)][MIDX(k)][loc][a];
         }
-        gdt[ij * NPG + loc] = gdet[i][j][k][loc];
+        gdt[ij * NPG + loc] = gdet[MIDX(i)][MIDX(j)][MIDX(k)][loc];
       }
       if (in_cells) {
         struct of_geom geom;
         FTYPE prfloor[NPR];
         for (a = 0; a < NDIM; a++)
           for (b = 0; b < NDIM; b++)
-            for (c = 0; c < NDIM; c++) cnn[ij * 64 + 16 * a + 4 * b + c] = conn[i][j][k][a][b][c];
+            for (c = 0; c < NDIM; c++) cnn[ij * 64 + 16 * a + 4 * b + c] = conn[MIDX(i)][MIDX(j)][MIDX(k)][a][b][c];
         get_geometry(i, j, k, CENT, &geom);
         set_density_floors(&geom, p[i][j][k], prfloor);
         flr[ij * 2 + 0] = prfloor[RHO];

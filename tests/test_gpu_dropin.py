@@ -110,3 +110,20 @@ def test_reference_bondi_flow_on_gpu_tracks_its_cpu_run():
             m = rd.meta_of(f"s{s}")
             assert abs(m["t"] - ref[s]["t"]) <= 1e-13 * ref[s]["t"]
 
+
+def test_reference_shock_tube_on_gpu_matches_its_cpu_run():
+    # the generic init.c's relativistic shock tube 6.1 (TESTNUMBER 106: failed
+    # inversions, the Lorentz-factor limit, checksolution) on the Minkowski
+    # line, the drop-in built with -DHARMGPU_GENERIC_BOUNDS
+    pr, ref = load("ram106_400_mc_hll")
+    steps = sorted(ref)
+    tmp, rd = run_shim("harm_ram106_400x1x1_MC_HLL_jon_gpushim", steps[-1], steps[:-1])
+    with tmp:
+        for s in steps:
+            tag = f"s{s}"
+            r = ref[s]
+            assert same(rd.crop(rd.p(tag), pr.ng), r["p"]), f"primitives differ after step {s}"
+            assert np.array_equal(rd.crop(rd.pflag(tag), pr.ng)[..., 0], r["pflag"])
+            m = rd.meta_of(tag)
+            assert m["t"] == r["t"] and m["dt"] == r["dt"] and m["nstroke"] == r["nstroke"]
+
