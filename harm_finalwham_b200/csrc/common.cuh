@@ -89,6 +89,7 @@ struct Scalars {
   int err;
   int nfail;                       // failures after Utoprimgen in the last stage
   int ncand;                       // checksolution candidates
+  int ndep;                        // checksolution candidates that depend on earlier ones
   int nfixlist;                    // fixup_utoprim list length
   int nfixed;
   int overflow;

@@ -829,66 +829,147 @@ __global__ void checksol_gamma_kernel(Dims d, Params P, Box box, const double *_
 // In the reference the candidates are visited in loop order (i, then j, then
 // k) and each visit may overwrite the zone's pflag with 12/13, which later
 // visits of its neighbours read.  The zone index z is lexicographic in
-// (i,j,k), so "visited earlier" is "smaller z".  This single-block kernel
-// iterates a fixpoint in which every candidate sees the current decision of
-// its earlier candidate neighbours and the unchanged flags of everything
-// else; a dependency chain of length L settles after L sweeps, which gives
-// exactly the reference's sequential result.  candmap maps a zone to its
-// candidate slot (-1 otherwise) and is restored to -1 before returning.
-__global__ void __launch_bounds__(1024) checksol_resolve_kernel(Dims d, const double *__restrict__ pv,
-                                                                const double *__restrict__ gammacheck, int *pflag,
-                                                                const long long *__restrict__ cand, int *candmap,
-                                                                int *orig, int *dec, int cap, Scalars *sc) {
+// (i,j,k), so "visited earlier" is "smaller z".  Four kernels resolve it:
+//   checksol_map_kernel     candidate slots in candmap, the original flags;
+//   checksol_prep_kernel    per candidate, what does not change while the
+//                           decisions settle: for each of its 8 neighbours
+//                           (fixup.c:508-526) the vote bits of the gamma and
+//                           u ratios (the divisions), whether a neighbour's
+//                           flag is fixed and not failed (a non-candidate or
+//                           a later candidate: its original flag) and whether
+//                           it is an earlier candidate (its decision counts);
+//                           the decision of every candidate that earlier
+//                           ones cannot change, the list of the others;
+//   checksol_resolve_kernel one block iterating a fixpoint over that list in
+//                           which every candidate sees the current decision
+//                           of its earlier candidate neighbours and the fixed
+//                           flags of everything else; the dependencies point
+//                           to strictly earlier zones, so the fixpoint is
+//                           unique and a chain of length L settles after L
+//                           sweeps: exactly the reference's sequential result;
+//   checksol_apply_kernel   the decisions into pflag, candmap back to -1.
+// A failed neighbour's ratio is -1 in the reference, whose |.| = 1 votes for
+// nothing, so a neighbour's vote is its precomputed bit while it is not
+// failed; the votes count only while neighbour 0's ratio is >= 0, i.e. while
+// neighbour 0 is not failed and its gamma ratio is not negative or NaN
+// (pd[0] >= 0 gates every vote in fixup.c:530-540).
+__device__ __forceinline__ void checksol_neighbours(const Dims &d, long long z, long long nb[8]) {
+  const long long o1 = (long long)d.nt2 * d.nt3, o2 = d.nt3;
+  // neighbour order of fixup.c:508-526
+  nb[0] = z + d.s2 * o2;
+  nb[1] = z - d.s2 * o2;
+  nb[2] = z + d.s1 * o1;
+  nb[3] = z - d.s1 * o1;
+  nb[4] = z + d.s1 * o1 + d.s2 * o2;
+  nb[5] = z + d.s1 * o1 - d.s2 * o2;
+  nb[6] = z + d.s1 * o1 + d.s2 * o2;
+  nb[7] = z - d.s1 * o1 - d.s2 * o2;
+}
+
+__constant__ int kChecksolCodes[3] = {0, UTOPRIMFAILGAMMAPERC, UTOPRIMFAILUPERC};
+
+// The vote of fixup_checksolution for one candidate (fixup.c:530-556) from
+// its packed bits and the "not failed" mask of its neighbours: 0 = keep the
+// flag, 1 = UTOPRIMFAILGAMMAPERC, 2 = UTOPRIMFAILUPERC.
+__device__ __forceinline__ int checksol_vote(unsigned int b, unsigned int ok) {
+  int vote0 = 0, vote1 = 0, numvotes = 0;
+  if (ok & 1u) {
+    vote0 = __popc(ok & b & 0xffu);
+    vote1 = __popc(ok & (b >> 8) & 0xffu);
+    numvotes = 8;
+  }
+  int v = 0;
+  if (vote0 > numvotes * 0.5) v = 1;
+  if (vote1 > numvotes * 0.5) v = 2;
+  return v;
+}
+
+__global__ void checksol_map_kernel(const long long *__restrict__ cand, const int *__restrict__ pflag, int *candmap,
+                                    int *orig, int cap, const Scalars *sc) {
   int n = sc->ncand;
   if (n > cap) n = cap;
-  if (n == 0) return;
-  const int tid = threadIdx.x, nt = blockDim.x;
-  for (int a = tid; a < n; a += nt) {
-    long long z = cand[a];
+  for (int a = blockIdx.x * blockDim.x + threadIdx.x; a < n; a += gridDim.x * blockDim.x) {
+    const long long z = cand[a];
     candmap[z] = a;
     orig[a] = pflag[z];
-    dec[a] = orig[a];
   }
-  __syncthreads();
+}
+
+// packed per candidate: bits 0-7 gamma vote, 8-15 u vote, 16-23 fixed
+// neighbour not failed, 24-31 neighbour is an earlier candidate.  The
+// earlier candidates' decisions can change this one's when neighbour 0 is
+// such a candidate or when the vote differs between all of them failed and
+// all of them not (the votes only grow with more neighbours not failed):
+// those candidates go to deplist with their original flag as the first
+// guess; every other candidate's decision is final here.
+__global__ void checksol_prep_kernel(Dims d, const double *__restrict__ pv, const double *__restrict__ gammacheck,
+                                     const int *__restrict__ pflag, const long long *__restrict__ cand,
+                                     const int *__restrict__ candmap, const int *__restrict__ orig,
+                                     int *__restrict__ dec, unsigned int *__restrict__ bits,
+                                     int *__restrict__ deplist, int cap, Scalars *sc) {
+  int n = sc->ncand;
+  if (n > cap) n = cap;
+  for (int a = blockIdx.x * blockDim.x + threadIdx.x; a < n; a += gridDim.x * blockDim.x) {
+    const long long z = cand[a];
+    const double gc = gammacheck[z], uc = pv[(long long)UU * d.nz + z];
+    long long nb[8];
+    checksol_neighbours(d, z, nb);
+    unsigned int v0 = 0, v1 = 0, okfix = 0, earlier = 0;
+    bool gate = true;
+#pragma unroll
+    for (int q = 0; q < 8; q++) {
+      const double pd = gammacheck[nb[q]] / gc;
+      const double pd2 = pv[(long long)UU * d.nz + nb[q]] / uc;
+      if (q == 0) gate = pd >= 0.0;
+      if ((fabs(pd) > 2.0) || (fabs(pd) < 1.0 / 2.0)) v0 |= 1u << q;
+      if ((fabs(pd2) > 10.0) || (fabs(pd2) < 1.0 / 10.0)) v1 |= 1u << q;
+      if (nb[q] < z && candmap[nb[q]] >= 0) earlier |= 1u << q;
+      else if (pflag[nb[q]] <= UTOPRIMNOFAIL) okfix |= 1u << q;
+    }
+    // a not-failed neighbour 0 with a negative (or NaN) ratio gates all votes
+    if (!gate) v0 = v1 = 0;
+    const unsigned int bw = v0 | (v1 << 8) | (okfix << 16) | (earlier << 24);
+    bits[a] = bw;
+    const int vlo = checksol_vote(bw, okfix);
+    if (earlier != 0 && ((earlier & 1u) || vlo != checksol_vote(bw, okfix | earlier))) {
+      dec[a] = orig[a];
+      deplist[atomicAdd(&sc->ndep, 1)] = a;
+    } else {
+      dec[a] = vlo ? kChecksolCodes[vlo] : orig[a];
+    }
+  }
+}
+
+// one block: sweeps over the dependent candidates until no decision changes
+__global__ void __launch_bounds__(1024) checksol_resolve_kernel(Dims d, const long long *__restrict__ cand,
+                                                                const int *__restrict__ candmap,
+                                                                const int *__restrict__ orig, int *dec,
+                                                                const unsigned int *__restrict__ bits,
+                                                                const int *__restrict__ deplist, int cap, Scalars *sc) {
+  int m = sc->ndep;
+  if (m > cap) m = cap;
+  if (m == 0) return;
   __shared__ int changed;
-  const long long o1 = (long long)d.nt2 * d.nt3, o2 = d.nt3;
-  // a chain can be at most n long; the sweep count is also capped so that a
-  // pathological input ends with an error flag instead of a long kernel
-  const int max_sweeps = n + 1 < 4096 ? n + 1 : 4096;
+  // a chain can be at most m long; the sweep count is also capped so that a
+  // pathological input ends with an error bit instead of a long kernel
+  const int max_sweeps = m + 1 < 4096 ? m + 1 : 4096;
   for (int sweep = 0; sweep < max_sweeps; sweep++) {
-    if (sweep == max_sweeps - 1 && tid == 0 && max_sweeps < n + 1) atomicOr(&sc->overflow, 4);
-    if (tid == 0) changed = 0;
+    if (sweep == max_sweeps - 1 && threadIdx.x == 0 && max_sweeps < m + 1) atomicOr(&sc->overflow, 4);
+    if (threadIdx.x == 0) changed = 0;
     __syncthreads();
-    for (int a = tid; a < n; a += nt) {
-      long long z = cand[a];
-      double gc = gammacheck[z], uc = pv[(long long)UU * d.nz + z];
-      // neighbour order of fixup.c:508-526
-      long long nb[8] = {z + d.s2 * o2,        z - d.s2 * o2,        z + d.s1 * o1,        z - d.s1 * o1,
-                         z + d.s1 * o1 + d.s2 * o2, z + d.s1 * o1 - d.s2 * o2, z + d.s1 * o1 + d.s2 * o2,
-                         z - d.s1 * o1 - d.s2 * o2};
-      double pd[8], pd2[8];
+    for (int e = threadIdx.x; e < m; e += blockDim.x) {
+      const int a = deplist[e];
+      const unsigned int b = bits[a];
+      unsigned int ok = (b >> 16) & 0xffu;
+      const unsigned int earlier = b >> 24;
+      long long nb[8];
+      checksol_neighbours(d, cand[a], nb);
 #pragma unroll
-      for (int q = 0; q < 8; q++) {
-        int f = pflag[nb[q]];
-        if (nb[q] < z) {
-          int c = candmap[nb[q]];
-          if (c >= 0) f = dec[c];
-        }
-        pd[q] = (f <= UTOPRIMNOFAIL) ? (gammacheck[nb[q]] / gc) : -1;
-        pd2[q] = (f <= UTOPRIMNOFAIL) ? (pv[(long long)UU * d.nz + nb[q]] / uc) : -1;
-      }
-      int vote0 = 0, vote1 = 0, numvotes = 0;
-#pragma unroll
-      for (int l = 0; l < 8; l++) {
-        if (pd[0] >= 0.0) {
-          if ((fabs(pd[l]) > 2.0) || (fabs(pd[l]) < 1.0 / 2.0)) vote0++;
-          if ((fabs(pd2[l]) > 10.0) || (fabs(pd2[l]) < 1.0 / 10.0)) vote1++;
-          numvotes++;
-        }
-      }
-      int nd = orig[a];
-      if (vote0 > numvotes * 0.5) nd = UTOPRIMFAILGAMMAPERC;
-      if (vote1 > numvotes * 0.5) nd = UTOPRIMFAILUPERC;
+      for (int q = 0; q < 8; q++)
+        if ((earlier >> q) & 1u)
+          if (dec[candmap[nb[q]]] <= UTOPRIMNOFAIL) ok |= 1u << q;
+      const int v = checksol_vote(b, ok);
+      const int nd = v ? kChecksolCodes[v] : orig[a];
       if (nd != dec[a]) {
         dec[a] = nd;
         changed = 1;
@@ -898,9 +979,15 @@ __global__ void __launch_bounds__(1024) checksol_resolve_kernel(Dims d, const do
     if (!changed) break;
     __syncthreads();
   }
-  __syncthreads();
-  for (int a = tid; a < n; a += nt) {
-    long long z = cand[a];
+}
+
+// the decisions into pflag; candmap back to -1
+__global__ void checksol_apply_kernel(const long long *__restrict__ cand, const int *__restrict__ dec, int *pflag,
+                                      int *candmap, int cap, const Scalars *sc) {
+  int n = sc->ncand;
+  if (n > cap) n = cap;
+  for (int a = blockIdx.x * blockDim.x + threadIdx.x; a < n; a += gridDim.x * blockDim.x) {
+    const long long z = cand[a];
     pflag[z] = dec[a];
     candmap[z] = -1;
   }
@@ -1172,6 +1259,7 @@ __global__ void reset_stage_kernel(Scalars *sc) {
   sc->ndtbits[3] = big;
   sc->nfail = 0;
   sc->ncand = 0;
+  sc->ndep = 0;
   sc->nfixlist = 0;
 }
 
@@ -1446,6 +1534,8 @@ struct hgpu_ctx {
   double *gammacheck = nullptr;
   long long *cand = nullptr, *fixlist = nullptr;
   int *cand_orig = nullptr, *cand_dec = nullptr, *candmap = nullptr;
+  unsigned int *cand_bits = nullptr;  // checksolution: per-candidate vote and neighbour bits
+  int *cand_deplist = nullptr;        // checksolution: candidates whose vote earlier ones can change
   double *fixvals = nullptr;
   int cap = 0;
   Scalars *sc = nullptr;
@@ -1576,7 +1666,7 @@ void hgpu_destroy(hgpu_ctx *x) {
   collect_profile(x);
   for (cudaEvent_t e : x->freelist) cudaEventDestroy(e);
   void *ptrs[] = {x->p, x->pk, x->uf, x->ucum, x->F[1], x->F[2], x->F[3], x->E, x->G, x->pflag, x->gammacheck,
-                  x->cand, x->fixlist, x->cand_orig, x->cand_dec, x->candmap, x->fixvals, x->sc, x->staging, x->istaging,
+                  x->cand, x->fixlist, x->cand_orig, x->cand_dec, x->cand_bits, x->cand_deplist, x->candmap, x->fixvals, x->sc, x->staging, x->istaging,
                   x->pL, x->pR, x->w5pu, x->bsqf, x->ffc, x->bondi_tab, x->cell_inst, x->inst, x->progress, x->pk1, x->ui};
   for (void *q : ptrs)
     if (q) cudaFree(q);
@@ -1717,6 +1807,8 @@ int hgpu_create(const hgpu_config *cfg, hgpu_ctx **out) {
             cudaMalloc(&x->fixlist, sizeof(long long) * x->cap) == cudaSuccess &&
             cudaMalloc(&x->cand_orig, sizeof(int) * x->cap) == cudaSuccess &&
             cudaMalloc(&x->cand_dec, sizeof(int) * x->cap) == cudaSuccess &&
+            cudaMalloc(&x->cand_bits, sizeof(unsigned int) * x->cap) == cudaSuccess &&
+            cudaMalloc(&x->cand_deplist, sizeof(int) * x->cap) == cudaSuccess &&
             cudaMalloc(&x->candmap, sizeof(int) * nz) == cudaSuccess &&
             cudaMalloc(&x->fixvals, sizeof(double) * 5 * x->cap) == cudaSuccess &&
             cudaMalloc(&x->sc, sizeof(Scalars)) == cudaSuccess &&
@@ -2159,8 +2251,17 @@ static void launch_stage_fixup(hgpu_ctx *x, int timeorder) {
   double *ufv = (x->cfg.doenoflux == HGPU_ENOFINITEVOLUME && finalstep) ? x->ucum : nullptr;
   LAUNCH(x, K_CHECK_GAMMA, checksol_gamma_kernel, grid_for(x->dq_box.size(), 128), 128, d, x->P, x->dq_box, pf, x->G,
          x->gammacheck, x->cand, x->cap, x->sc);
-  LAUNCH(x, K_CHECK_RESOLVE, checksol_resolve_kernel, 1, 1024, d, pf, x->gammacheck, x->pflag, x->cand, x->candmap,
-         x->cand_orig, x->cand_dec, x->cap, x->sc);
+  // grid-stride over the device-side candidate count; idle blocks exit at once
+  int cgrid = (int)grid_for(x->cap, 256);
+  if (cgrid > 592) cgrid = 592;
+  LAUNCH(x, K_CHECK_RESOLVE, checksol_map_kernel, cgrid, 256, x->cand, x->pflag, x->candmap, x->cand_orig, x->cap,
+         x->sc);
+  LAUNCH(x, K_CHECK_RESOLVE, checksol_prep_kernel, cgrid, 256, d, pf, x->gammacheck, x->pflag, x->cand, x->candmap,
+         x->cand_orig, x->cand_dec, x->cand_bits, x->cand_deplist, x->cap, x->sc);
+  LAUNCH(x, K_CHECK_RESOLVE, checksol_resolve_kernel, 1, 1024, d, x->cand, x->candmap, x->cand_orig, x->cand_dec,
+         x->cand_bits, x->cand_deplist, x->cap, x->sc);
+  LAUNCH(x, K_CHECK_RESOLVE, checksol_apply_kernel, cgrid, 256, x->cand, x->cand_dec, x->pflag, x->candmap, x->cap,
+         x->sc);
   LAUNCH(x, K_FIX_COLLECT, fixup_collect_kernel, grid_for(x->active_box.size(), 256), 256, d, x->P, x->active_box, x->pflag,
          x->fixlist, x->cap, x->sc);
   // grid-stride over the device-side list length; idle blocks exit at once
@@ -2190,7 +2291,11 @@ static int read_stats(hgpu_ctx *x, hgpu_stats *st) {
     st->nfixed = s.nfixed;
   }
   if (s.overflow) {
-    set_err("fixup list capacity exceeded (%s%d)", "", s.overflow);
+    // bit 0: checksolution candidate list full; bit 1: fixup list full;
+    // bit 2: a checksolution dependency chain longer than the sweep cap
+    set_err("%s (overflow bits %d)",
+            (s.overflow & 3) ? "fixup list capacity exceeded" : "checksolution dependency chain over 4096 zones",
+            s.overflow);
     return HGPU_E_PHYSICS;
   }
   if (s.err) {
@@ -3085,7 +3190,7 @@ extern "C" size_t hgpu_context_bytes(const hgpu_config *c) {
              + (size_t)nz                     // b^2 flags
              + sizeof(unsigned int) * NFFC * nz  // failure/floor counters
              + sizeof(double) * nz            // gamma check
-             + cap * (2 * sizeof(long long) + 2 * sizeof(int) + 5 * sizeof(double))
+             + cap * (2 * sizeof(long long) + 4 * sizeof(int) + 5 * sizeof(double))
              + plane;                         // staging for uploads and downloads
   if (c->lim == HGPU_LIM_WENO5) b += 2 * plane + sizeof(double) * 2 * nz;  // pL, pR, dP/P state pieces
   if (c->timeorder >= 3) b += plane;                     // pk1

@@ -103,3 +103,37 @@ def domain(prob, ng=3, cour=0.5):
     dom.p = primitives(prob, ng)
     dom.meta = dict(kind="shock tube", n=n, gam=prob.gam)
     return dom
+
+
+def _main(argv=None):
+    """Advance a seeded batch of problems on the GPU as one batch context:
+    `python -m harm_finalwham_b200.riemann --count 256 --steps 20` (steps of
+    the shared step graph; 0 runs every instance to tf)."""
+    import argparse
+    from .gpu import HarmBatch
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--count", type=int, default=256)
+    ap.add_argument("--seed", type=int, default=2024)
+    ap.add_argument("--tf", type=float, default=0.4)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--ng", type=int, default=3)
+    args = ap.parse_args(argv)
+    probs = draw(args.count, seed=args.seed)
+    b = HarmBatch([p.n for p in probs], [p.dx for p in probs], [p.gam for p in probs], [args.tf] * len(probs),
+                  ng=args.ng, lim="MC", flux="HLL", cour=0.5)
+    try:
+        b.upload_geometry(*minkowski_geometry(b.nt[0]))
+        b.upload_state(b.join([primitives(p, args.ng) for p in probs]), None, 0.0, 0.0)
+        b.init_dt()
+        if args.steps > 0:
+            b.step_ch(args.steps)
+        else:
+            b.run()
+        b.sync()
+        print(f"{args.count} problems, {sum(p.n for p in probs)} zones: ok")
+    finally:
+        b.close()
+
+
+if __name__ == "__main__":
+    _main()
