@@ -2244,10 +2244,9 @@ static void launch_stage_advance(hgpu_ctx *x, int timeorder) {
     LAUNCH(x, K_BOUND_PFLAG, bound_pflag_kernel, grid_for(d.nz, 256), 256, d, x->P, x->pflag, x->sc);
 }
 
-static void launch_stage_fixup(hgpu_ctx *x, int timeorder) {
+// fixup_checksolution and fixup_utoprim on pf with the context's flags
+static void launch_checksol_fixup(hgpu_ctx *x, double *pf, int finalstep) {
   const Dims &d = x->d;
-  double *pf = stage_output(x, timeorder);
-  const int finalstep = (timeorder == num_orders(x) - 1);
   double *ufv = (x->cfg.doenoflux == HGPU_ENOFINITEVOLUME && finalstep) ? x->ucum : nullptr;
   LAUNCH(x, K_CHECK_GAMMA, checksol_gamma_kernel, grid_for(x->dq_box.size(), 128), 128, d, x->P, x->dq_box, pf, x->G,
          x->gammacheck, x->cand, x->cap, x->sc);
@@ -2271,6 +2270,11 @@ static void launch_stage_fixup(hgpu_ctx *x, int timeorder) {
          x->cap, finalstep, x->sc);
   LAUNCH(x, K_FIX_SCATTER, fixup_scatter_kernel, fixgrid, 128, d, x->P, pf, x->pflag, x->fixlist, x->fixvals, x->cap,
          finalstep, x->sc, x->G, ufv);
+}
+
+static void launch_stage_fixup(hgpu_ctx *x, int timeorder) {
+  double *pf = stage_output(x, timeorder);
+  launch_checksol_fixup(x, pf, timeorder == num_orders(x) - 1);
   launch_bound(x, pf);
 }
 
@@ -3394,6 +3398,23 @@ extern "C" int hgpu_stage_fixup(hgpu_ctx *x, int stage) {
   launch_stage_fixup(x, stage);
   CUDA_TRY(cudaGetLastError());
   return HGPU_OK;
+}
+
+// post_fixup (fixup.c:37-96) on the context's state and flags, between
+// steps: bound_pflag, fixup_checksolution, fixup_utoprim.  The candidate and
+// fixup lists start empty; the stage's dt accumulators are left alone.
+extern "C" int hgpu_post_fixup(hgpu_ctx *x, int finalstep, hgpu_stats *stats) {
+  if (!x || x->P.cell_inst) return HGPU_E_INVALID;
+  if (boundaries_ready(x)) return HGPU_E_INVALID;
+  const Dims &d = x->d;
+  clear_counters(x);
+  CUDA_TRY(cudaMemsetAsync(&x->sc->ncand, 0, sizeof(int), x->stream));
+  CUDA_TRY(cudaMemsetAsync(&x->sc->ndep, 0, sizeof(int), x->stream));
+  CUDA_TRY(cudaMemsetAsync(&x->sc->nfixlist, 0, sizeof(int), x->stream));
+  LAUNCH(x, K_BOUND_PFLAG, bound_pflag_kernel, grid_for(d.nz, 256), 256, d, x->P, x->pflag, x->sc);
+  launch_checksol_fixup(x, x->p, finalstep ? 1 : 0);
+  CUDA_TRY(cudaGetLastError());
+  return read_stats(x, stats);
 }
 
 // start-up ndt (set_dt, advance.c:957) of a split domain: the fluxes of p,

@@ -91,6 +91,7 @@ def load_library(path=None):
     L.hgpu_advance_stage.argtypes = [ctypes.c_void_p, ctypes.c_int, _dp, _P(hgpu_stats)]
     L.hgpu_fluxcalc.argtypes = [ctypes.c_void_p, ctypes.c_int, _dp, _dp, _dp, _dp, _dp, _dp]
     L.hgpu_bound_prim.argtypes = [ctypes.c_void_p, ctypes.c_int]
+    L.hgpu_post_fixup.argtypes = [ctypes.c_void_p, ctypes.c_int, _P(hgpu_stats)]
     L.hgpu_utoprim_batch.argtypes = [_dp, _dp, _dp, _dp, _dp, _ip, ctypes.c_longlong, ctypes.c_double,
                                      ctypes.c_double, _P(ctypes.c_longlong)]
     L.hgpu_utoprimgen_batch.argtypes = [_dp, _dp, _dp, _dp, _dp, _ip, ctypes.c_longlong, ctypes.c_double,
@@ -156,7 +157,7 @@ def load_library(path=None):
                  "hgpu_free_pinned", "hgpu_fp64_peak"):
         getattr(L, name).restype = ctypes.c_int
     for name in ("hgpu_create", "hgpu_upload_geometry", "hgpu_upload_state", "hgpu_download_state", "hgpu_step_ch",
-                 "hgpu_advance_stage", "hgpu_fluxcalc", "hgpu_bound_prim", "hgpu_utoprim_batch", "hgpu_utoprimgen_batch",
+                 "hgpu_advance_stage", "hgpu_fluxcalc", "hgpu_bound_prim", "hgpu_post_fixup", "hgpu_utoprim_batch", "hgpu_utoprimgen_batch",
                  "hgpu_device_prims", "hgpu_sync", "hgpu_create_batch", "hgpu_batch_layout", "hgpu_batch_status", "hgpu_batch_set_time",
                  "hgpu_step_graph", "hgpu_autotune", "hgpu_set_tuning", "hgpu_batch_run", "hgpu_diagnostics", "hgpu_download_conserved", "hgpu_upload_conserved",
                  "hgpu_write_rdump", "hgpu_read_rdump", "hgpu_download_failfloorcount", "hgpu_set_bondi_boundaries", "hgpu_upload_active", "hgpu_download_active", "hgpu_server_create", "hgpu_server_submit", "hgpu_server_submit_borrowed",
@@ -484,6 +485,13 @@ class HarmGPU:
 
     def bound_prim(self, which=0):
         _check(self.L, self.L.hgpu_bound_prim(self.h, int(which)))
+
+    def post_fixup(self, finalstep=1):
+        """hgpu_post_fixup: bound_pflag, fixup_checksolution, fixup_utoprim on
+        the state and its flags; returns hgpu_stats."""
+        st = hgpu_stats()
+        _check(self.L, self.L.hgpu_post_fixup(self.h, int(finalstep), ctypes.byref(st)))
+        return st
 
     def sync(self):
         _check(self.L, self.L.hgpu_sync(self.h))

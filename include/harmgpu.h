@@ -33,7 +33,7 @@
 extern "C" {
 #endif
 
-#define HGPU_ABI_VERSION 15
+#define HGPU_ABI_VERSION 16
 
 /* return codes */
 #define HGPU_OK 0
@@ -187,6 +187,15 @@ int hgpu_fluxcalc(hgpu_ctx *ctx, int which, double *F1, double *F2, double *F3, 
 
 /* bound_prim (step_ch.c:568) on p (which=0) or pk (which=1). */
 int hgpu_bound_prim(hgpu_ctx *ctx, int which);
+
+/* post_fixup (fixup.c:37-96) on the state p and its flags, as step_ch.c:144
+   and :403 call it: bound_pflag, fixup_checksolution, fixup_utoprim
+   (finalstep as the reference's argument: fixup_utoprim's final-step
+   counting, and with the finite-volume scheme the diag_fixup corrections of
+   unew).  The bound_prim that step_ch runs after it is hgpu_bound_prim.
+   Synchronises; stats (may be NULL) receives nfixed and the error bits.
+   Not for batch contexts, whose fixups run per instance inside a step. */
+int hgpu_post_fixup(hgpu_ctx *ctx, int finalstep, hgpu_stats *stats);
 
 /* Utoprimgen (utoprimgen.c:23) for a batch of n zones in host memory:
    U (evolved conserved, with gdet) [n][8], per-zone CENT metric gcov/gcon [n][16],

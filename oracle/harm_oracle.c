@@ -2462,6 +2462,22 @@ int hgo_step_u(const hgo_config *c, const hgo_geometry *g, double *p, int *pflag
   return d.err;
 }
 
+/* post_fixup (fixup.c:37-96) on its own: bound_pflag, fixup_checksolution,
+   fixup_utoprim; unew (may be NULL) receives the finite-volume scheme's
+   diag_fixup corrections on a final step */
+int hgo_post_fixup(const hgo_config *c, const hgo_geometry *g, double *p, int *pflag, int finalstep, double *unew)
+{
+  dom d;
+  scratch sc;
+  dom_init(&d, c, g);
+  if (alloc_scratch(&d, &sc)) return -1;
+  bound_pflag(&d, pflag);
+  fixup_checksolution(&d, p, pflag, sc.gammacheck);
+  fixup_utoprim(&d, p, sc.ptoavg, pflag, finalstep, unew);
+  free_scratch(&sc);
+  return d.err;
+}
+
 int hgo_bound_prim(const hgo_config *c, const hgo_geometry *g, double *p)
 {
   dom d;

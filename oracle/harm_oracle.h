@@ -115,6 +115,12 @@ int hgo_utoprim_batch(const double *U, const double *gcov, const double *gcon, c
 int hgo_utoprim_batch_v(const double *U, const double *gcov, const double *gcon, const double *gdet, double *pr,
                         int *pflag, long n, double gam, double gammafail, int utoprimversion, long *iters);
 
+/* post_fixup (fixup.c:37-96) on p and pflag in place: bound_pflag,
+   fixup_checksolution, fixup_utoprim (the bound_prim that follows it in
+   step_ch is not part of it).  unew may be NULL; with the finite-volume
+   scheme on a final step it receives the diag_fixup corrections. */
+int hgo_post_fixup(const hgo_config *c, const hgo_geometry *g, double *p, int *pflag, int finalstep, double *unew);
+
 /* Bound the primitives in place (bound_prim). */
 int hgo_bound_prim(const hgo_config *c, const hgo_geometry *g, double *p);
 

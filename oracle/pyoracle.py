@@ -262,6 +262,10 @@ class Oracle:
         L.hgo_pi2u.argtypes = [ctypes.POINTER(hgo_config), ctypes.POINTER(hgo_geometry),
                                ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double)]
         L.hgo_pi2u.restype = ctypes.c_int
+        L.hgo_post_fixup.argtypes = [ctypes.POINTER(hgo_config), ctypes.POINTER(hgo_geometry),
+                                     ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_int), ctypes.c_int,
+                                     ctypes.POINTER(ctypes.c_double)]
+        L.hgo_post_fixup.restype = ctypes.c_int
         L.hgo_utoprim_batch.argtypes = [ctypes.POINTER(ctypes.c_double)] * 5 + [ctypes.POINTER(ctypes.c_int),
                                         ctypes.c_long, ctypes.c_double, ctypes.c_double,
                                         ctypes.POINTER(ctypes.c_long)]
@@ -299,6 +303,14 @@ class Oracle:
                               ctypes.byref(dt), nsteps, ctypes.byref(st))
         pr.t, pr.dt = t.value, dt.value
         return st
+
+    def post_fixup(self, pr, finalstep=1):
+        """post_fixup (fixup.c:37-96) on pr.p / pr.pflag in place; returns the
+        error bits."""
+        assert pr.p.flags.c_contiguous and pr.pflag.flags.c_contiguous
+        u = getattr(pr, "u", None)
+        return self.lib.hgo_post_fixup(ctypes.byref(pr.config()), ctypes.byref(self.geometry(pr)), _dp(pr.p),
+                                       _ip(pr.pflag), int(finalstep), _dp(u) if u is not None else None)
 
     def pi2u(self, pr):
         """pi2Uavg: the conserved state U(p) in every zone (init_conservatives)."""
