@@ -2478,6 +2478,20 @@ int hgo_post_fixup(const hgo_config *c, const hgo_geometry *g, double *p, int *p
   return d.err;
 }
 
+/* fixup_checksolution (fixup.c:460-560) alone on p and pflag; gammacheck
+   (may be NULL) receives the Lorentz factors it compares, zone layout */
+int hgo_checksolution(const hgo_config *c, const hgo_geometry *g, const double *p, int *pflag, double *gammacheck)
+{
+  dom d;
+  scratch sc;
+  dom_init(&d, c, g);
+  if (alloc_scratch(&d, &sc)) return -1;
+  fixup_checksolution(&d, p, pflag, sc.gammacheck);
+  if (gammacheck) memcpy(gammacheck, sc.gammacheck, sizeof(double) * dom_ntot(&d));
+  free_scratch(&sc);
+  return d.err;
+}
+
 int hgo_bound_prim(const hgo_config *c, const hgo_geometry *g, double *p)
 {
   dom d;

@@ -121,6 +121,10 @@ int hgo_utoprim_batch_v(const double *U, const double *gcov, const double *gcon,
    scheme on a final step it receives the diag_fixup corrections. */
 int hgo_post_fixup(const hgo_config *c, const hgo_geometry *g, double *p, int *pflag, int finalstep, double *unew);
 
+/* fixup_checksolution (fixup.c:460-560) alone: pflag in place; gammacheck
+   (may be NULL, else zone layout) receives the Lorentz factors compared. */
+int hgo_checksolution(const hgo_config *c, const hgo_geometry *g, const double *p, int *pflag, double *gammacheck);
+
 /* Bound the primitives in place (bound_prim). */
 int hgo_bound_prim(const hgo_config *c, const hgo_geometry *g, double *p);
 

@@ -266,6 +266,10 @@ class Oracle:
                                      ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_int), ctypes.c_int,
                                      ctypes.POINTER(ctypes.c_double)]
         L.hgo_post_fixup.restype = ctypes.c_int
+        L.hgo_checksolution.argtypes = [ctypes.POINTER(hgo_config), ctypes.POINTER(hgo_geometry),
+                                        ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_int),
+                                        ctypes.POINTER(ctypes.c_double)]
+        L.hgo_checksolution.restype = ctypes.c_int
         L.hgo_utoprim_batch.argtypes = [ctypes.POINTER(ctypes.c_double)] * 5 + [ctypes.POINTER(ctypes.c_int),
                                         ctypes.c_long, ctypes.c_double, ctypes.c_double,
                                         ctypes.POINTER(ctypes.c_long)]
@@ -311,6 +315,15 @@ class Oracle:
         u = getattr(pr, "u", None)
         return self.lib.hgo_post_fixup(ctypes.byref(pr.config()), ctypes.byref(self.geometry(pr)), _dp(pr.p),
                                        _ip(pr.pflag), int(finalstep), _dp(u) if u is not None else None)
+
+    def checksolution(self, pr):
+        """fixup_checksolution (fixup.c:460-560) alone on pr.pflag in place;
+        returns (error bits, the Lorentz factors it compared)."""
+        assert pr.p.flags.c_contiguous and pr.pflag.flags.c_contiguous
+        gam = np.zeros(pr.pflag.shape)
+        e = self.lib.hgo_checksolution(ctypes.byref(pr.config()), ctypes.byref(self.geometry(pr)), _dp(pr.p),
+                                       _ip(pr.pflag), _dp(gam))
+        return e, gam
 
     def pi2u(self, pr):
         """pi2Uavg: the conserved state U(p) in every zone (init_conservatives)."""

@@ -1,0 +1,89 @@
+"""fixup_checksolution's visiting order, on the CPU.
+
+The reference visits its candidates in (i, j, k) order and each visit may
+flag the zone for its later neighbours; the device resolves this with the
+formulation of tests/checksol_model.py (independent candidates final at
+once, a fixpoint over the rest).  Here: the sequential restatement equals
+the oracle's checksolution on states drawn to be rich in candidates, and
+the device formulation equals the sequential loop on many random grids (1D,
+2D, 3D; dense candidates, long chains, every flag code, zero and negative u,
+NaN gamma), whatever order the candidates are listed and swept in."""
+import numpy as np
+import pytest
+
+from oracle.pyoracle import Oracle
+from tests.checksol_model import FAIL_CODES, craft, device_scheme, sequential
+from tests.fixtures import load
+
+
+@pytest.mark.parametrize("name", ["torus2d_16x16_mc_hll", "torus3d_12x12x6_mc_hll"])
+def test_sequential_restatement_matches_oracle(name):
+    orc = Oracle()
+    for seed in range(4):
+        pr, _ = load(name)
+        craft(pr, 2000 + seed)
+        flags0 = pr.pflag.copy()
+        err, gam = orc.checksolution(pr)
+        assert err == 0
+        want = sequential(flags0, gam, pr.p[..., 1], pr.n, pr.g, pr.s)
+        assert np.array_equal(pr.pflag, want)
+        assert np.count_nonzero(pr.pflag != flags0) > 0
+
+
+def _random_grid(rng, n, dense):
+    s = tuple(1 if x > 1 else 0 for x in n)
+    g = tuple(2 if x > 1 else 0 for x in n)
+    nt = tuple(x + 2 * y for x, y in zip(n, g))
+    gam_choices = [1.0, 1.5, 1.99, 2.0, 2.5, 3.9, 4.0, 4.1, 8.0, 8.1, 16.5, np.nan]
+    p = [.02, .04, .04, .1, .15, .1, .1, .1, .1, .1, .1, .05] if dense else \
+        [.2, .2, .1, .1, .1, .05, .05, .05, .05, .05, .04, .01]
+    gam = rng.choice(gam_choices, size=nt, p=p)
+    uu = 10.0 ** rng.uniform(-3.0, 1.0, size=nt)
+    uu[rng.random(nt) < 0.03] = 0.0
+    uu[rng.random(nt) < 0.03] *= -1.0
+    fail = rng.random(nt) < rng.uniform(0.05, 0.5)
+    flags = np.where(fail, rng.choice(FAIL_CODES, size=nt), 0).astype(np.int32)
+    return flags, gam, uu, g, s
+
+
+@pytest.mark.parametrize("n", [(400, 1, 1), (20, 20, 1), (10, 9, 4)])
+def test_device_formulation_equals_sequential_loop(n):
+    rng = np.random.default_rng(7)
+    ndep = nchanged = norder = 0
+    for trial in range(40):
+        flags, gam, uu, g, s = _random_grid(rng, n, dense=trial % 2 == 0)
+        want = sequential(flags, gam, uu, n, g, s)
+        for jacobi in (False, True):
+            got, m = device_scheme(flags, gam, uu, n, g, s, rng, jacobi=jacobi)
+            assert np.array_equal(got, want), f"trial {trial} jacobi {jacobi}"
+            ndep += m
+        nchanged += int(np.count_nonzero(want != flags))
+        norder += int(np.count_nonzero(want != sequential(flags, gam, uu, n, g, s, order_free=True)))
+    # the grids exercise the votes, the visiting order and the dependent
+    # candidates
+    assert nchanged > 0
+    if n[1] > 1:
+        assert norder > 0
+    if n[1] > 1:
+        assert ndep > 0
+
+
+def test_device_formulation_on_a_long_chain():
+    # a diagonal of candidates each voted failed by its neighbours, so every
+    # decision waits for the one before it
+    n = (40, 40, 1)
+    g, s = (2, 2, 0), (1, 1, 0)
+    nt = (44, 44, 1)
+    gam = np.full(nt, 1.0)
+    uu = np.ones(nt)
+    for d in range(40):
+        gam[d + 2, d + 2, 0] = 2.5
+        gam[d + 2, min(d + 3, 43), 0] = 8.0
+    flags = np.zeros(nt, dtype=np.int32)
+    rng = np.random.default_rng(3)
+    want = sequential(flags, gam, uu, n, g, s)
+    assert np.count_nonzero(want != sequential(flags, gam, uu, n, g, s, order_free=True)) > 30
+    for jacobi in (False, True):
+        got, m = device_scheme(flags, gam, uu, n, g, s, rng, jacobi=jacobi)
+        assert m > 30
+        assert np.array_equal(got, want)

@@ -8,78 +8,19 @@ vote.  The torus steps of the other tests produce few candidates, so these
 states are drawn to make many: Lorentz factors from 1.1 to 9 and internal
 energies over four decades zone by zone (every vote threshold is crossed),
 and failure codes on a quarter of the zones.  A plain-Python restatement of
-the loop shows that the sequential result differs from an order-free one on
-these states, i.e. the chains are exercised; the device's post_fixup
-(checksolution, then fixup_utoprim's neighbour averages) must equal the
-oracle's bit for bit."""
+the loop (tests/checksol_model.py) shows that the sequential result differs
+from an order-free one on these states, i.e. the chains are exercised; the
+device's post_fixup (checksolution, then fixup_utoprim's neighbour averages)
+must equal the oracle's bit for bit."""
 import numpy as np
 import pytest
 
 from harm_finalwham_b200.gpu import HarmGPU
-from oracle.pyoracle import CENT, Oracle
+from oracle.pyoracle import Oracle
+from tests.checksol_model import craft, sequential
 from tests.fixtures import load
 
 pytestmark = pytest.mark.gpu
-
-RHO, UU, U1 = 0, 1, 2
-FAIL_CODES = [1, 1, 1, 9, 10, 11, 12, 13, 14, 15, -1]
-
-
-def craft(pr, seed):
-    """Overwrite pr.p / pr.pflag with a seeded state rich in candidates."""
-    rng = np.random.default_rng(seed)
-    nt = pr.nt
-    g11 = pr.gcov[:nt[0], :nt[1], CENT, 1, 1][:, :, None]
-    target = rng.choice([1.1, 1.6, 2.1, 2.6, 3.5, 5.0, 9.0], size=nt, p=[.1, .1, .2, .2, .15, .15, .1])
-    sign = rng.choice([-1.0, 1.0], size=nt)
-    pr.p[..., U1] = sign * np.sqrt(target * target - 1.0) / np.sqrt(g11)
-    pr.p[..., U1 + 1] = 0.0
-    pr.p[..., U1 + 2] = 0.0
-    pr.p[..., RHO] = 10.0 ** rng.uniform(-2.0, 0.0, size=nt)
-    pr.p[..., UU] = pr.p[..., RHO] * 10.0 ** rng.uniform(-4.0, 0.0, size=nt)
-    fail = rng.random(nt) < 0.25
-    pr.pflag[...] = np.where(fail, rng.choice(FAIL_CODES, size=nt), 0).astype(np.int32)
-    pr.p = np.ascontiguousarray(pr.p)
-    pr.pflag = np.ascontiguousarray(pr.pflag)
-
-
-def checksolution_py(pr, pflag, sequential):
-    """fixup_checksolution as a Python loop; sequential=False reads every
-    neighbour's original flag instead of the flags earlier visits wrote."""
-    nt, g, s = pr.nt, pr.g, pr.s
-    qsq = pr.gcov[:nt[0], :nt[1], CENT, 1, 1][:, :, None] * pr.p[..., U1] ** 2
-    gam = np.sqrt(1.0 + qsq)
-    uu = pr.p[..., UU]
-    src = pflag.copy()
-    out = pflag.copy()
-    for i in range(pr.n[0]):
-        for j in range(pr.n[1]):
-            for k in range(pr.n[2]):
-                z = (i + g[0], j + g[1], k + g[2])
-                if gam[z] < 2.0:
-                    continue
-                # neighbour order of fixup.c:508-526
-                offs = [(0, s[1]), (0, -s[1]), (s[0], 0), (-s[0], 0), (s[0], s[1]), (s[0], -s[1]), (s[0], s[1]),
-                        (-s[0], -s[1])]
-                flags = out if sequential else src
-                pd, pd2 = [], []
-                for di, dj in offs:
-                    nb = (z[0] + di, z[1] + dj, z[2])
-                    ok = flags[nb] <= 0
-                    pd.append(gam[nb] / gam[z] if ok else -1.0)
-                    pd2.append(uu[nb] / uu[z] if ok else -1.0)
-                v0 = v1 = nv = 0
-                for q in range(8):
-                    if pd[0] >= 0.0:
-                        v0 += abs(pd[q]) > 2.0 or abs(pd[q]) < 0.5
-                        v1 += abs(pd2[q]) > 10.0 or abs(pd2[q]) < 0.1
-                        nv += 1
-                if v0 > nv * 0.5:
-                    out[z] = 12
-                if v1 > nv * 0.5:
-                    out[z] = 13
-    return out
-
 
 CASES = [("torus2d_16x16_mc_hll", 1), ("torus2d_16x16_mc_hll", 0), ("torus3d_12x12x6_mc_hll", 1)]
 
@@ -91,8 +32,12 @@ def test_post_fixup_matches_oracle_on_crafted_states(name, finalstep):
     for seed in range(6):
         pr, _ = load(name)
         craft(pr, 1000 + seed)
-        seq = checksolution_py(pr, pr.pflag, True)
-        order_dependent += int(np.count_nonzero(seq != checksolution_py(pr, pr.pflag, False)))
+        # the sequential loop against an order-free pass (every neighbour's
+        # original flag): where they differ, the visiting order matters
+        _, gam = orc.checksolution(pr.copy())
+        seq = sequential(pr.pflag, gam, pr.p[..., 1], pr.n, pr.g, pr.s)
+        free = sequential(pr.pflag, gam, pr.p[..., 1], pr.n, pr.g, pr.s, order_free=True)
+        order_dependent += int(np.count_nonzero(seq != free))
         with HarmGPU.from_problem(pr) as gpu:
             gpu.upload_state(pr.p, pr.pflag, pr.t, pr.dt)
             st = gpu.post_fixup(finalstep)
