@@ -50,3 +50,28 @@ def test_post_fixup_matches_oracle_on_crafted_states(name, finalstep):
         assert same.all(), f"seed {seed}: {np.count_nonzero(~same)} primitive values differ"
     # the drawn states do make checksolution's visiting order matter
     assert order_dependent > 0
+
+
+def test_post_fixup_finite_volume_corrects_unew():
+    # with the finite-volume scheme a final step's fixups carry every
+    # primitive change into the evolved conserved state (diag_fixup,
+    # fixup.c:240-250); unew is compared on the active zones it is defined on
+    orc = Oracle()
+    for seed in range(3):
+        pr, _ = load("torus2d_16x16_mc_hll_fv")
+        craft(pr, 3000 + seed)
+        pr.u = orc.pi2u(pr)
+        with HarmGPU.from_problem(pr) as gpu:
+            gpu.upload_state(pr.p, pr.pflag, pr.t, pr.dt)
+            gpu.upload_conserved(pr.u)
+            st = gpu.post_fixup(1)
+            p, pf, _, _ = gpu.download_state()
+            u = gpu.active(gpu.download_conserved())
+        q = pr.copy()
+        assert orc.post_fixup(q, 1) == 0
+        assert st.err == 0 and st.nfixed > 0
+        assert np.array_equal(pf, q.pflag)
+        assert ((p == q.p) | (np.isnan(p) & np.isnan(q.p))).all()
+        uq = q.active(q.u)
+        assert ((u == uq) | (np.isnan(u) & np.isnan(uq))).all()
+        assert not np.array_equal(uq, pr.active(pr.u))
