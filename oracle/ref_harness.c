@@ -56,6 +56,15 @@
  *   with gdet, gcov[16], gcon[16], gdet, guess primitives[8]) after init(),
  *   and writes <outfile>: n x 8 doubles (primitives), n int32 FLAGUTOPRIMFAIL
  *   flags, n int32 Newton iteration counts (nstroke per zone).
+ *
+ * usage: harm_ref --postfixup <infile> <outfile> <finalstep>
+ *   after init(), replaces the primitives and the FLAGUTOPRIMFAIL flags by
+ *   those of <infile> (the bytes of the reference's p array, N1M x N2M x N3M
+ *   x NPR doubles with its MAXBND ghosts, then N1M x N2M x N3M int32 flags in
+ *   the same zone order), runs the reference's own post_fixup(STAGEM1, p, p,
+ *   finalstep) (fixup.c:37-96: bound_pflag, fixup_checksolution,
+ *   fixup_utoprim) and writes the two arrays back to <outfile> in the same
+ *   form.
  */
 #include "defs.h"  /* defines the reference globals, as the reference main.c does */
 #include <sys/stat.h>
@@ -328,6 +337,31 @@ static int invert_file(const char *in, const char *out)
   return 0;
 }
 
+static int postfixup_file(const char *in, const char *out, int finalstep)
+{
+  const size_t nzone = (size_t)N1M * N2M * N3M;
+  int *fl = (int *)malloc(sizeof(int) * nzone);
+  int *pf = &a_pflag[0][0][0][0];
+  size_t z;
+  FILE *f = fopen(in, "rb");
+  if (!fl || !f || fread(a_p, sizeof(a_p), 1, f) != 1 || fread(fl, sizeof(int), nzone, f) != nzone) {
+    fprintf(stderr, "harness: bad %s\n", in);
+    return 3;
+  }
+  fclose(f);
+  for (z = 0; z < nzone; z++) pf[z * NUMPFLAGS + FLAGUTOPRIMFAIL] = fl[z];
+  post_fixup(STAGEM1, p, p, finalstep);
+  for (z = 0; z < nzone; z++) fl[z] = pf[z * NUMPFLAGS + FLAGUTOPRIMFAIL];
+  f = fopen(out, "wb");
+  if (!f || fwrite(a_p, sizeof(a_p), 1, f) != 1 || fwrite(fl, sizeof(int), nzone, f) != nzone) {
+    fprintf(stderr, "harness: cannot write %s\n", out);
+    return 3;
+  }
+  fclose(f);
+  free(fl);
+  return 0;
+}
+
 int main(int argc, char *argv[])
 {
   char *fakeargv[2];
@@ -343,6 +377,15 @@ int main(int argc, char *argv[])
       return 1;
     }
     return invert_file(argv[2], argv[3]);
+  }
+  if (argc == 5 && strcmp(argv[1], "--postfixup") == 0) {
+    fakeargv[0] = argv[0];
+    fakeargv[1] = NULL;
+    if (init(1, fakeargv) >= 1) {
+      fprintf(stderr, "harness: init failed\n");
+      return 1;
+    }
+    return postfixup_file(argv[2], argv[3], atoi(argv[4]));
   }
 
   while (argc >= 2 && strncmp(argv[1], "--", 2) == 0) {

@@ -16,6 +16,12 @@ from oracle.pyoracle import CENT
 RHO, UU, U1 = 0, 1, 2
 GAMMAPERCDIFFMAX, UPERCDIFFMAX = 2.0, 10.0
 GAMMAPERC, UPERC = 12, 13
+# failure codes drawn into crafted states: every code the reference's
+# fixup_utoprim accepts (fixup.c:1346-1425) ...
+REF_FAIL_CODES = [1, 1, 1, 2, 5, 8, 9, 10, 11, 12, 13, 14, 15, 101]
+# ... and the set the GPU test draws, which adds -1 (UTOPRIMFAILFIXED, a code
+# fixup_utoprim writes but rejects on input) to compare the device's
+# handling of it with the oracle's
 FAIL_CODES = [1, 1, 1, 9, 10, 11, 12, 13, 14, 15, -1]
 
 
@@ -135,7 +141,7 @@ def device_scheme(flags, gam, uu, n, g, s, rng, jacobi=False):
     return out, len(deplist)
 
 
-def craft(pr, seed):
+def craft(pr, seed, codes=FAIL_CODES):
     """Overwrite pr.p / pr.pflag with a seeded state rich in candidates:
     Lorentz factors from 1.1 to 9 (u~^1 alone, sized by g_11 at the zone
     centre), internal energies over four decades, failure codes on a quarter
@@ -151,6 +157,6 @@ def craft(pr, seed):
     pr.p[..., RHO] = 10.0 ** rng.uniform(-2.0, 0.0, size=nt)
     pr.p[..., UU] = pr.p[..., RHO] * 10.0 ** rng.uniform(-4.0, 0.0, size=nt)
     fail = rng.random(nt) < 0.25
-    pr.pflag[...] = np.where(fail, rng.choice(FAIL_CODES, size=nt), 0).astype(np.int32)
+    pr.pflag[...] = np.where(fail, rng.choice(codes, size=nt), 0).astype(np.int32)
     pr.p = np.ascontiguousarray(pr.p)
     pr.pflag = np.ascontiguousarray(pr.pflag)

@@ -17,7 +17,7 @@ import pytest
 
 from harm_finalwham_b200.gpu import HarmGPU
 from oracle.pyoracle import Oracle
-from tests.checksol_model import craft, sequential
+from tests.checksol_model import FAIL_CODES, REF_FAIL_CODES, craft, sequential
 from tests.fixtures import load
 
 pytestmark = pytest.mark.gpu
@@ -25,13 +25,17 @@ pytestmark = pytest.mark.gpu
 CASES = [("torus2d_16x16_mc_hll", 1), ("torus2d_16x16_mc_hll", 0), ("torus3d_12x12x6_mc_hll", 1)]
 
 
+@pytest.mark.parametrize("codes", ["reference", "with_fixed"])
 @pytest.mark.parametrize("name,finalstep", CASES)
-def test_post_fixup_matches_oracle_on_crafted_states(name, finalstep):
+def test_post_fixup_matches_oracle_on_crafted_states(name, finalstep, codes):
+    # "reference": the failure codes the reference's fixup_utoprim accepts,
+    # where the oracle's post_fixup is pinned to the reference's own
+    # (tests/test_checksol_order.py); "with_fixed" adds -1
     orc = Oracle()
     order_dependent = 0
     for seed in range(6):
         pr, _ = load(name)
-        craft(pr, 1000 + seed)
+        craft(pr, 1000 + seed, REF_FAIL_CODES if codes == "reference" else FAIL_CODES)
         # the sequential loop against an order-free pass (every neighbour's
         # original flag): where they differ, the visiting order matters
         _, gam = orc.checksolution(pr.copy())
