@@ -266,6 +266,9 @@ class Oracle:
                                      ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_int), ctypes.c_int,
                                      ctypes.POINTER(ctypes.c_double)]
         L.hgo_post_fixup.restype = ctypes.c_int
+        L.hgo_bound_prim.argtypes = [ctypes.POINTER(hgo_config), ctypes.POINTER(hgo_geometry),
+                                     ctypes.POINTER(ctypes.c_double)]
+        L.hgo_bound_prim.restype = ctypes.c_int
         L.hgo_checksolution.argtypes = [ctypes.POINTER(hgo_config), ctypes.POINTER(hgo_geometry),
                                         ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_int),
                                         ctypes.POINTER(ctypes.c_double)]
@@ -315,6 +318,12 @@ class Oracle:
         u = getattr(pr, "u", None)
         return self.lib.hgo_post_fixup(ctypes.byref(pr.config()), ctypes.byref(self.geometry(pr)), _dp(pr.p),
                                        _ip(pr.pflag), int(finalstep), _dp(u) if u is not None else None)
+
+    def bound_prim(self, pr):
+        """bound_prim (the problem file's boundaries) on pr.p in place;
+        returns the error bits."""
+        assert pr.p.flags.c_contiguous
+        return self.lib.hgo_bound_prim(ctypes.byref(pr.config()), ctypes.byref(self.geometry(pr)), _dp(pr.p))
 
     def checksolution(self, pr):
         """fixup_checksolution (fixup.c:460-560) alone on pr.pflag in place;

@@ -65,6 +65,11 @@
  *   finalstep) (fixup.c:37-96: bound_pflag, fixup_checksolution,
  *   fixup_utoprim) and writes the two arrays back to <outfile> in the same
  *   form.
+ *
+ * usage: harm_ref --boundprim <infile> <outfile>
+ *   the same for the reference's own bound_prim(STAGEM1, p) (the problem
+ *   file's boundaries, e.g. bounds.fishmon.c:29-345 with the inflow check
+ *   of fixup.c:2271); <infile> and <outfile> hold the p array only.
  */
 #include "defs.h"  /* defines the reference globals, as the reference main.c does */
 #include <sys/stat.h>
@@ -362,6 +367,24 @@ static int postfixup_file(const char *in, const char *out, int finalstep)
   return 0;
 }
 
+static int boundprim_file(const char *in, const char *out)
+{
+  FILE *f = fopen(in, "rb");
+  if (!f || fread(a_p, sizeof(a_p), 1, f) != 1) {
+    fprintf(stderr, "harness: bad %s\n", in);
+    return 3;
+  }
+  fclose(f);
+  bound_prim(STAGEM1, p);
+  f = fopen(out, "wb");
+  if (!f || fwrite(a_p, sizeof(a_p), 1, f) != 1) {
+    fprintf(stderr, "harness: cannot write %s\n", out);
+    return 3;
+  }
+  fclose(f);
+  return 0;
+}
+
 int main(int argc, char *argv[])
 {
   char *fakeargv[2];
@@ -386,6 +409,15 @@ int main(int argc, char *argv[])
       return 1;
     }
     return postfixup_file(argv[2], argv[3], atoi(argv[4]));
+  }
+  if (argc == 4 && strcmp(argv[1], "--boundprim") == 0) {
+    fakeargv[0] = argv[0];
+    fakeargv[1] = NULL;
+    if (init(1, fakeargv) >= 1) {
+      fprintf(stderr, "harness: init failed\n");
+      return 1;
+    }
+    return boundprim_file(argv[2], argv[3]);
   }
 
   while (argc >= 2 && strncmp(argv[1], "--", 2) == 0) {

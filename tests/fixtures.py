@@ -103,3 +103,48 @@ def summarise(p_active, pflag_active, stride):
 def load_record(name):
     d = np.load(os.path.join(RECORDS, name + ".npz"))
     return {k: d[k] for k in d.files}
+
+
+def reference_on_state(exe, tmp, mode, pr, args=(), with_flags=False):
+    """Run the reference build `exe` (oracle/ref_harness.c --postfixup /
+    --boundprim) on the state of `pr` and return its arrays cropped to pr's
+    layout: p, or (p, FLAGUTOPRIMFAIL flags) with `with_flags`.  The init
+    dump of `exe` in tmp/init gives the reference's
+    own array shape (reference_problem writes it); its outer ghosts beyond
+    pr's keep init's values."""
+    import subprocess
+
+    from oracle.pyoracle import RefDump
+    rd = RefDump(os.path.join(tmp, "init"))
+    off = tuple(b - g for b, g in zip(rd.bnd, pr.g))
+    sl = tuple(slice(o, o + nt) for o, nt in zip(off, pr.nt))
+    p_ref = rd.p("init").copy()
+    p_ref[sl] = pr.p
+    fin, fout = os.path.join(tmp, "in.bin"), os.path.join(tmp, "out.bin")
+    with open(fin, "wb") as f:
+        f.write(np.ascontiguousarray(p_ref).tobytes())
+        if with_flags:
+            f_ref = np.zeros(rd.NM, dtype=np.int32)
+            f_ref[sl] = pr.pflag
+            f.write(f_ref.tobytes())
+    if os.path.exists(fout):
+        os.remove(fout)
+    r = subprocess.run([exe, mode, fin, fout] + [str(a) for a in args], cwd=tmp, capture_output=True, text=True)
+    assert r.returncode == 0 and os.path.exists(fout), r.stderr[-400:]
+    raw = np.fromfile(fout, dtype=np.uint8)
+    nb = p_ref.nbytes
+    p_out = raw[:nb].view(np.float64).reshape(p_ref.shape)[sl]
+    if not with_flags:
+        return p_out
+    return p_out, raw[nb:].view(np.int32).reshape(rd.NM)[sl]
+
+
+def reference_problem(exe, tmp, ng=3):
+    """The initial state of the reference build `exe` as a Problem with ng
+    ghosts (runs its init into tmp/init)."""
+    import subprocess
+
+    from oracle.pyoracle import RefDump
+    out = os.path.join(tmp, "init")
+    subprocess.run([exe, out, "0"], cwd=tmp, check=True, stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL)
+    return RefDump(out).to_problem(ng, "init")

@@ -96,40 +96,19 @@ def test_oracle_post_fixup_matches_reference_on_crafted_states(build, finalstep)
     # --postfixup) on the candidate-rich states the GPU test uses: pins the
     # oracle there, beyond what the stepped fixtures reach
     import os
-    import subprocess
     import tempfile
 
-    from oracle.pyoracle import LIBDIR, RefDump
+    from oracle.pyoracle import LIBDIR
+    from tests.fixtures import reference_on_state, reference_problem
     exe = os.path.join(LIBDIR, build)
     if not os.path.exists(exe):
         pytest.skip("reference binary not built (__graft_entry__.build builds it where the reference tree is)")
     orc = Oracle()
     with tempfile.TemporaryDirectory() as tmp:
-        out = os.path.join(tmp, "init")
-        subprocess.run([exe, out, "0"], cwd=tmp, check=True, stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL)
-        rd = RefDump(out)
         for seed in range(3):
-            pr = rd.to_problem(3, "init")
+            pr = reference_problem(exe, tmp)
             craft(pr, 4000 + seed, REF_FAIL_CODES)
-            # the crafted state inside the reference's arrays (its outer
-            # ghosts keep init's values: nothing here reads them)
-            off = tuple(b - g for b, g in zip(rd.bnd, pr.g))
-            sl = tuple(slice(o, o + nt) for o, nt in zip(off, pr.nt))
-            p_ref = rd.p("init").copy()
-            f_ref = np.zeros(rd.NM, dtype=np.int32)
-            p_ref[sl] = pr.p
-            f_ref[sl] = pr.pflag
-            fin, fout = os.path.join(tmp, "in.bin"), os.path.join(tmp, "out.bin")
-            with open(fin, "wb") as f:
-                f.write(np.ascontiguousarray(p_ref).tobytes())
-                f.write(np.ascontiguousarray(f_ref).tobytes())
-            r = subprocess.run([exe, "--postfixup", fin, fout, str(finalstep)], cwd=tmp, capture_output=True,
-                               text=True)
-            assert r.returncode == 0 and os.path.exists(fout), r.stderr[-400:]
-            raw = np.fromfile(fout, dtype=np.uint8)
-            nb = p_ref.nbytes
-            p_out = raw[:nb].view(np.float64).reshape(p_ref.shape)[sl]
-            f_out = raw[nb:].view(np.int32).reshape(rd.NM)[sl]
+            p_out, f_out = reference_on_state(exe, tmp, "--postfixup", pr, (finalstep,), with_flags=True)
             q = pr.copy()
             assert orc.post_fixup(q, finalstep) == 0
             assert np.array_equal(q.pflag, f_out), f"seed {seed}: {np.count_nonzero(q.pflag != f_out)} flags differ"
