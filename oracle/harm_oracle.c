@@ -2478,6 +2478,24 @@ int hgo_post_fixup(const hgo_config *c, const hgo_geometry *g, double *p, int *p
   return d.err;
 }
 
+/* fluxcalc (flux.c:7-318) with flux_ct (fluxct.c:10) on p: F1..F3 receive
+   the face fluxes the update reads (others untouched), ndt[0..2] the three
+   directions' dt estimates */
+int hgo_fluxcalc(const hgo_config *c, const hgo_geometry *g, const double *p, double *F1, double *F2, double *F3,
+                 double *ndt)
+{
+  dom d;
+  scratch sc;
+  dom_init(&d, c, g);
+  if (alloc_scratch(&d, &sc)) return -1;
+  fluxcalc_dir(&d, p, 1, F1, sc.dq, &ndt[0]);
+  fluxcalc_dir(&d, p, 2, F2, sc.dq, &ndt[1]);
+  fluxcalc_dir(&d, p, 3, F3, sc.dq, &ndt[2]);
+  flux_ct(&d, F1, F2, F3, sc.emf);
+  free_scratch(&sc);
+  return d.err;
+}
+
 /* fixup_checksolution (fixup.c:460-560) alone on p and pflag; gammacheck
    (may be NULL) receives the Lorentz factors it compares, zone layout */
 int hgo_checksolution(const hgo_config *c, const hgo_geometry *g, const double *p, int *pflag, double *gammacheck)

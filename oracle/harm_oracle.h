@@ -121,6 +121,12 @@ int hgo_utoprim_batch_v(const double *U, const double *gcov, const double *gcon,
    scheme on a final step it receives the diag_fixup corrections. */
 int hgo_post_fixup(const hgo_config *c, const hgo_geometry *g, double *p, int *pflag, int finalstep, double *unew);
 
+/* fluxcalc (flux.c:7-318) including flux_ct (fluxct.c:10) on p: F1..F3
+   (zone layout x NPR) receive the face fluxes the update reads, the others
+   are left as they were; ndt[0..2] the per-direction dt estimates. */
+int hgo_fluxcalc(const hgo_config *c, const hgo_geometry *g, const double *p, double *F1, double *F2, double *F3,
+                 double *ndt);
+
 /* fixup_checksolution (fixup.c:460-560) alone: pflag in place; gammacheck
    (may be NULL, else zone layout) receives the Lorentz factors compared. */
 int hgo_checksolution(const hgo_config *c, const hgo_geometry *g, const double *p, int *pflag, double *gammacheck);

@@ -266,6 +266,9 @@ class Oracle:
                                      ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_int), ctypes.c_int,
                                      ctypes.POINTER(ctypes.c_double)]
         L.hgo_post_fixup.restype = ctypes.c_int
+        L.hgo_fluxcalc.argtypes = [ctypes.POINTER(hgo_config), ctypes.POINTER(hgo_geometry)] + \
+            [ctypes.POINTER(ctypes.c_double)] * 5
+        L.hgo_fluxcalc.restype = ctypes.c_int
         L.hgo_bound_prim.argtypes = [ctypes.POINTER(hgo_config), ctypes.POINTER(hgo_geometry),
                                      ctypes.POINTER(ctypes.c_double)]
         L.hgo_bound_prim.restype = ctypes.c_int
@@ -318,6 +321,16 @@ class Oracle:
         u = getattr(pr, "u", None)
         return self.lib.hgo_post_fixup(ctypes.byref(pr.config()), ctypes.byref(self.geometry(pr)), _dp(pr.p),
                                        _ip(pr.pflag), int(finalstep), _dp(u) if u is not None else None)
+
+    def fluxcalc(self, pr, fill=0.0):
+        """fluxcalc + flux_ct on pr.p: (error bits, [F1, F2, F3], [ndt1, ndt2,
+        ndt3]); faces the update does not read keep `fill`."""
+        assert pr.p.flags.c_contiguous
+        F = [np.full(pr.p.shape, fill) for _ in range(3)]
+        ndt = np.zeros(3)
+        e = self.lib.hgo_fluxcalc(ctypes.byref(pr.config()), ctypes.byref(self.geometry(pr)), _dp(pr.p), _dp(F[0]),
+                                  _dp(F[1]), _dp(F[2]), _dp(ndt))
+        return e, F, list(ndt)
 
     def bound_prim(self, pr):
         """bound_prim (the problem file's boundaries) on pr.p in place;

@@ -70,6 +70,12 @@
  *   the same for the reference's own bound_prim(STAGEM1, p) (the problem
  *   file's boundaries, e.g. bounds.fishmon.c:29-345 with the inflow check
  *   of fixup.c:2271); <infile> and <outfile> hold the p array only.
+ *
+ * usage: harm_ref --fluxcalc <infile> <outfile>
+ *   the reference's own fluxcalc(STAGEM1, p, F1, F2, F3, 1.0, &ndt1, &ndt2,
+ *   &ndt3) (flux.c:7: reconstruction, wave speeds, Riemann fluxes and
+ *   flux_ct) on the p of <infile>; <outfile>: F1, F2, F3 (each N1M x N2M x
+ *   N3M x NPR doubles, zeros for a direction of one zone) then ndt1..3.
  */
 #include "defs.h"  /* defines the reference globals, as the reference main.c does */
 #include <sys/stat.h>
@@ -107,6 +113,8 @@ static double sm_uniform(void)
 extern int fixup(int stage, FTYPE (*pv)[N2M][N3M][NPR], int finalstep);
 extern int pre_fixup(int stage, FTYPE (*pv)[N2M][N3M][NPR]);
 extern int bound_prim(int boundstage, FTYPE prim[][N2M][N3M][NPR]);
+extern int fluxcalc(int stage, FTYPE pr[][N2M][N3M][NPR], FTYPE F1[][N2M][N3M][NPR], FTYPE F2[][N2M][N3M][NPR],
+                    FTYPE F3[][N2M][N3M][NPR], FTYPE CUf, FTYPE *ndt1, FTYPE *ndt2, FTYPE *ndt3);
 extern int set_dt(FTYPE (*prim)[N2M][N3M][NPR], SFTYPE *dt);
 extern int init_conservatives(FTYPE p[][N2M][N3M][NPR], FTYPE Utemp[][N2M][N3M][NPR], FTYPE U[][N2M][N3M][NPR]);
 extern void coord(int i, int j, int k, int loc, FTYPE *X);
@@ -385,6 +393,44 @@ static int boundprim_file(const char *in, const char *out)
   return 0;
 }
 
+static int fluxcalc_file(const char *in, const char *out)
+{
+  const size_t nf = (size_t)N1M * N2M * N3M * NPR;
+  double *zero = (double *)calloc(nf, sizeof(double));
+  FTYPE ndt[3] = {0.0, 0.0, 0.0};
+  FILE *f = fopen(in, "rb");
+  if (!zero || !f || fread(a_p, sizeof(a_p), 1, f) != 1) {
+    fprintf(stderr, "harness: bad %s\n", in);
+    return 3;
+  }
+  fclose(f);
+  fluxcalc(STAGEM1, p, F1, F2, F3, 1.0, &ndt[0], &ndt[1], &ndt[2]);
+  f = fopen(out, "wb");
+  if (!f) {
+    fprintf(stderr, "harness: cannot write %s\n", out);
+    return 3;
+  }
+#if(N1>1)
+  fwrite(a_F1, sizeof(a_F1), 1, f);
+#else
+  fwrite(zero, sizeof(double), nf, f);
+#endif
+#if(N2>1)
+  fwrite(a_F2, sizeof(a_F2), 1, f);
+#else
+  fwrite(zero, sizeof(double), nf, f);
+#endif
+#if(N3>1)
+  fwrite(a_F3, sizeof(a_F3), 1, f);
+#else
+  fwrite(zero, sizeof(double), nf, f);
+#endif
+  fwrite(ndt, sizeof(FTYPE), 3, f);
+  fclose(f);
+  free(zero);
+  return 0;
+}
+
 int main(int argc, char *argv[])
 {
   char *fakeargv[2];
@@ -418,6 +464,15 @@ int main(int argc, char *argv[])
       return 1;
     }
     return boundprim_file(argv[2], argv[3]);
+  }
+  if (argc == 4 && strcmp(argv[1], "--fluxcalc") == 0) {
+    fakeargv[0] = argv[0];
+    fakeargv[1] = NULL;
+    if (init(1, fakeargv) >= 1) {
+      fprintf(stderr, "harness: init failed\n");
+      return 1;
+    }
+    return fluxcalc_file(argv[2], argv[3]);
   }
 
   while (argc >= 2 && strncmp(argv[1], "--", 2) == 0) {
