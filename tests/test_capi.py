@@ -91,6 +91,7 @@ def test_split_entry_points_reject_bad_arguments_without_gpu_work():
     assert L.hgpu_stats_read(None, None) == HGPU_E_INVALID
     assert L.hgpu_stage_advance(None, 0) == HGPU_E_INVALID
     assert L.hgpu_stage_fixup(None, 0) == HGPU_E_INVALID
+    assert L.hgpu_post_fixup(None, 1, None) == HGPU_E_INVALID
     assert L.hgpu_dt_probe(None) == HGPU_E_INVALID
     assert L.hgpu_step_end(None, 1) == HGPU_E_INVALID
     assert L.hgpu_ndt_pack(None, ctypes.addressof(buf)) == HGPU_E_INVALID
